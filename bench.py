@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Throughput of the PySpectral RK4 step on B200.
+
+Metric: grid-point x RK4-steps per second (N^3 * steps / s) of a 64^3 LES of
+decaying isotropic turbulence, FP32 fields with Kahan-compensated stage
+accumulation, next to the plain FP64 path of the same closure.  One step is
+one full RK4 step (four RHS evaluations and stage updates) over the whole
+grid.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value: K steps timed with CUDA events on the launching stream, state
+  resident in HBM, L2 flushed (256 MiB write) before every timed step and
+  excluded from the timing; max over ranks; whole-job aggregate.
+* e2e: the same metric through the public API with the state copied from
+  pinned host memory before every step and the new state read back after it.
+* roofline: dominant kernel of the step, its compulsory bytes per launch over
+  its CUDA-event duration, against MEASURED_PEAKS.json.
+* cpu_baseline: the NumPy oracle port (FP64, scipy.fft with all host cores),
+  a bounded sample of the same workload, rank 0 at N=1 only.
+* --impl reference: the reference's CPU implementation of the path (the
+  oracle port of it; the reference itself is not present on the GPU box),
+  same config and metric, rank 0 only.
+
+Multi-GPU: one independent replica per GPU (the runs do not exchange data),
+``scaling: weak``; launch with torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "grid-pt·RK4-steps/s at 64^3 LES: learned/FP32 vs plain FP64, same E(k) error"
+UNIT = "grid-pt·RK4-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--N", type=int, default=64)
+    ap.add_argument("--closure", choices=["smag", "dns"], default="smag")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(", ") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = []
+        maxm = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                maxm = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": maxm, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": maxm, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_state(N, seed):
+    from pyspectral_b200.initial_conditions import isotropic_state
+    return isotropic_state(N, seed, k0=4.0)
+
+
+def cpu_baseline(N, closure, budget_s):
+    """Oracle port timed on the host cores: steps of the same workload until
+    the budget is spent (at least one)."""
+    import numpy as np
+    from oracle import spectral_oracle as orc
+    cores = os.cpu_count() or 1
+    orc.set_workers(cores)
+    g = orc.Grid.periodic(N)
+    st = orc.isotropic_state(N, 1, k0=4.0)
+    p = orc.Params(nu=1e-3)
+    fn = orc.rhs_smag if closure == "smag" else orc.rhs_nosgs
+    t0 = time.perf_counter()
+    n = 0
+    Q = st
+    while True:
+        Q, _ = orc.advance_rk4(Q, lambda q: (fn(g, q, p)[0], None), 2e-3)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    assert np.isfinite(Q).all()
+    return {"value": N ** 3 * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} RK4 steps of {N}^3 {closure} FP64 (NumPy oracle, scipy.fft workers={cores}) in {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    # a bounded sample: one warm-up step, then steps until ~60 s of host work
+    # (at most --steps), so the whole run ends within a couple of minutes
+    cpu_baseline(args.N, args.closure, 0.0)
+    cb = cpu_baseline(args.N, args.closure, min(60.0, max(args.cpu_seconds, 1.0) * max(1, min(args.steps, 5))))
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.N}^3 decaying isotropic LES, {args.closure}, RK4 dt=2e-3 "
+                                   f"(reference CPU path: NumPy oracle port)", "N": args.N},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from pyspectral_b200 import _capi
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advance
+
+    N = args.N
+    tm = 1 if args.closure == "smag" else 0
+    code = _capi.SMAG if tm == 1 else _capi.DNS
+    st64 = make_state(N, 1 + rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def build(precision):
+        grid = C.gridclass.periodic(N, device=local)
+        main = C.variables(0, tm, 0, 0, 0, 0, grid, st64[0], st64[1], st64[2], 0.0, 2e-3, 1e-3,
+                           precision=precision)
+        grid.ctx(precision).prepare(code)
+        return grid, main
+
+    def timed(grid, main, K, W):
+        ctx = grid.ctx(main.precision)
+        for _ in range(W):
+            advance(main, grid, 1)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        l0 = ctx.launch_count()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        for k in range(K):
+            flush.zero_()
+            ev[k][0].record()
+            advance(main, grid, 1)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        launches = ctx.launch_count() - l0
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        if dist is not None:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches
+
+    # FP32 + Kahan (headline) and the plain FP64 path of the same closure
+    grid32, m32 = build(32)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ms32, launches = timed(grid32, m32, args.steps, args.warmup)
+    clocks = sampler.stop() if sampler else None
+    grid64, m64 = build(64)
+    ms64, _ = timed(grid64, m64, max(1, args.steps // 2), args.warmup)
+    ok = grid32.ctx(32).count_nonfinite(m32.Q) == 0 and grid64.ctx(64).count_nonfinite(m64.Q) == 0
+    value = world * N ** 3 * args.steps / (ms32 / 1e3)
+    value64 = world * N ** 3 * max(1, args.steps // 2) / (ms64 / 1e3)
+
+    # e2e through the public API: pinned host state -> device, step, device -> host
+    ctx = grid32.ctx(32)
+    host = torch.empty_like(m32.Q, device="cpu").pin_memory()
+    host.copy_(m32.Q.cpu())
+    hostc = torch.empty_like(m32.comp, device="cpu").pin_memory()
+    hostc.copy_(m32.comp.cpu())
+    out = torch.empty_like(host).pin_memory()
+    Ke = max(10, args.steps // 4)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(Ke):
+        m32.Q.copy_(host, non_blocking=True)
+        m32.comp.copy_(hostc, non_blocking=True)
+        advance(m32, grid32, 1)
+        out.copy_(m32.Q, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * N ** 3 * Ke / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(host.numel() * host.element_size() * 2),
+           "d2h_bytes_per_step": int(out.numel() * out.element_size())}
+
+    # live per-kernel timing of 3 flushed steps for the roofline
+    ctx.timing(True)
+    for _ in range(3):
+        flush.zero_()
+        advance(m32, grid32, 1)
+    recs = ctx.timing_records()
+    ctx.timing(False)
+    per = {}
+    for name, ms, by in recs:
+        a = per.setdefault(name, [0, 0.0, 0.0])
+        a[0] += 1
+        a[1] += ms
+        a[2] += by
+    dom = max(per.items(), key=lambda kv: kv[1][1])
+    n_l, tot_ms, tot_b = dom[1]
+    pk, pk_kind = peaks()
+    achieved = (tot_b / n_l) / (tot_ms / n_l / 1e3) / 1e9
+    step_ms = sum(v[1] for v in per.values()) / 3.0
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": pk, "unit": "GB/s",
+                "frac": achieved / pk, "peak_kind": pk_kind, "traffic": None,
+                "bytes_per_launch": tot_b / n_l, "avg_launch_ms": tot_ms / n_l,
+                "share_of_step": tot_ms / 3.0 / step_ms,
+                "kernels": {k: {"launches_per_step": v[0] / 3, "ms_per_step": v[1] / 3,
+                                "GBps": (v[2] / v[1] * 1e3 / 1e9) if v[1] > 0 else None} for k, v in per.items()}}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(traffic_file):
+        try:
+            tf = json.load(open(traffic_file))
+            roofline["traffic"] = tf.get(dom[0], {}).get(f"N{N}_f32")
+        except Exception:
+            pass
+
+    if rank == 0:
+        cb = cpu_baseline(N, args.closure, args.cpu_seconds) if world == 1 else None
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{N}^3 decaying isotropic LES (E(k)~k^4 exp(-2k^2/k0^2), k0=4), "
+                                   f"{args.closure} closure, RK4 dt=2e-3, nu=1e-3, FP32 fields + Kahan stage "
+                                   f"accumulation; learned closure not built yet", "N": N,
+                       "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "fp64_plain": {"value": value64, "ms_per_step": ms64 / max(1, args.steps // 2),
+                           "ratio_f32_over_f64": value / value64},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clocks,
+            "gpu_launches": int(launches), "finite": bool(ok),
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        rank, world, _ = dist_env()
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

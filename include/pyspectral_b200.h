@@ -1,0 +1,151 @@
+/*
+ * pyspectral_b200 -- C ABI of the B200-native PySpectral right-hand-side and
+ * RK4 path.
+ *
+ * Plain pointers and sizes only.  Every field argument is a DEVICE pointer to
+ * a dense array of `nfields` spectra laid out (nfields, N1, N2, N3/2+1),
+ * complex interleaved (re, im), FP64 or FP32 according to the context's
+ * precision.  All work is queued on the context's stream; functions that
+ * return host scalars synchronise that stream.  Every entry point returns a
+ * status code (PSB_OK on success) and never aborts; psb_last_error() gives
+ * the message.  A context is not thread-safe: use one per host thread/stream.
+ *
+ * Paths in citations are relative to the PySpectral project.
+ */
+#ifndef PYSPECTRAL_B200_H
+#define PYSPECTRAL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PSB_OK 0
+#define PSB_ERR_ARG 1         /* null pointer / bad value */
+#define PSB_ERR_SHAPE 2       /* unsupported grid size */
+#define PSB_ERR_CUDA 3        /* a CUDA call failed */
+#define PSB_ERR_UNSUPPORTED 4 /* closure/precision combination not built */
+#define PSB_ERR_NONFINITE 6   /* NaN/Inf detected by psb_check_finite */
+
+/* ---- closures: the reference's turb_model switch
+ *      (src/Classes.py:28-229, src_MPI/Classes.py:59-149) ----------------- */
+#define PSB_DNS 0         /* turb_model 0      -> computeRHS_NOSGS  (src/RHSfunctions.py:3-50)    */
+#define PSB_SMAG 1        /* turb_model 1      -> computeRHS_SMAG   (src/RHSfunctions.py:146-237)  */
+#define PSB_TMODEL 2      /* turb_model 2      -> computeRHS_tmodel (src/RHSfunctions.py:240-363)  */
+#define PSB_TAU_STATIC 3  /* 'Static tau-model'  (src/RHSfunctions.py:366-497)                       */
+#define PSB_TAU_DYNAMIC 4 /* 'Dynamic tau-model' (src/RHSfunctions.py:592-878)                       */
+#define PSB_MHD 5         /* 'MHD' of the MPI solver (src_MPI/RHSfunctions.py:95-175)                */
+
+/* ---- diagnostic flags --------------------------------------------------- */
+#define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
+#define PSB_NORM_MPI 1      /* divide by (N1*N2*N3)^2  (src_MPI/Classes.py:269-285)  */
+#define PSB_FILTER_GF 2     /* apply the sharp cutoff Gf first (src/Classes.py:584-588) */
+
+typedef struct psb_ctx psb_ctx;
+
+/* gridclass(N1,N2,N3,x,y,z,kc,L1,L2,L3) (src/Classes.py:548-588).  dx,dy,dz
+ * are the spacings of the caller's coordinate arrays (Delta=(dx dy dz)^(1/3)). */
+typedef struct {
+  int N1, N2, N3;
+  double L1, L2, L3;
+  double dx, dy, dz;
+  int kc;
+} psb_grid;
+
+/* Run parameters carried by the reference's `variables` object
+ * (src/Classes.py:8-26, defaults src/PySpec_3d.py:9-72). */
+typedef struct {
+  double nu;           /* viscosity */
+  double eta;          /* magnetic diffusivity; <0 -> nu (src_MPI/Classes.py:95) */
+  double t;            /* time, frozen across the four stages (src/PySpec_3d.py:122) */
+  double dt;           /* time step */
+  double Ct;           /* t-model constant (src/Classes.py:103-108) */
+  double tau_a, tau_b; /* static tau-model tau = max(0, tau_a + tau_b t) (src/Classes.py:194-195) */
+  int kf;              /* dynamic tau test-filter wavenumber; 0 -> int(kc*2/3) (src/Classes.py:131) */
+  int rotate;          /* Coriolis on/off (src/RHSfunctions.py:33-36,47-50) */
+  double Om1, Om2, Om3;
+  const void* force;   /* MHD: constant forcing spectra, 3 fields, or NULL (src_MPI/Classes.py:91-94) */
+} psb_params;
+
+/* FFTclass + gridclass construction (src/Classes.py:548-625; src/PySpec_3d.py:79-80).
+ * precision: 32 or 64.  N1,N2,N3 must be multiples of 4 whose 3/2 and 2x
+ * padded sizes factor as 2^a 3^b (8,12,16,24,32,48,64,96,128,192,256,...). */
+int psb_ctx_create(const psb_grid* grid, int precision, int device, psb_ctx** out);
+int psb_ctx_destroy(psb_ctx* ctx);
+/* Stream (cudaStream_t) on which the context queues its work; NULL = legacy default. */
+int psb_ctx_set_stream(psb_ctx* ctx, void* stream);
+/* Message of the last failure on this context ("" if none). */
+const char* psb_last_error(const psb_ctx* ctx);
+/* Message of the last psb_ctx_create failure (no context exists then). */
+const char* psb_create_error(void);
+
+/* One right-hand-side evaluation: main.computeRHS(main,grid,myFFT,utilities)
+ * (src/Classes.py:44,95,124,186,227; src_MPI/Classes.py:147).
+ * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD).
+ * w0       : optional closure force main.w0_u/v/w (3 fields) or NULL.
+ * read_out : optional copy of the state as the RHS read it (the reference
+ *            rebinds main.uhat/vhat/what to it, src/RHSfunctions.py:10-12;
+ *            the MPI solver dealiases it in place, src_MPI/RHSfunctions.py:102-107).
+ * tau_out  : optional host scalar main.tau (tau-models; src/RHSfunctions.py:480,857). */
+int psb_rhs(psb_ctx* ctx, int closure, const void* state, void* rhs, void* w0, void* read_out,
+            const psb_params* p, double* tau_out);
+
+/* nsteps of advanceQ_RK4 (src/PySpec_3d.py:96-105; src_MPI/time_schemes.py:2-7):
+ * Q <- Q0 + dt*c_i*RHS(Q), c = [1/4,1/3,1/2,1], in place on `state`.
+ * comp     : Kahan compensation array (same shape as state) for FP32 runs, or NULL.
+ * read_out : optional; receives the state read by the LAST stage of the LAST
+ *            step (the reference's per-step diagnostics read main.uhat,
+ *            src/PySpec_3d.py:129).  dt is fixed (cfl<=0 in compute_dt).
+ * For an unsupported graph-captured first call see psb_prepare. */
+int psb_step_rk4(psb_ctx* ctx, int closure, void* state, void* comp, void* read_out, const psb_params* p,
+                 int nsteps);
+
+/* Allocate the context's scratch for `closure` now (so that a later call can
+ * be captured in a CUDA graph without allocating). */
+int psb_prepare(psb_ctx* ctx, int closure);
+
+/* ---- diagnostics (FP64 results on the host) ----------------------------- */
+/* computeEnergy / computeEnergy_resolved (src/Classes.py:652-676), MPI
+ * computeEnergy / computeMHDEnergy (src_MPI/Classes.py:269-303). 3 fields. */
+int psb_energy(psb_ctx* ctx, const void* fields3, int flags, double* out);
+/* computeEnstrophy (src/Classes.py:733-744; src_MPI/Classes.py:350-368). */
+int psb_enstrophy(psb_ctx* ctx, const void* fields3, int flags, double* out);
+/* Cross-helicity <u.B> with the MPI energy weighting (no reference counterpart). */
+int psb_cross_helicity(psb_ctx* ctx, const void* u3, const void* b3, int flags, double* out);
+/* computeSpectrum / computeSpectrum_resolved (src/Classes.py:762-797,825-844):
+ * out[nbins*3] (row-major [bin][component]), int8 shell index with the
+ * reference's wrap-around.  nbins must be the reference's kmax+1
+ * (psb_spectrum_nbins). */
+int psb_spectrum(psb_ctx* ctx, const void* fields3, int flags, double* out, int nbins);
+int psb_spectrum_nbins(const psb_ctx* ctx, int flags, int* nbins);
+/* MPI computeSpectrum / computeMHDSpectrum (src_MPI/Classes.py:370-448):
+ * out[nbins] summed over components, int16 shells, k3=N/2 included. */
+int psb_spectrum_mpi(psb_ctx* ctx, const void* fields3, double* out, int nbins);
+/* compute_dt (src/Classes.py:687-698): CFL time step for cfl>0, else -cfl. */
+int psb_cfl_dt(psb_ctx* ctx, const void* fields3, double cfl, double nu, double* dt_out);
+/* computeSGS_DNS (src/Classes.py:861-929): w0 (3 fields) and optional tauhat (6 fields). */
+int psb_sgs_dns(psb_ctx* ctx, const void* fields3, void* w0, void* tau6);
+
+/* ---- transforms and setup ----------------------------------------------- */
+/* numpy rfftn (unnormalised) of nfields physical fields (N1,N2,N3) real. */
+int psb_fft_r2c(psb_ctx* ctx, const void* phys, void* spec, int nfields);
+/* numpy irfftn (1/(N1N2N3)-normalised) of nfields spectra. */
+int psb_fft_c2r(psb_ctx* ctx, const void* spec, void* phys, int nfields);
+/* Count of non-finite values in n complex entries -> *count (0 = all finite). */
+int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* count);
+
+/* ---- launch accounting and per-kernel timing (no reference counterpart;
+ *      the reference only prints wall time, src/PySpec_3d.py:107,136,144) --- */
+/* Number of kernels this context has launched since creation. */
+int psb_launch_count(const psb_ctx* ctx, unsigned long long* n);
+/* Turn per-launch CUDA-event timing on/off; either call clears the records. */
+int psb_timing_enable(psb_ctx* ctx, int on);
+/* Synchronise the stream and return the number of timed launches. */
+int psb_timing_count(psb_ctx* ctx, int* n);
+/* Record i: kernel name, device time (ms) and compulsory HBM bytes of the launch. */
+int psb_timing_get(psb_ctx* ctx, int i, char* name, int name_len, double* ms, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYSPECTRAL_B200_H */

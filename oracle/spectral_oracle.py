@@ -1,0 +1,770 @@
+"""CPU oracle for the PySpectral right-hand-side evaluation and RK4 step.
+
+TEST INFRASTRUCTURE ONLY.  This module is the parity checker: only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` may import
+it.  The product path (``pyspectral_b200``) never calls it and fails loudly when
+its CUDA library is missing.
+
+It is a from-scratch NumPy restatement of the reference algorithm, written in
+FP64 (complex128 / float64) like the reference.  Each function cites the
+reference file and lines it restates; paths are relative to the PySpectral
+project (``PySpectral/src`` is the serial solver, ``PySpectral/src_MPI`` the MPI
+solver that carries the MHD equations).
+
+Parity is pinned: ``tests/test_oracle_golden.py`` checks every routine here
+against fixtures produced by executing the unmodified reference sources
+(``tests/golden/make_golden.py``) and against the reference's own known-answer
+energy history (``run/TGV_Validate100/benchmark_sol_64.npz``).
+
+State layout used throughout: ``state[f, i1, i2, i3]`` complex128 with shape
+``(nfields, N1, N2, N3//2+1)``; field order u, v, w (then B1, B2, B3 for MHD).
+The reference keeps the same three spectra in the diagonal of a stride-3 array
+``Q[0::3,0::3,0::3]`` (``PySpectral/src/Classes.py:30-34``); the dense layout
+here holds the identical numbers.
+"""
+from __future__ import annotations
+
+import math
+import os
+
+import numpy as np
+
+try:  # pocketfft with threads when SciPy is present; NumPy otherwise
+    import scipy.fft as _fft
+
+    def _rfftn(a, workers=None):
+        return _fft.rfftn(a, workers=workers or _WORKERS)
+
+    def _irfftn(a, s, workers=None):
+        return _fft.irfftn(a, s=s, workers=workers or _WORKERS)
+except Exception:  # pragma: no cover
+    def _rfftn(a, workers=None):
+        return np.fft.rfftn(a)
+
+    def _irfftn(a, s, workers=None):
+        return np.fft.irfftn(a, s=s)
+
+_WORKERS = 1
+
+
+def set_workers(n: int) -> None:
+    """Number of FFT worker threads (the reference's ``nthreads``)."""
+    global _WORKERS
+    _WORKERS = max(1, int(n))
+
+
+# --------------------------------------------------------------------------
+# Grid / wavenumbers                      PySpectral/src/Classes.py:548-588
+# --------------------------------------------------------------------------
+class Grid:
+    """Wavenumber arrays of ``gridclass`` (``src/Classes.py:548-588``).
+
+    ``dx, dy, dz`` are the spacings of the caller's x, y, z arrays
+    (``:561-564``); ``Delta=(dx dy dz)^(1/3)`` (``:581-582``).  ``ksqr`` carries
+    the reference's ``+1e-50`` (``:576``)."""
+
+    def __init__(self, N1, N2, N3, dx, dy, dz, kc, L1=2 * np.pi, L2=2 * np.pi, L3=2 * np.pi):
+        self.N1, self.N2, self.N3 = N1, N2, N3
+        self.L1, self.L2, self.L3 = L1, L2, L3
+        self.dx, self.dy, self.dz = dx, dy, dz
+        self.kc = kc
+        k1 = np.fft.fftshift(np.linspace(-(N1 // 2), N1 // 2 - 1, N1)) * 2.0 * np.pi / L1
+        k2 = np.fft.fftshift(np.linspace(-(N2 // 2), N2 // 2 - 1, N2)) * 2.0 * np.pi / L2
+        k3 = np.linspace(0, N3 // 2, N3 // 2 + 1) * 2.0 * np.pi / L3
+        k1f = np.fft.fftshift(np.linspace(-N1, N1 - 1, 2 * N1)) * 2.0 * np.pi / L1
+        k2f = np.fft.fftshift(np.linspace(-N2, N2 - 1, 2 * N2)) * 2.0 * np.pi / L2
+        k3f = np.linspace(0, N3, N3 + 1) * 2.0 * np.pi / L3
+        self.k1d, self.k2d, self.k3d = k1, k2, k3
+        self.k1fd, self.k2fd, self.k3fd = k1f, k2f, k3f
+        self.k2, self.k1, self.k3 = np.meshgrid(k2, k1, k3)
+        self.k2f, self.k1f, self.k3f = np.meshgrid(k2f, k1f, k3f)
+        self.ksqr = self.k1 * self.k1 + self.k2 * self.k2 + self.k3 * self.k3 + 1.0e-50
+        self.ksqr_i = 1.0 / self.ksqr
+        self.ksqrf = self.k1f * self.k1f + self.k2f * self.k2f + self.k3f * self.k3f + 1.0e-50
+        self.ksqrf_i = 1.0 / self.ksqrf
+        self.Delta = (dx * dy * dz) ** (1.0 / 3.0)
+        # sharp spectral cutoff at kc, Nyquist index excluded (:584-588)
+        Gf = np.zeros(self.k1.shape)
+        Gf[0:kc, 0:kc, 0:kc] = 1
+        Gf[0:kc, N2 - kc + 1:, 0:kc] = 1
+        Gf[N1 - kc + 1:, 0:kc, 0:kc] = 1
+        Gf[N1 - kc + 1:, N2 - kc + 1:, 0:kc] = 1
+        self.Gf = Gf
+
+    @classmethod
+    def periodic(cls, N, kc=None, L=2 * np.pi):
+        """Cube with the exactly periodic spacing ``dx = L/N``."""
+        return cls(N, N, N, L / N, L / N, L / N, N // 2 if kc is None else kc, L, L, L)
+
+
+# --------------------------------------------------------------------------
+# Padding / truncation                     PySpectral/src/padding.py
+# --------------------------------------------------------------------------
+def pad(uhat):
+    """3/2 zero padding, ``src/padding.py:16-25``.  Copies the four corner
+    blocks; index N/2 of axes 0 and 1 and the k3=N/2 plane are dropped."""
+    N1, N2, N3h = uhat.shape
+    h1, h2 = N1 // 2, N2 // 2
+    M1, M2 = 3 * N1 // 2, 3 * N2 // 2
+    out = np.zeros((M1, M2, N3h + (N3h - 1) // 2), dtype=complex)
+    z = slice(0, N3h - 1)
+    out[0:h1, 0:h2, z] = uhat[0:h1, 0:h2, z]
+    out[0:h1, M2 - h2 + 1:, z] = uhat[0:h1, h2 + 1:, z]
+    out[M1 - h1 + 1:, 0:h2, z] = uhat[h1 + 1:, 0:h2, z]
+    out[M1 - h1 + 1:, M2 - h2 + 1:, z] = uhat[h1 + 1:, h2 + 1:, z]
+    return out
+
+
+def unpad(upad):
+    """Inverse of :func:`pad`, ``src/padding.py:2-13``."""
+    M1, M2, M3h = upad.shape
+    N1, N2 = int(M1 * 2.0 / 3.0), int(M2 * 2.0 / 3.0)
+    N3h = int(M3h * 2.0 / 3.0 + 1)
+    h1, h2 = N1 // 2, N2 // 2
+    out = np.zeros((N1, N2, N3h), dtype=complex)
+    z = slice(0, N3h - 1)
+    out[0:h1, 0:h2, z] = upad[0:h1, 0:h2, z]
+    out[0:h1, h2 + 1:, z] = upad[0:h1, M2 - h2 + 1:, z]
+    out[h1 + 1:, 0:h2, z] = upad[M1 - h1 + 1:, 0:h2, z]
+    out[h1 + 1:, h2 + 1:, z] = upad[M1 - h1 + 1:, M2 - h2 + 1:, z]
+    return out
+
+
+def pad_2x(uhat):
+    """2x zero padding, ``src/padding.py:41-49`` (keeps index N/2 of axes 0,1
+    as the -N/2 mode; drops k3=N/2)."""
+    N1, N2, N3h = uhat.shape
+    h1, h2 = N1 // 2, N2 // 2
+    out = np.zeros((2 * N1, 2 * N2, 2 * N3h - 1), dtype=complex)
+    z = slice(0, N3h - 1)
+    out[0:h1, 0:h2, z] = uhat[0:h1, 0:h2, z]
+    out[0:h1, 2 * N2 - h2:, z] = uhat[0:h1, h2:, z]
+    out[2 * N1 - h1:, 0:h2, z] = uhat[h1:, 0:h2, z]
+    out[2 * N1 - h1:, 2 * N2 - h2:, z] = uhat[h1:, h2:, z]
+    return out
+
+
+def unpad_2x(upad):
+    """Inverse of :func:`pad_2x`, ``src/padding.py:28-38``."""
+    M1, M2, M3h = upad.shape
+    N1, N2, N3h = M1 // 2, M2 // 2, (M3h + 1) // 2
+    h1, h2 = N1 // 2, N2 // 2
+    out = np.zeros((N1, N2, N3h), dtype=complex)
+    z = slice(0, N3h - 1)
+    out[0:h1, 0:h2, z] = upad[0:h1, 0:h2, z]
+    out[0:h1, h2:, z] = upad[0:h1, 2 * N2 - h2:, z]
+    out[h1:, 0:h2, z] = upad[2 * N1 - h1:, 0:h2, z]
+    out[h1:, h2:, z] = upad[2 * N1 - h1:, 2 * N2 - h2:, z]
+    return out
+
+
+def separate_modes(upad):
+    """Resolved/unresolved split on the 2x grid, ``src/padding.py:67-79``:
+    p = {|k1|,|k2| < N/2, 0 <= k3 < N/2}; q = the rest (Nyquist included)."""
+    M1, M2, M3h = upad.shape
+    N1, N2, N3h = M1 // 2, M2 // 2, (M3h + 1) // 2
+    p = np.zeros_like(upad)
+    z = slice(0, M3h - N3h)
+    a1, b1 = slice(0, N1 // 2), slice(M1 - N1 // 2 + 1, M1)
+    a2, b2 = slice(0, N2 // 2), slice(M2 - N2 // 2 + 1, M2)
+    for s1 in (a1, b1):
+        for s2 in (a2, b2):
+            p[s1, s2, z] = upad[s1, s2, z]
+    return p, upad - p
+
+
+def separate_modes_testfilter(upad, kf):
+    """Test-filter split on the 2x grid, ``src/padding.py:52-64``:
+    p = {|k1|,|k2| < kf, 0 <= k3 < kf}."""
+    M1, M2, _ = upad.shape
+    p = np.zeros_like(upad)
+    z = slice(0, kf)
+    for s1 in (slice(0, kf), slice(M1 - kf + 1, M1)):
+        for s2 in (slice(0, kf), slice(M2 - kf + 1, M2)):
+            p[s1, s2, z] = upad[s1, s2, z]
+    return p, upad - p
+
+
+# --------------------------------------------------------------------------
+# Transforms                               PySpectral/src/Classes.py:590-625
+# --------------------------------------------------------------------------
+def scale_32(g):
+    """``scale`` of ``FFTclass`` (``src/Classes.py:593``)."""
+    return math.sqrt((3.0 / 2.0) ** 3 * math.sqrt(g.N1 * g.N2 * g.N3))
+
+
+def scale_2x(g):
+    """``scale`` of the 2x-padded closures (``src/RHSfunctions.py:244``)."""
+    return math.sqrt(2.0 ** 3 * math.sqrt(g.N1 * g.N2 * g.N3))
+
+
+def ifft32(g, X):
+    """``ifftT_obj``: c2r on the 3/2 grid with 1/M normalisation
+    (pyFFTW ``normalise_idft=True``), ``src/Classes.py:596-599``."""
+    return _irfftn(X, s=(3 * g.N1 // 2, 3 * g.N2 // 2, 3 * g.N3 // 2))
+
+
+def fft32(x):
+    """``fft_obj``: unnormalised r2c, ``src/Classes.py:601-605``."""
+    return _rfftn(x)
+
+
+def ifft2x(g, X):
+    """``ifftT_obj2`` on the 2x grid, ``src/Classes.py:607-610``."""
+    return _irfftn(X, s=(2 * g.N1, 2 * g.N2, 2 * g.N3))
+
+
+def fft2x(x):
+    """``fft_obj2``, ``src/Classes.py:612-615``."""
+    return _rfftn(x)
+
+
+def nyquist_zero(uhat):
+    """``unpad(pad(uhat))`` as applied on read at ``src/RHSfunctions.py:10-12``."""
+    return unpad(pad(uhat))
+
+
+def _coriolis_pressure(k1, k2, k3, ksqr_i, u, v, w, Om):
+    Om1, Om2, Om3 = Om
+    return -2.0 * ksqr_i * 1j * (k1 * (v * Om3 - w * Om2) + k2 * (w * Om1 - u * Om3)
+                                 + k3 * (u * Om2 - v * Om1))
+
+
+def _coriolis_force(u, v, w, Om):
+    Om1, Om2, Om3 = Om
+    return (2.0 * (v * Om3 - w * Om2), 2.0 * (w * Om1 - u * Om3), 2.0 * (u * Om2 - v * Om1))
+
+
+class Params:
+    """Run parameters carried by the reference's ``variables`` object
+    (``src/Classes.py:8-26``) and its driver defaults (``src/PySpec_3d.py:9-72``)."""
+
+    def __init__(self, nu, t=0.0, dt=0.0, rotate=0, Om=(0.0, 0.0, 0.0), Ct=0.1,
+                 tau_a=0.0, tau_b=0.0, kf=None):
+        self.nu, self.t, self.dt = nu, t, dt
+        self.rotate, self.Om = rotate, tuple(Om)
+        self.Ct, self.tau_a, self.tau_b, self.kf = Ct, tau_a, tau_b, kf
+
+
+# --------------------------------------------------------------------------
+# Right-hand sides                          PySpectral/src/RHSfunctions.py
+# --------------------------------------------------------------------------
+def _products_32(g, u, v, w):
+    """The six 3/2-dealiased quadratic products (``src/RHSfunctions.py:14-23``)."""
+    s = scale_32(g)
+    ur = ifft32(g, pad(u)) * s
+    vr = ifft32(g, pad(v)) * s
+    wr = ifft32(g, pad(w)) * s
+    return [unpad(fft32(a * b)) for a, b in ((ur, ur), (vr, vr), (wr, wr), (ur, vr), (ur, wr), (vr, wr))]
+
+
+def _pressure(k1, k2, k3, ksqr_i, uu, vv, ww, uv, uw, vw):
+    return ksqr_i * (-k1 * k1 * uu - k2 * k2 * vv - k3 * k3 * ww - 2.0 * k1 * k2 * uv
+                     - 2.0 * k1 * k3 * uw - 2.0 * k2 * k3 * vw)
+
+
+def _advection(k1, k2, k3, nu, ksqr, phat, P, u, v, w):
+    uu, vv, ww, uv, uw, vw = P
+    ru = -1j * k1 * uu - 1j * k2 * uv - 1j * k3 * uw - 1j * k1 * phat - nu * ksqr * u
+    rv = -1j * k1 * uv - 1j * k2 * vv - 1j * k3 * vw - 1j * k2 * phat - nu * ksqr * v
+    rw = -1j * k1 * uw - 1j * k2 * vw - 1j * k3 * ww - 1j * k3 * phat - nu * ksqr * w
+    return ru, rv, rw
+
+
+def rhs_nosgs(g, state, p):
+    """DNS right-hand side, ``computeRHS_NOSGS`` (``src/RHSfunctions.py:3-50``).
+
+    Returns ``(rhs, uhat_read)``; ``uhat_read`` is the Nyquist-zeroed state the
+    reference rebinds to ``main.uhat`` (``:10-12``)."""
+    u, v, w = (nyquist_zero(state[i]) for i in range(3))
+    P = _products_32(g, u, v, w)
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    phat = _pressure(k1, k2, k3, g.ksqr_i, *P)
+    if p.rotate == 1:
+        phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, u, v, w, p.Om)
+    r = list(_advection(k1, k2, k3, p.nu, g.ksqr, phat, P, u, v, w))
+    if p.rotate == 1:
+        c = _coriolis_force(u, v, w, p.Om)
+        r = [r[i] + c[i] for i in range(3)]
+    return np.stack(r), np.stack([u, v, w])
+
+
+def _sgs_divergence(g, tau):
+    """Projected divergence of a stress, ``src/RHSfunctions.py:215-222``
+    (identical form at ``src/Classes.py:917-927``).  Note the reference's
+    projection term is ``1j*k_i * (1j*ksqr_i*k_m k_j tau_jm)``."""
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    t11, t22, t33, t12, t13, t23 = tau
+    proj = 1j * g.ksqr_i * (k1 * k1 * t11 + k2 * k2 * t22 + k3 * k3 * t33 + 2.0 * k1 * k2 * t12
+                            + 2.0 * k1 * k3 * t13 + 2.0 * k2 * k3 * t23)
+    w0u = -1j * k1 * t11 - 1j * k2 * t12 - 1j * k3 * t13 + 1j * k1 * proj
+    w0v = -1j * k1 * t12 - 1j * k2 * t22 - 1j * k3 * t23 + 1j * k2 * proj
+    w0w = -1j * k1 * t13 - 1j * k2 * t23 - 1j * k3 * t33 + 1j * k3 * proj
+    return np.stack([w0u, w0v, w0w])
+
+
+def smag_stress(g, u, v, w):
+    """Smagorinsky stress in Fourier space, ``src/RHSfunctions.py:174-212``
+    (Cs = 0.16 fixed, ``:197``)."""
+    s = scale_32(g)
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    Shat = (1j * k1 * u, 1j * k2 * v, 1j * k3 * w, 0.5 * (1j * k2 * u + 1j * k1 * v),
+            0.5 * (1j * k3 * u + 1j * k1 * w), 0.5 * (1j * k3 * v + 1j * k2 * w))
+    S = [ifft32(g, pad(x) * s) for x in Shat]
+    S11, S22, S33, S12, S13, S23 = S
+    Smag = np.sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * S12 * S12 + 2.0 * S13 * S13
+                          + 2.0 * S23 * S23))
+    nut = 0.16 * g.Delta * 0.16 * g.Delta * np.abs(Smag)
+    return [unpad(fft32(-2.0 * nut * x)) for x in S]
+
+
+def rhs_smag(g, state, p):
+    """Smagorinsky right-hand side, ``computeRHS_SMAG``
+    (``src/RHSfunctions.py:146-237``).  No Nyquist re-zeroing on read.
+
+    Returns ``(rhs, w0)`` where ``w0`` is the SGS force (``main.w0_*``)."""
+    u, v, w = state[0], state[1], state[2]
+    P = _products_32(g, u, v, w)
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    phat = _pressure(k1, k2, k3, g.ksqr_i, *P)
+    if p.rotate == 1:
+        phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, u, v, w, p.Om)
+    w0 = _sgs_divergence(g, smag_stress(g, u, v, w))
+    r = list(_advection(k1, k2, k3, p.nu, g.ksqr, phat, P, u, v, w))
+    r = [r[i] + w0[i] for i in range(3)]
+    if p.rotate == 1:
+        c = _coriolis_force(u, v, w, p.Om)
+        r = [r[i] + c[i] for i in range(3)]
+    return np.stack(r), w0
+
+
+def _pl_2x(g, up, vp, wp, nu, rotate, Om):
+    """``PLu`` on the 2x grid (``src/RHSfunctions.py:269-315``): returns the
+    full-grid PL fields, the physical velocities and the 2x product spectra."""
+    s = scale_2x(g)
+    ur, vr, wr = ifft2x(g, up * s), ifft2x(g, vp * s), ifft2x(g, wp * s)
+    P = [fft2x(a * b) for a, b in ((ur, ur), (vr, vr), (wr, wr), (ur, vr), (ur, wr), (vr, wr))]
+    k1, k2, k3 = g.k1f, g.k2f, g.k3f
+    phat = _pressure(k1, k2, k3, g.ksqrf_i, *P)
+    if rotate == 1:
+        phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqrf_i, up, vp, wp, Om)
+    PL = _advection(k1, k2, k3, nu, g.ksqrf, phat, P, up, vp, wp)
+    return PL, (ur, vr, wr), P, phat
+
+
+def _plql(g, vel_real, PLq):
+    """``PLQLu`` from the q-part of PL (``src/RHSfunctions.py:321-352``
+    and ``:451-478``)."""
+    s = scale_2x(g)
+    ur, vr, wr = vel_real
+    qr = [ifft2x(g, x * s) for x in PLq]
+    # a[j][i] = unpad_2x(fft(u_j * PL_q,i))
+    a = [[unpad_2x(fft2x(vel * q)) for q in qr] for vel in (ur, vr, wr)]
+    up_u, up_v, up_w = a[0]
+    vp_u, vp_v, vp_w = a[1]
+    wp_u, wp_v, wp_w = a[2]
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    pterm = 2.0 * g.ksqr_i * (k1 * k1 * up_u + k2 * k2 * vp_v + k3 * k3 * wp_w
+                              + k1 * k2 * (up_v + vp_u) + k1 * k3 * (up_w + wp_u)
+                              + k2 * k3 * (vp_w + wp_v))
+    Lu = (-1j * k1 * up_u - 1j * k2 * vp_u - 1j * k3 * wp_u
+          - 1j * k1 * up_u - 1j * k2 * up_v - 1j * k3 * up_w + 1j * k1 * pterm)
+    Lv = (-1j * k1 * up_v - 1j * k2 * vp_v - 1j * k3 * wp_v
+          - 1j * k1 * vp_u - 1j * k2 * vp_v - 1j * k3 * vp_w + 1j * k2 * pterm)
+    Lw = (-1j * k1 * up_w - 1j * k2 * vp_w - 1j * k3 * wp_w
+          - 1j * k1 * wp_u - 1j * k2 * wp_v - 1j * k3 * wp_w + 1j * k3 * pterm)
+    return np.stack([Lu, Lv, Lw])
+
+
+def _memory_rhs(g, state, p, coef_fn):
+    """Shared body of the t-model and tau-models
+    (``src/RHSfunctions.py:240-363`` / ``:366-497``)."""
+    u, v, w = (nyquist_zero(state[i]) for i in range(3))
+    up, vp, wp = pad_2x(u), pad_2x(v), pad_2x(w)
+    PL, vel, P, phat = _pl_2x(g, up, vp, wp, p.nu, p.rotate, p.Om)
+    PLq = [separate_modes(x)[1] for x in PL]
+    PLQL = _plql(g, vel, PLq)
+    coef, extra = coef_fn(u, v, w, up, vp, wp, P, phat, PLQL)
+    w0 = coef * PLQL
+    r = [unpad_2x(PL[i]) + w0[i] for i in range(3)]
+    if p.rotate == 1:
+        c = _coriolis_force(u, v, w, p.Om)
+        r = [r[i] + c[i] for i in range(3)]
+    return np.stack(r), w0, np.stack([u, v, w]), PLQL, extra
+
+
+def rhs_tmodel(g, state, p):
+    """t-model, ``computeRHS_tmodel`` (``src/RHSfunctions.py:240-363``):
+    ``w0 = Ct * t * PLQLu``.  Returns ``(rhs, w0, uhat_read)``."""
+    r, w0, ur, _, _ = _memory_rhs(g, state, p, lambda *a: (p.Ct * p.t, None))
+    return r, w0, ur
+
+
+def rhs_staumodel(g, state, p):
+    """Static tau-model, ``computeRHS_staumodel`` (``src/RHSfunctions.py:366-497``):
+    ``tau = max(0, tau_a + tau_b*t)``.  Returns ``(rhs, w0, uhat_read, tau)``
+    with ``tau`` before the clamp (``main.tau``, ``:480``)."""
+    tau = p.tau_a + p.tau_b * p.t
+    r, w0, ur, _, _ = _memory_rhs(g, state, p, lambda *a: (max(0.0, tau), None))
+    return r, w0, ur, tau
+
+
+def test_filter_masks(g, kf):
+    """``test_filter`` / ``test_filter_2x`` masks, ``src/Classes.py:131-170``."""
+    f1 = (np.abs(g.k1d) < kf).astype(float)
+    f2 = (np.abs(g.k2d) < kf).astype(float)
+    f3 = (np.abs(g.k3d) < kf).astype(float)
+    F1 = (np.abs(g.k1fd) < kf).astype(float)
+    F2 = (np.abs(g.k2fd) < kf).astype(float)
+    F3 = (np.abs(g.k3fd) < kf).astype(float)
+    return (f1[:, None, None] * f2[None, :, None] * f3[None, None, :],
+            F1[:, None, None] * F2[None, :, None] * F3[None, None, :])
+
+
+def _weighted_dot(a, b, nk3):
+    """``sum(a[:,:,1:nk3]*conj(b[:,:,1:nk3]*2)) + sum(a[:,:,0]*conj(b[:,:,0]))``."""
+    return np.sum(a[:, :, 1:nk3] * np.conj(b[:, :, 1:nk3] * 2)) + np.sum(a[:, :, 0] * np.conj(b[:, :, 0]))
+
+
+def rhs_dtaumodel(g, state, p):
+    """Dynamic tau-model, ``computeRHS_Dtaumodel`` (``src/RHSfunctions.py:592-878``).
+
+    Returns ``(rhs, w0, uhat_read, tau)``; ``tau`` is ``main.tau`` before the
+    clamp (``:857-859``).  ``p.kf`` defaults to ``int(kc*2/3)``
+    (``src/Classes.py:131``)."""
+    kf = p.kf if p.kf is not None else int(g.kc * 2.0 / 3.0)
+    G, G2 = test_filter_masks(g, kf)
+    N3 = g.N3
+    NNN = g.N1 * g.N2 * g.N3
+    k1f, k2f, k3f = g.k1f, g.k2f, g.k3f
+
+    def coef(u, v, w, up, vp, wp, P, phat, PLQL):
+        uf, vf, wf = G * u, G * v, G * w
+        ufp, vfp, wfp = pad_2x(uf), pad_2x(vf), pad_2x(wf)
+        PLf, velf, Pf, phatf = _pl_2x(g, ufp, vfp, wfp, p.nu, p.rotate, p.Om)
+        PLqf = [separate_modes_testfilter(x, kf)[1] for x in PLf]
+        PLQLf = _plql(g, velf, PLqf)
+        uu, vv, ww, uv, uw, vw = P
+        fuu, fvv, fww, fuv, fuw, fvw = Pf
+        # Leonard-type term (:813-819); note the "+1j*k*phat" sign
+        Lu = G2 * (-1j * k1f * uu - 1j * k2f * uv - 1j * k3f * uw + 1j * k1f * phat) - \
+            G2 * (-1j * k1f * fuu - 1j * k2f * fuv - 1j * k3f * fuw + 1j * k1f * phatf)
+        Lv = G2 * (-1j * k1f * uv - 1j * k2f * vv - 1j * k3f * vw + 1j * k2f * phat) - \
+            G2 * (-1j * k1f * fuv - 1j * k2f * fvv - 1j * k3f * fvw + 1j * k2f * phatf)
+        Lw = G2 * (-1j * k1f * uw - 1j * k2f * vw - 1j * k3f * ww + 1j * k3f * phat) - \
+            G2 * (-1j * k1f * fuw - 1j * k2f * fvw - 1j * k3f * fww + 1j * k3f * phatf)
+        h = N3 // 2
+        LE = (_weighted_dot(Lu, ufp, h) + _weighted_dot(Lv, vfp, h) + _weighted_dot(Lw, wfp, h)) / NNN
+        PLQLE_filt = sum(_weighted_dot(G * PLQLf[i], x, h) for i, x in enumerate((uf, vf, wf))) / NNN
+        # the reference sums the *unfiltered* PLQL here (:846-852)
+        filt_PLQLE = sum(_weighted_dot(PLQL[i], x, h) for i, x in enumerate((uf, vf, wf))) / NNN
+        tau = np.abs(LE) / (np.abs(PLQLE_filt) - np.abs(filt_PLQLE) + 1.0e-5)
+        return max(0.0, tau), (tau, LE, PLQLE_filt, filt_PLQLE)
+
+    r, w0, ur, _, extra = _memory_rhs(g, state, p, coef)
+    return r, w0, ur, extra[0], extra
+
+
+# --------------------------------------------------------------------------
+# MHD (MPI solver, single rank)      PySpectral/src_MPI/RHSfunctions.py:95-175
+# --------------------------------------------------------------------------
+class MHDGrid:
+    """Single-rank ``gridclass`` of the MPI solver (``src_MPI/Classes.py:177-236``).
+    Wavenumbers are 1-D; the 2/3-rule masks follow ``:206-218`` exactly,
+    including the ``int((N3/2)*2/3)`` cut along k3."""
+
+    def __init__(self, N1, N2, N3, kc, L1=2 * np.pi, L2=2 * np.pi, L3=2 * np.pi, dx=None):
+        self.N1, self.N2, self.N3 = N1, N2, N3
+        self.L1, self.L2, self.L3 = L1, L2, L3
+        self.k1 = np.fft.fftshift(np.linspace(-(N1 // 2), N1 // 2 - 1, N1)) * 2.0 * np.pi / L1
+        self.k2 = np.fft.fftshift(np.linspace(-(N2 // 2), N2 // 2 - 1, N2)) * 2.0 * np.pi / L2
+        self.k3 = np.linspace(0, N3 // 2, N3 // 2 + 1) * 2.0 * np.pi / L3
+        self.ksqr = (self.k1[:, None, None] ** 2 + self.k2[None, :, None] ** 2
+                     + self.k3[None, None, :] ** 2 + 1.0e-50)
+        self.ksqr_i = 1.0 / self.ksqr
+        self.kc = kc
+        self.Delta = np.pi / kc
+        dx_ = np.ones(N1)
+        dy_ = np.ones(N2)
+        dz_ = np.ones(N3 // 2 + 1)
+        dx_[np.abs(self.k1) >= (N1 // 2) * 2.0 / 3.0 * 2.0 * np.pi / L1] = 0.0
+        dy_[np.abs(self.k2) >= (N2 // 2) * 2.0 / 3.0 * 2.0 * np.pi / L2] = 0.0
+        if N3 != 2:
+            dz_[int((N3 // 2) * 2.0 / 3.0):] = 0.0
+        self.dealias_mask = dx_[:, None, None] * dy_[None, :, None] * dz_[None, None, :]
+
+
+def mhd_forcing(g, x, y, z, kf=2, f0=0.25):
+    """Constant forcing of ``src_MPI/Classes.py:91-94`` (unnormalised rfftn)."""
+    f = np.zeros((3, g.N1, g.N2, g.N3 // 2 + 1), dtype=complex)
+    f[0] = np.fft.rfftn(f0 * np.sin(kf * x) * np.cos(kf * y) * np.cos(kf * z))
+    f[1] = np.fft.rfftn(-f0 * np.cos(kf * x) * np.sin(kf * y) * np.cos(kf * z))
+    return f
+
+
+def rhs_mhd(g, state, nu, force=None, eta=None):
+    """Incompressible MHD, ``computeRHS_MHD`` (``src_MPI/RHSfunctions.py:95-175``).
+
+    State is ``(u, v, w, B1, B2, B3)`` as unnormalised ``rfftn`` spectra;
+    ``eta`` defaults to ``nu`` (``main.lam = main.nu``, ``src_MPI/Classes.py:95``).
+    Returns ``(rhs, dealiased_state)``: the reference dealiases the six fields
+    in place (``:102-107``; ``dealias`` writes into its argument,
+    ``src_MPI/Classes.py:262-264``)."""
+    eta = nu if eta is None else eta
+    D = g.dealias_mask
+    s = [D * state[i] for i in range(6)]
+    shape = (g.N1, g.N2, g.N3)
+    u, v, w, B1, B2, B3 = (_irfftn(x, s=shape) for x in s)
+    NL = [_rfftn(a * b) for a, b in ((u, u), (v, v), (w, w), (u, v), (u, w), (v, w))]
+    uxB = [_rfftn(v * B3 - w * B2), _rfftn(w * B1 - u * B3), _rfftn(u * B2 - v * B1)]
+    MN = [_rfftn(a * b) for a, b in ((B1, B1), (B2, B2), (B3, B3), (B1, B2), (B1, B3), (B2, B3))]
+    k1 = g.k1[:, None, None]
+    k2 = g.k2[None, :, None]
+    k3 = g.k3[None, None, :]
+    phat = _pressure(k1, k2, k3, g.ksqr_i, *NL) - _pressure(k1, k2, k3, g.ksqr_i, *MN)
+    f = force if force is not None else np.zeros((3,) + g.ksqr.shape, dtype=complex)
+    n0, n1, n2, n3, n4, n5 = NL
+    m0, m1, m2, m3, m4, m5 = MN
+    r = np.empty((6,) + g.ksqr.shape, dtype=complex)
+    r[0] = D * (-1j * k1 * n0 - 1j * k2 * n3 - 1j * k3 * n4 + 1j * k1 * m0 + 1j * k2 * m3 + 1j * k3 * m4
+                - 1j * k1 * phat - nu * g.ksqr * s[0] + f[0])
+    r[1] = D * (-1j * k1 * n3 - 1j * k2 * n1 - 1j * k3 * n5 + 1j * k1 * m3 + 1j * k2 * m1 + 1j * k3 * m5
+                - 1j * k2 * phat - nu * g.ksqr * s[1] + f[1])
+    r[2] = D * (-1j * k1 * n4 - 1j * k2 * n5 - 1j * k3 * n2 + 1j * k1 * m4 + 1j * k2 * m5 + 1j * k3 * m2
+                - 1j * k3 * phat - nu * g.ksqr * s[2] + f[2])
+    r[3] = D * ((1j * k2 * uxB[2] - 1j * k3 * uxB[1]) - eta * g.ksqr * s[3])
+    r[4] = D * ((1j * k3 * uxB[0] - 1j * k1 * uxB[2]) - eta * g.ksqr * s[4])
+    r[5] = D * ((1j * k1 * uxB[1] - 1j * k2 * uxB[0]) - eta * g.ksqr * s[5])
+    return r, np.stack(s)
+
+
+# --------------------------------------------------------------------------
+# Time stepping                         PySpectral/src/PySpec_3d.py:96-105
+# --------------------------------------------------------------------------
+RK4_CONST = (1.0 / 4, 1.0 / 3, 1.0 / 2, 1.0)
+
+
+def advance_rk4(state, rhs_fn, dt):
+    """Low-storage 4-stage scheme ``Q = Q0 + dt*c_i*RHS(Q)``,
+    c = [1/4, 1/3, 1/2, 1] (``src/PySpec_3d.py:96-105``,
+    ``src_MPI/time_schemes.py:2-7``).  ``rhs_fn(Q)`` returns ``(rhs, read)``
+    where ``read`` is the field the RHS rebinds to ``main.uhat``; the value
+    of the last stage is returned with the new state because the reference's
+    per-step diagnostics read it (``src/PySpec_3d.py:129``)."""
+    Q0 = state.copy()
+    Q = state
+    read = None
+    for c in RK4_CONST:
+        rhs, read = rhs_fn(Q)
+        Q = Q0 + dt * c * rhs
+    return Q, read
+
+
+# --------------------------------------------------------------------------
+# Diagnostics                          PySpectral/src/Classes.py:652-929
+# --------------------------------------------------------------------------
+def energy(g, uvw):
+    """``computeEnergy`` (``src/Classes.py:652-659``): k3=N/2 plane excluded."""
+    h = g.N3 // 2
+    tot = sum(_weighted_dot(uvw[i], uvw[i], h) for i in range(3))
+    return float(np.real(0.5 * tot / (g.N1 * g.N2 * g.N3)))
+
+
+def energy_resolved(g, uvw):
+    """``computeEnergy_resolved`` (``src/Classes.py:666-676``)."""
+    return energy(g, np.stack([g.Gf * uvw[i] for i in range(3)]))
+
+
+def vorticity(g, uvw):
+    u, v, w = uvw
+    return (1j * g.k2 * w - 1j * g.k3 * v, 1j * g.k3 * u - 1j * g.k1 * w, 1j * g.k1 * v - 1j * g.k2 * u)
+
+
+def enstrophy(g, uvw):
+    """``computeEnstrophy`` (``src/Classes.py:733-744``)."""
+    h = g.N3 // 2
+    om = vorticity(g, uvw)
+    tot = sum(_weighted_dot(x, x, h) for x in om)
+    return float(np.real(0.5 * tot / (g.N1 * g.N2 * g.N3)))
+
+
+def all_stats(g, uvw, nu):
+    """``computeAllStats`` (``src/Classes.py:701-731``): returns
+    (enstrophy, energy, dissipation, lambda_k, tau_k, Re_lambda)."""
+    ens = enstrophy(g, uvw)
+    en = energy(g, uvw)
+    diss = 2 * ens * nu
+    lambda_k = (nu ** 3 / diss) ** 0.25
+    tau_k = (nu / diss) ** 0.5
+    Re_lambda = en * np.sqrt(20.0 / (3.0 * nu * diss))
+    return ens, en, diss, lambda_k, tau_k, Re_lambda
+
+
+def spectrum(g, uvw, filtered=False):
+    """``computeSpectrum`` (``src/Classes.py:762-797``) / ``computeSpectrum_resolved``
+    (``:825-844``).  Shell index ``int8(rint(|k|))`` with NumPy negative-index
+    wrap (the reference's int8 cast), k3=N/2 plane excluded.  Returns
+    ``(kdata, spectrum[kmax+1, 3])`` (complex, like the reference)."""
+    N1, N2, N3 = g.N1, g.N2, g.N3
+    h = N3 // 2
+    if filtered:
+        uvw = np.stack([g.Gf * uvw[i] for i in range(3)])
+    ks = ((g.k1 * g.L1 / (2 * np.pi)) ** 2 + (g.k2 * g.L2 / (2 * np.pi)) ** 2
+          + (g.k3 * g.L3 / (2 * np.pi)) ** 2)
+    km = np.rint(np.sqrt(ks[:, :, 1:h]))
+    k0 = np.rint(np.sqrt(ks[:, :, 0]))
+    kmax = int(np.round(np.amax(km)))
+    spec = np.zeros((kmax + 1, 3), dtype=complex)
+    bm = km.astype(np.int64).astype(np.int8).ravel()
+    b0 = k0.astype(np.int64).astype(np.int8).ravel()
+    for i in range(3):
+        np.add.at(spec[:, i], bm, (2 * uvw[i][:, :, 1:h] * np.conj(uvw[i][:, :, 1:h])).ravel())
+        np.add.at(spec[:, i], b0, (uvw[i][:, :, 0] * np.conj(uvw[i][:, :, 0])).ravel())
+    kdata = np.linspace(0, kmax, kmax + 1)
+    return kdata, spec / (N1 * N2 * N3)
+
+
+def compute_dt(g, uvw, cfl, nu, dt_prev):
+    """``compute_dt`` (``src/Classes.py:687-698``).  ``cfl <= 0`` means a fixed
+    ``dt = -cfl``."""
+    if cfl > 0:
+        n = math.sqrt(g.N1 * g.N2 * g.N3)
+        s = (g.N1, g.N2, g.N3)
+        u, v, w = (np.fft.irfftn(uvw[i], s=s, axes=(0, 1, 2)) * n for i in range(3))
+        max_vel = np.amax(np.abs(u) / g.dx + np.abs(v) / g.dy + np.abs(w) / g.dz)
+        dt = cfl / (max_vel + 1e-10)
+        if nu > 0:
+            dt = min(dt, 0.634 / (1.0 / g.dx ** 2 + 1.0 / g.dy ** 2 + 1.0 / g.dz ** 2) / nu * cfl / 1.35)
+        return dt
+    return -cfl
+
+
+def sgs_dns(g, uvw):
+    """``computeSGS_DNS`` (``src/Classes.py:861-929``): sharp-cutoff SGS stress
+    ``tau_ij = Gf*(u_i u_j)^ - (Gf u_i Gf u_j)^`` and its projected divergence.
+    Returns ``(w0[3], tauhat[6])``."""
+    s = scale_32(g)
+    u, v, w = uvw
+    uf, vf, wf = g.Gf * u, g.Gf * v, g.Gf * w
+    r = [ifft32(g, pad(x) * s) for x in (u, v, w)]
+    rf = [ifft32(g, pad(x) * s) for x in (uf, vf, wf)]
+    pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+    full = [unpad(fft32(r[a] * r[b])) for a, b in pairs]
+    filt = [unpad(fft32(rf[a] * rf[b])) for a, b in pairs]
+    tau = [g.Gf * full[i] - filt[i] for i in range(6)]
+    return _sgs_divergence(g, tau), np.stack(tau)
+
+
+def mhd_energy(g, fields3):
+    """``computeEnergy`` / ``computeMHDEnergy`` of the MPI solver
+    (``src_MPI/Classes.py:269-303``): normalised by (N1 N2 N3)^2."""
+    h = g.N3 // 2
+    tot = sum(_weighted_dot(fields3[i], fields3[i], h) for i in range(3))
+    return float(np.real(0.5 * tot)) / (g.N1 * g.N2 * g.N3) ** 2
+
+
+def mhd_spectrum(g, fields3):
+    """``computeSpectrum`` / ``computeMHDSpectrum`` of the MPI solver
+    (``src_MPI/Classes.py:370-448``): int16 shells, k3=N/2 included with
+    weight 2, normalised by (N1 N2 N3)^2."""
+    N1, N2, N3 = g.N1, g.N2, g.N3
+    k1 = (g.k1 * g.L1 / (2 * np.pi))[:, None, None]
+    k2 = (g.k2 * g.L2 / (2 * np.pi))[None, :, None]
+    k3 = (g.k3 * g.L3 / (2 * np.pi))[None, None, :]
+    kmag = np.sqrt(k1 ** 2 + k2 ** 2 + k3 ** 2)
+    E = sum(np.real(x * np.conj(x)) for x in fields3)
+    E = E.copy()
+    E[:, :, 1:] *= 2.0
+    kmax = int(np.round(np.sqrt((N1 // 2) ** 2 + (N2 // 2) ** 2 + (N3 // 2) ** 2)))
+    bins = np.round(kmag).astype(np.int16).astype(np.int64).ravel()
+    spec = np.bincount(bins, E.ravel(), minlength=kmax + 1)[:kmax + 1]
+    return np.linspace(0, kmax, kmax + 1), spec / (N1 * N2 * N3) ** 2
+
+
+def cross_helicity(g, uvw, B):
+    """Cross-helicity ``H_c = <u.B>`` with the MPI solver's energy weighting and
+    normalisation (no reference counterpart; defined like ``src_MPI/Classes.py:269-285``)."""
+    h = g.N3 // 2
+    tot = sum(_weighted_dot(uvw[i], B[i], h) for i in range(3))
+    return float(np.real(tot)) / (g.N1 * g.N2 * g.N3) ** 2
+
+
+# --------------------------------------------------------------------------
+# Initial conditions
+# --------------------------------------------------------------------------
+def periodic_coords(N, L=2 * np.pi):
+    """Exactly periodic grid ``x_i = L*i/N`` in the reference's meshgrid order
+    (``run/TGV_Validate100/inputfile.py:31-38`` uses an off-grid linspace)."""
+    a = np.arange(N) * (L / N)
+    y, x, z = np.meshgrid(a, a, a)
+    return x, y, z
+
+
+def tgv_state(N, variant="sin"):
+    """Taylor-Green vortex, ``uhat = rfftn(u)/sqrt(N^3)``
+    (``run/TGV_Validate100/inputfile.py:38-44``).  ``variant="sin"`` is
+    u=(sin x cos y cos z, -cos x sin y cos z, 0); ``"cos"`` the reference
+    script's (cos x sin y cos z, -sin x cos y cos z, 0)."""
+    x, y, z = periodic_coords(N)
+    if variant == "sin":
+        u = np.sin(x) * np.cos(y) * np.cos(z)
+        v = -np.cos(x) * np.sin(y) * np.cos(z)
+    else:
+        u = np.cos(x) * np.sin(y) * np.cos(z)
+        v = -np.sin(x) * np.cos(y) * np.cos(z)
+    w = np.zeros_like(u)
+    n = np.sqrt(N ** 3)
+    return np.stack([np.fft.rfftn(u) / n, np.fft.rfftn(v) / n, np.fft.rfftn(w) / n])
+
+
+def spectrum_k4(k, k0=4.0, u0=1.0):
+    """E(k) = 16 sqrt(2/pi) u0^2 k^4 / k0^5 exp(-2 (k/k0)^2)."""
+    return 16.0 * np.sqrt(2.0 / np.pi) * u0 ** 2 * k ** 4 / k0 ** 5 * np.exp(-2.0 * (k / k0) ** 2)
+
+
+def isotropic_phases(N, seed):
+    """Seeded phases theta1, theta2, phi drawn as in
+    ``run/HIT/MansourWray/inputfile.py:72-75`` (NumPy legacy seeding)."""
+    rs = np.random.RandomState(seed)
+    sh = (N, N, N // 2 + 1)
+    th1 = rs.rand(*sh) * 2.0 * np.pi
+    th2 = rs.rand(*sh) * 2.0 * np.pi
+    phi = rs.rand(*sh) * 2.0 * np.pi
+    return th1, th2, phi
+
+
+def isotropic_state(N, seed, k0=4.0, u0=1.0, L=2 * np.pi, phases=None, normalise="sqrtN3"):
+    """Random-phase solenoidal field from E(k) by the Craya-Herring construction
+    of ``run/HIT/MansourWray/inputfile.py:52-95``, with the spectrum
+    :func:`spectrum_k4`.  The raw construction is not Hermitian on the k3=0
+    plane, so it is symmetrised by a c2r/r2c round trip (as the MPI solver's
+    ``initDomain='Fourier'`` does, ``src_MPI/Classes.py:33-45``) and then
+    projected divergence-free.  ``normalise="sqrtN3"`` gives the serial
+    solver's ``uhat = rfftn(u)/sqrt(N^3)``; ``"none"`` the MPI solver's
+    unnormalised spectra."""
+    th1, th2, phi = phases if phases is not None else isotropic_phases(N, seed)
+    k1 = np.fft.fftshift(np.linspace(-(N // 2), N // 2 - 1, N))
+    k3 = np.linspace(0, N // 2, N // 2 + 1)
+    K2, K1, K3 = np.meshgrid(k1, k1, k3)
+    ksqr = K1 ** 2 + K2 ** 2 + K3 ** 2
+    kmag = np.sqrt(ksqr) + 1e-30
+    E = spectrum_k4(np.sqrt(ksqr), k0, u0)
+    alpha = np.sqrt(E / (4.0 * np.pi * ksqr + 1e-30)) * np.exp(1j * th1) * np.cos(phi)
+    beta = np.sqrt(E / (4.0 * np.pi * ksqr + 1e-30)) * np.exp(1j * th2) * np.sin(phi)
+    tp = 2.0 * np.pi / L
+    kperp = np.sqrt(K1 ** 2 + K2 ** 2)
+    uh = (alpha * kmag * K2 * tp + beta * K1 * tp * K3 * tp) / (kmag * kperp + 1e-30)
+    vh = (-alpha * kmag * K1 * tp + beta * K2 * tp * K3 * tp) / (kmag * kperp + 1e-30)
+    wh = -beta * kperp / kmag
+    n3 = N ** 3
+    st = np.stack([uh, vh, wh]) * np.sqrt(n3)
+    # Hermitian symmetrisation by a round trip (unit-normalised irfftn/rfftn)
+    st = np.stack([np.fft.rfftn(np.fft.irfftn(st[i], s=(N, N, N), axes=(0, 1, 2))) for i in range(3)])
+    # divergence-free projection
+    kk = (K1 * tp, K2 * tp, K3 * tp)
+    ks = kk[0] ** 2 + kk[1] ** 2 + kk[2] ** 2 + 1e-50
+    div = (kk[0] * st[0] + kk[1] * st[1] + kk[2] * st[2]) / ks
+    st = np.stack([st[i] - kk[i] * div for i in range(3)])
+    if normalise == "none":
+        return st * np.sqrt(n3)
+    return st

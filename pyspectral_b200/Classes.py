@@ -1,0 +1,269 @@
+"""Serial-solver objects with the reference's names and signatures.
+
+``gridclass``, ``FFTclass``, ``variables`` and ``utilitiesClass`` mirror
+PySpectral/src/Classes.py (:7-545, :548-588, :590-625, :631-1385) for the RHS /
+RK4 path.  State lives in CUDA tensors; every computation runs in
+libpyspectral_b200 through the C ABI (``_capi``).
+
+One layout difference: the reference packs uhat, vhat, what into the diagonal
+of a stride-3 array ``Q[i::3, i::3, i::3]`` (src/Classes.py:30-34).  Here
+``main.Q`` is the dense ``(3, N1, N2, N3//2+1)`` tensor holding the same three
+spectra; :func:`to_stride3` / :func:`from_stride3` convert for interop.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _capi
+
+TWO_PI = 2.0 * np.pi
+
+
+def _cdtype(precision):
+    return torch.complex128 if precision == 64 else torch.complex64
+
+
+def _to_dev(a, dtype, device):
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), device=device).to(dtype).contiguous()
+
+
+def to_stride3(Q):
+    """Dense (3,N1,N2,N3h) -> the reference's stride-3 ``Q`` (NumPy)."""
+    Q = Q.detach().cpu().numpy() if isinstance(Q, torch.Tensor) else np.asarray(Q)
+    _, N1, N2, N3h = Q.shape
+    out = np.zeros((3 * N1, 3 * N2, 3 * N3h), dtype=Q.dtype)
+    for i in range(3):
+        out[i::3, i::3, i::3] = Q[i]
+    return out
+
+
+def from_stride3(Q3):
+    """The reference's stride-3 ``Q`` -> dense (3,N1,N2,N3h)."""
+    return np.stack([Q3[i::3, i::3, i::3] for i in range(3)])
+
+
+class gridclass:
+    """``gridclass(N1,N2,N3,x,y,z,kc,L1,L2,L3)`` (src/Classes.py:548-588).
+
+    ``x, y, z`` are the caller's coordinate arrays; only their spacings are
+    used (``dx = x[1,0,0]-x[0,0,0]``, ``Delta = (dx dy dz)^(1/3)``).  The
+    wavenumber arrays of the reference are available as lazily built FP64
+    tensors (``k1``, ``k2``, ``k3``, ``ksqr``, ``Gf`` ...)."""
+
+    def __init__(self, N1, N2, N3, x, y, z, kc, L1=TWO_PI, L2=TWO_PI, L3=TWO_PI, device=0):
+        self.N1, self.N2, self.N3 = int(N1), int(N2), int(N3)
+        self.L1, self.L2, self.L3 = float(L1), float(L2), float(L3)
+        self.dx = float(x[1, 0, 0] - x[0, 0, 0])
+        self.dy = float(y[0, 1, 0] - y[0, 0, 0])
+        self.dz = float(z[0, 0, 1] - z[0, 0, 0])
+        self.x, self.y, self.z = x, y, z
+        self.kc = int(kc)
+        self.Delta = (self.dx * self.dy * self.dz) ** (1.0 / 3.0)
+        self.device = device
+        self._ctx = {}
+        self._tabs = None
+
+    @classmethod
+    def periodic(cls, N, kc=None, L=TWO_PI, device=0):
+        a = np.arange(N) * (L / N)
+        y, x, z = np.meshgrid(a, a, a)
+        return cls(N, N, N, x, y, z, N // 2 if kc is None else kc, L, L, L, device=device)
+
+    def ctx(self, precision=64) -> _capi.Context:
+        c = self._ctx.get(precision)
+        if c is None:
+            c = _capi.Context(self.N1, self.N2, self.N3, (self.L1, self.L2, self.L3), (self.dx, self.dy, self.dz),
+                              self.kc, precision, self.device)
+            self._ctx[precision] = c
+        return c
+
+    def _tables(self):
+        if self._tabs is None:
+            N1, N2, N3 = self.N1, self.N2, self.N3
+            k1 = np.fft.fftshift(np.linspace(-(N1 // 2), N1 // 2 - 1, N1)) * 2.0 * np.pi / self.L1
+            k2 = np.fft.fftshift(np.linspace(-(N2 // 2), N2 // 2 - 1, N2)) * 2.0 * np.pi / self.L2
+            k3 = np.linspace(0, N3 // 2, N3 // 2 + 1) * 2.0 * np.pi / self.L3
+            dev = torch.device("cuda", self.device)
+            K2, K1, K3 = np.meshgrid(k2, k1, k3)
+            self._tabs = {n: torch.as_tensor(a, device=dev) for n, a in
+                          (("k1", K1), ("k2", K2), ("k3", K3))}
+            ks = K1 * K1 + K2 * K2 + K3 * K3 + 1.0e-50
+            self._tabs["ksqr"] = torch.as_tensor(ks, device=dev)
+            self._tabs["ksqr_i"] = torch.as_tensor(1.0 / ks, device=dev)
+            kc = self.kc
+            Gf = np.zeros(K1.shape)
+            Gf[0:kc, 0:kc, 0:kc] = 1
+            Gf[0:kc, N2 - kc + 1:, 0:kc] = 1
+            Gf[N1 - kc + 1:, 0:kc, 0:kc] = 1
+            Gf[N1 - kc + 1:, N2 - kc + 1:, 0:kc] = 1
+            self._tabs["Gf"] = torch.as_tensor(Gf, device=dev)
+        return self._tabs
+
+    def __getattr__(self, name):
+        if name in ("k1", "k2", "k3", "ksqr", "ksqr_i", "Gf"):
+            return self._tables()[name]
+        raise AttributeError(name)
+
+
+class FFTclass:
+    """``FFTclass(N1,N2,N3,nthreads)`` (src/Classes.py:590-625).
+
+    The padded plans live in the grid's context; ``nthreads`` is accepted and
+    ignored.  ``scale`` is the reference's 3/2-padding scale."""
+
+    def __init__(self, N1, N2, N3, nthreads=1):
+        self.N1, self.N2, self.N3 = N1, N2, N3
+        self.nthreads = nthreads
+        self.scale = math.sqrt((3.0 / 2.0) ** 3 * math.sqrt(N1 * N2 * N3))
+
+
+class variables:
+    """``variables(weave,turb_model,rotate,Om1,Om2,Om3,grid,uhat,vhat,what,t,dt,nu,
+    Ct,dt0,dt0_subintegrations,dt1,dt1_subintegrations,cfl,dim)``
+    (src/Classes.py:7-229).
+
+    turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
+    'Dynamic tau-model'.  ``precision`` (64 or 32) selects FP64 or FP32
+    fields; FP32 runs carry a Kahan compensation array ``comp``."""
+
+    def __init__(self, weave, turb_model, rotate, Om1, Om2, Om3, grid, uhat, vhat, what, t, dt, nu, Ct=-10,
+                 dt0=-10, dt0_subintegrations=-10, dt1=-10, dt1_subintegrations=-10, cfl=None, dim=3,
+                 precision=64, kahan=None):
+        from . import RHSfunctions as R
+        self.turb_model = turb_model
+        self.rotate = int(rotate)
+        self.Om1, self.Om2, self.Om3 = float(Om1), float(Om2), float(Om3)
+        self.t = float(t)
+        self.dt = float(dt)
+        self.nu = float(nu)
+        self.cfl = -float(dt) if cfl is None else float(cfl)
+        self.precision = precision
+        self.grid = grid
+        self.kc = float(np.amax(np.fft.fftshift(np.linspace(-(grid.N1 // 2), grid.N1 // 2 - 1, grid.N1))
+                                * 2.0 * np.pi / grid.L1))
+        dev = torch.device("cuda", grid.device)
+        cd = _cdtype(precision)
+        self.Q = torch.stack([_to_dev(a, cd, dev) for a in (uhat, vhat, what)]).contiguous()
+        self.U = self.Q.clone()
+        self.nvars = 3
+        self.Ct = 0.1 if Ct == -10 else float(Ct)
+        self.tau_a, self.tau_b = float(dt0), float(dt1)
+        self.tau = 0.0
+        self.kf = None
+        use_kahan = (precision == 32) if kahan is None else bool(kahan)
+        self.comp = torch.zeros_like(self.Q) if use_kahan else None
+        self.W0 = None
+        table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
+                 "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel}
+        if turb_model not in table:
+            raise ValueError(f"turb_model {turb_model!r} is not on this path")
+        self.computeRHS = table[turb_model]
+        if turb_model != 0:
+            self.W0 = torch.zeros_like(self.Q)
+        if turb_model == "Dynamic tau-model":
+            self.kf = int(grid.kc * 2.0 / 3.0)
+        if turb_model == "Static tau-model":
+            self.kf = int(grid.kc / 2.0)
+
+    # views of the reference's per-component names
+    @property
+    def uhat(self):
+        return self.U[0]
+
+    @property
+    def vhat(self):
+        return self.U[1]
+
+    @property
+    def what(self):
+        return self.U[2]
+
+    @property
+    def w0_u(self):
+        return None if self.W0 is None else self.W0[0].unsqueeze(-1)
+
+    @property
+    def w0_v(self):
+        return None if self.W0 is None else self.W0[1].unsqueeze(-1)
+
+    @property
+    def w0_w(self):
+        return None if self.W0 is None else self.W0[2].unsqueeze(-1)
+
+    def U2Q(self):
+        self.Q.copy_(self.U)
+
+    def Q2U(self):
+        self.U.copy_(self.Q)
+
+    def params(self):
+        return _capi.make_params(nu=self.nu, t=self.t, dt=self.dt, Ct=self.Ct, tau_a=self.tau_a,
+                                 tau_b=self.tau_b, kf=self.kf or 0, rotate=self.rotate,
+                                 Om=(self.Om1, self.Om2, self.Om3))
+
+    def closure_code(self):
+        return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
+                "Dynamic tau-model": _capi.TAU_DYNAMIC}[self.turb_model]
+
+
+class utilitiesClass:
+    """Diagnostics of src/Classes.py:631-929 (FP64 reductions on the GPU)."""
+
+    def preAdvanceQ_hook(self, main, grid, myFFT):
+        pass
+
+    def postAdvanceQ_hook(self, main, grid, myFFT):
+        pass
+
+    def computeEnergy(self, main, grid):
+        return grid.ctx(main.precision).energy(main.U, _capi.NORM_SERIAL)
+
+    def computeEnergy_resolved(self, main, grid):
+        return grid.ctx(main.precision).energy(main.U, _capi.FILTER_GF)
+
+    def computeEnstrophy(self, main, grid):
+        return grid.ctx(main.precision).enstrophy(main.U, _capi.NORM_SERIAL)
+
+    def compute_dt(self, main, grid):
+        if main.cfl > 0:
+            main.dt = grid.ctx(main.precision).cfl_dt(main.U, main.cfl, main.nu)
+        else:
+            main.dt = -main.cfl
+
+    def computeAllStats(self, main, grid):
+        enstrophy = self.computeEnstrophy(main, grid)
+        energy = self.computeEnergy(main, grid)
+        dissipation = 2 * enstrophy * main.nu
+        lambda_k = (main.nu ** 3 / dissipation) ** 0.25
+        tau_k = (main.nu / dissipation) ** 0.5
+        Re_lambda = energy * np.sqrt(20.0 / (3.0 * main.nu * dissipation))
+        return enstrophy, energy, dissipation, lambda_k, tau_k, Re_lambda
+
+    def _spectrum(self, main, grid, flags):
+        spec = grid.ctx(main.precision).spectrum(main.U, flags)
+        return spec.astype(np.complex128)
+
+    def computeSpectrum(self, main, grid):
+        spec = self._spectrum(main, grid, _capi.NORM_SERIAL)
+        kmax = spec.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), spec
+
+    def computeSpectrum_resolved(self, main, grid):
+        spec = self._spectrum(main, grid, _capi.FILTER_GF)
+        N1, N2, N3 = grid.N1, grid.N2, grid.N3
+        i1 = np.fft.fftfreq(N1, 1.0 / N1)
+        i2 = np.fft.fftfreq(N2, 1.0 / N2)
+        i3 = np.arange(1, N3 // 2)
+        ks = i1[:, None, None] ** 2 + i2[None, :, None] ** 2 + i3[None, None, :] ** 2
+        k_m = np.unique(np.rint(np.sqrt(ks.ravel())))
+        return k_m, spec
+
+    def computeSGS_DNS(self, main, grid, myFFT):
+        w0 = torch.zeros_like(main.Q)
+        grid.ctx(main.precision).sgs_dns(main.U, w0)
+        return w0[0].unsqueeze(-1), w0[1].unsqueeze(-1), w0[2].unsqueeze(-1)

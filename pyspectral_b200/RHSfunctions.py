@@ -1,0 +1,67 @@
+"""Right-hand-side routines with the reference's names and signatures.
+
+``computeRHS_X(main, grid, myFFT, utilities)`` evaluates the RHS of the
+closure on the GPU and keeps the reference's side effects
+(PySpectral/src/RHSfunctions.py): ``main.Q`` becomes the RHS, ``main.uhat``
+(``main.U``) holds the state as the RHS read it (Nyquist-zeroed except in
+Smagorinsky, :10-12), ``main.w0_*`` holds the closure force and the
+tau-models set ``main.tau``.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _capi
+
+
+def _rhs(main, grid, closure):
+    ctx = grid.ctx(main.precision)
+    rhs = torch.empty_like(main.Q)
+    tau = ctx.rhs(closure, main.Q, rhs, main.params(), w0=main.W0, read_out=main.U)
+    main.Q = rhs
+    return tau
+
+
+def computeRHS_NOSGS(main, grid, myFFT=None, utilities=None):
+    """DNS, src/RHSfunctions.py:3-50."""
+    _rhs(main, grid, _capi.DNS)
+
+
+def computeRHS_SMAG(main, grid, myFFT=None, utilities=None):
+    """Smagorinsky (Cs = 0.16), src/RHSfunctions.py:146-237."""
+    _rhs(main, grid, _capi.SMAG)
+
+
+def computeRHS_tmodel(main, grid, myFFT=None, utilities=None):
+    """t-model ``w0 = Ct t PLQLu``, src/RHSfunctions.py:240-363."""
+    _rhs(main, grid, _capi.TMODEL)
+
+
+def computeRHS_staumodel(main, grid, myFFT=None, utilities=None):
+    """Static tau-model ``tau = max(0, tau_a + tau_b t)``, src/RHSfunctions.py:366-497."""
+    main.tau = _rhs(main, grid, _capi.TAU_STATIC)
+
+
+def computeRHS_Dtaumodel(main, grid, myFFT=None, utilities=None):
+    """Dynamic tau-model, src/RHSfunctions.py:592-878 (``main.tau`` before the clamp)."""
+    main.tau = _rhs(main, grid, _capi.TAU_DYNAMIC)
+
+
+def advanceQ_RK4(main, grid, myFFT=None, utilities=None):
+    """``advanceQ_RK4`` (src/PySpec_3d.py:96-105): four low-storage stages
+    ``Q = Q0 + dt c_i RHS(Q)``, c = [1/4, 1/3, 1/2, 1], fused into the RHS
+    epilogues.  ``main.uhat`` ends as the state read by the last stage, which
+    is what the reference's per-step diagnostics read (src/PySpec_3d.py:129)."""
+    if utilities is not None:
+        utilities.preAdvanceQ_hook(main, grid, myFFT)
+        utilities.compute_dt(main, grid)
+    ctx = grid.ctx(main.precision)
+    ctx.step(main.closure_code(), main.Q, main.params(), 1, comp=main.comp, read_out=main.U)
+    if utilities is not None:
+        utilities.postAdvanceQ_hook(main, grid, myFFT)
+
+
+def advance(main, grid, nsteps):
+    """``nsteps`` fixed-dt RK4 steps in one call (no per-step host work)."""
+    ctx = grid.ctx(main.precision)
+    ctx.step(main.closure_code(), main.Q, main.params(), int(nsteps), comp=main.comp, read_out=main.U)

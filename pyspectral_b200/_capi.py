@@ -1,0 +1,261 @@
+"""ctypes binding of the C ABI declared in ``include/pyspectral_b200.h``.
+
+Only plain pointers and sizes cross the boundary.  Tensors are passed as
+``data_ptr()`` values; the context queues its work on the caller's current
+torch CUDA stream.  There is no CPU fallback: if the shared library is missing
+or no GPU is visible every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
+
+PSB_OK = 0
+PSB_ERR_NONFINITE = 6
+DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD = 0, 1, 2, 3, 4, 5
+NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
+
+EXPORTS = (
+    "psb_ctx_create", "psb_ctx_destroy", "psb_ctx_set_stream", "psb_last_error", "psb_create_error",
+    "psb_rhs", "psb_step_rk4", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
+    "psb_spectrum", "psb_spectrum_nbins", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
+    "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
+    "psb_timing_count", "psb_timing_get",
+)
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("N1", ctypes.c_int), ("N2", ctypes.c_int), ("N3", ctypes.c_int),
+                ("L1", ctypes.c_double), ("L2", ctypes.c_double), ("L3", ctypes.c_double),
+                ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+                ("kc", ctypes.c_int)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("nu", ctypes.c_double), ("eta", ctypes.c_double), ("t", ctypes.c_double),
+                ("dt", ctypes.c_double), ("Ct", ctypes.c_double), ("tau_a", ctypes.c_double),
+                ("tau_b", ctypes.c_double), ("kf", ctypes.c_int), ("rotate", ctypes.c_int),
+                ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
+                ("force", ctypes.c_void_p)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m pyspectral_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp, ip, dp, i = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_int
+    d = ctypes.c_double
+    sig = {
+        "psb_ctx_create": ([ctypes.POINTER(Grid), i, i, ctypes.POINTER(vp)], i),
+        "psb_ctx_destroy": ([vp], i),
+        "psb_ctx_set_stream": ([vp, vp], i),
+        "psb_last_error": ([vp], ctypes.c_char_p),
+        "psb_create_error": ([], ctypes.c_char_p),
+        "psb_rhs": ([vp, i, vp, vp, vp, vp, ctypes.POINTER(Params), dp], i),
+        "psb_step_rk4": ([vp, i, vp, vp, vp, ctypes.POINTER(Params), i], i),
+        "psb_prepare": ([vp, i], i),
+        "psb_energy": ([vp, vp, i, dp], i),
+        "psb_enstrophy": ([vp, vp, i, dp], i),
+        "psb_cross_helicity": ([vp, vp, vp, i, dp], i),
+        "psb_spectrum": ([vp, vp, i, dp, i], i),
+        "psb_spectrum_nbins": ([vp, i, ip], i),
+        "psb_spectrum_mpi": ([vp, vp, dp, i], i),
+        "psb_cfl_dt": ([vp, vp, d, d, dp], i),
+        "psb_sgs_dns": ([vp, vp, vp, vp], i),
+        "psb_fft_r2c": ([vp, vp, vp, i], i),
+        "psb_fft_c2r": ([vp, vp, vp, i], i),
+        "psb_check_finite": ([vp, vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], i),
+        "psb_launch_count": ([vp, ctypes.POINTER(ctypes.c_ulonglong)], i),
+        "psb_timing_enable": ([vp, i], i),
+        "psb_timing_count": ([vp, ip], i),
+        "psb_timing_get": ([vp, i, ctypes.c_char_p, i, dp, dp], i),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
+                Om=(0.0, 0.0, 0.0), force=None) -> Params:
+    return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
+                  int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force)
+
+
+class Context:
+    """Owns one ``psb_ctx`` (grid + precision + device)."""
+
+    def __init__(self, N1, N2, N3, L=(2 * 3.141592653589793,) * 3, d=None, kc=None, precision=64, device=0):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("pyspectral_b200 needs a CUDA device; none is visible")
+        self.lib = load()
+        L1, L2, L3 = L
+        if d is None:
+            d = (L1 / N1, L2 / N2, L3 / N3)
+        self.grid = Grid(N1, N2, N3, L1, L2, L3, d[0], d[1], d[2], N1 // 2 if kc is None else int(kc))
+        self.precision = precision
+        self.device = device
+        h = ctypes.c_void_p()
+        st = self.lib.psb_ctx_create(ctypes.byref(self.grid), precision, device, ctypes.byref(h))
+        if st != PSB_OK:
+            raise RuntimeError(f"psb_ctx_create failed ({st}): {self.lib.psb_create_error().decode()}")
+        self.h = h
+        self.N1, self.N2, self.N3 = N1, N2, N3
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                self.lib.psb_ctx_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+    def check(self, st: int, what: str):
+        if st != PSB_OK:
+            raise RuntimeError(f"{what} failed ({st}): {self.lib.psb_last_error(self.h).decode()}")
+
+    def bind_stream(self):
+        import torch
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        self.lib.psb_ctx_set_stream(self.h, ctypes.c_void_p(s))
+
+    # -- tensor helpers
+    def _ptr(self, t, ncomplex=None):
+        import torch
+        if t is None:
+            return None
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError("tensors passed to pyspectral_b200 must be contiguous CUDA tensors")
+        want = torch.complex128 if self.precision == 64 else torch.complex64
+        if t.is_complex() and t.dtype != want:
+            raise ValueError(f"expected {want}, got {t.dtype}")
+        if ncomplex is not None and t.numel() < ncomplex:
+            raise ValueError("tensor too small for the grid")
+        return ctypes.c_void_p(t.data_ptr())
+
+    def spec_numel(self, nfields):
+        return nfields * self.N1 * self.N2 * (self.N3 // 2 + 1)
+
+    def rhs(self, closure, state, rhs, params, w0=None, read_out=None):
+        nf = 6 if closure == MHD else 3
+        self.bind_stream()
+        tau = ctypes.c_double(0.0)
+        st = self.lib.psb_rhs(self.h, closure, self._ptr(state, self.spec_numel(nf)),
+                              self._ptr(rhs, self.spec_numel(nf)), self._ptr(w0), self._ptr(read_out),
+                              ctypes.byref(params), ctypes.byref(tau))
+        self.check(st, "psb_rhs")
+        return tau.value
+
+    def step(self, closure, state, params, nsteps=1, comp=None, read_out=None):
+        nf = 6 if closure == MHD else 3
+        self.bind_stream()
+        st = self.lib.psb_step_rk4(self.h, closure, self._ptr(state, self.spec_numel(nf)), self._ptr(comp),
+                                   self._ptr(read_out), ctypes.byref(params), int(nsteps))
+        self.check(st, "psb_step_rk4")
+
+    def prepare(self, closure):
+        self.check(self.lib.psb_prepare(self.h, closure), "psb_prepare")
+
+    def energy(self, f3, flags=0):
+        self.bind_stream()
+        out = ctypes.c_double()
+        self.check(self.lib.psb_energy(self.h, self._ptr(f3, self.spec_numel(3)), flags, ctypes.byref(out)),
+                   "psb_energy")
+        return out.value
+
+    def enstrophy(self, f3, flags=0):
+        self.bind_stream()
+        out = ctypes.c_double()
+        self.check(self.lib.psb_enstrophy(self.h, self._ptr(f3, self.spec_numel(3)), flags, ctypes.byref(out)),
+                   "psb_enstrophy")
+        return out.value
+
+    def cross_helicity(self, u3, b3, flags=NORM_MPI):
+        self.bind_stream()
+        out = ctypes.c_double()
+        self.check(self.lib.psb_cross_helicity(self.h, self._ptr(u3), self._ptr(b3), flags, ctypes.byref(out)),
+                   "psb_cross_helicity")
+        return out.value
+
+    def spectrum(self, f3, flags=0):
+        import numpy as np
+        self.bind_stream()
+        nb = ctypes.c_int()
+        self.check(self.lib.psb_spectrum_nbins(self.h, flags, ctypes.byref(nb)), "psb_spectrum_nbins")
+        out = np.zeros((nb.value, 3), dtype=np.float64)
+        self.check(self.lib.psb_spectrum(self.h, self._ptr(f3), flags,
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nb.value),
+                   "psb_spectrum")
+        return out
+
+    def spectrum_mpi(self, f3):
+        import numpy as np
+        self.bind_stream()
+        N1, N2, N3 = self.N1, self.N2, self.N3
+        kmax = int(np.round(np.sqrt((N1 // 2) ** 2 + (N2 // 2) ** 2 + (N3 // 2) ** 2)))
+        out = np.zeros(kmax + 1, dtype=np.float64)
+        self.check(self.lib.psb_spectrum_mpi(self.h, self._ptr(f3), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                             kmax + 1), "psb_spectrum_mpi")
+        return out
+
+    def cfl_dt(self, f3, cfl, nu):
+        self.bind_stream()
+        out = ctypes.c_double()
+        self.check(self.lib.psb_cfl_dt(self.h, self._ptr(f3), float(cfl), float(nu), ctypes.byref(out)),
+                   "psb_cfl_dt")
+        return out.value
+
+    def sgs_dns(self, f3, w0, tau6=None):
+        self.bind_stream()
+        self.check(self.lib.psb_sgs_dns(self.h, self._ptr(f3), self._ptr(w0), self._ptr(tau6)), "psb_sgs_dns")
+
+    def r2c(self, phys, spec, nfields):
+        self.bind_stream()
+        self.check(self.lib.psb_fft_r2c(self.h, self._ptr(phys), self._ptr(spec), int(nfields)), "psb_fft_r2c")
+
+    def c2r(self, spec, phys, nfields):
+        self.bind_stream()
+        self.check(self.lib.psb_fft_c2r(self.h, self._ptr(spec), self._ptr(phys), int(nfields)), "psb_fft_c2r")
+
+    def launch_count(self):
+        n = ctypes.c_ulonglong()
+        self.check(self.lib.psb_launch_count(self.h, ctypes.byref(n)), "psb_launch_count")
+        return n.value
+
+    def timing(self, on: bool):
+        self.check(self.lib.psb_timing_enable(self.h, 1 if on else 0), "psb_timing_enable")
+
+    def timing_records(self):
+        """[(kernel name, device ms, compulsory bytes)] of the timed launches."""
+        n = ctypes.c_int()
+        self.check(self.lib.psb_timing_count(self.h, ctypes.byref(n)), "psb_timing_count")
+        out = []
+        buf = ctypes.create_string_buffer(128)
+        ms, by = ctypes.c_double(), ctypes.c_double()
+        for i in range(n.value):
+            self.check(self.lib.psb_timing_get(self.h, i, buf, 128, ctypes.byref(ms), ctypes.byref(by)),
+                       "psb_timing_get")
+            out.append((buf.value.decode(), ms.value, by.value))
+        return out
+
+    def count_nonfinite(self, t):
+        self.bind_stream()
+        n = ctypes.c_longlong()
+        st = self.lib.psb_check_finite(self.h, self._ptr(t), t.numel(), ctypes.byref(n))
+        if st not in (PSB_OK, PSB_ERR_NONFINITE):
+            self.check(st, "psb_check_finite")
+        return n.value

@@ -1,0 +1,239 @@
+// Host-side context shared by the translation units of libpyspectral_b200:
+// grid constants, FFT plans and twiddle pools, wavenumber/mask tables on the
+// device, the scratch arena and launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pyspectral_b200.h"
+#include "psb_physics.cuh"
+
+struct psb_ctx {
+  int N1 = 0, N2 = 0, N3 = 0, N3h = 0;
+  int prec = 64;
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  double L1 = 0, L2 = 0, L3 = 0, dx = 0, dy = 0, dz = 0, Delta = 0;
+  int kc = 0;
+  // device tables (double): N grid, 2x grid, MHD dealias masks, Gf masks
+  double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  double *kxf = nullptr, *kyf = nullptr, *kzf = nullptr;
+  double *mx = nullptr, *my = nullptr, *mz = nullptr;
+  double *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  int kz_mhd = 0;  // retained k3 count of the 2/3 rule
+  int dtau_kf = -1;  // test-filter wavenumber of the cached dynamic-tau masks
+  void* tw_d = nullptr;  // Cx<double> pool
+  void* tw_f = nullptr;  // Cx<float> pool
+  std::map<int, psb::FFTPlan> plans;
+  struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+  };
+  std::map<std::string, Buf> scratch;
+  double* red_dev = nullptr;   // reduction partials
+  double* red_host = nullptr;  // pinned
+  size_t red_cap = 0;
+  std::string err;
+  std::vector<void*> owned;  // table allocations
+  // launch accounting: every kernel launch counts; with timing on, each
+  // launch is bracketed by CUDA events on the context stream and tagged
+  // with its compulsory HBM bytes (inputs read once + outputs written once)
+  unsigned long long launches = 0;
+  int timing = 0;
+  struct Rec {
+    std::string name;
+    double bytes;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> recs;
+  std::vector<cudaEvent_t> ev_free;
+};
+
+namespace psbh {
+
+using psb::Cx;
+using psb::FFTPlan;
+
+inline int fail(psb_ctx* c, int code, const std::string& msg) {
+  c->err = msg;
+  return code;
+}
+
+inline int cuda_ok(psb_ctx* c, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return PSB_OK;
+  return fail(c, PSB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+inline int launch_ok(psb_ctx* c, const char* what) { return cuda_ok(c, cudaGetLastError(), what); }
+
+#define PSB_TRY(expr)              \
+  do {                             \
+    int _s = (expr);               \
+    if (_s != PSB_OK) return _s;   \
+  } while (0)
+
+inline const FFTPlan* plan_for(psb_ctx* c, int L) {
+  auto it = c->plans.find(L);
+  return it == c->plans.end() ? nullptr : &it->second;
+}
+
+template <typename T>
+inline const Cx<T>* twiddles(psb_ctx* c) {
+  return reinterpret_cast<const Cx<T>*>(sizeof(T) == 8 ? c->tw_d : c->tw_f);
+}
+
+// Named scratch buffer of at least `n` complex elements (grows; contents undefined).
+template <typename T>
+inline Cx<T>* scratch(psb_ctx* c, const char* name, size_t n, int* status) {
+  const size_t bytes = n * sizeof(Cx<T>);
+  auto& b = c->scratch[name];
+  if (b.bytes < bytes) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+      *status = fail(c, PSB_ERR_CUDA, std::string("scratch ") + name + ": " + cudaGetErrorString(e));
+      return nullptr;
+    }
+    b.bytes = bytes;
+  }
+  return reinterpret_cast<Cx<T>*>(b.p);
+}
+
+inline cudaEvent_t take_event(psb_ctx* c) {
+  if (!c->ev_free.empty()) {
+    cudaEvent_t e = c->ev_free.back();
+    c->ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Bracket one kernel launch: count it and, when timing is on, record events.
+struct LaunchScope {
+  psb_ctx* c;
+  psb_ctx::Rec rec;
+  bool on;
+  LaunchScope(psb_ctx* ctx, const char* name, double bytes) : c(ctx), on(ctx->timing != 0) {
+    ++c->launches;
+    if (on) {
+      rec.name = name;
+      rec.bytes = bytes;
+      rec.a = take_event(c);
+      rec.b = take_event(c);
+      cudaEventRecord(rec.a, c->stream);
+    }
+  }
+  ~LaunchScope() {
+    if (on) {
+      cudaEventRecord(rec.b, c->stream);
+      c->recs.push_back(rec);
+    }
+  }
+};
+
+inline int count_mapped(const psb::RowMap& m, int rows) {
+  int n = 0;
+  for (int i = 0; i < rows; ++i) n += m.lo > i ? 1 : (i >= m.hi ? 1 : 0);
+  return n;
+}
+
+constexpr size_t kSmemBudget = 100 * 1024;
+
+template <typename K>
+inline void set_smem(K kernel, size_t smem) {
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+inline int pow2_floor(int x) {
+  int p = 1;
+  while (p * 2 <= x) p *= 2;
+  return p;
+}
+
+// columns per CTA for strided passes
+inline int pick_ct(int ncols, int F, int L, size_t esz) {
+  int ct = 32;
+  int cap = pow2_floor(ncols < 1 ? 1 : ncols);
+  if (ncols > cap) cap *= 2;
+  if (ct > cap) ct = cap;
+  while (ct > 1 && (size_t)(L + 2 * L * F * ct) * esz > kSmemBudget) ct /= 2;
+  return ct;
+}
+
+template <typename T, bool INV, class Pre>
+int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what) {
+  const size_t esz = sizeof(Cx<T>);
+  const int L = a.plan.L;
+  a.col_tile = pick_ct(a.ncols, Pre::F_DST, L, esz);
+  const size_t smem = (size_t)(L + 2 * L * Pre::F_DST * a.col_tile) * esz;
+  dim3 grid((a.ncols + a.col_tile - 1) / a.col_tile, a.nouter);
+  auto k = psb::axis_pass_kernel<T, INV, Pre>;
+  set_smem(k, smem);
+  const double bytes = (double)esz * a.nouter * a.ncols *
+                       ((double)Pre::F_SRC * count_mapped(a.in_map, a.in_rows) + (double)Pre::F_DST * a.out_rows);
+  LaunchScope scope(c, what, bytes);
+  k<<<grid, 256, smem, c->stream>>>(a, pre);
+  return launch_ok(c, what);
+}
+
+template <typename T, class Phys>
+int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double extra_bytes = 0.0) {
+  const size_t esz = sizeof(Cx<T>);
+  const int M = z.plan.L;
+  constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
+  auto smem_for = [&](int P) { return (size_t)(M + 2 * ((FMAX * P + 1) / 2) * M) * esz; };
+  int P = 8;
+  while (P > 1 && smem_for(P) > kSmemBudget) P /= 2;
+  while (P > 1 && (z.npencils + P - 1) / P < 2 * 148) P /= 2;
+  z.ppc = P;
+  const size_t smem = smem_for(P);
+  const long long grid = (z.npencils + P - 1) / P;
+  auto k = psb::zpass_kernel<T, Phys>;
+  set_smem(k, smem);
+  double bytes = extra_bytes + (double)esz * z.npencils * Phys::F_OUT * z.out_kz;
+  for (int f = 0; f < Phys::F_IN; ++f) bytes += (double)esz * z.npencils * z.in_kz[f];
+  LaunchScope scope(c, what, bytes);
+  k<<<(unsigned)grid, 256, smem, c->stream>>>(z, phys);
+  return launch_ok(c, what);
+}
+
+// bytes: the transform input plus the epilogue's own state traffic (epi.io_bytes)
+template <typename T, class Epi>
+int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what) {
+  const size_t esz = sizeof(Cx<T>);
+  const int L = e.plan.L;
+  e.col_tile = pick_ct(e.kz, Epi::F_IN, L, esz);
+  const int ntile = (e.kz + e.col_tile - 1) / e.col_tile;
+  e.main_blocks = ntile * e.n2;
+  int extra = 0;
+  if (e.n3h > e.kz) {
+    const long long pts = (long long)e.n1 * e.n2 * (e.n3h - e.kz);
+    extra = (int)std::min<long long>((pts + 255) / 256, 1024);
+  }
+  const size_t smem = (size_t)(L + 2 * L * Epi::F_IN * e.col_tile) * esz;
+  auto k = psb::xfwd_epi_kernel<T, Epi>;
+  set_smem(k, smem);
+  const double bytes = epi.io_bytes((long long)e.n1 * e.n2 * e.n3h) + (double)esz * Epi::F_IN * L * e.n2 * e.kz;
+  LaunchScope scope(c, what, bytes);
+  k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
+  return launch_ok(c, what);
+}
+
+inline psb::RowMap map_id(int L) { return psb::RowMap{L, L, 0}; }
+// pad/unpad (3/2): drops index N/2 (PySpectral/src/padding.py:2-25)
+inline psb::RowMap map_pad32(int N) { return psb::RowMap{N / 2, N / 2 + 1, 3 * N / 2 - N}; }
+// pad_2x/unpad_2x: keeps N/2 as the -N/2 mode (PySpectral/src/padding.py:28-49)
+inline psb::RowMap map_pad2x(int N) { return psb::RowMap{N / 2, N / 2, N}; }
+// unpad(pad()) followed by pad_2x: Nyquist dropped, upper half shifted by N
+inline psb::RowMap map_pad2x_nyq0(int N) { return psb::RowMap{N / 2, N / 2 + 1, N}; }
+
+}  // namespace psbh

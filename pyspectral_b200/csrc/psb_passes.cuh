@@ -1,0 +1,287 @@
+// Pencil passes of the padded 3-D real FFTs, each fused with the pointwise
+// work that sits next to it in the reference's dataflow.
+//
+// Spectral layout  : field-major (F, N1, N2, N3/2+1), k3 contiguous.
+// Intermediates    : (F, rows_x, rows_y, Kz) with Kz the retained k3 count, so
+//                    every pass reads and writes rows of Kz contiguous complex
+//                    values (coalesced, no transposes).
+//
+//  axis_pass_kernel   one strided axis (x or y): gathers the retained rows
+//                     into their padded FFT positions (or the reverse on the
+//                     forward side), runs the transform along that axis for a
+//                     tile of contiguous columns, scatters the result.  A
+//                     `Pre` functor can expand the source fields on load
+//                     (e.g. u -> u, S_ij = (i/2)(k_j u_i + k_i u_j)).
+//  zpass_kernel       the contiguous axis: c2r of F_IN spectral pencils
+//                     (two real lines packed per complex transform), the
+//                     physical-space products of a `Phys` functor, r2c of the
+//                     F_OUT results truncated to the retained k3 -- physical
+//                     space never touches HBM.
+//  xfwd_epi_kernel    the last forward pass (x) fused with the spectral
+//                     epilogue (`Epi`): pressure projection, viscous term,
+//                     closure divergence, Coriolis, RK stage update.
+//
+// The padding maps reproduce PySpectral/src/padding.py:2-49 (pad/unpad drop
+// index N/2 of x and y and the k3=N/2 plane; pad_2x/unpad_2x keep the -N/2
+// mode).
+#pragma once
+#include "psb_fft.cuh"
+
+namespace psb {
+
+// Spectral row index i -> FFT position j (or -1 when the row is not carried).
+struct RowMap {
+  int lo, hi, shift;
+  __device__ __forceinline__ int operator()(int i) const { return i < lo ? i : (i >= hi ? i + shift : -1); }
+};
+
+constexpr int kMaxZFields = 16;
+
+template <typename T>
+struct AxisArgs {
+  const Cx<T>* in;
+  Cx<T>* out;
+  long long in_fstride, in_ostride, in_rstride;
+  long long out_fstride, out_ostride, out_rstride;
+  int nouter;    // outer (batch) indices
+  int ncols;     // contiguous columns per outer index
+  int col_tile;  // columns per CTA
+  int in_rows, out_rows;
+  RowMap in_map, out_map;
+  T scale;  // applied on store
+  FFTPlan plan;
+  const Cx<T>* tw;
+  const double* k_row;  // wavenumbers of the input rows (for Pre)
+  const double* k_outer;
+  const double* k_col;
+};
+
+template <typename T>
+struct PreCopy {
+  static constexpr int F_SRC = 1, F_DST = 1;
+  __device__ void operator()(int, int, int, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const { d[0] = s[0]; }
+};
+
+// grid = (ceil(ncols/col_tile), nouter); smem = tw[L] + 2 * L*lines
+template <typename T, bool INV, class Pre>
+__global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int L = a.plan.L;
+  const int ct = a.col_tile;
+  const int lines = Pre::F_DST * ct;
+  Cx<T>* bufA = tw + L;
+  Cx<T>* bufB = bufA + (size_t)L * lines;
+  const int o = blockIdx.y;
+  const int c0 = blockIdx.x * ct;
+  stage_twiddles(tw, a.tw, a.plan);
+  const Cx<T> zero = mk<T>(0, 0);
+  for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) bufA[idx] = zero;
+  __syncthreads();
+  const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
+  for (int idx = threadIdx.x; idx < a.in_rows * ct; idx += blockDim.x) {
+    const int c = idx % ct, i = idx / ct;
+    const int col = c0 + c;
+    const int j = a.in_map(i);
+    if (j < 0 || col >= a.ncols) continue;
+    Cx<T> s[Pre::F_SRC], d[Pre::F_DST];
+#pragma unroll
+    for (int f = 0; f < Pre::F_SRC; ++f) s[f] = inb[f * a.in_fstride + i * a.in_rstride + col];
+    pre(i, o, col, a, s, d);
+#pragma unroll
+    for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
+  }
+  __syncthreads();
+  Cx<T>* res = block_fft<T, INV>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  Cx<T>* outb = a.out + (long long)o * a.out_ostride;
+  const int nst = a.out_rows * Pre::F_DST * ct;
+  for (int idx = threadIdx.x; idx < nst; idx += blockDim.x) {
+    const int c = idx % ct;
+    const int t = idx / ct;
+    const int g = t % Pre::F_DST, i = t / Pre::F_DST;
+    const int col = c0 + c;
+    if (col >= a.ncols) continue;
+    const int j = a.out_map(i);
+    outb[g * a.out_fstride + i * a.out_rstride + col] = j >= 0 ? a.scale * res[(size_t)j * lines + g * ct + c] : zero;
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+struct ZArgs {
+  const Cx<T>* in[kMaxZFields];  // per input field: pencil p at in[f] + p*in_pstride[f]
+  long long in_pstride[kMaxZFields];
+  int in_kz[kMaxZFields];  // stored k3 entries (0..kz-1); higher k3 are zero
+  Cx<T>* out[kMaxZFields];
+  long long out_pstride[kMaxZFields];
+  int out_kz;  // retained k3 entries on output
+  long long npencils;
+  int ppc;  // pencils per CTA
+  T fac;    // physical normalisation after the inverse transform
+  FFTPlan plan;
+  const Cx<T>* tw;
+};
+
+// grid = ceil(npencils/ppc); smem = tw[M] + 2 * nl*M with nl = ceil(max(F_IN,F_OUT)*ppc/2)
+template <typename T, class Phys>
+__global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  constexpr int FI = Phys::F_IN, FO = Phys::F_OUT;
+  const int M = a.plan.L;
+  const int P = a.ppc;
+  constexpr int FMAX = FI > FO ? FI : FO;
+  const int nl = (FMAX * P + 1) / 2;
+  Cx<T>* X = tw + M;
+  Cx<T>* Y = X + (size_t)nl * M;
+  const long long p0 = (long long)blockIdx.x * P;
+  stage_twiddles(tw, a.tw, a.plan);
+  const Cx<T> zero = mk<T>(0, 0);
+  const int half = M / 2;
+  Cx<T>* R = X;
+  if constexpr (FI > 0) {
+    const int nin = (FI * P + 1) / 2;
+    for (int idx = threadIdx.x; idx < nin * M; idx += blockDim.x) X[idx] = zero;
+    __syncthreads();
+    // pack pairs of Hermitian half-spectra: Z = A + iB, Z[M-k] = conj(A_k) + i conj(B_k);
+    // the k=0 and k=M/2 terms keep their real parts only (c2r convention)
+    for (int idx = threadIdx.x; idx < nin * (half + 1); idx += blockDim.x) {
+      const int k = idx % (half + 1), c = idx / (half + 1);
+      Cx<T> A = zero, B = zero;
+#pragma unroll 1
+      for (int part = 0; part < 2; ++part) {
+        const int r = 2 * c + part;
+        if (r >= FI * P) break;
+        const int f = r / P, p = r % P;
+        const long long pen = p0 + p;
+        if (pen >= a.npencils || k >= a.in_kz[f]) continue;
+        const Cx<T> v = a.in[f][pen * a.in_pstride[f] + k];
+        if (part == 0) A = v; else B = v;
+      }
+      Cx<T>* Z = X + (size_t)c * M;
+      if (k == 0 || k == half) {
+        Z[k] = mk<T>(A.x, B.x);
+      } else {
+        Z[k] = mk<T>(A.x - B.y, A.y + B.x);
+        Z[M - k] = mk<T>(A.x + B.y, B.x - A.y);
+      }
+    }
+    __syncthreads();
+    R = block_fft<T, true>(X, Y, a.plan, tw, nin, M, 1, false);
+  }
+  Cx<T>* W = (R == X) ? Y : X;
+  const int nout = (FO * P + 1) / 2;
+  // pointwise physics
+  for (int idx = threadIdx.x; idx < P * M; idx += blockDim.x) {
+    const int z = idx % M, p = idx / M;
+    T vin[FI > 0 ? FI : 1], vout[FO > 0 ? FO : 1];
+#pragma unroll
+    for (int f = 0; f < FI; ++f) {
+      const int r = f * P + p;
+      const Cx<T> v = R[(size_t)(r >> 1) * M + z];
+      vin[f] = a.fac * ((r & 1) ? v.y : v.x);
+    }
+    phys(p0 + p, z, vin, vout);
+#pragma unroll
+    for (int g = 0; g < FO; ++g) {
+      const int r = g * P + p;
+      T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + z);
+      w[r & 1] = vout[g];
+    }
+    if ((FO * P) & 1) {  // odd count: the last packed line has no partner
+      if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * M + z)[1] = (T)0;
+    }
+  }
+  if constexpr (FO > 0) {
+    __syncthreads();
+    Cx<T>* R2 = block_fft<T, false>(W, R, a.plan, tw, nout, M, 1, false);
+    // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
+    const int kzo = a.out_kz;
+    for (int idx = threadIdx.x; idx < nout * kzo; idx += blockDim.x) {
+      const int k = idx % kzo, c = idx / kzo;
+      const Cx<T>* Z = R2 + (size_t)c * M;
+      const Cx<T> zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
+#pragma unroll
+      for (int part = 0; part < 2; ++part) {
+        const int r = 2 * c + part;
+        if (r >= FO * P) break;
+        const int g = r / P, p = r % P;
+        const long long pen = p0 + p;
+        if (pen >= a.npencils) continue;
+        const Cx<T> v = part == 0 ? mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y))
+                                  : mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zm.x - zk.x));
+        a.out[g][pen * a.out_pstride[g] + k] = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <typename T>
+struct XEpiArgs {
+  const Cx<T>* in;  // (F, L rows, n2, kz)
+  long long in_fstride, in_rstride, in_ostride;
+  int n1, n2, n3h;  // spectral output dims (rows, outer, k3 count)
+  int kz;           // k3 < kz come from the transform, the rest have zero products
+  int col_tile;
+  RowMap out_map;  // spectral row -> FFT position
+  int main_blocks;
+  FFTPlan plan;
+  const Cx<T>* tw;
+};
+
+// grid = main_blocks + extra; main block b -> (col tile b % ntile, outer b / ntile)
+template <typename T, class Epi>
+__global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int F = Epi::F_IN;
+  Cx<T> P[F];
+  const Cx<T> zero = mk<T>(0, 0);
+  if ((int)blockIdx.x >= a.main_blocks) {
+    // columns kz..n3h-1 carry no products
+    const int ncz = a.n3h - a.kz;
+    const long long tot = (long long)a.n1 * a.n2 * ncz;
+    const int nextra = gridDim.x - a.main_blocks;
+    for (long long idx = (long long)(blockIdx.x - a.main_blocks) * blockDim.x + threadIdx.x; idx < tot;
+         idx += (long long)nextra * blockDim.x) {
+      const int c = (int)(idx % ncz);
+      const long long t = idx / ncz;
+      const int i2 = (int)(t % a.n2), i1 = (int)(t / a.n2);
+#pragma unroll
+      for (int f = 0; f < F; ++f) P[f] = zero;
+      epi(i1, i2, a.kz + c, P);
+    }
+    return;
+  }
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int L = a.plan.L;
+  const int ct = a.col_tile;
+  const int lines = F * ct;
+  Cx<T>* bufA = tw + L;
+  Cx<T>* bufB = bufA + (size_t)L * lines;
+  const int ntile = (a.kz + ct - 1) / ct;
+  const int o = blockIdx.x / ntile;
+  const int c0 = (blockIdx.x % ntile) * ct;
+  stage_twiddles(tw, a.tw, a.plan);
+  const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
+  for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) {
+    const int c = idx % ct;
+    const int t = idx / ct;
+    const int f = t % F, j = t / F;
+    const int col = c0 + c;
+    bufA[(size_t)j * lines + f * ct + c] = col < a.kz ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
+  }
+  __syncthreads();
+  Cx<T>* res = block_fft<T, false>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  for (int idx = threadIdx.x; idx < a.n1 * ct; idx += blockDim.x) {
+    const int c = idx % ct, i1 = idx / ct;
+    const int col = c0 + c;
+    if (col >= a.kz) continue;
+    const int j = a.out_map(i1);
+#pragma unroll
+    for (int f = 0; f < F; ++f) P[f] = j >= 0 ? res[(size_t)j * lines + f * ct + c] : zero;
+    epi(i1, o, col, P);
+  }
+}
+
+}  // namespace psb

@@ -1,0 +1,673 @@
+// Right-hand-side pipelines of every closure and the RK4 driver.
+//
+// One RHS = x-inverse -> y-inverse -> fused z (c2r, products, r2c) ->
+// y-forward -> x-forward fused with the spectral epilogue.  In RK mode the
+// epilogue applies the stage update Q = Q0 + dt*c_i*RHS in place, so a stage
+// is five kernels and the state is read twice and written once.
+#include "psb_ctx.cuh"
+
+using namespace psb;
+using namespace psbh;
+
+namespace {
+
+template <typename T>
+KTabs<T> ktabs(const double* a, const double* b, const double* c) {
+  KTabs<T> k;
+  k.k1 = a;
+  k.k2 = b;
+  k.k3 = c;
+  return k;
+}
+
+template <typename T>
+AxisArgs<T> axis_common(psb_ctx* c, int L) {
+  AxisArgs<T> a{};
+  a.plan = *plan_for(c, L);
+  a.tw = twiddles<T>(c);
+  a.scale = (T)1;
+  return a;
+}
+
+// ---------------------------------------------------------------------------
+// 3/2-padded Navier-Stokes (DNS, Smagorinsky, SGS of filtered DNS)
+// ---------------------------------------------------------------------------
+template <typename T, class Pre, class Phys, class Epi>
+int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
+  constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
+  static_assert(Phys::F_IN == Pre::F_DST, "pre/phys mismatch");
+  static_assert(Epi::F_IN == Phys::F_OUT, "phys/epi mismatch");
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "ns.A", (size_t)Fi * M1 * N2 * Kz, &st);
+  Cx<T>* B = scratch<T>(c, "ns.B", (size_t)Fi * M1 * M2 * Kz, &st);
+  Cx<T>* C = scratch<T>(c, "ns.C", (size_t)Fo * M1 * M2 * Kz, &st);
+  Cx<T>* D = scratch<T>(c, "ns.D", (size_t)Fo * M1 * N2 * Kz, &st);
+  if (st != PSB_OK) return st;
+  if (!Qin) return PSB_OK;  // allocation only
+  const long long fsN = (long long)N1 * N2 * N3h;
+  // x inverse: spectral rows k1 -> padded positions
+  AxisArgs<T> a = axis_common<T>(c, M1);
+  a.in = Qin;
+  a.out = A;
+  a.in_fstride = fsN;
+  a.in_ostride = N3h;
+  a.in_rstride = (long long)N2 * N3h;
+  a.out_fstride = (long long)M1 * N2 * Kz;
+  a.out_ostride = Kz;
+  a.out_rstride = (long long)N2 * Kz;
+  a.nouter = N2;
+  a.ncols = Kz;
+  a.in_rows = N1;
+  a.out_rows = M1;
+  a.in_map = map_pad32(N1);
+  a.out_map = map_id(M1);
+  a.k_row = c->kx;
+  a.k_outer = c->ky;
+  a.k_col = c->kz;
+  PSB_TRY((launch_axis<T, true>(c, a, pre, "x-inverse")));
+  // y inverse (fields folded into the outer index)
+  AxisArgs<T> b = axis_common<T>(c, M2);
+  b.in = A;
+  b.out = B;
+  b.in_ostride = (long long)N2 * Kz;
+  b.in_rstride = Kz;
+  b.out_ostride = (long long)M2 * Kz;
+  b.out_rstride = Kz;
+  b.nouter = Fi * M1;
+  b.ncols = Kz;
+  b.in_rows = N2;
+  b.out_rows = M2;
+  b.in_map = map_pad32(N2);
+  b.out_map = map_id(M2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "y-inverse")));
+  // fused z
+  ZArgs<T> z{};
+  const long long fsP = (long long)M1 * M2 * Kz;
+  for (int f = 0; f < Fi; ++f) {
+    z.in[f] = B + f * fsP;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+  }
+  for (int g = 0; g < Fo; ++g) {
+    z.out[g] = C + g * fsP;
+    z.out_pstride[g] = Kz;
+  }
+  z.out_kz = Kz;
+  z.npencils = (long long)M1 * M2;
+  const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)N1 * N2 * N3));
+  z.fac = (T)(s32 / ((double)M1 * M2 * M3));
+  z.plan = *plan_for(c, M3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, phys, "z-fused"));
+  // y forward with truncation
+  AxisArgs<T> d = axis_common<T>(c, M2);
+  d.in = C;
+  d.out = D;
+  d.in_ostride = (long long)M2 * Kz;
+  d.in_rstride = Kz;
+  d.out_ostride = (long long)N2 * Kz;
+  d.out_rstride = Kz;
+  d.nouter = Fo * M1;
+  d.ncols = Kz;
+  d.in_rows = M2;
+  d.out_rows = N2;
+  d.in_map = map_id(M2);
+  d.out_map = map_pad32(N2);
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "y-forward")));
+  // x forward + epilogue
+  XEpiArgs<T> e{};
+  e.in = D;
+  e.in_fstride = (long long)M1 * N2 * Kz;
+  e.in_rstride = (long long)N2 * Kz;
+  e.in_ostride = Kz;
+  e.n1 = N1;
+  e.n2 = N2;
+  e.n3h = N3h;
+  e.kz = Kz;
+  e.out_map = map_pad32(N1);
+  e.plan = *plan_for(c, M1);
+  e.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e, epi, "x-forward+epilogue");
+}
+
+// Products of u and of the sharp-cutoff filtered u for computeSGS_DNS
+// (PySpectral/src/Classes.py:861-915)
+template <typename T>
+struct PreFiltered {
+  static constexpr int F_SRC = 3, F_DST = 6;
+  const double *g1, *g2, *g3;
+  __device__ void operator()(int i, int o, int cc, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const {
+    const T g = (T)(g1[i] * g2[o] * g3[cc]);
+    d[0] = s[0];
+    d[1] = s[1];
+    d[2] = s[2];
+    d[3] = g * s[0];
+    d[4] = g * s[1];
+    d[5] = g * s[2];
+  }
+};
+
+// test filter applied on load (PySpectral/src/Classes.py:147-150)
+template <typename T>
+struct PreMask3 {
+  static constexpr int F_SRC = 3, F_DST = 3;
+  const double *g1, *g2, *g3;
+  __device__ void operator()(int i, int o, int cc, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const {
+    const T g = (T)(g1[i] * g2[o] * g3[cc]);
+    d[0] = g * s[0];
+    d[1] = g * s[1];
+    d[2] = g * s[2];
+  }
+};
+
+template <typename T>
+struct PhysSGSDNS {
+  static constexpr int F_IN = 6, F_OUT = 12;
+  __device__ __forceinline__ void operator()(long long, int, const T* in, T* out) const {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const T u = in[3 * h], v = in[3 * h + 1], w = in[3 * h + 2];
+      out[6 * h + 0] = u * u;
+      out[6 * h + 1] = v * v;
+      out[6 * h + 2] = w * w;
+      out[6 * h + 3] = u * v;
+      out[6 * h + 4] = u * w;
+      out[6 * h + 5] = v * w;
+    }
+  }
+};
+
+// tau_ij = Gf*(u_i u_j)^ - (Gf u_i Gf u_j)^ and its projected divergence
+// (PySpectral/src/Classes.py:917-928)
+template <typename T>
+struct EpiSGSDNS {
+  static constexpr int F_IN = 12;
+  __host__ double io_bytes(long long npts) const {
+    return (double)sizeof(Cx<T>) * npts * (3 + (tau ? 6 : 0));
+  }
+  KTabs<T> k;
+  const double *g1, *g2, *g3;
+  Cx<T>* w0;
+  Cx<T>* tau;
+  long long fstride;
+  int n2, n3h;
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = ((long long)i1 * n2 + i2) * n3h + i3;
+    const T g = (T)(g1[i1] * g2[i2] * g3[i3]);
+    Cx<T> t[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) t[m] = g * P[m] - P[6 + m];
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    const Cx<T> kk = (k1 * k1) * t[0] + (k2 * k2) * t[1] + (k3 * k3) * t[2] + ((T)2 * k1 * k2) * t[3] +
+                     ((T)2 * k1 * k3) * t[4] + ((T)2 * k2 * k3) * t[5];
+    const Cx<T> proj = mul_i(ksqi * kk);
+    w0[s] = mik(k1, t[0]) + mik(k2, t[3]) + mik(k3, t[4]) + pik(k1, proj);
+    w0[fstride + s] = mik(k1, t[3]) + mik(k2, t[1]) + mik(k3, t[5]) + pik(k2, proj);
+    w0[2 * fstride + s] = mik(k1, t[4]) + mik(k2, t[5]) + mik(k3, t[2]) + pik(k3, proj);
+    if (tau) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) tau[m * fstride + s] = t[m];
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// MHD: unpadded transforms under the 2/3 rule
+// ---------------------------------------------------------------------------
+template <typename T>
+int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int Kz = c->kz_mhd;
+  constexpr int Fi = 6, Fo = 9;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "mhd.A", (size_t)Fi * N1 * N2 * Kz, &st);
+  Cx<T>* B = scratch<T>(c, "mhd.B", (size_t)Fi * N1 * N2 * Kz, &st);
+  Cx<T>* C = scratch<T>(c, "mhd.C", (size_t)Fo * N1 * N2 * Kz, &st);
+  Cx<T>* D = scratch<T>(c, "mhd.D", (size_t)Fo * N1 * N2 * Kz, &st);
+  if (st != PSB_OK) return st;
+  if (!Qin) return PSB_OK;
+  const long long fsN = (long long)N1 * N2 * N3h;
+  const long long fsP = (long long)N1 * N2 * Kz;
+  AxisArgs<T> a = axis_common<T>(c, N1);
+  a.in = Qin;
+  a.out = A;
+  a.in_fstride = fsN;
+  a.in_ostride = N3h;
+  a.in_rstride = (long long)N2 * N3h;
+  a.out_fstride = fsP;
+  a.out_ostride = Kz;
+  a.out_rstride = (long long)N2 * Kz;
+  a.nouter = N2;
+  a.ncols = Kz;
+  a.in_rows = N1;
+  a.out_rows = N1;
+  a.in_map = map_id(N1);
+  a.out_map = map_id(N1);
+  PreMask6<T> pre{c->mx, c->my, c->mz};
+  PSB_TRY((launch_axis<T, true>(c, a, pre, "mhd x-inverse")));
+  AxisArgs<T> b = axis_common<T>(c, N2);
+  b.in = A;
+  b.out = B;
+  b.in_ostride = (long long)N2 * Kz;
+  b.in_rstride = Kz;
+  b.out_ostride = (long long)N2 * Kz;
+  b.out_rstride = Kz;
+  b.nouter = Fi * N1;
+  b.ncols = Kz;
+  b.in_rows = N2;
+  b.out_rows = N2;
+  b.in_map = map_id(N2);
+  b.out_map = map_id(N2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "mhd y-inverse")));
+  ZArgs<T> z{};
+  for (int f = 0; f < Fi; ++f) {
+    z.in[f] = B + f * fsP;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+  }
+  for (int g = 0; g < Fo; ++g) {
+    z.out[g] = C + g * fsP;
+    z.out_pstride[g] = Kz;
+  }
+  z.out_kz = Kz;
+  z.npencils = (long long)N1 * N2;
+  z.fac = (T)(1.0 / ((double)N1 * N2 * N3));
+  z.plan = *plan_for(c, N3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysMHD<T>{}, "mhd z-fused"));
+  AxisArgs<T> d = axis_common<T>(c, N2);
+  d.in = C;
+  d.out = D;
+  d.in_ostride = (long long)N2 * Kz;
+  d.in_rstride = Kz;
+  d.out_ostride = (long long)N2 * Kz;
+  d.out_rstride = Kz;
+  d.nouter = Fo * N1;
+  d.ncols = Kz;
+  d.in_rows = N2;
+  d.out_rows = N2;
+  d.in_map = map_id(N2);
+  d.out_map = map_id(N2);
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "mhd y-forward")));
+  XEpiArgs<T> e{};
+  e.in = D;
+  e.in_fstride = fsP;
+  e.in_rstride = (long long)N2 * Kz;
+  e.in_ostride = Kz;
+  e.n1 = N1;
+  e.n2 = N2;
+  e.n3h = N3h;
+  e.kz = Kz;
+  e.out_map = map_id(N1);
+  e.plan = *plan_for(c, N1);
+  e.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e, epi, "mhd x-forward+epilogue");
+}
+
+// ---------------------------------------------------------------------------
+// 2x-padded memory closures (t-model, static and dynamic tau-model)
+// ---------------------------------------------------------------------------
+struct MemCfg {
+  const char* tag;     // scratch name prefix
+  const double* filt;  // test filter masks (N grid) or null
+  int kfp;             // test-filter split (0 = seperateModes)
+  bool want_plp;
+  bool want_box;
+  int kfb;
+};
+
+// Stage A: u -> PL on the full 2x grid (q part and unpad_2x part).
+template <typename T>
+int run_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const MemCfg& m, Cx<T>** B2_out,
+           Cx<T>** PLq_out, Cx<T>* PLp, Cx<T>* Lbox) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int F1 = 2 * N1, F2 = 2 * N2, F3 = 2 * N3, F3h = N3 + 1, Kz = N3 / 2;
+  int st = PSB_OK;
+  std::string t = m.tag;
+  Cx<T>* A2 = scratch<T>(c, (t + ".A2").c_str(), (size_t)3 * F1 * N2 * Kz, &st);
+  Cx<T>* B2 = scratch<T>(c, (t + ".B2").c_str(), (size_t)3 * F1 * F2 * Kz, &st);
+  Cx<T>* C2 = scratch<T>(c, "mem.C2", (size_t)6 * F1 * F2 * F3h, &st);
+  Cx<T>* D2 = scratch<T>(c, "mem.D2", (size_t)6 * F1 * F2 * F3h, &st);
+  Cx<T>* E = scratch<T>(c, (t + ".E").c_str(), (size_t)3 * F1 * F2 * F3h, &st);
+  if (st != PSB_OK) return st;
+  *B2_out = B2;
+  *PLq_out = E;
+  if (!Qin) return PSB_OK;
+  const long long fsN = (long long)N1 * N2 * N3h;
+  AxisArgs<T> a = axis_common<T>(c, F1);
+  a.in = Qin;
+  a.out = A2;
+  a.in_fstride = fsN;
+  a.in_ostride = N3h;
+  a.in_rstride = (long long)N2 * N3h;
+  a.out_fstride = (long long)F1 * N2 * Kz;
+  a.out_ostride = Kz;
+  a.out_rstride = (long long)N2 * Kz;
+  a.nouter = N2;
+  a.ncols = Kz;
+  a.in_rows = N1;
+  a.out_rows = F1;
+  a.in_map = map_pad2x_nyq0(N1);
+  a.out_map = map_id(F1);
+  a.k_row = c->kx;
+  a.k_outer = c->ky;
+  a.k_col = c->kz;
+  if (m.filt) {
+    PSB_TRY((launch_axis<T, true>(c, a, PreMask3<T>{m.filt, m.filt + N1, m.filt + N1 + N2},
+                                  "2x x-inverse (test-filtered)")));
+  } else {
+    PSB_TRY((launch_axis<T, true>(c, a, PreCopyN<T, 3>{}, "2x x-inverse")));
+  }
+  AxisArgs<T> b = axis_common<T>(c, F2);
+  b.in = A2;
+  b.out = B2;
+  b.in_ostride = (long long)N2 * Kz;
+  b.in_rstride = Kz;
+  b.out_ostride = (long long)F2 * Kz;
+  b.out_rstride = Kz;
+  b.nouter = 3 * F1;
+  b.ncols = Kz;
+  b.in_rows = N2;
+  b.out_rows = F2;
+  b.in_map = map_pad2x_nyq0(N2);
+  b.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "2x y-inverse")));
+  ZArgs<T> z{};
+  const long long fsB = (long long)F1 * F2 * Kz, fsC = (long long)F1 * F2 * F3h;
+  for (int f = 0; f < 3; ++f) {
+    z.in[f] = B2 + f * fsB;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+  }
+  for (int g = 0; g < 6; ++g) {
+    z.out[g] = C2 + g * fsC;
+    z.out_pstride[g] = F3h;
+  }
+  z.out_kz = F3h;
+  z.npencils = (long long)F1 * F2;
+  const double s2 = std::sqrt(8.0 * std::sqrt((double)N1 * N2 * N3));
+  z.fac = (T)(s2 / ((double)F1 * F2 * F3));
+  z.plan = *plan_for(c, F3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysProducts<T>{}, "2x z-products"));
+  AxisArgs<T> d = axis_common<T>(c, F2);
+  d.in = C2;
+  d.out = D2;
+  d.in_ostride = (long long)F2 * F3h;
+  d.in_rstride = F3h;
+  d.out_ostride = (long long)F2 * F3h;
+  d.out_rstride = F3h;
+  d.nouter = 6 * F1;
+  d.ncols = F3h;
+  d.in_rows = F2;
+  d.out_rows = F2;
+  d.in_map = map_id(F2);
+  d.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "2x y-forward")));
+  EpiPL<T> epi{};
+  epi.Q = Qin;
+  epi.fstride_n = fsN;
+  epi.N1 = N1;
+  epi.N2 = N2;
+  epi.N3 = N3;
+  epi.n3h = N3h;
+  epi.nf2 = F2;
+  epi.nf3h = F3h;
+  epi.fstride_2x = fsC;
+  epi.kf = ktabs<T>(c->kxf, c->kyf, c->kzf);
+  epi.nu = (T)p->nu;
+  epi.rotate = p->rotate;
+  epi.Om1 = (T)p->Om1;
+  epi.Om2 = (T)p->Om2;
+  epi.Om3 = (T)p->Om3;
+  epi.filt = m.filt;
+  epi.kfp = m.kfp;
+  epi.PLq = E;
+  epi.PLp = PLp;
+  epi.Lbox = Lbox;
+  epi.kfb = m.kfb;
+  XEpiArgs<T> e{};
+  e.in = D2;
+  e.in_fstride = fsC;
+  e.in_rstride = (long long)F2 * F3h;
+  e.in_ostride = F3h;
+  e.n1 = F1;
+  e.n2 = F2;
+  e.n3h = F3h;
+  e.kz = F3h;
+  e.out_map = map_id(F1);
+  e.plan = *plan_for(c, F1);
+  e.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e, epi, "2x x-forward+PL");
+}
+
+// Stage B: PLQL from u (B2) and PL_q (E) -> 9 products -> N-grid epilogue.
+template <typename T>
+int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int F1 = 2 * N1, F2 = 2 * N2, F3 = 2 * N3, F3h = N3 + 1, Kz = N3 / 2;
+  int st = PSB_OK;
+  Cx<T>* A3 = scratch<T>(c, "mem.A3", (size_t)3 * F1 * F2 * F3h, &st);
+  Cx<T>* B3 = scratch<T>(c, "mem.B3", (size_t)3 * F1 * F2 * F3h, &st);
+  Cx<T>* C3 = scratch<T>(c, "mem.C3", (size_t)9 * F1 * F2 * Kz, &st);
+  Cx<T>* D3 = scratch<T>(c, "mem.D3", (size_t)9 * F1 * N2 * Kz, &st);
+  if (st != PSB_OK) return st;
+  if (!B2) return PSB_OK;
+  const long long fsC = (long long)F1 * F2 * F3h;
+  AxisArgs<T> a = axis_common<T>(c, F1);
+  a.in = E;
+  a.out = A3;
+  a.in_fstride = fsC;
+  a.in_ostride = F3h;
+  a.in_rstride = (long long)F2 * F3h;
+  a.out_fstride = fsC;
+  a.out_ostride = F3h;
+  a.out_rstride = (long long)F2 * F3h;
+  a.nouter = F2;
+  a.ncols = F3h;
+  a.in_rows = F1;
+  a.out_rows = F1;
+  a.in_map = map_id(F1);
+  a.out_map = map_id(F1);
+  PSB_TRY((launch_axis<T, true>(c, a, PreCopyN<T, 3>{}, "PLq x-inverse")));
+  AxisArgs<T> b = axis_common<T>(c, F2);
+  b.in = A3;
+  b.out = B3;
+  b.in_ostride = (long long)F2 * F3h;
+  b.in_rstride = F3h;
+  b.out_ostride = (long long)F2 * F3h;
+  b.out_rstride = F3h;
+  b.nouter = 3 * F1;
+  b.ncols = F3h;
+  b.in_rows = F2;
+  b.out_rows = F2;
+  b.in_map = map_id(F2);
+  b.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "PLq y-inverse")));
+  ZArgs<T> z{};
+  const long long fsB = (long long)F1 * F2 * Kz;
+  for (int f = 0; f < 3; ++f) {
+    z.in[f] = B2 + f * fsB;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+    z.in[3 + f] = B3 + f * fsC;
+    z.in_pstride[3 + f] = F3h;
+    z.in_kz[3 + f] = F3h;
+  }
+  const long long fsO = (long long)F1 * F2 * Kz;
+  for (int g = 0; g < 9; ++g) {
+    z.out[g] = C3 + g * fsO;
+    z.out_pstride[g] = Kz;
+  }
+  z.out_kz = Kz;
+  z.npencils = (long long)F1 * F2;
+  const double s2 = std::sqrt(8.0 * std::sqrt((double)N1 * N2 * N3));
+  z.fac = (T)(s2 / ((double)F1 * F2 * F3));
+  z.plan = *plan_for(c, F3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysPLQL<T>{}, "PLQL z-products"));
+  AxisArgs<T> d = axis_common<T>(c, F2);
+  d.in = C3;
+  d.out = D3;
+  d.in_ostride = (long long)F2 * Kz;
+  d.in_rstride = Kz;
+  d.out_ostride = (long long)N2 * Kz;
+  d.out_rstride = Kz;
+  d.nouter = 9 * F1;
+  d.ncols = Kz;
+  d.in_rows = F2;
+  d.out_rows = N2;
+  d.in_map = map_id(F2);
+  d.out_map = map_pad2x(N2);
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "PLQL y-forward")));
+  XEpiArgs<T> e{};
+  e.in = D3;
+  e.in_fstride = (long long)F1 * N2 * Kz;
+  e.in_rstride = (long long)N2 * Kz;
+  e.in_ostride = Kz;
+  e.n1 = N1;
+  e.n2 = N2;
+  e.n3h = N3h;
+  e.kz = Kz;
+  e.out_map = map_pad2x(N1);
+  e.plan = *plan_for(c, F1);
+  e.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e, epi, "PLQL x-forward+epilogue");
+}
+
+}  // namespace
+
+// ===========================================================================
+// dispatch
+// ===========================================================================
+namespace psbh {
+
+template <typename T>
+StepIO<T> make_io(psb_ctx* c, void* Q, void* Q0, void* comp, void* rhs, void* read_out, void* w0, int mode,
+                  double dtc) {
+  StepIO<T> io{};
+  io.Q = reinterpret_cast<Cx<T>*>(Q);
+  io.Q0 = reinterpret_cast<Cx<T>*>(Q0);
+  io.comp = reinterpret_cast<Cx<T>*>(comp);
+  io.rhs_out = reinterpret_cast<Cx<T>*>(rhs);
+  io.read_out = reinterpret_cast<Cx<T>*>(read_out);
+  io.w0_out = reinterpret_cast<Cx<T>*>(w0);
+  io.fstride = (long long)c->N1 * c->N2 * c->N3h;
+  io.n2 = c->N2;
+  io.n3h = c->N3h;
+  io.mode = mode;
+  io.dtc = (T)dtc;
+  return io;
+}
+
+template StepIO<double> make_io<double>(psb_ctx*, void*, void*, void*, void*, void*, void*, int, double);
+template StepIO<float> make_io<float>(psb_ctx*, void*, void*, void*, void*, void*, void*, int, double);
+
+int dtau_rhs_d(psb_ctx* c, StepIO<double> io, const psb_params* p, double* tau_out);
+int dtau_rhs_f(psb_ctx* c, StepIO<float> io, const psb_params* p, double* tau_out);
+
+template <typename T>
+int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, double* tau_out) {
+  const Cx<T>* Qin = io.Q;
+  switch (closure) {
+    case PSB_DNS:
+    case PSB_SMAG: {
+      const bool smag = closure == PSB_SMAG;
+      if (smag) {
+        EpiNS<T, true> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
+                           (T)p->Om3, 0, c->N1 / 2, c->N2 / 2, c->N3 / 2};
+        const double csd2 = 0.16 * c->Delta * 0.16 * c->Delta;
+        return run_ns32<T>(c, Qin, PreStrain<T>{}, PhysSmag<T>{(T)csd2}, epi);
+      }
+      EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
+                          (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
+      return run_ns32<T>(c, Qin, PreCopyN<T, 3>{}, PhysProducts<T>{}, epi);
+    }
+    case PSB_MHD: {
+      EpiMHD<T> epi{io, ktabs<T>(c->kx, c->ky, c->kz), c->mx, c->my, c->mz,
+                    reinterpret_cast<const Cx<T>*>(p->force), (T)p->nu, (T)(p->eta < 0 ? p->nu : p->eta)};
+      return run_mhd<T>(c, Qin, epi);
+    }
+    case PSB_TMODEL:
+    case PSB_TAU_STATIC: {
+      int st = PSB_OK;
+      Cx<T>* PLp = scratch<T>(c, "mem.PLp", (size_t)3 * c->N1 * c->N2 * c->N3h, &st);
+      if (st != PSB_OK) return st;
+      MemCfg m{"memu", nullptr, 0, true, false, 0};
+      Cx<T>*B2 = nullptr, *E = nullptr;
+      if (Qin) {
+        st = cuda_ok(c, cudaMemsetAsync(PLp, 0, sizeof(Cx<T>) * 3 * c->N1 * c->N2 * c->N3h, c->stream), "memset");
+        if (st != PSB_OK) return st;
+      }
+      PSB_TRY(run_pl<T>(c, Qin, p, m, &B2, &E, PLp, nullptr));
+      double coef;
+      if (closure == PSB_TMODEL) {
+        coef = p->Ct * p->t;
+      } else {
+        const double tau = p->tau_a + p->tau_b * p->t;
+        if (tau_out) *tau_out = tau;
+        coef = tau > 0.0 ? tau : 0.0;
+      }
+      EpiPLQL<T> epi{};
+      epi.io = io;
+      epi.k = ktabs<T>(c->kx, c->ky, c->kz);
+      epi.PLp = PLp;
+      epi.coef = (T)coef;
+      epi.rotate = p->rotate;
+      epi.Om1 = (T)p->Om1;
+      epi.Om2 = (T)p->Om2;
+      epi.Om3 = (T)p->Om3;
+      epi.ny1 = c->N1 / 2;
+      epi.ny2 = c->N2 / 2;
+      epi.ny3 = c->N3 / 2;
+      epi.plql_out = nullptr;
+      return run_plql<T>(c, m, Qin ? B2 : nullptr, E, epi);
+    }
+    case PSB_TAU_DYNAMIC:
+      if constexpr (sizeof(T) == 8)
+        return dtau_rhs_d(c, io, p, tau_out);
+      else
+        return dtau_rhs_f(c, io, p, tau_out);
+    default:
+      return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");
+  }
+}
+
+template int rhs_dispatch<double>(psb_ctx*, int, StepIO<double>, const psb_params*, double*);
+template int rhs_dispatch<float>(psb_ctx*, int, StepIO<float>, const psb_params*, double*);
+
+// SGS of a filtered DNS field
+template <typename T>
+int sgs_dns_run(psb_ctx* c, const void* fields, void* w0, void* tau6) {
+  EpiSGSDNS<T> epi{ktabs<T>(c->kx, c->ky, c->kz), c->gx, c->gy, c->gz, reinterpret_cast<Cx<T>*>(w0),
+                   reinterpret_cast<Cx<T>*>(tau6), (long long)c->N1 * c->N2 * c->N3h, c->N2, c->N3h};
+  PreFiltered<T> pre{c->gx, c->gy, c->gz};
+  return run_ns32<T>(c, reinterpret_cast<const Cx<T>*>(fields), pre, PhysSGSDNS<T>{}, epi);
+}
+template int sgs_dns_run<double>(psb_ctx*, const void*, void*, void*);
+template int sgs_dns_run<float>(psb_ctx*, const void*, void*, void*);
+
+// exported for the dynamic tau-model translation unit
+template <typename T>
+int mem_stage_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const char* tag, const double* filt, int kfp,
+                 Cx<T>* PLp, Cx<T>* Lbox, int kfb, Cx<T>** B2, Cx<T>** E) {
+  MemCfg m{tag, filt, kfp, PLp != nullptr, Lbox != nullptr, kfb};
+  return run_pl<T>(c, Qin, p, m, B2, E, PLp, Lbox);
+}
+template <typename T>
+int mem_stage_plql(psb_ctx* c, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
+  MemCfg m{"", nullptr, 0, false, false, 0};
+  return run_plql<T>(c, m, B2, E, epi);
+}
+template int mem_stage_pl<double>(psb_ctx*, const Cx<double>*, const psb_params*, const char*, const double*, int,
+                                  Cx<double>*, Cx<double>*, int, Cx<double>**, Cx<double>**);
+template int mem_stage_pl<float>(psb_ctx*, const Cx<float>*, const psb_params*, const char*, const double*, int,
+                                 Cx<float>*, Cx<float>*, int, Cx<float>**, Cx<float>**);
+template int mem_stage_plql<double>(psb_ctx*, Cx<double>*, Cx<double>*, EpiPLQL<double>);
+template int mem_stage_plql<float>(psb_ctx*, Cx<float>*, Cx<float>*, EpiPLQL<float>);
+
+}  // namespace psbh

@@ -1,0 +1,214 @@
+"""MHD path of the MPI solver, single GPU, with the reference's names.
+
+Mirrors PySpectral/src_MPI: ``gridclass`` (Classes.py:177-236), ``FFTclass``
+(Classes.py:238-265), ``variables`` for ``turb_model='MHD'``
+(Classes.py:5-149), ``computeRHS_MHD`` (RHSfunctions.py:95-175),
+``advanceQ_RK4`` (time_schemes.py:2-7) and the MHD diagnostics
+(Classes.py:269-448).  The slab decomposition and its Alltoall transposes are
+replaced by single-GPU pencil passes, so ``num_processes`` must be 1.
+Spectra are unnormalised ``rfftn`` results, as in the MPI solver.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _capi
+
+TWO_PI = 2.0 * np.pi
+
+
+def _cdtype(p):
+    return torch.complex128 if p == 64 else torch.complex64
+
+
+def _rdtype(p):
+    return torch.float64 if p == 64 else torch.float32
+
+
+class gridclass:
+    def __init__(self, N1, N2, N3, x, y, z, kc, num_processes=1, L1=TWO_PI, L2=TWO_PI, L3=TWO_PI, mpi_rank=0,
+                 comm=None, turb_model="MHD", device=0):
+        if num_processes != 1:
+            raise ValueError("the GPU build runs one rank per run; num_processes must be 1")
+        self.N1, self.N2, self.N3 = int(N1), int(N2), int(N3)
+        self.Npx, self.Npy = self.N1, self.N2
+        self.num_processes, self.mpi_rank, self.comm = 1, 0, comm
+        self.L1, self.L2, self.L3 = float(L1), float(L2), float(L3)
+        self.x, self.y, self.z = x, y, z
+        self.dx = float(x[1, 0, 0] - x[0, 0, 0])
+        self.dy = float(y[0, 1, 0] - y[0, 0, 0])
+        self.dz = float(z[0, 0, 1] - z[0, 0, 0])
+        self.kc = int(kc)
+        self.Delta = np.pi / self.kc
+        self.device = device
+        self._ctx = {}
+
+    @classmethod
+    def periodic(cls, N, kc=None, device=0):
+        a = np.arange(N) * (TWO_PI / N)
+        y, x, z = np.meshgrid(a, a, a)
+        return cls(N, N, N, x, y, z, N // 2 if kc is None else kc, device=device)
+
+    def ctx(self, precision=64):
+        c = self._ctx.get(precision)
+        if c is None:
+            c = _capi.Context(self.N1, self.N2, self.N3, (self.L1, self.L2, self.L3), (self.dx, self.dy, self.dz),
+                              self.kc, precision, self.device)
+            self._ctx[precision] = c
+        return c
+
+
+class FFTclass:
+    """``myfft3D`` (unnormalised rfftn) / ``myifft3D`` (normalised irfftn) and
+    the in-place 2/3-rule ``dealias``."""
+
+    def __init__(self, N1, N2, N3, nthreads=1, fft_type=None, Npx=None, Npy=None, num_processes=1, comm=None,
+                 mpi_rank=0, grid=None, precision=64):
+        self.N1, self.N2, self.N3 = N1, N2, N3
+        self.grid = grid
+        self.precision = precision
+        self._own = None
+
+    def _ctx(self):
+        if self.grid is not None:
+            return self.grid.ctx(self.precision)
+        if self._own is None:
+            self._own = _capi.Context(self.N1, self.N2, self.N3, precision=self.precision)
+        return self._own
+
+    def myfft3D(self, u, uhat):
+        self._ctx().r2c(u.contiguous(), uhat, 1)
+        return uhat
+
+    def myifft3D(self, uhat, u):
+        self._ctx().c2r(uhat.contiguous(), u, 1)
+        return u
+
+
+class variables:
+    """MPI ``variables`` for ``turb_model='MHD'`` (src_MPI/Classes.py:82-149).
+    ``u,v,w,B1,B2,B3`` are physical fields (``initDomain='Physical'``) or
+    ``uhat..`` spectra (``'Fourier'``, re-symmetrised by a round trip)."""
+
+    def __init__(self, turb_model, rotate, Om1, Om2, Om3, grid, u, v, w, B1, B2, B3, uhat=None, vhat=None,
+                 what=None, t=0.0, dt=0.0, nu=0.0, myFFT=None, mpi_rank=0, initDomain="Physical",
+                 time_scheme="RK4", precision=64, kahan=None, Bhat=None, forcing=True):
+        if turb_model != "MHD":
+            raise ValueError("only turb_model='MHD' of the MPI solver is on this path")
+        if time_scheme != "RK4":
+            raise ValueError("Error, time scheme " + str(time_scheme) + " not implemented for MHD equations")
+        self.turb_model, self.rotate = turb_model, int(rotate)
+        self.t, self.dt, self.nu = float(t), float(dt), float(nu)
+        self.lam = self.nu
+        self.precision = precision
+        self.time_scheme = time_scheme
+        dev = torch.device("cuda", grid.device)
+        ctx = grid.ctx(precision)
+        N1, N2, N3 = grid.N1, grid.N2, grid.N3
+        sh = (N1, N2, N3 // 2 + 1)
+        self.Q = torch.zeros((6,) + sh, dtype=_cdtype(precision), device=dev)
+        if initDomain == "Physical":
+            phys = torch.stack([torch.as_tensor(np.asarray(a), device=dev).to(_rdtype(precision))
+                                for a in (u, v, w, B1, B2, B3)]).contiguous()
+            ctx.r2c(phys, self.Q, 6)
+        else:
+            src = torch.stack([torch.as_tensor(np.asarray(a), device=dev).to(_cdtype(precision))
+                               for a in (uhat, vhat, what)] +
+                              [torch.as_tensor(np.asarray(a), device=dev).to(_cdtype(precision)) for a in Bhat])
+            phys = torch.empty((6, N1, N2, N3), dtype=_rdtype(precision), device=dev)
+            ctx.c2r(src.contiguous(), phys, 6)
+            ctx.r2c(phys, self.Q, 6)
+        self.U = self.Q.clone()
+        self.nvars = 6
+        self.force = torch.zeros((3,) + sh, dtype=_cdtype(precision), device=dev)
+        if forcing:  # kf = 2, f0 = 0.25 (src_MPI/Classes.py:91-94)
+            kf, f0 = 2, 0.25
+            X = torch.as_tensor(np.asarray(grid.x), device=dev, dtype=torch.float64)
+            Y = torch.as_tensor(np.asarray(grid.y), device=dev, dtype=torch.float64)
+            Z = torch.as_tensor(np.asarray(grid.z), device=dev, dtype=torch.float64)
+            fp = torch.zeros((3, N1, N2, N3), dtype=_rdtype(precision), device=dev)
+            fp[0] = (f0 * torch.sin(kf * X) * torch.cos(kf * Y) * torch.cos(kf * Z)).to(fp.dtype)
+            fp[1] = (-f0 * torch.cos(kf * X) * torch.sin(kf * Y) * torch.cos(kf * Z)).to(fp.dtype)
+            ctx.r2c(fp, self.force, 3)
+        use_kahan = (precision == 32) if kahan is None else bool(kahan)
+        self.comp = torch.zeros_like(self.Q) if use_kahan else None
+        self.computeRHS = computeRHS_MHD
+        self.advanceQ = advanceQ_RK4
+
+    @property
+    def uhat(self):
+        return self.U[0]
+
+    @property
+    def vhat(self):
+        return self.U[1]
+
+    @property
+    def what(self):
+        return self.U[2]
+
+    @property
+    def B1hat(self):
+        return self.U[3]
+
+    @property
+    def B2hat(self):
+        return self.U[4]
+
+    @property
+    def B3hat(self):
+        return self.U[5]
+
+    def U2Q(self):
+        self.Q.copy_(self.U)
+
+    def Q2U(self):
+        self.U.copy_(self.Q)
+
+    def params(self):
+        return _capi.make_params(nu=self.nu, eta=self.lam, t=self.t, dt=self.dt,
+                                 force=self.force.data_ptr() if self.force is not None else None)
+
+
+def computeRHS_MHD(main, grid, myFFT=None):
+    """src_MPI/RHSfunctions.py:95-175; ``main.Q`` becomes the RHS and the
+    six stored fields are dealiased in place, as in the reference."""
+    ctx = grid.ctx(main.precision)
+    rhs = torch.empty_like(main.Q)
+    ctx.rhs(_capi.MHD, main.Q, rhs, main.params(), read_out=main.U)
+    main.Q = rhs
+
+
+def advanceQ_RK4(main, grid, myFFT=None):
+    """src_MPI/time_schemes.py:2-7."""
+    grid.ctx(main.precision).step(_capi.MHD, main.Q, main.params(), 1, comp=main.comp, read_out=main.U)
+
+
+def advance(main, grid, nsteps):
+    grid.ctx(main.precision).step(_capi.MHD, main.Q, main.params(), int(nsteps), comp=main.comp, read_out=main.U)
+
+
+class utilitiesClass:
+    """MPI diagnostics (src_MPI/Classes.py:269-448), normalised by (N1 N2 N3)^2."""
+
+    def computeEnergy(self, main, grid):
+        return grid.ctx(main.precision).energy(main.U[0:3].contiguous(), _capi.NORM_MPI)
+
+    def computeMHDEnergy(self, main, grid):
+        return grid.ctx(main.precision).energy(main.U[3:6].contiguous(), _capi.NORM_MPI)
+
+    def computeEnstrophy(self, main, grid):
+        return grid.ctx(main.precision).enstrophy(main.U[0:3].contiguous(), _capi.NORM_MPI)
+
+    def computeCrossHelicity(self, main, grid):
+        return grid.ctx(main.precision).cross_helicity(main.U[0:3].contiguous(), main.U[3:6].contiguous(),
+                                                      _capi.NORM_MPI)
+
+    def computeSpectrum(self, main, grid):
+        s = grid.ctx(main.precision).spectrum_mpi(main.U[0:3].contiguous())
+        return np.linspace(0, s.shape[0] - 1, s.shape[0]), s
+
+    def computeMHDSpectrum(self, main, grid):
+        s = grid.ctx(main.precision).spectrum_mpi(main.U[3:6].contiguous())
+        return np.linspace(0, s.shape[0] - 1, s.shape[0]), s

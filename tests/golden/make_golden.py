@@ -1,0 +1,327 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container that has the PySpectral sources (default
+``/root/reference``; override with ``PYSPECTRAL_REF``):
+
+    python tests/golden/make_golden.py
+
+The reference is Python 2 code that imports pyFFTW, mpi4py and scipy.weave.
+This script executes its unmodified sources under a load-time shim:
+
+* every ``/`` is rewritten by an AST pass into ``_py2div(a, b)`` (floor
+  division when both operands are integers, true division otherwise);
+* ``np`` is a thin proxy over NumPy 2 that restores ``np.int`` and accepts a
+  float ``num`` in ``np.linspace``;
+* ``pyfftw`` is a stand-in whose ``FFTW`` object copies into its input buffer,
+  runs ``scipy.fft`` (normalised inverse, like pyFFTW's default
+  ``normalise_idft=True``) and returns its internal output buffer;
+* ``RHSfunctionsWEAVE`` is an empty module; ``mpi4py`` a single-rank stand-in.
+
+``advanceQ_RK4`` lives in the driver script, which runs a whole simulation at
+import time, so its four lines (``src/PySpec_3d.py:96-105``) are restated in
+:func:`ref_rk4_step`.
+
+Outputs (all FP64, a few hundred KB in total):
+
+* ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
+  closure (DNS, Smagorinsky, t-model, static and dynamic tau-model; DNS and
+  t-model also with rotation), plus the diagnostics;
+* ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
+* ``tgv64_benchmark.npz`` -- the reference's known-answer energy and
+  dissipation history (``run/TGV_Validate100/benchmark_sol_64.npz``).
+"""
+from __future__ import annotations
+
+import ast
+import contextlib
+import io
+import math
+import os
+import sys
+import types
+
+import numpy as np
+import scipy.fft
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+from oracle import spectral_oracle as orc  # noqa: E402  (inputs only)
+
+REF = os.environ.get("PYSPECTRAL_REF", "/root/reference")
+SRC = os.path.join(REF, "PySpectral", "src")
+SRC_MPI = os.path.join(REF, "PySpectral", "src_MPI")
+
+
+# ---------------------------------------------------------------- shim ----
+def _py2div(a, b):
+    def isint(x):
+        if isinstance(x, (bool, int, np.integer)):
+            return True
+        return isinstance(x, np.ndarray) and np.issubdtype(x.dtype, np.integer)
+    if isint(a) and isint(b):
+        return a // b
+    return a / b
+
+
+class _DivRewrite(ast.NodeTransformer):
+    def visit_BinOp(self, node):
+        self.generic_visit(node)
+        if isinstance(node.op, ast.Div):
+            return ast.copy_location(
+                ast.Call(func=ast.Name(id="_py2div", ctx=ast.Load()), args=[node.left, node.right],
+                         keywords=[]), node)
+        return node
+
+    def visit_AugAssign(self, node):
+        self.generic_visit(node)
+        if isinstance(node.op, ast.Div):
+            tgt = node.target
+            load = ast.Name(id=tgt.id, ctx=ast.Load()) if isinstance(tgt, ast.Name) else tgt
+            return ast.copy_location(ast.Assign(targets=[tgt], value=ast.Call(
+                func=ast.Name(id="_py2div", ctx=ast.Load()), args=[load, node.value], keywords=[])), node)
+        return node
+
+
+class _NumpyProxy(types.ModuleType):
+    def __init__(self):
+        super().__init__("numpy_py2_proxy")
+        self.int = int
+
+    def __getattr__(self, name):
+        return getattr(np, name)
+
+    @staticmethod
+    def linspace(start, stop, num=50, *a, **k):
+        return np.linspace(start, stop, int(num), *a, **k)
+
+
+class _FFTW:
+    def __init__(self, inp, out, axes=(0, 1, 2), direction="FFTW_FORWARD", threads=1, **kw):
+        self.input_array, self.output_array = inp, out
+        self.direction = direction
+
+    def __call__(self, input_array=None):
+        if input_array is not None:
+            self.input_array[...] = input_array
+        if self.direction == "FFTW_BACKWARD":
+            self.output_array[...] = scipy.fft.irfftn(self.input_array, s=self.output_array.shape)
+        else:
+            self.output_array[...] = scipy.fft.rfftn(self.input_array)
+        return self.output_array
+
+
+def _install_stubs():
+    pyfftw = types.ModuleType("pyfftw")
+    pyfftw.n_byte_align_empty = lambda shape, align, dtype: np.empty(shape, dtype=dtype)
+    pyfftw.FFTW = _FFTW
+    sys.modules["pyfftw"] = pyfftw
+    sys.modules["RHSfunctionsWEAVE"] = types.ModuleType("RHSfunctionsWEAVE")
+
+    class _Comm:
+        def Get_size(self):
+            return 1
+
+        def Get_rank(self):
+            return 0
+
+        def Alltoall(self, send, recv):
+            recv[...] = np.asarray(send).reshape(recv.shape)
+
+        def gather(self, x, root=0):
+            return [x]
+
+    mpi4py = types.ModuleType("mpi4py")
+    mpi = types.ModuleType("mpi4py.MPI")
+    mpi.COMM_WORLD = _Comm()
+    mpi4py.MPI = mpi
+    sys.modules["mpi4py"] = mpi4py
+    sys.modules["mpi4py.MPI"] = mpi
+
+
+def _load(path, name):
+    with open(path) as f:
+        tree = ast.parse(f.read(), filename=path)
+    tree = ast.fix_missing_locations(_DivRewrite().visit(tree))
+    mod = types.ModuleType(name)
+    mod.__dict__["_py2div"] = _py2div
+    mod.__dict__["__name__"] = name
+    sys.modules[name] = mod
+    code = compile(tree, path, "exec")
+    # the sources do "import numpy as np": bind np to the proxy afterwards
+    exec(code, mod.__dict__)
+    mod.__dict__["np"] = _NumpyProxy()
+    return mod
+
+
+def load_serial():
+    _install_stubs()
+    for n in ("padding", "RHSfunctions", "Classes"):
+        sys.modules.pop(n, None)
+    pad = _load(os.path.join(SRC, "padding.py"), "padding")
+    rhs = _load(os.path.join(SRC, "RHSfunctions.py"), "RHSfunctions")
+    for k, v in pad.__dict__.items():  # "from padding import *"
+        if not k.startswith("__"):
+            rhs.__dict__.setdefault(k, v)
+    cls = _load(os.path.join(SRC, "Classes.py"), "Classes")
+    for k, v in rhs.__dict__.items():  # "from RHSfunctions import *"
+        if not k.startswith("__") and k != "np":
+            cls.__dict__.setdefault(k, v)
+    return cls
+
+
+def load_mpi():
+    _install_stubs()
+    for n in ("padding", "RHSfunctions", "Classes", "time_schemes"):
+        sys.modules.pop(n, None)
+    _load(os.path.join(SRC_MPI, "padding.py"), "padding")
+    rhs = _load(os.path.join(SRC_MPI, "RHSfunctions.py"), "RHSfunctions")
+    ts = _load(os.path.join(SRC_MPI, "time_schemes.py"), "time_schemes")
+    cls = _load(os.path.join(SRC_MPI, "Classes.py"), "Classes")
+    for src in (rhs, ts):
+        for k, v in src.__dict__.items():
+            if not k.startswith("__") and k != "np":
+                cls.__dict__.setdefault(k, v)
+    return cls
+
+
+# ------------------------------------------------------------ drivers ----
+def ref_rk4_step(main, grid, myFFT, utilities):
+    """``advanceQ_RK4`` restated from ``src/PySpec_3d.py:96-105``."""
+    Q0 = np.zeros(np.shape(main.Q), dtype="complex")
+    Q0[:, :, :] = main.Q[:, :, :]
+    rk4const = np.array([1.0 / 4, 1.0 / 3, 1.0 / 2, 1.0])
+    utilities.preAdvanceQ_hook(main, grid, myFFT)
+    utilities.compute_dt(main, grid)
+    for i in range(0, 4):
+        main.computeRHS(main, grid, myFFT, utilities)
+        main.Q = Q0 + main.dt * rk4const[i] * main.Q
+    utilities.postAdvanceQ_hook(main, grid, myFFT)
+
+
+def _diag(Q):
+    return np.stack([Q[0::3, 0::3, 0::3], Q[1::3, 1::3, 1::3], Q[2::3, 2::3, 2::3]])
+
+
+def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), Ct=-10, dt0=-10,
+                dt1=-10, kc=None, cfl=None):
+    kc = N // 2 if kc is None else kc
+    x, y, z = orc.periodic_coords(N)
+    grid = C.gridclass(N, N, N, x, y, z, kc, 2 * np.pi, 2 * np.pi, 2 * np.pi)
+    myFFT = C.FFTclass(N, N, N, 1)
+    util = C.utilitiesClass()
+    cfl = -dt if cfl is None else cfl
+    with contextlib.redirect_stdout(io.StringIO()):
+        main = C.variables(0, turb_model, rotate, Om[0], Om[1], Om[2], grid, state[0].copy(),
+                           state[1].copy(), state[2].copy(), t, dt, nu, Ct, dt0, -10, dt1, -10, cfl, 3)
+    main.iteration = 1
+    return grid, myFFT, util, main
+
+
+def gen_serial(N, seed):
+    C = load_serial()
+    st = orc.isotropic_state(N, seed, k0=3.0)
+    st[:, 1:3, 2:4, 1] += 0.05 * (1 + 1j)          # non-Hermitian-free nudge off the analytic IC
+    out = {"state": st, "N": N}
+    nu, dt, t = 0.02, 0.01, 0.37
+    cases = [
+        ("dns", 0, {}),
+        ("dns_rot", 0, dict(rotate=1, Om=(0.3, -0.2, 0.5))),
+        ("smag", 1, {}),
+        ("smag_rot", 1, dict(rotate=1, Om=(0.1, 0.4, -0.25))),
+        ("tmodel", 2, dict(Ct=0.13)),
+        ("tmodel_rot", 2, dict(rotate=1, Om=(0.2, 0.0, 0.3))),
+        ("stau", "Static tau-model", dict(dt0=0.05, dt1=0.2)),
+        ("dtau", "Dynamic tau-model", {}),
+    ]
+    for name, tm, kw in cases:
+        grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
+        with contextlib.redirect_stdout(io.StringIO()):
+            main.computeRHS(main, grid, myFFT, util)
+        out[f"{name}_rhs"] = _diag(main.Q)
+        out[f"{name}_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+        if hasattr(main, "w0_u"):
+            out[f"{name}_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
+        if hasattr(main, "tau"):
+            out[f"{name}_tau"] = np.float64(np.real(main.tau))
+        grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
+        with contextlib.redirect_stdout(io.StringIO()):
+            ref_rk4_step(main, grid, myFFT, util)
+        out[f"{name}_step"] = _diag(main.Q)
+        out[f"{name}_step_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+    # diagnostics on the input state; kc = N/4 so that the sharp cutoff Gf
+    # (and with it the SGS stress of computeSGS_DNS) is not trivial
+    out["diag_kc"] = np.int64(N // 4)
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, kc=N // 4)
+    out["energy"] = np.float64(util.computeEnergy(main, grid))
+    out["energy_resolved"] = np.float64(util.computeEnergy_resolved(main, grid))
+    out["enstrophy"] = np.float64(util.computeEnstrophy(main, grid))
+    out["allstats"] = np.array([np.real(v) for v in util.computeAllStats(main, grid)], dtype=np.float64)
+    k, spec = util.computeSpectrum(main, grid)
+    out["spectrum_k"], out["spectrum"] = k, spec
+    k, spec = util.computeSpectrum_resolved(main, grid)
+    out["spectrum_res_k"], out["spectrum_res"] = k, spec
+    w0u, w0v, w0w = util.computeSGS_DNS(main, grid, myFFT)
+    out["sgs_dns_w0"] = np.stack([w0u[..., 0], w0v[..., 0], w0w[..., 0]])
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, cfl=0.4)
+    util.compute_dt(main, grid)
+    out["cfl_dt"] = np.float64(main.dt)
+    return out
+
+
+def gen_mhd(N, seed):
+    C = load_mpi()
+    comm = sys.modules["mpi4py.MPI"].COMM_WORLD
+    x, y, z = orc.periodic_coords(N)
+    u = orc.isotropic_state(N, seed, k0=3.0, normalise="none")
+    B = orc.isotropic_state(N, seed + 1, k0=3.0, normalise="none") * 0.7
+    phys = [np.fft.irfftn(a, s=(N, N, N), axes=(0, 1, 2)) for a in list(u) + list(B)]
+    nu, dt = 0.02, 0.005
+    out = {"N": N, "nu": nu, "dt": dt}
+    res = {}
+    for name in ("rhs", "step"):
+        with contextlib.redirect_stdout(io.StringIO()):
+            grid = C.gridclass(N, N, N, x, y, z, N // 2, 1, 2 * np.pi, 2 * np.pi, 2 * np.pi, 0, comm, "MHD")
+            myFFT = C.FFTclass(N, N, N, 1, "pyfftw", N, N, 1, comm, 0)
+            uh = np.zeros((N, N, N // 2 + 1), dtype=complex)
+            vh, wh = uh.copy(), uh.copy()
+            main = C.variables("MHD", 0, 0, 0, 0, grid, phys[0].copy(), phys[1].copy(), phys[2].copy(),
+                               phys[3], phys[4], phys[5], uh, vh, wh, 0.0, dt, nu, myFFT, 0,
+                               "Physical", "RK4")
+        if name == "rhs":
+            out["state"] = main.Q.copy()
+            out["force"] = main.force.copy()
+            main.computeRHS(main, grid, myFFT)
+            res["rhs"] = main.Q.copy()
+        else:
+            main.advanceQ(main, grid, myFFT)
+            res["step"] = main.Q.copy()
+    out.update(res)
+    util = C.utilitiesClass()
+    out["energy_u"] = np.float64(util.computeEnergy(main, grid))
+    out["energy_B"] = np.float64(util.computeMHDEnergy(main, grid))
+    k, s = util.computeSpectrum(main, grid)
+    out["spectrum_u"] = s
+    k, s = util.computeMHDSpectrum(main, grid)
+    out["spectrum_B"] = s
+    out["diag_state"] = np.stack([main.uhat, main.vhat, main.what, main.B1hat, main.B2hat, main.B3hat])
+    return out
+
+
+def main():
+    os.makedirs(HERE, exist_ok=True)
+    for N, seed in ((12, 11), (16, 5)):
+        d = gen_serial(N, seed)
+        np.savez_compressed(os.path.join(HERE, f"serial_N{N}.npz"), **d)
+        print("serial", N, sorted(d.keys())[:4], "...")
+    for N, seed in ((12, 21), (16, 7)):
+        d = gen_mhd(N, seed)
+        np.savez_compressed(os.path.join(HERE, f"mhd_N{N}.npz"), **d)
+        print("mhd", N)
+    b = np.load(os.path.join(REF, "PySpectral", "run", "TGV_Validate100", "benchmark_sol_64.npz"))
+    np.savez_compressed(os.path.join(HERE, "tgv64_benchmark.npz"), t=np.real(b["t"]),
+                        Energy=np.real(b["Energy"]), Dissipation=np.real(b["Dissipation"]))
+    print("tgv64 benchmark copied")
+
+
+if __name__ == "__main__":
+    main()

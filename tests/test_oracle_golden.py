@@ -1,0 +1,120 @@
+"""Pin the CPU oracle to the reference: fixtures produced by running the
+unmodified PySpectral sources (tests/golden/make_golden.py) and the
+reference's own known-answer TGV energy history."""
+import numpy as np
+import pytest
+
+from oracle import spectral_oracle as orc
+from tests.helpers import CASES, DT, NU, T, golden, rel
+
+FN = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "stau": orc.rhs_staumodel,
+      "dtau": orc.rhs_dtaumodel}
+
+
+def _fn(name):
+    return FN[name.split("_")[0]]
+
+
+def _read(name, res, Q):
+    base = name.split("_")[0]
+    if base == "dns":
+        return res[1]
+    if base == "smag":
+        return Q
+    return res[2]
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("name", list(CASES))
+def test_rhs_and_step_match_reference(N, name):
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT, **CASES[name][2])
+    st = d["state"]
+    res = _fn(name)(g, st, p)
+    assert rel(res[0], d[f"{name}_rhs"]) < 1e-13
+    if f"{name}_w0" in d:
+        assert rel(res[1], d[f"{name}_w0"]) < 1e-13
+    if f"{name}_tau" in d:
+        assert abs(res[3] - float(d[f"{name}_tau"])) <= 1e-13 * max(1.0, abs(float(d[f"{name}_tau"])))
+    Q, read = orc.advance_rk4(st, lambda q: (lambda r: (r[0], _read(name, r, q)))(_fn(name)(g, q, p)), DT)
+    assert rel(Q, d[f"{name}_step"]) < 1e-13
+    assert rel(read, d[f"{name}_step_uhat"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_diagnostics_match_reference(N):
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N, kc=int(d["diag_kc"]))
+    st = d["state"]
+    assert orc.energy(g, st) == pytest.approx(float(d["energy"]), rel=1e-14)
+    assert orc.energy_resolved(g, st) == pytest.approx(float(d["energy_resolved"]), rel=1e-14)
+    assert orc.enstrophy(g, st) == pytest.approx(float(d["enstrophy"]), rel=1e-14)
+    np.testing.assert_allclose(np.array(orc.all_stats(g, st, NU)), d["allstats"], rtol=1e-13)
+    k, s = orc.spectrum(g, st)
+    np.testing.assert_array_equal(k, d["spectrum_k"])
+    assert rel(s, d["spectrum"]) < 1e-14
+    _, s = orc.spectrum(g, st, filtered=True)
+    assert rel(s, d["spectrum_res"]) < 1e-14
+    w0, _ = orc.sgs_dns(g, st)
+    assert np.abs(d["sgs_dns_w0"]).max() > 1e-3
+    assert rel(w0, d["sgs_dns_w0"]) < 1e-13
+    assert orc.compute_dt(g, st, 0.4, NU, DT) == pytest.approx(float(d["cfl_dt"]), rel=1e-14)
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_mhd_matches_reference(N):
+    d = golden(f"mhd_N{N}.npz")
+    g = orc.MHDGrid(N, N, N, N // 2)
+    nu, dt = float(d["nu"]), float(d["dt"])
+    x, y, z = orc.periodic_coords(N)
+    assert rel(orc.mhd_forcing(g, x, y, z), d["force"]) < 1e-13
+    r, _ = orc.rhs_mhd(g, d["state"], nu, force=d["force"])
+    assert rel(r, d["rhs"]) < 1e-13
+    Q, _ = orc.advance_rk4(d["state"], lambda q: (orc.rhs_mhd(g, q, nu, force=d["force"])[0], None), dt)
+    assert rel(Q, d["step"]) < 1e-13
+    ds = d["diag_state"]
+    assert orc.mhd_energy(g, ds[:3]) == pytest.approx(float(d["energy_u"]), rel=1e-14)
+    assert orc.mhd_energy(g, ds[3:]) == pytest.approx(float(d["energy_B"]), rel=1e-14)
+    assert rel(orc.mhd_spectrum(g, ds[:3])[1], d["spectrum_u"]) < 1e-13
+    assert rel(orc.mhd_spectrum(g, ds[3:])[1], d["spectrum_B"]) < 1e-13
+
+
+def test_tgv64_known_answer_start():
+    """First 5 steps of the reference's TGV validation run (64^3, nu=1/100,
+    dt=0.010005) against its shipped energy history.  The shipped history
+    was produced with slightly different settings (its E agrees with the
+    reference code itself only to ~2.5e-4), so the bound is 5e-4."""
+    b = golden("tgv64_benchmark.npz")
+    t, E = b["t"], b["Energy"]
+    N = 64
+    g = orc.Grid.periodic(N)
+    orc.set_workers(4)
+    try:
+        st = orc.tgv_state(N)
+        assert orc.energy(g, st) == pytest.approx(0.125, rel=1e-14)
+        assert orc.enstrophy(g, st) == pytest.approx(3 * 0.125, rel=1e-14)
+        p = orc.Params(nu=0.01)
+        dt = t[2] - t[1]
+        Q = st
+        for n in range(1, 6):
+            Q, read = orc.advance_rk4(Q, lambda q: orc.rhs_nosgs(g, q, p), dt)
+            assert abs(orc.energy(g, read) - E[n]) / E[n] < 5e-4
+    finally:
+        orc.set_workers(1)
+
+
+def test_analytic_properties_of_the_oracle():
+    """Single-mode RHS = -nu k^2 uhat; divergence-free DNS RHS."""
+    N = 12
+    g = orc.Grid.periodic(N)
+    st = np.zeros((3, N, N, N // 2 + 1), dtype=complex)
+    st[1, 2, 0, 0] = 3.0 + 1.0j  # v(k=(2,0,0)) : transverse, k.u = 0
+    st[1, N - 2, 0, 0] = 3.0 - 1.0j
+    r, _ = orc.rhs_nosgs(g, st, orc.Params(nu=0.1))
+    expect = -0.1 * g.ksqr * st
+    assert rel(r, expect) < 1e-13
+    d = orc.isotropic_state(N, 3)
+    r, _ = orc.rhs_nosgs(g, d, orc.Params(nu=0.01))
+    div = g.k1 * r[0] + g.k2 * r[1] + g.k3 * r[2]
+    assert np.abs(div).max() < 1e-10 * np.abs(r).max()
