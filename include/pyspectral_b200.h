@@ -90,6 +90,18 @@ const char* psb_create_error(void);
 int psb_rhs(psb_ctx* ctx, int closure, const void* state, void* rhs, void* w0, void* read_out,
             const psb_params* p, double* tau_out);
 
+/* DNS right-hand side (same result as psb_rhs with PSB_DNS) that allocates no
+ * device memory.  No counterpart in the reference.  For callers that cannot
+ * call cudaMalloc when they evaluate the RHS: code inside a CUDA stream
+ * capture, hosts whose pool allocator owns the device memory, time-critical
+ * loops that cannot take cudaMalloc's implicit synchronisation.  Scratch is a
+ * fixed 8,847,360-byte __device__ array in the library (enough for a 32^3
+ * grid, FP64 or FP32); larger grids return PSB_ERR_SHAPE.  The first call on
+ * a device looks up the array's address (make it before any stream capture).
+ * All calls share the array, so calls that overlap on the GPU race; serialise
+ * them.  The context itself must already exist (psb_ctx_create allocates). */
+int psb_rhs_dns_noalloc(psb_ctx* ctx, const void* state, void* rhs, const psb_params* p);
+
 /* nsteps of advanceQ_RK4 (src/PySpec_3d.py:96-105; src_MPI/time_schemes.py:2-7):
  * Q <- Q0 + dt*c_i*RHS(Q), c = [1/4,1/3,1/2,1], in place on `state`.
  * comp     : Kahan compensation array (same shape as state) for FP32 runs, or NULL.

@@ -23,7 +23,7 @@ EXPORTS = (
     "psb_rhs", "psb_step_rk4", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
     "psb_spectrum", "psb_spectrum_nbins", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
     "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
-    "psb_timing_count", "psb_timing_get",
+    "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc",
 )
 
 
@@ -79,6 +79,7 @@ def load(path: str = LIB_PATH):
         "psb_timing_enable": ([vp, i], i),
         "psb_timing_count": ([vp, ip], i),
         "psb_timing_get": ([vp, i, ctypes.c_char_p, i, dp, dp], i),
+        "psb_rhs_dns_noalloc": ([vp, vp, vp, ctypes.POINTER(Params)], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
