@@ -149,6 +149,82 @@ def cpu_baseline(N, closure, budget_s):
             "sample": f"{n} RK4 steps of {N}^3 {closure} FP64 (NumPy oracle, scipy.fft workers={cores}) in {dt:.1f} s"}
 
 
+def cufft_baseline_ms(N, steps, closure, flush):
+    """The same RK4 step built from library calls: torch.fft (cuFFT) 3/2-padded
+    transforms and torch elementwise kernels, FP32.  A comparison arm only."""
+    import torch
+    dev = torch.device("cuda")
+    M = 3 * N // 2
+    h = N // 2
+    k1 = torch.fft.fftfreq(N, 1.0 / N, device=dev)
+    k3 = torch.arange(N // 2 + 1, device=dev, dtype=torch.float32)
+    K1, K2, K3 = torch.meshgrid(k1, k1, k3, indexing="ij")
+    ks = K1 * K1 + K2 * K2 + K3 * K3
+    ksi = torch.where(ks > 0, 1.0 / ks, torch.zeros_like(ks))
+    s = math.sqrt(1.5 ** 3 * math.sqrt(N ** 3))
+    keep = torch.ones(N, dtype=torch.bool, device=dev)
+    keep[h] = False
+    rows = torch.arange(N, device=dev)[keep]
+    prow = torch.where(rows < h, rows, rows + (M - N))
+
+    def pad(x):
+        out = torch.zeros((x.shape[0], M, M, M // 2 + 1), dtype=x.dtype, device=dev)
+        out[:, prow[:, None], prow[None, :], :h] = x[:, rows[:, None], rows[None, :], :h]
+        return out
+
+    def unpad(X):
+        out = torch.zeros((X.shape[0], N, N, N // 2 + 1), dtype=X.dtype, device=dev)
+        out[:, rows[:, None], rows[None, :], :h] = X[:, prow[:, None], prow[None, :], :h]
+        return out
+
+    def rhs(u):
+        fields = [u[0], u[1], u[2]]
+        if closure == "smag":
+            fields += [1j * K1 * u[0], 1j * K2 * u[1], 1j * K3 * u[2], 0.5j * (K2 * u[0] + K1 * u[1]),
+                       0.5j * (K3 * u[0] + K1 * u[2]), 0.5j * (K3 * u[1] + K2 * u[2])]
+        r = torch.fft.irfftn(pad(torch.stack(fields)), s=(M, M, M), dim=(1, 2, 3)) * s
+        ur, vr, wr = r[0], r[1], r[2]
+        prods = [ur * ur, vr * vr, wr * wr, ur * vr, ur * wr, vr * wr]
+        if closure == "smag":
+            S = r[3:9]
+            sm = torch.sqrt(2 * (S[0] ** 2 + S[1] ** 2 + S[2] ** 2 + 2 * S[3] ** 2 + 2 * S[4] ** 2 + 2 * S[5] ** 2))
+            nut = (0.16 * 2 * math.pi / N) ** 2 * sm
+            prods += [-2 * nut * S[m] for m in range(6)]
+        P = unpad(torch.fft.rfftn(torch.stack(prods), dim=(1, 2, 3)))
+        uu, vv, ww, uv, uw, vw = P[0:6]
+        ph = ksi * (-K1 * K1 * uu - K2 * K2 * vv - K3 * K3 * ww - 2 * K1 * K2 * uv - 2 * K1 * K3 * uw
+                    - 2 * K2 * K3 * vw)
+        R = torch.stack([-1j * (K1 * uu + K2 * uv + K3 * uw + K1 * ph), -1j * (K1 * uv + K2 * vv + K3 * vw + K2 * ph),
+                         -1j * (K1 * uw + K2 * vw + K3 * ww + K3 * ph)]) - 1e-3 * ks * u
+        if closure == "smag":
+            t11, t22, t33, t12, t13, t23 = P[6:12]
+            proj = 1j * ksi * (K1 * K1 * t11 + K2 * K2 * t22 + K3 * K3 * t33 + 2 * K1 * K2 * t12
+                               + 2 * K1 * K3 * t13 + 2 * K2 * K3 * t23)
+            R = R + torch.stack([-1j * (K1 * t11 + K2 * t12 + K3 * t13) + 1j * K1 * proj,
+                                 -1j * (K1 * t12 + K2 * t22 + K3 * t23) + 1j * K2 * proj,
+                                 -1j * (K1 * t13 + K2 * t23 + K3 * t33) + 1j * K3 * proj])
+        return R
+
+    def step(u):
+        u0 = u
+        for c in (0.25, 1 / 3, 0.5, 1.0):
+            u = u0 + (2e-3 * c) * rhs(u)
+        return u
+
+    u = make_state(N, 1).to(torch.complex64)
+    for _ in range(3):
+        u = step(u)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record()
+        u = step(u)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev) / steps
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -179,7 +255,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     from pyspectral_b200 import _capi
     from pyspectral_b200 import Classes as C
-    from pyspectral_b200.RHSfunctions import advance
+    from pyspectral_b200.RHSfunctions import StepGraph, advance
 
     N = args.N
     tm = 1 if args.closure == "smag" else 0
@@ -195,37 +271,40 @@ def run_ours(args):
         return grid, main
 
     def timed(grid, main, K, W):
+        """K steps, each one CUDA-graph replay bracketed by events; L2 flushed
+        before each (outside the events)."""
         ctx = grid.ctx(main.precision)
+        l0 = ctx.launch_count()
+        g = StepGraph(main, grid, 1)
+        per_step = (ctx.launch_count() - l0) // 2  # warm-up + capture each issue one step
         for _ in range(W):
-            advance(main, grid, 1)
+            g.replay()
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        l0 = ctx.launch_count()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
         for k in range(K):
             flush.zero_()
             ev[k][0].record()
-            advance(main, grid, 1)
+            g.replay()
             ev[k][1].record()
         torch.cuda.synchronize()
-        launches = ctx.launch_count() - l0
         ms = sum(a.elapsed_time(b) for a, b in ev)
         if dist is not None:
             t = torch.tensor([ms], device="cuda", dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        return ms, launches
+        return ms, per_step * K, g
 
     # FP32 + Kahan (headline) and the plain FP64 path of the same closure
     grid32, m32 = build(32)
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
-    ms32, launches = timed(grid32, m32, args.steps, args.warmup)
+    ms32, launches, g32 = timed(grid32, m32, args.steps, args.warmup)
     clocks = sampler.stop() if sampler else None
     grid64, m64 = build(64)
-    ms64, _ = timed(grid64, m64, max(1, args.steps // 2), args.warmup)
+    ms64, _, _ = timed(grid64, m64, max(1, args.steps // 2), args.warmup)
     ok = grid32.ctx(32).count_nonfinite(m32.Q) == 0 and grid64.ctx(64).count_nonfinite(m64.Q) == 0
     value = world * N ** 3 * args.steps / (ms32 / 1e3)
     value64 = world * N ** 3 * max(1, args.steps // 2) / (ms64 / 1e3)
@@ -246,7 +325,7 @@ def run_ours(args):
     for _ in range(Ke):
         m32.Q.copy_(host, non_blocking=True)
         m32.comp.copy_(hostc, non_blocking=True)
-        advance(m32, grid32, 1)
+        g32.replay()
         out.copy_(m32.Q, non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
@@ -291,6 +370,7 @@ def run_ours(args):
         except Exception:
             pass
 
+    cufft_ms = cufft_baseline_ms(N, max(5, args.steps // 10), args.closure, flush) if rank == 0 else None
     if rank == 0:
         cb = cpu_baseline(N, args.closure, args.cpu_seconds) if world == 1 else None
         line = {
@@ -300,10 +380,12 @@ def run_ours(args):
             "config": {"workload": f"{N}^3 decaying isotropic LES (E(k)~k^4 exp(-2k^2/k0^2), k0=4), "
                                    f"{args.closure} closure, RK4 dt=2e-3, nu=1e-3, FP32 fields + Kahan stage "
                                    f"accumulation; learned closure not built yet", "N": N,
-                       "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)",
+                       "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)", "launch": "one CUDA graph per RK4 step",
                        "parallelism": f"replicas x{world}"},
             "fp64_plain": {"value": value64, "ms_per_step": ms64 / max(1, args.steps // 2),
                            "ratio_f32_over_f64": value / value64},
+            "cufft_library_baseline": {"value": N ** 3 / (cufft_ms / 1e3), "ms_per_step": cufft_ms,
+                                       "what": "same FP32 step from torch.fft (cuFFT) + torch elementwise ops"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clocks,
             "gpu_launches": int(launches), "finite": bool(ok),
         }

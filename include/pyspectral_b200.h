@@ -35,6 +35,8 @@ extern "C" {
 #define PSB_TAU_STATIC 3  /* 'Static tau-model'  (src/RHSfunctions.py:366-497)                       */
 #define PSB_TAU_DYNAMIC 4 /* 'Dynamic tau-model' (src/RHSfunctions.py:592-878)                       */
 #define PSB_MHD 5         /* 'MHD' of the MPI solver (src_MPI/RHSfunctions.py:95-175)                */
+#define PSB_LEARNED 6     /* learned MLP subgrid stress (no reference counterpart; replaces the
+                             Smagorinsky stress of src/RHSfunctions.py:195-212)                    */
 
 /* ---- diagnostic flags --------------------------------------------------- */
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
@@ -65,6 +67,9 @@ typedef struct {
   int rotate;          /* Coriolis on/off (src/RHSfunctions.py:33-36,47-50) */
   double Om1, Om2, Om3;
   const void* force;   /* MHD: constant forcing spectra, 3 fields, or NULL (src_MPI/Classes.py:91-94) */
+  const void* mlp_params; /* PSB_LEARNED: FP32 parameter block (psb_mlp_sizes) on the device */
+  const void* mlp_norm;   /* PSB_LEARNED: FP32 normalisation block on the device */
+  double les_delta;       /* PSB_LEARNED: filter width fed to the MLP; <=0 -> (dx dy dz)^(1/3) */
 } psb_params;
 
 /* FFTclass + gridclass construction (src/Classes.py:548-625; src/PySpec_3d.py:79-80).
@@ -145,6 +150,35 @@ int psb_fft_r2c(psb_ctx* ctx, const void* phys, void* spec, int nfields);
 int psb_fft_c2r(psb_ctx* ctx, const void* spec, void* phys, int nfields);
 /* Count of non-finite values in n complex entries -> *count (0 = all finite). */
 int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* count);
+
+/* ---- learned subgrid closure (no counterpart in the reference) ----------
+ * MLP 10 -> 64 -> 64 -> 6 (GELU), BF16 tensor-core math with FP32
+ * accumulation.  Features: the 9 velocity gradients du_i/dx_j (order 3i+j)
+ * and the filter width; targets: tau_11,22,33,12,13,23.  Parameters are an
+ * FP32 master block of *nparams floats, normalisation a block of *nnorm
+ * floats (xmean[10] xistd[10] ymean[6] ystd[6]); all device pointers. */
+int psb_mlp_sizes(int* nparams, int* nnorm);
+/* Y[B][6] = tau(X[B][10]) (raw units in and out). */
+int psb_mlp_forward(psb_ctx* ctx, const float* params, const float* norm, const float* X, int B, float* Y);
+/* grad += d(MSE of normalised outputs)/d(params) over the B points X[idx[b]],
+ * T[idx[b]]; *loss (device double) += the MSE. */
+int psb_mlp_grad(psb_ctx* ctx, const float* params, const float* norm, const float* X, const float* T, const int* idx,
+                 int B, float* grad, double* loss);
+/* One Adam(W) update of params from grad (step >= 1); clears grad. */
+int psb_mlp_adam(psb_ctx* ctx, float* params, float* m, float* v, float* grad, int step, float lr, float beta1,
+                 float beta2, float eps, float weight_decay);
+/* Physical fields on the N grid (irfftn(uhat)*sqrt(N1N2N3)): what=0 -> u,v,w
+ * (3 fields); what=1 -> u,v,w and the 9 gradients du_i/dx_j (12 fields). */
+int psb_physical_fields(psb_ctx* ctx, const void* fields3, int what, void* out);
+/* The six 3/2-dealiased product spectra u_i u_j (11,22,33,12,13,23) in the
+ * state normalisation: uuhat... of src/RHSfunctions.py:18-23. */
+int psb_products(psb_ctx* ctx, const void* fields3, void* out6);
+/* Copy the modes |k_i| < kc (per axis, index units) of nfields spectra from a
+ * (N1,N2,N3) grid to a (n1,n2,n3) grid times `scale`, all other modes zero
+ * (sharp spectral cutoff and change of resolution).  precision 32 or 64;
+ * stream is a cudaStream_t or NULL. */
+int psb_spectral_resample(const void* src, int N1, int N2, int N3, void* dst, int n1, int n2, int n3, int nfields,
+                          int kc, double scale, int precision, void* stream);
 
 /* ---- launch accounting and per-kernel timing (no reference counterpart;
  *      the reference only prints wall time, src/PySpec_3d.py:107,136,144) --- */

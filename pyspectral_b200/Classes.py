@@ -133,7 +133,7 @@ class variables:
 
     def __init__(self, weave, turb_model, rotate, Om1, Om2, Om3, grid, uhat, vhat, what, t, dt, nu, Ct=-10,
                  dt0=-10, dt0_subintegrations=-10, dt1=-10, dt1_subintegrations=-10, cfl=None, dim=3,
-                 precision=64, kahan=None):
+                 precision=64, kahan=None, model=None, les_delta=None):
         from . import RHSfunctions as R
         self.turb_model = turb_model
         self.rotate = int(rotate)
@@ -159,11 +159,18 @@ class variables:
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
-                 "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel}
+                 "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
+                 "learned": R.computeRHS_learned}
         if turb_model not in table:
             raise ValueError(f"turb_model {turb_model!r} is not on this path")
         self.computeRHS = table[turb_model]
-        if turb_model != 0:
+        # learned closure (no reference counterpart): an MLPModel from pyspectral_b200.learned
+        self.model = model
+        self.les_delta = float(les_delta) if les_delta else 2.0 * np.pi / grid.N1
+        if turb_model == "learned" and model is None:
+            from .learned import MLPModel
+            self.model = MLPModel.load(device=grid.device)
+        if turb_model not in (0, "learned"):
             self.W0 = torch.zeros_like(self.Q)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
@@ -202,13 +209,17 @@ class variables:
         self.U.copy_(self.Q)
 
     def params(self):
+        m = self.model
         return _capi.make_params(nu=self.nu, t=self.t, dt=self.dt, Ct=self.Ct, tau_a=self.tau_a,
                                  tau_b=self.tau_b, kf=self.kf or 0, rotate=self.rotate,
-                                 Om=(self.Om1, self.Om2, self.Om3))
+                                 Om=(self.Om1, self.Om2, self.Om3),
+                                 mlp_params=m.params.data_ptr() if m is not None else None,
+                                 mlp_norm=m.norm.data_ptr() if m is not None else None,
+                                 les_delta=self.les_delta)
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC}[self.turb_model]
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, "learned": _capi.LEARNED}[self.turb_model]
 
 
 class utilitiesClass:

@@ -47,6 +47,14 @@ def computeRHS_Dtaumodel(main, grid, myFFT=None, utilities=None):
     main.tau = _rhs(main, grid, _capi.TAU_DYNAMIC)
 
 
+def computeRHS_learned(main, grid, myFFT=None, utilities=None):
+    """LES with the learned MLP subgrid stress (no reference counterpart;
+    takes the place of the Smagorinsky stress of src/RHSfunctions.py:195-212).
+    The stress enters with the solenoidal projection -i k_j (u_i u_j + tau_ij)
+    projected, like the advection term."""
+    _rhs(main, grid, _capi.LEARNED)
+
+
 def advanceQ_RK4(main, grid, myFFT=None, utilities=None):
     """``advanceQ_RK4`` (src/PySpec_3d.py:96-105): four low-storage stages
     ``Q = Q0 + dt c_i RHS(Q)``, c = [1/4, 1/3, 1/2, 1], fused into the RHS
@@ -65,3 +73,40 @@ def advance(main, grid, nsteps):
     """``nsteps`` fixed-dt RK4 steps in one call (no per-step host work)."""
     ctx = grid.ctx(main.precision)
     ctx.step(main.closure_code(), main.Q, main.params(), int(nsteps), comp=main.comp, read_out=main.U)
+
+
+class StepGraph:
+    """``nsteps`` fixed-dt RK4 steps captured once into a CUDA graph.
+
+    ``replay()`` advances ``main`` in place exactly like ``advance(main, grid,
+    nsteps)`` but with one graph launch.  Kernel arguments (dt, nu, t, closure
+    coefficients) are frozen at capture, so this suits closures without an
+    explicit time dependence (DNS, Smagorinsky, MHD) or a fixed t; re-capture
+    after changing them."""
+
+    def __init__(self, main, grid, nsteps=1):
+        import torch
+        self.main, self.grid, self.nsteps = main, grid, int(nsteps)
+        ctx = grid.ctx(main.precision)
+        ctx.prepare(main.closure_code())
+        saved = [t.clone() for t in self._state()]
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # warm-up outside the capture (sets kernel attributes)
+            advance(main, grid, self.nsteps)
+        torch.cuda.current_stream().wait_stream(side)
+        for t, s in zip(self._state(), saved):
+            t.copy_(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            advance(main, grid, self.nsteps)
+        torch.cuda.synchronize()
+
+    def _state(self):
+        out = [self.main.Q, self.main.U]
+        if self.main.comp is not None:
+            out.append(self.main.comp)
+        return out
+
+    def replay(self):
+        self.graph.replay()

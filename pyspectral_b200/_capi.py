@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
 
 PSB_OK = 0
 PSB_ERR_NONFINITE = 6
-DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD = 0, 1, 2, 3, 4, 5
+DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED = 0, 1, 2, 3, 4, 5, 6
 NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
 
 EXPORTS = (
@@ -23,7 +23,8 @@ EXPORTS = (
     "psb_rhs", "psb_step_rk4", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
     "psb_spectrum", "psb_spectrum_nbins", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
     "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
-    "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc",
+    "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
+    "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
 )
 
 
@@ -39,7 +40,8 @@ class Params(ctypes.Structure):
                 ("dt", ctypes.c_double), ("Ct", ctypes.c_double), ("tau_a", ctypes.c_double),
                 ("tau_b", ctypes.c_double), ("kf", ctypes.c_int), ("rotate", ctypes.c_int),
                 ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
-                ("force", ctypes.c_void_p)]
+                ("force", ctypes.c_void_p), ("mlp_params", ctypes.c_void_p), ("mlp_norm", ctypes.c_void_p),
+                ("les_delta", ctypes.c_double)]
 
 
 _lib = None
@@ -90,9 +92,10 @@ def load(path: str = LIB_PATH):
 
 
 def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
-                Om=(0.0, 0.0, 0.0), force=None) -> Params:
+                Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0) -> Params:
     return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
-                  int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force)
+                  int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force, mlp_params, mlp_norm,
+                  float(les_delta))
 
 
 class Context:

@@ -16,6 +16,8 @@ StepIO<T> make_io(psb_ctx* c, void* Q, void* Q0, void* comp, void* rhs, void* re
                   double dtc);
 template <typename T>
 int sgs_dns_run(psb_ctx* c, const void* fields, void* w0, void* tau6);
+template <typename T>
+int products_run(psb_ctx* c, const void* fields, void* out6);
 }  // namespace psbh
 
 namespace {
@@ -33,22 +35,34 @@ bool smooth23(int L) {
 FFTPlan make_plan(int L) {
   FFTPlan p{};
   p.L = L;
+  int radix[kMaxPasses], np = 0;
   int n = L;
   while (n % 8 == 0) {
-    p.radix[p.npass++] = 8;
+    radix[np++] = 8;
     n /= 8;
   }
   while (n % 4 == 0) {
-    p.radix[p.npass++] = 4;
+    radix[np++] = 4;
     n /= 4;
   }
   while (n % 2 == 0) {
-    p.radix[p.npass++] = 2;
+    radix[np++] = 2;
     n /= 2;
   }
   while (n % 3 == 0) {
-    p.radix[p.npass++] = 3;
+    radix[np++] = 3;
     n /= 3;
+  }
+  p.npass = np;
+  int Ns = 1;
+  for (int s = 0; s < np; ++s) {
+    FFTPass& q = p.pass[s];
+    q.R = radix[s];
+    q.nb = L / q.R;
+    q.Ns = Ns;
+    q.tstride = L / (Ns * q.R);
+    q.mag_ns = fdiv_magic((unsigned)Ns);
+    Ns *= q.R;
   }
   return p;
 }
@@ -348,6 +362,105 @@ int r2c_impl(psb_ctx* c, const void* phys, void* spec, int nfields) {
     PSB_TRY((launch_axis<T, false>(c, a, PreCopy<T>{}, "r2c x")));
   }
   return PSB_OK;
+}
+
+template <typename T, int F>
+struct PhysStoreN {
+  static constexpr int F_IN = F, F_OUT = 0;
+  T* phys;
+  long long fs;
+  int n3;
+  __device__ __forceinline__ void operator()(long long pen, int z, const T* in, T*) const {
+#pragma unroll
+    for (int f = 0; f < F; ++f) phys[f * fs + pen * n3 + z] = in[f];
+  }
+};
+
+// physical u (and its gradients) on the N grid, irfftn(uhat)*sqrt(N1 N2 N3)
+template <typename T, class Pre>
+int physical_impl(psb_ctx* c, const void* fields, void* out, Pre pre) {
+  constexpr int F = Pre::F_DST;
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "phys.A", (size_t)F * N1 * N2 * N3h, &st);
+  Cx<T>* B = scratch<T>(c, "phys.B", (size_t)F * N1 * N2 * N3h, &st);
+  if (st != PSB_OK) return st;
+  AxisArgs<T> a{};
+  a.plan = *plan_for(c, N1);
+  a.tw = twiddles<T>(c);
+  a.scale = (T)1;
+  a.in = reinterpret_cast<const Cx<T>*>(fields);
+  a.out = A;
+  a.in_fstride = (long long)N1 * N2 * N3h;
+  a.in_ostride = N3h;
+  a.in_rstride = (long long)N2 * N3h;
+  a.out_fstride = (long long)N1 * N2 * N3h;
+  a.out_ostride = N3h;
+  a.out_rstride = (long long)N2 * N3h;
+  a.nouter = N2;
+  a.ncols = N3h;
+  a.in_rows = N1;
+  a.out_rows = N1;
+  a.in_map = map_id(N1);
+  a.out_map = map_id(N1);
+  a.k_row = c->kx;
+  a.k_outer = c->ky;
+  a.k_col = c->kz;
+  PSB_TRY((launch_axis<T, true>(c, a, pre, "physical x")));
+  AxisArgs<T> b{};
+  b.plan = *plan_for(c, N2);
+  b.tw = twiddles<T>(c);
+  b.scale = (T)1;
+  b.in = A;
+  b.out = B;
+  b.in_ostride = (long long)N2 * N3h;
+  b.in_rstride = N3h;
+  b.out_ostride = (long long)N2 * N3h;
+  b.out_rstride = N3h;
+  b.nouter = F * N1;
+  b.ncols = N3h;
+  b.in_rows = N2;
+  b.out_rows = N2;
+  b.in_map = map_id(N2);
+  b.out_map = map_id(N2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "physical y")));
+  ZArgs<T> z{};
+  const long long fs = (long long)N1 * N2 * N3h;
+  for (int f = 0; f < F; ++f) {
+    z.in[f] = B + f * fs;
+    z.in_pstride[f] = N3h;
+    z.in_kz[f] = N3h;
+  }
+  z.npencils = (long long)N1 * N2;
+  z.fac = (T)(std::sqrt((double)N1 * N2 * N3) / ((double)N1 * N2 * N3));
+  z.plan = *plan_for(c, N3);
+  z.tw = twiddles<T>(c);
+  PhysStoreN<T, F> ph{reinterpret_cast<T*>(out), (long long)N1 * N2 * N3, N3};
+  return launch_z<T>(c, z, ph, "physical z", (double)sizeof(T) * F * N1 * N2 * N3);
+}
+
+template <typename T>
+__global__ void resample_kernel(const Cx<T>* __restrict__ src, int N1, int N2, int N3, Cx<T>* __restrict__ dst,
+                                int n1, int n2, int n3, int nf, int kc, T scale) {
+  const int h3 = n3 / 2 + 1, H3 = N3 / 2 + 1;
+  const long long npts = (long long)n1 * n2 * h3;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts * nf;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(s / npts);
+    const long long q = s - f * npts;
+    const int i3 = (int)(q % h3);
+    const long long t = q / h3;
+    const int i2 = (int)(t % n2), i1 = (int)(t / n2);
+    const int k1 = i1 < n1 / 2 ? i1 : i1 - n1, k2 = i2 < n2 / 2 ? i2 : i2 - n2, k3 = i3;
+    Cx<T> v = mk<T>(0, 0);
+    const bool keep = abs(k1) < kc && abs(k2) < kc && k3 < kc && abs(k1) < N1 / 2 && abs(k2) < N2 / 2 &&
+                      k3 < N3 / 2 && !(i1 == n1 / 2) && !(i2 == n2 / 2);
+    if (keep) {
+      const int j1 = k1 >= 0 ? k1 : k1 + N1, j2 = k2 >= 0 ? k2 : k2 + N2;
+      v = scale * src[(long long)f * N1 * N2 * H3 + ((long long)j1 * N2 + j2) * H3 + k3];
+    }
+    dst[s] = v;
+  }
 }
 
 template <typename T>
@@ -776,6 +889,41 @@ int psb_check_finite(psb_ctx* c, const void* data, long long n, long long* count
   PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "finite sync"));
   *count = (long long)h;
   return h ? fail(c, PSB_ERR_NONFINITE, "non-finite values found") : PSB_OK;
+}
+
+int psb_physical_fields(psb_ctx* c, const void* f, int what, void* out) {
+  PSB_TRY(check_ctx(c));
+  if (!f || !out || (what != 0 && what != 1)) return fail(c, PSB_ERR_ARG, "psb_physical_fields: bad argument");
+  PSB_TRY(set_device(c));
+  if (c->prec == 64)
+    return what ? physical_impl<double>(c, f, out, PreGrad<double>{})
+                : physical_impl<double>(c, f, out, PreCopyN<double, 3>{});
+  return what ? physical_impl<float>(c, f, out, PreGrad<float>{}) : physical_impl<float>(c, f, out, PreCopyN<float, 3>{});
+}
+
+int psb_products(psb_ctx* c, const void* f, void* out6) {
+  PSB_TRY(check_ctx(c));
+  if (!f || !out6) return fail(c, PSB_ERR_ARG, "psb_products: null argument");
+  PSB_TRY(set_device(c));
+  return c->prec == 64 ? products_run<double>(c, f, out6) : products_run<float>(c, f, out6);
+}
+
+int psb_spectral_resample(const void* src, int N1, int N2, int N3, void* dst, int n1, int n2, int n3, int nfields,
+                          int kc, double scale, int precision, void* stream) {
+  if (!src || !dst || nfields <= 0 || N1 < 2 || N2 < 2 || N3 < 2 || n1 < 2 || n2 < 2 || n3 < 2 || kc < 1)
+    return PSB_ERR_ARG;
+  if (precision != 32 && precision != 64) return PSB_ERR_ARG;
+  const long long n = (long long)n1 * n2 * (n3 / 2 + 1) * nfields;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (precision == 64)
+    resample_kernel<double><<<blocks, 256, 0, s>>>(reinterpret_cast<const Cx<double>*>(src), N1, N2, N3,
+                                                   reinterpret_cast<Cx<double>*>(dst), n1, n2, n3, nfields, kc, scale);
+  else
+    resample_kernel<float><<<blocks, 256, 0, s>>>(reinterpret_cast<const Cx<float>*>(src), N1, N2, N3,
+                                                  reinterpret_cast<Cx<float>*>(dst), n1, n2, n3, nfields, kc,
+                                                  (float)scale);
+  return cudaGetLastError() == cudaSuccess ? PSB_OK : PSB_ERR_CUDA;
 }
 
 int psb_launch_count(const psb_ctx* c, unsigned long long* n) {

@@ -148,9 +148,39 @@ inline int count_mapped(const psb::RowMap& m, int rows) {
 
 constexpr size_t kSmemBudget = 100 * 1024;
 
+// Raise a kernel's dynamic shared-memory limit once per (kernel, device); a
+// fixed table, so that launching never allocates host memory either.
+struct SmemCache {
+  const void* fn[512];
+  int dev[512];
+  size_t bytes[512];
+  int n = 0;
+};
+inline SmemCache& smem_cache() {
+  static SmemCache c;
+  return c;
+}
 template <typename K>
 inline void set_smem(K kernel, size_t smem) {
-  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem <= 48 * 1024) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  SmemCache& c = smem_cache();
+  const void* f = reinterpret_cast<const void*>(kernel);
+  for (int i = 0; i < c.n; ++i)
+    if (c.fn[i] == f && c.dev[i] == dev) {
+      if (c.bytes[i] >= smem) return;
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      c.bytes[i] = smem;
+      return;
+    }
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (c.n < 512) {
+    c.fn[c.n] = f;
+    c.dev[c.n] = dev;
+    c.bytes[c.n] = smem;
+    ++c.n;
+  }
 }
 
 inline int pow2_floor(int x) {
@@ -160,12 +190,15 @@ inline int pow2_floor(int x) {
 }
 
 // columns per CTA for strided passes
-inline int pick_ct(int ncols, int F, int L, size_t esz) {
+// nouter > 0: also shrink the tile until the grid has ~2 CTAs per SM (148 SMs)
+inline int pick_ct(int ncols, int F, int L, size_t esz, int nouter = 0) {
   int ct = 32;
   int cap = pow2_floor(ncols < 1 ? 1 : ncols);
   if (ncols > cap) cap *= 2;
   if (ct > cap) ct = cap;
   while (ct > 1 && (size_t)(L + 2 * L * F * ct) * esz > kSmemBudget) ct /= 2;
+  if (nouter > 0)
+    while (ct > 4 && (long long)((ncols + ct - 1) / ct) * nouter < 2 * 148) ct /= 2;
   return ct;
 }
 
@@ -173,7 +206,7 @@ template <typename T, bool INV, class Pre>
 int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what) {
   const size_t esz = sizeof(Cx<T>);
   const int L = a.plan.L;
-  a.col_tile = pick_ct(a.ncols, Pre::F_DST, L, esz);
+  a.col_tile = pick_ct(a.ncols, Pre::F_DST, L, esz, a.nouter);
   const size_t smem = (size_t)(L + 2 * L * Pre::F_DST * a.col_tile) * esz;
   dim3 grid((a.ncols + a.col_tile - 1) / a.col_tile, a.nouter);
   auto k = psb::axis_pass_kernel<T, INV, Pre>;
@@ -190,7 +223,9 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   const size_t esz = sizeof(Cx<T>);
   const int M = z.plan.L;
   constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
-  auto smem_for = [&](int P) { return (size_t)(M + 2 * ((FMAX * P + 1) / 2) * M) * esz; };
+  constexpr size_t extra = (size_t)psb::phys_is_block<Phys>::extra;
+  (void)esz;
+  auto smem_for = [&](int P) { return psb::zpass_smem_bytes<T>(FMAX, P, M, extra); };
   int P = 8;
   while (P > 1 && smem_for(P) > kSmemBudget) P /= 2;
   while (P > 1 && (z.npencils + P - 1) / P < 2 * 148) P /= 2;
@@ -211,7 +246,7 @@ template <typename T, class Epi>
 int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what) {
   const size_t esz = sizeof(Cx<T>);
   const int L = e.plan.L;
-  e.col_tile = pick_ct(e.kz, Epi::F_IN, L, esz);
+  e.col_tile = pick_ct(e.kz, Epi::F_IN, L, esz, e.n2);
   const int ntile = (e.kz + e.col_tile - 1) / e.col_tile;
   e.main_blocks = ntile * e.n2;
   int extra = 0;

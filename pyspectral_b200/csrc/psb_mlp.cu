@@ -1,0 +1,330 @@
+// Training and stand-alone inference of the subgrid-stress MLP on BF16 tensor
+// cores (mma.sync m16n8k16, FP32 accumulation).  See psb_mlp.cuh for the
+// parameter layout.  One training step = psb_mlp_train_step: a fused forward /
+// loss / backward kernel over the minibatch (each CTA: 128 points, weight
+// gradients of its points reduced with tensor-core GEMMs over the point axis,
+// then added to the global FP32 gradient), followed by an Adam update that also
+// clears the gradient.
+#include <cuda_bf16.h>
+
+#include "psb_ctx.cuh"
+#include "psb_mlp.cuh"
+
+using namespace psb;
+using namespace psbh;
+
+namespace {
+
+constexpr int kRows = 128;  // points per CTA (8 warps x 16)
+
+struct TrainSmem {
+  MlpSmem m;
+  __nv_bfloat16 X[kRows * 16];
+  __nv_bfloat16 H1[kRows * kMlpH];
+  __nv_bfloat16 H2[kRows * kMlpH];
+  __nv_bfloat16 dY[kRows * 16];
+  __nv_bfloat16 dZ2[kRows * kMlpH];
+  __nv_bfloat16 dZ1[kRows * kMlpH];
+  float db1[kMlpH], db2[kMlpH], db3[8];
+  float loss;
+};
+
+// A fragment of M = S^T where S is stored [k][m] row-major (ld = m stride).
+__device__ __forceinline__ void afrag_km(uint32_t* a, const __nv_bfloat16* S, int ld, int m0, int k0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int k = k0 + 2 * t;
+  a[0] = pack_raw(S[k * ld + m0 + g], S[(k + 1) * ld + m0 + g]);
+  a[1] = pack_raw(S[k * ld + m0 + g + 8], S[(k + 1) * ld + m0 + g + 8]);
+  a[2] = pack_raw(S[(k + 8) * ld + m0 + g], S[(k + 9) * ld + m0 + g]);
+  a[3] = pack_raw(S[(k + 8) * ld + m0 + g + 8], S[(k + 9) * ld + m0 + g + 8]);
+}
+// B fragment of a matrix stored [k][n] row-major.
+__device__ __forceinline__ void bfrag_kn(uint32_t* b, const __nv_bfloat16* W, int ld, int k0, int n0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int k = k0 + 2 * t;
+  b[0] = pack_raw(W[k * ld + n0 + g], W[(k + 1) * ld + n0 + g]);
+  b[1] = pack_raw(W[(k + 8) * ld + n0 + g], W[(k + 9) * ld + n0 + g]);
+}
+
+// grad[kMlpParams] += dL/dparams over B points; loss_acc += sum of squared errors / (6B)
+__global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
+                                                        const float* __restrict__ X, const float* __restrict__ T,
+                                                        const int* __restrict__ idx, int B, float* __restrict__ grad,
+                                                        double* __restrict__ loss_acc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw);
+  mlp_stage(s.m, P, nrm);
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    s.db1[i] = 0.f;
+    s.db2[i] = 0.f;
+  }
+  if (threadIdx.x < 8) s.db3[threadIdx.x] = 0.f;
+  if (threadIdx.x == 0) s.loss = 0.f;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int r0 = blockIdx.x * kRows + warp * 16;  // first batch row of this warp
+  auto rowid = [&](int r) -> int { return r0 + r < B ? idx[r0 + r] : -1; };
+  const int id_lo = rowid(g), id_hi = rowid(g + 8);
+  uint32_t xa[4];
+  mlp_xfrag(s.m, xa, [&](int r, int f) {
+    const int id = r == g ? id_lo : id_hi;
+    return id >= 0 ? X[(long long)id * kMlpIn + f] : s.m.xmean[f];
+  });
+  float z1[8][4], z2[8][4], y[4];
+  mlp_forward_warp(s.m, xa, y, z1, z2);
+  // dY = 2 (y - t) / (6B), rows without a point contribute nothing
+  const float sc = 2.f / (6.f * (float)B);
+  float dy[4];
+  float lsum = 0.f;
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int c = 2 * t + (e & 1);
+    const int id = e < 2 ? id_lo : id_hi;
+    float d = 0.f;
+    if (c < kMlpOut && id >= 0) {
+      const float tn = (T[(long long)id * kMlpOut + c] - s.m.ymean[c]) / s.m.ystd[c];
+      d = y[e] - tn;
+      lsum += d * d;
+    }
+    dy[e] = sc * d;
+  }
+  atomicAdd(&s.loss, lsum);
+  // stage X, H1, H2 (bf16) and dY for the weight-gradient GEMMs
+  {
+    const int ra = warp * 16 + g, rb = ra + 8;
+    // X: features in the same positions as xa
+    const __nv_bfloat162* xv = reinterpret_cast<const __nv_bfloat162*>(xa);
+    *reinterpret_cast<__nv_bfloat162*>(&s.X[ra * 16 + 2 * t]) = xv[0];
+    *reinterpret_cast<__nv_bfloat162*>(&s.X[rb * 16 + 2 * t]) = xv[1];
+    *reinterpret_cast<__nv_bfloat162*>(&s.X[ra * 16 + 2 * t + 8]) = xv[2];
+    *reinterpret_cast<__nv_bfloat162*>(&s.X[rb * 16 + 2 * t + 8]) = xv[3];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int col = 8 * j + 2 * t;
+      *reinterpret_cast<__nv_bfloat162*>(&s.H1[ra * kMlpH + col]) =
+          __floats2bfloat162_rn(gelu_f(z1[j][0]), gelu_f(z1[j][1]));
+      *reinterpret_cast<__nv_bfloat162*>(&s.H1[rb * kMlpH + col]) =
+          __floats2bfloat162_rn(gelu_f(z1[j][2]), gelu_f(z1[j][3]));
+      *reinterpret_cast<__nv_bfloat162*>(&s.H2[ra * kMlpH + col]) =
+          __floats2bfloat162_rn(gelu_f(z2[j][0]), gelu_f(z2[j][1]));
+      *reinterpret_cast<__nv_bfloat162*>(&s.H2[rb * kMlpH + col]) =
+          __floats2bfloat162_rn(gelu_f(z2[j][2]), gelu_f(z2[j][3]));
+    }
+    *reinterpret_cast<__nv_bfloat162*>(&s.dY[ra * 16 + 2 * t]) = __floats2bfloat162_rn(dy[0], dy[1]);
+    *reinterpret_cast<__nv_bfloat162*>(&s.dY[rb * 16 + 2 * t]) = __floats2bfloat162_rn(dy[2], dy[3]);
+    *reinterpret_cast<__nv_bfloat162*>(&s.dY[ra * 16 + 2 * t + 8]) = __floats2bfloat162_rn(0.f, 0.f);
+    *reinterpret_cast<__nv_bfloat162*>(&s.dY[rb * 16 + 2 * t + 8]) = __floats2bfloat162_rn(0.f, 0.f);
+    if (t < 3) {
+      atomicAdd(&s.db3[2 * t], dy[0] + dy[2]);
+      atomicAdd(&s.db3[2 * t + 1], dy[1] + dy[3]);
+    }
+  }
+  // dH2 = dY W3 (k = 8 outputs, padded to 16), dZ2 = dH2 * gelu'(z2)
+  uint32_t da[4];
+  da[0] = pack_bf16(dy[0], dy[1]);
+  da[1] = pack_bf16(dy[2], dy[3]);
+  da[2] = 0u;
+  da[3] = 0u;
+  float dz2[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    dz2[j][0] = dz2[j][1] = dz2[j][2] = dz2[j][3] = 0.f;
+    uint32_t b[2];
+    b[0] = pack_raw(s.m.w3[(2 * t) * kMlpH + 8 * j + g], s.m.w3[(2 * t + 1) * kMlpH + 8 * j + g]);
+    b[1] = 0u;
+    mma16816(dz2[j], da, b);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dz2[j][e] *= gelu_d(z2[j][e]);
+  }
+  uint32_t a2[4][4];
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a2[kk][0] = pack_bf16(dz2[2 * kk][0], dz2[2 * kk][1]);
+    a2[kk][1] = pack_bf16(dz2[2 * kk][2], dz2[2 * kk][3]);
+    a2[kk][2] = pack_bf16(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
+    a2[kk][3] = pack_bf16(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
+  }
+  // dH1 = dZ2 W2 (W2 stored [out=k][in=n]), dZ1 = dH1 * gelu'(z1)
+  float dz1[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    dz1[j][0] = dz1[j][1] = dz1[j][2] = dz1[j][3] = 0.f;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      uint32_t b[2];
+      bfrag_kn(b, s.m.w2, kMlpH, 16 * kk, 8 * j, lane);
+      mma16816(dz1[j], a2[kk], b);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) dz1[j][e] *= gelu_d(z1[j][e]);
+  }
+  {
+    const int ra = warp * 16 + g, rb = ra + 8;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int col = 8 * j + 2 * t;
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[ra * kMlpH + col]) = __floats2bfloat162_rn(dz2[j][0], dz2[j][1]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[rb * kMlpH + col]) = __floats2bfloat162_rn(dz2[j][2], dz2[j][3]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[ra * kMlpH + col]) = __floats2bfloat162_rn(dz1[j][0], dz1[j][1]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[rb * kMlpH + col]) = __floats2bfloat162_rn(dz1[j][2], dz1[j][3]);
+      atomicAdd(&s.db2[col], dz2[j][0] + dz2[j][2]);
+      atomicAdd(&s.db2[col + 1], dz2[j][1] + dz2[j][3]);
+      atomicAdd(&s.db1[col], dz1[j][0] + dz1[j][2]);
+      atomicAdd(&s.db1[col + 1], dz1[j][1] + dz1[j][3]);
+    }
+  }
+  __syncthreads();
+  // weight gradients, contracting over the 128 points of the CTA
+  // dW2[o][i] = sum_r dZ2[r][o] H1[r][i]: 4 x 8 tiles, 4 per warp
+#pragma unroll 1
+  for (int tile = warp; tile < 32; tile += 8) {
+    const int m0 = (tile / 8) * 16, n0 = (tile % 8) * 8;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k0 = 0; k0 < kRows; k0 += 16) {
+      uint32_t a[4], b[2];
+      afrag_km(a, s.dZ2, kMlpH, m0, k0, lane);
+      bfrag_kn(b, s.H1, kMlpH, k0, n0, lane);
+      mma16816(c, a, b);
+    }
+    float* G = grad + kOffW2;
+    atomicAdd(&G[(m0 + g) * kMlpH + n0 + 2 * t], c[0]);
+    atomicAdd(&G[(m0 + g) * kMlpH + n0 + 2 * t + 1], c[1]);
+    atomicAdd(&G[(m0 + g + 8) * kMlpH + n0 + 2 * t], c[2]);
+    atomicAdd(&G[(m0 + g + 8) * kMlpH + n0 + 2 * t + 1], c[3]);
+  }
+  // dW1[o][f] = sum_r dZ1[r][o] X[r][f]: 4 x 2 tiles, 1 per warp
+  {
+    const int m0 = (warp / 2) * 16, n0 = (warp % 2) * 8;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k0 = 0; k0 < kRows; k0 += 16) {
+      uint32_t a[4], b[2];
+      afrag_km(a, s.dZ1, kMlpH, m0, k0, lane);
+      bfrag_kn(b, s.X, 16, k0, n0, lane);
+      mma16816(c, a, b);
+    }
+    float* G = grad + kOffW1;
+    const int f0 = n0 + 2 * t;
+    if (f0 < kMlpIn) {
+      atomicAdd(&G[(m0 + g) * kMlpIn + f0], c[0]);
+      atomicAdd(&G[(m0 + g + 8) * kMlpIn + f0], c[2]);
+    }
+    if (f0 + 1 < kMlpIn) {
+      atomicAdd(&G[(m0 + g) * kMlpIn + f0 + 1], c[1]);
+      atomicAdd(&G[(m0 + g + 8) * kMlpIn + f0 + 1], c[3]);
+    }
+  }
+  // dW3[c][i] = sum_r dY[r][c] H2[r][i]: m = 16 (6 used) x 8 n-tiles, 1 per warp
+  {
+    const int n0 = warp * 8;
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int k0 = 0; k0 < kRows; k0 += 16) {
+      uint32_t a[4], b[2];
+      afrag_km(a, s.dY, 16, 0, k0, lane);
+      bfrag_kn(b, s.H2, kMlpH, k0, n0, lane);
+      mma16816(c, a, b);
+    }
+    float* G = grad + kOffW3;
+    if (g < kMlpOut) {
+      atomicAdd(&G[g * kMlpH + n0 + 2 * t], c[0]);
+      atomicAdd(&G[g * kMlpH + n0 + 2 * t + 1], c[1]);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    atomicAdd(&grad[kOffB1 + i], s.db1[i]);
+    atomicAdd(&grad[kOffB2 + i], s.db2[i]);
+  }
+  if (threadIdx.x < kMlpOut) atomicAdd(&grad[kOffB3 + threadIdx.x], s.db3[threadIdx.x]);
+  if (threadIdx.x == 0) atomicAdd(loss_acc, (double)s.loss / (6.0 * (double)B));
+}
+
+__global__ void adam_kernel(float* __restrict__ P, float* __restrict__ m, float* __restrict__ v,
+                            float* __restrict__ grad, int n, float lr, float b1, float b2, float eps, float c1,
+                            float c2, float wd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gr = grad[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gr;
+  const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+  m[i] = mi;
+  v[i] = vi;
+  P[i] -= lr * ((mi / c1) / (sqrtf(vi / c2) + eps) + wd * P[i]);
+  grad[i] = 0.f;
+}
+
+__global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
+                                                          const float* __restrict__ X, int B,
+                                                          float* __restrict__ Y) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
+  mlp_stage(s, P, nrm);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  const int nw = blockDim.x >> 5;
+  for (int r0 = (blockIdx.x * nw + warp) * 16; r0 < B; r0 += gridDim.x * nw * 16) {
+    uint32_t xa[4];
+    mlp_xfrag(s, xa, [&](int r, int f) {
+      return r0 + r < B ? X[(long long)(r0 + r) * kMlpIn + f] : s.xmean[f];
+    });
+    float y[4];
+    mlp_forward_warp(s, xa, y, nullptr, nullptr);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int c = 2 * t + (e & 1), r = r0 + g + (e < 2 ? 0 : 8);
+      if (c < kMlpOut && r < B) Y[(long long)r * kMlpOut + c] = y[e] * s.ystd[c] + s.ymean[c];
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_mlp_sizes(int* nparams, int* nnorm) {
+  if (!nparams || !nnorm) return PSB_ERR_ARG;
+  *nparams = kMlpParams;
+  *nnorm = kMlpNorm;
+  return PSB_OK;
+}
+
+int psb_mlp_forward(psb_ctx* c, const float* params, const float* norm, const float* X, int B, float* Y) {
+  if (!c) return PSB_ERR_ARG;
+  if (!params || !norm || !X || !Y || B < 0) return fail(c, PSB_ERR_ARG, "psb_mlp_forward: bad argument");
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  if (B == 0) return PSB_OK;
+  const size_t smem = sizeof(MlpSmem);
+  const int blocks = (int)std::min<long long>(((long long)B + 127) / 128, 148 * 8);
+  ++c->launches;
+  mlp_forward_kernel<<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
+  return launch_ok(c, "mlp forward");
+}
+
+int psb_mlp_grad(psb_ctx* c, const float* params, const float* norm, const float* X, const float* T, const int* idx,
+                 int B, float* grad, double* loss) {
+  if (!c) return PSB_ERR_ARG;
+  if (!params || !norm || !X || !T || !idx || !grad || !loss || B <= 0)
+    return fail(c, PSB_ERR_ARG, "psb_mlp_grad: bad argument");
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  const size_t smem = sizeof(TrainSmem);
+  set_smem(mlp_train_kernel, smem);
+  ++c->launches;
+  mlp_train_kernel<<<(B + kRows - 1) / kRows, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
+  return launch_ok(c, "mlp train");
+}
+
+int psb_mlp_adam(psb_ctx* c, float* params, float* m, float* v, float* grad, int step, float lr, float beta1,
+                 float beta2, float eps, float weight_decay) {
+  if (!c) return PSB_ERR_ARG;
+  if (!params || !m || !v || !grad || step < 1) return fail(c, PSB_ERR_ARG, "psb_mlp_adam: bad argument");
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  const float c1 = 1.f - std::pow(beta1, (float)step), c2 = 1.f - std::pow(beta2, (float)step);
+  ++c->launches;
+  adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, c->stream>>>(params, m, v, grad, kMlpParams, lr, beta1, beta2, eps,
+                                                              c1, c2, weight_decay);
+  return launch_ok(c, "adam");
+}
+
+}  // extern "C"

@@ -1,0 +1,189 @@
+// Pointwise subgrid-stress MLP 10 -> 64 -> 64 -> 6 (GELU) on BF16 tensor cores
+// with FP32 accumulation (mma.sync.m16n8k16.bf16, FP32 C/D fragments).
+//
+// This closure has no counterpart in the reference; it replaces the
+// Smagorinsky stress of PySpectral/src/RHSfunctions.py:195-212 by a learned
+// map from the 9 resolved velocity-gradient components and the filter width
+// to the 6 subgrid-stress components tau_ij = filter(u_i u_j) - u_i u_j.
+//
+// Parameter block (FP32 master copy, kMlpParams floats, row-major [out][in]):
+//   W1[64][10] b1[64] W2[64][64] b2[64] W3[6][64] b3[6]
+// Normalisation block (kMlpNorm floats):
+//   xmean[10] xistd[10] ymean[6] ystd[6]
+// Features x = (raw - xmean) * xistd; outputs tau = y * ystd + ymean.
+#pragma once
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace psb {
+
+constexpr int kMlpIn = 10, kMlpH = 64, kMlpOut = 6;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kMlpH * kMlpIn, kOffW2 = kOffB1 + kMlpH,
+              kOffB2 = kOffW2 + kMlpH * kMlpH, kOffW3 = kOffB2 + kMlpH, kOffB3 = kOffW3 + kMlpOut * kMlpH,
+              kMlpParams = kOffB3 + kMlpOut;
+constexpr int kMlpNorm = 32;
+
+// BF16 operand copies staged in shared memory, padded for the m16n8k16 tiles:
+//   w1[64][16] (k padded 10->16), w2[64][64], w3[8][64] (n padded 6->8)
+struct MlpSmem {
+  __nv_bfloat16 w1[kMlpH * 16];
+  __nv_bfloat16 w2[kMlpH * kMlpH];
+  __nv_bfloat16 w3[8 * kMlpH];
+  float b1[kMlpH], b2[kMlpH], b3[8];
+  float xmean[16], xistd[16], ymean[8], ystd[8];
+};
+
+__device__ __forceinline__ void mlp_stage(MlpSmem& s, const float* __restrict__ P, const float* __restrict__ nrm) {
+  for (int i = threadIdx.x; i < kMlpH * 16; i += blockDim.x) {
+    const int o = i / 16, k = i % 16;
+    s.w1[i] = __float2bfloat16_rn(k < kMlpIn ? P[kOffW1 + o * kMlpIn + k] : 0.f);
+  }
+  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) s.w2[i] = __float2bfloat16_rn(P[kOffW2 + i]);
+  for (int i = threadIdx.x; i < 8 * kMlpH; i += blockDim.x) {
+    const int o = i / kMlpH;
+    s.w3[i] = __float2bfloat16_rn(o < kMlpOut ? P[kOffW3 + i] : 0.f);
+  }
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    s.b1[i] = P[kOffB1 + i];
+    s.b2[i] = P[kOffB2 + i];
+  }
+  if (threadIdx.x < 16) {
+    s.xmean[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[threadIdx.x] : 0.f;
+    s.xistd[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[kMlpIn + threadIdx.x] : 0.f;
+  }
+  if (threadIdx.x < 8) {
+    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[kOffB3 + threadIdx.x] : 0.f;
+    s.ymean[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + threadIdx.x] : 0.f;
+    s.ystd[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + kMlpOut + threadIdx.x] : 0.f;
+  }
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+__device__ __forceinline__ uint32_t pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi) {
+  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+}
+
+// D = A(16x16, row) * B(16x8, col) + D, BF16 in, FP32 accumulate.
+__device__ __forceinline__ void mma16816(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// exact GELU and its derivative (erf form)
+__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_d(float x) {
+  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// B fragment of a weight stored [n][k] row-major (ld = k stride) for the tile (k0, n0).
+__device__ __forceinline__ void bfrag_nk(uint32_t* b, const __nv_bfloat16* W, int ld, int k0, int n0, int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const __nv_bfloat16* r = W + (n0 + g) * ld + k0 + 2 * t;
+  b[0] = pack_raw(r[0], r[1]);
+  b[1] = pack_raw(r[8], r[9]);
+}
+
+// Warp-level forward pass of 16 points.  xa: A fragment of the normalised
+// features (16 x 16, k 10..15 zero).  Returns y[4]: C fragment of the 16 x 8
+// outputs (normalised; columns 6,7 unused).  If z1/z2 are given, the
+// pre-activations are kept (for the backward pass).
+__device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_t* xa, float* y, float (*z1)[4],
+                                                 float (*z2)[4]) {
+  const int lane = threadIdx.x & 31, t = lane & 3;
+  float h[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float b0 = s.b1[8 * j + 2 * t], b1 = s.b1[8 * j + 2 * t + 1];
+    h[j][0] = b0;
+    h[j][1] = b1;
+    h[j][2] = b0;
+    h[j][3] = b1;
+    uint32_t b[2];
+    bfrag_nk(b, s.w1, 16, 0, 8 * j, lane);
+    mma16816(h[j], xa, b);
+  }
+  uint32_t a[4][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (z1) z1[j][e] = h[j][e];
+      h[j][e] = gelu_f(h[j][e]);
+    }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a[kk][0] = pack_bf16(h[2 * kk][0], h[2 * kk][1]);
+    a[kk][1] = pack_bf16(h[2 * kk][2], h[2 * kk][3]);
+    a[kk][2] = pack_bf16(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+    a[kk][3] = pack_bf16(h[2 * kk + 1][2], h[2 * kk + 1][3]);
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float b0 = s.b2[8 * j + 2 * t], b1 = s.b2[8 * j + 2 * t + 1];
+    h[j][0] = b0;
+    h[j][1] = b1;
+    h[j][2] = b0;
+    h[j][3] = b1;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      uint32_t b[2];
+      bfrag_nk(b, s.w2, kMlpH, 16 * kk, 8 * j, lane);
+      mma16816(h[j], a[kk], b);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (z2) z2[j][e] = h[j][e];
+      h[j][e] = gelu_f(h[j][e]);
+    }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a[kk][0] = pack_bf16(h[2 * kk][0], h[2 * kk][1]);
+    a[kk][1] = pack_bf16(h[2 * kk][2], h[2 * kk][3]);
+    a[kk][2] = pack_bf16(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+    a[kk][3] = pack_bf16(h[2 * kk + 1][2], h[2 * kk + 1][3]);
+  }
+  const float c0 = s.b3[2 * t], c1 = s.b3[2 * t + 1];
+  y[0] = c0;
+  y[1] = c1;
+  y[2] = c0;
+  y[3] = c1;
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    uint32_t b[2];
+    bfrag_nk(b, s.w3, kMlpH, 16 * kk, 0, lane);
+    mma16816(y, a[kk], b);
+  }
+}
+
+// A fragment of normalised features for 16 points; feat(r, f) returns the raw
+// feature f (< 10) of row r (< 16) of this warp's tile.
+template <class F>
+__device__ __forceinline__ void mlp_xfrag(const MlpSmem& s, uint32_t* xa, F feat) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  float v[8];
+  const int rows[2] = {g, g + 8};
+#pragma unroll
+  for (int hr = 0; hr < 2; ++hr)
+#pragma unroll
+    for (int hk = 0; hk < 2; ++hk)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int f = 2 * t + 8 * hk + e;
+        v[hr * 4 + hk * 2 + e] = f < kMlpIn ? (feat(rows[hr], f) - s.xmean[f]) * s.xistd[f] : 0.f;
+      }
+  xa[0] = pack_bf16(v[0], v[1]);  // row g,   k 2t..2t+1
+  xa[1] = pack_bf16(v[4], v[5]);  // row g+8, k 2t..2t+1
+  xa[2] = pack_bf16(v[2], v[3]);  // row g,   k 2t+8..
+  xa[3] = pack_bf16(v[6], v[7]);  // row g+8, k 2t+8..
+}
+
+}  // namespace psb

@@ -124,7 +124,7 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
   z.plan = *plan_for(c, M3);
   z.tw = tw;
   {
-    auto smem_for = [&](int P) { return (size_t)(M3 + 2 * ((6 * P + 1) / 2) * M3) * e; };
+    auto smem_for = [&](int P) { return zpass_smem_bytes<T>(6, P, M3, 0); };
     int P = 8;
     while (P > 1 && smem_for(P) > kSmemBudget) P /= 2;
     while (P > 1 && (z.npencils + P - 1) / P < 2 * 148) P /= 2;

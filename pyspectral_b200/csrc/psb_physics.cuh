@@ -481,3 +481,81 @@ struct EpiPLQL {
 };
 
 }  // namespace psb
+
+// ---- learned subgrid closure (no counterpart in the reference) -------------
+#include "psb_mlp.cuh"
+
+namespace psb {
+
+// (u,v,w) -> (u,v,w, du_i/dx_j = i k_j u_i for i,j = 1..3), gradient order
+// g[3*i + j]; the spectral expander of the learned closure's x-inverse pass.
+template <typename T>
+struct PreGrad {
+  static constexpr int F_SRC = 3, F_DST = 12;
+  __device__ void operator()(int i, int o, int c, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    const T k[3] = {(T)a.k_row[i], (T)a.k_outer[o], (T)a.k_col[c]};
+#pragma unroll
+    for (int f = 0; f < 3; ++f) d[f] = s[f];
+#pragma unroll
+    for (int f = 0; f < 3; ++f)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) d[3 + 3 * f + j] = pik(k[j], s[f]);
+  }
+};
+
+// Products u_i u_j plus the MLP subgrid stress, summed so that one forward
+// transform per component carries both: out_ij = u_i u_j + tau_ij / s^2 in the
+// reference's real-space scaling (real-space arrays equal physical / s).
+// The MLP runs warp-cooperatively on tensor cores over all points of the CTA.
+template <typename T>
+struct PhysLearned {
+  static constexpr int F_IN = 12, F_OUT = 6;
+  static constexpr bool BLOCK = true;
+  static constexpr int EXTRA_SMEM = (int)((sizeof(MlpSmem) + 15) / 16 * 16);
+  const float* params;
+  const float* norm;
+  T sphys;      // s: physical = real-space * s
+  float delta;  // filter width fed to the MLP
+  __device__ void setup(unsigned char* extra) const {
+    mlp_stage(*reinterpret_cast<MlpSmem*>(extra), params, norm);
+  }
+  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, int es, T fac, long long, long long,
+                        unsigned char* extra) const {
+    const MlpSmem& s = *reinterpret_cast<const MlpSmem*>(extra);
+    const int npts = P * M;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int nw = blockDim.x >> 5;
+    auto val = [&](int f, int pt) -> T {
+      const int p = pt / M, z = pt - p * M;
+      const int r = f * P + p;
+      const Cx<T> v = R[(size_t)z * es + (r >> 1)];
+      return fac * ((r & 1) ? v.y : v.x);
+    };
+    const T is2 = (T)1 / (sphys * sphys);
+    for (int pt0 = warp * 16; pt0 < npts; pt0 += nw * 16) {
+      uint32_t xa[4];
+      mlp_xfrag(s, xa, [&](int r, int f) -> float {
+        const int pt = pt0 + r;
+        if (pt >= npts) return s.xmean[f];
+        return f < 9 ? (float)(val(3 + f, pt) * sphys) : delta;
+      });
+      float y[4];
+      mlp_forward_warp(s, xa, y, nullptr, nullptr);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int c = 2 * t + (e & 1);
+        const int pt = pt0 + g + (e < 2 ? 0 : 8);
+        if (c >= kMlpOut || pt >= npts) continue;
+        const int ii = c < 3 ? c : (c == 5 ? 1 : 0);
+        const int jj = c < 3 ? c : (c == 3 ? 1 : 2);
+        const T tau = (T)(y[e] * s.ystd[c] + s.ymean[c]);
+        const T o = val(ii, pt) * val(jj, pt) + tau * is2;
+        const int p = pt / M, z = pt - p * M;
+        const int r = c * P + p;
+        reinterpret_cast<T*>(W + (size_t)z * es + (r >> 1))[r & 1] = o;
+      }
+    }
+  }
+};
+
+}  // namespace psb

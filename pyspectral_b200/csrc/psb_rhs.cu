@@ -632,6 +632,16 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
         return dtau_rhs_d(c, io, p, tau_out);
       else
         return dtau_rhs_f(c, io, p, tau_out);
+    case PSB_LEARNED: {
+      if (Qin && (!p->mlp_params || !p->mlp_norm))
+        return fail(c, PSB_ERR_ARG, "PSB_LEARNED needs mlp_params and mlp_norm");
+      EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
+                          (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
+      const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
+      PhysLearned<T> phys{reinterpret_cast<const float*>(p->mlp_params), reinterpret_cast<const float*>(p->mlp_norm),
+                          (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta)};
+      return run_ns32<T>(c, Qin, PreGrad<T>{}, phys, epi);
+    }
     default:
       return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");
   }
@@ -650,6 +660,29 @@ int sgs_dns_run(psb_ctx* c, const void* fields, void* w0, void* tau6) {
 }
 template int sgs_dns_run<double>(psb_ctx*, const void*, void*, void*);
 template int sgs_dns_run<float>(psb_ctx*, const void*, void*, void*);
+
+// The six dealiased product spectra (uuhat.. of src/RHSfunctions.py:18-23).
+template <typename T>
+struct EpiProducts {
+  static constexpr int F_IN = 6;
+  Cx<T>* out;
+  long long fstride;
+  int n2, n3h;
+  __host__ double io_bytes(long long npts) const { return (double)sizeof(Cx<T>) * npts * 6; }
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = ((long long)i1 * n2 + i2) * n3h + i3;
+#pragma unroll
+    for (int m = 0; m < 6; ++m) out[m * fstride + s] = P[m];
+  }
+};
+
+template <typename T>
+int products_run(psb_ctx* c, const void* fields, void* out6) {
+  EpiProducts<T> epi{reinterpret_cast<Cx<T>*>(out6), (long long)c->N1 * c->N2 * c->N3h, c->N2, c->N3h};
+  return run_ns32<T>(c, reinterpret_cast<const Cx<T>*>(fields), PreCopyN<T, 3>{}, PhysProducts<T>{}, epi);
+}
+template int products_run<double>(psb_ctx*, const void*, void*);
+template int products_run<float>(psb_ctx*, const void*, void*);
 
 // exported for the dynamic tau-model translation unit
 template <typename T>

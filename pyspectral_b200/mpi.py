@@ -166,6 +166,9 @@ class variables:
     def Q2U(self):
         self.U.copy_(self.Q)
 
+    def closure_code(self):
+        return _capi.MHD
+
     def params(self):
         return _capi.make_params(nu=self.nu, eta=self.lam, t=self.t, dt=self.dt,
                                  force=self.force.data_ptr() if self.force is not None else None)

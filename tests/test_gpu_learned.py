@@ -1,0 +1,105 @@
+"""Learned subgrid closure on the GPU: tensor-core forward and gradients vs the
+CPU oracle, training, the learned LES right-hand side vs the oracle."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+from oracle import spectral_oracle as orc
+from tests.helpers import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _data(n, seed=0):
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, 9)) * 3.0
+    X = np.concatenate([G, np.full((n, 1), 2 * np.pi / 64) + 0.01 * rng.standard_normal((n, 1))], axis=1)
+    S = 0.5 * (G.reshape(n, 3, 3) + G.reshape(n, 3, 3).transpose(0, 2, 1))
+    Sm = np.sqrt(2 * (S * S).sum((1, 2)))
+    d = X[:, 9]
+    tau = -2 * ((0.16 * d) ** 2 * Sm)[:, None, None] * S
+    T = np.stack([tau[:, 0, 0], tau[:, 1, 1], tau[:, 2, 2], tau[:, 0, 1], tau[:, 0, 2], tau[:, 1, 2]], axis=1)
+    norm = np.r_[X.mean(0), 1 / X.std(0), T.mean(0), T.std(0)]
+    return X, T, norm
+
+
+def _model(torch, seed, norm):
+    from pyspectral_b200.learned import MLPModel
+    P = mo.init_params(seed)
+    P = P + 0.05 * np.random.default_rng(seed).standard_normal(P.shape)  # nonzero biases
+    return MLPModel(params=P, norm=norm), P
+
+
+def test_forward_and_gradients_match_cpu_oracle():
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    X, T, norm = _data(300)
+    m, P = _model(torch, 3, norm)
+    ctx = _capi.Context(16, 16, 16, precision=32)
+    Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
+    Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
+    Pf = m.params.cpu().numpy().astype(np.float64)
+    nf = m.norm.cpu().numpy().astype(np.float64)
+    Xf = Xd.cpu().numpy().astype(np.float64)
+    Tf = Td.cpu().numpy().astype(np.float64)
+    Y = m.forward(ctx, Xd).cpu().numpy()
+    Yo = mo.forward(Pf, nf, Xf)
+    assert rel(Y, Yo) < 2e-3
+    idx = torch.arange(300, dtype=torch.int32, device="cuda")
+    loss, grad = m.grad_of(ctx, Xd, Td, idx)
+    lo, go = mo.loss_and_grad(Pf, nf, Xf, Tf)
+    assert loss == pytest.approx(lo, rel=2e-3)
+    g = grad.cpu().numpy()
+    # per block: W1 b1 W2 b2 W3 b3
+    o = 0
+    for name, shp in mo.SIZES:
+        k = int(np.prod(shp))
+        assert rel(g[o:o + k], go[o:o + k]) < 5e-3, name
+        o += k
+
+
+def test_training_reduces_loss():
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.learned import MLPModel
+    X, T, _ = _data(1 << 15, seed=1)
+    Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
+    Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
+    m = MLPModel(seed=0)
+    m.fit_norm(Xd, Td)
+    ctx = _capi.Context(16, 16, 16, precision=32)
+    idx = torch.arange(4096, dtype=torch.int32, device="cuda")
+    l0, _ = m.grad_of(ctx, Xd, Td, idx)
+    m.grad.zero_()
+    m.train(ctx, Xd, Td, 600, batch=4096, lr=3e-3)
+    l1, _ = m.grad_of(ctx, Xd, Td, idx)
+    assert np.isfinite(l1) and l1 < 0.1 * l0, (l0, l1)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_learned_rhs_matches_oracle(precision):
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    N = 16
+    st = orc.isotropic_state(N, 9, k0=3.0)
+    _, _, norm = _data(500, seed=2)
+    m, P = _model(torch, 5, norm)
+    grid = C.gridclass.periodic(N)
+    main = C.variables(0, "learned", 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 0.01, 0.02, precision=precision,
+                       model=m)
+    main.computeRHS(main, grid, None, None)
+    g = orc.Grid.periodic(N)
+    ref = mo.rhs_learned(g, st, 0.02, m.params.cpu().numpy().astype(np.float64),
+                         m.norm.cpu().numpy().astype(np.float64), 2 * np.pi / N)
+    tol = 1e-4 if precision == 64 else 5e-4
+    assert rel(main.Q.cpu().numpy(), ref) < tol
+    # the closure changes the RHS (it is not the DNS one)
+    dns = orc.rhs_nosgs(g, st, orc.Params(nu=0.02))[0]
+    assert rel(dns, ref) > 1e-3

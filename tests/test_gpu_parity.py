@@ -235,3 +235,23 @@ def test_tgv64_known_answer_history():
     dE = np.diff(Es[1:]) / dt
     dEm = np.diff(E[1:]) / dt
     assert np.abs(dE - dEm).max() < 0.02 * np.abs(dEm).max()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_cuda_graph_replay_equals_eager_steps(precision):
+    """A captured 3-step graph replayed twice gives bit-identical state to
+    6 eager steps."""
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import StepGraph, advance
+    d = golden("serial_N16.npz")
+    grid, a = _main("smag", 16, d["state"], precision)
+    grid2, b = _main("smag", 16, d["state"], precision)
+    g = StepGraph(a, grid, 3)
+    g.replay()
+    g.replay()
+    advance(b, grid2, 6)
+    torch.cuda.synchronize()
+    assert torch.equal(a.Q, b.Q)
+    assert torch.equal(a.U, b.U)
+    del C

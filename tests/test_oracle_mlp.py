@@ -1,0 +1,28 @@
+"""The MLP oracle's analytic gradient agrees with central finite differences
+(BF16 rounding switched off for the check)."""
+import numpy as np
+
+from oracle import mlp_oracle as mo
+
+
+def test_mlp_oracle_gradient_matches_finite_differences(monkeypatch):
+    monkeypatch.setattr(mo, "bf16", lambda x: np.asarray(x, np.float64))
+    rng = np.random.default_rng(0)
+    X = rng.standard_normal((40, 10))
+    T = rng.standard_normal((40, 6))
+    norm = np.r_[np.zeros(10), np.ones(10), np.zeros(6), np.ones(6)]
+    P = mo.init_params(1) + 0.01 * rng.standard_normal(mo.NPARAMS)
+    _, g = mo.loss_and_grad(P, norm, X, T)
+    for i in (0, 5, 650, 700, 4800, 5250, mo.NPARAMS - 1):
+        e = np.zeros_like(P)
+        e[i] = 1e-6
+        fd = (mo.loss_and_grad(P + e, norm, X, T)[0] - mo.loss_and_grad(P - e, norm, X, T)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i])) + 1e-9
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8, -2.5, 3.0e-3], dtype=np.float32)
+    r = mo.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6
+    assert r[3] == -2.5
+    assert abs(r[4] - 3.0e-3) / 3.0e-3 < 2 ** -8
