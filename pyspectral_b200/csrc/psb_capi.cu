@@ -35,34 +35,22 @@ bool smooth23(int L) {
 FFTPlan make_plan(int L) {
   FFTPlan p{};
   p.L = L;
-  int radix[kMaxPasses], np = 0;
   int n = L;
   while (n % 8 == 0) {
-    radix[np++] = 8;
+    p.radix[p.npass++] = 8;
     n /= 8;
   }
   while (n % 4 == 0) {
-    radix[np++] = 4;
+    p.radix[p.npass++] = 4;
     n /= 4;
   }
   while (n % 2 == 0) {
-    radix[np++] = 2;
+    p.radix[p.npass++] = 2;
     n /= 2;
   }
   while (n % 3 == 0) {
-    radix[np++] = 3;
+    p.radix[p.npass++] = 3;
     n /= 3;
-  }
-  p.npass = np;
-  int Ns = 1;
-  for (int s = 0; s < np; ++s) {
-    FFTPass& q = p.pass[s];
-    q.R = radix[s];
-    q.nb = L / q.R;
-    q.Ns = Ns;
-    q.tstride = L / (Ns * q.R);
-    q.mag_ns = fdiv_magic((unsigned)Ns);
-    Ns *= q.R;
   }
   return p;
 }

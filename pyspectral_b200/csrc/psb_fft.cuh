@@ -50,29 +50,13 @@ __device__ __forceinline__ Cx<T> mul_mi(Cx<T> a) { return mk<T>(a.y, -a.x); }
 
 constexpr int kMaxPasses = 12;
 
-// One Stockham pass: radix R, nb = L/R butterflies per line, Ns = product of
-// the previous radices, tstride = L/(Ns*R) (twiddle index step), and the
-// multiply-high reciprocal of Ns (exact for numerators * Ns < 2^32).
-struct FFTPass {
-  int R, nb, Ns, tstride;
-  unsigned long long mag_ns;
-};
-
 // Radix schedule of one transform length (host-built).
 struct FFTPlan {
   int L;
   int npass;
-  FFTPass pass[kMaxPasses];
+  int radix[kMaxPasses];
   int tw_off;  // offset of this length's twiddle table in the pool
 };
-
-// q = n / d for the divisor d of mag = ceil(2^32 / d), n * d < 2^32
-__host__ __device__ __forceinline__ unsigned long long fdiv_magic(unsigned d) {
-  return ((1ULL << 32) + d - 1) / d;
-}
-__device__ __forceinline__ int fdivu(int n, unsigned long long mag) {
-  return (int)(((unsigned long long)(unsigned)n * mag) >> 32);
-}
 
 // ---- small DFTs ----------------------------------------------------------
 // Forward uses exp(-2 pi i m r / R); INV uses the conjugate.
@@ -146,16 +130,17 @@ __device__ __forceinline__ void small_dft(Cx<T>* v) {
   }
 }
 
-// One Stockham butterfly: sub-transform position j (k = j mod Ns) of a pass
-// of radix R; element (line, j) lives at buf[j*es] relative to the line.
+// One Stockham butterfly: sub-transform position j of a pass of radix R.
 template <typename T, int R, bool INV>
-__device__ __forceinline__ void stockham_bfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst, int j,
-                                              int k, const FFTPass& P, const Cx<T>* __restrict__ tw, int es) {
+__device__ __forceinline__ void stockham_bfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst,
+                                              int j, int nb, int Ns, int L, const Cx<T>* __restrict__ tw,
+                                              int es) {
   Cx<T> v[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = src[(j + r * P.nb) * es];
-  if (k) {
-    const int tstep = k * P.tstride;
+  for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
+  const int k = j % Ns;
+  if (Ns > 1) {
+    const int tstep = k * (L / (Ns * R));
 #pragma unroll
     for (int r = 1; r < R; ++r) {
       Cx<T> w = tw[r * tstep];
@@ -166,38 +151,46 @@ __device__ __forceinline__ void stockham_bfly(const Cx<T>* __restrict__ src, Cx<
   small_dft<T, R, INV>(v);
   const int base = (j - k) * R + k;
 #pragma unroll
-  for (int r = 0; r < R; ++r) dst[(base + r * P.Ns) * es] = v[r];
+  for (int r = 0; r < R; ++r) dst[(base + r * Ns) * es] = v[r];
 }
 
-// Transform `nlines` lines held at buf[j*es + line] (j < L, line < nlines <=
-// es).  `a` holds the input; `b` is scratch of the same footprint.  Returns the
-// buffer holding the result.  Consecutive threads take consecutive lines, so
-// every shared-memory access of a warp is contiguous.  Must be called by all
-// threads of the CTA; ends with __syncthreads.
+// Transform `nlines` lines held at buf[line*ls + j*es] (j < L).  `a` holds the
+// input; `b` is scratch of the same footprint.  Returns the buffer holding the
+// result.  lines_fast selects the thread->work mapping: true when consecutive
+// lines are adjacent in memory (es > 1, ls == 1), false for contiguous lines.
+// Must be called by all threads of the CTA; ends with __syncthreads.
 template <typename T, bool INV>
-__device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* __restrict__ tw, int nlines,
-                            int es) {
-  const unsigned long long mag_lines = fdiv_magic((unsigned)nlines);
+__device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* __restrict__ tw,
+                            int nlines, int ls, int es, bool lines_fast) {
+  const int L = p.L;
+  int Ns = 1;
   for (int s = 0; s < p.npass; ++s) {
-    const FFTPass P = p.pass[s];
-    const int total = P.nb * nlines;
+    const int R = p.radix[s];
+    const int nb = L / R;
+    const int total = nb * nlines;
     for (int id = threadIdx.x; id < total; id += blockDim.x) {
-      const int j = fdivu(id, mag_lines);
-      const int line = id - j * nlines;
-      const int k = j - fdivu(j, P.mag_ns) * P.Ns;
-      const Cx<T>* src = a + line;
-      Cx<T>* dst = b + line;
-      switch (P.R) {
-        case 8: stockham_bfly<T, 8, INV>(src, dst, j, k, P, tw, es); break;
-        case 4: stockham_bfly<T, 4, INV>(src, dst, j, k, P, tw, es); break;
-        case 3: stockham_bfly<T, 3, INV>(src, dst, j, k, P, tw, es); break;
-        default: stockham_bfly<T, 2, INV>(src, dst, j, k, P, tw, es); break;
+      int line, j;
+      if (lines_fast) {
+        line = id % nlines;
+        j = id / nlines;
+      } else {
+        j = id % nb;
+        line = id / nb;
+      }
+      const Cx<T>* src = a + (size_t)line * ls;
+      Cx<T>* dst = b + (size_t)line * ls;
+      switch (R) {
+        case 8: stockham_bfly<T, 8, INV>(src, dst, j, nb, Ns, L, tw, es); break;
+        case 4: stockham_bfly<T, 4, INV>(src, dst, j, nb, Ns, L, tw, es); break;
+        case 3: stockham_bfly<T, 3, INV>(src, dst, j, nb, Ns, L, tw, es); break;
+        default: stockham_bfly<T, 2, INV>(src, dst, j, nb, Ns, L, tw, es); break;
       }
     }
     __syncthreads();
     Cx<T>* t = a;
     a = b;
     b = t;
+    Ns *= R;
   }
   return a;
 }

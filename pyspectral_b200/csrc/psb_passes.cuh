@@ -39,7 +39,9 @@ constexpr int kMaxZFields = 16;
 
 // Phys functors with `static constexpr bool BLOCK = true` provide
 // setup(extra_smem) and block(R, W, P, M, fac, p0, npencils, extra_smem) and
-// ask for EXTRA_SMEM bytes behind the z-pass buffers.
+// ask for EXTRA_SMEM bytes behind the z-pass buffers.  R and W hold packed
+// real line r (field f, pencil p: r = f*P + p) at component r&1 of complex
+// line r>>1, position z at buf[(r>>1)*M + z].
 template <class P, class = void>
 struct phys_is_block {
   static constexpr bool value = false;
@@ -76,13 +78,13 @@ struct PreCopy {
   __device__ void operator()(int, int, int, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const { d[0] = s[0]; }
 };
 
-// grid = (ceil(ncols/col_tile), nouter); smem = tw[L] + 2 * L*lines; col_tile is a power of two
+// grid = (ceil(ncols/col_tile), nouter); smem = tw[L] + 2 * L*lines
 template <typename T, bool INV, class Pre>
 __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   const int L = a.plan.L;
-  const int ct = a.col_tile, lct = __ffs(ct) - 1;
+  const int ct = a.col_tile;
   const int lines = Pre::F_DST * ct;
   Cx<T>* bufA = tw + L;
   Cx<T>* bufB = bufA + (size_t)L * lines;
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) 
   __syncthreads();
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
   for (int idx = threadIdx.x; idx < a.in_rows * ct; idx += blockDim.x) {
-    const int c = idx & (ct - 1), i = idx >> lct;
+    const int c = idx % ct, i = idx / ct;
     const int col = c0 + c;
     const int j = a.in_map(i);
     if (j < 0 || col >= a.ncols) continue;
@@ -106,13 +108,13 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) 
     for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, INV>(bufA, bufB, a.plan, tw, lines, lines);
+  Cx<T>* res = block_fft<T, INV>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
   Cx<T>* outb = a.out + (long long)o * a.out_ostride;
   const int nst = a.out_rows * Pre::F_DST * ct;
   for (int idx = threadIdx.x; idx < nst; idx += blockDim.x) {
-    const int c = idx & (ct - 1);
-    const int t = idx >> lct;
-    const int i = t / Pre::F_DST, g = t - i * Pre::F_DST;
+    const int c = idx % ct;
+    const int t = idx / ct;
+    const int g = t % Pre::F_DST, i = t / Pre::F_DST;
     const int col = c0 + c;
     if (col >= a.ncols) continue;
     const int j = a.out_map(i);
@@ -136,16 +138,14 @@ struct ZArgs {
   const Cx<T>* tw;
 };
 
-// Packed-line count of the z-pass buffers, rounded to an odd stride so that a
-// warp walking the transform axis hits distinct banks.
-__host__ __device__ __forceinline__ int zpass_es(int fmax, int P) { return ((fmax * P + 1) / 2) | 1; }
+// Shared memory of one z-pass CTA: twiddles, two buffers of
+// nl = ceil(fmax*P/2) packed lines of length M, and the Phys extra.
 template <typename T>
 __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
-  return (size_t)(M + 2 * (size_t)zpass_es(fmax, P) * M) * sizeof(Cx<T>) + extra;
+  return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * M) * sizeof(Cx<T>) + extra;
 }
 
-// grid = ceil(npencils/ppc); smem = zpass_smem_bytes.  Buffers hold packed
-// complex line c at position k in buf[k*es + c].
+// grid = ceil(npencils/ppc); smem = zpass_smem_bytes
 template <typename T, class Phys>
 __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -154,93 +154,96 @@ __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
   const int M = a.plan.L;
   const int P = a.ppc;
   constexpr int FMAX = FI > FO ? FI : FO;
-  const int es = zpass_es(FMAX, P);
+  const int nl = (FMAX * P + 1) / 2;
   Cx<T>* X = tw + M;
-  Cx<T>* Y = X + (size_t)es * M;
-  unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)es * M);
+  Cx<T>* Y = X + (size_t)nl * M;
+  unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * M);
   const long long p0 = (long long)blockIdx.x * P;
   stage_twiddles(tw, a.tw, a.plan);
   if constexpr (phys_is_block<Phys>::value) phys.setup(extra);
   const Cx<T> zero = mk<T>(0, 0);
   const int half = M / 2;
-  const unsigned long long magM = fdiv_magic((unsigned)M);
   Cx<T>* R = X;
   if constexpr (FI > 0) {
     const int nin = (FI * P + 1) / 2;
-    for (int idx = threadIdx.x; idx < es * M; idx += blockDim.x) X[idx] = zero;
+    for (int idx = threadIdx.x; idx < nin * M; idx += blockDim.x) X[idx] = zero;
     __syncthreads();
     // pack pairs of Hermitian half-spectra: Z = A + iB, Z[M-k] = conj(A_k) + i conj(B_k);
     // the k=0 and k=M/2 terms keep their real parts only (c2r convention)
-    const unsigned long long magH = fdiv_magic((unsigned)(half + 1));
     for (int idx = threadIdx.x; idx < nin * (half + 1); idx += blockDim.x) {
-      const int c = fdivu(idx, magH), k = idx - c * (half + 1);
+      const int k = idx % (half + 1), c = idx / (half + 1);
       Cx<T> A = zero, B = zero;
 #pragma unroll 1
       for (int part = 0; part < 2; ++part) {
         const int r = 2 * c + part;
         if (r >= FI * P) break;
-        const int f = r / P, p = r - f * P;
+        const int f = r / P, p = r % P;
         const long long pen = p0 + p;
         if (pen >= a.npencils || k >= a.in_kz[f]) continue;
         const Cx<T> v = a.in[f][pen * a.in_pstride[f] + k];
         if (part == 0) A = v; else B = v;
       }
+      Cx<T>* Z = X + (size_t)c * M;
       if (k == 0 || k == half) {
-        X[(size_t)k * es + c] = mk<T>(A.x, B.x);
+        Z[k] = mk<T>(A.x, B.x);
       } else {
-        X[(size_t)k * es + c] = mk<T>(A.x - B.y, A.y + B.x);
-        X[(size_t)(M - k) * es + c] = mk<T>(A.x + B.y, B.x - A.y);
+        Z[k] = mk<T>(A.x - B.y, A.y + B.x);
+        Z[M - k] = mk<T>(A.x + B.y, B.x - A.y);
       }
     }
     __syncthreads();
-    R = block_fft<T, true>(X, Y, a.plan, tw, nin, es);
+    R = block_fft<T, true>(X, Y, a.plan, tw, nin, M, 1, false);
   }
   Cx<T>* W = (R == X) ? Y : X;
   const int nout = (FO * P + 1) / 2;
   if constexpr (phys_is_block<Phys>::value) {
-    // block-cooperative physics (e.g. a tensor-core MLP over the CTA's points)
-    phys.block(R, W, P, M, es, a.fac, p0, a.npencils, extra);
+    // block-cooperative physics (a tensor-core MLP over the CTA's points)
+    phys.block(R, W, P, M, a.fac, p0, a.npencils, extra);
     if ((FO * P) & 1) {
-      for (int z = threadIdx.x; z < M; z += blockDim.x)
-        reinterpret_cast<T*>(W + (size_t)z * es + (nout - 1))[1] = (T)0;
+      for (int z = threadIdx.x; z < M; z += blockDim.x) reinterpret_cast<T*>(W + (size_t)(nout - 1) * M + z)[1] = (T)0;
     }
   } else {
-    // pointwise physics
+    // pointwise physics; the last CTA may hold fewer than P pencils
     for (int idx = threadIdx.x; idx < P * M; idx += blockDim.x) {
-      const int p = fdivu(idx, magM), z = idx - p * M;
+      const int z = idx % M, p = idx / M;
       T vin[FI > 0 ? FI : 1], vout[FO > 0 ? FO : 1];
 #pragma unroll
       for (int f = 0; f < FI; ++f) {
         const int r = f * P + p;
-        const Cx<T> v = R[(size_t)z * es + (r >> 1)];
+        const Cx<T> v = R[(size_t)(r >> 1) * M + z];
         vin[f] = a.fac * ((r & 1) ? v.y : v.x);
       }
-      phys(p0 + p, z, vin, vout);
+      if (p0 + p < a.npencils) {
+        phys(p0 + p, z, vin, vout);
+      } else {
+#pragma unroll
+        for (int g = 0; g < FO; ++g) vout[g] = (T)0;
+      }
 #pragma unroll
       for (int g = 0; g < FO; ++g) {
         const int r = g * P + p;
-        T* w = reinterpret_cast<T*>(W + (size_t)z * es + (r >> 1));
+        T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + z);
         w[r & 1] = vout[g];
       }
       if ((FO * P) & 1) {  // odd count: the last packed line has no partner
-        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)z * es + (nout - 1))[1] = (T)0;
+        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * M + z)[1] = (T)0;
       }
     }
   }
   if constexpr (FO > 0) {
     __syncthreads();
-    Cx<T>* R2 = block_fft<T, false>(W, R, a.plan, tw, nout, es);
+    Cx<T>* R2 = block_fft<T, false>(W, R, a.plan, tw, nout, M, 1, false);
     // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
     const int kzo = a.out_kz;
-    const unsigned long long magK = fdiv_magic((unsigned)kzo);
     for (int idx = threadIdx.x; idx < nout * kzo; idx += blockDim.x) {
-      const int c = fdivu(idx, magK), k = idx - c * kzo;
-      const Cx<T> zk = R2[(size_t)k * es + c], zm = R2[(size_t)(k == 0 ? 0 : M - k) * es + c];
+      const int k = idx % kzo, c = idx / kzo;
+      const Cx<T>* Z = R2 + (size_t)c * M;
+      const Cx<T> zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
 #pragma unroll
       for (int part = 0; part < 2; ++part) {
         const int r = 2 * c + part;
         if (r >= FO * P) break;
-        const int g = r / P, p = r - g * P;
+        const int g = r / P, p = r % P;
         const long long pen = p0 + p;
         if (pen >= a.npencils) continue;
         const Cx<T> v = part == 0 ? mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y))
@@ -299,18 +302,17 @@ __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
   const int c0 = (blockIdx.x % ntile) * ct;
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
-  const int lct = __ffs(ct) - 1;
   for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) {
-    const int c = idx & (ct - 1);
-    const int t = idx >> lct;
-    const int j = t / F, f = t - j * F;
+    const int c = idx % ct;
+    const int t = idx / ct;
+    const int f = t % F, j = t / F;
     const int col = c0 + c;
     bufA[(size_t)j * lines + f * ct + c] = col < a.kz ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, false>(bufA, bufB, a.plan, tw, lines, lines);
+  Cx<T>* res = block_fft<T, false>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
   for (int idx = threadIdx.x; idx < a.n1 * ct; idx += blockDim.x) {
-    const int c = idx & (ct - 1), i1 = idx >> lct;
+    const int c = idx % ct, i1 = idx / ct;
     const int col = c0 + c;
     if (col >= a.kz) continue;
     const int j = a.out_map(i1);

@@ -519,7 +519,7 @@ struct PhysLearned {
   __device__ void setup(unsigned char* extra) const {
     mlp_stage(*reinterpret_cast<MlpSmem*>(extra), params, norm);
   }
-  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, int es, T fac, long long, long long,
+  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
                         unsigned char* extra) const {
     const MlpSmem& s = *reinterpret_cast<const MlpSmem*>(extra);
     const int npts = P * M;
@@ -528,7 +528,7 @@ struct PhysLearned {
     auto val = [&](int f, int pt) -> T {
       const int p = pt / M, z = pt - p * M;
       const int r = f * P + p;
-      const Cx<T> v = R[(size_t)z * es + (r >> 1)];
+      const Cx<T> v = R[(size_t)(r >> 1) * M + z];
       return fac * ((r & 1) ? v.y : v.x);
     };
     const T is2 = (T)1 / (sphys * sphys);
@@ -552,7 +552,7 @@ struct PhysLearned {
         const T o = val(ii, pt) * val(jj, pt) + tau * is2;
         const int p = pt / M, z = pt - p * M;
         const int r = c * P + p;
-        reinterpret_cast<T*>(W + (size_t)z * es + (r >> 1))[r & 1] = o;
+        reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + z)[r & 1] = o;
       }
     }
   }
