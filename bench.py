@@ -2,10 +2,12 @@
 """Throughput of the PySpectral RK4 step on B200.
 
 Metric: grid-point x RK4-steps per second (N^3 * steps / s) of a 64^3 LES of
-decaying isotropic turbulence, FP32 fields with Kahan-compensated stage
-accumulation, next to the plain FP64 path of the same closure.  One step is
-one full RK4 step (four RHS evaluations and stage updates) over the whole
-grid.
+decaying isotropic turbulence with the learned MLP subgrid closure, FP32
+fields with Kahan-compensated stage accumulation, next to the plain FP64
+Smagorinsky path (and the FP32 Smagorinsky path) on the same state.  One step
+is one full RK4 step (four RHS evaluations and stage updates) over the whole
+grid.  The line carries the a-posteriori E(k) error of both closures against
+the filtered 256^3 DNS, as recorded with the shipped model.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -50,7 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--N", type=int, default=64)
-    ap.add_argument("--closure", choices=["smag", "dns"], default="smag")
+    ap.add_argument("--closure", choices=["learned", "smag", "dns"], default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -124,6 +126,21 @@ def make_state(N, seed):
     return isotropic_state(N, seed, k0=4.0)
 
 
+def cpu_rhs(N, closure):
+    """The FP64 CPU right-hand side of `closure` (oracle port) and its grid."""
+    from oracle import spectral_oracle as orc
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=1e-3)
+    if closure == "learned":
+        import numpy as np
+        from oracle import mlp_oracle as mo
+        d = np.load(os.path.join(ROOT, "pyspectral_b200", "models", "sgs_mlp.npz"))
+        P, nrm = d["params"].astype(np.float64), d["norm"].astype(np.float64)
+        return g, (lambda q: mo.rhs_learned(g, q, 1e-3, P, nrm, 2 * math.pi / N))
+    fn = orc.rhs_smag if closure == "smag" else orc.rhs_nosgs
+    return g, (lambda q: fn(g, q, p)[0])
+
+
 def cpu_baseline(N, closure, budget_s):
     """Oracle port timed on the host cores: steps of the same workload until
     the budget is spent (at least one)."""
@@ -131,15 +148,13 @@ def cpu_baseline(N, closure, budget_s):
     from oracle import spectral_oracle as orc
     cores = os.cpu_count() or 1
     orc.set_workers(cores)
-    g = orc.Grid.periodic(N)
+    g, rhs = cpu_rhs(N, closure)
     st = orc.isotropic_state(N, 1, k0=4.0)
-    p = orc.Params(nu=1e-3)
-    fn = orc.rhs_smag if closure == "smag" else orc.rhs_nosgs
     t0 = time.perf_counter()
     n = 0
     Q = st
     while True:
-        Q, _ = orc.advance_rk4(Q, lambda q: (fn(g, q, p)[0], None), 2e-3)
+        Q, _ = orc.advance_rk4(Q, lambda q: (rhs(q), None), 2e-3)
         n += 1
         if time.perf_counter() - t0 >= budget_s:
             break
@@ -225,20 +240,38 @@ def cufft_baseline_ms(N, steps, closure, flush):
     return sum(a.elapsed_time(b) for a, b in ev) / steps
 
 
+def accuracy_record(closure, model):
+    """A-posteriori E(k) error against the filtered 256^3 DNS, as recorded when
+    the shipped model was trained and evaluated on a B200 (learned.main)."""
+    if closure != "learned" or model is None or "eval" not in model.meta:
+        return None
+    ev = model.meta["eval"]
+    out = {"what": f"max/mean relative E(k) error for 1<=k<={ev['k_compare']} vs the {ev['N_dns']}^3 DNS "
+                   f"sharp-cutoff filtered to {ev['n_les']}^3, LES from t={ev['t0']} to t={ev['t_end']}",
+           "source": "model metadata (pyspectral_b200/models/sgs_mlp.json)"}
+    for k in ("learned_fp32", "smagorinsky_fp64", "smagorinsky_fp32", "no_model_fp32"):
+        if k in ev:
+            out[k] = {"max": ev[k]["max_rel_err_k_le_kc_half"], "mean": ev[k]["mean_rel_err"]}
+    return out
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
     # a bounded sample: one warm-up step, then steps until ~60 s of host work
-    # (at most --steps), so the whole run ends within a couple of minutes
-    cpu_baseline(args.N, args.closure, 0.0)
-    cb = cpu_baseline(args.N, args.closure, min(60.0, max(args.cpu_seconds, 1.0) * max(1, min(args.steps, 5))))
+    # (at most --steps), so the whole run ends within a couple of minutes.  The
+    # reference has no learned closure: for that workload its own method, the
+    # plain FP64 Smagorinsky RHS, is what runs.
+    ref_closure = "smag" if args.closure == "learned" else args.closure
+    cpu_baseline(args.N, ref_closure, 0.0)
+    cb = cpu_baseline(args.N, ref_closure, min(60.0, max(args.cpu_seconds, 1.0) * max(1, min(args.steps, 5))))
     v = cb["value"]
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{args.N}^3 decaying isotropic LES, {args.closure}, RK4 dt=2e-3 "
-                                   f"(reference CPU path: NumPy oracle port)", "N": args.N},
+                                   f"(reference CPU path, {ref_closure} FP64: NumPy oracle port)", "N": args.N},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -258,16 +291,19 @@ def run_ours(args):
     from pyspectral_b200.RHSfunctions import StepGraph, advance
 
     N = args.N
-    tm = 1 if args.closure == "smag" else 0
-    code = _capi.SMAG if tm == 1 else _capi.DNS
     st64 = make_state(N, 1 + rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    model = None
+    if args.closure == "learned":
+        from pyspectral_b200.learned import MLPModel
+        model = MLPModel.load(device=local)
 
-    def build(precision):
+    def build(precision, closure):
+        tm = {"learned": "learned", "smag": 1, "dns": 0}[closure]
         grid = C.gridclass.periodic(N, device=local)
         main = C.variables(0, tm, 0, 0, 0, 0, grid, st64[0], st64[1], st64[2], 0.0, 2e-3, 1e-3,
-                           precision=precision)
-        grid.ctx(precision).prepare(code)
+                           precision=precision, model=model if closure == "learned" else None)
+        grid.ctx(precision).prepare(main.closure_code())
         return grid, main
 
     def timed(grid, main, K, W):
@@ -296,18 +332,29 @@ def run_ours(args):
             ms = float(t.item())
         return ms, per_step * K, g
 
-    # FP32 + Kahan (headline) and the plain FP64 path of the same closure
-    grid32, m32 = build(32)
+    # FP32 + Kahan with the chosen closure (headline), the plain FP64
+    # Smagorinsky path and, for context, FP32 Smagorinsky
+    plain = "smag" if args.closure in ("learned", "smag") else "dns"
+    grid32, m32 = build(32, args.closure)
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
     ms32, launches, g32 = timed(grid32, m32, args.steps, args.warmup)
     clocks = sampler.stop() if sampler else None
-    grid64, m64 = build(64)
-    ms64, _, _ = timed(grid64, m64, max(1, args.steps // 2), args.warmup)
+    K64 = max(1, args.steps // 2)
+    grid64, m64 = build(64, plain)
+    ms64, _, g64 = timed(grid64, m64, K64, args.warmup)
     ok = grid32.ctx(32).count_nonfinite(m32.Q) == 0 and grid64.ctx(64).count_nonfinite(m64.Q) == 0
+    del g64
     value = world * N ** 3 * args.steps / (ms32 / 1e3)
-    value64 = world * N ** 3 * max(1, args.steps // 2) / (ms64 / 1e3)
+    value64 = world * N ** 3 * K64 / (ms64 / 1e3)
+    plain32 = None
+    if args.closure == "learned":
+        gridp, mp = build(32, plain)
+        msp, _, gp = timed(gridp, mp, K64, args.warmup)
+        del gp
+        plain32 = {"value": world * N ** 3 * K64 / (msp / 1e3), "ms_per_step": msp / K64,
+                   "what": f"FP32 + Kahan {plain} on the same state"}
 
     # e2e through the public API: pinned host state -> device, step, device -> host
     ctx = grid32.ctx(32)
@@ -370,22 +417,24 @@ def run_ours(args):
         except Exception:
             pass
 
-    cufft_ms = cufft_baseline_ms(N, max(5, args.steps // 10), args.closure, flush) if rank == 0 else None
+    cufft_ms = cufft_baseline_ms(N, max(5, args.steps // 10), plain, flush) if rank == 0 else None
     if rank == 0:
         cb = cpu_baseline(N, args.closure, args.cpu_seconds) if world == 1 else None
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{N}^3 decaying isotropic LES (E(k)~k^4 exp(-2k^2/k0^2), k0=4), "
-                                   f"{args.closure} closure, RK4 dt=2e-3, nu=1e-3, FP32 fields + Kahan stage "
-                                   f"accumulation; learned closure not built yet", "N": N,
-                       "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)", "launch": "one CUDA graph per RK4 step",
-                       "parallelism": f"replicas x{world}"},
-            "fp64_plain": {"value": value64, "ms_per_step": ms64 / max(1, args.steps // 2),
-                           "ratio_f32_over_f64": value / value64},
+            "config": {"workload": f"{N}^3 decaying isotropic LES (E(k)~k^4 exp(-2k^2/k0^2), k0=4, seed "
+                                   f"1+rank), {args.closure} closure, RK4 dt=2e-3, nu=1e-3, FP32 fields + Kahan "
+                                   f"stage accumulation", "N": N,
+                       "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)",
+                       "launch": "one CUDA graph per RK4 step", "parallelism": f"replicas x{world}"},
+            "fp64_plain": {"value": value64, "ms_per_step": ms64 / K64, "closure": plain,
+                           "ratio_headline_over_fp64_plain": value / value64},
+            "fp32_plain": plain32,
+            "accuracy": accuracy_record(args.closure, model),
             "cufft_library_baseline": {"value": N ** 3 / (cufft_ms / 1e3), "ms_per_step": cufft_ms,
-                                       "what": "same FP32 step from torch.fft (cuFFT) + torch elementwise ops"},
+                                       "what": f"FP32 {plain} step from torch.fft (cuFFT) + torch elementwise ops"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clocks,
             "gpu_launches": int(launches), "finite": bool(ok),
         }

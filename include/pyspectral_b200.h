@@ -37,6 +37,9 @@ extern "C" {
 #define PSB_MHD 5         /* 'MHD' of the MPI solver (src_MPI/RHSfunctions.py:95-175)                */
 #define PSB_LEARNED 6     /* learned MLP subgrid stress (no reference counterpart; replaces the
                              Smagorinsky stress of src/RHSfunctions.py:195-212)                    */
+#define PSB_MHD_TMODEL 7  /* MHD + t-model memory term Ct t PLQL on both fields (no reference
+                             counterpart; the construction of src/RHSfunctions.py:240-363 applied
+                             to src_MPI/RHSfunctions.py:95-175, resolved set = 2/3-rule set)      */
 
 /* ---- diagnostic flags --------------------------------------------------- */
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
@@ -87,7 +90,8 @@ const char* psb_create_error(void);
 /* One right-hand-side evaluation: main.computeRHS(main,grid,myFFT,utilities)
  * (src/Classes.py:44,95,124,186,227; src_MPI/Classes.py:147).
  * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD).
- * w0       : optional closure force main.w0_u/v/w (3 fields) or NULL.
+ * w0       : optional closure force main.w0_u/v/w (3 fields; 6 fields u then B for
+ *            PSB_MHD_TMODEL) or NULL.
  * read_out : optional copy of the state as the RHS read it (the reference
  *            rebinds main.uhat/vhat/what to it, src/RHSfunctions.py:10-12;
  *            the MPI solver dealiases it in place, src_MPI/RHSfunctions.py:102-107).

@@ -538,6 +538,93 @@ def rhs_mhd(g, state, nu, force=None, eta=None):
     return r, np.stack(s)
 
 
+def _mhd_nonlinear(k1, k2, k3, ksqr_i, P):
+    """Nonlinear MHD operator from the nine product spectra
+    P = (u_iu_j - B_iB_j for 11,22,33,12,13,23, then u x B): the momentum
+    terms with the pressure projection and the induction term of
+    ``src_MPI/RHSfunctions.py:117-170``, without dissipation, forcing or mask."""
+    n0, n1, n2, n3, n4, n5, x0, x1, x2 = P
+    ph = _pressure(k1, k2, k3, ksqr_i, n0, n1, n2, n3, n4, n5)
+    return np.stack([
+        -1j * k1 * n0 - 1j * k2 * n3 - 1j * k3 * n4 - 1j * k1 * ph,
+        -1j * k1 * n3 - 1j * k2 * n1 - 1j * k3 * n5 - 1j * k2 * ph,
+        -1j * k1 * n4 - 1j * k2 * n5 - 1j * k3 * n2 - 1j * k3 * ph,
+        1j * k2 * x2 - 1j * k3 * x1,
+        1j * k3 * x0 - 1j * k1 * x2,
+        1j * k1 * x1 - 1j * k2 * x0])
+
+
+def mhd_tmodel_memory(g, state, Ct, t, return_ql=False):
+    """t-model memory term ``Ct t PLQL`` of the MHD system (no reference
+    counterpart; the construction of ``computeRHS_tmodel``,
+    ``src/RHSfunctions.py:240-363``, applied to ``computeRHS_MHD``,
+    ``src_MPI/RHSfunctions.py:95-175``).
+
+    The resolved set p is the 2/3-rule set of the MPI grid, q its complement.
+    L(u, B) is the nonlinear MHD operator evaluated without aliasing on the
+    2x grid; QL its q part; PLQL the linearisation of L about (u, B) in the
+    direction QL, restricted to p:
+    momentum products  u_i q_j + q_i u_j - B_i r_j - r_i B_j,
+    induction products q x B + u x r, with (q, r) = QL(u, B).
+    Spectra use the MPI solver's unnormalised convention on the N grid."""
+    N1, N2, N3 = g.N1, g.N2, g.N3
+    F1, F2, F3 = 2 * N1, 2 * N2, 2 * N3
+    D = g.dealias_mask
+    s = [D * state[i] for i in range(6)]
+    up_scale = (F1 * F2 * F3) / (N1 * N2 * N3)
+
+    def rows(N):  # N-grid row index -> 2x-grid row index (the N/2 row is masked anyway)
+        i = np.arange(N)
+        return np.where(i < N // 2, i, i + N)
+
+    r1, r2 = rows(N1), rows(N2)
+
+    def up(x):
+        out = np.zeros((F1, F2, F3 // 2 + 1), dtype=complex)
+        out[np.ix_(r1, r2, np.arange(N3 // 2 + 1))] = x
+        return out
+
+    def down(X):
+        return X[np.ix_(r1, r2, np.arange(N3 // 2 + 1))]
+
+    def phys(X):
+        return _irfftn(X, s=(F1, F2, F3)) * up_scale
+
+    def spec(a):
+        return _rfftn(a) / up_scale
+
+    K1 = (np.fft.fftfreq(F1, 1.0 / F1) * 2.0 * np.pi / g.L1)[:, None, None]
+    K2 = (np.fft.fftfreq(F2, 1.0 / F2) * 2.0 * np.pi / g.L2)[None, :, None]
+    K3 = (np.arange(F3 // 2 + 1) * 2.0 * np.pi / g.L3)[None, None, :]
+    Ki = 1.0 / (K1 ** 2 + K2 ** 2 + K3 ** 2 + 1.0e-50)
+    Dp = np.zeros((F1, F2, F3 // 2 + 1))
+    Dp[np.ix_(r1, r2, np.arange(N3 // 2 + 1))] = D
+    u, v, w, b1, b2, b3 = (phys(up(x)) for x in s)
+
+    def products(u, v, w, b1, b2, b3):
+        return [spec(a) for a in (u * u - b1 * b1, v * v - b2 * b2, w * w - b3 * b3, u * v - b1 * b2,
+                                  u * w - b1 * b3, v * w - b2 * b3, v * b3 - w * b2, w * b1 - u * b3,
+                                  u * b2 - v * b1)]
+
+    QL = (1.0 - Dp) * _mhd_nonlinear(K1, K2, K3, Ki, products(u, v, w, b1, b2, b3))
+    q1, q2, q3, r1_, r2_, r3_ = (phys(x) for x in QL)
+    lin = [spec(a) for a in (
+        2 * u * q1 - 2 * b1 * r1_, 2 * v * q2 - 2 * b2 * r2_, 2 * w * q3 - 2 * b3 * r3_,
+        u * q2 + q1 * v - b1 * r2_ - r1_ * b2, u * q3 + q1 * w - b1 * r3_ - r1_ * b3,
+        v * q3 + q2 * w - b2 * r3_ - r2_ * b3,
+        (q2 * b3 - q3 * b2) + (v * r3_ - w * r2_), (q3 * b1 - q1 * b3) + (w * r1_ - u * r3_),
+        (q1 * b2 - q2 * b1) + (u * r2_ - v * r1_))]
+    PLQL = Dp * _mhd_nonlinear(K1, K2, K3, Ki, lin)
+    mem = Ct * t * np.stack([down(x) for x in PLQL])
+    return (mem, QL) if return_ql else mem
+
+
+def rhs_mhd_tmodel(g, state, nu, Ct, t, force=None, eta=None):
+    """``rhs_mhd`` plus the MHD t-model memory term ``mhd_tmodel_memory``."""
+    r, s = rhs_mhd(g, state, nu, force=force, eta=eta)
+    return r + mhd_tmodel_memory(g, state, Ct, t), s
+
+
 # --------------------------------------------------------------------------
 # Time stepping                         PySpectral/src/PySpec_3d.py:96-105
 # --------------------------------------------------------------------------

@@ -480,6 +480,112 @@ struct EpiPLQL {
   }
 };
 
+// ---- MHD t-model (no reference counterpart) ----------------------------------
+// The t-model construction of PySpectral/src/RHSfunctions.py:240-363 applied to
+// the MHD operator of PySpectral/src_MPI/RHSfunctions.py:95-175: resolved set
+// p = the 2/3-rule set, L evaluated without aliasing on the 2x grid, QL its q
+// part, PLQL the linearisation of L about (u, B) in the direction QL.
+
+// Nonlinear MHD operator from the nine product spectra (u_iu_j - B_iB_j for
+// 11,22,33,12,13,23, then u x B): momentum with the pressure projection and the
+// induction curl, as in EpiMHD without dissipation, forcing and mask.
+template <typename T>
+__device__ __forceinline__ void mhd_nonlinear(T k1, T k2, T k3, T ksqi, const Cx<T>* P, Cx<T>* r) {
+  const Cx<T> ph = ksqi * ((-k1 * k1) * P[0] - (k2 * k2) * P[1] - (k3 * k3) * P[2] - ((T)2 * k1 * k2) * P[3] -
+                           ((T)2 * k1 * k3) * P[4] - ((T)2 * k2 * k3) * P[5]);
+  r[0] = mik(k1, P[0]) + mik(k2, P[3]) + mik(k3, P[4]) + mik(k1, ph);
+  r[1] = mik(k1, P[3]) + mik(k2, P[1]) + mik(k3, P[5]) + mik(k2, ph);
+  r[2] = mik(k1, P[4]) + mik(k2, P[5]) + mik(k3, P[2]) + mik(k3, ph);
+  r[3] = pik(k2, P[8]) - pik(k3, P[7]);
+  r[4] = pik(k3, P[6]) - pik(k1, P[8]);
+  r[5] = pik(k1, P[7]) - pik(k2, P[6]);
+}
+
+// 2x-grid epilogue: QL = L(u, B) on the modes outside the 2/3-rule set.
+template <typename T>
+struct EpiMHDQ {
+  static constexpr int F_IN = 9;
+  __host__ double io_bytes(long long npts) const { return (double)sizeof(Cx<T>) * 6 * npts; }
+  KTabs<T> kf;                 // 2x-grid wavenumbers
+  const double *m1, *m2, *m3;  // N-grid 2/3-rule masks
+  int N1, N2, n3h;             // N-grid sizes (k3 count N3/2+1)
+  int nf2, nf3h;               // 2x-grid rows along y, k3 count
+  long long fstride_2x;
+  T scale;  // 2x-grid transform sums -> N-grid convention (1/8)
+  Cx<T>* QL;  // (6, 2N1, 2N2, N3+1)
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const int n1 = unpad2x_idx(i1, N1), n2 = unpad2x_idx(i2, N2);
+    const bool resolved = n1 >= 0 && n2 >= 0 && i3 < n3h && m1[n1] * m2[n2] * m3[i3] != 0.0;
+    const long long s = ((long long)i1 * nf2 + i2) * nf3h + i3;
+    Cx<T> r[6];
+    if (resolved) {
+#pragma unroll
+      for (int f = 0; f < 6; ++f) r[f] = mk<T>(0, 0);
+    } else {
+      Cx<T> Ps[9];
+#pragma unroll
+      for (int m = 0; m < 9; ++m) Ps[m] = scale * P[m];
+      const T k1 = (T)kf.k1[i1], k2 = (T)kf.k2[i2], k3 = (T)kf.k3[i3];
+      T ksq, ksqi;
+      ksq_pair(k1, k2, k3, ksq, ksqi);
+      mhd_nonlinear(k1, k2, k3, ksqi, Ps, r);
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) QL[f * fstride_2x + s] = r[f];
+  }
+};
+
+// Linearised MHD products about (u, B) in the direction (q, r) = QL:
+// u_i q_j + q_i u_j - B_i r_j - r_i B_j and q x B + u x r.
+template <typename T>
+struct PhysMHDLin {
+  static constexpr int F_IN = 12, F_OUT = 9;
+  __device__ __forceinline__ void operator()(long long, int, const T* in, T* out) const {
+    const T u = in[0], v = in[1], w = in[2], b1 = in[3], b2 = in[4], b3 = in[5];
+    const T q1 = in[6], q2 = in[7], q3 = in[8], r1 = in[9], r2 = in[10], r3 = in[11];
+    out[0] = (T)2 * (u * q1 - b1 * r1);
+    out[1] = (T)2 * (v * q2 - b2 * r2);
+    out[2] = (T)2 * (w * q3 - b3 * r3);
+    out[3] = u * q2 + q1 * v - b1 * r2 - r1 * b2;
+    out[4] = u * q3 + q1 * w - b1 * r3 - r1 * b3;
+    out[5] = v * q3 + q2 * w - b2 * r3 - r2 * b3;
+    out[6] = (q2 * b3 - q3 * b2) + (v * r3 - w * r2);
+    out[7] = (q3 * b1 - q1 * b3) + (w * r1 - u * r3);
+    out[8] = (q1 * b2 - q2 * b1) + (u * r2 - v * r1);
+  }
+};
+
+// N-grid epilogue: RHS = (plain MHD RHS, precomputed) + Ct t D PLQL, then the
+// RK stage update.
+template <typename T>
+struct EpiMHDT {
+  static constexpr int F_IN = 9;
+  __host__ double io_bytes(long long npts) const {
+    return io.bytes(npts, 6) + (double)sizeof(Cx<T>) * 6 * npts + (w0_out ? (double)sizeof(Cx<T>) * 6 * npts : 0.0);
+  }
+  StepIO<T> io;
+  KTabs<T> k;
+  const double *m1, *m2, *m3;
+  const Cx<T>* rhs6;  // plain MHD RHS (6 fields)
+  T coef;             // Ct t / 8 (2x-grid sums -> N-grid convention)
+  Cx<T>* w0_out;      // memory term (6 fields) or null
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = io.sidx(i1, i2, i3);
+    const T D = (T)(m1[i1] * m2[i2] * m3[i3]);
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    Cx<T> r[6];
+    mhd_nonlinear(k1, k2, k3, ksqi, P, r);
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+      const Cx<T> w0 = (coef * D) * r[f];
+      if (w0_out) w0_out[f * io.fstride + s] = w0;
+      io.finish(s, f, rhs6[f * io.fstride + s] + w0);
+    }
+  }
+};
+
 }  // namespace psb
 
 // ---- learned subgrid closure (no counterpart in the reference) -------------

@@ -539,6 +539,201 @@ int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
   return launch_epi<T>(c, e, epi, "PLQL x-forward+epilogue");
 }
 
+// ---------------------------------------------------------------------------
+// MHD t-model: plain MHD RHS (2/3 rule, N grid) + Ct t PLQL from two 2x-grid
+// stages.  Stage A: (u, B) -> nine products -> QL on the 2x grid.  Stage B:
+// (u, B) and QL -> nine linearised products -> PLQL on the N grid, fused with
+// the RK stage update.
+// ---------------------------------------------------------------------------
+template <typename T>
+int run_mhd_tmodel(psb_ctx* c, StepIO<T> io, const psb_params* p) {
+  const Cx<T>* Qin = io.Q;
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int F1 = 2 * N1, F2 = 2 * N2, F3 = 2 * N3, F3h = N3 + 1, Kz = c->kz_mhd;
+  const long long fsN = (long long)N1 * N2 * N3h, fsC = (long long)F1 * F2 * F3h;
+  int st = PSB_OK;
+  Cx<T>* R6 = scratch<T>(c, "mt.R6", (size_t)6 * fsN, &st);
+  Cx<T>* A2 = scratch<T>(c, "mt.A2", (size_t)6 * F1 * N2 * Kz, &st);
+  Cx<T>* B2 = scratch<T>(c, "mt.B2", (size_t)6 * F1 * F2 * Kz, &st);
+  Cx<T>* C2 = scratch<T>(c, "mt.C2", (size_t)9 * fsC, &st);  // products; later QL x-inverse, PLQL y-forward
+  Cx<T>* D2 = scratch<T>(c, "mt.D2", (size_t)9 * fsC, &st);  // products y-forward; later QL y-inverse
+  Cx<T>* E = scratch<T>(c, "mt.E", (size_t)6 * fsC, &st);    // QL; later the linearised products
+  if (st != PSB_OK) return st;
+  const double* m1 = c->mx;
+  const double* m2 = c->my;
+  const double* m3 = c->mz;
+  const T nu = (T)p->nu, eta = (T)(p->eta < 0 ? p->nu : p->eta);
+  StepIO<T> ior = io;
+  ior.mode = kRHS;
+  ior.rhs_out = R6;
+  ior.comp = nullptr;
+  ior.w0_out = nullptr;
+  EpiMHD<T> plain{ior, ktabs<T>(c->kx, c->ky, c->kz), m1, m2, m3, reinterpret_cast<const Cx<T>*>(p->force), nu,
+                  eta};
+  PSB_TRY(run_mhd<T>(c, Qin, plain));
+  if (!Qin) return PSB_OK;
+  const double fac = 1.0 / ((double)N1 * N2 * N3);
+  const double down = (double)N1 * N2 * N3 / ((double)F1 * F2 * F3);
+  // stage A: masked (u, B) onto the 2x grid
+  AxisArgs<T> a = axis_common<T>(c, F1);
+  a.in = Qin;
+  a.out = A2;
+  a.in_fstride = fsN;
+  a.in_ostride = N3h;
+  a.in_rstride = (long long)N2 * N3h;
+  a.out_fstride = (long long)F1 * N2 * Kz;
+  a.out_ostride = Kz;
+  a.out_rstride = (long long)N2 * Kz;
+  a.nouter = N2;
+  a.ncols = Kz;
+  a.in_rows = N1;
+  a.out_rows = F1;
+  a.in_map = map_pad2x(N1);
+  a.out_map = map_id(F1);
+  PSB_TRY((launch_axis<T, true>(c, a, PreMask6<T>{m1, m2, m3}, "mhd-t 2x x-inverse")));
+  AxisArgs<T> b = axis_common<T>(c, F2);
+  b.in = A2;
+  b.out = B2;
+  b.in_ostride = (long long)N2 * Kz;
+  b.in_rstride = Kz;
+  b.out_ostride = (long long)F2 * Kz;
+  b.out_rstride = Kz;
+  b.nouter = 6 * F1;
+  b.ncols = Kz;
+  b.in_rows = N2;
+  b.out_rows = F2;
+  b.in_map = map_pad2x(N2);
+  b.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "mhd-t 2x y-inverse")));
+  ZArgs<T> z{};
+  const long long fsB = (long long)F1 * F2 * Kz;
+  for (int f = 0; f < 6; ++f) {
+    z.in[f] = B2 + f * fsB;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+  }
+  for (int g = 0; g < 9; ++g) {
+    z.out[g] = C2 + g * fsC;
+    z.out_pstride[g] = F3h;
+  }
+  z.out_kz = F3h;
+  z.npencils = (long long)F1 * F2;
+  z.fac = (T)fac;
+  z.plan = *plan_for(c, F3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysMHD<T>{}, "mhd-t 2x z-products"));
+  AxisArgs<T> d = axis_common<T>(c, F2);
+  d.in = C2;
+  d.out = D2;
+  d.in_ostride = (long long)F2 * F3h;
+  d.in_rstride = F3h;
+  d.out_ostride = (long long)F2 * F3h;
+  d.out_rstride = F3h;
+  d.nouter = 9 * F1;
+  d.ncols = F3h;
+  d.in_rows = F2;
+  d.out_rows = F2;
+  d.in_map = map_id(F2);
+  d.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "mhd-t 2x y-forward")));
+  EpiMHDQ<T> eq{ktabs<T>(c->kxf, c->kyf, c->kzf), m1, m2, m3, N1, N2, N3h, F2, F3h, fsC, (T)down, E};
+  XEpiArgs<T> e{};
+  e.in = D2;
+  e.in_fstride = fsC;
+  e.in_rstride = (long long)F2 * F3h;
+  e.in_ostride = F3h;
+  e.n1 = F1;
+  e.n2 = F2;
+  e.n3h = F3h;
+  e.kz = F3h;
+  e.out_map = map_id(F1);
+  e.plan = *plan_for(c, F1);
+  e.tw = twiddles<T>(c);
+  PSB_TRY(launch_epi<T>(c, e, eq, "mhd-t 2x x-forward+QL"));
+  // stage B: QL back to physical space next to (u, B)
+  Cx<T>* A3 = C2;
+  Cx<T>* B3 = D2;
+  AxisArgs<T> a3 = axis_common<T>(c, F1);
+  a3.in = E;
+  a3.out = A3;
+  a3.in_fstride = fsC;
+  a3.in_ostride = F3h;
+  a3.in_rstride = (long long)F2 * F3h;
+  a3.out_fstride = fsC;
+  a3.out_ostride = F3h;
+  a3.out_rstride = (long long)F2 * F3h;
+  a3.nouter = F2;
+  a3.ncols = F3h;
+  a3.in_rows = F1;
+  a3.out_rows = F1;
+  a3.in_map = map_id(F1);
+  a3.out_map = map_id(F1);
+  PSB_TRY((launch_axis<T, true>(c, a3, PreCopyN<T, 6>{}, "mhd-t QL x-inverse")));
+  AxisArgs<T> b3 = axis_common<T>(c, F2);
+  b3.in = A3;
+  b3.out = B3;
+  b3.in_ostride = (long long)F2 * F3h;
+  b3.in_rstride = F3h;
+  b3.out_ostride = (long long)F2 * F3h;
+  b3.out_rstride = F3h;
+  b3.nouter = 6 * F1;
+  b3.ncols = F3h;
+  b3.in_rows = F2;
+  b3.out_rows = F2;
+  b3.in_map = map_id(F2);
+  b3.out_map = map_id(F2);
+  PSB_TRY((launch_axis<T, true>(c, b3, PreCopy<T>{}, "mhd-t QL y-inverse")));
+  Cx<T>* C3 = E;
+  Cx<T>* D3 = C2;
+  ZArgs<T> z3{};
+  for (int f = 0; f < 6; ++f) {
+    z3.in[f] = B2 + f * fsB;
+    z3.in_pstride[f] = Kz;
+    z3.in_kz[f] = Kz;
+    z3.in[6 + f] = B3 + f * fsC;
+    z3.in_pstride[6 + f] = F3h;
+    z3.in_kz[6 + f] = F3h;
+  }
+  for (int g = 0; g < 9; ++g) {
+    z3.out[g] = C3 + g * fsB;
+    z3.out_pstride[g] = Kz;
+  }
+  z3.out_kz = Kz;
+  z3.npencils = (long long)F1 * F2;
+  z3.fac = (T)fac;
+  z3.plan = *plan_for(c, F3);
+  z3.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z3, PhysMHDLin<T>{}, "mhd-t PLQL z-products"));
+  AxisArgs<T> d3 = axis_common<T>(c, F2);
+  d3.in = C3;
+  d3.out = D3;
+  d3.in_ostride = (long long)F2 * Kz;
+  d3.in_rstride = Kz;
+  d3.out_ostride = (long long)N2 * Kz;
+  d3.out_rstride = Kz;
+  d3.nouter = 9 * F1;
+  d3.ncols = Kz;
+  d3.in_rows = F2;
+  d3.out_rows = N2;
+  d3.in_map = map_id(F2);
+  d3.out_map = map_pad2x(N2);
+  PSB_TRY((launch_axis<T, false>(c, d3, PreCopy<T>{}, "mhd-t PLQL y-forward")));
+  EpiMHDT<T> et{io, ktabs<T>(c->kx, c->ky, c->kz), m1, m2, m3, R6, (T)(p->Ct * p->t * down), io.w0_out};
+  XEpiArgs<T> e3{};
+  e3.in = D3;
+  e3.in_fstride = (long long)F1 * N2 * Kz;
+  e3.in_rstride = (long long)N2 * Kz;
+  e3.in_ostride = Kz;
+  e3.n1 = N1;
+  e3.n2 = N2;
+  e3.n3h = N3h;
+  e3.kz = Kz;
+  e3.out_map = map_pad2x(N1);
+  e3.plan = *plan_for(c, F1);
+  e3.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e3, et, "mhd-t PLQL x-forward+epilogue");
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -592,6 +787,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
                     reinterpret_cast<const Cx<T>*>(p->force), (T)p->nu, (T)(p->eta < 0 ? p->nu : p->eta)};
       return run_mhd<T>(c, Qin, epi);
     }
+    case PSB_MHD_TMODEL:
+      return run_mhd_tmodel<T>(c, io, p);
     case PSB_TMODEL:
     case PSB_TAU_STATIC: {
       int st = PSB_OK;

@@ -26,6 +26,13 @@ def _rdtype(p):
     return torch.float64 if p == 64 else torch.float32
 
 
+def _on(a, dev, dtype):
+    """Host array or tensor -> tensor of `dtype` on `dev`."""
+    if isinstance(a, torch.Tensor):
+        return a.to(device=dev, dtype=dtype)
+    return torch.as_tensor(np.asarray(a), device=dev).to(dtype)
+
+
 class gridclass:
     def __init__(self, N1, N2, N3, x, y, z, kc, num_processes=1, L1=TWO_PI, L2=TWO_PI, L3=TWO_PI, mpi_rank=0,
                  comm=None, turb_model="MHD", device=0):
@@ -93,11 +100,15 @@ class variables:
 
     def __init__(self, turb_model, rotate, Om1, Om2, Om3, grid, u, v, w, B1, B2, B3, uhat=None, vhat=None,
                  what=None, t=0.0, dt=0.0, nu=0.0, myFFT=None, mpi_rank=0, initDomain="Physical",
-                 time_scheme="RK4", precision=64, kahan=None, Bhat=None, forcing=True):
+                 time_scheme="RK4", precision=64, kahan=None, Bhat=None, forcing=True, closure=None, Ct=0.1):
         if turb_model != "MHD":
             raise ValueError("only turb_model='MHD' of the MPI solver is on this path")
         if time_scheme != "RK4":
             raise ValueError("Error, time scheme " + str(time_scheme) + " not implemented for MHD equations")
+        if closure not in (None, "tmodel"):
+            raise ValueError("closure must be None (plain MHD) or 'tmodel'")
+        self.closure = closure
+        self.Ct = float(Ct)
         self.turb_model, self.rotate = turb_model, int(rotate)
         self.t, self.dt, self.nu = float(t), float(dt), float(nu)
         self.lam = self.nu
@@ -109,13 +120,11 @@ class variables:
         sh = (N1, N2, N3 // 2 + 1)
         self.Q = torch.zeros((6,) + sh, dtype=_cdtype(precision), device=dev)
         if initDomain == "Physical":
-            phys = torch.stack([torch.as_tensor(np.asarray(a), device=dev).to(_rdtype(precision))
-                                for a in (u, v, w, B1, B2, B3)]).contiguous()
+            phys = torch.stack([_on(a, dev, _rdtype(precision)) for a in (u, v, w, B1, B2, B3)]).contiguous()
             ctx.r2c(phys, self.Q, 6)
         else:
-            src = torch.stack([torch.as_tensor(np.asarray(a), device=dev).to(_cdtype(precision))
-                               for a in (uhat, vhat, what)] +
-                              [torch.as_tensor(np.asarray(a), device=dev).to(_cdtype(precision)) for a in Bhat])
+            src = torch.stack([_on(a, dev, _cdtype(precision)) for a in (uhat, vhat, what)] +
+                              [_on(a, dev, _cdtype(precision)) for a in Bhat])
             phys = torch.empty((6, N1, N2, N3), dtype=_rdtype(precision), device=dev)
             ctx.c2r(src.contiguous(), phys, 6)
             ctx.r2c(phys, self.Q, 6)
@@ -167,10 +176,10 @@ class variables:
         self.U.copy_(self.Q)
 
     def closure_code(self):
-        return _capi.MHD
+        return _capi.MHD_TMODEL if self.closure == "tmodel" else _capi.MHD
 
     def params(self):
-        return _capi.make_params(nu=self.nu, eta=self.lam, t=self.t, dt=self.dt,
+        return _capi.make_params(nu=self.nu, eta=self.lam, t=self.t, dt=self.dt, Ct=self.Ct,
                                  force=self.force.data_ptr() if self.force is not None else None)
 
 
@@ -179,17 +188,18 @@ def computeRHS_MHD(main, grid, myFFT=None):
     six stored fields are dealiased in place, as in the reference."""
     ctx = grid.ctx(main.precision)
     rhs = torch.empty_like(main.Q)
-    ctx.rhs(_capi.MHD, main.Q, rhs, main.params(), read_out=main.U)
+    ctx.rhs(main.closure_code(), main.Q, rhs, main.params(), read_out=main.U)
     main.Q = rhs
 
 
 def advanceQ_RK4(main, grid, myFFT=None):
     """src_MPI/time_schemes.py:2-7."""
-    grid.ctx(main.precision).step(_capi.MHD, main.Q, main.params(), 1, comp=main.comp, read_out=main.U)
+    grid.ctx(main.precision).step(main.closure_code(), main.Q, main.params(), 1, comp=main.comp, read_out=main.U)
 
 
 def advance(main, grid, nsteps):
-    grid.ctx(main.precision).step(_capi.MHD, main.Q, main.params(), int(nsteps), comp=main.comp, read_out=main.U)
+    grid.ctx(main.precision).step(main.closure_code(), main.Q, main.params(), int(nsteps), comp=main.comp,
+                                  read_out=main.U)
 
 
 class utilitiesClass:
