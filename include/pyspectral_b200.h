@@ -195,6 +195,30 @@ int psb_timing_count(psb_ctx* ctx, int* n);
 /* Record i: kernel name, device time (ms) and compulsory HBM bytes of the launch. */
 int psb_timing_get(psb_ctx* ctx, int i, char* name, int name_len, double* ms, double* bytes);
 
+/* ---- batched ensembles (no reference counterpart: the reference advances one
+ *      run per process, src/PySpec_3d.py:96-144) ------------------------------
+ * nruns independent runs on ctx's grid and precision with one closure (PSB_DNS,
+ * PSB_SMAG or PSB_LEARNED), each with its own state, Kahan compensation and
+ * parameters (nu, dt, rotation, MLP).  Every pass of an RK4 stage is one launch
+ * over all runs.  The batch owns its scratch; states stay caller-owned.  Calls
+ * go to ctx's stream and may be captured into a CUDA graph once the batch has
+ * stepped (or been tuned) outside the capture. */
+typedef struct psb_batch psb_batch;
+int psb_batch_create(psb_ctx* ctx, int closure, int nruns, psb_batch** out);
+/* Run r: state (3 fields), comp (Kahan compensation, 3 fields, or NULL), params. */
+int psb_batch_set_run(psb_batch* b, int r, void* state, void* comp, const psb_params* p);
+/* Time the candidate launch shapes (column tiles, pencils per CTA, radix
+ * orders) of every pass on the batch's data and keep the fastest; states are
+ * not modified. */
+int psb_batch_autotune(psb_batch* b);
+/* nsteps RK4 steps of every run (src/PySpec_3d.py:96-105 per run). */
+int psb_batch_step_rk4(psb_batch* b, int nsteps);
+/* Launch shape of pass 0..4 (x-inverse, y-inverse, z, y-forward, x-forward):
+ * tile (columns per CTA, or pencils per CTA for the z pass) and the radix
+ * order of its transform (maxr entries, 0-terminated). */
+int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int maxr);
+int psb_batch_destroy(psb_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,566 @@
+// Batched ensembles: many independent runs of one grid size, precision and
+// closure advanced together, every pass of the RK4 step one launch over all
+// runs (the run index is a grid dimension; each run reads its own argument
+// block from device memory).  No counterpart in the reference, which advances
+// one run per process (PySpectral/src/PySpec_3d.py:96-144).
+//
+// Launch shapes are chosen by an autotuner: for every pass it times the
+// candidate column tiles (x/y passes), pencils per CTA (z-pass) and radix
+// orders of the transform length on the batch's own data, and keeps the
+// fastest.  Timing runs the passes in RHS mode into scratch, so tuning leaves
+// the runs' states untouched.
+#include <algorithm>
+#include <array>
+#include <cstring>
+
+#include "psb_ctx.cuh"
+
+using namespace psb;
+using namespace psbh;
+
+struct psb_batch {
+  psb_ctx* c = nullptr;
+  int closure = 0;
+  int nruns = 0;
+  std::vector<void*> state, comp;
+  std::vector<psb_params> params;
+  void* arena = nullptr;  // per-run scratch: A, B, C, D, Q0, RHS (tuning)
+  size_t arena_bytes = 0;
+  void* dargs = nullptr;  // device argument blocks
+  size_t dargs_bytes = 0;
+  bool dirty = true;
+  // launch shape per pass: 0 x-inverse, 1 y-inverse, 2 z, 3 y-forward, 4 x-forward
+  std::array<int, 5> tile{{0, 0, 0, 0, 0}};
+  std::array<FFTPlan, 5> plan{};
+  bool tuned = false;
+  std::vector<char> host;  // staging of the argument blocks
+};
+
+namespace {
+
+template <typename T>
+KTabs<T> ktab(const double* a, const double* b, const double* c) {
+  KTabs<T> k;
+  k.k1 = a;
+  k.k2 = b;
+  k.k3 = c;
+  return k;
+}
+
+// Sizes of one run's buffers (complex elements).
+struct Dims {
+  int N1, N2, N3, N3h, M1, M2, M3, Kz;
+  long long nA, nB, nC, nD, nQ;
+};
+Dims dims(const psb_ctx* c, int Fi, int Fo) {
+  Dims d;
+  d.N1 = c->N1;
+  d.N2 = c->N2;
+  d.N3 = c->N3;
+  d.N3h = c->N3h;
+  d.M1 = 3 * d.N1 / 2;
+  d.M2 = 3 * d.N2 / 2;
+  d.M3 = 3 * d.N3 / 2;
+  d.Kz = d.N3 / 2;
+  d.nA = (long long)Fi * d.M1 * d.N2 * d.Kz;
+  d.nB = (long long)Fi * d.M1 * d.M2 * d.Kz;
+  d.nC = (long long)Fo * d.M1 * d.M2 * d.Kz;
+  d.nD = (long long)Fo * d.M1 * d.N2 * d.Kz;
+  d.nQ = 3LL * d.N1 * d.N2 * d.N3h;
+  return d;
+}
+long long al(long long n) { return (n + 63) / 64 * 64; }
+
+// Every radix order of a length's factors (distinct permutations).
+std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
+  std::vector<int> r(p.radix, p.radix + p.npass);
+  std::sort(r.begin(), r.end());
+  std::vector<FFTPlan> out;
+  do {
+    FFTPlan q = p;
+    for (int s = 0; s < p.npass; ++s) q.radix[s] = r[s];
+    out.push_back(q);
+  } while (std::next_permutation(r.begin(), r.end()) && out.size() < 24);
+  return out;
+}
+
+template <typename T, class Pre, class Phys, class Epi>
+struct Batch {
+  static constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
+  psb_batch* b;
+  psb_ctx* c;
+  Dims d;
+  int R;
+  // device views
+  AxisArgs<T>*ax, *ay, *ayf;
+  ZArgs<T>* az;
+  XEpiArgs<T>* ae;
+  Pre* pre;
+  PreCopy<T>* cpy;
+  Phys* phys;
+  Epi* epi;  // [5][R]: stages 0..3, then RHS mode into scratch (tuning)
+
+  static size_t arg_bytes(int R) {
+    return al(sizeof(AxisArgs<T>) * R) * 3 + al(sizeof(ZArgs<T>) * R) + al(sizeof(XEpiArgs<T>) * R) +
+           al(sizeof(Pre) * R) + al(sizeof(PreCopy<T>) * R) + al(sizeof(Phys) * R) + al(sizeof(Epi) * R * 5);
+  }
+  static size_t run_bytes(const Dims& d) { return sizeof(Cx<T>) * (al(d.nA) + al(d.nB) + al(d.nC) + al(d.nD) + 2 * al(d.nQ)); }
+
+  Cx<T>* run_buf(int r, int which) const {
+    Cx<T>* base = reinterpret_cast<Cx<T>*>(reinterpret_cast<char*>(b->arena) + (size_t)r * run_bytes(d));
+    const long long off[6] = {0, al(d.nA), al(d.nA) + al(d.nB), al(d.nA) + al(d.nB) + al(d.nC),
+                              al(d.nA) + al(d.nB) + al(d.nC) + al(d.nD),
+                              al(d.nA) + al(d.nB) + al(d.nC) + al(d.nD) + al(d.nQ)};
+    return base + off[which];
+  }
+
+  void views(char* base) {
+    char* p = base;
+    auto take = [&](size_t n) {
+      char* q = p;
+      p += al(n);
+      return q;
+    };
+    ax = reinterpret_cast<AxisArgs<T>*>(take(sizeof(AxisArgs<T>) * R));
+    ay = reinterpret_cast<AxisArgs<T>*>(take(sizeof(AxisArgs<T>) * R));
+    ayf = reinterpret_cast<AxisArgs<T>*>(take(sizeof(AxisArgs<T>) * R));
+    az = reinterpret_cast<ZArgs<T>*>(take(sizeof(ZArgs<T>) * R));
+    ae = reinterpret_cast<XEpiArgs<T>*>(take(sizeof(XEpiArgs<T>) * R));
+    pre = reinterpret_cast<Pre*>(take(sizeof(Pre) * R));
+    cpy = reinterpret_cast<PreCopy<T>*>(take(sizeof(PreCopy<T>) * R));
+    phys = reinterpret_cast<Phys*>(take(sizeof(Phys) * R));
+    epi = reinterpret_cast<Epi*>(take(sizeof(Epi) * R * 5));
+  }
+
+  // Argument blocks of every run (host copy, then one upload).
+  int build(const Pre& pre0, Phys (*mkphys)(psb_ctx*, const psb_params&),
+            Epi (*mkepi)(psb_ctx*, StepIO<T>, const psb_params&)) {
+    const size_t ab = arg_bytes(R);
+    b->host.assign(ab, 0);
+    views(b->host.data());
+    const long long fsN = (long long)d.N1 * d.N2 * d.N3h;
+    const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)d.N1 * d.N2 * d.N3));
+    const double rk[4] = {1. / 4, 1. / 3, 1. / 2, 1.};
+    for (int r = 0; r < R; ++r) {
+      const Cx<T>* Q = reinterpret_cast<const Cx<T>*>(b->state[r]);
+      Cx<T>*A = run_buf(r, 0), *B = run_buf(r, 1), *C = run_buf(r, 2), *D = run_buf(r, 3);
+      AxisArgs<T> a{};
+      a.plan = b->plan[0];
+      a.tw = twiddles<T>(c);
+      a.scale = (T)1;
+      a.in = Q;
+      a.out = A;
+      a.in_fstride = fsN;
+      a.in_ostride = d.N3h;
+      a.in_rstride = (long long)d.N2 * d.N3h;
+      a.out_fstride = (long long)d.M1 * d.N2 * d.Kz;
+      a.out_ostride = d.Kz;
+      a.out_rstride = (long long)d.N2 * d.Kz;
+      a.nouter = d.N2;
+      a.ncols = d.Kz;
+      a.col_tile = b->tile[0];
+      a.in_rows = d.N1;
+      a.out_rows = d.M1;
+      a.in_map = map_pad32(d.N1);
+      a.out_map = map_id(d.M1);
+      a.k_row = c->kx;
+      a.k_outer = c->ky;
+      a.k_col = c->kz;
+      ax[r] = a;
+      AxisArgs<T> y{};
+      y.plan = b->plan[1];
+      y.tw = twiddles<T>(c);
+      y.scale = (T)1;
+      y.in = A;
+      y.out = B;
+      y.in_ostride = (long long)d.N2 * d.Kz;
+      y.in_rstride = d.Kz;
+      y.out_ostride = (long long)d.M2 * d.Kz;
+      y.out_rstride = d.Kz;
+      y.nouter = Fi * d.M1;
+      y.ncols = d.Kz;
+      y.col_tile = b->tile[1];
+      y.in_rows = d.N2;
+      y.out_rows = d.M2;
+      y.in_map = map_pad32(d.N2);
+      y.out_map = map_id(d.M2);
+      ay[r] = y;
+      ZArgs<T> z{};
+      const long long fsP = (long long)d.M1 * d.M2 * d.Kz;
+      for (int f = 0; f < Fi; ++f) {
+        z.in[f] = B + f * fsP;
+        z.in_pstride[f] = d.Kz;
+        z.in_kz[f] = d.Kz;
+      }
+      for (int g = 0; g < Fo; ++g) {
+        z.out[g] = C + g * fsP;
+        z.out_pstride[g] = d.Kz;
+      }
+      z.out_kz = d.Kz;
+      z.npencils = (long long)d.M1 * d.M2;
+      z.ppc = b->tile[2];
+      z.fac = (T)(s32 / ((double)d.M1 * d.M2 * d.M3));
+      z.plan = b->plan[2];
+      z.tw = twiddles<T>(c);
+      az[r] = z;
+      AxisArgs<T> yf{};
+      yf.plan = b->plan[3];
+      yf.tw = twiddles<T>(c);
+      yf.scale = (T)1;
+      yf.in = C;
+      yf.out = D;
+      yf.in_ostride = (long long)d.M2 * d.Kz;
+      yf.in_rstride = d.Kz;
+      yf.out_ostride = (long long)d.N2 * d.Kz;
+      yf.out_rstride = d.Kz;
+      yf.nouter = Fo * d.M1;
+      yf.ncols = d.Kz;
+      yf.col_tile = b->tile[3];
+      yf.in_rows = d.M2;
+      yf.out_rows = d.N2;
+      yf.in_map = map_id(d.M2);
+      yf.out_map = map_pad32(d.N2);
+      ayf[r] = yf;
+      XEpiArgs<T> e{};
+      e.in = D;
+      e.in_fstride = (long long)d.M1 * d.N2 * d.Kz;
+      e.in_rstride = (long long)d.N2 * d.Kz;
+      e.in_ostride = d.Kz;
+      e.n1 = d.N1;
+      e.n2 = d.N2;
+      e.n3h = d.N3h;
+      e.kz = d.Kz;
+      e.col_tile = b->tile[4];
+      e.out_map = map_pad32(d.N1);
+      e.main_blocks = ((d.Kz + e.col_tile - 1) / e.col_tile) * d.N2;
+      e.plan = b->plan[4];
+      e.tw = twiddles<T>(c);
+      ae[r] = e;
+      pre[r] = pre0;
+      cpy[r] = PreCopy<T>{};
+      phys[r] = mkphys(c, b->params[r]);
+      for (int i = 0; i < 5; ++i) {
+        StepIO<T> io{};
+        io.Q = reinterpret_cast<Cx<T>*>(b->state[r]);
+        io.Q0 = run_buf(r, 4);
+        io.comp = reinterpret_cast<Cx<T>*>(b->comp[r]);
+        io.fstride = fsN;
+        io.n2 = d.N2;
+        io.n3h = d.N3h;
+        if (i < 4) {
+          io.mode = i == 0 ? kStage1 : (i == 3 ? kStageLast : kStageMid);
+          io.dtc = (T)(b->params[r].dt * rk[i]);
+        } else {
+          io.mode = kRHS;
+          io.rhs_out = run_buf(r, 5);
+          io.comp = nullptr;
+        }
+        epi[i * R + r] = mkepi(c, io, b->params[r]);
+      }
+    }
+    if (b->dargs_bytes < ab) {
+      if (b->dargs) cudaFree(b->dargs);
+      b->dargs = nullptr;
+      b->dargs_bytes = 0;
+      PSB_TRY(cuda_ok(c, cudaMalloc(&b->dargs, ab), "batch arguments"));
+      b->dargs_bytes = ab;
+    }
+    PSB_TRY(cuda_ok(c, cudaMemcpy(b->dargs, b->host.data(), ab, cudaMemcpyHostToDevice), "batch arguments upload"));
+    views(reinterpret_cast<char*>(b->dargs));
+    return PSB_OK;
+  }
+
+  // ---- launches -----------------------------------------------------------
+  size_t smem_axis(int L, int F, int ct) const { return (size_t)(L + 2 * L * F * ct) * sizeof(Cx<T>); }
+  size_t smem_z(int P) const {
+    constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
+    return zpass_smem_bytes<T>(FMAX, P, d.M3, (size_t)phys_is_block<Phys>::extra);
+  }
+  int launch(int pass, int stage) {
+    const size_t esz = sizeof(Cx<T>);
+    switch (pass) {
+      case 0: {
+        const int ct = b->tile[0];
+        dim3 g((d.Kz + ct - 1) / ct, d.N2, R);
+        const size_t sm = smem_axis(d.M1, Fi, ct);
+        auto k = axis_pass_batch<T, true, Pre>;
+        set_smem(k, sm);
+        LaunchScope s(c, "batch x-inverse", (double)R * esz * d.N2 * d.Kz * (3.0 * d.N1 + (double)Fi * d.M1));
+        k<<<g, 256, sm, c->stream>>>(ax, pre);
+        return launch_ok(c, "batch x-inverse");
+      }
+      case 1:
+      case 3: {
+        const bool inv = pass == 1;
+        const int ct = b->tile[pass];
+        const int F = inv ? Fi : Fo;
+        dim3 g((d.Kz + ct - 1) / ct, F * d.M1, R);
+        const size_t sm = smem_axis(d.M2, 1, ct);
+        const double by = (double)R * esz * F * d.M1 * d.Kz * (double)(d.N2 + d.M2);
+        if (inv) {
+          auto k = axis_pass_batch<T, true, PreCopy<T>>;
+          set_smem(k, sm);
+          LaunchScope s(c, "batch y-inverse", by);
+          k<<<g, 256, sm, c->stream>>>(ay, cpy);
+        } else {
+          auto k = axis_pass_batch<T, false, PreCopy<T>>;
+          set_smem(k, sm);
+          LaunchScope s(c, "batch y-forward", by);
+          k<<<g, 256, sm, c->stream>>>(ayf, cpy);
+        }
+        return launch_ok(c, inv ? "batch y-inverse" : "batch y-forward");
+      }
+      case 2: {
+        const int P = b->tile[2];
+        const long long np = (long long)d.M1 * d.M2;
+        dim3 g((unsigned)((np + P - 1) / P), R);
+        const size_t sm = smem_z(P);
+        auto k = zpass_batch<T, Phys>;
+        set_smem(k, sm);
+        LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fi + Fo));
+        k<<<g, 256, sm, c->stream>>>(az, phys);
+        return launch_ok(c, "batch z-fused");
+      }
+      default: {
+        const int ct = b->tile[4];
+        const int ntile = (d.Kz + ct - 1) / ct;
+        const int mainb = ntile * d.N2;
+        const long long pts = (long long)d.N1 * d.N2 * (d.N3h - d.Kz);
+        const int extra = (int)std::min<long long>((pts + 255) / 256, 1024);
+        dim3 g(mainb + extra, R);
+        const size_t sm = smem_axis(d.M1, Fo, ct);
+        auto k = xfwd_epi_batch<T, Epi>;
+        set_smem(k, sm);
+        const double by = (double)R * (esz * Fo * d.M1 * d.N2 * d.Kz + esz * 3.0 * d.N1 * d.N2 * d.N3h *
+                                                                           (stage == 4 ? 2.0 : 3.0));
+        LaunchScope s(c, "batch x-forward+epilogue", by);
+        k<<<g, 256, sm, c->stream>>>(ae, epi + (size_t)stage * R);
+        return launch_ok(c, "batch x-forward+epilogue");
+      }
+    }
+  }
+
+  int step(int nsteps) {
+    for (int s = 0; s < nsteps; ++s)
+      for (int i = 0; i < 4; ++i)
+        for (int pass = 0; pass < 5; ++pass) PSB_TRY(launch(pass, i));
+    return PSB_OK;
+  }
+
+  // ---- autotuning -----------------------------------------------------------
+  // Mean time of `reps` launches of one pass (RHS-mode epilogue), ms.
+  int time_pass(int pass, int reps, float* ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = launch(pass, 4);  // warm-up (and shape check)
+    if (st == PSB_OK) {
+      cudaEventRecord(e0, c->stream);
+      for (int k = 0; k < reps && st == PSB_OK; ++k) st = launch(pass, 4);
+      cudaEventRecord(e1, c->stream);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(ms, e0, e1);
+      *ms /= reps;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+  }
+
+  int autotune(const Pre& pre0, Phys (*mkphys)(psb_ctx*, const psb_params&),
+               Epi (*mkepi)(psb_ctx*, StepIO<T>, const psb_params&)) {
+    const size_t esz = sizeof(Cx<T>);
+    const int Ls[5] = {d.M1, d.M2, d.M3, d.M2, d.M1};
+    const int Fs[5] = {Fi, 1, 0, 1, Fo};
+    // RHS-mode passes read the runs' states and write only scratch; run one
+    // full RHS first so that every intermediate buffer holds real data.
+    for (int pass = 0; pass < 5; ++pass) PSB_TRY(launch(pass, 4));
+    for (int pass = 0; pass < 5; ++pass) {
+      std::vector<int> tiles;
+      if (pass == 2) {
+        for (int P : {1, 2, 4, 8})
+          if (P <= phys_max_ppc<Phys>::value && smem_z(P) <= kSmemBudget) tiles.push_back(P);
+      } else {
+        for (int ct : {2, 4, 8, 16, 32})
+          if (ct <= std::max(2, 2 * d.Kz) && smem_axis(Ls[pass], Fs[pass], ct) <= kSmemBudget) tiles.push_back(ct);
+      }
+      const std::vector<FFTPlan> orders = radix_orders(*plan_for(c, Ls[pass]));
+      float best = 1e30f;
+      int bt = b->tile[pass];
+      FFTPlan bp = b->plan[pass];
+      for (int t : tiles)
+        for (const FFTPlan& q : orders) {
+          b->tile[pass] = t;
+          b->plan[pass] = q;
+          PSB_TRY(build(pre0, mkphys, mkepi));
+          float ms = 0;
+          PSB_TRY(time_pass(pass, 3, &ms));
+          if (ms < best) {
+            best = ms;
+            bt = t;
+            bp = q;
+          }
+        }
+      b->tile[pass] = bt;
+      b->plan[pass] = bp;
+      PSB_TRY(build(pre0, mkphys, mkepi));
+    }
+    (void)esz;
+    b->tuned = true;
+    return PSB_OK;
+  }
+};
+
+// per-closure functor makers
+template <typename T>
+PhysProducts<T> mk_products(psb_ctx*, const psb_params&) {
+  return PhysProducts<T>{};
+}
+template <typename T>
+PhysSmag<T> mk_smag(psb_ctx* c, const psb_params&) {
+  return PhysSmag<T>{(T)(0.16 * c->Delta * 0.16 * c->Delta)};
+}
+template <typename T>
+PhysLearned<T> mk_learned(psb_ctx* c, const psb_params& p) {
+  const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
+  return PhysLearned<T>{reinterpret_cast<const float*>(p.mlp_params), reinterpret_cast<const float*>(p.mlp_norm),
+                        (T)s32, (float)(p.les_delta > 0 ? p.les_delta : c->Delta)};
+}
+template <typename T, bool SMAG>
+EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
+  return EpiNS<T, SMAG>{io, ktab<T>(c->kx, c->ky, c->kz), (T)p.nu, p.rotate, (T)p.Om1, (T)p.Om2, (T)p.Om3,
+                        SMAG ? 0 : 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
+}
+
+// Default launch shapes: the single-run rules of the library.
+void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int max_ppc, size_t zextra) {
+  psb_ctx* c = b->c;
+  const Dims d = dims(c, Fi, Fo);
+  b->tile[0] = pick_ct(d.Kz, Fi, d.M1, esz, d.N2);
+  b->tile[1] = pick_ct(d.Kz, 1, d.M2, esz, Fi * d.M1);
+  b->tile[3] = pick_ct(d.Kz, 1, d.M2, esz, Fo * d.M1);
+  b->tile[4] = pick_ct(d.Kz, Fo, d.M1, esz, d.N2);
+  const int FMAX = std::max(Fi, Fo);
+  int P = max_ppc;
+  auto sm = [&](int P) { return (size_t)(d.M3 + 2 * (size_t)((FMAX * P + 1) / 2) * d.M3) * esz + zextra; };
+  while (P > 1 && sm(P) > kSmemBudget) P /= 2;
+  b->tile[2] = P;
+  b->plan[0] = *plan_for(c, d.M1);
+  b->plan[1] = *plan_for(c, d.M2);
+  b->plan[2] = *plan_for(c, d.M3);
+  b->plan[3] = *plan_for(c, d.M2);
+  b->plan[4] = *plan_for(c, d.M1);
+}
+
+template <typename T, class Pre, class Phys, class Epi>
+int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_ctx*, const psb_params&),
+              Epi (*mkepi)(psb_ctx*, StepIO<T>, const psb_params&)) {
+  psb_ctx* c = b->c;
+  using BT = Batch<T, Pre, Phys, Epi>;
+  BT x;
+  x.b = b;
+  x.c = c;
+  x.d = dims(c, BT::Fi, BT::Fo);
+  x.R = b->nruns;
+  const size_t need = BT::run_bytes(x.d) * (size_t)b->nruns;
+  if (b->arena_bytes < need) {
+    if (b->arena) cudaFree(b->arena);
+    b->arena = nullptr;
+    b->arena_bytes = 0;
+    PSB_TRY(cuda_ok(c, cudaMalloc(&b->arena, need), "batch scratch"));
+    b->arena_bytes = need;
+  }
+  if (b->plan[0].L == 0)
+    default_shapes(b, BT::Fi, BT::Fo, sizeof(Cx<T>), phys_max_ppc<Phys>::value, (size_t)phys_is_block<Phys>::extra);
+  if (b->dirty) {
+    PSB_TRY(x.build(pre0, mkphys, mkepi));
+    b->dirty = false;
+  } else {
+    x.views(reinterpret_cast<char*>(b->dargs));
+  }
+  if (tune) return x.autotune(pre0, mkphys, mkepi);
+  return x.step(nsteps);
+}
+
+template <typename T>
+int dispatch(psb_batch* b, int nsteps, bool tune) {
+  switch (b->closure) {
+    case PSB_DNS:
+      return run_batch<T>(b, nsteps, tune, PreCopyN<T, 3>{}, &mk_products<T>, &mk_epi<T, false>);
+    case PSB_SMAG:
+      return run_batch<T>(b, nsteps, tune, PreStrain<T>{}, &mk_smag<T>, &mk_epi<T, true>);
+    case PSB_LEARNED:
+      return run_batch<T>(b, nsteps, tune, PreGrad<T>{}, &mk_learned<T>, &mk_epi<T, false>);
+    default:
+      return fail(b->c, PSB_ERR_UNSUPPORTED, "psb_batch: closure not batched (DNS, SMAG, LEARNED are)");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int psb_batch_create(psb_ctx* c, int closure, int nruns, psb_batch** out) {
+  if (!c || !out) return PSB_ERR_ARG;
+  *out = nullptr;
+  if (nruns <= 0 || nruns > 65535) return fail(c, PSB_ERR_ARG, "psb_batch_create: nruns must be in 1..65535");
+  if (closure != PSB_DNS && closure != PSB_SMAG && closure != PSB_LEARNED)
+    return fail(c, PSB_ERR_UNSUPPORTED, "psb_batch_create: closure not batched (DNS, SMAG, LEARNED are)");
+  psb_batch* b = new psb_batch();
+  b->c = c;
+  b->closure = closure;
+  b->nruns = nruns;
+  b->state.assign(nruns, nullptr);
+  b->comp.assign(nruns, nullptr);
+  b->params.assign(nruns, psb_params{});
+  *out = b;
+  return PSB_OK;
+}
+
+int psb_batch_set_run(psb_batch* b, int r, void* state, void* comp, const psb_params* p) {
+  if (!b) return PSB_ERR_ARG;
+  if (r < 0 || r >= b->nruns || !state || !p) return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: bad argument");
+  if (b->closure == PSB_LEARNED && (!p->mlp_params || !p->mlp_norm))
+    return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: PSB_LEARNED needs mlp_params and mlp_norm");
+  b->state[r] = state;
+  b->comp[r] = comp;
+  b->params[r] = *p;
+  b->dirty = true;
+  return PSB_OK;
+}
+
+int psb_batch_autotune(psb_batch* b) {
+  if (!b) return PSB_ERR_ARG;
+  for (int r = 0; r < b->nruns; ++r)
+    if (!b->state[r]) return fail(b->c, PSB_ERR_ARG, "psb_batch_autotune: run without state");
+  PSB_TRY(cuda_ok(b->c, cudaSetDevice(b->c->dev), "cudaSetDevice"));
+  return b->c->prec == 64 ? dispatch<double>(b, 0, true) : dispatch<float>(b, 0, true);
+}
+
+int psb_batch_step_rk4(psb_batch* b, int nsteps) {
+  if (!b) return PSB_ERR_ARG;
+  if (nsteps < 0) return fail(b->c, PSB_ERR_ARG, "psb_batch_step_rk4: nsteps < 0");
+  for (int r = 0; r < b->nruns; ++r)
+    if (!b->state[r]) return fail(b->c, PSB_ERR_ARG, "psb_batch_step_rk4: run without state");
+  PSB_TRY(cuda_ok(b->c, cudaSetDevice(b->c->dev), "cudaSetDevice"));
+  return b->c->prec == 64 ? dispatch<double>(b, nsteps, false) : dispatch<float>(b, nsteps, false);
+}
+
+int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int maxr) {
+  if (!b || pass < 0 || pass > 4 || !tile) return PSB_ERR_ARG;
+  *tile = b->tile[pass];
+  const FFTPlan& p = b->plan[pass];
+  for (int s = 0; s < maxr; ++s) radices[s] = s < p.npass ? p.radix[s] : 0;
+  return PSB_OK;
+}
+
+int psb_batch_destroy(psb_batch* b) {
+  if (!b) return PSB_ERR_ARG;
+  cudaSetDevice(b->c->dev);
+  if (b->arena) cudaFree(b->arena);
+  if (b->dargs) cudaFree(b->dargs);
+  delete b;
+  return PSB_OK;
+}
+
+}  // extern "C"

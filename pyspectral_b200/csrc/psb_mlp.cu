@@ -259,8 +259,8 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
                                                           const float* __restrict__ X, int B,
                                                           float* __restrict__ Y) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MlpSmem& s = *reinterpret_cast<MlpSmem*>(smem_raw);
-  mlp_stage(s, P, nrm);
+  MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
+  mlp_stage_fwd(s, P, nrm);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int nw = blockDim.x >> 5;
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
       return r0 + r < B ? X[(long long)(r0 + r) * kMlpIn + f] : s.xmean[f];
     });
     float y[4];
-    mlp_forward_warp(s, xa, y, nullptr, nullptr);
+    mlp_forward_fast(s, xa, y);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int c = 2 * t + (e & 1), r = r0 + g + (e < 2 ? 0 : 8);
@@ -295,7 +295,7 @@ int psb_mlp_forward(psb_ctx* c, const float* params, const float* norm, const fl
   if (!params || !norm || !X || !Y || B < 0) return fail(c, PSB_ERR_ARG, "psb_mlp_forward: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   if (B == 0) return PSB_OK;
-  const size_t smem = sizeof(MlpSmem);
+  const size_t smem = sizeof(MlpFwdSmem);
   const int blocks = (int)std::min<long long>(((long long)B + 127) / 128, 148 * 8);
   ++c->launches;
   mlp_forward_kernel<<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);

@@ -164,10 +164,123 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
   }
 }
 
+// Inference copy of the network: B fragments of W1, W2, W3 stored in the order
+// the m16n8k16 B operand is consumed (tile-major, then lane), so each lane
+// fetches its two registers of a tile with one conflict-free 64-bit load.
+//   f1[j][lane]      W1 tile (k 0..15, n 8j..8j+7)
+//   f2[kk][j][lane]  W2 tile (k 16kk.., n 8j..)
+//   f3[kk][lane]     W3 tile (k 16kk.., n 0..7)
+struct MlpFwdSmem {
+  uint2 f1[8 * 32];
+  uint2 f2[4 * 8 * 32];
+  uint2 f3[4 * 32];
+  float b1[kMlpH], b2[kMlpH], b3[8];
+  float xmean[16], xistd[16], ymean[8], ystd[8];
+};
+
+// One B-fragment register pair of the [n][k] row-major FP32 weight W (k < kin,
+// n < nout valid; zero elsewhere) for tile (k0, n0) and lane.
+__device__ __forceinline__ uint2 bfrag_from_f32(const float* __restrict__ W, int kin, int nout, int k0, int n0,
+                                                int lane) {
+  const int g = lane >> 2, t = lane & 3;
+  const int n = n0 + g;
+  float v[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = k0 + 2 * t + (e & 1) + (e >> 1) * 8;
+    v[e] = (n < nout && k < kin) ? W[n * kin + k] : 0.f;
+  }
+  return make_uint2(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]));
+}
+
+__device__ __forceinline__ void mlp_stage_fwd(MlpFwdSmem& s, const float* __restrict__ P,
+                                              const float* __restrict__ nrm) {
+  for (int i = threadIdx.x; i < 8 * 32; i += blockDim.x) s.f1[i] = bfrag_from_f32(P + kOffW1, kMlpIn, kMlpH, 0, 8 * (i >> 5), i & 31);
+  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+    const int tile = i >> 5, kk = tile >> 3, j = tile & 7;
+    s.f2[i] = bfrag_from_f32(P + kOffW2, kMlpH, kMlpH, 16 * kk, 8 * j, i & 31);
+  }
+  for (int i = threadIdx.x; i < 4 * 32; i += blockDim.x) s.f3[i] = bfrag_from_f32(P + kOffW3, kMlpH, kMlpOut, 16 * (i >> 5), 0, i & 31);
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    s.b1[i] = P[kOffB1 + i];
+    s.b2[i] = P[kOffB2 + i];
+  }
+  if (threadIdx.x < 16) {
+    s.xmean[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[threadIdx.x] : 0.f;
+    s.xistd[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[kMlpIn + threadIdx.x] : 0.f;
+  }
+  if (threadIdx.x < 8) {
+    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[kOffB3 + threadIdx.x] : 0.f;
+    s.ymean[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + threadIdx.x] : 0.f;
+    s.ystd[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + kMlpOut + threadIdx.x] : 0.f;
+  }
+}
+
+// Forward pass of 16 points from the fragment-ordered weights; same
+// arithmetic as mlp_forward_warp (BF16 operands, FP32 accumulation, GELU on
+// the FP32 pre-activations, BF16 rounding of the activations).
+__device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint32_t* xa, float* y) {
+  const int lane = threadIdx.x & 31, t = lane & 3;
+  float h[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float b0 = s.b1[8 * j + 2 * t], b1 = s.b1[8 * j + 2 * t + 1];
+    h[j][0] = b0;
+    h[j][1] = b1;
+    h[j][2] = b0;
+    h[j][3] = b1;
+    const uint2 bb = s.f1[j * 32 + lane];
+    const uint32_t b[2] = {bb.x, bb.y};
+    mma16816(h[j], xa, b);
+  }
+  uint32_t a[4][4];
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a[kk][0] = pack_bf16(gelu_f(h[2 * kk][0]), gelu_f(h[2 * kk][1]));
+    a[kk][1] = pack_bf16(gelu_f(h[2 * kk][2]), gelu_f(h[2 * kk][3]));
+    a[kk][2] = pack_bf16(gelu_f(h[2 * kk + 1][0]), gelu_f(h[2 * kk + 1][1]));
+    a[kk][3] = pack_bf16(gelu_f(h[2 * kk + 1][2]), gelu_f(h[2 * kk + 1][3]));
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const float b0 = s.b2[8 * j + 2 * t], b1 = s.b2[8 * j + 2 * t + 1];
+    h[j][0] = b0;
+    h[j][1] = b1;
+    h[j][2] = b0;
+    h[j][3] = b1;
+  }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const uint2 bb = s.f2[(kk * 8 + j) * 32 + lane];
+      const uint32_t b[2] = {bb.x, bb.y};
+      mma16816(h[j], a[kk], b);
+    }
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    a[kk][0] = pack_bf16(gelu_f(h[2 * kk][0]), gelu_f(h[2 * kk][1]));
+    a[kk][1] = pack_bf16(gelu_f(h[2 * kk][2]), gelu_f(h[2 * kk][3]));
+    a[kk][2] = pack_bf16(gelu_f(h[2 * kk + 1][0]), gelu_f(h[2 * kk + 1][1]));
+    a[kk][3] = pack_bf16(gelu_f(h[2 * kk + 1][2]), gelu_f(h[2 * kk + 1][3]));
+  }
+  const float c0 = s.b3[2 * t], c1 = s.b3[2 * t + 1];
+  y[0] = c0;
+  y[1] = c1;
+  y[2] = c0;
+  y[3] = c1;
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const uint2 bb = s.f3[kk * 32 + lane];
+    const uint32_t b[2] = {bb.x, bb.y};
+    mma16816(y, a[kk], b);
+  }
+}
+
 // A fragment of normalised features for 16 points; feat(r, f) returns the raw
 // feature f (< 10) of row r (< 16) of this warp's tile.
-template <class F>
-__device__ __forceinline__ void mlp_xfrag(const MlpSmem& s, uint32_t* xa, F feat) {
+template <class S, class F>
+__device__ __forceinline__ void mlp_xfrag(const S& s, uint32_t* xa, F feat) {
   const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   float v[8];
   const int rows[2] = {g, g + 8};

@@ -53,6 +53,16 @@ struct phys_is_block<P, decltype((void)P::BLOCK, void())> {
   static constexpr int extra = P::EXTRA_SMEM;
 };
 
+// Upper bound on the pencils per z-pass CTA (Phys::MAX_PPC, default 8).
+template <class P, class = void>
+struct phys_max_ppc {
+  static constexpr int value = 8;
+};
+template <class P>
+struct phys_max_ppc<P, decltype((void)P::MAX_PPC, void())> {
+  static constexpr int value = P::MAX_PPC;
+};
+
 template <typename T>
 struct AxisArgs {
   const Cx<T>* in;
@@ -78,9 +88,10 @@ struct PreCopy {
   __device__ void operator()(int, int, int, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const { d[0] = s[0]; }
 };
 
-// grid = (ceil(ncols/col_tile), nouter); smem = tw[L] + 2 * L*lines
+// One CTA of an axis pass: column tile bx, outer index by.
+// smem = tw[L] + 2 * L*lines
 template <typename T, bool INV, class Pre>
-__global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
+__device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   const int L = a.plan.L;
@@ -88,8 +99,8 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) 
   const int lines = Pre::F_DST * ct;
   Cx<T>* bufA = tw + L;
   Cx<T>* bufB = bufA + (size_t)L * lines;
-  const int o = blockIdx.y;
-  const int c0 = blockIdx.x * ct;
+  const int o = by;
+  const int c0 = bx * ct;
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T> zero = mk<T>(0, 0);
   for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) bufA[idx] = zero;
@@ -122,6 +133,19 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) 
   }
 }
 
+// grid = (ceil(ncols/col_tile), nouter)
+template <typename T, bool INV, class Pre>
+__global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
+  axis_pass_body<T, INV>(a, pre, blockIdx.x, blockIdx.y);
+}
+
+// Batched: grid = (ceil(ncols/col_tile), nouter, runs); run blockIdx.z takes
+// its arguments from A[z] and pre[z] (same tile shape for every run).
+template <typename T, bool INV, class Pre>
+__global__ void __launch_bounds__(256) axis_pass_batch(const AxisArgs<T>* __restrict__ A, const Pre* __restrict__ pre) {
+  axis_pass_body<T, INV>(A[blockIdx.z], pre[blockIdx.z], blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 struct ZArgs {
@@ -145,9 +169,9 @@ __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
   return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * M) * sizeof(Cx<T>) + extra;
 }
 
-// grid = ceil(npencils/ppc); smem = zpass_smem_bytes
+// One CTA of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes
 template <typename T, class Phys>
-__global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
+__device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   constexpr int FI = Phys::F_IN, FO = Phys::F_OUT;
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
   Cx<T>* X = tw + M;
   Cx<T>* Y = X + (size_t)nl * M;
   unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * M);
-  const long long p0 = (long long)blockIdx.x * P;
+  const long long p0 = (long long)bx * P;
   stage_twiddles(tw, a.tw, a.plan);
   if constexpr (phys_is_block<Phys>::value) phys.setup(extra);
   const Cx<T> zero = mk<T>(0, 0);
@@ -254,6 +278,18 @@ __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
   }
 }
 
+// grid = ceil(npencils/ppc)
+template <typename T, class Phys>
+__global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
+  zpass_body<T>(a, phys, blockIdx.x);
+}
+
+// Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
+template <typename T, class Phys>
+__global__ void __launch_bounds__(256) zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
+  zpass_body<T>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
 struct XEpiArgs {
@@ -268,19 +304,20 @@ struct XEpiArgs {
   const Cx<T>* tw;
 };
 
-// grid = main_blocks + extra; main block b -> (col tile b % ntile, outer b / ntile)
+// One CTA of the x-forward epilogue pass: block bx of gx = main_blocks + extra;
+// main block b -> (col tile b % ntile, outer b / ntile)
 template <typename T, class Epi>
-__global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
+__device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& epi, int bx, int gx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int F = Epi::F_IN;
   Cx<T> P[F];
   const Cx<T> zero = mk<T>(0, 0);
-  if ((int)blockIdx.x >= a.main_blocks) {
+  if (bx >= a.main_blocks) {
     // columns kz..n3h-1 carry no products
     const int ncz = a.n3h - a.kz;
     const long long tot = (long long)a.n1 * a.n2 * ncz;
-    const int nextra = gridDim.x - a.main_blocks;
-    for (long long idx = (long long)(blockIdx.x - a.main_blocks) * blockDim.x + threadIdx.x; idx < tot;
+    const int nextra = gx - a.main_blocks;
+    for (long long idx = (long long)(bx - a.main_blocks) * blockDim.x + threadIdx.x; idx < tot;
          idx += (long long)nextra * blockDim.x) {
       const int c = (int)(idx % ncz);
       const long long t = idx / ncz;
@@ -298,8 +335,8 @@ __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
   Cx<T>* bufA = tw + L;
   Cx<T>* bufB = bufA + (size_t)L * lines;
   const int ntile = (a.kz + ct - 1) / ct;
-  const int o = blockIdx.x / ntile;
-  const int c0 = (blockIdx.x % ntile) * ct;
+  const int o = bx / ntile;
+  const int c0 = (bx % ntile) * ct;
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
   for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) {
@@ -320,6 +357,18 @@ __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
     for (int f = 0; f < F; ++f) P[f] = j >= 0 ? res[(size_t)j * lines + f * ct + c] : zero;
     epi(i1, o, col, P);
   }
+}
+
+// grid = main_blocks + extra
+template <typename T, class Epi>
+__global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
+  xfwd_epi_body<T>(a, epi, blockIdx.x, gridDim.x);
+}
+
+// Batched: grid = (main_blocks + extra, runs); run blockIdx.y reads A[y], epi[y].
+template <typename T, class Epi>
+__global__ void __launch_bounds__(256) xfwd_epi_batch(const XEpiArgs<T>* __restrict__ A, const Epi* __restrict__ epi) {
+  xfwd_epi_body<T>(A[blockIdx.y], epi[blockIdx.y], blockIdx.x, gridDim.x);
 }
 
 }  // namespace psb

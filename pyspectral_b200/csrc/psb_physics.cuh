@@ -617,48 +617,60 @@ template <typename T>
 struct PhysLearned {
   static constexpr int F_IN = 12, F_OUT = 6;
   static constexpr bool BLOCK = true;
-  static constexpr int EXTRA_SMEM = (int)((sizeof(MlpSmem) + 15) / 16 * 16);
+  static constexpr int EXTRA_SMEM = (int)((sizeof(MlpFwdSmem) + 15) / 16 * 16);
+  static constexpr int MAX_PPC = 4;  // 4 pencils per CTA: 3-4 CTAs per SM at 3N/2 = 96 (FP32)
   const float* params;
   const float* norm;
   T sphys;      // s: physical = real-space * s
   float delta;  // filter width fed to the MLP
   __device__ void setup(unsigned char* extra) const {
-    mlp_stage(*reinterpret_cast<MlpSmem*>(extra), params, norm);
+    mlp_stage_fwd(*reinterpret_cast<MlpFwdSmem*>(extra), params, norm);
   }
+  // Each warp takes tiles of 16 consecutive points (pencil-major); a lane
+  // holds rows g and g+8 of a tile and locates them once per tile.
   __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
                         unsigned char* extra) const {
-    const MlpSmem& s = *reinterpret_cast<const MlpSmem*>(extra);
+    const MlpFwdSmem& s = *reinterpret_cast<const MlpFwdSmem*>(extra);
     const int npts = P * M;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int nw = blockDim.x >> 5;
-    auto val = [&](int f, int pt) -> T {
-      const int p = pt / M, z = pt - p * M;
-      const int r = f * P + p;
-      const Cx<T> v = R[(size_t)(r >> 1) * M + z];
-      return fac * ((r & 1) ? v.y : v.x);
-    };
     const T is2 = (T)1 / (sphys * sphys);
+    const T fs = fac * sphys;
     for (int pt0 = warp * 16; pt0 < npts; pt0 += nw * 16) {
+      // rows g and g+8 of the tile: pencil p, position z
+      int rp[2], rz[2];
+      bool ok[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int pt = pt0 + g + 8 * h;
+        ok[h] = pt < npts;
+        rp[h] = ok[h] ? pt / M : 0;
+        rz[h] = ok[h] ? pt - rp[h] * M : 0;
+      }
+      auto val = [&](int f, int h) -> T {
+        const int r = f * P + rp[h];
+        const Cx<T> v = R[(size_t)(r >> 1) * M + rz[h]];
+        return (r & 1) ? v.y : v.x;
+      };
       uint32_t xa[4];
       mlp_xfrag(s, xa, [&](int r, int f) -> float {
-        const int pt = pt0 + r;
-        if (pt >= npts) return s.xmean[f];
-        return f < 9 ? (float)(val(3 + f, pt) * sphys) : delta;
+        const int h = r >= 8 ? 1 : 0;
+        if (!ok[h]) return s.xmean[f];
+        return f < 9 ? (float)(val(3 + f, h) * fs) : delta;
       });
       float y[4];
-      mlp_forward_warp(s, xa, y, nullptr, nullptr);
+      mlp_forward_fast(s, xa, y);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int c = 2 * t + (e & 1);
-        const int pt = pt0 + g + (e < 2 ? 0 : 8);
-        if (c >= kMlpOut || pt >= npts) continue;
+        const int h = e < 2 ? 0 : 1;
+        if (c >= kMlpOut || !ok[h]) continue;
         const int ii = c < 3 ? c : (c == 5 ? 1 : 0);
         const int jj = c < 3 ? c : (c == 3 ? 1 : 2);
         const T tau = (T)(y[e] * s.ystd[c] + s.ymean[c]);
-        const T o = val(ii, pt) * val(jj, pt) + tau * is2;
-        const int p = pt / M, z = pt - p * M;
-        const int r = c * P + p;
-        reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + z)[r & 1] = o;
+        const T o = (fac * val(ii, h)) * (fac * val(jj, h)) + tau * is2;
+        const int r = c * P + rp[h];
+        reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + rz[h])[r & 1] = o;
       }
     }
   }

@@ -1,0 +1,249 @@
+"""Batched ensembles of independent decaying-turbulence runs.
+
+No counterpart in the reference, which advances one run per process
+(PySpectral/src/PySpec_3d.py:96-144).  Runs of one grid size, precision and
+closure form a batch (``psb_batch``): every pass of an RK4 stage is one launch
+over all runs of the batch, with launch shapes picked by the library's
+autotuner.  All batches of an ensemble are captured together into one CUDA
+graph, so K steps of the whole ensemble are one graph launch.
+
+Ensemble case (uneven sizes): 96 runs, 32 each at 32^3, 48^3 and 64^3; run i
+has seed 1000+i, k0 drawn uniformly from {2,3,4,5}, nu log-uniform in
+[5e-4, 5e-3]; FP32 fields with Kahan stage accumulation; RK4 with dt = 2e-3.
+The learned closure is used where the model was trained (the filter width
+of its training data, 2 pi/64); the other sizes fall back to Smagorinsky.
+
+    python -m pyspectral_b200.ensemble [--steps 500] [--per-size 32]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _capi
+from .initial_conditions import isotropic_state
+
+PASSES = ("x-inverse", "y-inverse", "z-fused", "y-forward", "x-forward+epilogue")
+
+
+def _lib():
+    lib = _capi.load()
+    if not getattr(lib, "_psb_batch_sigs", False):
+        vp, i = ctypes.c_void_p, ctypes.c_int
+        for name, args in (("psb_batch_create", [vp, i, i, ctypes.POINTER(vp)]),
+                           ("psb_batch_set_run", [vp, i, vp, vp, ctypes.POINTER(_capi.Params)]),
+                           ("psb_batch_autotune", [vp]), ("psb_batch_step_rk4", [vp, i]),
+                           ("psb_batch_shape", [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), i]),
+                           ("psb_batch_destroy", [vp])):
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        lib._psb_batch_sigs = True
+    return lib
+
+
+class Batch:
+    """``nruns`` runs on one context (grid size + precision) with one closure."""
+
+    def __init__(self, ctx, closure, nruns):
+        self.lib = _lib()
+        self.ctx = ctx
+        self.closure = closure
+        self.nruns = nruns
+        h = ctypes.c_void_p()
+        ctx.check(self.lib.psb_batch_create(ctx.h, closure, nruns, ctypes.byref(h)), "psb_batch_create")
+        self.h = h
+        self.runs = [None] * nruns
+
+    def set_run(self, r, state, comp, params):
+        self.runs[r] = (state, comp, params)  # keep the tensors and params alive
+        self.ctx.check(self.lib.psb_batch_set_run(self.h, r, self.ctx._ptr(state), self.ctx._ptr(comp),
+                                                  ctypes.byref(params)), "psb_batch_set_run")
+
+    def autotune(self):
+        self.ctx.bind_stream()
+        self.ctx.check(self.lib.psb_batch_autotune(self.h), "psb_batch_autotune")
+
+    def step(self, nsteps=1):
+        self.ctx.bind_stream()
+        self.ctx.check(self.lib.psb_batch_step_rk4(self.h, int(nsteps)), "psb_batch_step_rk4")
+
+    def shapes(self):
+        out = {}
+        for p, name in enumerate(PASSES):
+            t = ctypes.c_int()
+            rad = (ctypes.c_int * 12)()
+            self.ctx.check(self.lib.psb_batch_shape(self.h, p, ctypes.byref(t), rad, 12), "psb_batch_shape")
+            out[name] = {"tile": t.value, "radices": [x for x in rad if x]}
+        return out
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                self.lib.psb_batch_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+def ensemble_specs(sizes=(32, 48, 64), per_size=32, seed0=1000, nu_range=(5e-4, 5e-3), k0s=(2, 3, 4, 5)):
+    """Per-run (N, seed, k0, nu) of the ensemble case, reproducible from seed0."""
+    rng = np.random.default_rng(seed0)
+    specs = []
+    i = 0
+    for N in sizes:
+        for _ in range(per_size):
+            k0 = int(rng.choice(k0s))
+            nu = float(math.exp(rng.uniform(math.log(nu_range[0]), math.log(nu_range[1]))))
+            specs.append({"N": N, "seed": seed0 + i, "k0": k0, "nu": nu})
+            i += 1
+    return specs
+
+
+class Ensemble:
+    """All runs of an ensemble, grouped into one batch per grid size."""
+
+    def __init__(self, specs, dt=2e-3, precision=32, model=None, learned_N=64, tune=True, device=0):
+        self.specs = specs
+        self.dt = dt
+        self.precision = precision
+        self.device = device
+        self.model = model
+        self.groups = []
+        cdt = torch.complex64 if precision == 32 else torch.complex128
+        for N in sorted({s["N"] for s in specs}):
+            runs = [s for s in specs if s["N"] == N]
+            ctx = _capi.Context(N, N, N, precision=precision, device=device)
+            ctx64 = _capi.Context(N, N, N, precision=64, device=device)
+            use_learned = model is not None and N == learned_N
+            closure = _capi.LEARNED if use_learned else _capi.SMAG
+            b = Batch(ctx, closure, len(runs))
+            states, comps, params = [], [], []
+            for r, s in enumerate(runs):
+                st = isotropic_state(N, s["seed"], k0=float(s["k0"]), device=device, ctx=ctx64).to(cdt).contiguous()
+                comp = torch.zeros_like(st) if precision == 32 else None
+                p = _capi.make_params(nu=s["nu"], dt=dt,
+                                      mlp_params=model.params.data_ptr() if use_learned else None,
+                                      mlp_norm=model.norm.data_ptr() if use_learned else None,
+                                      les_delta=2 * math.pi / N)
+                b.set_run(r, st, comp, p)
+                states.append(st)
+                comps.append(comp)
+                params.append(p)
+            if tune:
+                b.autotune()
+            self.groups.append({"N": N, "ctx": ctx, "batch": b, "states": states, "comps": comps,
+                                "closure": "learned" if use_learned else "smag", "runs": runs})
+        self.graph = None
+
+    def points(self):
+        return sum(s["N"] ** 3 for s in self.specs)
+
+    def step(self, nsteps=1):
+        for g in self.groups:
+            g["batch"].step(nsteps)
+
+    def capture(self, nsteps=1):
+        """One CUDA graph holding nsteps steps of every batch."""
+        saved = [[t.clone() for t in g["states"] + [c for c in g["comps"] if c is not None]] for g in self.groups]
+        self.step(nsteps)  # outside the capture: kernel attributes and argument blocks
+        torch.cuda.synchronize()
+        for g, sv in zip(self.groups, saved):
+            for t, s in zip(g["states"] + [c for c in g["comps"] if c is not None], sv):
+                t.copy_(s)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=side):
+            self.step(nsteps)
+        torch.cuda.synchronize()
+        self.graph_steps = nsteps
+
+    def replay(self):
+        self.graph.replay()
+
+    def shapes(self):
+        return {g["N"]: g["batch"].shapes() for g in self.groups}
+
+
+def time_batched(ens, steps, graph_steps=10):
+    """Aggregate grid-pt x steps / s of the whole ensemble, CUDA-graph replays."""
+    ens.capture(graph_steps)
+    reps = max(1, steps // graph_steps)
+    ens.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        ens.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = reps * graph_steps
+    return {"steps": n, "ms": ms, "value": ens.points() * n / (ms / 1e3)}
+
+
+def time_sequential(specs, steps, dt=2e-3, model=None, learned_N=64, device=0):
+    """The same runs one after another, each through the single-run path
+    (one CUDA graph of `steps` steps per run)."""
+    from . import Classes as C
+    from .RHSfunctions import StepGraph
+    total_ms = 0.0
+    pts = 0
+    ctxs = {}
+    for s in specs:
+        N = s["N"]
+        if N not in ctxs:
+            ctxs[N] = _capi.Context(N, N, N, precision=64, device=device)
+        st = isotropic_state(N, s["seed"], k0=float(s["k0"]), device=device, ctx=ctxs[N])
+        use_learned = model is not None and N == learned_N
+        grid = C.gridclass.periodic(N, device=device)
+        main = C.variables(0, "learned" if use_learned else 1, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, dt,
+                           s["nu"], precision=32, model=model if use_learned else None)
+        g = StepGraph(main, grid, steps)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        pts += N ** 3
+        del g
+    return {"steps": steps, "ms": total_ms, "value": pts * steps / (total_ms / 1e3)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--per-size", type=int, default=32)
+    ap.add_argument("--seq-steps", type=int, default=50)
+    ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    from .learned import MLPModel
+    model = MLPModel.load()
+    specs = ensemble_specs(per_size=a.per_size)
+    t0 = time.time()
+    ens = Ensemble(specs, model=model, tune=not a.no_tune)
+    setup_s = time.time() - t0
+    batched = time_batched(ens, a.steps)
+    finite = all(bool(torch.isfinite(torch.view_as_real(s)).all()) for g in ens.groups for s in g["states"])
+    seq = time_sequential(specs, a.seq_steps, model=model)
+    res = {"runs": len(specs), "sizes": sorted({s["N"] for s in specs}), "batched": batched, "sequential": seq,
+           "speedup": batched["value"] / seq["value"], "shapes": ens.shapes(), "setup_s": setup_s,
+           "closures": {g["N"]: g["closure"] for g in ens.groups}, "finite": finite}
+    print(json.dumps(res))
+    if a.out:
+        with open(a.out, "w") as fh:
+            json.dump(res, fh)
+
+
+if __name__ == "__main__":
+    main()

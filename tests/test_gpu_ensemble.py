@@ -1,0 +1,99 @@
+"""Batched ensembles on the GPU: every run of a batch advances exactly like the
+same run through the single-run path (FP64: 1e-12 relative), before and after
+the autotuner changes the launch shapes, and the ensemble driver runs an
+uneven-size ensemble in one CUDA graph."""
+import numpy as np
+import pytest
+
+from tests.helpers import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def _single(torch, N, st, nu, dt, closure, precision, model=None, steps=2):
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advance
+    tm = {"dns": 0, "smag": 1, "learned": "learned"}[closure]
+    grid = C.gridclass.periodic(N)
+    main = C.variables(0, tm, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, dt, nu, precision=precision,
+                       model=model)
+    advance(main, grid, steps)
+    return np_(main.Q)
+
+
+def _batch_runs(torch, N, closure, precision, tune, model=None, steps=2, nruns=3):
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.ensemble import Batch
+    from pyspectral_b200.initial_conditions import isotropic_state
+    code = {"dns": _capi.DNS, "smag": _capi.SMAG, "learned": _capi.LEARNED}[closure]
+    cdt = torch.complex128 if precision == 64 else torch.complex64
+    ctx = _capi.Context(N, N, N, precision=precision)
+    b = Batch(ctx, code, nruns)
+    init, states, nus = [], [], []
+    for r in range(nruns):
+        st = isotropic_state(N, 10 + r, k0=3.0 + r).to(cdt).contiguous()
+        init.append(st.clone())
+        nu = 1e-3 * (1 + r)
+        comp = torch.zeros_like(st) if precision == 32 else None
+        p = _capi.make_params(nu=nu, dt=2e-3, mlp_params=model.params.data_ptr() if model else None,
+                              mlp_norm=model.norm.data_ptr() if model else None, les_delta=2 * np.pi / N)
+        b.set_run(r, st, comp, p)
+        states.append(st)
+        nus.append(nu)
+    if tune:
+        b.autotune()
+        for s, s0 in zip(states, init):
+            assert torch.equal(s, s0)  # tuning leaves the states alone
+    b.step(steps)
+    torch.cuda.synchronize()
+    return b, [np_(s) for s in states], [np_(s) for s in init], nus
+
+
+@pytest.mark.parametrize("closure", ["dns", "smag"])
+@pytest.mark.parametrize("tune", [False, True])
+def test_batch_matches_single_runs_fp64(closure, tune):
+    torch = _torch()
+    N = 16
+    b, out, init, nus = _batch_runs(torch, N, closure, 64, tune)
+    for r in range(len(out)):
+        ref = _single(torch, N, init[r], nus[r], 2e-3, closure, 64)
+        assert rel(out[r], ref) < 1e-12
+    sh = b.shapes()
+    assert sh["z-fused"]["tile"] >= 1 and np.prod(sh["x-inverse"]["radices"]) == 3 * N // 2
+
+
+def test_learned_batch_tracks_single_runs_fp32():
+    torch = _torch()
+    from pyspectral_b200.learned import MLPModel
+    model = MLPModel.load()
+    N = 32
+    b, out, init, nus = _batch_runs(torch, N, "learned", 32, True, model=model)
+    for r in range(len(out)):
+        ref = _single(torch, N, init[r].astype(np.complex128), nus[r], 2e-3, "learned", 32, model=model)
+        assert rel(out[r], ref) < 2e-5
+
+
+def test_uneven_ensemble_in_one_graph():
+    torch = _torch()
+    from pyspectral_b200.ensemble import Ensemble, ensemble_specs, time_batched
+    from pyspectral_b200.learned import MLPModel
+    specs = ensemble_specs(sizes=(16, 24, 32), per_size=3)
+    ens = Ensemble(specs, model=MLPModel.load(), learned_N=32, tune=True)
+    before = [s.clone() for g in ens.groups for s in g["states"]]
+    res = time_batched(ens, 4, graph_steps=2)
+    after = [s for g in ens.groups for s in g["states"]]
+    assert res["value"] > 0 and res["steps"] == 4
+    assert all(bool(torch.isfinite(torch.view_as_real(s)).all()) for s in after)
+    assert all(not torch.equal(a, b) for a, b in zip(after, before))
+    assert {g["closure"] for g in ens.groups} == {"learned", "smag"}
