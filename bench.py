@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--N", type=int, default=64)
     ap.add_argument("--closure", choices=["learned", "smag", "dns"], default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="run warmup+steps plain RK4 steps of the headline case and exit (for ncu captures)")
     return ap.parse_args()
 
 
@@ -444,8 +446,30 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """The headline case's steps without timing, baselines or JSON: a short,
+    deterministic launch sequence for profilers."""
+    import torch
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advance
+    N = args.N
+    st = make_state(N, 1)
+    model = None
+    if args.closure == "learned":
+        from pyspectral_b200.learned import MLPModel
+        model = MLPModel.load()
+    tm = {"learned": "learned", "smag": 1, "dns": 0}[args.closure]
+    grid = C.gridclass.periodic(N)
+    main = C.variables(0, tm, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 2e-3, 1e-3, precision=32, model=model)
+    advance(main, grid, args.warmup + args.steps)
+    torch.cuda.synchronize()
+
+
 def main():
     args = parse()
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         rank, world, _ = dist_env()

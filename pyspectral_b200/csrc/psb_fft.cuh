@@ -130,28 +130,61 @@ __device__ __forceinline__ void small_dft(Cx<T>* v) {
   }
 }
 
-// One Stockham butterfly: sub-transform position j of a pass of radix R.
+// One Stockham pass of radix R over `nlines` lines held at buf[line*ls + j*es]
+// (j < L).  Work item (line, j < L/R) reads element j + r*L/R of its line,
+// applies the twiddles W_{Ns R}^{r k} (k = j mod Ns), runs the R-point DFT and
+// writes element (j - k) R + k + r Ns.  Items are walked as a (fast, slow)
+// counter pair advanced by blockDim.x items per iteration without a division
+// (fast = line when lines_fast, else j); k follows j modulo Ns the same way
+// (Ns divides L/R, so a wrap of j leaves k's step unchanged).
 template <typename T, int R, bool INV>
-__device__ __forceinline__ void stockham_bfly(const Cx<T>* __restrict__ src, Cx<T>* __restrict__ dst,
-                                              int j, int nb, int Ns, int L, const Cx<T>* __restrict__ tw,
-                                              int es) {
-  Cx<T> v[R];
+__device__ __forceinline__ void stockham_pass(const Cx<T>* __restrict__ a, Cx<T>* __restrict__ b,
+                                              const Cx<T>* __restrict__ tw, int L, int Ns, int nlines, int ls,
+                                              int es, bool lines_fast) {
+  const int nb = L / R;
+  const int tstride = L / (Ns * R);
+  const int mf = lines_fast ? nlines : nb;
+  const int ms = lines_fast ? nb : nlines;
+  const int nt = blockDim.x;
+  int f = threadIdx.x % mf, sl = threadIdx.x / mf;
+  const int df = nt % mf, ds = nt / mf;
+  int j = lines_fast ? sl : f;
+  int k = j % Ns;
+  const int dk = lines_fast ? ds % Ns : df % Ns;
+  const size_t rs = (size_t)nb * es, ws = (size_t)Ns * es;
+  while (sl < ms) {
+    const int line = lines_fast ? f : sl;
+    const Cx<T>* src = a + (size_t)line * ls + (size_t)j * es;
+    Cx<T> v[R];
 #pragma unroll
-  for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
-  const int k = j % Ns;
-  if (Ns > 1) {
-    const int tstep = k * (L / (Ns * R));
+    for (int r = 0; r < R; ++r) v[r] = src[r * rs];
+    if (k) {
+      const int tstep = k * tstride;
 #pragma unroll
-    for (int r = 1; r < R; ++r) {
-      Cx<T> w = tw[r * tstep];
-      if (INV) w.y = -w.y;
-      v[r] = cmul(v[r], w);
+      for (int r = 1; r < R; ++r) {
+        Cx<T> w = tw[r * tstep];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
     }
-  }
-  small_dft<T, R, INV>(v);
-  const int base = (j - k) * R + k;
+    small_dft<T, R, INV>(v);
+    Cx<T>* dst = b + (size_t)line * ls + (size_t)((j - k) * R + k) * es;
 #pragma unroll
-  for (int r = 0; r < R; ++r) dst[(base + r * Ns) * es] = v[r];
+    for (int r = 0; r < R; ++r) dst[r * ws] = v[r];
+    f += df;
+    sl += ds;
+    const int carry = f >= mf ? 1 : 0;
+    f -= carry * mf;
+    sl += carry;
+    if (lines_fast) {
+      j = sl;
+      k += dk + carry;
+    } else {
+      j = f;
+      k += dk;
+    }
+    if (k >= Ns) k -= Ns;
+  }
 }
 
 // Transform `nlines` lines held at buf[line*ls + j*es] (j < L).  `a` holds the
@@ -166,25 +199,11 @@ __device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* _
   int Ns = 1;
   for (int s = 0; s < p.npass; ++s) {
     const int R = p.radix[s];
-    const int nb = L / R;
-    const int total = nb * nlines;
-    for (int id = threadIdx.x; id < total; id += blockDim.x) {
-      int line, j;
-      if (lines_fast) {
-        line = id % nlines;
-        j = id / nlines;
-      } else {
-        j = id % nb;
-        line = id / nb;
-      }
-      const Cx<T>* src = a + (size_t)line * ls;
-      Cx<T>* dst = b + (size_t)line * ls;
-      switch (R) {
-        case 8: stockham_bfly<T, 8, INV>(src, dst, j, nb, Ns, L, tw, es); break;
-        case 4: stockham_bfly<T, 4, INV>(src, dst, j, nb, Ns, L, tw, es); break;
-        case 3: stockham_bfly<T, 3, INV>(src, dst, j, nb, Ns, L, tw, es); break;
-        default: stockham_bfly<T, 2, INV>(src, dst, j, nb, Ns, L, tw, es); break;
-      }
+    switch (R) {
+      case 8: stockham_pass<T, 8, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+      case 4: stockham_pass<T, 4, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+      case 3: stockham_pass<T, 3, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+      default: stockham_pass<T, 2, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
     }
     __syncthreads();
     Cx<T>* t = a;

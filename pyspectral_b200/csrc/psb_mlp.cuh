@@ -75,10 +75,35 @@ __device__ __forceinline__ void mma16816(float* d, const uint32_t* a, const uint
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// exact GELU and its derivative (erf form)
-__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
+// GELU x Phi(x) = x (1 + erf(x / sqrt 2)) / 2 and its derivative, with erf from
+// Abramowitz & Stegun, Handbook of Mathematical Functions (1964), formula
+// 7.1.26: for z >= 0, erf z = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-z^2},
+// t = 1 / (1 + p z), |error| <= 1.5e-7; erf(-z) = -erf z.  Branch-free: with
+// q = poly(t) e^{-x^2/2} (z = |x|/sqrt 2), 1 + erf(x/sqrt 2) = 2 - q for x >= 0
+// and q for x < 0.
+struct GeluAS {
+  static constexpr float p = 0.3275911f, a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f,
+                         a4 = -1.453152027f, a5 = 1.061405429f;
+};
+// 1 + erf(x / sqrt 2), and the Gaussian factor e^{-x^2/2} it used
+__device__ __forceinline__ float one_plus_erf_s2(float x, float* gauss) {
+  const float z = fabsf(x) * 0.70710678118654752f;
+  const float t = __fdividef(1.f, fmaf(GeluAS::p, z, 1.f));
+  const float poly =
+      t * fmaf(t, fmaf(t, fmaf(t, fmaf(t, GeluAS::a5, GeluAS::a4), GeluAS::a3), GeluAS::a2), GeluAS::a1);
+  const float g = __expf(-0.5f * x * x);
+  *gauss = g;
+  const float q = poly * g;
+  return x >= 0.f ? 2.f - q : q;
+}
+__device__ __forceinline__ float gelu_f(float x) {
+  float g;
+  return 0.5f * x * one_plus_erf_s2(x, &g);
+}
 __device__ __forceinline__ float gelu_d(float x) {
-  return 0.5f * (1.f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  float g;
+  const float e = one_plus_erf_s2(x, &g);
+  return 0.5f * e + x * 0.39894228040143268f * g;
 }
 
 // B fragment of a weight stored [n][k] row-major (ld = k stride) for the tile (k0, n0).

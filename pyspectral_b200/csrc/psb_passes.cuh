@@ -37,6 +37,38 @@ struct RowMap {
 
 constexpr int kMaxZFields = 16;
 
+// Walks the work items (fast, slow) = (id % mf, id / mf) of id = threadIdx.x +
+// n * blockDim.x without a division per item.
+struct Walk2 {
+  int f, s, df, ds, mf;
+  __device__ __forceinline__ explicit Walk2(int m) : mf(m) {
+    f = threadIdx.x % m;
+    s = threadIdx.x / m;
+    df = blockDim.x % m;
+    ds = blockDim.x / m;
+  }
+  __device__ __forceinline__ void next() {
+    f += df;
+    s += ds;
+    if (f >= mf) {
+      f -= mf;
+      ++s;
+    }
+  }
+};
+
+// (field, pencil) of packed real line r = f*P + p; P is a power of two in
+// every launch (lp = log2 P), otherwise divide
+__device__ __forceinline__ void split_line(int r, int P, int lp, int& f, int& p) {
+  if ((P & (P - 1)) == 0) {
+    f = r >> lp;
+    p = r & (P - 1);
+  } else {
+    f = r / P;
+    p = r - f * P;
+  }
+}
+
 // Phys functors with `static constexpr bool BLOCK = true` provide
 // setup(extra_smem) and block(R, W, P, M, fac, p0, npencils, extra_smem) and
 // ask for EXTRA_SMEM bytes behind the z-pass buffers.  R and W hold packed
@@ -103,31 +135,46 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
   const int c0 = bx * ct;
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T> zero = mk<T>(0, 0);
-  for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) bufA[idx] = zero;
-  __syncthreads();
+  // A thread keeps one column c of the tile and walks rows with stride nt/ct
+  // (launches use power-of-two tiles, which divide the CTA size).
+  const int nt = blockDim.x;
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
+  const int col = c0 + c;
+  const bool colok = col < a.ncols;
+  // zero the FFT positions that no input row fills: [lo, hi+shift) and
+  // [in_rows+shift, L) of the row map (every map used has in_rows >= hi)
+  {
+    const RowMap m = a.in_map;
+    const int g0 = m.lo < L ? m.lo : L, g1 = min(m.hi + m.shift, L);
+    const int t0 = min(a.in_rows + m.shift, L);
+    for (int j = g0; j < g1; ++j)
+      for (int l = threadIdx.x; l < lines; l += nt) bufA[(size_t)j * lines + l] = zero;
+    for (int j = t0; j < L; ++j)
+      for (int l = threadIdx.x; l < lines; l += nt) bufA[(size_t)j * lines + l] = zero;
+  }
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
-  for (int idx = threadIdx.x; idx < a.in_rows * ct; idx += blockDim.x) {
-    const int c = idx % ct, i = idx / ct;
-    const int col = c0 + c;
+  for (int i = r0; i < a.in_rows; i += dr) {
     const int j = a.in_map(i);
-    if (j < 0 || col >= a.ncols) continue;
+    if (j < 0) continue;
     Cx<T> s[Pre::F_SRC], d[Pre::F_DST];
+    if (colok) {
 #pragma unroll
-    for (int f = 0; f < Pre::F_SRC; ++f) s[f] = inb[f * a.in_fstride + i * a.in_rstride + col];
-    pre(i, o, col, a, s, d);
+      for (int f = 0; f < Pre::F_SRC; ++f) s[f] = inb[f * a.in_fstride + i * a.in_rstride + col];
+      pre(i, o, col, a, s, d);
+    } else {
+#pragma unroll
+      for (int g = 0; g < Pre::F_DST; ++g) d[g] = zero;
+    }
 #pragma unroll
     for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
   }
   __syncthreads();
   Cx<T>* res = block_fft<T, INV>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
   Cx<T>* outb = a.out + (long long)o * a.out_ostride;
-  const int nst = a.out_rows * Pre::F_DST * ct;
-  for (int idx = threadIdx.x; idx < nst; idx += blockDim.x) {
-    const int c = idx % ct;
-    const int t = idx / ct;
-    const int g = t % Pre::F_DST, i = t / Pre::F_DST;
-    const int col = c0 + c;
-    if (col >= a.ncols) continue;
+  if (!colok || threadIdx.x >= dr * ct) return;
+  const int nrow = a.out_rows * Pre::F_DST;
+  for (int t = r0; t < nrow; t += dr) {
+    const int i = t / Pre::F_DST, g = t - i * Pre::F_DST;
     const int j = a.out_map(i);
     outb[g * a.out_fstride + i * a.out_rstride + col] = j >= 0 ? a.scale * res[(size_t)j * lines + g * ct + c] : zero;
   }
@@ -183,6 +230,7 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
   Cx<T>* Y = X + (size_t)nl * M;
   unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * M);
   const long long p0 = (long long)bx * P;
+  const int lp = __ffs(P) - 1;
   stage_twiddles(tw, a.tw, a.plan);
   if constexpr (phys_is_block<Phys>::value) phys.setup(extra);
   const Cx<T> zero = mk<T>(0, 0);
@@ -194,14 +242,15 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
     __syncthreads();
     // pack pairs of Hermitian half-spectra: Z = A + iB, Z[M-k] = conj(A_k) + i conj(B_k);
     // the k=0 and k=M/2 terms keep their real parts only (c2r convention)
-    for (int idx = threadIdx.x; idx < nin * (half + 1); idx += blockDim.x) {
-      const int k = idx % (half + 1), c = idx / (half + 1);
+    for (Walk2 w(half + 1); w.s < nin; w.next()) {
+      const int k = w.f, c = w.s;
       Cx<T> A = zero, B = zero;
 #pragma unroll 1
       for (int part = 0; part < 2; ++part) {
         const int r = 2 * c + part;
         if (r >= FI * P) break;
-        const int f = r / P, p = r % P;
+        int f, p;
+        split_line(r, P, lp, f, p);
         const long long pen = p0 + p;
         if (pen >= a.npencils || k >= a.in_kz[f]) continue;
         const Cx<T> v = a.in[f][pen * a.in_pstride[f] + k];
@@ -228,8 +277,8 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
     }
   } else {
     // pointwise physics; the last CTA may hold fewer than P pencils
-    for (int idx = threadIdx.x; idx < P * M; idx += blockDim.x) {
-      const int z = idx % M, p = idx / M;
+    for (Walk2 w(M); w.s < P; w.next()) {
+      const int z = w.f, p = w.s;
       T vin[FI > 0 ? FI : 1], vout[FO > 0 ? FO : 1];
 #pragma unroll
       for (int f = 0; f < FI; ++f) {
@@ -259,15 +308,16 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
     Cx<T>* R2 = block_fft<T, false>(W, R, a.plan, tw, nout, M, 1, false);
     // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
     const int kzo = a.out_kz;
-    for (int idx = threadIdx.x; idx < nout * kzo; idx += blockDim.x) {
-      const int k = idx % kzo, c = idx / kzo;
+    for (Walk2 w(kzo); w.s < nout; w.next()) {
+      const int k = w.f, c = w.s;
       const Cx<T>* Z = R2 + (size_t)c * M;
       const Cx<T> zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
 #pragma unroll
       for (int part = 0; part < 2; ++part) {
         const int r = 2 * c + part;
         if (r >= FO * P) break;
-        const int g = r / P, p = r % P;
+        int g, p;
+        split_line(r, P, lp, g, p);
         const long long pen = p0 + p;
         if (pen >= a.npencils) continue;
         const Cx<T> v = part == 0 ? mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y))
@@ -339,19 +389,21 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
   const int c0 = (bx % ntile) * ct;
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
-  for (int idx = threadIdx.x; idx < L * lines; idx += blockDim.x) {
-    const int c = idx % ct;
-    const int t = idx / ct;
-    const int f = t % F, j = t / F;
-    const int col = c0 + c;
-    bufA[(size_t)j * lines + f * ct + c] = col < a.kz ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
+  // one column c per thread, rows walked with stride nt/ct (as in the axis pass)
+  const int nt = blockDim.x;
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
+  const int col = c0 + c;
+  const bool colok = col < a.kz;
+  for (int t = r0; t < L * F; t += dr) {
+    const int j = t / F, f = t - j * F;
+    bufA[(size_t)j * lines + f * ct + c] = colok ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
   }
   __syncthreads();
   Cx<T>* res = block_fft<T, false>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
-  for (int idx = threadIdx.x; idx < a.n1 * ct; idx += blockDim.x) {
-    const int c = idx % ct, i1 = idx / ct;
-    const int col = c0 + c;
-    if (col >= a.kz) continue;
+  // threads past the last full row of columns would repeat a (row, column)
+  // (only when ct does not divide the CTA size): the epilogue is not idempotent
+  if (!colok || threadIdx.x >= dr * ct) return;
+  for (int i1 = r0; i1 < a.n1; i1 += dr) {
     const int j = a.out_map(i1);
 #pragma unroll
     for (int f = 0; f < F; ++f) P[f] = j >= 0 ? res[(size_t)j * lines + f * ct + c] : zero;

@@ -26,3 +26,25 @@ def test_bf16_rounding_is_nearest_even():
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 ** -6
     assert r[3] == -2.5
     assert abs(r[4] - 3.0e-3) / 3.0e-3 < 2 ** -8
+
+
+def test_device_gelu_erf_constants_meet_the_published_bound():
+    """The device GELU evaluates erf by Abramowitz & Stegun 7.1.26 (|error| <=
+    1.5e-7); the constants in the CUDA header must reproduce that bound."""
+    import math
+    import os
+    import re
+    from tests.helpers import ROOT
+    src = open(os.path.join(ROOT, "pyspectral_b200", "csrc", "psb_mlp.cuh")).read()
+    body = src[src.index("struct GeluAS"):]
+    body = body[:body.index("};")]
+    c = {k: float(v) for k, v in re.findall(r"(p|a[1-5]) = (-?[0-9.]+)f", body)}
+    assert set(c) == {"p", "a1", "a2", "a3", "a4", "a5"}
+    x = np.linspace(-8, 8, 40001)
+    z = np.abs(x) / math.sqrt(2)
+    t = 1 / (1 + c["p"] * z)
+    poly = t * (c["a1"] + t * (c["a2"] + t * (c["a3"] + t * (c["a4"] + t * c["a5"]))))
+    q = poly * np.exp(-0.5 * x * x)
+    approx = np.where(x >= 0, 2 - q, q)
+    exact = 1 + np.array([math.erf(v / math.sqrt(2)) for v in x])
+    assert np.abs(approx - exact).max() < 1.5e-7
