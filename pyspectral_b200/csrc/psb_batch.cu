@@ -71,16 +71,43 @@ Dims dims(const psb_ctx* c, int Fi, int Fo) {
 }
 long long al(long long n) { return (n + 63) / 64 * 64; }
 
-// Every radix order of a length's factors (distinct permutations).
+// The fewest-pass schedule of n over radices {16, 12, 8, 6, 4, 3, 2}.
+std::vector<int> fewest_passes(int n) {
+  if (n == 1) return {};
+  std::vector<int> best;
+  bool found = false;
+  for (int r : {16, 12, 8, 6, 4, 3, 2}) {
+    if (n % r) continue;
+    std::vector<int> rest = fewest_passes(n / r);
+    if (n / r != 1 && rest.empty()) continue;
+    rest.insert(rest.begin(), r);
+    if (!found || rest.size() < best.size()) {
+      best = rest;
+      found = true;
+    }
+  }
+  return best;
+}
+
+// Candidate schedules of a length: every order of the default schedule's
+// radices and of the fewest-pass schedule's (distinct permutations).
 std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
-  std::vector<int> r(p.radix, p.radix + p.npass);
-  std::sort(r.begin(), r.end());
   std::vector<FFTPlan> out;
-  do {
-    FFTPlan q = p;
-    for (int s = 0; s < p.npass; ++s) q.radix[s] = r[s];
-    out.push_back(q);
-  } while (std::next_permutation(r.begin(), r.end()) && out.size() < 24);
+  auto add_perms = [&](std::vector<int> r) {
+    std::sort(r.begin(), r.end());
+    int n = 0;
+    do {
+      FFTPlan q = p;
+      q.npass = (int)r.size();
+      for (int s = 0; s < q.npass; ++s) q.radix[s] = r[s];
+      bool dup = false;
+      for (const FFTPlan& o : out)
+        if (o.npass == q.npass && std::equal(o.radix, o.radix + o.npass, q.radix)) dup = true;
+      if (!dup) out.push_back(q);
+    } while (std::next_permutation(r.begin(), r.end()) && ++n < 24);
+  };
+  add_perms(std::vector<int>(p.radix, p.radix + p.npass));
+  add_perms(fewest_passes(p.L));
   return out;
 }
 
@@ -276,14 +303,22 @@ struct Batch {
     constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
     return zpass_smem_bytes<T>(FMAX, P, d.M3, (size_t)phys_is_block<Phys>::extra);
   }
-  int launch(int pass, int stage) {
+  // radix 6/12/16 passes need the wide kernel instantiations
+  bool wide(int pass) const {
+    const FFTPlan& p = b->plan[pass];
+    for (int s = 0; s < p.npass; ++s)
+      if (p.radix[s] > 8 || p.radix[s] == 6) return true;
+    return false;
+  }
+  template <bool W>
+  int launch_w(int pass, int stage) {
     const size_t esz = sizeof(Cx<T>);
     switch (pass) {
       case 0: {
         const int ct = b->tile[0];
         dim3 g((d.Kz + ct - 1) / ct, d.N2, R);
         const size_t sm = smem_axis(d.M1, Fi, ct);
-        auto k = axis_pass_batch<T, true, Pre>;
+        auto k = axis_pass_batch<T, true, Pre, W>;
         set_smem(k, sm);
         LaunchScope s(c, "batch x-inverse", (double)R * esz * d.N2 * d.Kz * (3.0 * d.N1 + (double)Fi * d.M1));
         k<<<g, 256, sm, c->stream>>>(ax, pre);
@@ -298,12 +333,12 @@ struct Batch {
         const size_t sm = smem_axis(d.M2, 1, ct);
         const double by = (double)R * esz * F * d.M1 * d.Kz * (double)(d.N2 + d.M2);
         if (inv) {
-          auto k = axis_pass_batch<T, true, PreCopy<T>>;
+          auto k = axis_pass_batch<T, true, PreCopy<T>, W>;
           set_smem(k, sm);
           LaunchScope s(c, "batch y-inverse", by);
           k<<<g, 256, sm, c->stream>>>(ay, cpy);
         } else {
-          auto k = axis_pass_batch<T, false, PreCopy<T>>;
+          auto k = axis_pass_batch<T, false, PreCopy<T>, W>;
           set_smem(k, sm);
           LaunchScope s(c, "batch y-forward", by);
           k<<<g, 256, sm, c->stream>>>(ayf, cpy);
@@ -315,7 +350,7 @@ struct Batch {
         const long long np = (long long)d.M1 * d.M2;
         dim3 g((unsigned)((np + P - 1) / P), R);
         const size_t sm = smem_z(P);
-        auto k = zpass_batch<T, Phys>;
+        auto k = zpass_batch<T, Phys, W>;
         set_smem(k, sm);
         LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fi + Fo));
         k<<<g, 256, sm, c->stream>>>(az, phys);
@@ -329,7 +364,7 @@ struct Batch {
         const int extra = (int)std::min<long long>((pts + 255) / 256, 1024);
         dim3 g(mainb + extra, R);
         const size_t sm = smem_axis(d.M1, Fo, ct);
-        auto k = xfwd_epi_batch<T, Epi>;
+        auto k = xfwd_epi_batch<T, Epi, W>;
         set_smem(k, sm);
         const double by = (double)R * (esz * Fo * d.M1 * d.N2 * d.Kz + esz * 3.0 * d.N1 * d.N2 * d.N3h *
                                                                            (stage == 4 ? 2.0 : 3.0));
@@ -339,6 +374,8 @@ struct Batch {
       }
     }
   }
+
+  int launch(int pass, int stage) { return wide(pass) ? launch_w<true>(pass, stage) : launch_w<false>(pass, stage); }
 
   int step(int nsteps) {
     for (int s = 0; s < nsteps; ++s)

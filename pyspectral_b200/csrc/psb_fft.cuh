@@ -117,6 +117,81 @@ __device__ __forceinline__ void dft8(Cx<T>* v) {
   }
 }
 
+// cos and sin of 2 pi q / 48 from a quarter-wave table (steps of 7.5 degrees)
+struct Trig48 {
+  static constexpr double c[13] = {1.0,
+                                   0.99144486137381041114455,
+                                   0.96592582628906828674974,
+                                   0.92387953251128675612818,
+                                   0.86602540378443864676372,
+                                   0.79335334029123516457751,
+                                   0.70710678118654752440084,
+                                   0.60876142900872063941609,
+                                   0.5,
+                                   0.38268343236508977172846,
+                                   0.25881904510252076234890,
+                                   0.13052619222005159154840,
+                                   0.0};
+  static constexpr double cosq(int q) {
+    q = ((q % 48) + 48) % 48;
+    return q <= 12 ? c[q] : (q <= 24 ? -c[24 - q] : (q <= 36 ? -c[q - 24] : c[48 - q]));
+  }
+  static constexpr double sinq(int q) { return cosq(12 - q); }
+};
+
+// x * W_R^M, W_R = exp(-2 pi i / R) (conjugate for INV); 48 % R == 0
+template <typename T, bool INV, int M, int R>
+__device__ __forceinline__ Cx<T> twc(Cx<T> x) {
+  constexpr int q = (M * (48 / R)) % 48;
+  if constexpr (q == 0) {
+    return x;
+  } else {
+    constexpr T c = (T)Trig48::cosq(q), s = (T)Trig48::sinq(q);
+    return INV ? mk<T>(c * x.x - s * x.y, c * x.y + s * x.x) : mk<T>(c * x.x + s * x.y, c * x.y - s * x.x);
+  }
+}
+
+template <typename T, int R, bool INV>
+__device__ __forceinline__ void small_dft(Cx<T>* v);
+
+// R1 x R2 Cooley-Tukey in registers: X[k1 + R1 k2] =
+// sum_n2 W_R2^{n2 k2} W_R^{n2 k1} sum_n1 x[R2 n1 + n2] W_R1^{n1 k1}
+template <typename T, int R1, int R2, bool INV>
+struct DftCT {
+  static constexpr int R = R1 * R2;
+  template <int N2>
+  __device__ __forceinline__ static void col(const Cx<T>* v, Cx<T>* a) {
+    if constexpr (N2 < R2) {
+      Cx<T> u[R1];
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) u[n1] = v[R2 * n1 + N2];
+      small_dft<T, R1, INV>(u);
+      tw<N2, 0>(u, a);
+      col<N2 + 1>(v, a);
+    }
+  }
+  template <int N2, int K1>
+  __device__ __forceinline__ static void tw(const Cx<T>* u, Cx<T>* a) {
+    if constexpr (K1 < R1) {
+      a[N2 * R1 + K1] = twc<T, INV, N2 * K1, R>(u[K1]);
+      tw<N2, K1 + 1>(u, a);
+    }
+  }
+  __device__ __forceinline__ static void run(Cx<T>* v) {
+    Cx<T> a[R];
+    col<0>(v, a);
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      Cx<T> w[R2];
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) w[n2] = a[n2 * R1 + k1];
+      small_dft<T, R2, INV>(w);
+#pragma unroll
+      for (int k2 = 0; k2 < R2; ++k2) v[k1 + R1 * k2] = w[k2];
+    }
+  }
+};
+
 template <typename T, int R, bool INV>
 __device__ __forceinline__ void small_dft(Cx<T>* v) {
   if constexpr (R == 2) {
@@ -125,8 +200,15 @@ __device__ __forceinline__ void small_dft(Cx<T>* v) {
     dft3<T, INV>(v[0], v[1], v[2]);
   } else if constexpr (R == 4) {
     dft4<T, INV>(v[0], v[1], v[2], v[3]);
-  } else {
+  } else if constexpr (R == 8) {
     dft8<T, INV>(v);
+  } else if constexpr (R == 6) {
+    DftCT<T, 2, 3, INV>::run(v);
+  } else if constexpr (R == 12) {
+    DftCT<T, 4, 3, INV>::run(v);
+  } else {
+    static_assert(R == 16, "radix 2, 3, 4, 6, 8, 12 or 16");
+    DftCT<T, 4, 4, INV>::run(v);
   }
 }
 
@@ -192,18 +274,33 @@ __device__ __forceinline__ void stockham_pass(const Cx<T>* __restrict__ a, Cx<T>
 // result.  lines_fast selects the thread->work mapping: true when consecutive
 // lines are adjacent in memory (es > 1, ls == 1), false for contiguous lines.
 // Must be called by all threads of the CTA; ends with __syncthreads.
-template <typename T, bool INV>
+// WIDE compiles the radix 6/12/16 passes in as well (plans that use them must
+// run a WIDE instantiation); without it only 2/3/4/8 exist, which keeps the
+// register budget of every kernel at what radix 8 needs.
+template <typename T, bool INV, bool WIDE = false>
 __device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* __restrict__ tw,
                             int nlines, int ls, int es, bool lines_fast) {
   const int L = p.L;
   int Ns = 1;
   for (int s = 0; s < p.npass; ++s) {
     const int R = p.radix[s];
-    switch (R) {
-      case 8: stockham_pass<T, 8, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
-      case 4: stockham_pass<T, 4, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
-      case 3: stockham_pass<T, 3, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
-      default: stockham_pass<T, 2, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+    if constexpr (WIDE) {
+      switch (R) {
+        case 16: stockham_pass<T, 16, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 12: stockham_pass<T, 12, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 8: stockham_pass<T, 8, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 6: stockham_pass<T, 6, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 4: stockham_pass<T, 4, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 3: stockham_pass<T, 3, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        default: stockham_pass<T, 2, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+      }
+    } else {
+      switch (R) {
+        case 8: stockham_pass<T, 8, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 4: stockham_pass<T, 4, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        case 3: stockham_pass<T, 3, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+        default: stockham_pass<T, 2, INV>(a, b, tw, L, Ns, nlines, ls, es, lines_fast); break;
+      }
     }
     __syncthreads();
     Cx<T>* t = a;

@@ -122,7 +122,7 @@ struct PreCopy {
 
 // One CTA of an axis pass: column tile bx, outer index by.
 // smem = tw[L] + 2 * L*lines
-template <typename T, bool INV, class Pre>
+template <typename T, bool INV, class Pre, bool WIDE = false>
 __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -169,7 +169,7 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
     for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, INV>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  Cx<T>* res = block_fft<T, INV, WIDE>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
   Cx<T>* outb = a.out + (long long)o * a.out_ostride;
   if (!colok || threadIdx.x >= dr * ct) return;
   const int nrow = a.out_rows * Pre::F_DST;
@@ -188,9 +188,9 @@ __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) 
 
 // Batched: grid = (ceil(ncols/col_tile), nouter, runs); run blockIdx.z takes
 // its arguments from A[z] and pre[z] (same tile shape for every run).
-template <typename T, bool INV, class Pre>
+template <typename T, bool INV, class Pre, bool WIDE>
 __global__ void __launch_bounds__(256) axis_pass_batch(const AxisArgs<T>* __restrict__ A, const Pre* __restrict__ pre) {
-  axis_pass_body<T, INV>(A[blockIdx.z], pre[blockIdx.z], blockIdx.x, blockIdx.y);
+  axis_pass_body<T, INV, Pre, WIDE>(A[blockIdx.z], pre[blockIdx.z], blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -217,7 +217,7 @@ __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
 }
 
 // One CTA of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes
-template <typename T, class Phys>
+template <typename T, class Phys, bool WIDE = false>
 __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -265,7 +265,7 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
       }
     }
     __syncthreads();
-    R = block_fft<T, true>(X, Y, a.plan, tw, nin, M, 1, false);
+    R = block_fft<T, true, WIDE>(X, Y, a.plan, tw, nin, M, 1, false);
   }
   Cx<T>* W = (R == X) ? Y : X;
   const int nout = (FO * P + 1) / 2;
@@ -305,7 +305,7 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
   }
   if constexpr (FO > 0) {
     __syncthreads();
-    Cx<T>* R2 = block_fft<T, false>(W, R, a.plan, tw, nout, M, 1, false);
+    Cx<T>* R2 = block_fft<T, false, WIDE>(W, R, a.plan, tw, nout, M, 1, false);
     // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
     const int kzo = a.out_kz;
     for (Walk2 w(kzo); w.s < nout; w.next()) {
@@ -335,9 +335,9 @@ __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
 }
 
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
-template <typename T, class Phys>
+template <typename T, class Phys, bool WIDE>
 __global__ void __launch_bounds__(256) zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
-  zpass_body<T>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
+  zpass_body<T, Phys, WIDE>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -356,7 +356,7 @@ struct XEpiArgs {
 
 // One CTA of the x-forward epilogue pass: block bx of gx = main_blocks + extra;
 // main block b -> (col tile b % ntile, outer b / ntile)
-template <typename T, class Epi>
+template <typename T, class Epi, bool WIDE = false>
 __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& epi, int bx, int gx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int F = Epi::F_IN;
@@ -399,7 +399,7 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
     bufA[(size_t)j * lines + f * ct + c] = colok ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, false>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  Cx<T>* res = block_fft<T, false, WIDE>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
   // threads past the last full row of columns would repeat a (row, column)
   // (only when ct does not divide the CTA size): the epilogue is not idempotent
   if (!colok || threadIdx.x >= dr * ct) return;
@@ -418,9 +418,9 @@ __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
 }
 
 // Batched: grid = (main_blocks + extra, runs); run blockIdx.y reads A[y], epi[y].
-template <typename T, class Epi>
+template <typename T, class Epi, bool WIDE>
 __global__ void __launch_bounds__(256) xfwd_epi_batch(const XEpiArgs<T>* __restrict__ A, const Epi* __restrict__ epi) {
-  xfwd_epi_body<T>(A[blockIdx.y], epi[blockIdx.y], blockIdx.x, gridDim.x);
+  xfwd_epi_body<T, Epi, WIDE>(A[blockIdx.y], epi[blockIdx.y], blockIdx.x, gridDim.x);
 }
 
 }  // namespace psb

@@ -255,3 +255,46 @@ def test_cuda_graph_replay_equals_eager_steps(precision):
     assert torch.equal(a.Q, b.Q)
     assert torch.equal(a.U, b.U)
     del C
+
+
+@pytest.mark.parametrize("tm,fn", [(1, "rhs_smag"), (2, "rhs_tmodel")])
+def test_1000_step_histories_and_spectrum_match_oracle(tm, fn):
+    """1000 RK4 steps of decaying isotropic turbulence (E(k) ~ k^4 exp(-2k^2/k0^2),
+    k0 = 4, seed 1, nu = 1e-3, dt = 2e-3) at 16^3 in FP64: the energy and
+    dissipation histories (every step) and the final E(k) against the oracle
+    run of the same case.  Smagorinsky, and the t-model with t advancing."""
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advanceQ_RK4
+    N, nu, dt, nsteps = 16, 1e-3, 2e-3, 1000
+    st = orc.isotropic_state(N, 1, k0=4.0)
+    grid = C.gridclass.periodic(N)
+    main = C.variables(0, tm, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, dt, nu)
+    util = C.utilitiesClass()
+    g = orc.Grid.periodic(N)
+    rhs = getattr(orc, fn)
+    Q = st
+    E_gpu, D_gpu, E_cpu, D_cpu = [], [], [], []
+    t = 0.0
+    for n in range(nsteps):
+        main.t = t
+        advanceQ_RK4(main, grid, None, util)
+        ens, en, diss = util.computeAllStats(main, grid)[:3]
+        E_gpu.append(en)
+        D_gpu.append(diss)
+        p = orc.Params(nu=nu, t=t)
+        if fn == "rhs_smag":  # (rhs, w0); Smagorinsky reads the state as it is
+            step = lambda q: (rhs(g, q, p)[0], q)
+        else:  # (rhs, w0, uhat_read)
+            step = lambda q: (lambda o: (o[0], o[2]))(rhs(g, q, p))
+        Q, read = orc.advance_rk4(Q, step, dt)
+        E_cpu.append(orc.energy(g, read))
+        D_cpu.append(2 * nu * orc.enstrophy(g, read))
+        t += dt
+    assert rel(np.array(E_gpu), np.array(E_cpu)) < 1e-10
+    assert rel(np.array(D_gpu), np.array(D_cpu)) < 1e-10
+    assert E_gpu[-1] < E_gpu[0]  # decaying
+    Ek_gpu = np.abs(util.computeSpectrum(main, grid)[1])
+    Ek_cpu = np.abs(orc.spectrum(g, read)[1])
+    assert rel(Ek_gpu, Ek_cpu) < 1e-9
+    del torch
