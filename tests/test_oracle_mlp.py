@@ -48,3 +48,21 @@ def test_device_gelu_erf_constants_meet_the_published_bound():
     approx = np.where(x >= 0, 2 - q, q)
     exact = 1 + np.array([math.erf(v / math.sqrt(2)) for v in x])
     assert np.abs(approx - exact).max() < 1.5e-7
+
+
+def test_device_forward_gelu_erf_constants_meet_the_published_bound():
+    """The device forward GELU evaluates erf by Abramowitz & Stegun 7.1.28
+    (|error| <= 3e-7); the constants in the CUDA header must meet it."""
+    import math
+    import os
+    import re
+    from tests.helpers import ROOT
+    src = open(os.path.join(ROOT, "pyspectral_b200", "csrc", "psb_mlp.cuh")).read()
+    body = src[src.index("struct GeluAS28"):]
+    body = body[:body.index("};")]
+    c = {k: float(v) for k, v in re.findall(r"(a[1-6]) = (-?[0-9.]+)f", body)}
+    assert set(c) == {"a1", "a2", "a3", "a4", "a5", "a6"}
+    z = np.linspace(0, 8, 40001)
+    P = 1 + sum(c[f"a{i}"] * z ** i for i in range(1, 7))
+    exact = np.array([math.erf(v) for v in z])
+    assert np.abs((1 - P ** -16.0) - exact).max() < 3e-7
