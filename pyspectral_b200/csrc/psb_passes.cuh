@@ -238,10 +238,10 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
   Cx<T>* R = X;
   if constexpr (FI > 0) {
     const int nin = (FI * P + 1) / 2;
-    for (int idx = threadIdx.x; idx < nin * M; idx += blockDim.x) X[idx] = zero;
-    __syncthreads();
     // pack pairs of Hermitian half-spectra: Z = A + iB, Z[M-k] = conj(A_k) + i conj(B_k);
-    // the k=0 and k=M/2 terms keep their real parts only (c2r convention)
+    // the k=0 and k=M/2 terms keep their real parts only (c2r convention).  The
+    // items k = 0..M/2 of every packed line write all M positions of the line
+    // (zero where k is beyond the stored k3 range), so nothing needs clearing.
     for (Walk2 w(half + 1); w.s < nin; w.next()) {
       const int k = w.f, c = w.s;
       Cx<T> A = zero, B = zero;
