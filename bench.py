@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--N", type=int, default=64)
     ap.add_argument("--closure", choices=["learned", "smag", "dns"], default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of autotuned ones")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup+steps plain RK4 steps of the headline case and exit (for ncu captures)")
     return ap.parse_args()
@@ -290,7 +291,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     from pyspectral_b200 import _capi
     from pyspectral_b200 import Classes as C
-    from pyspectral_b200.RHSfunctions import StepGraph, advance
+    from pyspectral_b200.RHSfunctions import StepGraph, advance, autotune
 
     N = args.N
     st64 = make_state(N, 1 + rank)
@@ -305,6 +306,8 @@ def run_ours(args):
         grid = C.gridclass.periodic(N, device=local)
         main = C.variables(0, tm, 0, 0, 0, 0, grid, st64[0], st64[1], st64[2], 0.0, 2e-3, 1e-3,
                            precision=precision, model=model if closure == "learned" else None)
+        if closure in ("learned", "smag", "dns") and not args.no_tune:
+            autotune(main, grid)  # launch shapes timed on this state (state untouched)
         grid.ctx(precision).prepare(main.closure_code())
         return grid, main
 
@@ -430,7 +433,9 @@ def run_ours(args):
                                    f"1+rank), {args.closure} closure, RK4 dt=2e-3, nu=1e-3, FP32 fields + Kahan "
                                    f"stage accumulation", "N": N,
                        "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)",
-                       "launch": "one CUDA graph per RK4 step", "parallelism": f"replicas x{world}"},
+                       "launch": "one CUDA graph per RK4 step", "parallelism": f"replicas x{world}",
+                       "launch_shapes": "default" if args.no_tune else
+                       "autotuned per path (psb_autotune: tiles and radix orders timed on the state)"},
             "fp64_plain": {"value": value64, "ms_per_step": ms64 / K64, "closure": plain,
                            "ratio_headline_over_fp64_plain": value / value64},
             "fp32_plain": plain32,

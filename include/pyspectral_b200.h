@@ -219,6 +219,18 @@ int psb_batch_step_rk4(psb_batch* b, int nsteps);
 int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int maxr);
 int psb_batch_destroy(psb_batch* b);
 
+/* ---- autotuned single runs (no reference counterpart) --------------------
+ * Time the candidate launch shapes of the five passes of closure's RHS
+ * (PSB_DNS, PSB_SMAG or PSB_LEARNED) on `state` (not modified) with params p,
+ * and keep the fastest in ctx: later psb_rhs / psb_step_rk4 calls of that
+ * closure use them.  Results differ from the untuned ones only by rounding
+ * (other radix orders). */
+int psb_autotune(psb_ctx* ctx, int closure, void* state, const psb_params* p);
+/* The tuned shape of pass 0..4 of closure (tile 0 when not tuned). */
+int psb_tuned_shape(const psb_ctx* ctx, int closure, int pass, int* tile, int* radices, int maxr);
+/* Back to the default shapes for closure. */
+int psb_autotune_clear(psb_ctx* ctx, int closure);
+
 #ifdef __cplusplus
 }
 #endif

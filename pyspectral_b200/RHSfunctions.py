@@ -69,6 +69,12 @@ def advanceQ_RK4(main, grid, myFFT=None, utilities=None):
         utilities.postAdvanceQ_hook(main, grid, myFFT)
 
 
+def autotune(main, grid):
+    """Tune the launch shapes of main's closure on its current state (no
+    reference counterpart; DNS, Smagorinsky and the learned closure)."""
+    grid.ctx(main.precision).autotune(main.closure_code(), main.Q, main.params())
+
+
 def advance(main, grid, nsteps):
     """``nsteps`` fixed-dt RK4 steps in one call (no per-step host work)."""
     ctx = grid.ctx(main.precision)

@@ -26,7 +26,7 @@ EXPORTS = (
     "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
-    "psb_batch_destroy",
+    "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear",
 )
 
 
@@ -84,6 +84,9 @@ def load(path: str = LIB_PATH):
         "psb_timing_count": ([vp, ip], i),
         "psb_timing_get": ([vp, i, ctypes.c_char_p, i, dp, dp], i),
         "psb_rhs_dns_noalloc": ([vp, vp, vp, ctypes.POINTER(Params)], i),
+        "psb_autotune": ([vp, i, vp, ctypes.POINTER(Params)], i),
+        "psb_tuned_shape": ([vp, i, i, ip, ip, i], i),
+        "psb_autotune_clear": ([vp, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -236,6 +239,24 @@ class Context:
     def c2r(self, spec, phys, nfields):
         self.bind_stream()
         self.check(self.lib.psb_fft_c2r(self.h, self._ptr(spec), self._ptr(phys), int(nfields)), "psb_fft_c2r")
+
+    def autotune(self, closure, state, params):
+        """Pick the fastest launch shapes of closure's RHS passes on `state`
+        (unchanged) and use them for this closure from now on."""
+        self.bind_stream()
+        self.check(self.lib.psb_autotune(self.h, closure, self._ptr(state), ctypes.byref(params)), "psb_autotune")
+
+    def tuned_shapes(self, closure):
+        out = []
+        for p in range(5):
+            t = ctypes.c_int()
+            rad = (ctypes.c_int * 12)()
+            self.check(self.lib.psb_tuned_shape(self.h, closure, p, ctypes.byref(t), rad, 12), "psb_tuned_shape")
+            out.append({"tile": t.value, "radices": [x for x in rad if x]})
+        return out
+
+    def autotune_clear(self, closure):
+        self.check(self.lib.psb_autotune_clear(self.h, closure), "psb_autotune_clear")
 
     def launch_count(self):
         n = ctypes.c_ulonglong()

@@ -591,6 +591,52 @@ int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int m
   return PSB_OK;
 }
 
+// Single runs: tune a one-run batch on the caller's state (RHS mode, state
+// untouched) and keep its shapes in the context for psb_rhs / psb_step_rk4.
+int psb_autotune(psb_ctx* c, int closure, void* state, const psb_params* p) {
+  if (!c) return PSB_ERR_ARG;
+  if (!state || !p) return fail(c, PSB_ERR_ARG, "psb_autotune: null argument");
+  if (closure != PSB_DNS && closure != PSB_SMAG && closure != PSB_LEARNED)
+    return fail(c, PSB_ERR_UNSUPPORTED, "psb_autotune: closure not tunable (DNS, SMAG, LEARNED are)");
+  psb_batch* b = nullptr;
+  PSB_TRY(psb_batch_create(c, closure, 1, &b));
+  int st = psb_batch_set_run(b, 0, state, nullptr, p);
+  if (st == PSB_OK) st = psb_batch_autotune(b);
+  if (st == PSB_OK) {
+    psb_tuned t;
+    for (int k = 0; k < 5; ++k) {
+      t.pass[k].tile = b->tile[k];
+      t.pass[k].plan = b->plan[k];
+      bool wide = false;
+      for (int s = 0; s < b->plan[k].npass; ++s) wide |= b->plan[k].radix[s] > 8 || b->plan[k].radix[s] == 6;
+      t.pass[k].wide = wide;
+    }
+    c->tuned[closure] = t;
+  }
+  psb_batch_destroy(b);
+  return st;
+}
+
+int psb_tuned_shape(const psb_ctx* c, int closure, int pass, int* tile, int* radices, int maxr) {
+  if (!c || pass < 0 || pass > 4 || !tile) return PSB_ERR_ARG;
+  const auto it = c->tuned.find(closure);
+  if (it == c->tuned.end()) {
+    *tile = 0;
+    for (int s = 0; s < maxr; ++s) radices[s] = 0;
+    return PSB_OK;
+  }
+  const psb_pass_shape& sh = it->second.pass[pass];
+  *tile = sh.tile;
+  for (int s = 0; s < maxr; ++s) radices[s] = s < sh.plan.npass ? sh.plan.radix[s] : 0;
+  return PSB_OK;
+}
+
+int psb_autotune_clear(psb_ctx* c, int closure) {
+  if (!c) return PSB_ERR_ARG;
+  c->tuned.erase(closure);
+  return PSB_OK;
+}
+
 int psb_batch_destroy(psb_batch* b) {
   if (!b) return PSB_ERR_ARG;
   cudaSetDevice(b->c->dev);

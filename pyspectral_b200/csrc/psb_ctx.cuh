@@ -13,6 +13,20 @@
 #include "../../include/pyspectral_b200.h"
 #include "psb_physics.cuh"
 
+// Launch shape of one pass picked by the autotuner: tile (columns per CTA, or
+// pencils per CTA for the z pass), its transform's radix order, and whether
+// that order needs the wide (radix 6/12/16) kernels.
+struct psb_pass_shape {
+  int tile = 0;
+  psb::FFTPlan plan{};
+  bool wide = false;
+};
+// Shapes of the five passes (x-inverse, y-inverse, z, y-forward, x-forward) of
+// a 3/2-padded closure's RHS.
+struct psb_tuned {
+  psb_pass_shape pass[5];
+};
+
 struct psb_ctx {
   int N1 = 0, N2 = 0, N3 = 0, N3h = 0;
   int prec = 64;
@@ -35,6 +49,7 @@ struct psb_ctx {
     size_t bytes = 0;
   };
   std::map<std::string, Buf> scratch;
+  std::map<int, psb_tuned> tuned;  // autotuned launch shapes by closure (psb_autotune)
   double* red_dev = nullptr;   // reduction partials
   double* red_host = nullptr;  // pinned
   size_t red_cap = 0;
@@ -202,24 +217,39 @@ inline int pick_ct(int ncols, int F, int L, size_t esz, int nouter = 0) {
   return ct;
 }
 
-template <typename T, bool INV, class Pre>
-int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what) {
+// sh: an autotuned shape (TUNABLE launch sites only) or null for the default
+template <typename T, bool INV, class Pre, bool TUNABLE = false>
+int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const psb_pass_shape* sh = nullptr) {
   const size_t esz = sizeof(Cx<T>);
   const int L = a.plan.L;
   a.col_tile = pick_ct(a.ncols, Pre::F_DST, L, esz, a.nouter);
+  if (sh && sh->tile) {
+    a.col_tile = sh->tile;
+    a.plan = sh->plan;
+  }
   const size_t smem = (size_t)(L + 2 * L * Pre::F_DST * a.col_tile) * esz;
   dim3 grid((a.ncols + a.col_tile - 1) / a.col_tile, a.nouter);
-  auto k = psb::axis_pass_kernel<T, INV, Pre>;
-  set_smem(k, smem);
   const double bytes = (double)esz * a.nouter * a.ncols *
                        ((double)Pre::F_SRC * count_mapped(a.in_map, a.in_rows) + (double)Pre::F_DST * a.out_rows);
+  if constexpr (TUNABLE) {
+    if (sh && sh->wide) {
+      auto k = psb::axis_pass_kernel<T, INV, Pre, true>;
+      set_smem(k, smem);
+      LaunchScope scope(c, what, bytes);
+      k<<<grid, 256, smem, c->stream>>>(a, pre);
+      return launch_ok(c, what);
+    }
+  }
+  auto k = psb::axis_pass_kernel<T, INV, Pre>;
+  set_smem(k, smem);
   LaunchScope scope(c, what, bytes);
   k<<<grid, 256, smem, c->stream>>>(a, pre);
   return launch_ok(c, what);
 }
 
-template <typename T, class Phys>
-int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double extra_bytes = 0.0) {
+template <typename T, class Phys, bool TUNABLE = false>
+int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double extra_bytes = 0.0,
+             const psb_pass_shape* sh = nullptr) {
   const size_t esz = sizeof(Cx<T>);
   const int M = z.plan.L;
   constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
@@ -229,24 +259,41 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   int P = psb::phys_max_ppc<Phys>::value;
   while (P > 1 && smem_for(P) > kSmemBudget) P /= 2;
   while (P > 1 && (z.npencils + P - 1) / P < 2 * 148) P /= 2;
+  if (sh && sh->tile) {
+    P = sh->tile;
+    z.plan = sh->plan;
+  }
   z.ppc = P;
   const size_t smem = smem_for(P);
   const long long grid = (z.npencils + P - 1) / P;
-  auto k = psb::zpass_kernel<T, Phys>;
-  set_smem(k, smem);
   double bytes = extra_bytes + (double)esz * z.npencils * Phys::F_OUT * z.out_kz;
   for (int f = 0; f < Phys::F_IN; ++f) bytes += (double)esz * z.npencils * z.in_kz[f];
+  if constexpr (TUNABLE) {
+    if (sh && sh->wide) {
+      auto k = psb::zpass_kernel<T, Phys, true>;
+      set_smem(k, smem);
+      LaunchScope scope(c, what, bytes);
+      k<<<(unsigned)grid, 256, smem, c->stream>>>(z, phys);
+      return launch_ok(c, what);
+    }
+  }
+  auto k = psb::zpass_kernel<T, Phys>;
+  set_smem(k, smem);
   LaunchScope scope(c, what, bytes);
   k<<<(unsigned)grid, 256, smem, c->stream>>>(z, phys);
   return launch_ok(c, what);
 }
 
 // bytes: the transform input plus the epilogue's own state traffic (epi.io_bytes)
-template <typename T, class Epi>
-int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what) {
+template <typename T, class Epi, bool TUNABLE = false>
+int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const psb_pass_shape* sh = nullptr) {
   const size_t esz = sizeof(Cx<T>);
   const int L = e.plan.L;
   e.col_tile = pick_ct(e.kz, Epi::F_IN, L, esz, e.n2);
+  if (sh && sh->tile) {
+    e.col_tile = sh->tile;
+    e.plan = sh->plan;
+  }
   const int ntile = (e.kz + e.col_tile - 1) / e.col_tile;
   e.main_blocks = ntile * e.n2;
   int extra = 0;
@@ -255,9 +302,18 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what) {
     extra = (int)std::min<long long>((pts + 255) / 256, 1024);
   }
   const size_t smem = (size_t)(L + 2 * L * Epi::F_IN * e.col_tile) * esz;
+  const double bytes = epi.io_bytes((long long)e.n1 * e.n2 * e.n3h) + (double)esz * Epi::F_IN * L * e.n2 * e.kz;
+  if constexpr (TUNABLE) {
+    if (sh && sh->wide) {
+      auto k = psb::xfwd_epi_kernel<T, Epi, true>;
+      set_smem(k, smem);
+      LaunchScope scope(c, what, bytes);
+      k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
+      return launch_ok(c, what);
+    }
+  }
   auto k = psb::xfwd_epi_kernel<T, Epi>;
   set_smem(k, smem);
-  const double bytes = epi.io_bytes((long long)e.n1 * e.n2 * e.n3h) + (double)esz * Epi::F_IN * L * e.n2 * e.kz;
   LaunchScope scope(c, what, bytes);
   k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
   return launch_ok(c, what);

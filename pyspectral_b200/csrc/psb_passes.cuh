@@ -181,9 +181,9 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
 }
 
 // grid = (ceil(ncols/col_tile), nouter)
-template <typename T, bool INV, class Pre>
+template <typename T, bool INV, class Pre, bool WIDE = false>
 __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
-  axis_pass_body<T, INV>(a, pre, blockIdx.x, blockIdx.y);
+  axis_pass_body<T, INV, Pre, WIDE>(a, pre, blockIdx.x, blockIdx.y);
 }
 
 // Batched: grid = (ceil(ncols/col_tile), nouter, runs); run blockIdx.z takes
@@ -329,9 +329,9 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
 }
 
 // grid = ceil(npencils/ppc)
-template <typename T, class Phys>
+template <typename T, class Phys, bool WIDE = false>
 __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
-  zpass_body<T>(a, phys, blockIdx.x);
+  zpass_body<T, Phys, WIDE>(a, phys, blockIdx.x);
 }
 
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
@@ -412,9 +412,9 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
 }
 
 // grid = main_blocks + extra
-template <typename T, class Epi>
+template <typename T, class Epi, bool WIDE = false>
 __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
-  xfwd_epi_body<T>(a, epi, blockIdx.x, gridDim.x);
+  xfwd_epi_body<T, Epi, WIDE>(a, epi, blockIdx.x, gridDim.x);
 }
 
 // Batched: grid = (main_blocks + extra, runs); run blockIdx.y reads A[y], epi[y].

@@ -32,8 +32,12 @@ AxisArgs<T> axis_common(psb_ctx* c, int L) {
 // ---------------------------------------------------------------------------
 // 3/2-padded Navier-Stokes (DNS, Smagorinsky, SGS of filtered DNS)
 // ---------------------------------------------------------------------------
+// ts: autotuned launch shapes of the five passes (psb_autotune), or null
 template <typename T, class Pre, class Phys, class Epi>
-int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
+int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const psb_tuned* ts = nullptr) {
+  const psb_pass_shape* sh[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  if (ts)
+    for (int k = 0; k < 5; ++k) sh[k] = &ts->pass[k];
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
   constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
@@ -66,7 +70,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   a.k_row = c->kx;
   a.k_outer = c->ky;
   a.k_col = c->kz;
-  PSB_TRY((launch_axis<T, true>(c, a, pre, "x-inverse")));
+  PSB_TRY((launch_axis<T, true, Pre, true>(c, a, pre, "x-inverse", sh[0])));
   // y inverse (fields folded into the outer index)
   AxisArgs<T> b = axis_common<T>(c, M2);
   b.in = A;
@@ -81,7 +85,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   b.out_rows = M2;
   b.in_map = map_pad32(N2);
   b.out_map = map_id(M2);
-  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "y-inverse")));
+  PSB_TRY((launch_axis<T, true, PreCopy<T>, true>(c, b, PreCopy<T>{}, "y-inverse", sh[1])));
   // fused z
   ZArgs<T> z{};
   const long long fsP = (long long)M1 * M2 * Kz;
@@ -100,7 +104,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   z.fac = (T)(s32 / ((double)M1 * M2 * M3));
   z.plan = *plan_for(c, M3);
   z.tw = twiddles<T>(c);
-  PSB_TRY(launch_z<T>(c, z, phys, "z-fused"));
+  PSB_TRY((launch_z<T, Phys, true>(c, z, phys, "z-fused", 0.0, sh[2])));
   // y forward with truncation
   AxisArgs<T> d = axis_common<T>(c, M2);
   d.in = C;
@@ -115,7 +119,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   d.out_rows = N2;
   d.in_map = map_id(M2);
   d.out_map = map_pad32(N2);
-  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "y-forward")));
+  PSB_TRY((launch_axis<T, false, PreCopy<T>, true>(c, d, PreCopy<T>{}, "y-forward", sh[3])));
   // x forward + epilogue
   XEpiArgs<T> e{};
   e.in = D;
@@ -129,7 +133,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   e.out_map = map_pad32(N1);
   e.plan = *plan_for(c, M1);
   e.tw = twiddles<T>(c);
-  return launch_epi<T>(c, e, epi, "x-forward+epilogue");
+  return launch_epi<T, Epi, true>(c, e, epi, "x-forward+epilogue", sh[4]);
 }
 
 // Products of u and of the sharp-cutoff filtered u for computeSGS_DNS
@@ -768,6 +772,8 @@ int dtau_rhs_f(psb_ctx* c, StepIO<float> io, const psb_params* p, double* tau_ou
 template <typename T>
 int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, double* tau_out) {
   const Cx<T>* Qin = io.Q;
+  const auto tit = c->tuned.find(closure);
+  const psb_tuned* ts = tit == c->tuned.end() ? nullptr : &tit->second;
   switch (closure) {
     case PSB_DNS:
     case PSB_SMAG: {
@@ -776,11 +782,11 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
         EpiNS<T, true> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
                            (T)p->Om3, 0, c->N1 / 2, c->N2 / 2, c->N3 / 2};
         const double csd2 = 0.16 * c->Delta * 0.16 * c->Delta;
-        return run_ns32<T>(c, Qin, PreStrain<T>{}, PhysSmag<T>{(T)csd2}, epi);
+        return run_ns32<T>(c, Qin, PreStrain<T>{}, PhysSmag<T>{(T)csd2}, epi, ts);
       }
       EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
                           (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
-      return run_ns32<T>(c, Qin, PreCopyN<T, 3>{}, PhysProducts<T>{}, epi);
+      return run_ns32<T>(c, Qin, PreCopyN<T, 3>{}, PhysProducts<T>{}, epi, ts);
     }
     case PSB_MHD: {
       EpiMHD<T> epi{io, ktabs<T>(c->kx, c->ky, c->kz), c->mx, c->my, c->mz,
@@ -837,7 +843,7 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
       PhysLearned<T> phys{reinterpret_cast<const float*>(p->mlp_params), reinterpret_cast<const float*>(p->mlp_norm),
                           (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta)};
-      return run_ns32<T>(c, Qin, PreGrad<T>{}, phys, epi);
+      return run_ns32<T>(c, Qin, PreGrad<T>{}, phys, epi, ts);
     }
     default:
       return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");

@@ -97,3 +97,36 @@ def test_uneven_ensemble_in_one_graph():
     assert all(bool(torch.isfinite(torch.view_as_real(s)).all()) for s in after)
     assert all(not torch.equal(a, b) for a, b in zip(after, before))
     assert {g["closure"] for g in ens.groups} == {"learned", "smag"}
+
+
+@pytest.mark.parametrize("closure,precision,tol", [("smag", 64, 1e-12), ("dns", 64, 1e-12), ("learned", 32, 5e-5)])
+def test_autotuned_single_run_matches_default_shapes(closure, precision, tol):
+    """psb_autotune picks other tiles and radix orders for a single run's
+    passes; the RHS and two RK4 steps stay equal to the default shapes' up to
+    rounding, and the state is not touched by tuning."""
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advance, autotune
+    from pyspectral_b200.initial_conditions import isotropic_state
+    from pyspectral_b200.learned import MLPModel
+    N = 32
+    model = MLPModel.load() if closure == "learned" else None
+    tm = {"dns": 0, "smag": 1, "learned": "learned"}[closure]
+    st = isotropic_state(N, 4, k0=3.0)
+    out = []
+    for tune in (False, True):
+        grid = C.gridclass.periodic(N)
+        main = C.variables(0, tm, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 2e-3, 1e-3, precision=precision,
+                           model=model)
+        if tune:
+            q0 = main.Q.clone()
+            autotune(main, grid)
+            assert torch.equal(main.Q, q0)
+            sh = grid.ctx(precision).tuned_shapes(main.closure_code())
+            assert all(s["tile"] > 0 for s in sh)
+        rhs = torch.empty_like(main.Q)
+        grid.ctx(precision).rhs(main.closure_code(), main.Q, rhs, main.params())
+        advance(main, grid, 2)
+        out.append((np_(rhs), np_(main.Q)))
+    assert rel(out[1][0], out[0][0]) < tol
+    assert rel(out[1][1], out[0][1]) < tol
