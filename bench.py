@@ -439,6 +439,7 @@ def run_ours(args):
             "fp64_plain": {"value": value64, "ms_per_step": ms64 / K64, "closure": plain,
                            "ratio_headline_over_fp64_plain": value / value64},
             "fp32_plain": plain32,
+            "tuned_shapes": None if args.no_tune else grid32.ctx(32).tuned_shapes(m32.closure_code()),
             "accuracy": accuracy_record(args.closure, model),
             "cufft_library_baseline": {"value": N ** 3 / (cufft_ms / 1e3), "ms_per_step": cufft_ms,
                                        "what": f"FP32 {plain} step from torch.fft (cuFFT) + torch elementwise ops"},

@@ -7,8 +7,9 @@
 // Launch shapes are chosen by an autotuner: for every pass it times the
 // candidate column tiles (x/y passes), pencils per CTA (z-pass) and radix
 // orders of the transform length on the batch's own data, and keeps the
-// fastest.  Timing runs the passes in RHS mode into scratch, so tuning leaves
-// the runs' states untouched.
+// fastest.  Timing reads the runs' states and writes only scratch (the last
+// pass runs a middle-stage update on scratch copies), so tuning leaves the
+// runs' states untouched.
 #include <algorithm>
 #include <array>
 #include <cstring>
@@ -71,46 +72,6 @@ Dims dims(const psb_ctx* c, int Fi, int Fo) {
 }
 long long al(long long n) { return (n + 63) / 64 * 64; }
 
-// The fewest-pass schedule of n over radices {16, 12, 8, 6, 4, 3, 2}.
-std::vector<int> fewest_passes(int n) {
-  if (n == 1) return {};
-  std::vector<int> best;
-  bool found = false;
-  for (int r : {16, 12, 8, 6, 4, 3, 2}) {
-    if (n % r) continue;
-    std::vector<int> rest = fewest_passes(n / r);
-    if (n / r != 1 && rest.empty()) continue;
-    rest.insert(rest.begin(), r);
-    if (!found || rest.size() < best.size()) {
-      best = rest;
-      found = true;
-    }
-  }
-  return best;
-}
-
-// Candidate schedules of a length: every order of the default schedule's
-// radices and of the fewest-pass schedule's (distinct permutations).
-std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
-  std::vector<FFTPlan> out;
-  auto add_perms = [&](std::vector<int> r) {
-    std::sort(r.begin(), r.end());
-    int n = 0;
-    do {
-      FFTPlan q = p;
-      q.npass = (int)r.size();
-      for (int s = 0; s < q.npass; ++s) q.radix[s] = r[s];
-      bool dup = false;
-      for (const FFTPlan& o : out)
-        if (o.npass == q.npass && std::equal(o.radix, o.radix + o.npass, q.radix)) dup = true;
-      if (!dup) out.push_back(q);
-    } while (std::next_permutation(r.begin(), r.end()) && ++n < 24);
-  };
-  add_perms(std::vector<int>(p.radix, p.radix + p.npass));
-  add_perms(fewest_passes(p.L));
-  return out;
-}
-
 template <typename T, class Pre, class Phys, class Epi>
 struct Batch {
   static constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
@@ -125,7 +86,7 @@ struct Batch {
   Pre* pre;
   PreCopy<T>* cpy;
   Phys* phys;
-  Epi* epi;  // [5][R]: stages 0..3, then RHS mode into scratch (tuning)
+  Epi* epi;  // [5][R]: stages 0..3, then a middle stage on scratch copies (tuning)
 
   static size_t arg_bytes(int R) {
     return al(sizeof(AxisArgs<T>) * R) * 3 + al(sizeof(ZArgs<T>) * R) + al(sizeof(XEpiArgs<T>) * R) +
@@ -278,9 +239,13 @@ struct Batch {
           io.mode = i == 0 ? kStage1 : (i == 3 ? kStageLast : kStageMid);
           io.dtc = (T)(b->params[r].dt * rk[i]);
         } else {
-          io.mode = kRHS;
-          io.rhs_out = run_buf(r, 5);
-          io.comp = nullptr;
+          // tuning: the traffic of a middle RK stage (state, Q0 and the
+          // compensation read, state written) on scratch copies only
+          io.mode = kStageMid;
+          io.dtc = (T)(b->params[r].dt * rk[1]);
+          io.Q = run_buf(r, 5);
+          io.Q0 = run_buf(r, 4);
+          io.comp = b->comp[r] ? run_buf(r, 5) : nullptr;
         }
         epi[i * R + r] = mkepi(c, io, b->params[r]);
       }
@@ -367,7 +332,7 @@ struct Batch {
         auto k = xfwd_epi_batch<T, Epi, W>;
         set_smem(k, sm);
         const double by = (double)R * (esz * Fo * d.M1 * d.N2 * d.Kz + esz * 3.0 * d.N1 * d.N2 * d.N3h *
-                                                                           (stage == 4 ? 2.0 : 3.0));
+                                                                           3.0);
         LaunchScope s(c, "batch x-forward+epilogue", by);
         k<<<g, 256, sm, c->stream>>>(ae, epi + (size_t)stage * R);
         return launch_ok(c, "batch x-forward+epilogue");
@@ -422,16 +387,22 @@ struct Batch {
           if (ct <= std::max(2, 2 * d.Kz) && smem_axis(Ls[pass], Fs[pass], ct) <= kSmemBudget) tiles.push_back(ct);
       }
       const std::vector<FFTPlan> orders = radix_orders(*plan_for(c, Ls[pass]));
-      float best = 1e30f;
-      int bt = b->tile[pass];
-      FFTPlan bp = b->plan[pass];
+      // the default shape is the incumbent; a candidate must beat it by 3%,
+      // and the winner is re-timed against it before it is kept
+      const int t0 = b->tile[pass];
+      const FFTPlan p0 = b->plan[pass];
+      float base = 0;
+      PSB_TRY(time_pass(pass, 8, &base));
+      float best = 0.97f * base;
+      int bt = t0;
+      FFTPlan bp = p0;
       for (int t : tiles)
         for (const FFTPlan& q : orders) {
           b->tile[pass] = t;
           b->plan[pass] = q;
           PSB_TRY(build(pre0, mkphys, mkepi));
           float ms = 0;
-          PSB_TRY(time_pass(pass, 3, &ms));
+          PSB_TRY(time_pass(pass, 6, &ms));
           if (ms < best) {
             best = ms;
             bt = t;
@@ -441,6 +412,19 @@ struct Batch {
       b->tile[pass] = bt;
       b->plan[pass] = bp;
       PSB_TRY(build(pre0, mkphys, mkepi));
+      if (bt != t0 || bp.npass != p0.npass || !std::equal(bp.radix, bp.radix + bp.npass, p0.radix)) {
+        float again = 0, def = 0;
+        PSB_TRY(time_pass(pass, 10, &again));
+        b->tile[pass] = t0;
+        b->plan[pass] = p0;
+        PSB_TRY(build(pre0, mkphys, mkepi));
+        PSB_TRY(time_pass(pass, 10, &def));
+        if (again < 0.98f * def) {
+          b->tile[pass] = bt;
+          b->plan[pass] = bp;
+          PSB_TRY(build(pre0, mkphys, mkepi));
+        }
+      }
     }
     (void)esz;
     b->tuned = true;
@@ -481,6 +465,9 @@ void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int max_ppc, size_
   int P = max_ppc;
   auto sm = [&](int P) { return (size_t)(d.M3 + 2 * (size_t)((FMAX * P + 1) / 2) * d.M3) * esz + zextra; };
   while (P > 1 && sm(P) > kSmemBudget) P /= 2;
+  // at least ~2 CTAs per SM over the whole batch (the single-run rule at nruns = 1)
+  const long long np = (long long)d.M1 * d.M2;
+  while (P > 1 && (np + P - 1) / P * b->nruns < 2 * 148) P /= 2;
   b->tile[2] = P;
   b->plan[0] = *plan_for(c, d.M1);
   b->plan[1] = *plan_for(c, d.M2);
@@ -589,32 +576,6 @@ int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int m
   const FFTPlan& p = b->plan[pass];
   for (int s = 0; s < maxr; ++s) radices[s] = s < p.npass ? p.radix[s] : 0;
   return PSB_OK;
-}
-
-// Single runs: tune a one-run batch on the caller's state (RHS mode, state
-// untouched) and keep its shapes in the context for psb_rhs / psb_step_rk4.
-int psb_autotune(psb_ctx* c, int closure, void* state, const psb_params* p) {
-  if (!c) return PSB_ERR_ARG;
-  if (!state || !p) return fail(c, PSB_ERR_ARG, "psb_autotune: null argument");
-  if (closure != PSB_DNS && closure != PSB_SMAG && closure != PSB_LEARNED)
-    return fail(c, PSB_ERR_UNSUPPORTED, "psb_autotune: closure not tunable (DNS, SMAG, LEARNED are)");
-  psb_batch* b = nullptr;
-  PSB_TRY(psb_batch_create(c, closure, 1, &b));
-  int st = psb_batch_set_run(b, 0, state, nullptr, p);
-  if (st == PSB_OK) st = psb_batch_autotune(b);
-  if (st == PSB_OK) {
-    psb_tuned t;
-    for (int k = 0; k < 5; ++k) {
-      t.pass[k].tile = b->tile[k];
-      t.pass[k].plan = b->plan[k];
-      bool wide = false;
-      for (int s = 0; s < b->plan[k].npass; ++s) wide |= b->plan[k].radix[s] > 8 || b->plan[k].radix[s] == 6;
-      t.pass[k].wide = wide;
-    }
-    c->tuned[closure] = t;
-  }
-  psb_batch_destroy(b);
-  return st;
 }
 
 int psb_tuned_shape(const psb_ctx* c, int closure, int pass, int* tile, int* radices, int maxr) {

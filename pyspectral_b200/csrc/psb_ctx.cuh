@@ -319,6 +319,46 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
   return launch_ok(c, what);
 }
 
+// The fewest-pass schedule of n over radices {16, 12, 8, 6, 4, 3, 2}.
+inline std::vector<int> fewest_passes(int n) {
+  if (n == 1) return {};
+  std::vector<int> best;
+  bool found = false;
+  for (int r : {16, 12, 8, 6, 4, 3, 2}) {
+    if (n % r) continue;
+    std::vector<int> rest = fewest_passes(n / r);
+    if (n / r != 1 && rest.empty()) continue;
+    rest.insert(rest.begin(), r);
+    if (!found || rest.size() < best.size()) {
+      best = rest;
+      found = true;
+    }
+  }
+  return best;
+}
+
+// Candidate schedules of a length: every order of the default schedule's
+// radices and of the fewest-pass schedule's (distinct permutations).
+inline std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
+  std::vector<FFTPlan> out;
+  auto add_perms = [&](std::vector<int> r) {
+    std::sort(r.begin(), r.end());
+    int n = 0;
+    do {
+      FFTPlan q = p;
+      q.npass = (int)r.size();
+      for (int s = 0; s < q.npass; ++s) q.radix[s] = r[s];
+      bool dup = false;
+      for (const FFTPlan& o : out)
+        if (o.npass == q.npass && std::equal(o.radix, o.radix + o.npass, q.radix)) dup = true;
+      if (!dup) out.push_back(q);
+    } while (std::next_permutation(r.begin(), r.end()) && ++n < 24);
+  };
+  add_perms(std::vector<int>(p.radix, p.radix + p.npass));
+  add_perms(fewest_passes(p.L));
+  return out;
+}
+
 inline psb::RowMap map_id(int L) { return psb::RowMap{L, L, 0}; }
 // pad/unpad (3/2): drops index N/2 (PySpectral/src/padding.py:2-25)
 inline psb::RowMap map_pad32(int N) { return psb::RowMap{N / 2, N / 2 + 1, 3 * N / 2 - N}; }

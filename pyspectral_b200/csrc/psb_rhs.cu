@@ -853,6 +853,142 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
 template int rhs_dispatch<double>(psb_ctx*, int, StepIO<double>, const psb_params*, double*);
 template int rhs_dispatch<float>(psb_ctx*, int, StepIO<float>, const psb_params*, double*);
 
+// ---------------------------------------------------------------------------
+// Autotuning of a single run's five NS passes (DNS, Smagorinsky, learned).
+// Each candidate shape of a pass (column tile or pencils per CTA, and every
+// radix order of the default and the fewest-pass schedules) is timed with
+// CUDA events inside full RHS evaluations through the single-run kernels, in
+// a middle-RK-stage mode on scratch copies of the caller's state (so the
+// state is never written).  The default shape is the incumbent: a candidate
+// must beat it by 3% and win again in a longer re-timing.
+// ---------------------------------------------------------------------------
+namespace tuning {
+
+void clear_records(psb_ctx* c) {
+  for (auto& r : c->recs) {
+    c->ev_free.push_back(r.a);
+    c->ev_free.push_back(r.b);
+  }
+  c->recs.clear();
+}
+
+bool plan_is_wide(const FFTPlan& p) {
+  for (int s = 0; s < p.npass; ++s)
+    if (p.radix[s] > 8 || p.radix[s] == 6) return true;
+  return false;
+}
+
+template <typename T>
+int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
+  int Fi, Fo, maxppc;
+  size_t zextra = 0;
+  if (closure == PSB_DNS) {
+    Fi = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
+  } else if (closure == PSB_SMAG) {
+    Fi = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
+  } else {
+    Fi = 12, Fo = 6, maxppc = phys_max_ppc<PhysLearned<T>>::value;
+    zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
+  }
+  const size_t esz = sizeof(Cx<T>);
+  const size_t n = (size_t)3 * N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* q = scratch<T>(c, "tune.Q", n, &st);
+  Cx<T>* q0 = scratch<T>(c, "tune.Q0", n, &st);
+  Cx<T>* cp = c->prec == 32 ? scratch<T>(c, "tune.C", n, &st) : nullptr;
+  if (st != PSB_OK) return st;
+  PSB_TRY(cuda_ok(c, cudaMemcpyAsync(q, state, n * esz, cudaMemcpyDeviceToDevice, c->stream), "tune copy"));
+  PSB_TRY(cuda_ok(c, cudaMemcpyAsync(q0, state, n * esz, cudaMemcpyDeviceToDevice, c->stream), "tune copy"));
+  if (cp) PSB_TRY(cuda_ok(c, cudaMemsetAsync(cp, 0, n * esz, c->stream), "tune memset"));
+  const StepIO<T> io = make_io<T>(c, q, q0, cp, nullptr, nullptr, nullptr, kStageMid, p->dt / 3.0);
+  const int FMAX = std::max(Fi, Fo);
+  auto zsmem = [&](int P) { return zpass_smem_bytes<T>(FMAX, P, M3, zextra); };
+  int P = maxppc;
+  while (P > 1 && zsmem(P) > kSmemBudget) P /= 2;
+  while (P > 1 && ((long long)M1 * M2 + P - 1) / P < 2 * 148) P /= 2;
+  psb_tuned t;
+  const int Ls[5] = {M1, M2, M3, M2, M1};
+  const int Fs[5] = {Fi, 1, 0, 1, Fo};
+  t.pass[0].tile = pick_ct(Kz, Fi, M1, esz, N2);
+  t.pass[1].tile = pick_ct(Kz, 1, M2, esz, Fi * M1);
+  t.pass[2].tile = P;
+  t.pass[3].tile = pick_ct(Kz, 1, M2, esz, Fo * M1);
+  t.pass[4].tile = pick_ct(Kz, Fo, M1, esz, N2);
+  for (int k = 0; k < 5; ++k) t.pass[k].plan = *plan_for(c, Ls[k]);
+  c->tuned[closure] = t;
+  static const char* names[5] = {"x-inverse", "y-inverse", "z-fused", "y-forward", "x-forward+epilogue"};
+  const int timing_was = c->timing;
+  clear_records(c);
+  c->timing = 1;
+  auto time_pass = [&](int k, int reps, float* ms) -> int {
+    clear_records(c);
+    for (int r = 0; r < reps + 1; ++r) PSB_TRY(rhs_dispatch<T>(c, closure, io, p, nullptr));
+    PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "tune sync"));
+    float sum = 0.f;
+    int cnt = 0, seen = 0;
+    for (const auto& rec : c->recs) {
+      if (rec.name != names[k]) continue;
+      if (seen++ == 0) continue;  // the first evaluation warms up
+      float e = 0.f;
+      PSB_TRY(cuda_ok(c, cudaEventElapsedTime(&e, rec.a, rec.b), "tune elapsed"));
+      sum += e;
+      ++cnt;
+    }
+    *ms = cnt ? sum / cnt : 1e30f;
+    return PSB_OK;
+  };
+  int status = PSB_OK;
+  for (int k = 0; k < 5 && status == PSB_OK; ++k) {
+    psb_pass_shape& cur = c->tuned[closure].pass[k];
+    const psb_pass_shape inc = cur;
+    float base = 0.f;
+    if ((status = time_pass(k, 6, &base)) != PSB_OK) break;
+    std::vector<int> tiles;
+    if (k == 2) {
+      for (int pp : {1, 2, 4, 8})
+        if (pp <= maxppc && zsmem(pp) <= kSmemBudget) tiles.push_back(pp);
+    } else {
+      for (int ct : {2, 4, 8, 16, 32})
+        if (ct <= std::max(2, 2 * Kz) && (size_t)(Ls[k] + 2 * Ls[k] * Fs[k] * ct) * esz <= kSmemBudget)
+          tiles.push_back(ct);
+    }
+    psb_pass_shape best = inc;
+    float bms = 0.97f * base;
+    for (int tl : tiles) {
+      for (const FFTPlan& q2 : radix_orders(inc.plan)) {
+        cur.tile = tl;
+        cur.plan = q2;
+        cur.wide = plan_is_wide(q2);
+        float ms = 0.f;
+        if ((status = time_pass(k, 4, &ms)) != PSB_OK) break;
+        if (ms < bms) {
+          bms = ms;
+          best = cur;
+        }
+      }
+      if (status != PSB_OK) break;
+    }
+    if (status != PSB_OK) break;
+    cur = best;
+    if (best.tile != inc.tile || best.plan.npass != inc.plan.npass ||
+        !std::equal(best.plan.radix, best.plan.radix + best.plan.npass, inc.plan.radix)) {
+      float again = 0.f, def = 0.f;
+      if ((status = time_pass(k, 10, &again)) != PSB_OK) break;
+      cur = inc;
+      if ((status = time_pass(k, 10, &def)) != PSB_OK) break;
+      cur = again < 0.98f * def ? best : inc;
+    }
+  }
+  clear_records(c);
+  c->timing = timing_was;
+  if (status != PSB_OK) c->tuned.erase(closure);
+  return status;
+}
+
+}  // namespace tuning
+
 // SGS of a filtered DNS field
 template <typename T>
 int sgs_dns_run(psb_ctx* c, const void* fields, void* w0, void* tau6) {
@@ -907,3 +1043,16 @@ template int mem_stage_plql<double>(psb_ctx*, Cx<double>*, Cx<double>*, EpiPLQL<
 template int mem_stage_plql<float>(psb_ctx*, Cx<float>*, Cx<float>*, EpiPLQL<float>);
 
 }  // namespace psbh
+
+extern "C" int psb_autotune(psb_ctx* c, int closure, void* state, const psb_params* p) {
+  if (!c) return PSB_ERR_ARG;
+  if (!state || !p) return fail(c, PSB_ERR_ARG, "psb_autotune: null argument");
+  if (closure != PSB_DNS && closure != PSB_SMAG && closure != PSB_LEARNED)
+    return fail(c, PSB_ERR_UNSUPPORTED, "psb_autotune: closure not tunable (DNS, SMAG, LEARNED are)");
+  if (closure == PSB_LEARNED && (!p->mlp_params || !p->mlp_norm))
+    return fail(c, PSB_ERR_ARG, "psb_autotune: PSB_LEARNED needs mlp_params and mlp_norm");
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  return c->prec == 64 ? psbh::tuning::tune_rhs<double>(c, closure, state, p)
+                        : psbh::tuning::tune_rhs<float>(c, closure, state, p);
+}
+
