@@ -175,11 +175,7 @@ struct Batch {
       ay[r] = y;
       ZArgs<T> z{};
       const long long fsP = (long long)d.M1 * d.M2 * d.Kz;
-      for (int f = 0; f < Fi; ++f) {
-        z.in[f] = B + f * fsP;
-        z.in_pstride[f] = d.Kz;
-        z.in_kz[f] = d.Kz;
-      }
+      set_z_inputs<T, Pre, Phys::F_IN>(z, B, fsP, d.Kz, c->kz);
       for (int g = 0; g < Fo; ++g) {
         z.out[g] = C + g * fsP;
         z.out_pstride[g] = d.Kz;
@@ -514,7 +510,7 @@ int dispatch(psb_batch* b, int nsteps, bool tune) {
     case PSB_SMAG:
       return run_batch<T>(b, nsteps, tune, PreStrain<T>{}, &mk_smag<T>, &mk_epi<T, true>);
     case PSB_LEARNED:
-      return run_batch<T>(b, nsteps, tune, PreGrad<T>{}, &mk_learned<T>, &mk_epi<T, false>);
+      return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T>, &mk_epi<T, false>);
     default:
       return fail(b->c, PSB_ERR_UNSUPPORTED, "psb_batch: closure not batched (DNS, SMAG, LEARNED are)");
   }

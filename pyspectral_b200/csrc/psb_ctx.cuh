@@ -359,6 +359,24 @@ inline std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
   return out;
 }
 
+// z-pass inputs of a 3/2-padded pipeline: NIN fields from the y-pass output B
+// (field stride fsP, Kz stored k3 per pencil), with the z derivatives a Pre
+// leaves to the z-pass (pre_z_derived) formed from their stored field.
+template <typename T, class Pre, int NIN>
+void set_z_inputs(psb::ZArgs<T>& z, const Cx<T>* B, long long fsP, int Kz, const double* k3) {
+  static_assert(NIN == Pre::F_DST + psb::pre_z_derived<Pre>::value, "z-pass inputs mismatch");
+  for (int f = 0; f < NIN; ++f) {
+    int src = f;
+    bool der = false;
+    if constexpr (psb::pre_z_derived<Pre>::value > 0) Pre::zsrc(f, src, der);
+    z.in[f] = B + src * fsP;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+    z.dz[f] = der ? 1 : 0;
+  }
+  z.k3 = k3;
+}
+
 inline psb::RowMap map_id(int L) { return psb::RowMap{L, L, 0}; }
 // pad/unpad (3/2): drops index N/2 (PySpectral/src/padding.py:2-25)
 inline psb::RowMap map_pad32(int N) { return psb::RowMap{N / 2, N / 2 + 1, 3 * N / 2 - N}; }

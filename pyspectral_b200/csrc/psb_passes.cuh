@@ -207,6 +207,20 @@ struct ZArgs {
   T fac;    // physical normalisation after the inverse transform
   FFTPlan plan;
   const Cx<T>* tw;
+  unsigned char dz[kMaxZFields];  // 1: input field f enters as i*k3 times the stored spectrum (a d/dz)
+  const double* k3;               // k3 wavenumbers of the stored entries (for dz)
+};
+
+// Pre functors may leave derivatives along z to the z-pass: Pre::Z_DERIVED
+// extra z-pass inputs, Pre::zsrc(f, src, der) maps z-pass input f to the
+// stored field src, differentiated along z when der.
+template <class P, class = void>
+struct pre_z_derived {
+  static constexpr int value = 0;
+};
+template <class P>
+struct pre_z_derived<P, decltype((void)P::Z_DERIVED, void())> {
+  static constexpr int value = P::Z_DERIVED;
 };
 
 // Shared memory of one z-pass CTA: twiddles, two buffers of
@@ -253,7 +267,11 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
         split_line(r, P, lp, f, p);
         const long long pen = p0 + p;
         if (pen >= a.npencils || k >= a.in_kz[f]) continue;
-        const Cx<T> v = a.in[f][pen * a.in_pstride[f] + k];
+        Cx<T> v = a.in[f][pen * a.in_pstride[f] + k];
+        if (a.dz[f]) {
+          const T kk = (T)a.k3[k];
+          v = mk<T>(-kk * v.y, kk * v.x);
+        }
         if (part == 0) A = v; else B = v;
       }
       Cx<T>* Z = X + (size_t)c * M;

@@ -609,6 +609,34 @@ struct PreGrad {
   }
 };
 
+// (u,v,w) -> (u,v,w, du_i/dx, du_i/dy for i = 1..3) on the x-inverse pass; the
+// z-pass forms du_i/dz = i k3 u_i itself, so the x and y passes carry 9 fields
+// instead of 12.  z-pass input order is PreGrad's: u,v,w then g[3*i + j].
+template <typename T>
+struct PreGradXY {
+  static constexpr int F_SRC = 3, F_DST = 9, Z_DERIVED = 3;
+  __device__ void operator()(int i, int o, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    const T k1 = (T)a.k_row[i], k2 = (T)a.k_outer[o];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      d[f] = s[f];
+      d[3 + 2 * f] = pik(k1, s[f]);
+      d[4 + 2 * f] = pik(k2, s[f]);
+    }
+  }
+  // z-pass input f (0..11) -> stored field and whether it is differentiated along z
+  __host__ static void zsrc(int f, int& src, bool& der) {
+    if (f < 3) {
+      src = f;
+      der = false;
+      return;
+    }
+    const int i = (f - 3) / 3, j = (f - 3) % 3;
+    der = j == 2;
+    src = der ? i : 3 + 2 * i + j;
+  }
+};
+
 // Products u_i u_j plus the MLP subgrid stress, summed so that one forward
 // transform per component carries both: out_ij = u_i u_j + tau_ij / s^2 in the
 // reference's real-space scaling (real-space arrays equal physical / s).

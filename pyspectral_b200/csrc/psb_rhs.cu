@@ -41,7 +41,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const ps
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
   constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
-  static_assert(Phys::F_IN == Pre::F_DST, "pre/phys mismatch");
+  static_assert(Phys::F_IN == Pre::F_DST + pre_z_derived<Pre>::value, "pre/phys mismatch");
   static_assert(Epi::F_IN == Phys::F_OUT, "phys/epi mismatch");
   int st = PSB_OK;
   Cx<T>* A = scratch<T>(c, "ns.A", (size_t)Fi * M1 * N2 * Kz, &st);
@@ -89,11 +89,7 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const ps
   // fused z
   ZArgs<T> z{};
   const long long fsP = (long long)M1 * M2 * Kz;
-  for (int f = 0; f < Fi; ++f) {
-    z.in[f] = B + f * fsP;
-    z.in_pstride[f] = Kz;
-    z.in_kz[f] = Kz;
-  }
+  set_z_inputs<T, Pre, Phys::F_IN>(z, B, fsP, Kz, c->kz);
   for (int g = 0; g < Fo; ++g) {
     z.out[g] = C + g * fsP;
     z.out_pstride[g] = Kz;
@@ -843,7 +839,7 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
       PhysLearned<T> phys{reinterpret_cast<const float*>(p->mlp_params), reinterpret_cast<const float*>(p->mlp_norm),
                           (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta)};
-      return run_ns32<T>(c, Qin, PreGrad<T>{}, phys, epi, ts);
+      return run_ns32<T>(c, Qin, PreGradXY<T>{}, phys, epi, ts);
     }
     default:
       return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");
@@ -889,7 +885,7 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   } else if (closure == PSB_SMAG) {
     Fi = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
   } else {
-    Fi = 12, Fo = 6, maxppc = phys_max_ppc<PhysLearned<T>>::value;
+    Fi = PreGradXY<T>::F_DST, Fo = 6, maxppc = phys_max_ppc<PhysLearned<T>>::value;
     zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
   }
   const size_t esz = sizeof(Cx<T>);
