@@ -259,12 +259,13 @@ def generate(N_dns=256, les=(64, 32), seed=11, nu=5e-4, dt=2e-3, t_snap=(1.0, 8.
 
 
 def evaluate(model, N_dns=256, n=64, seed=23, nu=5e-4, dt_dns=2e-3, dt_les=4e-3, t0=1.0, les_steps=2000,
-             device=0, log=print):
+             every=250, device=0, log=print):
     """A-posteriori test (config 4): LES from the filtered DNS at t0, advanced
-    les_steps; E(k) vs the filtered DNS at the same time for k <= n/4."""
+    les_steps; E(k) vs the filtered DNS at the same time for 1 <= k <= n/4,
+    at every `every` LES steps and at the end, for the learned closure (FP32),
+    Smagorinsky (FP64 and FP32) and no model (FP32)."""
     from .RHSfunctions import advance
     grid, dns = make_run(N_dns, seed, nu, dt_dns, 0, 32, device=device)
-    cd = grid.ctx(32)
     n0 = int(round(t0 / dt_dns))
     advance(dns, grid, n0)
     ub0 = filtered_state(dns.Q, N_dns, n, 32).to(torch.complex128)
@@ -273,26 +274,36 @@ def evaluate(model, N_dns=256, n=64, seed=23, nu=5e-4, dt_dns=2e-3, dt_les=4e-3,
                                 ("smagorinsky_fp32", 1, 32), ("no_model_fp32", 0, 32)):
         g, m = make_run(n, 0, nu, dt_les, closure, prec, device=device, state=ub0, model=model)
         runs[name] = (g, m)
-    T_end = t0 + les_steps * dt_les
-    nd = int(round((T_end - t0) / dt_dns))
-    t1 = time.time()
-    advance(dns, grid, nd)
-    ref = filtered_state(dns.Q, N_dns, n, 32)
-    for name, (g, m) in runs.items():
-        advance(m, g, les_steps)
-    torch.cuda.synchronize()
-    gl = runs["learned_fp32"][0]
-    ctx_les64 = gl.ctx(32)
-    Eref = ctx_les64.spectrum(ref).sum(1)
     kmax = n // 4
-    out = {"t0": t0, "t_end": T_end, "N_dns": N_dns, "n_les": n, "k_compare": kmax,
-           "E_ref": Eref[:kmax + 1].tolist()}
-    for name, (g, m) in runs.items():
-        E = g.ctx(m.precision).spectrum(m.Q[0:3].contiguous()).sum(1)
-        rel = np.abs(E[1:kmax + 1] - Eref[1:kmax + 1]) / Eref[1:kmax + 1]
-        out[name] = {"max_rel_err_k_le_kc_half": float(rel.max()), "mean_rel_err": float(rel.mean()),
-                     "E": E[:kmax + 1].tolist(), "finite": bool(np.isfinite(E).all())}
-        log(f"  {name:18s} max rel E(k) err (1<=k<={kmax}) = {rel.max():.4f}  mean {rel.mean():.4f}")
+    ctx_les = runs["learned_fp32"][0].ctx(32)
+    hist = {name: [] for name in runs}
+    times = []
+    t1 = time.time()
+    done = 0
+    ratio = int(round(dt_les / dt_dns))
+    Eref = None
+    while done < les_steps:
+        chunk = min(every, les_steps - done)
+        advance(dns, grid, chunk * ratio)
+        for name, (g, m) in runs.items():
+            advance(m, g, chunk)
+        done += chunk
+        ref = filtered_state(dns.Q, N_dns, n, 32)
+        Eref = ctx_les.spectrum(ref).sum(1)
+        times.append(t0 + done * dt_les)
+        for name, (g, m) in runs.items():
+            E = g.ctx(m.precision).spectrum(m.Q[0:3].contiguous()).sum(1)
+            rel = np.abs(E[1:kmax + 1] - Eref[1:kmax + 1]) / Eref[1:kmax + 1]
+            hist[name].append({"t": times[-1], "max": float(rel.max()), "mean": float(rel.mean()),
+                               "E": E[:kmax + 1].tolist(), "finite": bool(np.isfinite(E).all())})
+        log(f"  t={times[-1]:5.2f}  " + "  ".join(f"{k}: {v[-1]['max']:.3f}/{v[-1]['mean']:.3f}"
+                                                for k, v in hist.items()))
+    torch.cuda.synchronize()
+    out = {"t0": t0, "t_end": times[-1], "N_dns": N_dns, "n_les": n, "k_compare": kmax,
+           "E_ref": Eref[:kmax + 1].tolist(), "times": times}
+    for name, h in hist.items():
+        out[name] = {"max_rel_err_k_le_kc_half": h[-1]["max"], "mean_rel_err": h[-1]["mean"], "E": h[-1]["E"],
+                     "finite": h[-1]["finite"], "history": [{k: r[k] for k in ("t", "max", "mean")} for r in h]}
     out["wall_s"] = time.time() - t1
     return out
 
@@ -306,10 +317,22 @@ def main():
     ap.add_argument("--batch", type=int, default=16384)
     ap.add_argument("--les-steps", type=int, default=2000)
     ap.add_argument("--no-eval", action="store_true")
+    ap.add_argument("--nu", type=float, default=5e-4, help="viscosity of the DNS and the LES")
+    ap.add_argument("--eval-only", action="store_true",
+                    help="re-run the a-posteriori evaluation of the model at --out and update its metadata")
     a = ap.parse_args()
     t0 = time.time()
+    if a.eval_only:
+        model = MLPModel.load(a.out)
+        meta = dict(model.meta)
+        meta["eval"] = evaluate(model, N_dns=a.N_dns, nu=meta.get("nu", a.nu), les_steps=a.les_steps)
+        model.save(a.out, **meta)
+        with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
+            json.dump(meta, f, indent=1)
+        print(f"updated {a.out} ({time.time() - t0:.1f} s)")
+        return
     print("generating training data ...")
-    X, T = generate(N_dns=a.N_dns, npoints=a.npoints)
+    X, T = generate(N_dns=a.N_dns, nu=a.nu, npoints=a.npoints)
     print(f"  {X.shape[0]} samples ({time.time() - t0:.1f} s)")
     model = MLPModel(seed=0)
     model.fit_norm(X, T)
@@ -318,12 +341,12 @@ def main():
     for s, l in hist:
         print(f"  step {s:6d}  loss {l:.5f}")
     meta = {"train_samples": int(X.shape[0]), "train_steps": a.steps, "batch": a.batch,
-            "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": 5e-4,
+            "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": a.nu,
             "spectrum": "E(k)=16 sqrt(2/pi) u0^2 k^4/k0^5 exp(-2 k^2/k0^2), k0=4, u0=1"}
     model.meta = meta
     if not a.no_eval:
         print("a-posteriori evaluation ...")
-        meta["eval"] = evaluate(model, N_dns=a.N_dns, les_steps=a.les_steps)
+        meta["eval"] = evaluate(model, N_dns=a.N_dns, nu=a.nu, les_steps=a.les_steps)
     model.save(a.out, **meta)
     with open(os.path.splitext(a.out)[0] + ".json", "w") as f:
         json.dump(meta, f, indent=1)
