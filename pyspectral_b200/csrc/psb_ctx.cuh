@@ -267,7 +267,9 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   const size_t smem = smem_for(P);
   const long long grid = (z.npencils + P - 1) / P;
   double bytes = extra_bytes + (double)esz * z.npencils * Phys::F_OUT * z.out_kz;
-  for (int f = 0; f < Phys::F_IN; ++f) bytes += (double)esz * z.npencils * z.in_kz[f];
+  // a field formed as d/dz of another input re-reads that input's line: no new bytes
+  for (int f = 0; f < Phys::F_IN; ++f)
+    if (!z.dz[f]) bytes += (double)esz * z.npencils * z.in_kz[f];
   if constexpr (TUNABLE) {
     if (sh && sh->wide) {
       auto k = psb::zpass_kernel<T, Phys, true>;
