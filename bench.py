@@ -139,7 +139,8 @@ def cpu_rhs(N, closure):
         from oracle import mlp_oracle as mo
         d = np.load(os.path.join(ROOT, "pyspectral_b200", "models", "sgs_mlp.npz"))
         P, nrm = d["params"].astype(np.float64), d["norm"].astype(np.float64)
-        return g, (lambda q: mo.rhs_learned(g, q, 1e-3, P, nrm, 2 * math.pi / N))
+        act = json.loads(str(d["meta"])).get("act", "gelu")
+        return g, (lambda q: mo.rhs_learned(g, q, 1e-3, P, nrm, 2 * math.pi / N, act=act))
     fn = orc.rhs_smag if closure == "smag" else orc.rhs_nosgs
     return g, (lambda q: fn(g, q, p)[0])
 

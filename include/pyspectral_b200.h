@@ -73,7 +73,12 @@ typedef struct {
   const void* mlp_params; /* PSB_LEARNED: FP32 parameter block (psb_mlp_sizes) on the device */
   const void* mlp_norm;   /* PSB_LEARNED: FP32 normalisation block on the device */
   double les_delta;       /* PSB_LEARNED: filter width fed to the MLP; <=0 -> (dx dy dz)^(1/3) */
+  int mlp_act;            /* PSB_LEARNED: hidden activation of the model, PSB_ACT_GELU or PSB_ACT_RELU */
 } psb_params;
+
+/* Hidden activation of the learned closure's MLP (a property of the trained model). */
+#define PSB_ACT_GELU 0 /* x Phi(x) */
+#define PSB_ACT_RELU 1 /* max(x, 0) */
 
 /* FFTclass + gridclass construction (src/Classes.py:548-625; src/PySpec_3d.py:79-80).
  * precision: 32 or 64.  N1,N2,N3 must be multiples of 4 whose 3/2 and 2x
@@ -156,18 +161,19 @@ int psb_fft_c2r(psb_ctx* ctx, const void* spec, void* phys, int nfields);
 int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* count);
 
 /* ---- learned subgrid closure (no counterpart in the reference) ----------
- * MLP 10 -> 64 -> 64 -> 6 (GELU), BF16 tensor-core math with FP32
+ * MLP 10 -> 64 -> 64 -> 6 (hidden activation act: PSB_ACT_GELU or
+ * PSB_ACT_RELU), BF16 tensor-core math with FP32
  * accumulation.  Features: the 9 velocity gradients du_i/dx_j (order 3i+j)
  * and the filter width; targets: tau_11,22,33,12,13,23.  Parameters are an
  * FP32 master block of *nparams floats, normalisation a block of *nnorm
  * floats (xmean[10] xistd[10] ymean[6] ystd[6]); all device pointers. */
 int psb_mlp_sizes(int* nparams, int* nnorm);
 /* Y[B][6] = tau(X[B][10]) (raw units in and out). */
-int psb_mlp_forward(psb_ctx* ctx, const float* params, const float* norm, const float* X, int B, float* Y);
+int psb_mlp_forward(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, int B, float* Y);
 /* grad += d(MSE of normalised outputs)/d(params) over the B points X[idx[b]],
  * T[idx[b]]; *loss (device double) += the MSE. */
-int psb_mlp_grad(psb_ctx* ctx, const float* params, const float* norm, const float* X, const float* T, const int* idx,
-                 int B, float* grad, double* loss);
+int psb_mlp_grad(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, const float* T,
+                 const int* idx, int B, float* grad, double* loss);
 /* One Adam(W) update of params from grad (step >= 1); clears grad. */
 int psb_mlp_adam(psb_ctx* ctx, float* params, float* m, float* v, float* grad, int step, float lr, float beta1,
                  float beta2, float eps, float weight_decay);

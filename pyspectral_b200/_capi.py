@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
 PSB_OK = 0
 PSB_ERR_NONFINITE = 6
 DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL = 0, 1, 2, 3, 4, 5, 6, 7
+ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
 
 EXPORTS = (
@@ -43,7 +44,7 @@ class Params(ctypes.Structure):
                 ("tau_b", ctypes.c_double), ("kf", ctypes.c_int), ("rotate", ctypes.c_int),
                 ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
                 ("force", ctypes.c_void_p), ("mlp_params", ctypes.c_void_p), ("mlp_norm", ctypes.c_void_p),
-                ("les_delta", ctypes.c_double)]
+                ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int)]
 
 
 _lib = None
@@ -97,10 +98,11 @@ def load(path: str = LIB_PATH):
 
 
 def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
-                Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0) -> Params:
+                Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0,
+                mlp_act=0) -> Params:
     return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
                   int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force, mlp_params, mlp_norm,
-                  float(les_delta))
+                  float(les_delta), int(mlp_act))
 
 
 class Context:

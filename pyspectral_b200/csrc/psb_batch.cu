@@ -441,7 +441,7 @@ template <typename T>
 PhysLearned<T> mk_learned(psb_ctx* c, const psb_params& p) {
   const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
   return PhysLearned<T>{reinterpret_cast<const float*>(p.mlp_params), reinterpret_cast<const float*>(p.mlp_norm),
-                        (T)s32, (float)(p.les_delta > 0 ? p.les_delta : c->Delta)};
+                        (T)s32, (float)(p.les_delta > 0 ? p.les_delta : c->Delta), p.mlp_act};
 }
 template <typename T, bool SMAG>
 EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
@@ -542,6 +542,8 @@ int psb_batch_set_run(psb_batch* b, int r, void* state, void* comp, const psb_pa
   if (r < 0 || r >= b->nruns || !state || !p) return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: bad argument");
   if (b->closure == PSB_LEARNED && (!p->mlp_params || !p->mlp_norm))
     return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: PSB_LEARNED needs mlp_params and mlp_norm");
+  if (b->closure == PSB_LEARNED && p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
+    return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
   b->state[r] = state;
   b->comp[r] = comp;
   b->params[r] = *p;

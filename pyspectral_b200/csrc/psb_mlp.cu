@@ -15,6 +15,8 @@ using namespace psbh;
 
 namespace {
 
+static_assert(kActGelu == PSB_ACT_GELU && kActRelu == PSB_ACT_RELU, "activation codes");
+
 constexpr int kRows = 128;  // points per CTA (8 warps x 16)
 
 struct TrainSmem {
@@ -47,6 +49,7 @@ __device__ __forceinline__ void bfrag_kn(uint32_t* b, const __nv_bfloat16* W, in
 }
 
 // grad[kMlpParams] += dL/dparams over B points; loss_acc += sum of squared errors / (6B)
+template <int ACT>
 __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
                                                         const float* __restrict__ X, const float* __restrict__ T,
                                                         const int* __restrict__ idx, int B, float* __restrict__ grad,
@@ -71,7 +74,7 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     return id >= 0 ? X[(long long)id * kMlpIn + f] : s.m.xmean[f];
   });
   float z1[8][4], z2[8][4], y[4];
-  mlp_forward_warp(s.m, xa, y, z1, z2);
+  mlp_forward_warp<ACT>(s.m, xa, y, z1, z2);
   // dY = 2 (y - t) / (6B), rows without a point contribute nothing
   const float sc = 2.f / (6.f * (float)B);
   float dy[4];
@@ -102,13 +105,13 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     for (int j = 0; j < 8; ++j) {
       const int col = 8 * j + 2 * t;
       *reinterpret_cast<__nv_bfloat162*>(&s.H1[ra * kMlpH + col]) =
-          __floats2bfloat162_rn(gelu_f(z1[j][0]), gelu_f(z1[j][1]));
+          __floats2bfloat162_rn(act_f<ACT>(z1[j][0]), act_f<ACT>(z1[j][1]));
       *reinterpret_cast<__nv_bfloat162*>(&s.H1[rb * kMlpH + col]) =
-          __floats2bfloat162_rn(gelu_f(z1[j][2]), gelu_f(z1[j][3]));
+          __floats2bfloat162_rn(act_f<ACT>(z1[j][2]), act_f<ACT>(z1[j][3]));
       *reinterpret_cast<__nv_bfloat162*>(&s.H2[ra * kMlpH + col]) =
-          __floats2bfloat162_rn(gelu_f(z2[j][0]), gelu_f(z2[j][1]));
+          __floats2bfloat162_rn(act_f<ACT>(z2[j][0]), act_f<ACT>(z2[j][1]));
       *reinterpret_cast<__nv_bfloat162*>(&s.H2[rb * kMlpH + col]) =
-          __floats2bfloat162_rn(gelu_f(z2[j][2]), gelu_f(z2[j][3]));
+          __floats2bfloat162_rn(act_f<ACT>(z2[j][2]), act_f<ACT>(z2[j][3]));
     }
     *reinterpret_cast<__nv_bfloat162*>(&s.dY[ra * 16 + 2 * t]) = __floats2bfloat162_rn(dy[0], dy[1]);
     *reinterpret_cast<__nv_bfloat162*>(&s.dY[rb * 16 + 2 * t]) = __floats2bfloat162_rn(dy[2], dy[3]);
@@ -119,7 +122,7 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
       atomicAdd(&s.db3[2 * t + 1], dy[1] + dy[3]);
     }
   }
-  // dH2 = dY W3 (k = 8 outputs, padded to 16), dZ2 = dH2 * gelu'(z2)
+  // dH2 = dY W3 (k = 8 outputs, padded to 16), dZ2 = dH2 * act'(z2)
   uint32_t da[4];
   da[0] = pack_bf16(dy[0], dy[1]);
   da[1] = pack_bf16(dy[2], dy[3]);
@@ -134,7 +137,7 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     b[1] = 0u;
     mma16816(dz2[j], da, b);
 #pragma unroll
-    for (int e = 0; e < 4; ++e) dz2[j][e] *= gelu_d(z2[j][e]);
+    for (int e = 0; e < 4; ++e) dz2[j][e] *= act_d<ACT>(z2[j][e]);
   }
   uint32_t a2[4][4];
 #pragma unroll
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     a2[kk][2] = pack_bf16(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
     a2[kk][3] = pack_bf16(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
   }
-  // dH1 = dZ2 W2 (W2 stored [out=k][in=n]), dZ1 = dH1 * gelu'(z1)
+  // dH1 = dZ2 W2 (W2 stored [out=k][in=n]), dZ1 = dH1 * act'(z1)
   float dz1[8][4];
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
@@ -156,7 +159,7 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
       mma16816(dz1[j], a2[kk], b);
     }
 #pragma unroll
-    for (int e = 0; e < 4; ++e) dz1[j][e] *= gelu_d(z1[j][e]);
+    for (int e = 0; e < 4; ++e) dz1[j][e] *= act_d<ACT>(z1[j][e]);
   }
   {
     const int ra = warp * 16 + g, rb = ra + 8;
@@ -255,6 +258,7 @@ __global__ void adam_kernel(float* __restrict__ P, float* __restrict__ m, float*
   grad[i] = 0.f;
 }
 
+template <int ACT>
 __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
                                                           const float* __restrict__ X, int B,
                                                           float* __restrict__ Y) {
@@ -270,7 +274,7 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
       return r0 + r < B ? X[(long long)(r0 + r) * kMlpIn + f] : s.xmean[f];
     });
     float y[4];
-    mlp_forward_fast(s, xa, y);
+    mlp_forward_fast<ACT>(s, xa, y);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int c = 2 * t + (e & 1), r = r0 + g + (e < 2 ? 0 : 8);
@@ -290,28 +294,38 @@ int psb_mlp_sizes(int* nparams, int* nnorm) {
   return PSB_OK;
 }
 
-int psb_mlp_forward(psb_ctx* c, const float* params, const float* norm, const float* X, int B, float* Y) {
+int psb_mlp_forward(psb_ctx* c, int act, const float* params, const float* norm, const float* X, int B, float* Y) {
   if (!c) return PSB_ERR_ARG;
-  if (!params || !norm || !X || !Y || B < 0) return fail(c, PSB_ERR_ARG, "psb_mlp_forward: bad argument");
+  if (!params || !norm || !X || !Y || B < 0 || (act != kActGelu && act != kActRelu))
+    return fail(c, PSB_ERR_ARG, "psb_mlp_forward: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   if (B == 0) return PSB_OK;
   const size_t smem = sizeof(MlpFwdSmem);
   const int blocks = (int)std::min<long long>(((long long)B + 127) / 128, 148 * 8);
   ++c->launches;
-  mlp_forward_kernel<<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
+  if (act == kActRelu)
+    mlp_forward_kernel<kActRelu><<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
+  else
+    mlp_forward_kernel<kActGelu><<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
   return launch_ok(c, "mlp forward");
 }
 
-int psb_mlp_grad(psb_ctx* c, const float* params, const float* norm, const float* X, const float* T, const int* idx,
-                 int B, float* grad, double* loss) {
+int psb_mlp_grad(psb_ctx* c, int act, const float* params, const float* norm, const float* X, const float* T,
+                 const int* idx, int B, float* grad, double* loss) {
   if (!c) return PSB_ERR_ARG;
-  if (!params || !norm || !X || !T || !idx || !grad || !loss || B <= 0)
+  if (!params || !norm || !X || !T || !idx || !grad || !loss || B <= 0 || (act != kActGelu && act != kActRelu))
     return fail(c, PSB_ERR_ARG, "psb_mlp_grad: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   const size_t smem = sizeof(TrainSmem);
-  set_smem(mlp_train_kernel, smem);
+  const unsigned grid = (unsigned)((B + kRows - 1) / kRows);
   ++c->launches;
-  mlp_train_kernel<<<(B + kRows - 1) / kRows, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
+  if (act == kActRelu) {
+    set_smem(mlp_train_kernel<kActRelu>, smem);
+    mlp_train_kernel<kActRelu><<<grid, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
+  } else {
+    set_smem(mlp_train_kernel<kActGelu>, smem);
+    mlp_train_kernel<kActGelu><<<grid, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
+  }
   return launch_ok(c, "mlp train");
 }
 

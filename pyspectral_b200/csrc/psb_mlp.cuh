@@ -1,5 +1,6 @@
-// Pointwise subgrid-stress MLP 10 -> 64 -> 64 -> 6 (GELU) on BF16 tensor cores
-// with FP32 accumulation (mma.sync.m16n8k16.bf16, FP32 C/D fragments).
+// Pointwise subgrid-stress MLP 10 -> 64 -> 64 -> 6 on BF16 tensor cores with
+// FP32 accumulation (mma.sync.m16n8k16.bf16, FP32 C/D fragments).  Hidden
+// activation: GELU (kActGelu) or ReLU (kActRelu), a property of the model.
 //
 // This closure has no counterpart in the reference; it replaces the
 // Smagorinsky stress of PySpectral/src/RHSfunctions.py:195-212 by a learned
@@ -22,6 +23,7 @@ constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kMlpH * kMlpIn, kOffW2 = kOffB1 + kM
               kOffB2 = kOffW2 + kMlpH * kMlpH, kOffW3 = kOffB2 + kMlpH, kOffB3 = kOffW3 + kMlpOut * kMlpH,
               kMlpParams = kOffB3 + kMlpOut;
 constexpr int kMlpNorm = 32;
+constexpr int kActGelu = 0, kActRelu = 1;
 
 // BF16 operand copies staged in shared memory, padded for the m16n8k16 tiles:
 //   w1[64][16] (k padded 10->16), w2[64][64], w3[8][64] (n padded 6->8)
@@ -150,6 +152,37 @@ __device__ __forceinline__ float gelu_d(float x) {
   return 0.5f * e + x * 0.39894228040143268f * g;
 }
 
+// ReLU of two FP32 pre-activations, rounded to BF16 and packed (lo in the low
+// half): one conversion instruction with the clamp built in.
+__device__ __forceinline__ uint32_t relu_pack(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
+
+// Activation, its derivative and the packed BF16 activation of two values.
+template <int ACT>
+__device__ __forceinline__ float act_f(float x) {
+  if constexpr (ACT == kActRelu)
+    return fmaxf(x, 0.f);
+  else
+    return gelu_f(x);
+}
+template <int ACT>
+__device__ __forceinline__ float act_d(float x) {
+  if constexpr (ACT == kActRelu)
+    return x > 0.f ? 1.f : 0.f;
+  else
+    return gelu_d(x);
+}
+template <int ACT>
+__device__ __forceinline__ uint32_t act_pack(float lo, float hi) {
+  if constexpr (ACT == kActRelu)
+    return relu_pack(lo, hi);
+  else
+    return gelu_pack(lo, hi);
+}
+
 // B fragment of a weight stored [n][k] row-major (ld = k stride) for the tile (k0, n0).
 __device__ __forceinline__ void bfrag_nk(uint32_t* b, const __nv_bfloat16* W, int ld, int k0, int n0, int lane) {
   const int g = lane >> 2, t = lane & 3;
@@ -162,6 +195,7 @@ __device__ __forceinline__ void bfrag_nk(uint32_t* b, const __nv_bfloat16* W, in
 // features (16 x 16, k 10..15 zero).  Returns y[4]: C fragment of the 16 x 8
 // outputs (normalised; columns 6,7 unused).  If z1/z2 are given, the
 // pre-activations are kept (for the backward pass).
+template <int ACT>
 __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_t* xa, float* y, float (*z1)[4],
                                                  float (*z2)[4]) {
   const int lane = threadIdx.x & 31, t = lane & 3;
@@ -183,7 +217,7 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (z1) z1[j][e] = h[j][e];
-      h[j][e] = gelu_f(h[j][e]);
+      h[j][e] = act_f<ACT>(h[j][e]);
     }
 #pragma unroll
   for (int kk = 0; kk < 4; ++kk) {
@@ -211,7 +245,7 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (z2) z2[j][e] = h[j][e];
-      h[j][e] = gelu_f(h[j][e]);
+      h[j][e] = act_f<ACT>(h[j][e]);
     }
 #pragma unroll
   for (int kk = 0; kk < 4; ++kk) {
@@ -286,8 +320,9 @@ __device__ __forceinline__ void mlp_stage_fwd(MlpFwdSmem& s, const float* __rest
 }
 
 // Forward pass of 16 points from the fragment-ordered weights; same
-// arithmetic as mlp_forward_warp (BF16 operands, FP32 accumulation, GELU on
-// the FP32 pre-activations, BF16 rounding of the activations).
+// arithmetic as mlp_forward_warp (BF16 operands, FP32 accumulation, the
+// activation on the FP32 pre-activations, BF16 rounding of the activations).
+template <int ACT>
 __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint32_t* xa, float* y) {
   const int lane = threadIdx.x & 31, t = lane & 3;
   float h[8][4];
@@ -305,10 +340,10 @@ __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint
   uint32_t a[4][4];
 #pragma unroll
   for (int kk = 0; kk < 4; ++kk) {
-    a[kk][0] = gelu_pack(h[2 * kk][0], h[2 * kk][1]);
-    a[kk][1] = gelu_pack(h[2 * kk][2], h[2 * kk][3]);
-    a[kk][2] = gelu_pack(h[2 * kk + 1][0], h[2 * kk + 1][1]);
-    a[kk][3] = gelu_pack(h[2 * kk + 1][2], h[2 * kk + 1][3]);
+    a[kk][0] = act_pack<ACT>(h[2 * kk][0], h[2 * kk][1]);
+    a[kk][1] = act_pack<ACT>(h[2 * kk][2], h[2 * kk][3]);
+    a[kk][2] = act_pack<ACT>(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+    a[kk][3] = act_pack<ACT>(h[2 * kk + 1][2], h[2 * kk + 1][3]);
   }
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
@@ -328,10 +363,10 @@ __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint
     }
 #pragma unroll
   for (int kk = 0; kk < 4; ++kk) {
-    a[kk][0] = gelu_pack(h[2 * kk][0], h[2 * kk][1]);
-    a[kk][1] = gelu_pack(h[2 * kk][2], h[2 * kk][3]);
-    a[kk][2] = gelu_pack(h[2 * kk + 1][0], h[2 * kk + 1][1]);
-    a[kk][3] = gelu_pack(h[2 * kk + 1][2], h[2 * kk + 1][3]);
+    a[kk][0] = act_pack<ACT>(h[2 * kk][0], h[2 * kk][1]);
+    a[kk][1] = act_pack<ACT>(h[2 * kk][2], h[2 * kk][3]);
+    a[kk][2] = act_pack<ACT>(h[2 * kk + 1][0], h[2 * kk + 1][1]);
+    a[kk][3] = act_pack<ACT>(h[2 * kk + 1][2], h[2 * kk + 1][3]);
   }
   const float c0 = s.b3[2 * t], c1 = s.b3[2 * t + 1];
   y[0] = c0;

@@ -651,13 +651,24 @@ struct PhysLearned {
   const float* norm;
   T sphys;      // s: physical = real-space * s
   float delta;  // filter width fed to the MLP
+  int act;      // kActGelu or kActRelu
   __device__ void setup(unsigned char* extra) const {
     mlp_stage_fwd(*reinterpret_cast<MlpFwdSmem*>(extra), params, norm);
   }
+  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long a, long long b,
+                        unsigned char* extra) const {
+    if (act == kActRelu)
+      block_act<kActRelu>(R, W, P, M, fac, extra);
+    else
+      block_act<kActGelu>(R, W, P, M, fac, extra);
+    (void)a;
+    (void)b;
+  }
   // Each warp takes tiles of 16 consecutive points (pencil-major); a lane
   // holds rows g and g+8 of a tile and locates them once per tile.
-  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
-                        unsigned char* extra) const {
+  template <int ACT>
+  __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, T fac,
+                                            unsigned char* extra) const {
     const MlpFwdSmem& s = *reinterpret_cast<const MlpFwdSmem*>(extra);
     const int npts = P * M;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -687,7 +698,7 @@ struct PhysLearned {
         return f < 9 ? (float)(val(3 + f, h) * fs) : delta;
       });
       float y[4];
-      mlp_forward_fast(s, xa, y);
+      mlp_forward_fast<ACT>(s, xa, y);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int c = 2 * t + (e & 1);

@@ -834,11 +834,13 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
     case PSB_LEARNED: {
       if (Qin && (!p->mlp_params || !p->mlp_norm))
         return fail(c, PSB_ERR_ARG, "PSB_LEARNED needs mlp_params and mlp_norm");
+      if (p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
+        return fail(c, PSB_ERR_ARG, "PSB_LEARNED: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
       EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
                           (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
       const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
       PhysLearned<T> phys{reinterpret_cast<const float*>(p->mlp_params), reinterpret_cast<const float*>(p->mlp_norm),
-                          (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta)};
+                          (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta), p->mlp_act};
       return run_ns32<T>(c, Qin, PreGradXY<T>{}, phys, epi, ts);
     }
     default:
@@ -1047,6 +1049,8 @@ extern "C" int psb_autotune(psb_ctx* c, int closure, void* state, const psb_para
     return fail(c, PSB_ERR_UNSUPPORTED, "psb_autotune: closure not tunable (DNS, SMAG, LEARNED are)");
   if (closure == PSB_LEARNED && (!p->mlp_params || !p->mlp_norm))
     return fail(c, PSB_ERR_ARG, "psb_autotune: PSB_LEARNED needs mlp_params and mlp_norm");
+  if (closure == PSB_LEARNED && p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
+    return fail(c, PSB_ERR_ARG, "psb_autotune: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   return c->prec == 64 ? psbh::tuning::tune_rhs<double>(c, closure, state, p)
                         : psbh::tuning::tune_rhs<float>(c, closure, state, p);

@@ -44,8 +44,8 @@ def _lib():
     if not hasattr(lib, "_mlp_bound"):
         vp, i, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
         lib.psb_mlp_sizes.argtypes = [ctypes.POINTER(i), ctypes.POINTER(i)]
-        lib.psb_mlp_forward.argtypes = [vp, vp, vp, vp, i, vp]
-        lib.psb_mlp_grad.argtypes = [vp, vp, vp, vp, vp, vp, i, vp, vp]
+        lib.psb_mlp_forward.argtypes = [vp, i, vp, vp, vp, i, vp]
+        lib.psb_mlp_grad.argtypes = [vp, i, vp, vp, vp, vp, vp, i, vp, vp]
         lib.psb_mlp_adam.argtypes = [vp, vp, vp, vp, vp, i, f, f, f, f, f]
         lib.psb_physical_fields.argtypes = [vp, vp, i, vp]
         lib.psb_products.argtypes = [vp, vp, vp]
@@ -67,10 +67,19 @@ def nparams():
     return a.value, b.value
 
 
-class MLPModel:
-    """FP32 master parameters, normalisation and Adam moments on the device."""
+ACTS = {"gelu": _capi.ACT_GELU, "relu": _capi.ACT_RELU}
 
-    def __init__(self, seed=0, device=0, params=None, norm=None):
+
+class MLPModel:
+    """FP32 master parameters, normalisation and Adam moments on the device;
+    `act` is the hidden activation ("gelu" or "relu"), a property of the
+    trained model (recorded in its metadata)."""
+
+    def __init__(self, seed=0, device=0, params=None, norm=None, act="gelu"):
+        if act not in ACTS:
+            raise ValueError(f"unknown activation {act!r} (expected one of {sorted(ACTS)})")
+        self.act_name = act
+        self.act = ACTS[act]
         n, nn = nparams()
         dev = torch.device("cuda", device)
         if params is None:
@@ -101,20 +110,21 @@ class MLPModel:
     def save(self, path, **meta):
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, params=self.params.cpu().numpy(), norm=self.norm.cpu().numpy(),
-                 meta=json.dumps({**self.meta, **meta}))
+                 meta=json.dumps({**self.meta, **meta, "act": self.act_name}))
 
     @classmethod
     def load(cls, path=DEFAULT_MODEL, device=0):
         d = np.load(path)
-        m = cls(device=device, params=d["params"], norm=d["norm"])
-        m.meta = json.loads(str(d["meta"])) if "meta" in d else {}
+        meta = json.loads(str(d["meta"])) if "meta" in d else {}
+        m = cls(device=device, params=d["params"], norm=d["norm"], act=meta.get("act", "gelu"))
+        m.meta = meta
         return m
 
     def forward(self, ctx, X):
         Y = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
         ctx.bind_stream()
-        ctx.check(_lib().psb_mlp_forward(ctx.h, _p(self.params), _p(self.norm), _p(X.contiguous()), X.shape[0],
-                                         _p(Y)), "psb_mlp_forward")
+        ctx.check(_lib().psb_mlp_forward(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X.contiguous()),
+                                         X.shape[0], _p(Y)), "psb_mlp_forward")
         return Y
 
     def grad_of(self, ctx, X, T, idx):
@@ -122,8 +132,8 @@ class MLPModel:
         self.grad.zero_()
         loss = torch.zeros(1, dtype=torch.float64, device=X.device)
         ctx.bind_stream()
-        ctx.check(_lib().psb_mlp_grad(ctx.h, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx), idx.numel(),
-                                      _p(self.grad), _p(loss)), "psb_mlp_grad")
+        ctx.check(_lib().psb_mlp_grad(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
+                                      idx.numel(), _p(self.grad), _p(loss)), "psb_mlp_grad")
         return float(loss.item()), self.grad.clone()
 
     def train(self, ctx, X, T, steps, batch=16384, lr=2e-3, lr_end=1e-4, beta1=0.9, beta2=0.999, eps=1e-8,
@@ -144,8 +154,8 @@ class MLPModel:
                 pos = 0
             idx = perm[pos:pos + batch]
             pos += batch
-            ctx.check(lib.psb_mlp_grad(ctx.h, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx), idx.numel(),
-                                       _p(self.grad), _p(loss)), "psb_mlp_grad")
+            ctx.check(lib.psb_mlp_grad(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
+                                       idx.numel(), _p(self.grad), _p(loss)), "psb_mlp_grad")
             self.step += 1
             lr_s = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * s / max(1, steps)))
             ctx.check(lib.psb_mlp_adam(ctx.h, _p(self.params), _p(self.m), _p(self.v), _p(self.grad), self.step,
@@ -318,6 +328,7 @@ def main():
     ap.add_argument("--les-steps", type=int, default=2000)
     ap.add_argument("--no-eval", action="store_true")
     ap.add_argument("--nu", type=float, default=5e-4, help="viscosity of the DNS and the LES")
+    ap.add_argument("--act", choices=sorted(ACTS), default="relu", help="hidden activation of the network")
     ap.add_argument("--eval-only", action="store_true",
                     help="re-run the a-posteriori evaluation of the model at --out and update its metadata")
     a = ap.parse_args()
@@ -334,14 +345,14 @@ def main():
     print("generating training data ...")
     X, T = generate(N_dns=a.N_dns, nu=a.nu, npoints=a.npoints)
     print(f"  {X.shape[0]} samples ({time.time() - t0:.1f} s)")
-    model = MLPModel(seed=0)
+    model = MLPModel(seed=0, act=a.act)
     model.fit_norm(X, T)
     ctx = _capi.Context(64, 64, 64, precision=32)
     hist = model.train(ctx, X, T, a.steps, batch=a.batch, log_every=max(1, a.steps // 20))
     for s, l in hist:
         print(f"  step {s:6d}  loss {l:.5f}")
     meta = {"train_samples": int(X.shape[0]), "train_steps": a.steps, "batch": a.batch,
-            "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": a.nu,
+            "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": a.nu, "act": a.act,
             "spectrum": "E(k)=16 sqrt(2/pi) u0^2 k^4/k0^5 exp(-2 k^2/k0^2), k0=4, u0=1"}
     model.meta = meta
     if not a.no_eval:

@@ -30,18 +30,19 @@ def _data(n, seed=0):
     return X, T, norm
 
 
-def _model(torch, seed, norm):
+def _model(torch, seed, norm, act="gelu"):
     from pyspectral_b200.learned import MLPModel
     P = mo.init_params(seed)
     P = P + 0.05 * np.random.default_rng(seed).standard_normal(P.shape)  # nonzero biases
-    return MLPModel(params=P, norm=norm), P
+    return MLPModel(params=P, norm=norm, act=act), P
 
 
-def test_forward_and_gradients_match_cpu_oracle():
+@pytest.mark.parametrize("act", ["gelu", "relu"])
+def test_forward_and_gradients_match_cpu_oracle(act):
     torch = _torch()
     from pyspectral_b200 import _capi
     X, T, norm = _data(300)
-    m, P = _model(torch, 3, norm)
+    m, P = _model(torch, 3, norm, act)
     ctx = _capi.Context(16, 16, 16, precision=32)
     Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
     Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
@@ -50,11 +51,11 @@ def test_forward_and_gradients_match_cpu_oracle():
     Xf = Xd.cpu().numpy().astype(np.float64)
     Tf = Td.cpu().numpy().astype(np.float64)
     Y = m.forward(ctx, Xd).cpu().numpy()
-    Yo = mo.forward(Pf, nf, Xf)
+    Yo = mo.forward(Pf, nf, Xf, act=act)
     assert rel(Y, Yo) < 2e-3
     idx = torch.arange(300, dtype=torch.int32, device="cuda")
     loss, grad = m.grad_of(ctx, Xd, Td, idx)
-    lo, go = mo.loss_and_grad(Pf, nf, Xf, Tf)
+    lo, go = mo.loss_and_grad(Pf, nf, Xf, Tf, act=act)
     assert loss == pytest.approx(lo, rel=2e-3)
     g = grad.cpu().numpy()
     # per block: W1 b1 W2 b2 W3 b3
@@ -65,14 +66,15 @@ def test_forward_and_gradients_match_cpu_oracle():
         o += k
 
 
-def test_training_reduces_loss():
+@pytest.mark.parametrize("act", ["gelu", "relu"])
+def test_training_reduces_loss(act):
     torch = _torch()
     from pyspectral_b200 import _capi
     from pyspectral_b200.learned import MLPModel
     X, T, _ = _data(1 << 15, seed=1)
     Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
     Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
-    m = MLPModel(seed=0)
+    m = MLPModel(seed=0, act=act)
     m.fit_norm(Xd, Td)
     ctx = _capi.Context(16, 16, 16, precision=32)
     idx = torch.arange(4096, dtype=torch.int32, device="cuda")
@@ -83,21 +85,21 @@ def test_training_reduces_loss():
     assert np.isfinite(l1) and l1 < 0.1 * l0, (l0, l1)
 
 
-@pytest.mark.parametrize("precision", [64, 32])
-def test_learned_rhs_matches_oracle(precision):
+@pytest.mark.parametrize("precision,act", [(64, "gelu"), (32, "gelu"), (64, "relu"), (32, "relu")])
+def test_learned_rhs_matches_oracle(precision, act):
     torch = _torch()
     from pyspectral_b200 import Classes as C
     N = 16
     st = orc.isotropic_state(N, 9, k0=3.0)
     _, _, norm = _data(500, seed=2)
-    m, P = _model(torch, 5, norm)
+    m, P = _model(torch, 5, norm, act)
     grid = C.gridclass.periodic(N)
     main = C.variables(0, "learned", 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 0.01, 0.02, precision=precision,
                        model=m)
     main.computeRHS(main, grid, None, None)
     g = orc.Grid.periodic(N)
     ref = mo.rhs_learned(g, st, 0.02, m.params.cpu().numpy().astype(np.float64),
-                         m.norm.cpu().numpy().astype(np.float64), 2 * np.pi / N)
+                         m.norm.cpu().numpy().astype(np.float64), 2 * np.pi / N, act=act)
     tol = 1e-4 if precision == 64 else 5e-4
     assert rel(main.Q.cpu().numpy(), ref) < tol
     # the closure changes the RHS (it is not the DNS one)
@@ -130,3 +132,21 @@ def test_trained_model_beats_no_model_on_unseen_dns():
     pi_model = -(Y.double() * Sv * w).sum(1)
     corr = float(torch.corrcoef(torch.stack([pi_true, pi_model]))[0, 1])
     assert corr > 0.3, corr
+
+
+def test_unknown_activation_is_rejected():
+    """mlp_act outside {GELU, ReLU} is an argument error, not a silent default."""
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.learned import MLPModel
+    N = 16
+    _, _, norm = _data(100, seed=4)
+    m, _ = _model(torch, 2, norm)
+    ctx = _capi.Context(N, N, N, precision=32)
+    st = torch.zeros((3, N, N, N // 2 + 1), dtype=torch.complex64, device="cuda")
+    rhs = torch.empty_like(st)
+    p = _capi.make_params(nu=0.01, mlp_params=m.params.data_ptr(), mlp_norm=m.norm.data_ptr(), mlp_act=7)
+    with pytest.raises(RuntimeError):
+        ctx.rhs(_capi.LEARNED, st, rhs, p)
+    with pytest.raises(ValueError):
+        MLPModel(act="tanh")
