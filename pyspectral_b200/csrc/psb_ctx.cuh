@@ -198,6 +198,20 @@ inline void set_smem(K kernel, size_t smem) {
   }
 }
 
+// Grid of a persistent kernel: at most (resident CTAs per SM) x SMs of the
+// current device, and no more CTAs than there are tiles.
+template <typename K>
+inline long long persistent_grid(K kernel, size_t smem, long long ntiles) {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, smem) != cudaSuccess || per < 1 || nsm < 1) {
+    (void)cudaGetLastError();
+    return ntiles;
+  }
+  return std::min<long long>(ntiles, (long long)per * nsm);
+}
+
 inline int pow2_floor(int x) {
   int p = 1;
   while (p * 2 <= x) p *= 2;
@@ -274,15 +288,17 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
     if (sh && sh->wide) {
       auto k = psb::zpass_kernel<T, Phys, true>;
       set_smem(k, smem);
+      const long long g = persistent_grid(k, smem, grid);
       LaunchScope scope(c, what, bytes);
-      k<<<(unsigned)grid, 256, smem, c->stream>>>(z, phys);
+      k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
       return launch_ok(c, what);
     }
   }
   auto k = psb::zpass_kernel<T, Phys>;
   set_smem(k, smem);
+  const long long g = persistent_grid(k, smem, grid);
   LaunchScope scope(c, what, bytes);
-  k<<<(unsigned)grid, 256, smem, c->stream>>>(z, phys);
+  k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
   return launch_ok(c, what);
 }
 

@@ -230,9 +230,25 @@ __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
   return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * M) * sizeof(Cx<T>) + extra;
 }
 
-// One CTA of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes
+// Per-CTA staging of the z-pass: the twiddle table and the Phys extra (the
+// MLP's fragment-ordered weights).  Done once per CTA, before its first tile.
+template <typename T, class Phys>
+__device__ __forceinline__ void zpass_setup(const ZArgs<T>& a, const Phys& phys) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  stage_twiddles(tw, a.tw, a.plan);
+  if constexpr (phys_is_block<Phys>::value) {
+    constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
+    const int nl = (FMAX * a.ppc + 1) / 2;
+    phys.setup(reinterpret_cast<unsigned char*>(tw + a.plan.L + (size_t)2 * nl * a.plan.L));
+  }
+}
+
+// One tile of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes, staged
+// by zpass_setup.  Ends with the results stored; the caller synchronises
+// before the CTA's next tile reuses the buffers.
 template <typename T, class Phys, bool WIDE = false>
-__device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
+__device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, int bx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   constexpr int FI = Phys::F_IN, FO = Phys::F_OUT;
@@ -245,8 +261,6 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
   unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * M);
   const long long p0 = (long long)bx * P;
   const int lp = __ffs(P) - 1;
-  stage_twiddles(tw, a.tw, a.plan);
-  if constexpr (phys_is_block<Phys>::value) phys.setup(extra);
   const Cx<T> zero = mk<T>(0, 0);
   const int half = M / 2;
   Cx<T>* R = X;
@@ -346,10 +360,24 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
   }
 }
 
-// grid = ceil(npencils/ppc)
+// One CTA, one tile (the batched kernel's unit).
+template <typename T, class Phys, bool WIDE = false>
+__device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
+  zpass_setup<T, Phys>(a, phys);
+  zpass_tile<T, Phys, WIDE>(a, phys, bx);
+}
+
+// Tiles bx = blockIdx.x, + gridDim.x, ... < ceil(npencils/ppc): any grid
+// size covers every tile; a grid of (resident CTAs per SM) x SMs stages the
+// twiddles and the Phys extra once per CTA instead of once per tile.
 template <typename T, class Phys, bool WIDE = false>
 __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
-  zpass_body<T, Phys, WIDE>(a, phys, blockIdx.x);
+  zpass_setup<T, Phys>(a, phys);
+  const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
+  for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
+    zpass_tile<T, Phys, WIDE>(a, phys, (int)bx);
+    __syncthreads();
+  }
 }
 
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].

@@ -670,6 +670,10 @@ struct PhysLearned {
   __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, T fac,
                                             unsigned char* extra) const {
     const MlpFwdSmem& s = *reinterpret_cast<const MlpFwdSmem*>(extra);
+    if ((M & 15) == 0 && (P & 1) == 0) {
+      block_tiles<ACT>(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, fac, s);
+      return;
+    }
     const int npts = P * M;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int nw = blockDim.x >> 5;
@@ -710,6 +714,80 @@ struct PhysLearned {
         const T o = (fac * val(ii, h)) * (fac * val(jj, h)) + tau * is2;
         const int r = c * P + rp[h];
         reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + rz[h])[r & 1] = o;
+      }
+    }
+  }
+  // The same computation when every tile is 16 consecutive z of one pencil
+  // (M % 16 == 0) and packed lines pair pencils of one field (P even): real
+  // line (f, p) is half p&1 of packed line f*P/2 + p/2, so field f of pencil
+  // p at z is T element f*P*M + 2((p/2) M + z) + (p&1).  Each lane keeps the
+  // offsets, normalisation and output coefficients of its fragment slots in
+  // registers; per tile it computes one base index per row.
+  template <int ACT>
+  __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, T fac,
+                                              const MlpFwdSmem& s) const {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int nw = blockDim.x >> 5;
+    const int fst = P * M;
+    const T is2 = (T)1 / (sphys * sphys);
+    const T fs = fac * sphys;
+    // feature slot q = 2 hk + e holds feature f = 2t + 8hk + e: a gradient
+    // (f < 9, physical field 3 + f), the filter width (f = 9) or padding
+    int foff[4];
+    float fm[4], fi[4], fc[4];
+    bool fg[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int f = 2 * t + 8 * (q >> 1) + (q & 1);
+      fg[q] = f < 9;
+      foff[q] = fg[q] ? (3 + f) * fst : 0;
+      fm[q] = f < kMlpIn ? s.xmean[f] : 0.f;
+      fi[q] = f < kMlpIn ? s.xistd[f] : 0.f;
+      fc[q] = f == 9 ? (delta - s.xmean[f]) * s.xistd[f] : 0.f;
+    }
+    // output slot e2 = e & 1: column c = 2t + e2 (valid for c < 6) = u_ii u_jj + tau_c / s^2
+    int ooff[2], ioff[2], joff[2];
+    float ys[2], ym[2];
+#pragma unroll
+    for (int e2 = 0; e2 < 2; ++e2) {
+      const int c = 2 * t + e2;
+      const int ii = c < 3 ? c : (c == 5 ? 1 : 0);
+      const int jj = c < 3 ? c : (c == 3 ? 1 : 2);
+      ooff[e2] = c * fst;
+      ioff[e2] = ii * fst;
+      joff[e2] = jj * fst;
+      ys[e2] = c < kMlpOut ? s.ystd[c] : 0.f;
+      ym[e2] = c < kMlpOut ? s.ymean[c] : 0.f;
+    }
+    const bool out_ok = t < 3;
+    const int tpp = M >> 4, ntile = P * tpp;
+    for (int tile = warp; tile < ntile; tile += nw) {
+      const int p = tile / tpp;
+      const int z0 = (tile - p * tpp) << 4;
+      const int b0 = 2 * ((p >> 1) * M + z0 + g) + (p & 1);  // row g; row g + 8 is b0 + 16
+      float v[8];
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float x = (float)(R[b0 + 16 * hr + foff[q]] * fs);
+          v[hr * 4 + q] = fg[q] ? (x - fm[q]) * fi[q] : fc[q];
+        }
+      uint32_t xa[4];
+      xa[0] = pack_bf16(v[0], v[1]);  // row g,   k 2t..2t+1
+      xa[1] = pack_bf16(v[4], v[5]);  // row g+8, k 2t..2t+1
+      xa[2] = pack_bf16(v[2], v[3]);  // row g,   k 2t+8..
+      xa[3] = pack_bf16(v[6], v[7]);  // row g+8, k 2t+8..
+      float y[4];
+      mlp_forward_fast<ACT>(s, xa, y);
+      if (out_ok) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int e2 = e & 1;
+          const int b = b0 + 16 * (e >> 1);
+          const T tau = (T)(y[e] * ys[e2] + ym[e2]);
+          W[b + ooff[e2]] = (fac * R[b + ioff[e2]]) * (fac * R[b + joff[e2]]) + tau * is2;
+        }
       }
     }
   }
