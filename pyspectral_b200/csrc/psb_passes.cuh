@@ -270,6 +270,69 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
     // the k=0 and k=M/2 terms keep their real parts only (c2r convention).  The
     // items k = 0..M/2 of every packed line write all M positions of the line
     // (zero where k is beyond the stored k3 range), so nothing needs clearing.
+    if ((P & 1) == 0) {
+      // P even: packed line c holds pencils p, p+1 (p = 2 (c mod P/2)) of
+      // field f = c / (P/2); one warp per line, lanes along k; a warp loads
+      // U of its lines before storing any, so their reads overlap
+      constexpr int U = 4;
+      const int hp = P >> 1, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      for (int cb = threadIdx.x >> 5; cb < nin; cb += U * nw) {
+        const Cx<T>* src[U];
+        long long ps[U];
+        int kz[U];
+        bool oka[U], okb[U], dz[U];
+        int kzmax = 0;
+        bool anydz = false;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int c = cb + u * nw;
+          const int f = c < nin ? c / hp : 0, p = 2 * (c - f * hp);
+          const long long pa = p0 + p;
+          kz[u] = c < nin ? min(a.in_kz[f], half + 1) : 0;
+          oka[u] = pa < a.npencils;
+          okb[u] = pa + 1 < a.npencils;
+          ps[u] = a.in_pstride[f];
+          src[u] = a.in[f] + (oka[u] ? pa * ps[u] : 0);
+          dz[u] = c < nin && a.dz[f] != 0;
+          anydz |= dz[u];
+          kzmax = max(kzmax, kz[u]);
+        }
+        for (int kb = 0; kb < kzmax; kb += 32) {
+          const int k = kb + lane;
+          Cx<T> A[U], B[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            A[u] = (k < kz[u] && oka[u]) ? src[u][k] : zero;
+            B[u] = (k < kz[u] && okb[u]) ? src[u][ps[u] + k] : zero;
+          }
+          // k3 (a table of every stored k3) exists whenever a line is a z derivative
+          const T kk = (anydz && k < kzmax) ? (T)a.k3[k] : (T)0;
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (k >= kz[u]) continue;
+            Cx<T> va = A[u], vb = B[u];
+            if (dz[u]) {
+              va = mk<T>(-kk * va.y, kk * va.x);
+              vb = mk<T>(-kk * vb.y, kk * vb.x);
+            }
+            Cx<T>* Z = X + (size_t)(cb + u * nw) * M;
+            if (k == 0 || k == half) {
+              Z[k] = mk<T>(va.x, vb.x);
+            } else {
+              Z[k] = mk<T>(va.x - vb.y, va.y + vb.x);
+              Z[M - k] = mk<T>(va.x + vb.y, vb.x - va.y);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int c = cb + u * nw;
+          if (c >= nin) continue;
+          Cx<T>* Z = X + (size_t)c * M;
+          for (int k = kz[u] + lane; k <= M - kz[u]; k += 32) Z[k] = zero;
+        }
+      }
+    } else
     for (Walk2 w(half + 1); w.s < nin; w.next()) {
       const int k = w.f, c = w.s;
       Cx<T> A = zero, B = zero;
@@ -340,6 +403,23 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
     Cx<T>* R2 = block_fft<T, false, WIDE>(W, R, a.plan, tw, nout, M, 1, false);
     // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
     const int kzo = a.out_kz;
+    if ((P & 1) == 0) {
+      // P even: one warp per packed line (field g, pencils p and p+1), lanes along k
+      const int hp = P >> 1, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+      for (int c = threadIdx.x >> 5; c < nout; c += nw) {
+        const int g = c / hp, p = 2 * (c - g * hp);
+        const long long pa = p0 + p;
+        const bool oka = pa < a.npencils, okb = pa + 1 < a.npencils;
+        const Cx<T>* Z = R2 + (size_t)c * M;
+        Cx<T>* dst = a.out[g] + pa * a.out_pstride[g];
+        const long long ps = a.out_pstride[g];
+        for (int k = lane; k < kzo; k += 32) {
+          const Cx<T> zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
+          if (oka) dst[k] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+          if (okb) dst[ps + k] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zm.x - zk.x));
+        }
+      }
+    } else
     for (Walk2 w(kzo); w.s < nout; w.next()) {
       const int k = w.f, c = w.s;
       const Cx<T>* Z = R2 + (size_t)c * M;
@@ -371,7 +451,7 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
 // size covers every tile; a grid of (resident CTAs per SM) x SMs stages the
 // twiddles and the Phys extra once per CTA instead of once per tile.
 template <typename T, class Phys, bool WIDE = false>
-__global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_kernel(ZArgs<T> a, Phys phys) {
   zpass_setup<T, Phys>(a, phys);
   const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
   for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
@@ -382,7 +462,7 @@ __global__ void __launch_bounds__(256) zpass_kernel(ZArgs<T> a, Phys phys) {
 
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
 template <typename T, class Phys, bool WIDE>
-__global__ void __launch_bounds__(256) zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
   zpass_body<T, Phys, WIDE>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
 }
 
