@@ -311,11 +311,25 @@ struct Batch {
         const long long np = (long long)d.M1 * d.M2;
         dim3 g((unsigned)((np + P - 1) / P), R);
         const size_t sm = smem_z(P);
-        auto k = zpass_batch<T, Phys, W>;
-        set_smem(k, sm);
-        LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fi + Fo));
-        k<<<g, 256, sm, c->stream>>>(az, phys);
-        return launch_ok(c, "batch z-fused");
+        auto go = [&](auto k) {
+          set_smem(k, sm);
+          LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fi + Fo));
+          k<<<g, 256, sm, c->stream>>>(az, phys);
+          return launch_ok(c, "batch z-fused");
+        };
+        if constexpr (phys_fixed_fft<Phys>::value) {
+          switch (fixed_plan_id(b->plan[2])) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (fixed_plan_compiled<T, ID>::value) return go(zpass_batch<T, Phys, false, ID>); \
+    break;
+            PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+            default:
+              break;
+          }
+        }
+        return go(zpass_batch<T, Phys, W>);
       }
       default: {
         const int ct = b->tile[4];

@@ -284,22 +284,29 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   // a field formed as d/dz of another input re-reads that input's line: no new bytes
   for (int f = 0; f < Phys::F_IN; ++f)
     if (!z.dz[f]) bytes += (double)esz * z.npencils * z.in_kz[f];
-  if constexpr (TUNABLE) {
-    if (sh && sh->wide) {
-      auto k = psb::zpass_kernel<T, Phys, true>;
-      set_smem(k, smem);
-      const long long g = persistent_grid(k, smem, grid);
-      LaunchScope scope(c, what, bytes);
-      k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
-      return launch_ok(c, what);
+  auto go = [&](auto k) {
+    set_smem(k, smem);
+    const long long g = persistent_grid(k, smem, grid);
+    LaunchScope scope(c, what, bytes);
+    k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
+    return launch_ok(c, what);
+  };
+  if constexpr (psb::phys_fixed_fft<Phys>::value) {
+    switch (psb::fixed_plan_id(z.plan)) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value) return go(psb::zpass_kernel<T, Phys, false, ID>); \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
     }
   }
-  auto k = psb::zpass_kernel<T, Phys>;
-  set_smem(k, smem);
-  const long long g = persistent_grid(k, smem, grid);
-  LaunchScope scope(c, what, bytes);
-  k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
-  return launch_ok(c, what);
+  if constexpr (TUNABLE) {
+    if (sh && sh->wide) return go(psb::zpass_kernel<T, Phys, true>);
+  }
+  return go(psb::zpass_kernel<T, Phys>);
 }
 
 // bytes: the transform input plus the epilogue's own state traffic (epi.io_bytes)

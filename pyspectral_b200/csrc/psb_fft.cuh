@@ -311,6 +311,101 @@ __device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* _
   return a;
 }
 
+
+// ---- transforms with a compile-time length and schedule --------------------
+// The same Stockham passes over `nlines` contiguous lines of length L (the
+// z-pass layout) with L, the radix and the sub-transform length Ns known to
+// the compiler: work items split into (line, j) by a constant divisor, and
+// every shared-memory offset of an item is a constant from its base.
+template <typename T, int R, bool INV, int L, int NS>
+__device__ __forceinline__ void stockham_pass_c(const Cx<T>* __restrict__ a, Cx<T>* __restrict__ b,
+                                                const Cx<T>* __restrict__ tw, int nlines) {
+  constexpr int NB = L / R;
+  constexpr int TS = L / (NS * R);
+  const int items = nlines * NB;
+  for (int it = threadIdx.x; it < items; it += blockDim.x) {
+    const int line = it / NB;
+    const int j = it - line * NB;
+    const int k = j % NS;
+    const Cx<T>* src = a + line * L + j;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[r * NB];
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        Cx<T> w = tw[r * k * TS];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    small_dft<T, R, INV>(v);
+    Cx<T>* dst = b + line * L + (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[r * NS] = v[r];
+  }
+}
+// Passes R, Rest... starting at sub-transform length NS; returns the buffer
+// holding the result.  Ends with __syncthreads.
+template <typename T, bool INV, int L, int NS, int R, int... Rest>
+__device__ __forceinline__ Cx<T>* fft_c(Cx<T>* a, Cx<T>* b, const Cx<T>* __restrict__ tw, int nlines) {
+  stockham_pass_c<T, R, INV, L, NS>(a, b, tw, nlines);
+  __syncthreads();
+  if constexpr (sizeof...(Rest) == 0)
+    return b;
+  else
+    return fft_c<T, INV, L, NS * R, Rest...>(b, a, tw, nlines);
+}
+
+// Schedules compiled in with their length (id, L, radices): the default
+// schedule of each common 3/2-padded length and its fewest-pass orders.
+#define PSB_FIXED_PLANS(X) \
+  X(1, 96, 8, 4, 3)        \
+  X(2, 96, 16, 6)          \
+  X(3, 96, 6, 16)          \
+  X(4, 48, 8, 2, 3)        \
+  X(5, 48, 16, 3)          \
+  X(6, 48, 3, 16)          \
+  X(7, 192, 8, 8, 3)       \
+  X(8, 192, 16, 12)        \
+  X(9, 192, 12, 16)
+constexpr int kFixedPlans = 9;
+
+template <int ID>
+struct FixedPlan;
+#define PSB_FIXED_PLAN_DEF(ID, LEN, ...)                                                       \
+  template <>                                                                                   \
+  struct FixedPlan<ID> {                                                                        \
+    static constexpr int L = LEN;                                                               \
+    template <typename T, bool INV>                                                             \
+    static __device__ __forceinline__ Cx<T>* run(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, int n) { \
+      return fft_c<T, INV, LEN, 1, __VA_ARGS__>(a, b, tw, n);                                   \
+    }                                                                                           \
+  };
+PSB_FIXED_PLANS(PSB_FIXED_PLAN_DEF)
+#undef PSB_FIXED_PLAN_DEF
+
+template <int... R>
+constexpr int count_radices() {
+  return (int)sizeof...(R);
+}
+// Id of the compiled-in schedule equal to p (0 if none).
+__host__ inline int fixed_plan_id(const FFTPlan& p) {
+  struct D {
+    int id, L, n, r[4];
+  };
+#define PSB_FIXED_PLAN_DESC(ID, LEN, ...) D{ID, LEN, count_radices<__VA_ARGS__>(), {__VA_ARGS__}},
+  static const D table[] = {PSB_FIXED_PLANS(PSB_FIXED_PLAN_DESC)};
+#undef PSB_FIXED_PLAN_DESC
+  for (const D& d : table) {
+    if (d.L != p.L || d.n != p.npass) continue;
+    bool same = true;
+    for (int s = 0; s < d.n; ++s) same = same && d.r[s] == p.radix[s];
+    if (same) return d.id;
+  }
+  return 0;
+}
+
 // Stage a length-L twiddle table into shared memory.
 template <typename T>
 __device__ __forceinline__ void stage_twiddles(Cx<T>* tw_s, const Cx<T>* __restrict__ pool, const FFTPlan& p) {

@@ -230,6 +230,16 @@ __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
   return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * M) * sizeof(Cx<T>) + extra;
 }
 
+// Transform of the z-pass's contiguous lines: the plan's schedule (FP = 0) or
+// the compiled-in schedule FP (which must equal the plan's).
+template <typename T, bool INV, bool WIDE, int FP>
+__device__ __forceinline__ Cx<T>* zfft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* tw, int nlines) {
+  if constexpr (FP == 0)
+    return block_fft<T, INV, WIDE>(a, b, p, tw, nlines, p.L, 1, false);
+  else
+    return FixedPlan<FP>::template run<T, INV>(a, b, tw, nlines);
+}
+
 // Per-CTA staging of the z-pass: the twiddle table and the Phys extra (the
 // MLP's fragment-ordered weights).  Done once per CTA, before its first tile.
 template <typename T, class Phys>
@@ -247,7 +257,7 @@ __device__ __forceinline__ void zpass_setup(const ZArgs<T>& a, const Phys& phys)
 // One tile of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes, staged
 // by zpass_setup.  Ends with the results stored; the caller synchronises
 // before the CTA's next tile reuses the buffers.
-template <typename T, class Phys, bool WIDE = false>
+template <typename T, class Phys, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, int bx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -360,7 +370,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
       }
     }
     __syncthreads();
-    R = block_fft<T, true, WIDE>(X, Y, a.plan, tw, nin, M, 1, false);
+    R = zfft<T, true, WIDE, FP>(X, Y, a.plan, tw, nin);
   }
   Cx<T>* W = (R == X) ? Y : X;
   const int nout = (FO * P + 1) / 2;
@@ -400,7 +410,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
   }
   if constexpr (FO > 0) {
     __syncthreads();
-    Cx<T>* R2 = block_fft<T, false, WIDE>(W, R, a.plan, tw, nout, M, 1, false);
+    Cx<T>* R2 = zfft<T, false, WIDE, FP>(W, R, a.plan, tw, nout);
     // unpack: A_k = (Z_k + conj(Z_{M-k}))/2, B_k = (Z_k - conj(Z_{M-k}))/(2i)
     const int kzo = a.out_kz;
     if ((P & 1) == 0) {
@@ -441,30 +451,44 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
 }
 
 // One CTA, one tile (the batched kernel's unit).
-template <typename T, class Phys, bool WIDE = false>
+template <typename T, class Phys, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
   zpass_setup<T, Phys>(a, phys);
-  zpass_tile<T, Phys, WIDE>(a, phys, bx);
+  zpass_tile<T, Phys, WIDE, FP>(a, phys, bx);
 }
 
 // Tiles bx = blockIdx.x, + gridDim.x, ... < ceil(npencils/ppc): any grid
 // size covers every tile; a grid of (resident CTAs per SM) x SMs stages the
 // twiddles and the Phys extra once per CTA instead of once per tile.
-template <typename T, class Phys, bool WIDE = false>
+// FP: compiled-in transform schedule (FixedPlan id) equal to a.plan, or 0.
+template <typename T, class Phys, bool WIDE = false, int FP = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_kernel(ZArgs<T> a, Phys phys) {
   zpass_setup<T, Phys>(a, phys);
   const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
   for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
-    zpass_tile<T, Phys, WIDE>(a, phys, (int)bx);
+    zpass_tile<T, Phys, WIDE, FP>(a, phys, (int)bx);
     __syncthreads();
   }
 }
 
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
-template <typename T, class Phys, bool WIDE>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
-  zpass_body<T, Phys, WIDE>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
+template <typename T, class Phys, bool WIDE, int FP = 0>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
+  zpass_body<T, Phys, WIDE, FP>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
 }
+
+// Closures whose z-pass is compiled with the fixed schedules (the 3/2-padded
+// Navier-Stokes closures: DNS products, Smagorinsky, learned); FP64 only with
+// the default schedule of each length.
+template <class Phys>
+struct phys_fixed_fft {
+  static constexpr bool value = false;
+};
+template <typename T, int FP>
+struct fixed_plan_compiled {
+  static constexpr bool value = sizeof(T) == 4 || FP == 1 || FP == 4 || FP == 7;
+};
 
 // ---------------------------------------------------------------------------
 template <typename T>

@@ -793,4 +793,17 @@ struct PhysLearned {
   }
 };
 
+template <typename T>
+struct phys_fixed_fft<PhysProducts<T>> {
+  static constexpr bool value = true;
+};
+template <typename T>
+struct phys_fixed_fft<PhysSmag<T>> {
+  static constexpr bool value = true;
+};
+template <typename T>
+struct phys_fixed_fft<PhysLearned<T>> {
+  static constexpr bool value = true;
+};
+
 }  // namespace psb
