@@ -12,6 +12,7 @@
 // runs' states untouched.
 #include <algorithm>
 #include <array>
+#include <type_traits>
 #include <cstring>
 
 #include "psb_ctx.cuh"
@@ -271,6 +272,22 @@ struct Batch {
       if (p.radix[s] > 8 || p.radix[s] == 6) return true;
     return false;
   }
+  // fix(integral_constant<int, ID>) when the pass's plan is a compiled-in
+  // schedule ID (for this precision), else def().
+  template <class Fix, class Def>
+  int by_plan(int pass, Fix fix, Def def) {
+    switch (fixed_plan_id(b->plan[pass])) {
+#define PSB_FIXED_CASE(ID, ...)                                                             \
+  case ID:                                                                                  \
+    if constexpr (fixed_plan_compiled<T, ID>::value) return fix(std::integral_constant<int, ID>{}); \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
+    }
+    return def();
+  }
   template <bool W>
   int launch_w(int pass, int stage) {
     const size_t esz = sizeof(Cx<T>);
@@ -279,11 +296,15 @@ struct Batch {
         const int ct = b->tile[0];
         dim3 g((d.Kz + ct - 1) / ct, d.N2, R);
         const size_t sm = smem_axis(d.M1, Fi, ct);
-        auto k = axis_pass_batch<T, true, Pre, W>;
-        set_smem(k, sm);
-        LaunchScope s(c, "batch x-inverse", (double)R * esz * d.N2 * d.Kz * (3.0 * d.N1 + (double)Fi * d.M1));
-        k<<<g, 256, sm, c->stream>>>(ax, pre);
-        return launch_ok(c, "batch x-inverse");
+        auto go = [&](auto k) {
+          set_smem(k, sm);
+          LaunchScope s(c, "batch x-inverse", (double)R * esz * d.N2 * d.Kz * (3.0 * d.N1 + (double)Fi * d.M1));
+          k<<<g, 256, sm, c->stream>>>(ax, pre);
+          return launch_ok(c, "batch x-inverse");
+        };
+        return by_plan(
+            0, [&](auto id) { return go(axis_pass_batch<T, true, Pre, false, decltype(id)::value>); },
+            [&] { return go(axis_pass_batch<T, true, Pre, W>); });
       }
       case 1:
       case 3: {
@@ -294,17 +315,25 @@ struct Batch {
         const size_t sm = smem_axis(d.M2, 1, ct);
         const double by = (double)R * esz * F * d.M1 * d.Kz * (double)(d.N2 + d.M2);
         if (inv) {
-          auto k = axis_pass_batch<T, true, PreCopy<T>, W>;
-          set_smem(k, sm);
-          LaunchScope s(c, "batch y-inverse", by);
-          k<<<g, 256, sm, c->stream>>>(ay, cpy);
-        } else {
-          auto k = axis_pass_batch<T, false, PreCopy<T>, W>;
+          auto go = [&](auto k) {
+            set_smem(k, sm);
+            LaunchScope s(c, "batch y-inverse", by);
+            k<<<g, 256, sm, c->stream>>>(ay, cpy);
+            return launch_ok(c, "batch y-inverse");
+          };
+          return by_plan(
+              1, [&](auto id) { return go(axis_pass_batch<T, true, PreCopy<T>, false, decltype(id)::value>); },
+              [&] { return go(axis_pass_batch<T, true, PreCopy<T>, W>); });
+        }
+        auto go = [&](auto k) {
           set_smem(k, sm);
           LaunchScope s(c, "batch y-forward", by);
           k<<<g, 256, sm, c->stream>>>(ayf, cpy);
-        }
-        return launch_ok(c, inv ? "batch y-inverse" : "batch y-forward");
+          return launch_ok(c, "batch y-forward");
+        };
+        return by_plan(
+            3, [&](auto id) { return go(axis_pass_batch<T, false, PreCopy<T>, false, decltype(id)::value>); },
+            [&] { return go(axis_pass_batch<T, false, PreCopy<T>, W>); });
       }
       case 2: {
         const int P = b->tile[2];
@@ -317,18 +346,10 @@ struct Batch {
           k<<<g, 256, sm, c->stream>>>(az, phys);
           return launch_ok(c, "batch z-fused");
         };
-        if constexpr (phys_fixed_fft<Phys>::value) {
-          switch (fixed_plan_id(b->plan[2])) {
-#define PSB_FIXED_CASE(ID, ...) \
-  case ID:                      \
-    if constexpr (fixed_plan_compiled<T, ID>::value) return go(zpass_batch<T, Phys, false, ID>); \
-    break;
-            PSB_FIXED_PLANS(PSB_FIXED_CASE)
-#undef PSB_FIXED_CASE
-            default:
-              break;
-          }
-        }
+        if constexpr (phys_fixed_fft<Phys>::value)
+          return by_plan(
+              2, [&](auto id) { return go(zpass_batch<T, Phys, false, decltype(id)::value>); },
+              [&] { return go(zpass_batch<T, Phys, W>); });
         return go(zpass_batch<T, Phys, W>);
       }
       default: {
@@ -339,13 +360,17 @@ struct Batch {
         const int extra = (int)std::min<long long>((pts + 255) / 256, 1024);
         dim3 g(mainb + extra, R);
         const size_t sm = smem_axis(d.M1, Fo, ct);
-        auto k = xfwd_epi_batch<T, Epi, W>;
-        set_smem(k, sm);
         const double by = (double)R * (esz * Fo * d.M1 * d.N2 * d.Kz + esz * 3.0 * d.N1 * d.N2 * d.N3h *
                                                                            3.0);
-        LaunchScope s(c, "batch x-forward+epilogue", by);
-        k<<<g, 256, sm, c->stream>>>(ae, epi + (size_t)stage * R);
-        return launch_ok(c, "batch x-forward+epilogue");
+        auto go = [&](auto k) {
+          set_smem(k, sm);
+          LaunchScope s(c, "batch x-forward+epilogue", by);
+          k<<<g, 256, sm, c->stream>>>(ae, epi + (size_t)stage * R);
+          return launch_ok(c, "batch x-forward+epilogue");
+        };
+        return by_plan(
+            4, [&](auto id) { return go(xfwd_epi_batch<T, Epi, false, decltype(id)::value>); },
+            [&] { return go(xfwd_epi_batch<T, Epi, W>); });
       }
     }
   }

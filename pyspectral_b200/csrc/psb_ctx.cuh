@@ -245,20 +245,26 @@ int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const
   dim3 grid((a.ncols + a.col_tile - 1) / a.col_tile, a.nouter);
   const double bytes = (double)esz * a.nouter * a.ncols *
                        ((double)Pre::F_SRC * count_mapped(a.in_map, a.in_rows) + (double)Pre::F_DST * a.out_rows);
+  auto go = [&](auto k) {
+    set_smem(k, smem);
+    LaunchScope scope(c, what, bytes);
+    k<<<grid, 256, smem, c->stream>>>(a, pre);
+    return launch_ok(c, what);
+  };
   if constexpr (TUNABLE) {
-    if (sh && sh->wide) {
-      auto k = psb::axis_pass_kernel<T, INV, Pre, true>;
-      set_smem(k, smem);
-      LaunchScope scope(c, what, bytes);
-      k<<<grid, 256, smem, c->stream>>>(a, pre);
-      return launch_ok(c, what);
+    switch (psb::fixed_plan_id(a.plan)) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value) return go(psb::axis_pass_kernel<T, INV, Pre, false, ID>); \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
     }
+    if (sh && sh->wide) return go(psb::axis_pass_kernel<T, INV, Pre, true>);
   }
-  auto k = psb::axis_pass_kernel<T, INV, Pre>;
-  set_smem(k, smem);
-  LaunchScope scope(c, what, bytes);
-  k<<<grid, 256, smem, c->stream>>>(a, pre);
-  return launch_ok(c, what);
+  return go(psb::axis_pass_kernel<T, INV, Pre>);
 }
 
 template <typename T, class Phys, bool TUNABLE = false>
@@ -328,20 +334,26 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
   }
   const size_t smem = (size_t)(L + 2 * L * Epi::F_IN * e.col_tile) * esz;
   const double bytes = epi.io_bytes((long long)e.n1 * e.n2 * e.n3h) + (double)esz * Epi::F_IN * L * e.n2 * e.kz;
+  auto go = [&](auto k) {
+    set_smem(k, smem);
+    LaunchScope scope(c, what, bytes);
+    k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
+    return launch_ok(c, what);
+  };
   if constexpr (TUNABLE) {
-    if (sh && sh->wide) {
-      auto k = psb::xfwd_epi_kernel<T, Epi, true>;
-      set_smem(k, smem);
-      LaunchScope scope(c, what, bytes);
-      k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
-      return launch_ok(c, what);
+    switch (psb::fixed_plan_id(e.plan)) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value) return go(psb::xfwd_epi_kernel<T, Epi, false, ID>); \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
     }
+    if (sh && sh->wide) return go(psb::xfwd_epi_kernel<T, Epi, true>);
   }
-  auto k = psb::xfwd_epi_kernel<T, Epi>;
-  set_smem(k, smem);
-  LaunchScope scope(c, what, bytes);
-  k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
-  return launch_ok(c, what);
+  return go(psb::xfwd_epi_kernel<T, Epi>);
 }
 
 // The fewest-pass schedule of n over radices {16, 12, 8, 6, 4, 3, 2}.

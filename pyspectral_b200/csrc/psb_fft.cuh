@@ -357,6 +357,53 @@ __device__ __forceinline__ Cx<T>* fft_c(Cx<T>* a, Cx<T>* b, const Cx<T>* __restr
     return fft_c<T, INV, L, NS * R, Rest...>(b, a, tw, nlines);
 }
 
+// The same for lines adjacent in memory (element j of line f at f + j*es, the
+// axis-pass layout): items walk (line fast, j slow) as a counter pair.
+template <typename T, int R, bool INV, int L, int NS>
+__device__ __forceinline__ void stockham_pass_cs(const Cx<T>* __restrict__ a, Cx<T>* __restrict__ b,
+                                                 const Cx<T>* __restrict__ tw, int nlines, int es) {
+  constexpr int NB = L / R;
+  constexpr int TS = L / (NS * R);
+  const int nt = blockDim.x;
+  int f = threadIdx.x % nlines, j = threadIdx.x / nlines;
+  const int df = nt % nlines, dj = nt / nlines;
+  const int rs = NB * es, ws = NS * es;
+  while (j < NB) {
+    const int k = j % NS;
+    const Cx<T>* src = a + f + j * es;
+    Cx<T> v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[r * rs];
+    if constexpr (NS > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        Cx<T> w = tw[r * k * TS];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    small_dft<T, R, INV>(v);
+    Cx<T>* dst = b + f + ((j - k) * R + k) * es;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[r * ws] = v[r];
+    f += df;
+    j += dj;
+    if (f >= nlines) {
+      f -= nlines;
+      ++j;
+    }
+  }
+}
+template <typename T, bool INV, int L, int NS, int R, int... Rest>
+__device__ __forceinline__ Cx<T>* fft_cs(Cx<T>* a, Cx<T>* b, const Cx<T>* __restrict__ tw, int nlines) {
+  stockham_pass_cs<T, R, INV, L, NS>(a, b, tw, nlines, nlines);
+  __syncthreads();
+  if constexpr (sizeof...(Rest) == 0)
+    return b;
+  else
+    return fft_cs<T, INV, L, NS * R, Rest...>(b, a, tw, nlines);
+}
+
 // Schedules compiled in with their length (id, L, radices): the default
 // schedule of each common 3/2-padded length and its fewest-pass orders.
 #define PSB_FIXED_PLANS(X) \
@@ -380,6 +427,11 @@ struct FixedPlan;
     template <typename T, bool INV>                                                             \
     static __device__ __forceinline__ Cx<T>* run(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, int n) { \
       return fft_c<T, INV, LEN, 1, __VA_ARGS__>(a, b, tw, n);                                   \
+    }                                                                                           \
+    template <typename T, bool INV>                                                             \
+    static __device__ __forceinline__ Cx<T>* run_adjacent(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, \
+                                                          int n) {                              \
+      return fft_cs<T, INV, LEN, 1, __VA_ARGS__>(a, b, tw, n);                                  \
     }                                                                                           \
   };
 PSB_FIXED_PLANS(PSB_FIXED_PLAN_DEF)

@@ -122,7 +122,17 @@ struct PreCopy {
 
 // One CTA of an axis pass: column tile bx, outer index by.
 // smem = tw[L] + 2 * L*lines
-template <typename T, bool INV, class Pre, bool WIDE = false>
+// Transform of `lines` adjacent lines (axis-pass layout): the plan's schedule
+// (FP = 0) or the compiled-in schedule FP (which must equal the plan's).
+template <typename T, bool INV, bool WIDE, int FP>
+__device__ __forceinline__ Cx<T>* axfft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* tw, int lines) {
+  if constexpr (FP == 0)
+    return block_fft<T, INV, WIDE>(a, b, p, tw, lines, 1, lines, true);
+  else
+    return FixedPlan<FP>::template run_adjacent<T, INV>(a, b, tw, lines);
+}
+
+template <typename T, bool INV, class Pre, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -169,7 +179,7 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
     for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, INV, WIDE>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  Cx<T>* res = axfft<T, INV, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
   Cx<T>* outb = a.out + (long long)o * a.out_ostride;
   if (!colok || threadIdx.x >= dr * ct) return;
   const int nrow = a.out_rows * Pre::F_DST;
@@ -181,16 +191,16 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
 }
 
 // grid = (ceil(ncols/col_tile), nouter)
-template <typename T, bool INV, class Pre, bool WIDE = false>
+template <typename T, bool INV, class Pre, bool WIDE = false, int FP = 0>
 __global__ void __launch_bounds__(256) axis_pass_kernel(AxisArgs<T> a, Pre pre) {
-  axis_pass_body<T, INV, Pre, WIDE>(a, pre, blockIdx.x, blockIdx.y);
+  axis_pass_body<T, INV, Pre, WIDE, FP>(a, pre, blockIdx.x, blockIdx.y);
 }
 
 // Batched: grid = (ceil(ncols/col_tile), nouter, runs); run blockIdx.z takes
 // its arguments from A[z] and pre[z] (same tile shape for every run).
-template <typename T, bool INV, class Pre, bool WIDE>
+template <typename T, bool INV, class Pre, bool WIDE, int FP = 0>
 __global__ void __launch_bounds__(256) axis_pass_batch(const AxisArgs<T>* __restrict__ A, const Pre* __restrict__ pre) {
-  axis_pass_body<T, INV, Pre, WIDE>(A[blockIdx.z], pre[blockIdx.z], blockIdx.x, blockIdx.y);
+  axis_pass_body<T, INV, Pre, WIDE, FP>(A[blockIdx.z], pre[blockIdx.z], blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,7 +516,7 @@ struct XEpiArgs {
 
 // One CTA of the x-forward epilogue pass: block bx of gx = main_blocks + extra;
 // main block b -> (col tile b % ntile, outer b / ntile)
-template <typename T, class Epi, bool WIDE = false>
+template <typename T, class Epi, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& epi, int bx, int gx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int F = Epi::F_IN;
@@ -549,7 +559,7 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
     bufA[(size_t)j * lines + f * ct + c] = colok ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
   }
   __syncthreads();
-  Cx<T>* res = block_fft<T, false, WIDE>(bufA, bufB, a.plan, tw, lines, 1, lines, true);
+  Cx<T>* res = axfft<T, false, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
   // threads past the last full row of columns would repeat a (row, column)
   // (only when ct does not divide the CTA size): the epilogue is not idempotent
   if (!colok || threadIdx.x >= dr * ct) return;
@@ -562,15 +572,15 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
 }
 
 // grid = main_blocks + extra
-template <typename T, class Epi, bool WIDE = false>
+template <typename T, class Epi, bool WIDE = false, int FP = 0>
 __global__ void __launch_bounds__(256) xfwd_epi_kernel(XEpiArgs<T> a, Epi epi) {
-  xfwd_epi_body<T, Epi, WIDE>(a, epi, blockIdx.x, gridDim.x);
+  xfwd_epi_body<T, Epi, WIDE, FP>(a, epi, blockIdx.x, gridDim.x);
 }
 
 // Batched: grid = (main_blocks + extra, runs); run blockIdx.y reads A[y], epi[y].
-template <typename T, class Epi, bool WIDE>
+template <typename T, class Epi, bool WIDE, int FP = 0>
 __global__ void __launch_bounds__(256) xfwd_epi_batch(const XEpiArgs<T>* __restrict__ A, const Epi* __restrict__ epi) {
-  xfwd_epi_body<T, Epi, WIDE>(A[blockIdx.y], epi[blockIdx.y], blockIdx.x, gridDim.x);
+  xfwd_epi_body<T, Epi, WIDE, FP>(A[blockIdx.y], epi[blockIdx.y], blockIdx.x, gridDim.x);
 }
 
 }  // namespace psb
