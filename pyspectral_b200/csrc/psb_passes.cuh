@@ -163,20 +163,33 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
       for (int l = threadIdx.x; l < lines; l += nt) bufA[(size_t)j * lines + l] = zero;
   }
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
-  for (int i = r0; i < a.in_rows; i += dr) {
-    const int j = a.in_map(i);
-    if (j < 0) continue;
-    Cx<T> s[Pre::F_SRC], d[Pre::F_DST];
-    if (colok) {
+  // U rows per round: every load of a round is issued before the first store
+  constexpr int U = Pre::F_SRC >= 3 ? 2 : (Pre::F_SRC == 2 ? 4 : 8);
+  for (int i0 = r0; i0 < a.in_rows; i0 += U * dr) {
+    Cx<T> s[U][Pre::F_SRC];
 #pragma unroll
-      for (int f = 0; f < Pre::F_SRC; ++f) s[f] = inb[f * a.in_fstride + i * a.in_rstride + col];
-      pre(i, o, col, a, s, d);
-    } else {
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * dr;
 #pragma unroll
-      for (int g = 0; g < Pre::F_DST; ++g) d[g] = zero;
+      for (int f = 0; f < Pre::F_SRC; ++f)
+        s[u][f] = (colok && i < a.in_rows) ? inb[f * a.in_fstride + i * a.in_rstride + col] : zero;
     }
 #pragma unroll
-    for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
+    for (int u = 0; u < U; ++u) {
+      const int i = i0 + u * dr;
+      if (i >= a.in_rows) break;
+      const int j = a.in_map(i);
+      if (j < 0) continue;
+      Cx<T> d[Pre::F_DST];
+      if (colok) {
+        pre(i, o, col, a, s[u], d);
+      } else {
+#pragma unroll
+        for (int g = 0; g < Pre::F_DST; ++g) d[g] = zero;
+      }
+#pragma unroll
+      for (int g = 0; g < Pre::F_DST; ++g) bufA[(size_t)j * lines + g * ct + c] = d[g];
+    }
   }
   __syncthreads();
   Cx<T>* res = axfft<T, INV, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
@@ -554,9 +567,22 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
   const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
   const int col = c0 + c;
   const bool colok = col < a.kz;
-  for (int t = r0; t < L * F; t += dr) {
-    const int j = t / F, f = t - j * F;
-    bufA[(size_t)j * lines + f * ct + c] = colok ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
+  // 8 loads in flight per thread before their stores
+  for (int t0 = r0; t0 < L * F; t0 += 8 * dr) {
+    Cx<T> v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * dr;
+      const int j = t / F, f = t - j * F;
+      v[u] = (colok && t < L * F) ? inb[f * a.in_fstride + j * a.in_rstride + col] : zero;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int t = t0 + u * dr;
+      if (t >= L * F) break;
+      const int j = t / F, f = t - j * F;
+      bufA[(size_t)j * lines + f * ct + c] = v[u];
+    }
   }
   __syncthreads();
   Cx<T>* res = axfft<T, false, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
