@@ -489,7 +489,7 @@ EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
 }
 
 // Default launch shapes: the single-run rules of the library.
-void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int max_ppc, size_t zextra) {
+void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int ppc, size_t zextra) {
   psb_ctx* c = b->c;
   const Dims d = dims(c, Fi, Fo);
   b->tile[0] = pick_ct(d.Kz, Fi, d.M1, esz, d.N2);
@@ -497,7 +497,7 @@ void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int max_ppc, size_
   b->tile[3] = pick_ct(d.Kz, 1, d.M2, esz, Fo * d.M1);
   b->tile[4] = pick_ct(d.Kz, Fo, d.M1, esz, d.N2);
   const int FMAX = std::max(Fi, Fo);
-  int P = max_ppc;
+  int P = ppc;
   auto sm = [&](int P) { return (size_t)(d.M3 + 2 * (size_t)((FMAX * P + 1) / 2) * d.M3) * esz + zextra; };
   while (P > 1 && sm(P) > kSmemBudget) P /= 2;
   // at least ~2 CTAs per SM over the whole batch (the single-run rule at nruns = 1)
@@ -530,7 +530,8 @@ int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_
     b->arena_bytes = need;
   }
   if (b->plan[0].L == 0)
-    default_shapes(b, BT::Fi, BT::Fo, sizeof(Cx<T>), phys_max_ppc<Phys>::value, (size_t)phys_is_block<Phys>::extra);
+    default_shapes(b, BT::Fi, BT::Fo, sizeof(Cx<T>), phys_default_ppc<Phys>::value,
+                   (size_t)phys_is_block<Phys>::extra);
   if (b->dirty) {
     PSB_TRY(x.build(pre0, mkphys, mkepi));
     b->dirty = false;

@@ -276,7 +276,7 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   constexpr size_t extra = (size_t)psb::phys_is_block<Phys>::extra;
   (void)esz;
   auto smem_for = [&](int P) { return psb::zpass_smem_bytes<T>(FMAX, P, M, extra); };
-  int P = psb::phys_max_ppc<Phys>::value;
+  int P = psb::phys_default_ppc<Phys>::value;
   while (P > 1 && smem_for(P) > kSmemBudget) P /= 2;
   while (P > 1 && (z.npencils + P - 1) / P < 2 * 148) P /= 2;
   if (sh && sh->tile) {

@@ -94,6 +94,15 @@ template <class P>
 struct phys_max_ppc<P, decltype((void)P::MAX_PPC, void())> {
   static constexpr int value = P::MAX_PPC;
 };
+// Pencils per CTA of the untuned launch shape (Phys::DEFAULT_PPC, else the bound).
+template <class P, class = void>
+struct phys_default_ppc {
+  static constexpr int value = phys_max_ppc<P>::value;
+};
+template <class P>
+struct phys_default_ppc<P, decltype((void)P::DEFAULT_PPC, void())> {
+  static constexpr int value = P::DEFAULT_PPC;
+};
 
 template <typename T>
 struct AxisArgs {

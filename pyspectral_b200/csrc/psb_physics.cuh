@@ -646,7 +646,9 @@ struct PhysLearned {
   static constexpr int F_IN = 12, F_OUT = 6;
   static constexpr bool BLOCK = true;
   static constexpr int EXTRA_SMEM = (int)((sizeof(MlpFwdSmem) + 15) / 16 * 16);
-  static constexpr int MAX_PPC = 4;  // 4 pencils per CTA: 3-4 CTAs per SM at 3N/2 = 96 (FP32)
+  // 4 pencils per CTA by default (3 CTAs per SM at 3N/2 = 96, FP32); the
+  // autotuner also tries 8 (fuller transform passes, 2 CTAs per SM)
+  static constexpr int DEFAULT_PPC = 4, MAX_PPC = 8;
   const float* params;
   const float* norm;
   T sphys;      // s: physical = real-space * s

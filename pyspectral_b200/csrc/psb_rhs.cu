@@ -880,14 +880,17 @@ template <typename T>
 int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
-  int Fi, Fo, maxppc;
+  int Fi, Fo, maxppc, defppc;
   size_t zextra = 0;
   if (closure == PSB_DNS) {
     Fi = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
+    defppc = phys_default_ppc<PhysProducts<T>>::value;
   } else if (closure == PSB_SMAG) {
     Fi = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
+    defppc = phys_default_ppc<PhysSmag<T>>::value;
   } else {
     Fi = PreGradXY<T>::F_DST, Fo = 6, maxppc = phys_max_ppc<PhysLearned<T>>::value;
+    defppc = phys_default_ppc<PhysLearned<T>>::value;
     zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
   }
   const size_t esz = sizeof(Cx<T>);
@@ -903,7 +906,7 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const StepIO<T> io = make_io<T>(c, q, q0, cp, nullptr, nullptr, nullptr, kStageMid, p->dt / 3.0);
   const int FMAX = std::max(Fi, Fo);
   auto zsmem = [&](int P) { return zpass_smem_bytes<T>(FMAX, P, M3, zextra); };
-  int P = maxppc;
+  int P = defppc;
   while (P > 1 && zsmem(P) > kSmemBudget) P /= 2;
   while (P > 1 && ((long long)M1 * M2 + P - 1) / P < 2 * 148) P /= 2;
   psb_tuned t;
