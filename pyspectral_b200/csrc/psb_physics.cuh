@@ -641,7 +641,9 @@ struct PreGradXY {
 // transform per component carries both: out_ij = u_i u_j + tau_ij / s^2 in the
 // reference's real-space scaling (real-space arrays equal physical / s).
 // The MLP runs warp-cooperatively on tensor cores over all points of the CTA.
-template <typename T>
+// ACT: the network's hidden activation (kActRelu or kActGelu); a separate
+// kernel per activation keeps the ReLU kernel free of the GELU's registers.
+template <typename T, int ACT = kActRelu>
 struct PhysLearned {
   static constexpr int F_IN = 12, F_OUT = 6;
   static constexpr bool BLOCK = true;
@@ -653,27 +655,20 @@ struct PhysLearned {
   const float* norm;
   T sphys;      // s: physical = real-space * s
   float delta;  // filter width fed to the MLP
-  int act;      // kActGelu or kActRelu
   __device__ void setup(unsigned char* extra) const {
     mlp_stage_fwd(*reinterpret_cast<MlpFwdSmem*>(extra), params, norm);
   }
-  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long a, long long b,
+  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
                         unsigned char* extra) const {
-    if (act == kActRelu)
-      block_act<kActRelu>(R, W, P, M, fac, extra);
-    else
-      block_act<kActGelu>(R, W, P, M, fac, extra);
-    (void)a;
-    (void)b;
+    block_act(R, W, P, M, fac, extra);
   }
   // Each warp takes tiles of 16 consecutive points (pencil-major); a lane
   // holds rows g and g+8 of a tile and locates them once per tile.
-  template <int ACT>
   __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, T fac,
                                             unsigned char* extra) const {
     const MlpFwdSmem& s = *reinterpret_cast<const MlpFwdSmem*>(extra);
     if ((M & 15) == 0 && (P & 1) == 0) {
-      block_tiles<ACT>(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, fac, s);
+      block_tiles(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, fac, s);
       return;
     }
     const int npts = P * M;
@@ -725,7 +720,6 @@ struct PhysLearned {
   // p at z is T element f*P*M + 2((p/2) M + z) + (p&1).  Each lane keeps the
   // offsets, normalisation and output coefficients of its fragment slots in
   // registers; per tile it computes one base index per row.
-  template <int ACT>
   __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, T fac,
                                               const MlpFwdSmem& s) const {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
@@ -803,8 +797,9 @@ template <typename T>
 struct phys_fixed_fft<PhysSmag<T>> {
   static constexpr bool value = true;
 };
+// (the GELU network keeps the runtime schedules: it is not the shipped model)
 template <typename T>
-struct phys_fixed_fft<PhysLearned<T>> {
+struct phys_fixed_fft<PhysLearned<T, kActRelu>> {
   static constexpr bool value = true;
 };
 

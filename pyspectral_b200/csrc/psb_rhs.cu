@@ -839,9 +839,12 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
                           (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
       const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
-      PhysLearned<T> phys{reinterpret_cast<const float*>(p->mlp_params), reinterpret_cast<const float*>(p->mlp_norm),
-                          (T)s32, (float)(p->les_delta > 0 ? p->les_delta : c->Delta), p->mlp_act};
-      return run_ns32<T>(c, Qin, PreGradXY<T>{}, phys, epi, ts);
+      const float* mp = reinterpret_cast<const float*>(p->mlp_params);
+      const float* mn = reinterpret_cast<const float*>(p->mlp_norm);
+      const float delta = (float)(p->les_delta > 0 ? p->les_delta : c->Delta);
+      if (p->mlp_act == PSB_ACT_GELU)
+        return run_ns32<T>(c, Qin, PreGradXY<T>{}, PhysLearned<T, kActGelu>{mp, mn, (T)s32, delta}, epi, ts);
+      return run_ns32<T>(c, Qin, PreGradXY<T>{}, PhysLearned<T, kActRelu>{mp, mn, (T)s32, delta}, epi, ts);
     }
     default:
       return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");

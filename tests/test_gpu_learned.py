@@ -152,3 +152,26 @@ def test_unknown_activation_is_rejected():
         ctx.rhs(_capi.LEARNED, st, rhs, p)
     with pytest.raises(ValueError):
         MLPModel(act="tanh")
+
+
+def test_batch_rejects_mixed_activations():
+    """A learned batch runs one kernel per activation: all its runs share it."""
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.ensemble import Batch
+    N = 16
+    _, _, norm = _data(100, seed=6)
+    m_relu, _ = _model(torch, 2, norm, "relu")
+    m_gelu, _ = _model(torch, 3, norm, "gelu")
+    ctx = _capi.Context(N, N, N, precision=32)
+    b = Batch(ctx, _capi.LEARNED, 2)
+    states = [torch.zeros((3, N, N, N // 2 + 1), dtype=torch.complex64, device="cuda") for _ in range(2)]
+    comps = [torch.zeros_like(s) for s in states]
+    for r, m in enumerate((m_relu, m_gelu)):
+        p = _capi.make_params(nu=0.01, dt=1e-3, mlp_params=m.params.data_ptr(), mlp_norm=m.norm.data_ptr(),
+                              les_delta=2 * np.pi / N, mlp_act=m.act)
+        if r == 0:
+            b.set_run(r, states[r], comps[r], p)
+        else:
+            with pytest.raises(RuntimeError):
+                b.set_run(r, states[r], comps[r], p)
