@@ -170,6 +170,11 @@ int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* cou
 int psb_mlp_sizes(int* nparams, int* nnorm);
 /* Y[B][6] = tau(X[B][10]) (raw units in and out). */
 int psb_mlp_forward(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, int B, float* Y);
+/* The same forward pass on the fifth-generation tensor cores (tcgen05.mma,
+ * 128-point tiles, FP32 accumulators in tensor memory).  err: optional device
+ * int set to 1 if an MMA did not complete within the kernel's wait bound. */
+int psb_mlp_forward_tc(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, int B, float* Y,
+                       int* err);
 /* grad += d(MSE of normalised outputs)/d(params) over the B points X[idx[b]],
  * T[idx[b]]; *loss (device double) += the MSE. */
 int psb_mlp_grad(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, const float* T,

@@ -25,6 +25,7 @@ EXPORTS = (
     "psb_spectrum", "psb_spectrum_nbins", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
     "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
     "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
+    "psb_mlp_forward_tc",
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
     "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear",

@@ -9,6 +9,7 @@
 
 #include "psb_ctx.cuh"
 #include "psb_mlp.cuh"
+#include "psb_tc.cuh"
 
 using namespace psb;
 using namespace psbh;
@@ -283,9 +284,219 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
   }
 }
 
+// ---- inference on the fifth-generation tensor cores (tcgen05) -------------
+// Tiles of 128 points: the CTA writes the tile's normalised features as the
+// A operand of layer 1 (one 128 x 16 slab), one thread issues the MMA into a
+// 128-lane x 64-column FP32 accumulator in tensor memory, the eight warps read
+// it back (warp w: lanes 32 (w % 4).., columns 32 (w / 4)..), add the bias,
+// apply the activation and write BF16 activations as the next layer's A
+// operand (four 128 x 16 slabs); layers 2 and 3 are four K-steps each.  The
+// weights are staged once per CTA as K-major slabs (B operands).
+struct MlpTcSmem {
+  unsigned char w1[64 * 16 * 2];      // 64 x 16 (k 10..15 zero)
+  unsigned char w2[4 * 64 * 16 * 2];  // 4 slabs of 64 x 16
+  unsigned char w3[4 * 16 * 16 * 2];  // 4 slabs of 16 x 16 (rows 6..15 zero)
+  unsigned char h[4 * 128 * 16 * 2];  // activations: 4 slabs of 128 x 16 (slab 0 = layer-1 input)
+  float b1[kMlpH], b2[kMlpH], b3[16];
+  float xmean[16], xistd[16], ymean[8], ystd[8];
+  unsigned long long mbar;
+  uint32_t tmem;
+};
+constexpr uint32_t kTcPolls = 1u << 22;  // bound on the polls of one MMA completion
+
+__device__ __forceinline__ void put_bf16(unsigned char* slab, int r, int k, float v) {
+  *reinterpret_cast<__nv_bfloat16*>(slab + tc::slab_off(r, k)) = __float2bfloat16_rn(v);
+}
+
+__device__ void mlp_tc_stage(MlpTcSmem& s, const float* __restrict__ P, const float* __restrict__ nrm) {
+  for (int i = threadIdx.x; i < 64 * 16; i += blockDim.x) {
+    const int n = i >> 4, k = i & 15;
+    put_bf16(s.w1, n, k, k < kMlpIn ? P[kOffW1 + n * kMlpIn + k] : 0.f);
+  }
+  for (int i = threadIdx.x; i < 64 * 64; i += blockDim.x) {
+    const int n = i >> 6, k = i & 63;
+    put_bf16(s.w2 + (k >> 4) * 2048, n, k & 15, P[kOffW2 + n * kMlpH + k]);
+  }
+  for (int i = threadIdx.x; i < 16 * 64; i += blockDim.x) {
+    const int n = i >> 6, k = i & 63;
+    put_bf16(s.w3 + (k >> 4) * 512, n, k & 15, n < kMlpOut ? P[kOffW3 + n * kMlpH + k] : 0.f);
+  }
+  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+    s.b1[i] = P[kOffB1 + i];
+    s.b2[i] = P[kOffB2 + i];
+  }
+  if (threadIdx.x < 16) {
+    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[kOffB3 + threadIdx.x] : 0.f;
+    s.xmean[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[threadIdx.x] : 0.f;
+    s.xistd[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[kMlpIn + threadIdx.x] : 0.f;
+  }
+  if (threadIdx.x < 8) {
+    s.ymean[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + threadIdx.x] : 0.f;
+    s.ystd[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + kMlpOut + threadIdx.x] : 0.f;
+  }
+}
+
+// Accumulator columns 32*half.. of this thread's row (+ bias, activation) as
+// BF16 into activation slabs 2*half, 2*half+1.
+template <int ACT>
+__device__ __forceinline__ void mlp_tc_hidden(MlpTcSmem& s, uint32_t taddr, const float* bias, int row, int half) {
+  float v[32];
+  tc::ld32(taddr, v);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t w[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int col = 32 * half + 8 * c + 2 * e;
+      w[e] = act_pack<ACT>(v[8 * c + 2 * e] + bias[col], v[8 * c + 2 * e + 1] + bias[col + 1]);
+    }
+    const int chunk = 4 * half + c;  // 8-column chunk of the 64 outputs
+    *reinterpret_cast<uint4*>(s.h + (chunk >> 1) * 4096 + tc::slab_off(row, (chunk & 1) * 8)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
+}
+
+// Thread 0 waits for the MMAs it committed; the CTA agrees on the outcome.
+__device__ __forceinline__ bool mlp_tc_wait(uint32_t mbar, uint32_t& phase) {
+  const bool ok = tc::mbar_wait(mbar, phase, kTcPolls);
+  phase ^= 1;
+  return __syncthreads_and(ok) != 0;
+}
+
+// The three layers of one 128-point tile whose layer-1 input is in slab 0 of
+// s.h; returns false if an MMA did not complete within the poll limit.  On
+// return warps 0-3 hold their row's 8 output columns (bias added) in y.
+template <int ACT>
+__device__ __forceinline__ bool mlp_tc_tile(MlpTcSmem& s, uint32_t& phase, float* y) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int q = warp & 3, half = warp >> 2, row = 32 * q + lane;
+  const uint32_t mbar = tc::smem_u32(&s.mbar), tbase = s.tmem;
+  const uint32_t trow = tbase + ((uint32_t)(32 * q) << 16);
+  const uint32_t hs = tc::smem_u32(s.h);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::fence_after();
+    tc::mma(tbase, tc::desc(hs), tc::desc(tc::smem_u32(s.w1)), tc::idesc_bf16(128, 64), false);
+    tc::commit(mbar);
+  }
+  if (!mlp_tc_wait(mbar, phase)) return false;
+  tc::fence_after();
+  mlp_tc_hidden<ACT>(s, trow + 32 * half, s.b1, row, half);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::fence_after();
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      tc::mma(tbase, tc::desc(hs + k * 4096), tc::desc(tc::smem_u32(s.w2) + k * 2048), tc::idesc_bf16(128, 64),
+              k > 0);
+    tc::commit(mbar);
+  }
+  if (!mlp_tc_wait(mbar, phase)) return false;
+  tc::fence_after();
+  mlp_tc_hidden<ACT>(s, trow + 32 * half, s.b2, row, half);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tc::fence_after();
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      tc::mma(tbase, tc::desc(hs + k * 4096), tc::desc(tc::smem_u32(s.w3) + k * 512), tc::idesc_bf16(128, 16),
+              k > 0);
+    tc::commit(mbar);
+  }
+  if (!mlp_tc_wait(mbar, phase)) return false;
+  tc::fence_after();
+  if (half == 0) {
+    tc::ld8(trow, y);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) y[c] += s.b3[c];
+  }
+  return true;
+}
+
+template <int ACT>
+__global__ void __launch_bounds__(256) mlp_forward_tc_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
+                                                             const float* __restrict__ X, int B,
+                                                             float* __restrict__ Y, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  MlpTcSmem& s = *reinterpret_cast<MlpTcSmem*>(smem_raw);
+  mlp_tc_stage(s, P, nrm);
+  if (threadIdx.x == 0) tc::mbar_init(tc::smem_u32(&s.mbar), 1);
+  if (threadIdx.x < 32) tc::alloc(tc::smem_u32(&s.tmem), 64);
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  uint32_t phase = 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  bool ok = true;
+  for (int t0 = blockIdx.x * 128; t0 < B && ok; t0 += gridDim.x * 128) {
+    // features: thread -> row m, K half hk (features 8 hk .. 8 hk + 7)
+    {
+      const int m = threadIdx.x & 127, hk = threadIdx.x >> 7;
+      const int r = t0 + m;
+      uint32_t w[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        float f2[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int f = 8 * hk + 2 * e + u;
+          f2[u] = (f < kMlpIn && r < B) ? (X[(long long)r * kMlpIn + f] - s.xmean[f]) * s.xistd[f] : 0.f;
+        }
+        w[e] = pack_bf16(f2[0], f2[1]);
+      }
+      *reinterpret_cast<uint4*>(s.h + tc::slab_off(m, 8 * hk)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    float y[8];
+    ok = mlp_tc_tile<ACT>(s, phase, y);
+    if (ok && warp < 4) {
+      const int r = t0 + 32 * warp + lane;
+      if (r < B)
+#pragma unroll
+        for (int c = 0; c < kMlpOut; ++c) Y[(long long)r * kMlpOut + c] = y[c] * s.ystd[c] + s.ymean[c];
+    }
+    tc::fence_before();
+    __syncthreads();
+  }
+  if (!ok) {
+    // the MMAs may still be in flight: wait once more (bounded) before freeing
+    if (threadIdx.x == 0) {
+      tc::mbar_wait(tc::smem_u32(&s.mbar), phase ^ 1, kTcPolls);
+      if (err) atomicExch(err, 1);
+    }
+    __syncthreads();
+  }
+  tc::fence_after();
+  if (threadIdx.x < 32) tc::dealloc(s.tmem, 64);
+}
+
 }  // namespace
 
 extern "C" {
+
+int psb_mlp_forward_tc(psb_ctx* c, int act, const float* params, const float* norm, const float* X, int B, float* Y,
+                       int* err) {
+  if (!c) return PSB_ERR_ARG;
+  if (!params || !norm || !X || !Y || B < 0 || (act != kActGelu && act != kActRelu))
+    return fail(c, PSB_ERR_ARG, "psb_mlp_forward_tc: bad argument");
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  if (B == 0) return PSB_OK;
+  const size_t smem = sizeof(MlpTcSmem);
+  auto go = [&](auto k) {
+    set_smem(k, smem);
+    const long long grid = persistent_grid(k, smem, ((long long)B + 127) / 128);
+    ++c->launches;
+    k<<<(unsigned)grid, 256, smem, c->stream>>>(params, norm, X, B, Y, err);
+    return launch_ok(c, "mlp forward (tcgen05)");
+  };
+  return act == kActRelu ? go(mlp_forward_tc_kernel<kActRelu>) : go(mlp_forward_tc_kernel<kActGelu>);
+}
+
 
 int psb_mlp_sizes(int* nparams, int* nnorm) {
   if (!nparams || !nnorm) return PSB_ERR_ARG;

@@ -45,12 +45,13 @@ def _lib():
         vp, i, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
         lib.psb_mlp_sizes.argtypes = [ctypes.POINTER(i), ctypes.POINTER(i)]
         lib.psb_mlp_forward.argtypes = [vp, i, vp, vp, vp, i, vp]
+        lib.psb_mlp_forward_tc.argtypes = [vp, i, vp, vp, vp, i, vp, vp]
         lib.psb_mlp_grad.argtypes = [vp, i, vp, vp, vp, vp, vp, i, vp, vp]
         lib.psb_mlp_adam.argtypes = [vp, vp, vp, vp, vp, i, f, f, f, f, f]
         lib.psb_physical_fields.argtypes = [vp, vp, i, vp]
         lib.psb_products.argtypes = [vp, vp, vp]
         lib.psb_spectral_resample.argtypes = [vp, i, i, i, vp, i, i, i, i, i, d, i, vp]
-        for n in ("psb_mlp_sizes", "psb_mlp_forward", "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields",
+        for n in ("psb_mlp_sizes", "psb_mlp_forward", "psb_mlp_forward_tc", "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields",
                   "psb_products", "psb_spectral_resample"):
             getattr(lib, n).restype = i
         lib._mlp_bound = True
@@ -125,6 +126,17 @@ class MLPModel:
         ctx.bind_stream()
         ctx.check(_lib().psb_mlp_forward(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X.contiguous()),
                                          X.shape[0], _p(Y)), "psb_mlp_forward")
+        return Y
+
+    def forward_tc(self, ctx, X):
+        """forward() on the tcgen05 tensor-core kernel; raises if an MMA timed out."""
+        Y = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
+        err = torch.zeros(1, dtype=torch.int32, device=X.device)
+        ctx.bind_stream()
+        ctx.check(_lib().psb_mlp_forward_tc(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X.contiguous()),
+                                            X.shape[0], _p(Y), _p(err)), "psb_mlp_forward_tc")
+        if int(err.item()):
+            raise RuntimeError("psb_mlp_forward_tc: an MMA did not complete")
         return Y
 
     def grad_of(self, ctx, X, T, idx):

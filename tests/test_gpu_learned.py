@@ -66,6 +66,27 @@ def test_forward_and_gradients_match_cpu_oracle(act):
         o += k
 
 
+@pytest.mark.parametrize("act", ["relu", "gelu"])
+@pytest.mark.parametrize("n", [300, 5000])
+def test_tcgen05_forward_matches_oracle_and_mma_sync(act, n):
+    """The tcgen05 kernel (128-point tiles, accumulators in tensor memory)
+    computes the network of the BF16-emulating oracle; against the mma.sync
+    kernel it differs only by FP32 summation order."""
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    X, _, norm = _data(n, seed=7)
+    m, _ = _model(torch, 4, norm, act)
+    ctx = _capi.Context(16, 16, 16, precision=32)
+    Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
+    Ytc = m.forward_tc(ctx, Xd).cpu().numpy()
+    Ysync = m.forward(ctx, Xd).cpu().numpy()
+    Yo = mo.forward(m.params.cpu().numpy().astype(np.float64), m.norm.cpu().numpy().astype(np.float64),
+                    Xd.cpu().numpy().astype(np.float64), act=act)
+    assert np.isfinite(Ytc).all()
+    assert rel(Ytc, Yo) < 2e-3
+    assert rel(Ytc, Ysync) < 2e-3
+
+
 @pytest.mark.parametrize("act", ["gelu", "relu"])
 def test_training_reduces_loss(act):
     torch = _torch()
