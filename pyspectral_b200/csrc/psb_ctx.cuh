@@ -199,15 +199,45 @@ inline void set_smem(K kernel, size_t smem) {
 }
 
 // Grid of a persistent kernel: at most (resident CTAs per SM) x SMs of the
-// current device, and no more CTAs than there are tiles.
+// current device, and no more CTAs than there are tiles.  The kernel asks for
+// the largest shared-memory carveout first: under 48 KB per CTA the default
+// carveout would otherwise leave room for fewer CTAs than the registers and
+// shared memory allow (one per SM was seen).  Results are cached per
+// (kernel, device, shared memory) in a fixed table.
+struct OccCache {
+  const void* fn[256];
+  int dev[256];
+  size_t smem[256];
+  int per[256], nsm[256];
+  int n = 0;
+};
+inline OccCache& occ_cache() {
+  static OccCache c;
+  return c;
+}
 template <typename K>
 inline long long persistent_grid(K kernel, size_t smem, long long ntiles) {
-  int dev = 0, nsm = 0, per = 0;
+  int dev = 0;
   cudaGetDevice(&dev);
+  OccCache& oc = occ_cache();
+  const void* f = reinterpret_cast<const void*>(kernel);
+  for (int i = 0; i < oc.n; ++i)
+    if (oc.fn[i] == f && oc.dev[i] == dev && oc.smem[i] == smem)
+      return std::min<long long>(ntiles, (long long)oc.per[i] * oc.nsm[i]);
+  int nsm = 0, per = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, smem) != cudaSuccess || per < 1 || nsm < 1) {
     (void)cudaGetLastError();
     return ntiles;
+  }
+  if (oc.n < 256) {
+    oc.fn[oc.n] = f;
+    oc.dev[oc.n] = dev;
+    oc.smem[oc.n] = smem;
+    oc.per[oc.n] = per;
+    oc.nsm[oc.n] = nsm;
+    ++oc.n;
   }
   return std::min<long long>(ntiles, (long long)per * nsm);
 }
