@@ -54,7 +54,8 @@ struct Dims {
   int N1, N2, N3, N3h, M1, M2, M3, Kz;
   long long nA, nB, nC, nD, nQ;
 };
-Dims dims(const psb_ctx* c, int Fi, int Fo) {
+// Fi / Fb: fields after the x / y pass, Fo: z-pass outputs
+Dims dims(const psb_ctx* c, int Fi, int Fb, int Fo) {
   Dims d;
   d.N1 = c->N1;
   d.N2 = c->N2;
@@ -65,7 +66,7 @@ Dims dims(const psb_ctx* c, int Fi, int Fo) {
   d.M3 = 3 * d.N3 / 2;
   d.Kz = d.N3 / 2;
   d.nA = (long long)Fi * d.M1 * d.N2 * d.Kz;
-  d.nB = (long long)Fi * d.M1 * d.M2 * d.Kz;
+  d.nB = (long long)Fb * d.M1 * d.M2 * d.Kz;
   d.nC = (long long)Fo * d.M1 * d.M2 * d.Kz;
   d.nD = (long long)Fo * d.M1 * d.N2 * d.Kz;
   d.nQ = 3LL * d.N1 * d.N2 * d.N3h;
@@ -75,7 +76,8 @@ long long al(long long n) { return (n + 63) / 64 * 64; }
 
 template <typename T, class Pre, class Phys, class Epi>
 struct Batch {
-  static constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
+  static constexpr int Fi = Pre::F_DST, Fb = pre_b_fields<Pre>::value, Fo = Phys::F_OUT;
+  using YPre = typename pre_ypass<T, Pre>::type;
   psb_batch* b;
   psb_ctx* c;
   Dims d;
@@ -85,13 +87,15 @@ struct Batch {
   ZArgs<T>* az;
   XEpiArgs<T>* ae;
   Pre* pre;
+  YPre* ypre;  // y-inverse pass
   PreCopy<T>* cpy;
   Phys* phys;
   Epi* epi;  // [5][R]: stages 0..3, then a middle stage on scratch copies (tuning)
 
   static size_t arg_bytes(int R) {
     return al(sizeof(AxisArgs<T>) * R) * 3 + al(sizeof(ZArgs<T>) * R) + al(sizeof(XEpiArgs<T>) * R) +
-           al(sizeof(Pre) * R) + al(sizeof(PreCopy<T>) * R) + al(sizeof(Phys) * R) + al(sizeof(Epi) * R * 5);
+           al(sizeof(Pre) * R) + al(sizeof(YPre) * R) + al(sizeof(PreCopy<T>) * R) + al(sizeof(Phys) * R) +
+           al(sizeof(Epi) * R * 5);
   }
   static size_t run_bytes(const Dims& d) { return sizeof(Cx<T>) * (al(d.nA) + al(d.nB) + al(d.nC) + al(d.nD) + 2 * al(d.nQ)); }
 
@@ -116,6 +120,7 @@ struct Batch {
     az = reinterpret_cast<ZArgs<T>*>(take(sizeof(ZArgs<T>) * R));
     ae = reinterpret_cast<XEpiArgs<T>*>(take(sizeof(XEpiArgs<T>) * R));
     pre = reinterpret_cast<Pre*>(take(sizeof(Pre) * R));
+    ypre = reinterpret_cast<YPre*>(take(sizeof(YPre) * R));
     cpy = reinterpret_cast<PreCopy<T>*>(take(sizeof(PreCopy<T>) * R));
     phys = reinterpret_cast<Phys*>(take(sizeof(Phys) * R));
     epi = reinterpret_cast<Epi*>(take(sizeof(Epi) * R * 5));
@@ -166,7 +171,8 @@ struct Batch {
       y.in_rstride = d.Kz;
       y.out_ostride = (long long)d.M2 * d.Kz;
       y.out_rstride = d.Kz;
-      y.nouter = Fi * d.M1;
+      y.nouter = Fb * d.M1;
+      y.k_row = c->ky;
       y.ncols = d.Kz;
       y.col_tile = b->tile[1];
       y.in_rows = d.N2;
@@ -222,6 +228,7 @@ struct Batch {
       e.tw = twiddles<T>(c);
       ae[r] = e;
       pre[r] = pre0;
+      ypre[r] = pre_ypass<T, Pre>::make(d.M1);
       cpy[r] = PreCopy<T>{};
       phys[r] = mkphys(c, b->params[r]);
       for (int i = 0; i < 5; ++i) {
@@ -310,7 +317,7 @@ struct Batch {
       case 3: {
         const bool inv = pass == 1;
         const int ct = b->tile[pass];
-        const int F = inv ? Fi : Fo;
+        const int F = inv ? Fb : Fo;
         dim3 g((d.Kz + ct - 1) / ct, F * d.M1, R);
         const size_t sm = smem_axis(d.M2, 1, ct);
         const double by = (double)R * esz * F * d.M1 * d.Kz * (double)(d.N2 + d.M2);
@@ -318,12 +325,12 @@ struct Batch {
           auto go = [&](auto k) {
             set_smem(k, sm);
             LaunchScope s(c, "batch y-inverse", by);
-            k<<<g, 256, sm, c->stream>>>(ay, cpy);
+            k<<<g, 256, sm, c->stream>>>(ay, ypre);
             return launch_ok(c, "batch y-inverse");
           };
           return by_plan(
-              1, [&](auto id) { return go(axis_pass_batch<T, true, PreCopy<T>, false, decltype(id)::value>); },
-              [&] { return go(axis_pass_batch<T, true, PreCopy<T>, W>); });
+              1, [&](auto id) { return go(axis_pass_batch<T, true, YPre, false, decltype(id)::value>); },
+              [&] { return go(axis_pass_batch<T, true, YPre, W>); });
         }
         auto go = [&](auto k) {
           set_smem(k, sm);
@@ -342,7 +349,7 @@ struct Batch {
         const size_t sm = smem_z(P);
         auto go = [&](auto k) {
           set_smem(k, sm);
-          LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fi + Fo));
+          LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fb + Fo));
           k<<<g, 256, sm, c->stream>>>(az, phys);
           return launch_ok(c, "batch z-fused");
         };
@@ -489,14 +496,15 @@ EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
 }
 
 // Default launch shapes: the single-run rules of the library.
-void default_shapes(psb_batch* b, int Fi, int Fo, size_t esz, int ppc, size_t zextra) {
+// Fz: z-pass inputs (with the fields it derives itself)
+void default_shapes(psb_batch* b, int Fi, int Fb, int Fz, int Fo, size_t esz, int ppc, size_t zextra) {
   psb_ctx* c = b->c;
-  const Dims d = dims(c, Fi, Fo);
+  const Dims d = dims(c, Fi, Fb, Fo);
   b->tile[0] = pick_ct(d.Kz, Fi, d.M1, esz, d.N2);
-  b->tile[1] = pick_ct(d.Kz, 1, d.M2, esz, Fi * d.M1);
+  b->tile[1] = pick_ct(d.Kz, 1, d.M2, esz, Fb * d.M1);
   b->tile[3] = pick_ct(d.Kz, 1, d.M2, esz, Fo * d.M1);
   b->tile[4] = pick_ct(d.Kz, Fo, d.M1, esz, d.N2);
-  const int FMAX = std::max(Fi, Fo);
+  const int FMAX = std::max(Fz, Fo);
   int P = ppc;
   auto sm = [&](int P) { return (size_t)(d.M3 + 2 * (size_t)((FMAX * P + 1) / 2) * d.M3) * esz + zextra; };
   while (P > 1 && sm(P) > kSmemBudget) P /= 2;
@@ -519,7 +527,7 @@ int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_
   BT x;
   x.b = b;
   x.c = c;
-  x.d = dims(c, BT::Fi, BT::Fo);
+  x.d = dims(c, BT::Fi, BT::Fb, BT::Fo);
   x.R = b->nruns;
   const size_t need = BT::run_bytes(x.d) * (size_t)b->nruns;
   if (b->arena_bytes < need) {
@@ -530,7 +538,7 @@ int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_
     b->arena_bytes = need;
   }
   if (b->plan[0].L == 0)
-    default_shapes(b, BT::Fi, BT::Fo, sizeof(Cx<T>), phys_default_ppc<Phys>::value,
+    default_shapes(b, BT::Fi, BT::Fb, Phys::F_IN, BT::Fo, sizeof(Cx<T>), phys_default_ppc<Phys>::value,
                    (size_t)phys_is_block<Phys>::extra);
   if (b->dirty) {
     PSB_TRY(x.build(pre0, mkphys, mkepi));

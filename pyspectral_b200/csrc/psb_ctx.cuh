@@ -431,7 +431,7 @@ inline std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
 // leaves to the z-pass (pre_z_derived) formed from their stored field.
 template <typename T, class Pre, int NIN>
 void set_z_inputs(psb::ZArgs<T>& z, const Cx<T>* B, long long fsP, int Kz, const double* k3) {
-  static_assert(NIN == Pre::F_DST + psb::pre_z_derived<Pre>::value, "z-pass inputs mismatch");
+  static_assert(NIN == psb::pre_b_fields<Pre>::value + psb::pre_z_derived<Pre>::value, "z-pass inputs mismatch");
   for (int f = 0; f < NIN; ++f) {
     int src = f;
     bool der = false;

@@ -609,19 +609,41 @@ struct PreGrad {
   }
 };
 
-// (u,v,w) -> (u,v,w, du_i/dx, du_i/dy for i = 1..3) on the x-inverse pass; the
-// z-pass forms du_i/dz = i k3 u_i itself, so the x and y passes carry 9 fields
-// instead of 12.  z-pass input order is PreGrad's: u,v,w then g[3*i + j].
+// y-inverse pass of the velocity-gradient pipeline: output field g of
+// (u, v, w, ux, uy, vx, vy, wx, wy) reads x-pass field src(g) of
+// (u, v, w, ux, vx, wx) and, for the y derivatives, multiplies it by i k_y
+// (k_y of the spectral row being transformed; derivatives commute with the
+// x transform, so the x pass need not carry them).
+template <typename T>
+struct PreYGrad {
+  static constexpr int F_SRC = 1, F_DST = 1;
+  int rows;  // outer indices per field (the padded x extent)
+  __host__ __device__ static int src(int g) { return g < 3 ? g : (((g - 3) & 1) ? (g - 3) >> 1 : 3 + ((g - 3) >> 1)); }
+  __host__ __device__ static bool der(int g) { return g >= 3 && ((g - 3) & 1); }
+  __device__ int in_outer(int o) const {
+    const int g = o / rows;
+    return src(g) * rows + (o - g * rows);
+  }
+  __device__ void operator()(int i, int o, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    d[0] = der(o / rows) ? pik((T)a.k_row[i], s[0]) : s[0];
+  }
+};
+
+// (u,v,w) -> (u,v,w, du_i/dx) on the x-inverse pass; the y-inverse pass
+// (PreYGrad) adds du_i/dy and the z-pass forms du_i/dz = i k3 u_i itself, so
+// the x pass carries 6 fields and the y pass 9 instead of 12.  z-pass input
+// order is PreGrad's: u,v,w then g[3*i + j]; after the y pass the stored
+// fields are (u, v, w, ux, uy, vx, vy, wx, wy).
 template <typename T>
 struct PreGradXY {
-  static constexpr int F_SRC = 3, F_DST = 9, Z_DERIVED = 3;
-  __device__ void operator()(int i, int o, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
-    const T k1 = (T)a.k_row[i], k2 = (T)a.k_outer[o];
+  static constexpr int F_SRC = 3, F_DST = 6, F_B = 9, Z_DERIVED = 3;
+  using YPass = PreYGrad<T>;
+  __device__ void operator()(int i, int, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    const T k1 = (T)a.k_row[i];
 #pragma unroll
     for (int f = 0; f < 3; ++f) {
       d[f] = s[f];
-      d[3 + 2 * f] = pik(k1, s[f]);
-      d[4 + 2 * f] = pik(k2, s[f]);
+      d[3 + f] = pik(k1, s[f]);
     }
   }
   // z-pass input f (0..11) -> stored field and whether it is differentiated along z

@@ -40,12 +40,13 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const ps
     for (int k = 0; k < 5; ++k) sh[k] = &ts->pass[k];
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
-  constexpr int Fi = Pre::F_DST, Fo = Phys::F_OUT;
-  static_assert(Phys::F_IN == Pre::F_DST + pre_z_derived<Pre>::value, "pre/phys mismatch");
+  // Fi: fields after the x pass; Fb: after the y pass (the y pass's Pre may derive some)
+  constexpr int Fi = Pre::F_DST, Fb = pre_b_fields<Pre>::value, Fo = Phys::F_OUT;
+  static_assert(Phys::F_IN == Fb + pre_z_derived<Pre>::value, "pre/phys mismatch");
   static_assert(Epi::F_IN == Phys::F_OUT, "phys/epi mismatch");
   int st = PSB_OK;
   Cx<T>* A = scratch<T>(c, "ns.A", (size_t)Fi * M1 * N2 * Kz, &st);
-  Cx<T>* B = scratch<T>(c, "ns.B", (size_t)Fi * M1 * M2 * Kz, &st);
+  Cx<T>* B = scratch<T>(c, "ns.B", (size_t)Fb * M1 * M2 * Kz, &st);
   Cx<T>* C = scratch<T>(c, "ns.C", (size_t)Fo * M1 * M2 * Kz, &st);
   Cx<T>* D = scratch<T>(c, "ns.D", (size_t)Fo * M1 * N2 * Kz, &st);
   if (st != PSB_OK) return st;
@@ -79,13 +80,15 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const ps
   b.in_rstride = Kz;
   b.out_ostride = (long long)M2 * Kz;
   b.out_rstride = Kz;
-  b.nouter = Fi * M1;
+  b.nouter = Fb * M1;
   b.ncols = Kz;
   b.in_rows = N2;
   b.out_rows = M2;
   b.in_map = map_pad32(N2);
   b.out_map = map_id(M2);
-  PSB_TRY((launch_axis<T, true, PreCopy<T>, true>(c, b, PreCopy<T>{}, "y-inverse", sh[1])));
+  b.k_row = c->ky;
+  using YPre = typename pre_ypass<T, Pre>::type;
+  PSB_TRY((launch_axis<T, true, YPre, true>(c, b, pre_ypass<T, Pre>::make(M1), "y-inverse", sh[1])));
   // fused z
   ZArgs<T> z{};
   const long long fsP = (long long)M1 * M2 * Kz;
@@ -883,16 +886,21 @@ template <typename T>
 int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
-  int Fi, Fo, maxppc, defppc;
+  // Fi / Fb: fields after the x / y pass; Fz: z-pass inputs (its smem bound)
+  int Fi, Fb, Fz, Fo, maxppc, defppc;
   size_t zextra = 0;
   if (closure == PSB_DNS) {
-    Fi = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
+    Fi = Fb = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
+    Fz = PhysProducts<T>::F_IN;
     defppc = phys_default_ppc<PhysProducts<T>>::value;
   } else if (closure == PSB_SMAG) {
-    Fi = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
+    Fi = Fb = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
+    Fz = PhysSmag<T>::F_IN;
     defppc = phys_default_ppc<PhysSmag<T>>::value;
   } else {
-    Fi = PreGradXY<T>::F_DST, Fo = 6, maxppc = phys_max_ppc<PhysLearned<T>>::value;
+    Fi = PreGradXY<T>::F_DST, Fb = pre_b_fields<PreGradXY<T>>::value, Fo = 6;
+    Fz = PhysLearned<T>::F_IN;
+    maxppc = phys_max_ppc<PhysLearned<T>>::value;
     defppc = phys_default_ppc<PhysLearned<T>>::value;
     zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
   }
@@ -907,7 +915,7 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   PSB_TRY(cuda_ok(c, cudaMemcpyAsync(q0, state, n * esz, cudaMemcpyDeviceToDevice, c->stream), "tune copy"));
   if (cp) PSB_TRY(cuda_ok(c, cudaMemsetAsync(cp, 0, n * esz, c->stream), "tune memset"));
   const StepIO<T> io = make_io<T>(c, q, q0, cp, nullptr, nullptr, nullptr, kStageMid, p->dt / 3.0);
-  const int FMAX = std::max(Fi, Fo);
+  const int FMAX = std::max(Fz, Fo);
   auto zsmem = [&](int P) { return zpass_smem_bytes<T>(FMAX, P, M3, zextra); };
   int P = defppc;
   while (P > 1 && zsmem(P) > kSmemBudget) P /= 2;
@@ -916,7 +924,7 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const int Ls[5] = {M1, M2, M3, M2, M1};
   const int Fs[5] = {Fi, 1, 0, 1, Fo};
   t.pass[0].tile = pick_ct(Kz, Fi, M1, esz, N2);
-  t.pass[1].tile = pick_ct(Kz, 1, M2, esz, Fi * M1);
+  t.pass[1].tile = pick_ct(Kz, 1, M2, esz, Fb * M1);
   t.pass[2].tile = P;
   t.pass[3].tile = pick_ct(Kz, 1, M2, esz, Fo * M1);
   t.pass[4].tile = pick_ct(Kz, Fo, M1, esz, N2);
