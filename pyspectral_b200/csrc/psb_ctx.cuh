@@ -423,6 +423,12 @@ inline std::vector<FFTPlan> radix_orders(const FFTPlan& p) {
   };
   add_perms(std::vector<int>(p.radix, p.radix + p.npass));
   add_perms(fewest_passes(p.L));
+  // every other two-pass schedule with radices 6..16 (e.g. 12 x 8 beside 16 x 6)
+  for (int r : {16, 12, 8, 6})
+    if (p.L % r == 0 && p.L / r != r) {
+      const int q = p.L / r;
+      if (q == 16 || q == 12 || q == 8 || q == 6) add_perms({r, q});
+    }
   return out;
 }
 

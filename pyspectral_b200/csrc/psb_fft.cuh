@@ -405,7 +405,7 @@ __device__ __forceinline__ Cx<T>* fft_cs(Cx<T>* a, Cx<T>* b, const Cx<T>* __rest
 }
 
 // Schedules compiled in with their length (id, L, radices): the default
-// schedule of each common 3/2-padded length and its fewest-pass orders.
+// schedule of each common 3/2-padded length and two-pass orders of it.
 #define PSB_FIXED_PLANS(X) \
   X(1, 96, 8, 4, 3)        \
   X(2, 96, 16, 6)          \
@@ -415,8 +415,12 @@ __device__ __forceinline__ Cx<T>* fft_cs(Cx<T>* a, Cx<T>* b, const Cx<T>* __rest
   X(6, 48, 3, 16)          \
   X(7, 192, 8, 8, 3)       \
   X(8, 192, 16, 12)        \
-  X(9, 192, 12, 16)
-constexpr int kFixedPlans = 9;
+  X(9, 192, 12, 16)        \
+  X(10, 96, 12, 8)         \
+  X(11, 96, 8, 12)         \
+  X(12, 48, 8, 6)          \
+  X(13, 48, 6, 8)
+constexpr int kFixedPlans = 13;
 
 template <int ID>
 struct FixedPlan;
