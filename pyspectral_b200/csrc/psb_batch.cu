@@ -77,7 +77,8 @@ long long al(long long n) { return (n + 63) / 64 * 64; }
 template <typename T, class Pre, class Phys, class Epi>
 struct Batch {
   static constexpr int Fi = Pre::F_DST, Fb = pre_b_fields<Pre>::value, Fo = Phys::F_OUT;
-  using YPre = typename pre_ypass<T, Pre>::type;
+  using YP = pre_ypass<T, Pre>;
+  using YPre = typename YP::type;
   psb_batch* b;
   psb_ctx* c;
   Dims d;
@@ -171,7 +172,9 @@ struct Batch {
       y.in_rstride = d.Kz;
       y.out_ostride = (long long)d.M2 * d.Kz;
       y.out_rstride = d.Kz;
-      y.nouter = Fb * d.M1;
+      y.nouter = YP::groups * d.M1;
+      y.in_fstride = (long long)YP::in_fields * d.M1 * d.N2 * d.Kz;
+      y.out_fstride = (long long)YP::out_fields * d.M1 * d.M2 * d.Kz;
       y.k_row = c->ky;
       y.ncols = d.Kz;
       y.col_tile = b->tile[1];
@@ -228,7 +231,7 @@ struct Batch {
       e.tw = twiddles<T>(c);
       ae[r] = e;
       pre[r] = pre0;
-      ypre[r] = pre_ypass<T, Pre>::make(d.M1);
+      ypre[r] = YPre{};
       cpy[r] = PreCopy<T>{};
       phys[r] = mkphys(c, b->params[r]);
       for (int i = 0; i < 5; ++i) {
@@ -317,9 +320,10 @@ struct Batch {
       case 3: {
         const bool inv = pass == 1;
         const int ct = b->tile[pass];
-        const int F = inv ? Fb : Fo;
-        dim3 g((d.Kz + ct - 1) / ct, F * d.M1, R);
-        const size_t sm = smem_axis(d.M2, 1, ct);
+        // y-inverse: YP::groups outer groups of YPre::F_DST lines per column
+        const int G = inv ? YP::groups : Fo, F = inv ? Fb : Fo;
+        dim3 g((d.Kz + ct - 1) / ct, G * d.M1, R);
+        const size_t sm = smem_axis(d.M2, inv ? YPre::F_DST : 1, ct);
         const double by = (double)R * esz * F * d.M1 * d.Kz * (double)(d.N2 + d.M2);
         if (inv) {
           auto go = [&](auto k) {
@@ -415,7 +419,7 @@ struct Batch {
                Epi (*mkepi)(psb_ctx*, StepIO<T>, const psb_params&)) {
     const size_t esz = sizeof(Cx<T>);
     const int Ls[5] = {d.M1, d.M2, d.M3, d.M2, d.M1};
-    const int Fs[5] = {Fi, 1, 0, 1, Fo};
+    const int Fs[5] = {Fi, YPre::F_DST, 0, 1, Fo};
     // RHS-mode passes read the runs' states and write only scratch; run one
     // full RHS first so that every intermediate buffer holds real data.
     for (int pass = 0; pass < 5; ++pass) PSB_TRY(launch(pass, 4));
@@ -496,12 +500,14 @@ EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
 }
 
 // Default launch shapes: the single-run rules of the library.
-// Fz: z-pass inputs (with the fields it derives itself)
-void default_shapes(psb_batch* b, int Fi, int Fb, int Fz, int Fo, size_t esz, int ppc, size_t zextra) {
+// Fz: z-pass inputs (with the fields it derives itself); Fy / Gy: lines per
+// column and outer groups of the y-inverse pass
+void default_shapes(psb_batch* b, int Fi, int Fb, int Fz, int Fo, int Fy, int Gy, size_t esz, int ppc,
+                    size_t zextra) {
   psb_ctx* c = b->c;
   const Dims d = dims(c, Fi, Fb, Fo);
   b->tile[0] = pick_ct(d.Kz, Fi, d.M1, esz, d.N2);
-  b->tile[1] = pick_ct(d.Kz, 1, d.M2, esz, Fb * d.M1);
+  b->tile[1] = pick_ct(d.Kz, Fy, d.M2, esz, Gy * d.M1);
   b->tile[3] = pick_ct(d.Kz, 1, d.M2, esz, Fo * d.M1);
   b->tile[4] = pick_ct(d.Kz, Fo, d.M1, esz, d.N2);
   const int FMAX = std::max(Fz, Fo);
@@ -538,8 +544,8 @@ int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_
     b->arena_bytes = need;
   }
   if (b->plan[0].L == 0)
-    default_shapes(b, BT::Fi, BT::Fb, Phys::F_IN, BT::Fo, sizeof(Cx<T>), phys_default_ppc<Phys>::value,
-                   (size_t)phys_is_block<Phys>::extra);
+    default_shapes(b, BT::Fi, BT::Fb, Phys::F_IN, BT::Fo, BT::YPre::F_DST, BT::YP::groups, sizeof(Cx<T>),
+                   phys_default_ppc<Phys>::value, (size_t)phys_is_block<Phys>::extra);
   if (b->dirty) {
     PSB_TRY(x.build(pre0, mkphys, mkepi));
     b->dirty = false;

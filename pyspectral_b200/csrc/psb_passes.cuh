@@ -25,7 +25,6 @@
 // index N/2 of x and y and the k3=N/2 plane; pad_2x/unpad_2x keep the -N/2
 // mode).
 #pragma once
-#include <utility>
 #include "psb_fft.cuh"
 
 namespace psb {
@@ -142,17 +141,6 @@ __device__ __forceinline__ Cx<T>* axfft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, co
     return FixedPlan<FP>::template run_adjacent<T, INV>(a, b, tw, lines);
 }
 
-// Pre functors may read another outer index than the one they write:
-// Pre::in_outer(o) (default o).
-template <class P, class = void>
-struct pre_in_outer {
-  __device__ static int of(const P&, int o) { return o; }
-};
-template <class P>
-struct pre_in_outer<P, decltype((void)std::declval<const P&>().in_outer(0), void())> {
-  __device__ static int of(const P& p, int o) { return p.in_outer(o); }
-};
-
 template <typename T, bool INV, class Pre, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -183,7 +171,7 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
     for (int j = t0; j < L; ++j)
       for (int l = threadIdx.x; l < lines; l += nt) bufA[(size_t)j * lines + l] = zero;
   }
-  const Cx<T>* inb = a.in + (long long)pre_in_outer<Pre>::of(pre, o) * a.in_ostride;
+  const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
   // U rows per round: every load of a round is issued before the first store
   constexpr int U = Pre::F_SRC >= 3 ? 2 : (Pre::F_SRC == 2 ? 4 : 8);
   for (int i0 = r0; i0 < a.in_rows; i0 += U * dr) {
@@ -276,20 +264,18 @@ template <class P>
 struct pre_b_fields<P, decltype((void)P::F_B, void())> {
   static constexpr int value = P::F_B;
 };
+// groups: outer groups of the y pass (x rows each); in_fields / out_fields:
+// the pass's field strides in fields (0: one field per CTA, folded into the
+// outer index)
 template <typename T, class P, class = void>
 struct pre_ypass {
   using type = PreCopy<T>;
-  __host__ static type make(int) { return type{}; }
+  static constexpr int groups = pre_b_fields<P>::value, in_fields = 0, out_fields = 0;
 };
 template <typename T, class P>
 struct pre_ypass<T, P, decltype((void)sizeof(typename P::YPass), void())> {
   using type = typename P::YPass;
-  // rows: outer indices per field of the y pass (the padded x extent)
-  __host__ static type make(int rows) {
-    type y{};
-    y.rows = rows;
-    return y;
-  }
+  static constexpr int groups = type::GROUPS, in_fields = type::IN_FIELDS, out_fields = type::OUT_FIELDS;
 };
 
 // Shared memory of one z-pass CTA: twiddles, two buffers of

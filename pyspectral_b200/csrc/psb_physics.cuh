@@ -609,23 +609,19 @@ struct PreGrad {
   }
 };
 
-// y-inverse pass of the velocity-gradient pipeline: output field g of
-// (u, v, w, ux, uy, vx, vy, wx, wy) reads x-pass field src(g) of
-// (u, v, w, ux, vx, wx) and, for the y derivatives, multiplies it by i k_y
-// (k_y of the spectral row being transformed; derivatives commute with the
-// x transform, so the x pass need not carry them).
+// y-inverse pass of the velocity-gradient pipeline: the CTA of component q
+// (outer index q*M1 + x) reads u_q and its x derivative (fields q and 3+q of
+// the x pass) and writes u_q, du_q/dx and du_q/dy = i k_y u_q (fields q, 3+q
+// and 6+q): the y derivative is formed on load (derivatives commute with the
+// x transform, so the x pass need not carry it) and every source field is
+// read once.  GROUPS outer groups; input and output field strides of 3 fields.
 template <typename T>
 struct PreYGrad {
-  static constexpr int F_SRC = 1, F_DST = 1;
-  int rows;  // outer indices per field (the padded x extent)
-  __host__ __device__ static int src(int g) { return g < 3 ? g : (((g - 3) & 1) ? (g - 3) >> 1 : 3 + ((g - 3) >> 1)); }
-  __host__ __device__ static bool der(int g) { return g >= 3 && ((g - 3) & 1); }
-  __device__ int in_outer(int o) const {
-    const int g = o / rows;
-    return src(g) * rows + (o - g * rows);
-  }
-  __device__ void operator()(int i, int o, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
-    d[0] = der(o / rows) ? pik((T)a.k_row[i], s[0]) : s[0];
+  static constexpr int F_SRC = 2, F_DST = 3, GROUPS = 3, IN_FIELDS = 3, OUT_FIELDS = 3;
+  __device__ void operator()(int i, int, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    d[0] = s[0];
+    d[1] = s[1];
+    d[2] = pik((T)a.k_row[i], s[0]);
   }
 };
 
@@ -633,7 +629,7 @@ struct PreYGrad {
 // (PreYGrad) adds du_i/dy and the z-pass forms du_i/dz = i k3 u_i itself, so
 // the x pass carries 6 fields and the y pass 9 instead of 12.  z-pass input
 // order is PreGrad's: u,v,w then g[3*i + j]; after the y pass the stored
-// fields are (u, v, w, ux, uy, vx, vy, wx, wy).
+// fields are (u, v, w, ux, vx, wx, uy, vy, wy).
 template <typename T>
 struct PreGradXY {
   static constexpr int F_SRC = 3, F_DST = 6, F_B = 9, Z_DERIVED = 3;
@@ -655,7 +651,7 @@ struct PreGradXY {
     }
     const int i = (f - 3) / 3, j = (f - 3) % 3;
     der = j == 2;
-    src = der ? i : 3 + 2 * i + j;
+    src = der ? i : 3 + 3 * j + i;
   }
 };
 

@@ -80,15 +80,17 @@ int run_ns32(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi, const ps
   b.in_rstride = Kz;
   b.out_ostride = (long long)M2 * Kz;
   b.out_rstride = Kz;
-  b.nouter = Fb * M1;
+  using YP = pre_ypass<T, Pre>;
+  b.nouter = YP::groups * M1;
+  b.in_fstride = (long long)YP::in_fields * M1 * N2 * Kz;
+  b.out_fstride = (long long)YP::out_fields * M1 * M2 * Kz;
   b.ncols = Kz;
   b.in_rows = N2;
   b.out_rows = M2;
   b.in_map = map_pad32(N2);
   b.out_map = map_id(M2);
   b.k_row = c->ky;
-  using YPre = typename pre_ypass<T, Pre>::type;
-  PSB_TRY((launch_axis<T, true, YPre, true>(c, b, pre_ypass<T, Pre>::make(M1), "y-inverse", sh[1])));
+  PSB_TRY((launch_axis<T, true, typename YP::type, true>(c, b, typename YP::type{}, "y-inverse", sh[1])));
   // fused z
   ZArgs<T> z{};
   const long long fsP = (long long)M1 * M2 * Kz;
@@ -886,19 +888,22 @@ template <typename T>
 int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
-  // Fi / Fb: fields after the x / y pass; Fz: z-pass inputs (its smem bound)
-  int Fi, Fb, Fz, Fo, maxppc, defppc;
+  // Fi / Fb: fields after the x / y pass; Fz: z-pass inputs (its smem bound);
+  // Fy / Gy: lines per column and outer groups of the y-inverse pass
+  int Fi, Fb, Fz, Fo, maxppc, defppc, Fy = 1, Gy;
   size_t zextra = 0;
   if (closure == PSB_DNS) {
-    Fi = Fb = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
+    Fi = Fb = Gy = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
     Fz = PhysProducts<T>::F_IN;
     defppc = phys_default_ppc<PhysProducts<T>>::value;
   } else if (closure == PSB_SMAG) {
-    Fi = Fb = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
+    Fi = Fb = Gy = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
     Fz = PhysSmag<T>::F_IN;
     defppc = phys_default_ppc<PhysSmag<T>>::value;
   } else {
     Fi = PreGradXY<T>::F_DST, Fb = pre_b_fields<PreGradXY<T>>::value, Fo = 6;
+    Fy = PreYGrad<T>::F_DST;
+    Gy = pre_ypass<T, PreGradXY<T>>::groups;
     Fz = PhysLearned<T>::F_IN;
     maxppc = phys_max_ppc<PhysLearned<T>>::value;
     defppc = phys_default_ppc<PhysLearned<T>>::value;
@@ -922,9 +927,9 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   while (P > 1 && ((long long)M1 * M2 + P - 1) / P < 2 * 148) P /= 2;
   psb_tuned t;
   const int Ls[5] = {M1, M2, M3, M2, M1};
-  const int Fs[5] = {Fi, 1, 0, 1, Fo};
+  const int Fs[5] = {Fi, Fy, 0, 1, Fo};
   t.pass[0].tile = pick_ct(Kz, Fi, M1, esz, N2);
-  t.pass[1].tile = pick_ct(Kz, 1, M2, esz, Fb * M1);
+  t.pass[1].tile = pick_ct(Kz, Fy, M2, esz, Gy * M1);
   t.pass[2].tile = P;
   t.pass[3].tile = pick_ct(Kz, 1, M2, esz, Fo * M1);
   t.pass[4].tile = pick_ct(Kz, Fo, M1, esz, N2);
