@@ -74,6 +74,7 @@ typedef struct {
   const void* mlp_norm;   /* PSB_LEARNED: FP32 normalisation block on the device */
   double les_delta;       /* PSB_LEARNED: filter width fed to the MLP; <=0 -> (dx dy dz)^(1/3) */
   int mlp_act;            /* PSB_LEARNED: hidden activation of the model, PSB_ACT_GELU or PSB_ACT_RELU */
+  int mlp_hidden;         /* PSB_LEARNED: hidden width of the model, 32 or 64 (0 = 64) */
 } psb_params;
 
 /* Hidden activation of the learned closure's MLP (a property of the trained model). */
@@ -161,27 +162,30 @@ int psb_fft_c2r(psb_ctx* ctx, const void* spec, void* phys, int nfields);
 int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* count);
 
 /* ---- learned subgrid closure (no counterpart in the reference) ----------
- * MLP 10 -> 64 -> 64 -> 6 (hidden activation act: PSB_ACT_GELU or
- * PSB_ACT_RELU), BF16 tensor-core math with FP32
- * accumulation.  Features: the 9 velocity gradients du_i/dx_j (order 3i+j)
- * and the filter width; targets: tau_11,22,33,12,13,23.  Parameters are an
- * FP32 master block of *nparams floats, normalisation a block of *nnorm
- * floats (xmean[10] xistd[10] ymean[6] ystd[6]); all device pointers. */
-int psb_mlp_sizes(int* nparams, int* nnorm);
+ * MLP 10 -> H -> H -> 6 (hidden width H = hidden: 32 or 64, 0 meaning 64;
+ * hidden activation act: PSB_ACT_GELU or PSB_ACT_RELU), BF16 tensor-core
+ * math with FP32 accumulation.  Features: the 9 velocity gradients du_i/dx_j
+ * (order 3i+j) and the filter width; targets: tau_11,22,33,12,13,23.
+ * Parameters are an FP32 master block of *nparams floats (W1[H][10] b1[H]
+ * W2[H][H] b2[H] W3[6][H] b3[6]), normalisation a block of *nnorm floats
+ * (xmean[10] xistd[10] ymean[6] ystd[6]); all device pointers. */
+int psb_mlp_sizes(int hidden, int* nparams, int* nnorm);
 /* Y[B][6] = tau(X[B][10]) (raw units in and out). */
-int psb_mlp_forward(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, int B, float* Y);
-/* The same forward pass on the fifth-generation tensor cores (tcgen05.mma,
- * 128-point tiles, FP32 accumulators in tensor memory).  err: optional device
- * int set to 1 if an MMA did not complete within the kernel's wait bound. */
+int psb_mlp_forward(psb_ctx* ctx, int act, int hidden, const float* params, const float* norm, const float* X, int B,
+                    float* Y);
+/* The same forward pass of a width-64 network on the fifth-generation tensor
+ * cores (tcgen05.mma, 128-point tiles, FP32 accumulators in tensor memory).
+ * err: optional device int set to 1 if an MMA did not complete within the
+ * kernel's wait bound. */
 int psb_mlp_forward_tc(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, int B, float* Y,
                        int* err);
 /* grad += d(MSE of normalised outputs)/d(params) over the B points X[idx[b]],
  * T[idx[b]]; *loss (device double) += the MSE. */
-int psb_mlp_grad(psb_ctx* ctx, int act, const float* params, const float* norm, const float* X, const float* T,
-                 const int* idx, int B, float* grad, double* loss);
-/* One Adam(W) update of params from grad (step >= 1); clears grad. */
-int psb_mlp_adam(psb_ctx* ctx, float* params, float* m, float* v, float* grad, int step, float lr, float beta1,
-                 float beta2, float eps, float weight_decay);
+int psb_mlp_grad(psb_ctx* ctx, int act, int hidden, const float* params, const float* norm, const float* X,
+                 const float* T, const int* idx, int B, float* grad, double* loss);
+/* One Adam(W) update of the width-`hidden` parameter block from grad (step >= 1); clears grad. */
+int psb_mlp_adam(psb_ctx* ctx, int hidden, float* params, float* m, float* v, float* grad, int step, float lr,
+                 float beta1, float beta2, float eps, float weight_decay);
 /* Physical fields on the N grid (irfftn(uhat)*sqrt(N1N2N3)): what=0 -> u,v,w
  * (3 fields); what=1 -> u,v,w and the 9 gradients du_i/dx_j (12 fields). */
 int psb_physical_fields(psb_ctx* ctx, const void* fields3, int what, void* out);

@@ -7,8 +7,9 @@ same BF16 rounding of the tensor-core operands (features, weights, hidden
 activations and back-propagated errors) as the GPU kernels; biases, pre-
 activations and bias gradients stay in full precision.
 
-Network: 10 -> 64 -> 64 -> 6, hidden activation exact GELU ("gelu") or ReLU
-("relu", derivative 0 at 0), MSE on normalised outputs.
+Network: 10 -> H -> H -> 6 (H = 32 or 64, read from the length of the
+parameter block), hidden activation exact GELU ("gelu") or ReLU ("relu",
+derivative 0 at 0), MSE on normalised outputs.
 Parameter block (row-major [out][in]): W1[64][10] b1[64] W2[64][64] b2[64]
 W3[6][64] b3[6].  Normalisation block: xmean[10] xistd[10] ymean[6] ystd[6].
 """
@@ -19,14 +20,33 @@ import math
 import numpy as np
 
 NIN, NH, NOUT = 10, 64, 6
-SIZES = [("W1", (NH, NIN)), ("b1", (NH,)), ("W2", (NH, NH)), ("b2", (NH,)), ("W3", (NOUT, NH)), ("b3", (NOUT,))]
-NPARAMS = sum(int(np.prod(s)) for _, s in SIZES)
 NNORM = 32
+
+
+def sizes(h=NH):
+    """(name, shape) of the parameter blocks of a width-h network."""
+    return [("W1", (h, NIN)), ("b1", (h,)), ("W2", (h, h)), ("b2", (h,)), ("W3", (NOUT, h)), ("b3", (NOUT,))]
+
+
+def nparams(h=NH):
+    return sum(int(np.prod(s)) for _, s in sizes(h))
+
+
+SIZES = sizes()
+NPARAMS = nparams()
+
+
+def width_of(P):
+    """Hidden width of a parameter block (h^2 + 18 h + 6 floats)."""
+    for h in (32, 64):
+        if len(P) == nparams(h):
+            return h
+    raise ValueError(f"{len(P)} parameters: not a width-32 or width-64 network")
 
 
 def unpack(P):
     out, o = {}, 0
-    for name, shp in SIZES:
+    for name, shp in sizes(width_of(P)):
         n = int(np.prod(shp))
         out[name] = np.asarray(P[o:o + n], dtype=np.float64).reshape(shp)
         o += n
@@ -34,7 +54,8 @@ def unpack(P):
 
 
 def pack(d):
-    return np.concatenate([np.asarray(d[name], dtype=np.float64).ravel() for name, _ in SIZES])
+    h = d["b1"].shape[0]
+    return np.concatenate([np.asarray(d[name], dtype=np.float64).ravel() for name, _ in sizes(h)])
 
 
 def bf16(x):
@@ -65,11 +86,11 @@ def act_fn(act):
     raise ValueError(act)
 
 
-def init_params(seed=0):
+def init_params(seed=0, hidden=NH):
     """Uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights, zero biases."""
     rs = np.random.RandomState(seed)
     d = {}
-    for name, shp in SIZES:
+    for name, shp in sizes(hidden):
         if name.startswith("W"):
             b = 1.0 / math.sqrt(shp[1])
             d[name] = rs.uniform(-b, b, size=shp)

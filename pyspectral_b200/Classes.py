@@ -215,7 +215,8 @@ class variables:
                                  Om=(self.Om1, self.Om2, self.Om3),
                                  mlp_params=m.params.data_ptr() if m is not None else None,
                                  mlp_norm=m.norm.data_ptr() if m is not None else None,
-                                 les_delta=self.les_delta, mlp_act=m.act if m is not None else 0)
+                                 les_delta=self.les_delta, mlp_act=m.act if m is not None else 0,
+                                 mlp_hidden=m.hidden if m is not None else 0)
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,

@@ -45,7 +45,7 @@ class Params(ctypes.Structure):
                 ("tau_b", ctypes.c_double), ("kf", ctypes.c_int), ("rotate", ctypes.c_int),
                 ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
                 ("force", ctypes.c_void_p), ("mlp_params", ctypes.c_void_p), ("mlp_norm", ctypes.c_void_p),
-                ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int)]
+                ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int), ("mlp_hidden", ctypes.c_int)]
 
 
 _lib = None
@@ -100,10 +100,10 @@ def load(path: str = LIB_PATH):
 
 def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
                 Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0,
-                mlp_act=0) -> Params:
+                mlp_act=0, mlp_hidden=0) -> Params:
     return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
                   int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force, mlp_params, mlp_norm,
-                  float(les_delta), int(mlp_act))
+                  float(les_delta), int(mlp_act), int(mlp_hidden))
 
 
 class Context:

@@ -487,11 +487,12 @@ template <typename T>
 PhysSmag<T> mk_smag(psb_ctx* c, const psb_params&) {
   return PhysSmag<T>{(T)(0.16 * c->Delta * 0.16 * c->Delta)};
 }
-template <typename T, int ACT>
-PhysLearned<T, ACT> mk_learned(psb_ctx* c, const psb_params& p) {
+template <typename T, int ACT, int H>
+PhysLearned<T, ACT, H> mk_learned(psb_ctx* c, const psb_params& p) {
   const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
-  return PhysLearned<T, ACT>{reinterpret_cast<const float*>(p.mlp_params), reinterpret_cast<const float*>(p.mlp_norm),
-                             (T)s32, (float)(p.les_delta > 0 ? p.les_delta : c->Delta)};
+  return PhysLearned<T, ACT, H>{reinterpret_cast<const float*>(p.mlp_params),
+                                reinterpret_cast<const float*>(p.mlp_norm), (T)s32,
+                                (float)(p.les_delta > 0 ? p.les_delta : c->Delta)};
 }
 template <typename T, bool SMAG>
 EpiNS<T, SMAG> mk_epi(psb_ctx* c, StepIO<T> io, const psb_params& p) {
@@ -564,10 +565,12 @@ int dispatch(psb_batch* b, int nsteps, bool tune) {
     case PSB_SMAG:
       return run_batch<T>(b, nsteps, tune, PreStrain<T>{}, &mk_smag<T>, &mk_epi<T, true>);
     case PSB_LEARNED:
-      // every run of a learned batch has the activation of run 0 (psb_batch_set_run)
+      // every run of a learned batch has the activation and width of run 0 (psb_batch_set_run)
       if (b->params[0].mlp_act == PSB_ACT_GELU)
-        return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T, kActGelu>, &mk_epi<T, false>);
-      return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T, kActRelu>, &mk_epi<T, false>);
+        return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T, kActGelu, 64>, &mk_epi<T, false>);
+      if (b->params[0].mlp_hidden == 32)
+        return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T, kActRelu, 32>, &mk_epi<T, false>);
+      return run_batch<T>(b, nsteps, tune, PreGradXY<T>{}, &mk_learned<T, kActRelu, 64>, &mk_epi<T, false>);
     default:
       return fail(b->c, PSB_ERR_UNSUPPORTED, "psb_batch: closure not batched (DNS, SMAG, LEARNED are)");
   }
@@ -601,10 +604,15 @@ int psb_batch_set_run(psb_batch* b, int r, void* state, void* comp, const psb_pa
     return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: PSB_LEARNED needs mlp_params and mlp_norm");
   if (b->closure == PSB_LEARNED && p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
     return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
+  if (b->closure == PSB_LEARNED &&
+      !(p->mlp_hidden == 0 || p->mlp_hidden == 64 || (p->mlp_hidden == 32 && p->mlp_act == PSB_ACT_RELU)))
+    return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: mlp_hidden must be 64 (0), or 32 with PSB_ACT_RELU");
   if (b->closure == PSB_LEARNED)
     for (int q = 0; q < b->nruns; ++q)
-      if (q != r && b->state[q] && b->params[q].mlp_act != p->mlp_act)
-        return fail(b->c, PSB_ERR_ARG, "psb_batch_set_run: every run of a learned batch needs the same mlp_act");
+      if (q != r && b->state[q] &&
+          (b->params[q].mlp_act != p->mlp_act || (b->params[q].mlp_hidden == 32) != (p->mlp_hidden == 32)))
+        return fail(b->c, PSB_ERR_ARG,
+                    "psb_batch_set_run: every run of a learned batch needs the same mlp_act and mlp_hidden");
   b->state[r] = state;
   b->comp[r] = comp;
   b->params[r] = *p;

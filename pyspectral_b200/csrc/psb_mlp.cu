@@ -20,15 +20,16 @@ static_assert(kActGelu == PSB_ACT_GELU && kActRelu == PSB_ACT_RELU, "activation 
 
 constexpr int kRows = 128;  // points per CTA (8 warps x 16)
 
+template <int H>
 struct TrainSmem {
-  MlpSmem m;
+  MlpSmem<H> m;
   __nv_bfloat16 X[kRows * 16];
-  __nv_bfloat16 H1[kRows * kMlpH];
-  __nv_bfloat16 H2[kRows * kMlpH];
+  __nv_bfloat16 H1[kRows * H];
+  __nv_bfloat16 H2[kRows * H];
   __nv_bfloat16 dY[kRows * 16];
-  __nv_bfloat16 dZ2[kRows * kMlpH];
-  __nv_bfloat16 dZ1[kRows * kMlpH];
-  float db1[kMlpH], db2[kMlpH], db3[8];
+  __nv_bfloat16 dZ2[kRows * H];
+  __nv_bfloat16 dZ1[kRows * H];
+  float db1[H], db2[H], db3[8];
   float loss;
 };
 
@@ -49,16 +50,18 @@ __device__ __forceinline__ void bfrag_kn(uint32_t* b, const __nv_bfloat16* W, in
   b[1] = pack_raw(W[(k + 8) * ld + n0 + g], W[(k + 9) * ld + n0 + g]);
 }
 
-// grad[kMlpParams] += dL/dparams over B points; loss_acc += sum of squared errors / (6B)
-template <int ACT>
+// grad[NPARAMS] += dL/dparams over B points; loss_acc += sum of squared errors / (6B)
+template <int ACT, int H>
 __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
                                                         const float* __restrict__ X, const float* __restrict__ T,
                                                         const int* __restrict__ idx, int B, float* __restrict__ grad,
                                                         double* __restrict__ loss_acc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainSmem& s = *reinterpret_cast<TrainSmem*>(smem_raw);
-  mlp_stage(s.m, P, nrm);
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
+  using L = MlpLayout<H>;
+  constexpr int NJ = H / 8, NK = H / 16;
+  TrainSmem<H>& s = *reinterpret_cast<TrainSmem<H>*>(smem_raw);
+  mlp_stage<H>(s.m, P, nrm);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
     s.db1[i] = 0.f;
     s.db2[i] = 0.f;
   }
@@ -74,8 +77,8 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     const int id = r == g ? id_lo : id_hi;
     return id >= 0 ? X[(long long)id * kMlpIn + f] : s.m.xmean[f];
   });
-  float z1[8][4], z2[8][4], y[4];
-  mlp_forward_warp<ACT>(s.m, xa, y, z1, z2);
+  float z1[NJ][4], z2[NJ][4], y[4];
+  mlp_forward_warp<ACT, H>(s.m, xa, y, z1, z2);
   // dY = 2 (y - t) / (6B), rows without a point contribute nothing
   const float sc = 2.f / (6.f * (float)B);
   float dy[4];
@@ -103,15 +106,15 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
     *reinterpret_cast<__nv_bfloat162*>(&s.X[ra * 16 + 2 * t + 8]) = xv[2];
     *reinterpret_cast<__nv_bfloat162*>(&s.X[rb * 16 + 2 * t + 8]) = xv[3];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       const int col = 8 * j + 2 * t;
-      *reinterpret_cast<__nv_bfloat162*>(&s.H1[ra * kMlpH + col]) =
+      *reinterpret_cast<__nv_bfloat162*>(&s.H1[ra * H + col]) =
           __floats2bfloat162_rn(act_f<ACT>(z1[j][0]), act_f<ACT>(z1[j][1]));
-      *reinterpret_cast<__nv_bfloat162*>(&s.H1[rb * kMlpH + col]) =
+      *reinterpret_cast<__nv_bfloat162*>(&s.H1[rb * H + col]) =
           __floats2bfloat162_rn(act_f<ACT>(z1[j][2]), act_f<ACT>(z1[j][3]));
-      *reinterpret_cast<__nv_bfloat162*>(&s.H2[ra * kMlpH + col]) =
+      *reinterpret_cast<__nv_bfloat162*>(&s.H2[ra * H + col]) =
           __floats2bfloat162_rn(act_f<ACT>(z2[j][0]), act_f<ACT>(z2[j][1]));
-      *reinterpret_cast<__nv_bfloat162*>(&s.H2[rb * kMlpH + col]) =
+      *reinterpret_cast<__nv_bfloat162*>(&s.H2[rb * H + col]) =
           __floats2bfloat162_rn(act_f<ACT>(z2[j][2]), act_f<ACT>(z2[j][3]));
     }
     *reinterpret_cast<__nv_bfloat162*>(&s.dY[ra * 16 + 2 * t]) = __floats2bfloat162_rn(dy[0], dy[1]);
@@ -129,34 +132,34 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
   da[1] = pack_bf16(dy[2], dy[3]);
   da[2] = 0u;
   da[3] = 0u;
-  float dz2[8][4];
+  float dz2[NJ][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     dz2[j][0] = dz2[j][1] = dz2[j][2] = dz2[j][3] = 0.f;
     uint32_t b[2];
-    b[0] = pack_raw(s.m.w3[(2 * t) * kMlpH + 8 * j + g], s.m.w3[(2 * t + 1) * kMlpH + 8 * j + g]);
+    b[0] = pack_raw(s.m.w3[(2 * t) * H + 8 * j + g], s.m.w3[(2 * t + 1) * H + 8 * j + g]);
     b[1] = 0u;
     mma16816(dz2[j], da, b);
 #pragma unroll
     for (int e = 0; e < 4; ++e) dz2[j][e] *= act_d<ACT>(z2[j][e]);
   }
-  uint32_t a2[4][4];
+  uint32_t a2[NK][4];
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     a2[kk][0] = pack_bf16(dz2[2 * kk][0], dz2[2 * kk][1]);
     a2[kk][1] = pack_bf16(dz2[2 * kk][2], dz2[2 * kk][3]);
     a2[kk][2] = pack_bf16(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
     a2[kk][3] = pack_bf16(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
   }
   // dH1 = dZ2 W2 (W2 stored [out=k][in=n]), dZ1 = dH1 * act'(z1)
-  float dz1[8][4];
+  float dz1[NJ][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     dz1[j][0] = dz1[j][1] = dz1[j][2] = dz1[j][3] = 0.f;
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
+    for (int kk = 0; kk < NK; ++kk) {
       uint32_t b[2];
-      bfrag_kn(b, s.m.w2, kMlpH, 16 * kk, 8 * j, lane);
+      bfrag_kn(b, s.m.w2, H, 16 * kk, 8 * j, lane);
       mma16816(dz1[j], a2[kk], b);
     }
 #pragma unroll
@@ -165,12 +168,12 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
   {
     const int ra = warp * 16 + g, rb = ra + 8;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < NJ; ++j) {
       const int col = 8 * j + 2 * t;
-      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[ra * kMlpH + col]) = __floats2bfloat162_rn(dz2[j][0], dz2[j][1]);
-      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[rb * kMlpH + col]) = __floats2bfloat162_rn(dz2[j][2], dz2[j][3]);
-      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[ra * kMlpH + col]) = __floats2bfloat162_rn(dz1[j][0], dz1[j][1]);
-      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[rb * kMlpH + col]) = __floats2bfloat162_rn(dz1[j][2], dz1[j][3]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[ra * H + col]) = __floats2bfloat162_rn(dz2[j][0], dz2[j][1]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ2[rb * H + col]) = __floats2bfloat162_rn(dz2[j][2], dz2[j][3]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[ra * H + col]) = __floats2bfloat162_rn(dz1[j][0], dz1[j][1]);
+      *reinterpret_cast<__nv_bfloat162*>(&s.dZ1[rb * H + col]) = __floats2bfloat162_rn(dz1[j][2], dz1[j][3]);
       atomicAdd(&s.db2[col], dz2[j][0] + dz2[j][2]);
       atomicAdd(&s.db2[col + 1], dz2[j][1] + dz2[j][3]);
       atomicAdd(&s.db1[col], dz1[j][0] + dz1[j][2]);
@@ -179,36 +182,37 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
   }
   __syncthreads();
   // weight gradients, contracting over the 128 points of the CTA
-  // dW2[o][i] = sum_r dZ2[r][o] H1[r][i]: 4 x 8 tiles, 4 per warp
+  // dW2[o][i] = sum_r dZ2[r][o] H1[r][i]: (H/16) x (H/8) tiles over the warps
 #pragma unroll 1
-  for (int tile = warp; tile < 32; tile += 8) {
-    const int m0 = (tile / 8) * 16, n0 = (tile % 8) * 8;
+  for (int tile = warp; tile < NK * NJ; tile += 8) {
+    const int m0 = (tile / NJ) * 16, n0 = (tile % NJ) * 8;
     float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int k0 = 0; k0 < kRows; k0 += 16) {
       uint32_t a[4], b[2];
-      afrag_km(a, s.dZ2, kMlpH, m0, k0, lane);
-      bfrag_kn(b, s.H1, kMlpH, k0, n0, lane);
+      afrag_km(a, s.dZ2, H, m0, k0, lane);
+      bfrag_kn(b, s.H1, H, k0, n0, lane);
       mma16816(c, a, b);
     }
-    float* G = grad + kOffW2;
-    atomicAdd(&G[(m0 + g) * kMlpH + n0 + 2 * t], c[0]);
-    atomicAdd(&G[(m0 + g) * kMlpH + n0 + 2 * t + 1], c[1]);
-    atomicAdd(&G[(m0 + g + 8) * kMlpH + n0 + 2 * t], c[2]);
-    atomicAdd(&G[(m0 + g + 8) * kMlpH + n0 + 2 * t + 1], c[3]);
+    float* G = grad + L::W2;
+    atomicAdd(&G[(m0 + g) * H + n0 + 2 * t], c[0]);
+    atomicAdd(&G[(m0 + g) * H + n0 + 2 * t + 1], c[1]);
+    atomicAdd(&G[(m0 + g + 8) * H + n0 + 2 * t], c[2]);
+    atomicAdd(&G[(m0 + g + 8) * H + n0 + 2 * t + 1], c[3]);
   }
-  // dW1[o][f] = sum_r dZ1[r][o] X[r][f]: 4 x 2 tiles, 1 per warp
-  {
-    const int m0 = (warp / 2) * 16, n0 = (warp % 2) * 8;
+  // dW1[o][f] = sum_r dZ1[r][o] X[r][f]: (H/16) x 2 tiles over the warps
+#pragma unroll 1
+  for (int tile = warp; tile < 2 * NK; tile += 8) {
+    const int m0 = (tile / 2) * 16, n0 = (tile % 2) * 8;
     float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int k0 = 0; k0 < kRows; k0 += 16) {
       uint32_t a[4], b[2];
-      afrag_km(a, s.dZ1, kMlpH, m0, k0, lane);
+      afrag_km(a, s.dZ1, H, m0, k0, lane);
       bfrag_kn(b, s.X, 16, k0, n0, lane);
       mma16816(c, a, b);
     }
-    float* G = grad + kOffW1;
+    float* G = grad + L::W1;
     const int f0 = n0 + 2 * t;
     if (f0 < kMlpIn) {
       atomicAdd(&G[(m0 + g) * kMlpIn + f0], c[0]);
@@ -219,29 +223,30 @@ __global__ void __launch_bounds__(256) mlp_train_kernel(const float* __restrict_
       atomicAdd(&G[(m0 + g + 8) * kMlpIn + f0 + 1], c[3]);
     }
   }
-  // dW3[c][i] = sum_r dY[r][c] H2[r][i]: m = 16 (6 used) x 8 n-tiles, 1 per warp
-  {
-    const int n0 = warp * 8;
+  // dW3[c][i] = sum_r dY[r][c] H2[r][i]: m = 16 (6 used) x H/8 n-tiles over the warps
+#pragma unroll 1
+  for (int tile = warp; tile < NJ; tile += 8) {
+    const int n0 = tile * 8;
     float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int k0 = 0; k0 < kRows; k0 += 16) {
       uint32_t a[4], b[2];
       afrag_km(a, s.dY, 16, 0, k0, lane);
-      bfrag_kn(b, s.H2, kMlpH, k0, n0, lane);
+      bfrag_kn(b, s.H2, H, k0, n0, lane);
       mma16816(c, a, b);
     }
-    float* G = grad + kOffW3;
+    float* G = grad + L::W3;
     if (g < kMlpOut) {
-      atomicAdd(&G[g * kMlpH + n0 + 2 * t], c[0]);
-      atomicAdd(&G[g * kMlpH + n0 + 2 * t + 1], c[1]);
+      atomicAdd(&G[g * H + n0 + 2 * t], c[0]);
+      atomicAdd(&G[g * H + n0 + 2 * t + 1], c[1]);
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    atomicAdd(&grad[kOffB1 + i], s.db1[i]);
-    atomicAdd(&grad[kOffB2 + i], s.db2[i]);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    atomicAdd(&grad[L::B1 + i], s.db1[i]);
+    atomicAdd(&grad[L::B2 + i], s.db2[i]);
   }
-  if (threadIdx.x < kMlpOut) atomicAdd(&grad[kOffB3 + threadIdx.x], s.db3[threadIdx.x]);
+  if (threadIdx.x < kMlpOut) atomicAdd(&grad[L::B3 + threadIdx.x], s.db3[threadIdx.x]);
   if (threadIdx.x == 0) atomicAdd(loss_acc, (double)s.loss / (6.0 * (double)B));
 }
 
@@ -259,13 +264,13 @@ __global__ void adam_kernel(float* __restrict__ P, float* __restrict__ m, float*
   grad[i] = 0.f;
 }
 
-template <int ACT>
+template <int ACT, int H>
 __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restrict__ P, const float* __restrict__ nrm,
                                                           const float* __restrict__ X, int B,
                                                           float* __restrict__ Y) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
-  mlp_stage_fwd(s, P, nrm);
+  MlpFwdSmem<H>& s = *reinterpret_cast<MlpFwdSmem<H>*>(smem_raw);
+  mlp_stage_fwd<H>(s, P, nrm);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
   const int nw = blockDim.x >> 5;
@@ -275,7 +280,7 @@ __global__ void __launch_bounds__(256) mlp_forward_kernel(const float* __restric
       return r0 + r < B ? X[(long long)(r0 + r) * kMlpIn + f] : s.xmean[f];
     });
     float y[4];
-    mlp_forward_fast<ACT>(s, xa, y);
+    mlp_forward_fast<ACT, H>(s, xa, y);
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int c = 2 * t + (e & 1), r = r0 + g + (e < 2 ? 0 : 8);
@@ -498,57 +503,69 @@ int psb_mlp_forward_tc(psb_ctx* c, int act, const float* params, const float* no
 }
 
 
-int psb_mlp_sizes(int* nparams, int* nnorm) {
-  if (!nparams || !nnorm) return PSB_ERR_ARG;
-  *nparams = kMlpParams;
+// width 0 means 64 (the models trained before the width became a property)
+static int mlp_width(int hidden) { return hidden == 0 ? 64 : hidden; }
+static bool mlp_width_ok(int hidden) { return mlp_width(hidden) == 32 || mlp_width(hidden) == 64; }
+
+int psb_mlp_sizes(int hidden, int* nparams, int* nnorm) {
+  if (!nparams || !nnorm || !mlp_width_ok(hidden)) return PSB_ERR_ARG;
+  *nparams = mlp_width(hidden) == 32 ? MlpLayout<32>::NPARAMS : MlpLayout<64>::NPARAMS;
   *nnorm = kMlpNorm;
   return PSB_OK;
 }
 
-int psb_mlp_forward(psb_ctx* c, int act, const float* params, const float* norm, const float* X, int B, float* Y) {
+int psb_mlp_forward(psb_ctx* c, int act, int hidden, const float* params, const float* norm, const float* X, int B,
+                    float* Y) {
   if (!c) return PSB_ERR_ARG;
-  if (!params || !norm || !X || !Y || B < 0 || (act != kActGelu && act != kActRelu))
+  if (!params || !norm || !X || !Y || B < 0 || (act != kActGelu && act != kActRelu) || !mlp_width_ok(hidden))
     return fail(c, PSB_ERR_ARG, "psb_mlp_forward: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   if (B == 0) return PSB_OK;
-  const size_t smem = sizeof(MlpFwdSmem);
   const int blocks = (int)std::min<long long>(((long long)B + 127) / 128, 148 * 8);
-  ++c->launches;
-  if (act == kActRelu)
-    mlp_forward_kernel<kActRelu><<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
-  else
-    mlp_forward_kernel<kActGelu><<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
-  return launch_ok(c, "mlp forward");
+  auto go = [&](auto k, size_t smem) {
+    ++c->launches;
+    k<<<blocks, 256, smem, c->stream>>>(params, norm, X, B, Y);
+    return launch_ok(c, "mlp forward");
+  };
+  if (mlp_width(hidden) == 32)
+    return act == kActRelu ? go(mlp_forward_kernel<kActRelu, 32>, sizeof(MlpFwdSmem<32>))
+                           : go(mlp_forward_kernel<kActGelu, 32>, sizeof(MlpFwdSmem<32>));
+  return act == kActRelu ? go(mlp_forward_kernel<kActRelu, 64>, sizeof(MlpFwdSmem<64>))
+                         : go(mlp_forward_kernel<kActGelu, 64>, sizeof(MlpFwdSmem<64>));
 }
 
-int psb_mlp_grad(psb_ctx* c, int act, const float* params, const float* norm, const float* X, const float* T,
-                 const int* idx, int B, float* grad, double* loss) {
+int psb_mlp_grad(psb_ctx* c, int act, int hidden, const float* params, const float* norm, const float* X,
+                 const float* T, const int* idx, int B, float* grad, double* loss) {
   if (!c) return PSB_ERR_ARG;
-  if (!params || !norm || !X || !T || !idx || !grad || !loss || B <= 0 || (act != kActGelu && act != kActRelu))
+  if (!params || !norm || !X || !T || !idx || !grad || !loss || B <= 0 || (act != kActGelu && act != kActRelu) ||
+      !mlp_width_ok(hidden))
     return fail(c, PSB_ERR_ARG, "psb_mlp_grad: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
-  const size_t smem = sizeof(TrainSmem);
   const unsigned grid = (unsigned)((B + kRows - 1) / kRows);
-  ++c->launches;
-  if (act == kActRelu) {
-    set_smem(mlp_train_kernel<kActRelu>, smem);
-    mlp_train_kernel<kActRelu><<<grid, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
-  } else {
-    set_smem(mlp_train_kernel<kActGelu>, smem);
-    mlp_train_kernel<kActGelu><<<grid, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
-  }
-  return launch_ok(c, "mlp train");
+  auto go = [&](auto k, size_t smem) {
+    set_smem(k, smem);
+    ++c->launches;
+    k<<<grid, 256, smem, c->stream>>>(params, norm, X, T, idx, B, grad, loss);
+    return launch_ok(c, "mlp train");
+  };
+  if (mlp_width(hidden) == 32)
+    return act == kActRelu ? go(mlp_train_kernel<kActRelu, 32>, sizeof(TrainSmem<32>))
+                           : go(mlp_train_kernel<kActGelu, 32>, sizeof(TrainSmem<32>));
+  return act == kActRelu ? go(mlp_train_kernel<kActRelu, 64>, sizeof(TrainSmem<64>))
+                         : go(mlp_train_kernel<kActGelu, 64>, sizeof(TrainSmem<64>));
 }
 
-int psb_mlp_adam(psb_ctx* c, float* params, float* m, float* v, float* grad, int step, float lr, float beta1,
-                 float beta2, float eps, float weight_decay) {
+int psb_mlp_adam(psb_ctx* c, int hidden, float* params, float* m, float* v, float* grad, int step, float lr,
+                 float beta1, float beta2, float eps, float weight_decay) {
   if (!c) return PSB_ERR_ARG;
-  if (!params || !m || !v || !grad || step < 1) return fail(c, PSB_ERR_ARG, "psb_mlp_adam: bad argument");
+  if (!params || !m || !v || !grad || step < 1 || !mlp_width_ok(hidden))
+    return fail(c, PSB_ERR_ARG, "psb_mlp_adam: bad argument");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  const int n = mlp_width(hidden) == 32 ? MlpLayout<32>::NPARAMS : MlpLayout<64>::NPARAMS;
   const float c1 = 1.f - std::pow(beta1, (float)step), c2 = 1.f - std::pow(beta2, (float)step);
   ++c->launches;
-  adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, c->stream>>>(params, m, v, grad, kMlpParams, lr, beta1, beta2, eps,
-                                                              c1, c2, weight_decay);
+  adam_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(params, m, v, grad, n, lr, beta1, beta2, eps, c1, c2,
+                                                       weight_decay);
   return launch_ok(c, "adam");
 }
 

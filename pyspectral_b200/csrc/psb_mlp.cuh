@@ -1,14 +1,15 @@
-// Pointwise subgrid-stress MLP 10 -> 64 -> 64 -> 6 on BF16 tensor cores with
+// Pointwise subgrid-stress MLP 10 -> H -> H -> 6 on BF16 tensor cores with
 // FP32 accumulation (mma.sync.m16n8k16.bf16, FP32 C/D fragments).  Hidden
-// activation: GELU (kActGelu) or ReLU (kActRelu), a property of the model.
+// width H (32 or 64) and activation (GELU, kActGelu, or ReLU, kActRelu) are
+// properties of the model.
 //
 // This closure has no counterpart in the reference; it replaces the
 // Smagorinsky stress of PySpectral/src/RHSfunctions.py:195-212 by a learned
 // map from the 9 resolved velocity-gradient components and the filter width
 // to the 6 subgrid-stress components tau_ij = filter(u_i u_j) - u_i u_j.
 //
-// Parameter block (FP32 master copy, kMlpParams floats, row-major [out][in]):
-//   W1[64][10] b1[64] W2[64][64] b2[64] W3[6][64] b3[6]
+// Parameter block (FP32 master copy, MlpLayout<H>::NPARAMS floats, row-major
+// [out][in]):  W1[H][10] b1[H] W2[H][H] b2[H] W3[6][H] b3[6]
 // Normalisation block (kMlpNorm floats):
 //   xmean[10] xistd[10] ymean[6] ystd[6]
 // Features x = (raw - xmean) * xistd; outputs tau = y * ystd + ymean.
@@ -18,43 +19,56 @@
 
 namespace psb {
 
-constexpr int kMlpIn = 10, kMlpH = 64, kMlpOut = 6;
-constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kMlpH * kMlpIn, kOffW2 = kOffB1 + kMlpH,
-              kOffB2 = kOffW2 + kMlpH * kMlpH, kOffW3 = kOffB2 + kMlpH, kOffB3 = kOffW3 + kMlpOut * kMlpH,
-              kMlpParams = kOffB3 + kMlpOut;
+constexpr int kMlpIn = 10, kMlpOut = 6;
 constexpr int kMlpNorm = 32;
 constexpr int kActGelu = 0, kActRelu = 1;
 
+// Offsets of the parameter block of a width-H network.
+template <int H>
+struct MlpLayout {
+  static_assert(H == 32 || H == 64, "hidden width 32 or 64");
+  static constexpr int W1 = 0, B1 = W1 + H * kMlpIn, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H,
+                       B3 = W3 + kMlpOut * H, NPARAMS = B3 + kMlpOut;
+};
+// the width-64 network's layout (the tcgen05 inference kernel's)
+constexpr int kMlpH = 64;
+constexpr int kOffW1 = MlpLayout<64>::W1, kOffB1 = MlpLayout<64>::B1, kOffW2 = MlpLayout<64>::W2,
+              kOffB2 = MlpLayout<64>::B2, kOffW3 = MlpLayout<64>::W3, kOffB3 = MlpLayout<64>::B3,
+              kMlpParams = MlpLayout<64>::NPARAMS;
+
 // BF16 operand copies staged in shared memory, padded for the m16n8k16 tiles:
-//   w1[64][16] (k padded 10->16), w2[64][64], w3[8][64] (n padded 6->8)
+//   w1[H][16] (k padded 10->16), w2[H][H], w3[8][H] (n padded 6->8)
+template <int H>
 struct MlpSmem {
-  __nv_bfloat16 w1[kMlpH * 16];
-  __nv_bfloat16 w2[kMlpH * kMlpH];
-  __nv_bfloat16 w3[8 * kMlpH];
-  float b1[kMlpH], b2[kMlpH], b3[8];
+  __nv_bfloat16 w1[H * 16];
+  __nv_bfloat16 w2[H * H];
+  __nv_bfloat16 w3[8 * H];
+  float b1[H], b2[H], b3[8];
   float xmean[16], xistd[16], ymean[8], ystd[8];
 };
 
-__device__ __forceinline__ void mlp_stage(MlpSmem& s, const float* __restrict__ P, const float* __restrict__ nrm) {
-  for (int i = threadIdx.x; i < kMlpH * 16; i += blockDim.x) {
+template <int H>
+__device__ __forceinline__ void mlp_stage(MlpSmem<H>& s, const float* __restrict__ P, const float* __restrict__ nrm) {
+  using L = MlpLayout<H>;
+  for (int i = threadIdx.x; i < H * 16; i += blockDim.x) {
     const int o = i / 16, k = i % 16;
-    s.w1[i] = __float2bfloat16_rn(k < kMlpIn ? P[kOffW1 + o * kMlpIn + k] : 0.f);
+    s.w1[i] = __float2bfloat16_rn(k < kMlpIn ? P[L::W1 + o * kMlpIn + k] : 0.f);
   }
-  for (int i = threadIdx.x; i < kMlpH * kMlpH; i += blockDim.x) s.w2[i] = __float2bfloat16_rn(P[kOffW2 + i]);
-  for (int i = threadIdx.x; i < 8 * kMlpH; i += blockDim.x) {
-    const int o = i / kMlpH;
-    s.w3[i] = __float2bfloat16_rn(o < kMlpOut ? P[kOffW3 + i] : 0.f);
+  for (int i = threadIdx.x; i < H * H; i += blockDim.x) s.w2[i] = __float2bfloat16_rn(P[L::W2 + i]);
+  for (int i = threadIdx.x; i < 8 * H; i += blockDim.x) {
+    const int o = i / H;
+    s.w3[i] = __float2bfloat16_rn(o < kMlpOut ? P[L::W3 + i] : 0.f);
   }
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    s.b1[i] = P[kOffB1 + i];
-    s.b2[i] = P[kOffB2 + i];
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    s.b1[i] = P[L::B1 + i];
+    s.b2[i] = P[L::B2 + i];
   }
   if (threadIdx.x < 16) {
     s.xmean[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[threadIdx.x] : 0.f;
     s.xistd[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[kMlpIn + threadIdx.x] : 0.f;
   }
   if (threadIdx.x < 8) {
-    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[kOffB3 + threadIdx.x] : 0.f;
+    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[L::B3 + threadIdx.x] : 0.f;
     s.ymean[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + threadIdx.x] : 0.f;
     s.ystd[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + kMlpOut + threadIdx.x] : 0.f;
   }
@@ -195,13 +209,14 @@ __device__ __forceinline__ void bfrag_nk(uint32_t* b, const __nv_bfloat16* W, in
 // features (16 x 16, k 10..15 zero).  Returns y[4]: C fragment of the 16 x 8
 // outputs (normalised; columns 6,7 unused).  If z1/z2 are given, the
 // pre-activations are kept (for the backward pass).
-template <int ACT>
-__device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_t* xa, float* y, float (*z1)[4],
+template <int ACT, int H>
+__device__ __forceinline__ void mlp_forward_warp(const MlpSmem<H>& s, const uint32_t* xa, float* y, float (*z1)[4],
                                                  float (*z2)[4]) {
+  constexpr int NJ = H / 8, NK = H / 16;  // n-tiles of 8 and k-steps of 16 over the hidden width
   const int lane = threadIdx.x & 31, t = lane & 3;
-  float h[8][4];
+  float h[NJ][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const float b0 = s.b1[8 * j + 2 * t], b1 = s.b1[8 * j + 2 * t + 1];
     h[j][0] = b0;
     h[j][1] = b1;
@@ -211,44 +226,44 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
     bfrag_nk(b, s.w1, 16, 0, 8 * j, lane);
     mma16816(h[j], xa, b);
   }
-  uint32_t a[4][4];
+  uint32_t a[NK][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j)
+  for (int j = 0; j < NJ; ++j)
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (z1) z1[j][e] = h[j][e];
       h[j][e] = act_f<ACT>(h[j][e]);
     }
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     a[kk][0] = pack_bf16(h[2 * kk][0], h[2 * kk][1]);
     a[kk][1] = pack_bf16(h[2 * kk][2], h[2 * kk][3]);
     a[kk][2] = pack_bf16(h[2 * kk + 1][0], h[2 * kk + 1][1]);
     a[kk][3] = pack_bf16(h[2 * kk + 1][2], h[2 * kk + 1][3]);
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const float b0 = s.b2[8 * j + 2 * t], b1 = s.b2[8 * j + 2 * t + 1];
     h[j][0] = b0;
     h[j][1] = b1;
     h[j][2] = b0;
     h[j][3] = b1;
 #pragma unroll
-    for (int kk = 0; kk < 4; ++kk) {
+    for (int kk = 0; kk < NK; ++kk) {
       uint32_t b[2];
-      bfrag_nk(b, s.w2, kMlpH, 16 * kk, 8 * j, lane);
+      bfrag_nk(b, s.w2, H, 16 * kk, 8 * j, lane);
       mma16816(h[j], a[kk], b);
     }
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j)
+  for (int j = 0; j < NJ; ++j)
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       if (z2) z2[j][e] = h[j][e];
       h[j][e] = act_f<ACT>(h[j][e]);
     }
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     a[kk][0] = pack_bf16(h[2 * kk][0], h[2 * kk][1]);
     a[kk][1] = pack_bf16(h[2 * kk][2], h[2 * kk][3]);
     a[kk][2] = pack_bf16(h[2 * kk + 1][0], h[2 * kk + 1][1]);
@@ -260,9 +275,9 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
   y[2] = c0;
   y[3] = c1;
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     uint32_t b[2];
-    bfrag_nk(b, s.w3, kMlpH, 16 * kk, 0, lane);
+    bfrag_nk(b, s.w3, H, 16 * kk, 0, lane);
     mma16816(y, a[kk], b);
   }
 }
@@ -273,11 +288,12 @@ __device__ __forceinline__ void mlp_forward_warp(const MlpSmem& s, const uint32_
 //   f1[j][lane]      W1 tile (k 0..15, n 8j..8j+7)
 //   f2[kk][j][lane]  W2 tile (k 16kk.., n 8j..)
 //   f3[kk][lane]     W3 tile (k 16kk.., n 0..7)
+template <int H>
 struct MlpFwdSmem {
-  uint2 f1[8 * 32];
-  uint2 f2[4 * 8 * 32];
-  uint2 f3[4 * 32];
-  float b1[kMlpH], b2[kMlpH], b3[8];
+  uint2 f1[(H / 8) * 32];
+  uint2 f2[(H / 16) * (H / 8) * 32];
+  uint2 f3[(H / 16) * 32];
+  float b1[H], b2[H], b3[8];
   float xmean[16], xistd[16], ymean[8], ystd[8];
 };
 
@@ -296,24 +312,29 @@ __device__ __forceinline__ uint2 bfrag_from_f32(const float* __restrict__ W, int
   return make_uint2(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]));
 }
 
-__device__ __forceinline__ void mlp_stage_fwd(MlpFwdSmem& s, const float* __restrict__ P,
+template <int H>
+__device__ __forceinline__ void mlp_stage_fwd(MlpFwdSmem<H>& s, const float* __restrict__ P,
                                               const float* __restrict__ nrm) {
-  for (int i = threadIdx.x; i < 8 * 32; i += blockDim.x) s.f1[i] = bfrag_from_f32(P + kOffW1, kMlpIn, kMlpH, 0, 8 * (i >> 5), i & 31);
-  for (int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
-    const int tile = i >> 5, kk = tile >> 3, j = tile & 7;
-    s.f2[i] = bfrag_from_f32(P + kOffW2, kMlpH, kMlpH, 16 * kk, 8 * j, i & 31);
+  using L = MlpLayout<H>;
+  constexpr int NJ = H / 8, NK = H / 16;
+  for (int i = threadIdx.x; i < NJ * 32; i += blockDim.x)
+    s.f1[i] = bfrag_from_f32(P + L::W1, kMlpIn, H, 0, 8 * (i >> 5), i & 31);
+  for (int i = threadIdx.x; i < NK * NJ * 32; i += blockDim.x) {
+    const int tile = i >> 5, kk = tile / NJ, j = tile - kk * NJ;
+    s.f2[i] = bfrag_from_f32(P + L::W2, H, H, 16 * kk, 8 * j, i & 31);
   }
-  for (int i = threadIdx.x; i < 4 * 32; i += blockDim.x) s.f3[i] = bfrag_from_f32(P + kOffW3, kMlpH, kMlpOut, 16 * (i >> 5), 0, i & 31);
-  for (int i = threadIdx.x; i < kMlpH; i += blockDim.x) {
-    s.b1[i] = P[kOffB1 + i];
-    s.b2[i] = P[kOffB2 + i];
+  for (int i = threadIdx.x; i < NK * 32; i += blockDim.x)
+    s.f3[i] = bfrag_from_f32(P + L::W3, H, kMlpOut, 16 * (i >> 5), 0, i & 31);
+  for (int i = threadIdx.x; i < H; i += blockDim.x) {
+    s.b1[i] = P[L::B1 + i];
+    s.b2[i] = P[L::B2 + i];
   }
   if (threadIdx.x < 16) {
     s.xmean[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[threadIdx.x] : 0.f;
     s.xistd[threadIdx.x] = threadIdx.x < kMlpIn ? nrm[kMlpIn + threadIdx.x] : 0.f;
   }
   if (threadIdx.x < 8) {
-    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[kOffB3 + threadIdx.x] : 0.f;
+    s.b3[threadIdx.x] = threadIdx.x < kMlpOut ? P[L::B3 + threadIdx.x] : 0.f;
     s.ymean[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + threadIdx.x] : 0.f;
     s.ystd[threadIdx.x] = threadIdx.x < kMlpOut ? nrm[2 * kMlpIn + kMlpOut + threadIdx.x] : 0.f;
   }
@@ -322,12 +343,13 @@ __device__ __forceinline__ void mlp_stage_fwd(MlpFwdSmem& s, const float* __rest
 // Forward pass of 16 points from the fragment-ordered weights; same
 // arithmetic as mlp_forward_warp (BF16 operands, FP32 accumulation, the
 // activation on the FP32 pre-activations, BF16 rounding of the activations).
-template <int ACT>
-__device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint32_t* xa, float* y) {
+template <int ACT, int H>
+__device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem<H>& s, const uint32_t* xa, float* y) {
+  constexpr int NJ = H / 8, NK = H / 16;
   const int lane = threadIdx.x & 31, t = lane & 3;
-  float h[8][4];
+  float h[NJ][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const float b0 = s.b1[8 * j + 2 * t], b1 = s.b1[8 * j + 2 * t + 1];
     h[j][0] = b0;
     h[j][1] = b1;
@@ -337,16 +359,16 @@ __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint
     const uint32_t b[2] = {bb.x, bb.y};
     mma16816(h[j], xa, b);
   }
-  uint32_t a[4][4];
+  uint32_t a[NK][4];
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     a[kk][0] = act_pack<ACT>(h[2 * kk][0], h[2 * kk][1]);
     a[kk][1] = act_pack<ACT>(h[2 * kk][2], h[2 * kk][3]);
     a[kk][2] = act_pack<ACT>(h[2 * kk + 1][0], h[2 * kk + 1][1]);
     a[kk][3] = act_pack<ACT>(h[2 * kk + 1][2], h[2 * kk + 1][3]);
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < NJ; ++j) {
     const float b0 = s.b2[8 * j + 2 * t], b1 = s.b2[8 * j + 2 * t + 1];
     h[j][0] = b0;
     h[j][1] = b1;
@@ -354,15 +376,15 @@ __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint
     h[j][3] = b1;
   }
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk)
+  for (int kk = 0; kk < NK; ++kk)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const uint2 bb = s.f2[(kk * 8 + j) * 32 + lane];
+    for (int j = 0; j < NJ; ++j) {
+      const uint2 bb = s.f2[(kk * NJ + j) * 32 + lane];
       const uint32_t b[2] = {bb.x, bb.y};
       mma16816(h[j], a[kk], b);
     }
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     a[kk][0] = act_pack<ACT>(h[2 * kk][0], h[2 * kk][1]);
     a[kk][1] = act_pack<ACT>(h[2 * kk][2], h[2 * kk][3]);
     a[kk][2] = act_pack<ACT>(h[2 * kk + 1][0], h[2 * kk + 1][1]);
@@ -374,7 +396,7 @@ __device__ __forceinline__ void mlp_forward_fast(const MlpFwdSmem& s, const uint
   y[2] = c0;
   y[3] = c1;
 #pragma unroll
-  for (int kk = 0; kk < 4; ++kk) {
+  for (int kk = 0; kk < NK; ++kk) {
     const uint2 bb = s.f3[kk * 32 + lane];
     const uint32_t b[2] = {bb.x, bb.y};
     mma16816(y, a[kk], b);

@@ -661,11 +661,12 @@ struct PreGradXY {
 // The MLP runs warp-cooperatively on tensor cores over all points of the CTA.
 // ACT: the network's hidden activation (kActRelu or kActGelu); a separate
 // kernel per activation keeps the ReLU kernel free of the GELU's registers.
-template <typename T, int ACT = kActRelu>
+// H: the network's hidden width (32 or 64).
+template <typename T, int ACT = kActRelu, int H = 64>
 struct PhysLearned {
   static constexpr int F_IN = 12, F_OUT = 6;
   static constexpr bool BLOCK = true;
-  static constexpr int EXTRA_SMEM = (int)((sizeof(MlpFwdSmem) + 15) / 16 * 16);
+  static constexpr int EXTRA_SMEM = (int)((sizeof(MlpFwdSmem<H>) + 15) / 16 * 16);
   // 4 pencils per CTA by default (3 CTAs per SM at 3N/2 = 96, FP32); the
   // autotuner also tries 8 (fuller transform passes, 2 CTAs per SM)
   static constexpr int DEFAULT_PPC = 4, MAX_PPC = 8;
@@ -674,7 +675,7 @@ struct PhysLearned {
   T sphys;      // s: physical = real-space * s
   float delta;  // filter width fed to the MLP
   __device__ void setup(unsigned char* extra) const {
-    mlp_stage_fwd(*reinterpret_cast<MlpFwdSmem*>(extra), params, norm);
+    mlp_stage_fwd<H>(*reinterpret_cast<MlpFwdSmem<H>*>(extra), params, norm);
   }
   __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
                         unsigned char* extra) const {
@@ -684,7 +685,7 @@ struct PhysLearned {
   // holds rows g and g+8 of a tile and locates them once per tile.
   __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, T fac,
                                             unsigned char* extra) const {
-    const MlpFwdSmem& s = *reinterpret_cast<const MlpFwdSmem*>(extra);
+    const MlpFwdSmem<H>& s = *reinterpret_cast<const MlpFwdSmem<H>*>(extra);
     if ((M & 15) == 0 && (P & 1) == 0) {
       block_tiles(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, fac, s);
       return;
@@ -717,7 +718,7 @@ struct PhysLearned {
         return f < 9 ? (float)(val(3 + f, h) * fs) : delta;
       });
       float y[4];
-      mlp_forward_fast<ACT>(s, xa, y);
+      mlp_forward_fast<ACT, H>(s, xa, y);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int c = 2 * t + (e & 1);
@@ -739,7 +740,7 @@ struct PhysLearned {
   // offsets, normalisation and output coefficients of its fragment slots in
   // registers; per tile it computes one base index per row.
   __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, T fac,
-                                              const MlpFwdSmem& s) const {
+                                              const MlpFwdSmem<H>& s) const {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int nw = blockDim.x >> 5;
     const int fst = P * M;
@@ -793,7 +794,7 @@ struct PhysLearned {
       xa[2] = pack_bf16(v[2], v[3]);  // row g,   k 2t+8..
       xa[3] = pack_bf16(v[6], v[7]);  // row g+8, k 2t+8..
       float y[4];
-      mlp_forward_fast<ACT>(s, xa, y);
+      mlp_forward_fast<ACT, H>(s, xa, y);
       if (out_ok) {
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -816,8 +817,8 @@ struct phys_fixed_fft<PhysSmag<T>> {
   static constexpr bool value = true;
 };
 // (the GELU network keeps the runtime schedules: it is not the shipped model)
-template <typename T>
-struct phys_fixed_fft<PhysLearned<T, kActRelu>> {
+template <typename T, int H>
+struct phys_fixed_fft<PhysLearned<T, kActRelu, H>> {
   static constexpr bool value = true;
 };
 

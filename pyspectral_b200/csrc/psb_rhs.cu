@@ -841,14 +841,19 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
         return fail(c, PSB_ERR_ARG, "PSB_LEARNED needs mlp_params and mlp_norm");
       if (p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
         return fail(c, PSB_ERR_ARG, "PSB_LEARNED: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
+      if (!(p->mlp_hidden == 0 || p->mlp_hidden == 64 || (p->mlp_hidden == 32 && p->mlp_act == PSB_ACT_RELU)))
+        return fail(c, PSB_ERR_ARG, "PSB_LEARNED: mlp_hidden must be 64 (0), or 32 with PSB_ACT_RELU");
       EpiNS<T, false> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
                           (T)p->Om3, 1, c->N1 / 2, c->N2 / 2, c->N3 / 2};
       const double s32 = std::sqrt(std::pow(1.5, 3) * std::sqrt((double)c->N1 * c->N2 * c->N3));
       const float* mp = reinterpret_cast<const float*>(p->mlp_params);
       const float* mn = reinterpret_cast<const float*>(p->mlp_norm);
       const float delta = (float)(p->les_delta > 0 ? p->les_delta : c->Delta);
+      // width-32 networks are built with ReLU only
       if (p->mlp_act == PSB_ACT_GELU)
         return run_ns32<T>(c, Qin, PreGradXY<T>{}, PhysLearned<T, kActGelu>{mp, mn, (T)s32, delta}, epi, ts);
+      if (p->mlp_hidden == 32)
+        return run_ns32<T>(c, Qin, PreGradXY<T>{}, PhysLearned<T, kActRelu, 32>{mp, mn, (T)s32, delta}, epi, ts);
       return run_ns32<T>(c, Qin, PreGradXY<T>{}, PhysLearned<T, kActRelu>{mp, mn, (T)s32, delta}, epi, ts);
     }
     default:
@@ -1070,6 +1075,9 @@ extern "C" int psb_autotune(psb_ctx* c, int closure, void* state, const psb_para
     return fail(c, PSB_ERR_ARG, "psb_autotune: PSB_LEARNED needs mlp_params and mlp_norm");
   if (closure == PSB_LEARNED && p->mlp_act != PSB_ACT_GELU && p->mlp_act != PSB_ACT_RELU)
     return fail(c, PSB_ERR_ARG, "psb_autotune: mlp_act must be PSB_ACT_GELU or PSB_ACT_RELU");
+  if (closure == PSB_LEARNED &&
+      !(p->mlp_hidden == 0 || p->mlp_hidden == 64 || (p->mlp_hidden == 32 && p->mlp_act == PSB_ACT_RELU)))
+    return fail(c, PSB_ERR_ARG, "psb_autotune: mlp_hidden must be 64 (0), or 32 with PSB_ACT_RELU");
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   return c->prec == 64 ? psbh::tuning::tune_rhs<double>(c, closure, state, p)
                         : psbh::tuning::tune_rhs<float>(c, closure, state, p);

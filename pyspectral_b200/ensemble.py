@@ -132,7 +132,8 @@ class Ensemble:
                 p = _capi.make_params(nu=s["nu"], dt=dt,
                                       mlp_params=model.params.data_ptr() if use_learned else None,
                                       mlp_norm=model.norm.data_ptr() if use_learned else None,
-                                      les_delta=2 * math.pi / N, mlp_act=model.act if use_learned else 0)
+                                      les_delta=2 * math.pi / N, mlp_act=model.act if use_learned else 0,
+                                      mlp_hidden=model.hidden if use_learned else 0)
                 b.set_run(r, st, comp, p)
                 states.append(st)
                 comps.append(comp)

@@ -43,11 +43,11 @@ def _lib():
     lib = _capi.load()
     if not hasattr(lib, "_mlp_bound"):
         vp, i, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
-        lib.psb_mlp_sizes.argtypes = [ctypes.POINTER(i), ctypes.POINTER(i)]
-        lib.psb_mlp_forward.argtypes = [vp, i, vp, vp, vp, i, vp]
+        lib.psb_mlp_sizes.argtypes = [i, ctypes.POINTER(i), ctypes.POINTER(i)]
+        lib.psb_mlp_forward.argtypes = [vp, i, i, vp, vp, vp, i, vp]
         lib.psb_mlp_forward_tc.argtypes = [vp, i, vp, vp, vp, i, vp, vp]
-        lib.psb_mlp_grad.argtypes = [vp, i, vp, vp, vp, vp, vp, i, vp, vp]
-        lib.psb_mlp_adam.argtypes = [vp, vp, vp, vp, vp, i, f, f, f, f, f]
+        lib.psb_mlp_grad.argtypes = [vp, i, i, vp, vp, vp, vp, vp, i, vp, vp]
+        lib.psb_mlp_adam.argtypes = [vp, i, vp, vp, vp, vp, i, f, f, f, f, f]
         lib.psb_physical_fields.argtypes = [vp, vp, i, vp]
         lib.psb_products.argtypes = [vp, vp, vp]
         lib.psb_spectral_resample.argtypes = [vp, i, i, i, vp, i, i, i, i, i, d, i, vp]
@@ -62,9 +62,10 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def nparams():
+def nparams(hidden=NH):
     a, b = ctypes.c_int(), ctypes.c_int()
-    _lib().psb_mlp_sizes(ctypes.byref(a), ctypes.byref(b))
+    if _lib().psb_mlp_sizes(int(hidden), ctypes.byref(a), ctypes.byref(b)) != 0:
+        raise ValueError(f"hidden width {hidden}: 32 or 64")
     return a.value, b.value
 
 
@@ -76,17 +77,20 @@ class MLPModel:
     `act` is the hidden activation ("gelu" or "relu"), a property of the
     trained model (recorded in its metadata)."""
 
-    def __init__(self, seed=0, device=0, params=None, norm=None, act="gelu"):
+    def __init__(self, seed=0, device=0, params=None, norm=None, act="gelu", hidden=NH):
         if act not in ACTS:
             raise ValueError(f"unknown activation {act!r} (expected one of {sorted(ACTS)})")
+        if hidden == 32 and act != "relu":
+            raise ValueError("width-32 networks are built with ReLU")
         self.act_name = act
         self.act = ACTS[act]
-        n, nn = nparams()
+        self.hidden = int(hidden)
+        n, nn = nparams(self.hidden)
         dev = torch.device("cuda", device)
         if params is None:
             rs = np.random.RandomState(seed)
             parts = []
-            for fan_out, fan_in in ((NH, NIN), (NH, NH), (NOUT, NH)):
+            for fan_out, fan_in in ((hidden, NIN), (hidden, hidden), (NOUT, hidden)):
                 b = 1.0 / math.sqrt(fan_in)
                 parts += [rs.uniform(-b, b, size=fan_out * fan_in), np.zeros(fan_out)]
             params = np.concatenate(parts)
@@ -111,25 +115,29 @@ class MLPModel:
     def save(self, path, **meta):
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
         np.savez(path, params=self.params.cpu().numpy(), norm=self.norm.cpu().numpy(),
-                 meta=json.dumps({**self.meta, **meta, "act": self.act_name}))
+                 meta=json.dumps({**self.meta, **meta, "act": self.act_name, "hidden": self.hidden}))
 
     @classmethod
     def load(cls, path=DEFAULT_MODEL, device=0):
         d = np.load(path)
         meta = json.loads(str(d["meta"])) if "meta" in d else {}
-        m = cls(device=device, params=d["params"], norm=d["norm"], act=meta.get("act", "gelu"))
+        m = cls(device=device, params=d["params"], norm=d["norm"], act=meta.get("act", "gelu"),
+                hidden=meta.get("hidden", NH))
         m.meta = meta
         return m
 
     def forward(self, ctx, X):
         Y = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
         ctx.bind_stream()
-        ctx.check(_lib().psb_mlp_forward(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X.contiguous()),
+        ctx.check(_lib().psb_mlp_forward(ctx.h, self.act, self.hidden, _p(self.params), _p(self.norm), _p(X.contiguous()),
                                          X.shape[0], _p(Y)), "psb_mlp_forward")
         return Y
 
     def forward_tc(self, ctx, X):
-        """forward() on the tcgen05 tensor-core kernel; raises if an MMA timed out."""
+        """forward() on the tcgen05 tensor-core kernel (width-64 networks);
+        raises if an MMA timed out."""
+        if self.hidden != 64:
+            raise ValueError("the tcgen05 kernel runs width-64 networks")
         Y = torch.empty((X.shape[0], NOUT), dtype=torch.float32, device=X.device)
         err = torch.zeros(1, dtype=torch.int32, device=X.device)
         ctx.bind_stream()
@@ -144,7 +152,7 @@ class MLPModel:
         self.grad.zero_()
         loss = torch.zeros(1, dtype=torch.float64, device=X.device)
         ctx.bind_stream()
-        ctx.check(_lib().psb_mlp_grad(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
+        ctx.check(_lib().psb_mlp_grad(ctx.h, self.act, self.hidden, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
                                       idx.numel(), _p(self.grad), _p(loss)), "psb_mlp_grad")
         return float(loss.item()), self.grad.clone()
 
@@ -166,11 +174,11 @@ class MLPModel:
                 pos = 0
             idx = perm[pos:pos + batch]
             pos += batch
-            ctx.check(lib.psb_mlp_grad(ctx.h, self.act, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
+            ctx.check(lib.psb_mlp_grad(ctx.h, self.act, self.hidden, _p(self.params), _p(self.norm), _p(X), _p(T), _p(idx),
                                        idx.numel(), _p(self.grad), _p(loss)), "psb_mlp_grad")
             self.step += 1
             lr_s = lr_end + 0.5 * (lr - lr_end) * (1 + math.cos(math.pi * s / max(1, steps)))
-            ctx.check(lib.psb_mlp_adam(ctx.h, _p(self.params), _p(self.m), _p(self.v), _p(self.grad), self.step,
+            ctx.check(lib.psb_mlp_adam(ctx.h, self.hidden, _p(self.params), _p(self.m), _p(self.v), _p(self.grad), self.step,
                                        lr_s, beta1, beta2, eps, 0.0), "psb_mlp_adam")
             if log_every and (s + 1) % log_every == 0:
                 hist.append((s + 1, float(loss.item()) / log_every))
@@ -341,6 +349,7 @@ def main():
     ap.add_argument("--no-eval", action="store_true")
     ap.add_argument("--nu", type=float, default=5e-4, help="viscosity of the DNS and the LES")
     ap.add_argument("--act", choices=sorted(ACTS), default="relu", help="hidden activation of the network")
+    ap.add_argument("--hidden", type=int, choices=(32, 64), default=NH, help="hidden width of the network")
     ap.add_argument("--eval-only", action="store_true",
                     help="re-run the a-posteriori evaluation of the model at --out and update its metadata")
     a = ap.parse_args()
@@ -357,7 +366,7 @@ def main():
     print("generating training data ...")
     X, T = generate(N_dns=a.N_dns, nu=a.nu, npoints=a.npoints)
     print(f"  {X.shape[0]} samples ({time.time() - t0:.1f} s)")
-    model = MLPModel(seed=0, act=a.act)
+    model = MLPModel(seed=0, act=a.act, hidden=a.hidden)
     model.fit_norm(X, T)
     ctx = _capi.Context(64, 64, 64, precision=32)
     hist = model.train(ctx, X, T, a.steps, batch=a.batch, log_every=max(1, a.steps // 20))
@@ -365,6 +374,7 @@ def main():
         print(f"  step {s:6d}  loss {l:.5f}")
     meta = {"train_samples": int(X.shape[0]), "train_steps": a.steps, "batch": a.batch,
             "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": a.nu, "act": a.act,
+            "hidden": a.hidden,
             "spectrum": "E(k)=16 sqrt(2/pi) u0^2 k^4/k0^5 exp(-2 k^2/k0^2), k0=4, u0=1"}
     model.meta = meta
     if not a.no_eval:

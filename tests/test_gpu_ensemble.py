@@ -48,7 +48,7 @@ def _batch_runs(torch, N, closure, precision, tune, model=None, steps=2, nruns=3
         comp = torch.zeros_like(st) if precision == 32 else None
         p = _capi.make_params(nu=nu, dt=2e-3, mlp_params=model.params.data_ptr() if model else None,
                               mlp_norm=model.norm.data_ptr() if model else None, les_delta=2 * np.pi / N,
-                              mlp_act=model.act if model else 0)
+                              mlp_act=model.act if model else 0, mlp_hidden=model.hidden if model else 0)
         b.set_run(r, st, comp, p)
         states.append(st)
         nus.append(nu)

@@ -30,19 +30,19 @@ def _data(n, seed=0):
     return X, T, norm
 
 
-def _model(torch, seed, norm, act="gelu"):
+def _model(torch, seed, norm, act="gelu", hidden=64):
     from pyspectral_b200.learned import MLPModel
-    P = mo.init_params(seed)
+    P = mo.init_params(seed, hidden)
     P = P + 0.05 * np.random.default_rng(seed).standard_normal(P.shape)  # nonzero biases
-    return MLPModel(params=P, norm=norm, act=act), P
+    return MLPModel(params=P, norm=norm, act=act, hidden=hidden), P
 
 
-@pytest.mark.parametrize("act", ["gelu", "relu"])
-def test_forward_and_gradients_match_cpu_oracle(act):
+@pytest.mark.parametrize("act,hidden", [("gelu", 64), ("relu", 64), ("relu", 32)])
+def test_forward_and_gradients_match_cpu_oracle(act, hidden):
     torch = _torch()
     from pyspectral_b200 import _capi
     X, T, norm = _data(300)
-    m, P = _model(torch, 3, norm, act)
+    m, P = _model(torch, 3, norm, act, hidden)
     ctx = _capi.Context(16, 16, 16, precision=32)
     Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
     Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
@@ -60,7 +60,7 @@ def test_forward_and_gradients_match_cpu_oracle(act):
     g = grad.cpu().numpy()
     # per block: W1 b1 W2 b2 W3 b3
     o = 0
-    for name, shp in mo.SIZES:
+    for name, shp in mo.sizes(hidden):
         k = int(np.prod(shp))
         assert rel(g[o:o + k], go[o:o + k]) < 5e-3, name
         o += k
@@ -87,15 +87,15 @@ def test_tcgen05_forward_matches_oracle_and_mma_sync(act, n):
     assert rel(Ytc, Ysync) < 2e-3
 
 
-@pytest.mark.parametrize("act", ["gelu", "relu"])
-def test_training_reduces_loss(act):
+@pytest.mark.parametrize("act,hidden", [("gelu", 64), ("relu", 64), ("relu", 32)])
+def test_training_reduces_loss(act, hidden):
     torch = _torch()
     from pyspectral_b200 import _capi
     from pyspectral_b200.learned import MLPModel
     X, T, _ = _data(1 << 15, seed=1)
     Xd = torch.as_tensor(X, dtype=torch.float32, device="cuda").contiguous()
     Td = torch.as_tensor(T, dtype=torch.float32, device="cuda").contiguous()
-    m = MLPModel(seed=0, act=act)
+    m = MLPModel(seed=0, act=act, hidden=hidden)
     m.fit_norm(Xd, Td)
     ctx = _capi.Context(16, 16, 16, precision=32)
     idx = torch.arange(4096, dtype=torch.int32, device="cuda")
@@ -106,16 +106,17 @@ def test_training_reduces_loss(act):
     assert np.isfinite(l1) and l1 < 0.1 * l0, (l0, l1)
 
 
-@pytest.mark.parametrize("N,precision,act", [(16, 64, "gelu"), (16, 32, "gelu"), (16, 64, "relu"), (16, 32, "relu"),
-                                             (32, 64, "relu"), (32, 32, "relu"), (32, 32, "gelu")])
-def test_learned_rhs_matches_oracle(N, precision, act):
+@pytest.mark.parametrize("N,precision,act,hidden", [
+    (16, 64, "gelu", 64), (16, 32, "gelu", 64), (16, 64, "relu", 64), (16, 32, "relu", 64), (32, 64, "relu", 64),
+    (32, 32, "relu", 64), (32, 32, "gelu", 64), (16, 32, "relu", 32), (32, 64, "relu", 32), (32, 32, "relu", 32)])
+def test_learned_rhs_matches_oracle(N, precision, act, hidden):
     """16^3 (3N/2 = 24: tiles straddle pencils) and 32^3 (3N/2 = 48: tiles of
     16 z of one pencil, the layout of every 3N/2 divisible by 16)."""
     torch = _torch()
     from pyspectral_b200 import Classes as C
     st = orc.isotropic_state(N, 9, k0=3.0)
     _, _, norm = _data(500, seed=2)
-    m, P = _model(torch, 5, norm, act)
+    m, P = _model(torch, 5, norm, act, hidden)
     grid = C.gridclass.periodic(N)
     main = C.variables(0, "learned", 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 0.01, 0.02, precision=precision,
                        model=m)
@@ -190,7 +191,7 @@ def test_batch_rejects_mixed_activations():
     comps = [torch.zeros_like(s) for s in states]
     for r, m in enumerate((m_relu, m_gelu)):
         p = _capi.make_params(nu=0.01, dt=1e-3, mlp_params=m.params.data_ptr(), mlp_norm=m.norm.data_ptr(),
-                              les_delta=2 * np.pi / N, mlp_act=m.act)
+                              les_delta=2 * np.pi / N, mlp_act=m.act, mlp_hidden=m.hidden)
         if r == 0:
             b.set_run(r, states[r], comps[r], p)
         else:

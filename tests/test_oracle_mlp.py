@@ -6,16 +6,17 @@ import pytest
 from oracle import mlp_oracle as mo
 
 
-@pytest.mark.parametrize("act", ["gelu", "relu"])
-def test_mlp_oracle_gradient_matches_finite_differences(monkeypatch, act):
+@pytest.mark.parametrize("act,hidden", [("gelu", 64), ("relu", 64), ("relu", 32)])
+def test_mlp_oracle_gradient_matches_finite_differences(monkeypatch, act, hidden):
     monkeypatch.setattr(mo, "bf16", lambda x: np.asarray(x, np.float64))
     rng = np.random.default_rng(0)
     X = rng.standard_normal((40, 10))
     T = rng.standard_normal((40, 6))
     norm = np.r_[np.zeros(10), np.ones(10), np.zeros(6), np.ones(6)]
-    P = mo.init_params(1) + 0.01 * rng.standard_normal(mo.NPARAMS)
+    P = mo.init_params(1, hidden) + 0.01 * rng.standard_normal(mo.nparams(hidden))
     _, g = mo.loss_and_grad(P, norm, X, T, act=act)
-    for i in (0, 5, 650, 700, 4800, 5250, mo.NPARAMS - 1):
+    n = mo.nparams(hidden)
+    for i in (0, 5, 10 * hidden + 3, 11 * hidden + 7, n - 7 * hidden, n - 20, n - 1):
         e = np.zeros_like(P)
         e[i] = 1e-6
         fd = (mo.loss_and_grad(P + e, norm, X, T, act=act)[0] - mo.loss_and_grad(P - e, norm, X, T, act=act)[0]) / 2e-6
