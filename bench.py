@@ -16,7 +16,8 @@ the filtered 256^3 DNS, as recorded with the shipped model.
   excluded from the timing; max over ranks; whole-job aggregate.
 * e2e: the same metric through the public API with the state copied from
   pinned host memory before every step and the new state read back after it
-  (copies on a second stream, overlapping the neighbouring steps' compute).
+  (copies on a second stream, overlapping the neighbouring steps' compute;
+  no L2 flush between these steps: each upload replaces the state).
 * roofline: dominant kernel of the step, its compulsory bytes per launch over
   its CUDA-event duration, against MEASURED_PEAKS.json.
 * cpu_baseline: the NumPy oracle port (FP64, scipy.fft with all host cores),
