@@ -309,7 +309,7 @@ struct Batch {
         auto go = [&](auto k) {
           set_smem(k, sm);
           LaunchScope s(c, "batch x-inverse", (double)R * esz * d.N2 * d.Kz * (3.0 * d.N1 + (double)Fi * d.M1));
-          k<<<g, 256, sm, c->stream>>>(ax, pre);
+          launch_pdl(k, g, 256, sm, c->stream, (const AxisArgs<T>*)ax, (const Pre*)pre);
           return launch_ok(c, "batch x-inverse");
         };
         return by_plan(
@@ -329,7 +329,7 @@ struct Batch {
           auto go = [&](auto k) {
             set_smem(k, sm);
             LaunchScope s(c, "batch y-inverse", by);
-            k<<<g, 256, sm, c->stream>>>(ay, ypre);
+            launch_pdl(k, g, 256, sm, c->stream, (const AxisArgs<T>*)ay, (const YPre*)ypre);
             return launch_ok(c, "batch y-inverse");
           };
           return by_plan(
@@ -339,7 +339,7 @@ struct Batch {
         auto go = [&](auto k) {
           set_smem(k, sm);
           LaunchScope s(c, "batch y-forward", by);
-          k<<<g, 256, sm, c->stream>>>(ayf, cpy);
+          launch_pdl(k, g, 256, sm, c->stream, (const AxisArgs<T>*)ayf, (const PreCopy<T>*)cpy);
           return launch_ok(c, "batch y-forward");
         };
         return by_plan(
@@ -354,7 +354,7 @@ struct Batch {
         auto go = [&](auto k) {
           set_smem(k, sm);
           LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fb + Fo));
-          k<<<g, 256, sm, c->stream>>>(az, phys);
+          launch_pdl(k, g, 256, sm, c->stream, (const ZArgs<T>*)az, (const Phys*)phys);
           return launch_ok(c, "batch z-fused");
         };
         if constexpr (phys_fixed_fft<Phys>::value)
@@ -376,7 +376,7 @@ struct Batch {
         auto go = [&](auto k) {
           set_smem(k, sm);
           LaunchScope s(c, "batch x-forward+epilogue", by);
-          k<<<g, 256, sm, c->stream>>>(ae, epi + (size_t)stage * R);
+          launch_pdl(k, g, 256, sm, c->stream, (const XEpiArgs<T>*)ae, (const Epi*)(epi + (size_t)stage * R));
           return launch_ok(c, "batch x-forward+epilogue");
         };
         return by_plan(

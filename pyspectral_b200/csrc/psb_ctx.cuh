@@ -198,6 +198,26 @@ inline void set_smem(K kernel, size_t smem) {
   }
 }
 
+// Launch of a pipeline kernel (axis, z and x-forward passes) with
+// programmatic stream serialisation: it may start while the previous kernel
+// in the stream drains; the kernels wait for their predecessor (pdl_wait)
+// before touching pipeline data.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, int block, size_t smem, cudaStream_t stream,
+                              Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Grid of a persistent kernel: at most (resident CTAs per SM) x SMs of the
 // current device, and no more CTAs than there are tiles.  The kernel asks for
 // the largest shared-memory carveout first: under 48 KB per CTA the default
@@ -278,7 +298,7 @@ int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const
   auto go = [&](auto k) {
     set_smem(k, smem);
     LaunchScope scope(c, what, bytes);
-    k<<<grid, 256, smem, c->stream>>>(a, pre);
+    launch_pdl(k, grid, 256, smem, c->stream, a, pre);
     return launch_ok(c, what);
   };
   if constexpr (TUNABLE) {
@@ -324,7 +344,7 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
     set_smem(k, smem);
     const long long g = persistent_grid(k, smem, grid);
     LaunchScope scope(c, what, bytes);
-    k<<<(unsigned)g, 256, smem, c->stream>>>(z, phys);
+    launch_pdl(k, dim3((unsigned)g), 256, smem, c->stream, z, phys);
     return launch_ok(c, what);
   };
   if constexpr (psb::phys_fixed_fft<Phys>::value) {
@@ -367,7 +387,7 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
   auto go = [&](auto k) {
     set_smem(k, smem);
     LaunchScope scope(c, what, bytes);
-    k<<<e.main_blocks + extra, 256, smem, c->stream>>>(e, epi);
+    launch_pdl(k, dim3((unsigned)(e.main_blocks + extra)), 256, smem, c->stream, e, epi);
     return launch_ok(c, what);
   };
   if constexpr (TUNABLE) {

@@ -29,6 +29,18 @@
 
 namespace psb {
 
+// Programmatic dependent launch (sm_90+): the pipeline's kernels are launched
+// so that the next one may start while this one drains.  Each kernel lets its
+// successor launch as soon as all of its own CTAs are running (pdl_trigger:
+// by then none of them waits for a free SM, so the successor's waiting CTAs
+// cannot starve them), stages what does not depend on its predecessor
+// (twiddles, network weights, shared-memory zero fill), and waits for the
+// predecessor grid to complete and flush its memory (pdl_wait) before the
+// first global read or write of pipeline data.  Both are no-ops in a launch
+// without the attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Spectral row index i -> FFT position j (or -1 when the row is not carried).
 struct RowMap {
   int lo, hi, shift;
@@ -152,6 +164,7 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
   Cx<T>* bufB = bufA + (size_t)L * lines;
   const int o = by;
   const int c0 = bx * ct;
+  pdl_trigger();
   stage_twiddles(tw, a.tw, a.plan);
   const Cx<T> zero = mk<T>(0, 0);
   // A thread keeps one column c of the tile and walks rows with stride nt/ct
@@ -171,6 +184,7 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
     for (int j = t0; j < L; ++j)
       for (int l = threadIdx.x; l < lines; l += nt) bufA[(size_t)j * lines + l] = zero;
   }
+  pdl_wait();
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
   // U rows per round: every load of a round is issued before the first store
   constexpr int U = Pre::F_SRC >= 3 ? 2 : (Pre::F_SRC == 2 ? 4 : 8);
@@ -508,7 +522,9 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
 // One CTA, one tile (the batched kernel's unit).
 template <typename T, class Phys, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, int bx) {
+  pdl_trigger();
   zpass_setup<T, Phys>(a, phys);
+  pdl_wait();
   zpass_tile<T, Phys, WIDE, FP>(a, phys, bx);
 }
 
@@ -518,7 +534,9 @@ __device__ __forceinline__ void zpass_body(const ZArgs<T>& a, const Phys& phys, 
 // FP: compiled-in transform schedule (FixedPlan id) equal to a.plan, or 0.
 template <typename T, class Phys, bool WIDE = false, int FP = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_kernel(ZArgs<T> a, Phys phys) {
+  pdl_trigger();
   zpass_setup<T, Phys>(a, phys);
+  pdl_wait();
   const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
   for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
     zpass_tile<T, Phys, WIDE, FP>(a, phys, (int)bx);
@@ -567,7 +585,9 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
   constexpr int F = Epi::F_IN;
   Cx<T> P[F];
   const Cx<T> zero = mk<T>(0, 0);
+  pdl_trigger();
   if (bx >= a.main_blocks) {
+    pdl_wait();
     // columns kz..n3h-1 carry no products
     const int ncz = a.n3h - a.kz;
     const long long tot = (long long)a.n1 * a.n2 * ncz;
@@ -593,6 +613,7 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
   const int o = bx / ntile;
   const int c0 = (bx % ntile) * ct;
   stage_twiddles(tw, a.tw, a.plan);
+  pdl_wait();
   const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
   // one column c per thread, rows walked with stride nt/ct (as in the axis pass)
   const int nt = blockDim.x;
