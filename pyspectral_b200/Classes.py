@@ -82,14 +82,21 @@ class gridclass:
             self._ctx[precision] = c
         return c
 
+    def numpy_k(self):
+        """The reference's (N1, N2, N3/2+1) wavenumber arrays k1, k2, k3 as NumPy
+        (src/Classes.py:565-570: fftshifted index ranges times 2 pi / L)."""
+        N1, N2, N3 = self.N1, self.N2, self.N3
+        k1 = np.fft.fftshift(np.linspace(-(N1 // 2), N1 // 2 - 1, N1)) * 2.0 * np.pi / self.L1
+        k2 = np.fft.fftshift(np.linspace(-(N2 // 2), N2 // 2 - 1, N2)) * 2.0 * np.pi / self.L2
+        k3 = np.linspace(0, N3 // 2, N3 // 2 + 1) * 2.0 * np.pi / self.L3
+        K2, K1, K3 = np.meshgrid(k2, k1, k3)
+        return K1, K2, K3
+
     def _tables(self):
         if self._tabs is None:
-            N1, N2, N3 = self.N1, self.N2, self.N3
-            k1 = np.fft.fftshift(np.linspace(-(N1 // 2), N1 // 2 - 1, N1)) * 2.0 * np.pi / self.L1
-            k2 = np.fft.fftshift(np.linspace(-(N2 // 2), N2 // 2 - 1, N2)) * 2.0 * np.pi / self.L2
-            k3 = np.linspace(0, N3 // 2, N3 // 2 + 1) * 2.0 * np.pi / self.L3
+            N1, N2 = self.N1, self.N2
             dev = torch.device("cuda", self.device)
-            K2, K1, K3 = np.meshgrid(k2, k1, k3)
+            K1, K2, K3 = self.numpy_k()
             self._tabs = {n: torch.as_tensor(a, device=dev) for n, a in
                           (("k1", K1), ("k2", K2), ("k3", K3))}
             ks = K1 * K1 + K2 * K2 + K3 * K3 + 1.0e-50
