@@ -145,6 +145,13 @@ int psb_cross_helicity(psb_ctx* ctx, const void* u3, const void* b3, int flags, 
  * (psb_spectrum_nbins). */
 int psb_spectrum(psb_ctx* ctx, const void* fields3, int flags, double* out, int nbins);
 int psb_spectrum_nbins(const psb_ctx* ctx, int flags, int* nbins);
+/* computeTransfer (src/Classes.py:988-1040): energy transfer spectrum of the
+ * 3 fields (Nyquist modes treated as zero, 3/2-dealiased products), binned
+ * like psb_spectrum; out[2*nbins] = (Re, Im) per bin, nbins from
+ * psb_spectrum_nbins(ctx, 0, &nbins).  flags PSB_FILTER_GF:
+ * computeTransfer_resolved (:1093-1150, the fields filtered by Gf).  w0 (3
+ * fields) non-NULL: computeTransfer_SGS (:1206-1239), Re sum_i conj(Gf u_i) w0_i. */
+int psb_transfer(psb_ctx* ctx, const void* fields3, const void* w0, int flags, double* out, int nbins);
 /* MPI computeSpectrum / computeMHDSpectrum (src_MPI/Classes.py:370-448):
  * out[nbins] summed over components, int16 shells, k3=N/2 included. */
 int psb_spectrum_mpi(psb_ctx* ctx, const void* fields3, double* out, int nbins);

@@ -272,6 +272,35 @@ class utilitiesClass:
         kmax = spec.shape[0] - 1
         return np.linspace(0, kmax, kmax + 1), spec
 
+    def computeTransfer(self, main, grid, myFFT=None):
+        """``computeTransfer`` (src/Classes.py:988-1040): ``(kdata, Transfer)``
+        with Transfer complex like the reference's.  As there, the velocity
+        views main.uhat/vhat/what lose their Nyquist modes (the reference
+        rebinds them to ``unpad(pad(.))``); the state main.Q is untouched."""
+        N1, N2, N3 = grid.N1, grid.N2, grid.N3
+        main.U[:, N1 // 2, :, :] = 0
+        main.U[:, :, N2 // 2, :] = 0
+        main.U[:, :, :, N3 // 2] = 0
+        tr = grid.ctx(main.precision).transfer(main.U)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
+    def computeTransfer_resolved(self, main, grid, myFFT=None):
+        """``computeTransfer_resolved`` (src/Classes.py:1093-1150): the transfer
+        spectrum of the Gf-filtered velocity (no side effect)."""
+        tr = grid.ctx(main.precision).transfer(main.U, flags=_capi.FILTER_GF)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
+    def computeTransfer_SGS(self, main, grid, myFFT=None):
+        """``computeTransfer_SGS`` (src/Classes.py:1206-1239): Re of
+        conj(Gf u_i) w0_i per shell, w0 the closure force of the last RHS."""
+        if main.W0 is None:
+            raise ValueError("computeTransfer_SGS needs a closure that keeps w0 (turb_model != 0)")
+        tr = grid.ctx(main.precision).transfer(main.U, w0=main.W0)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
     def computeSpectrum_resolved(self, main, grid):
         spec = self._spectrum(main, grid, _capi.FILTER_GF)
         N1, N2, N3 = grid.N1, grid.N2, grid.N3

@@ -22,7 +22,7 @@ NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
 EXPORTS = (
     "psb_ctx_create", "psb_ctx_destroy", "psb_ctx_set_stream", "psb_last_error", "psb_create_error",
     "psb_rhs", "psb_step_rk4", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
-    "psb_spectrum", "psb_spectrum_nbins", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
+    "psb_spectrum", "psb_spectrum_nbins", "psb_transfer", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
     "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
     "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
     "psb_mlp_forward_tc",
@@ -76,6 +76,7 @@ def load(path: str = LIB_PATH):
         "psb_spectrum": ([vp, vp, i, dp, i], i),
         "psb_spectrum_nbins": ([vp, i, ip], i),
         "psb_spectrum_mpi": ([vp, vp, dp, i], i),
+        "psb_transfer": ([vp, vp, vp, i, dp, i], i),
         "psb_cfl_dt": ([vp, vp, d, d, dp], i),
         "psb_sgs_dns": ([vp, vp, vp, vp], i),
         "psb_fft_r2c": ([vp, vp, vp, i], i),
@@ -213,6 +214,19 @@ class Context:
                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nb.value),
                    "psb_spectrum")
         return out
+
+    def transfer(self, f3, w0=None, flags=0):
+        """Complex transfer spectrum (kmax+1 bins) of the 3 fields f3; flags
+        FILTER_GF: of the Gf-filtered fields; w0: the SGS transfer with w0."""
+        import numpy as np
+        self.bind_stream()
+        nb = ctypes.c_int()
+        self.check(self.lib.psb_spectrum_nbins(self.h, 0, ctypes.byref(nb)), "psb_spectrum_nbins")
+        out = np.zeros((nb.value, 2), dtype=np.float64)
+        self.check(self.lib.psb_transfer(self.h, self._ptr(f3), self._ptr(w0), int(flags),
+                                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nb.value),
+                   "psb_transfer")
+        return out[:, 0] + 1j * out[:, 1]
 
     def spectrum_mpi(self, f3):
         import numpy as np

@@ -18,6 +18,8 @@ template <typename T>
 int sgs_dns_run(psb_ctx* c, const void* fields, void* w0, void* tau6);
 template <typename T>
 int products_run(psb_ctx* c, const void* fields, void* out6);
+template <typename T>
+int products_filtered_run(psb_ctx* c, const void* fields, void* out6);
 }  // namespace psbh
 
 namespace {
@@ -169,6 +171,82 @@ __global__ void __launch_bounds__(256) spectrum_kernel(const Cx<T>* __restrict__
       const Cx<T> u = a[f * fs + s];
       atomicAdd(&spec[bin * 3 + f], w * g * g * ((double)u.x * u.x + (double)u.y * u.y));
     }
+  }
+}
+
+// energy transfer spectra (PySpectral/src/Classes.py:988-1239), binned like
+// spectrum_kernel, Nyquist modes of the state zeroed (they contribute
+// nothing); spec[2 bin] += Re, spec[2 bin + 1] += Im.
+//  mode 0 (computeTransfer): sum_i conj(u_i) (-i k_j P_ij - i k_i p), P the
+//    3/2-dealiased products, p = ksqr_i (-k_i k_j P_ij);
+//  mode 1 (computeTransfer_resolved): the same with u -> Gf u (P of Gf u);
+//  mode 2 (computeTransfer_SGS): Re sum_i conj(Gf u_i) W_i (W = w0).
+template <typename T>
+__global__ void __launch_bounds__(256) transfer_kernel(const Cx<T>* __restrict__ a, const Cx<T>* __restrict__ P,
+                                                       int mode, const double* __restrict__ gx,
+                                                       const double* __restrict__ gy, const double* __restrict__ gz,
+                                                       const double* __restrict__ kx, const double* __restrict__ ky,
+                                                       const double* __restrict__ kz, int N1, int N2, int N3,
+                                                       int nbins, double* __restrict__ spec) {
+  const int n3h = N3 / 2 + 1;
+  const long long npts = (long long)N1 * N2 * n3h, fs = npts;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % n3h);
+    if (i3 >= N3 / 2 && i3 != 0) continue;
+    const long long t = s / n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    if (i1 == N1 / 2 || i2 == N2 / 2) continue;
+    const long long n1 = i1 < N1 / 2 ? i1 : i1 - N1, n2 = i2 < N2 / 2 ? i2 : i2 - N2, n3 = i3;
+    int bin = (int)(signed char)(long long)rint(sqrt((double)(n1 * n1 + n2 * n2 + n3 * n3)));
+    if (bin < 0) bin += nbins;
+    if (bin < 0 || bin >= nbins) continue;
+    const double gf = mode ? gx[i1] * gy[i2] * gz[i3] : 1.0;
+    if (mode == 2) {
+      double re = 0.0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        const Cx<T> u = a[i * fs + s], q = P[i * fs + s];
+        re += gf * ((double)u.x * q.x + (double)u.y * q.y);
+      }
+      atomicAdd(&spec[2 * bin], (i3 == 0 ? 1.0 : 2.0) * re);
+      continue;
+    }
+    const double k[3] = {kx[i1], ky[i2], kz[i3]};
+    double pr[6][2];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      const Cx<T> v = P[m * fs + s];
+      pr[m][0] = v.x;
+      pr[m][1] = v.y;
+    }
+    // P order 11, 22, 33, 12, 13, 23
+    const int idx[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+    const double ksi = 1.0 / (k[0] * k[0] + k[1] * k[1] + k[2] * k[2] + 1.0e-50);
+    double ph[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+      ph[c] = ksi * (-k[0] * k[0] * pr[0][c] - k[1] * k[1] * pr[1][c] - k[2] * k[2] * pr[2][c] -
+                     2.0 * k[0] * k[1] * pr[3][c] - 2.0 * k[0] * k[2] * pr[4][c] - 2.0 * k[1] * k[2] * pr[5][c]);
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      // z = k_j P_ij + k_i p; the advection term is -i z = (z.y, -z.x)
+      double zx = k[i] * ph[0], zy = k[i] * ph[1];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        zx += k[j] * pr[idx[i][j]][0];
+        zy += k[j] * pr[idx[i][j]][1];
+      }
+      const Cx<T> u = a[i * fs + s];
+      const double ux = gf * u.x, uy = gf * u.y;
+      const double ax = zy, ay = -zx;
+      re += ux * ax + uy * ay;  // conj(u) * (-i z)
+      im += ux * ay - uy * ax;
+    }
+    const double w = i3 == 0 ? 1.0 : 2.0;
+    atomicAdd(&spec[2 * bin], w * re);
+    atomicAdd(&spec[2 * bin + 1], w * im);
   }
 }
 
@@ -797,6 +875,51 @@ int psb_spectrum(psb_ctx* c, const void* f, int flags, double* out, int nbins) {
   PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "spectrum sync"));
   const double nnn = (double)c->N1 * c->N2 * c->N3;
   for (int i = 0; i < 3 * nbins; ++i) out[i] = c->red_host[i] / nnn;
+  return PSB_OK;
+}
+
+int psb_transfer(psb_ctx* c, const void* f, const void* w0, int flags, double* out, int nbins) {
+  PSB_TRY(check_ctx(c));
+  if (!f || !out || nbins <= 0) return fail(c, PSB_ERR_ARG, "psb_transfer: bad argument");
+  PSB_TRY(set_device(c));
+  const int mode = w0 ? 2 : ((flags & PSB_FILTER_GF) ? 1 : 0);
+  const void* Pp = w0;
+  if (mode < 2) {
+    const size_t esz = c->prec == 64 ? 16 : 8;
+    const size_t nP = (size_t)6 * c->N1 * c->N2 * c->N3h;
+    auto& buf = c->scratch["transfer.P"];
+    if (buf.bytes < nP * esz) {
+      if (buf.p) cudaFree(buf.p);
+      buf.p = nullptr;
+      buf.bytes = 0;
+      PSB_TRY(cuda_ok(c, cudaMalloc(&buf.p, nP * esz), "transfer scratch"));
+      buf.bytes = nP * esz;
+    }
+    if (mode == 0)
+      PSB_TRY(c->prec == 64 ? products_run<double>(c, f, buf.p) : products_run<float>(c, f, buf.p));
+    else
+      PSB_TRY(c->prec == 64 ? products_filtered_run<double>(c, f, buf.p)
+                            : products_filtered_run<float>(c, f, buf.p));
+    Pp = buf.p;
+  }
+  PSB_TRY(ensure_red(c, (size_t)2 * nbins));
+  PSB_TRY(cuda_ok(c, cudaMemsetAsync(c->red_dev, 0, sizeof(double) * 2 * nbins, c->stream), "memset"));
+  ++c->launches;
+  if (c->prec == 64)
+    transfer_kernel<double><<<kRedBlocks, 256, 0, c->stream>>>(
+        reinterpret_cast<const Cx<double>*>(f), reinterpret_cast<const Cx<double>*>(Pp), mode, c->gx, c->gy, c->gz,
+        c->kx, c->ky, c->kz, c->N1, c->N2, c->N3, nbins, c->red_dev);
+  else
+    transfer_kernel<float><<<kRedBlocks, 256, 0, c->stream>>>(
+        reinterpret_cast<const Cx<float>*>(f), reinterpret_cast<const Cx<float>*>(Pp), mode, c->gx, c->gy, c->gz,
+        c->kx, c->ky, c->kz, c->N1, c->N2, c->N3, nbins, c->red_dev);
+  PSB_TRY(launch_ok(c, "transfer"));
+  PSB_TRY(cuda_ok(c, cudaMemcpyAsync(c->red_host, c->red_dev, sizeof(double) * 2 * nbins, cudaMemcpyDeviceToHost,
+                                     c->stream),
+                  "transfer copy"));
+  PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "transfer sync"));
+  const double nnn = (double)c->N1 * c->N2 * c->N3;
+  for (int i = 0; i < 2 * nbins; ++i) out[i] = c->red_host[i] / nnn;
   return PSB_OK;
 }
 

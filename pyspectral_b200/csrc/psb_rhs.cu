@@ -1045,6 +1045,16 @@ int products_run(psb_ctx* c, const void* fields, void* out6) {
 template int products_run<double>(psb_ctx*, const void*, void*);
 template int products_run<float>(psb_ctx*, const void*, void*);
 
+// the six products of Gf u (the sharp-cutoff filtered field; transfer of the resolved scales)
+template <typename T>
+int products_filtered_run(psb_ctx* c, const void* fields, void* out6) {
+  EpiProducts<T> epi{reinterpret_cast<Cx<T>*>(out6), (long long)c->N1 * c->N2 * c->N3h, c->N2, c->N3h};
+  return run_ns32<T>(c, reinterpret_cast<const Cx<T>*>(fields), PreMask3<T>{c->gx, c->gy, c->gz},
+                     PhysProducts<T>{}, epi);
+}
+template int products_filtered_run<double>(psb_ctx*, const void*, void*);
+template int products_filtered_run<float>(psb_ctx*, const void*, void*);
+
 // exported for the dynamic tau-model translation unit
 template <typename T>
 int mem_stage_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const char* tag, const double* filt, int kfp,

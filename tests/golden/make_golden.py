@@ -265,6 +265,22 @@ def gen_serial(N, seed):
     grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, cfl=0.4)
     util.compute_dt(main, grid)
     out["cfl_dt"] = np.float64(main.dt)
+    # energy transfer spectrum (src/Classes.py:988-1040) on the input state
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t)
+    k, tr = util.computeTransfer(main, grid, myFFT)
+    out["transfer_k"], out["transfer"] = np.asarray(k), np.asarray(tr)
+    # resolved transfer (:1093-1150) with kc = N/4, and the SGS transfer
+    # (:1206-1239) of the Smagorinsky closure force w0 after one RHS
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, kc=N // 4)
+    k, tr = util.computeTransfer_resolved(main, grid, myFFT)
+    out["transfer_res"] = np.asarray(tr)
+    grid, myFFT, util, main = serial_case(C, N, st, 1, nu, dt, t, kc=N // 4)
+    with contextlib.redirect_stdout(io.StringIO()):
+        main.computeRHS(main, grid, myFFT, util)
+    out["transfer_sgs_u"] = np.stack([main.uhat, main.vhat, main.what])
+    out["transfer_sgs_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
+    k, tr = util.computeTransfer_SGS(main, grid, myFFT)
+    out["transfer_sgs"] = np.asarray(tr)
     return out
 
 
