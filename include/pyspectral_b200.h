@@ -40,6 +40,9 @@ extern "C" {
 #define PSB_MHD_TMODEL 7  /* MHD + t-model memory term Ct t PLQL on both fields (no reference
                              counterpart; the construction of src/RHSfunctions.py:240-363 applied
                              to src_MPI/RHSfunctions.py:95-175, resolved set = 2/3-rule set)      */
+#define PSB_DSMAG 8       /* turb_model 7      -> computeRHS_DSMAG  (src/RHSfunctions.py:1663-1862):
+                             Smagorinsky with Cs^2 = <L:M>/<M:M> from the test filter
+                             myFilter(., kc/2) (src/Classes.py:1271-1279)                          */
 
 /* ---- diagnostic flags --------------------------------------------------- */
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
@@ -101,7 +104,8 @@ const char* psb_create_error(void);
  * read_out : optional copy of the state as the RHS read it (the reference
  *            rebinds main.uhat/vhat/what to it, src/RHSfunctions.py:10-12;
  *            the MPI solver dealiases it in place, src_MPI/RHSfunctions.py:102-107).
- * tau_out  : optional host scalar main.tau (tau-models; src/RHSfunctions.py:480,857). */
+ * tau_out  : optional host scalar main.tau (tau-models; src/RHSfunctions.py:480,857);
+ *            for PSB_DSMAG the dynamic coefficient Cs_sqr (:1843). */
 int psb_rhs(psb_ctx* ctx, int closure, const void* state, void* rhs, void* w0, void* read_out,
             const psb_params* p, double* tau_out);
 

@@ -338,6 +338,91 @@ def rhs_smag(g, state, p):
     return np.stack(r), w0
 
 
+def myfilter_axes(g, kc):
+    """Index masks of ``utilitiesClass.myFilter(uhat, kc)`` (``src/Classes.py:1271-1279``):
+    rows ``[0:kc]`` and ``[-kc+1:]`` of axes 1 and 2, ``[0:kc]`` of axis 3,
+    with Python slice semantics (so ``kc = 1`` keeps whole rows, since
+    ``-kc+1 = 0``).  A fractional ``kc`` is truncated, as the NumPy the
+    reference was written for did with float slice bounds."""
+    kc = int(kc)
+
+    def rows(n):
+        m = np.zeros(n)
+        m[0:kc] = 1.0
+        m[-kc + 1:] = 1.0
+        return m
+    m3 = np.zeros(g.N3 // 2 + 1)
+    m3[0:kc] = 1.0
+    return rows(g.N1), rows(g.N2), m3
+
+
+def myfilter(g, uhat, kc):
+    m1, m2, m3 = myfilter_axes(g, kc)
+    return uhat * (m1[:, None, None] * m2[None, :, None] * m3[None, None, :])
+
+
+def dsmag_cs2(g, u, v, w, return_parts=False):
+    """The dynamic coefficient ``Cs_sqr = mean(L:M)/mean(M:M)`` of
+    ``computeRHS_DSMAG`` (``src/RHSfunctions.py:1693-1843``): Leonard stress
+    ``L = F(u_i u_j) - (F u_i F u_j)``, ``M = -2 Delta^2 (alpha^2 |S~|S~ - F(|S|S))``
+    with the test filter ``F = myFilter(., kc/alpha)``, ``alpha = 2``; both
+    means taken on the 3/2-padded physical grid, off-diagonal terms weighted 1
+    as written at ``:1838-1841``."""
+    alpha = 2.0
+    kL = g.kc / alpha
+    s = scale_32(g)
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    P = _products_32(g, u, v, w)
+    uF, vF, wF = (myfilter(g, x, kL) for x in (u, v, w))
+    PF = _products_32(g, uF, vF, wF)
+    L = [myfilter(g, P[i], kL) - PF[i] for i in range(6)]
+
+    def strain(a, b, c):
+        Sh = (1j * k1 * a, 1j * k2 * b, 1j * k3 * c, 0.5 * (1j * k2 * a + 1j * k1 * b),
+              0.5 * (1j * k3 * a + 1j * k1 * c), 0.5 * (1j * k3 * b + 1j * k2 * c))
+        S = [ifft32(g, pad(x) * s) for x in Sh]
+        S11, S22, S33, S12, S13, S23 = S
+        mag = np.sqrt(2.0 * (S11 * S11 + S22 * S22 + S33 * S33 + 2.0 * S12 * S12 + 2.0 * S13 * S13
+                             + 2.0 * S23 * S23))
+        return S, mag
+    S, Smag = strain(u, v, w)
+    SF, SmagF = strain(uF, vF, wF)
+    SFS = [unpad(fft32(SmagF * x)) for x in SF]
+    SSF = [myfilter(g, unpad(fft32(Smag * x)), kL) for x in S]
+    M = [-2.0 * g.Delta ** 2 * (alpha ** 2 * SFS[i] - SSF[i]) for i in range(6)]
+    Mr = [ifft32(g, pad(x)) * s for x in M]
+    Lr = [ifft32(g, pad(x)) * s for x in L]
+    num = sum(Mr[i] * Lr[i] for i in range(6))
+    den = sum(Mr[i] * Mr[i] for i in range(6))
+    cs2 = np.mean(num) / np.mean(den)
+    if return_parts:
+        return cs2, P, S, Smag
+    return cs2
+
+
+def rhs_dsmag(g, state, p):
+    """Dynamic Smagorinsky right-hand side, ``computeRHS_DSMAG``
+    (``src/RHSfunctions.py:1663-1862``): the Smagorinsky form of ``:146-237``
+    with ``Cs^2`` from :func:`dsmag_cs2` in place of ``0.16^2``.
+
+    Returns ``(rhs, w0, cs2)``."""
+    u, v, w = state[0], state[1], state[2]
+    cs2, P, S, Smag = dsmag_cs2(g, u, v, w, return_parts=True)
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    phat = _pressure(k1, k2, k3, g.ksqr_i, *P)
+    if p.rotate == 1:
+        phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, u, v, w, p.Om)
+    nut = cs2 * g.Delta * g.Delta * np.abs(Smag)
+    tau = [unpad(fft32(-2.0 * nut * x)) for x in S]
+    w0 = _sgs_divergence(g, tau)
+    r = list(_advection(k1, k2, k3, p.nu, g.ksqr, phat, P, u, v, w))
+    r = [r[i] + w0[i] for i in range(3)]
+    if p.rotate == 1:
+        c = _coriolis_force(u, v, w, p.Om)
+        r = [r[i] + c[i] for i in range(3)]
+    return np.stack(r), w0, cs2
+
+
 def _pl_2x(g, up, vp, wp, nu, rotate, Om):
     """``PLu`` on the 2x grid (``src/RHSfunctions.py:269-315``): returns the
     full-grid PL fields, the physical velocities and the 2x product spectra."""

@@ -135,7 +135,7 @@ class variables:
     (src/Classes.py:7-229).
 
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
-    'Dynamic tau-model'.  ``precision`` (64 or 32) selects FP64 or FP32
+    'Dynamic tau-model', 7 (dynamic Smagorinsky).  ``precision`` (64 or 32) selects FP64 or FP32
     fields; FP32 runs carry a Kahan compensation array ``comp``."""
 
     def __init__(self, weave, turb_model, rotate, Om1, Om2, Om3, grid, uhat, vhat, what, t, dt, nu, Ct=-10,
@@ -161,13 +161,14 @@ class variables:
         self.Ct = 0.1 if Ct == -10 else float(Ct)
         self.tau_a, self.tau_b = float(dt0), float(dt1)
         self.tau = 0.0
+        self.Cs_sqr = 0.0  # dynamic Smagorinsky coefficient of the last RHS (turb_model 7)
         self.kf = None
         use_kahan = (precision == 32) if kahan is None else bool(kahan)
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
-                 "learned": R.computeRHS_learned}
+                 7: R.computeRHS_DSMAG, "learned": R.computeRHS_learned}
         if turb_model not in table:
             raise ValueError(f"turb_model {turb_model!r} is not on this path")
         self.computeRHS = table[turb_model]
@@ -227,7 +228,7 @@ class variables:
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, "learned": _capi.LEARNED}[self.turb_model]
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 7: _capi.DSMAG, "learned": _capi.LEARNED}[self.turb_model]
 
 
 class utilitiesClass:

@@ -47,6 +47,14 @@ def computeRHS_Dtaumodel(main, grid, myFFT=None, utilities=None):
     main.tau = _rhs(main, grid, _capi.TAU_DYNAMIC)
 
 
+def computeRHS_DSMAG(main, grid, myFFT=None, utilities=None):
+    """Dynamic Smagorinsky (turb_model 7), src/RHSfunctions.py:1663-1862:
+    ``Cs^2 = <L:M>/<M:M>`` with the test filter ``myFilter(., kc/2)``, then the
+    Smagorinsky stress with that coefficient.  The coefficient, a local of the
+    reference, is kept as ``main.Cs_sqr``."""
+    main.Cs_sqr = _rhs(main, grid, _capi.DSMAG)
+
+
 def computeRHS_learned(main, grid, myFFT=None, utilities=None):
     """LES with the learned MLP subgrid stress (no reference counterpart;
     takes the place of the Smagorinsky stress of src/RHSfunctions.py:195-212).

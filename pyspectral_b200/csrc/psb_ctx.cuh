@@ -41,6 +41,7 @@ struct psb_ctx {
   double *gx = nullptr, *gy = nullptr, *gz = nullptr;
   int kz_mhd = 0;  // retained k3 count of the 2/3 rule
   int dtau_kf = -1;  // test-filter wavenumber of the cached dynamic-tau masks
+  int dsmag_kl = -1;  // test-filter cutoff of the cached dynamic-Smagorinsky masks
   void* tw_d = nullptr;  // Cx<double> pool
   void* tw_f = nullptr;  // Cx<float> pool
   std::map<int, psb::FFTPlan> plans;

@@ -739,6 +739,226 @@ int run_mhd_tmodel(psb_ctx* c, StepIO<T> io, const psb_params* p) {
   return launch_epi<T>(c, e3, et, "mhd-t PLQL x-forward+epilogue");
 }
 
+// ---------------------------------------------------------------------------
+// Dynamic Smagorinsky (PySpectral/src/RHSfunctions.py:1663-1862)
+//
+// Two pipeline passes store, for u and for the test-filtered u~, the six
+// dealiased products and the six |S| S_ij spectra (PhysSmag with
+// (Cs Delta)^2 = -1/2 gives |S| S_ij exactly).  One FP64 reduction forms
+// L = F(uu) - (u~u~), M = -2 Delta^2 (alpha^2 |S~|S~ - F(|S|S)) point by point
+// and Cs^2 = <L:M>/<M:M>; the reference takes both means on the 3/2 grid
+// after pad(), which by Parseval is the spectral sum over the modes pad()
+// keeps (k3 > 0 twice; the k3 = 0 plane as c2r reads it, i.e. its Hermitian
+// part).  The Smagorinsky epilogue then runs on the stored u spectra with
+// tau = -2 Cs^2 Delta^2 (|S| S)^ read from the device: no host round trip.
+// ---------------------------------------------------------------------------
+template <typename T, int F>
+struct EpiStore {
+  static constexpr int F_IN = F;
+  Cx<T>* out;
+  long long fstride;
+  int n2, n3h;
+  __host__ double io_bytes(long long npts) const { return (double)sizeof(Cx<T>) * npts * F; }
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = ((long long)i1 * n2 + i2) * n3h + i3;
+#pragma unroll
+    for (int m = 0; m < F; ++m) out[m * fstride + s] = P[m];
+  }
+};
+
+// myFilter(uhat, kL) (src/Classes.py:1271-1279) on load, then the strain of PreStrain
+template <typename T>
+struct PreStrainFiltered {
+  static constexpr int F_SRC = 3, F_DST = 9;
+  const double *g1, *g2, *g3;
+  __device__ void operator()(int i, int o, int cc, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
+    const T g = (T)(g1[i] * g2[o] * g3[cc]);
+    const Cx<T> f[3] = {g * s[0], g * s[1], g * s[2]};
+    PreStrain<T>{}(i, o, cc, a, f, d);
+  }
+};
+
+constexpr int kLmBlocks = 296;
+
+template <typename T>
+__device__ __forceinline__ void dsmag_lm(const Cx<T>* __restrict__ A, const Cx<T>* __restrict__ B, long long fs,
+                                         long long s, double g, double d2, double* Lr, double* Li, double* Mr,
+                                         double* Mi) {
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    const Cx<T> a = A[m * fs + s], b = B[m * fs + s];
+    const Cx<T> sa = A[(6 + m) * fs + s], sb = B[(6 + m) * fs + s];
+    Lr[m] = g * (double)a.x - (double)b.x;
+    Li[m] = g * (double)a.y - (double)b.y;
+    Mr[m] = d2 * (4.0 * (double)sb.x - g * (double)sa.x);  // alpha^2 = 4
+    Mi[m] = d2 * (4.0 * (double)sb.y - g * (double)sa.y);
+  }
+}
+
+// per-block partial sums of <L:M> and <M:M> (src/RHSfunctions.py:1838-1842)
+template <typename T>
+__global__ void __launch_bounds__(256) dsmag_lm_kernel(const Cx<T>* __restrict__ A, const Cx<T>* __restrict__ B,
+                                                       const double* __restrict__ g, int N1, int N2, int N3,
+                                                       int n3h, double d2, double* __restrict__ part) {
+  const long long fs = (long long)N1 * N2 * n3h;
+  const double *g1 = g, *g2 = g + N1, *g3 = g + N1 + N2;
+  double num = 0.0, den = 0.0;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % n3h);
+    const long long t = s / n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    if (i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2) continue;  // modes pad() drops
+    double Lr[6], Li[6], Mr[6], Mi[6];
+    dsmag_lm<T>(A, B, fs, s, g1[i1] * g2[i2] * g3[i3], d2, Lr, Li, Mr, Mi);
+    if (i3 > 0) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        num += 2.0 * (Lr[m] * Mr[m] + Li[m] * Mi[m]);
+        den += 2.0 * (Mr[m] * Mr[m] + Mi[m] * Mi[m]);
+      }
+    } else {
+      // Hermitian part of the k3 = 0 plane: 1/2 Re(L M*) + 1/2 Re(L(k) M(-k))
+      const int j1 = (N1 - i1) % N1, j2 = (N2 - i2) % N2;
+      const long long sp = ((long long)j1 * N2 + j2) * n3h;
+      double pLr[6], pLi[6], pMr[6], pMi[6];
+      dsmag_lm<T>(A, B, fs, sp, g1[j1] * g2[j2] * g3[0], d2, pLr, pLi, pMr, pMi);
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        num += 0.5 * (Lr[m] * Mr[m] + Li[m] * Mi[m]) + 0.5 * (Lr[m] * pMr[m] - Li[m] * pMi[m]);
+        den += 0.5 * (Mr[m] * Mr[m] + Mi[m] * Mi[m]) + 0.5 * (Mr[m] * pMr[m] - Mi[m] * pMi[m]);
+      }
+    }
+  }
+  __shared__ double red[2][256];
+  red[0][threadIdx.x] = num;
+  red[1][threadIdx.x] = den;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + h];
+      red[1][threadIdx.x] += red[1][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    part[2 * blockIdx.x] = red[0][0];
+    part[2 * blockIdx.x + 1] = red[1][0];
+  }
+}
+
+// out[0] = Cs^2 = num/den (IEEE: 0/0 -> NaN, as the reference's np.mean ratio), out[1..2] = num, den
+__global__ void __launch_bounds__(256) dsmag_cs2_kernel(const double* __restrict__ part, int nblk,
+                                                        double* __restrict__ out) {
+  __shared__ double red[2][256];
+  double num = 0.0, den = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    num += part[2 * b];
+    den += part[2 * b + 1];
+  }
+  red[0][threadIdx.x] = num;
+  red[1][threadIdx.x] = den;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if ((int)threadIdx.x < h) {
+      red[0][threadIdx.x] += red[0][threadIdx.x + h];
+      red[1][threadIdx.x] += red[1][threadIdx.x + h];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = red[0][0] / red[1][0];
+    out[1] = red[0][0];
+    out[2] = red[1][0];
+  }
+}
+
+// the Smagorinsky epilogue on the stored u spectra, tau scaled by -2 Cs^2 Delta^2
+template <typename T>
+__global__ void __launch_bounds__(256) dsmag_epi_kernel(EpiNS<T, true> epi, const Cx<T>* __restrict__ A, int N1,
+                                                        int N2, int n3h, const double* __restrict__ cs2,
+                                                        double delta) {
+  const long long fs = (long long)N1 * N2 * n3h;
+  const T f = (T)(-2.0 * (cs2[0] * delta * delta));
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % n3h);
+    const long long t = s / n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    Cx<T> P[12];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) P[m] = A[m * fs + s];
+#pragma unroll
+    for (int m = 6; m < 12; ++m) P[m] = f * A[m * fs + s];
+    epi(i1, i2, i3, P);
+  }
+}
+
+// myFilter's kept rows (src/Classes.py:1271-1279) with Python slice bounds:
+// [0:kc] and [-kc+1:] on axes 1 and 2, [0:kc] on axis 3
+inline void myfilter_rows(int n, int kc, bool two_sided, double* out) {
+  for (int i = 0; i < n; ++i) out[i] = 0.0;
+  for (int i = 0; i < std::min(kc, n); ++i) out[i] = 1.0;
+  if (!two_sided) return;
+  int lo = 1 - kc;
+  if (lo < 0) lo += n;
+  lo = std::max(0, std::min(lo, n));
+  for (int i = lo; i < n; ++i) out[i] = 1.0;
+}
+
+template <typename T>
+int dsmag_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p, const psb_tuned* ts, double* cs2_out) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "dsmag.A", (size_t)12 * fs, &st);
+  Cx<T>* B = scratch<T>(c, "dsmag.B", (size_t)12 * fs, &st);
+  double* g = reinterpret_cast<double*>(scratch<double>(c, "dsmag.g", (size_t)(N1 + N2 + N3h), &st));
+  double* part = reinterpret_cast<double*>(scratch<double>(c, "dsmag.part", kLmBlocks, &st));
+  double* cs2 = reinterpret_cast<double*>(scratch<double>(c, "dsmag.cs2", 2, &st));
+  if (st != PSB_OK) return st;
+  // test filter kL = kc/alpha, alpha = 2 (:1695-1697); a fractional kL is truncated
+  const int kl = (int)(c->kc / 2.0);
+  if (c->dsmag_kl != kl) {
+    std::vector<double> h(N1 + N2 + N3h);
+    myfilter_rows(N1, kl, true, h.data());
+    myfilter_rows(N2, kl, true, h.data() + N1);
+    myfilter_rows(N3h, kl, false, h.data() + N1 + N2);
+    PSB_TRY(cuda_ok(c, cudaMemcpy(g, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "filter upload"));
+    c->dsmag_kl = kl;
+  }
+  const Cx<T>* Qin = io.Q;
+  EpiStore<T, 12> sa{A, fs, N2, N3h}, sb{B, fs, N2, N3h};
+  const PhysSmag<T> ss{(T)-0.5};  // -2 (-1/2) |S| S_ij = |S| S_ij
+  PSB_TRY(run_ns32<T>(c, Qin, PreStrain<T>{}, ss, sa, ts));
+  PSB_TRY(run_ns32<T>(c, Qin, PreStrainFiltered<T>{g, g + N1, g + N1 + N2}, ss, sb, ts));
+  if (!Qin) return PSB_OK;  // allocation only
+  const double d2 = -2.0 * c->Delta * c->Delta;
+  {
+    LaunchScope ls(c, "dsmag L:M reduction", (double)sizeof(Cx<T>) * 24 * fs);
+    dsmag_lm_kernel<T><<<kLmBlocks, 256, 0, c->stream>>>(A, B, g, N1, N2, N3, N3h, d2, part);
+  }
+  PSB_TRY(launch_ok(c, "dsmag L:M"));
+  {
+    LaunchScope ls(c, "dsmag Cs^2", 16.0 * kLmBlocks);
+    dsmag_cs2_kernel<<<1, 256, 0, c->stream>>>(part, kLmBlocks, cs2);
+  }
+  PSB_TRY(launch_ok(c, "dsmag Cs^2"));
+  EpiNS<T, true> epi{io, ktabs<T>(c->kx, c->ky, c->kz), (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
+                     (T)p->Om3, 0, N1 / 2, N2 / 2, N3 / 2};
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "dsmag epilogue", (double)sizeof(Cx<T>) * 12 * fs + epi.io_bytes(fs));
+    dsmag_epi_kernel<T><<<blocks, 256, 0, c->stream>>>(epi, A, N1, N2, N3h, cs2, c->Delta);
+  }
+  PSB_TRY(launch_ok(c, "dsmag epilogue"));
+  if (cs2_out) {
+    double h[3];
+    PSB_TRY(cuda_ok(c, cudaMemcpyAsync(h, cs2, sizeof(h), cudaMemcpyDeviceToHost, c->stream), "Cs^2 copy"));
+    PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "Cs^2 sync"));
+    *cs2_out = h[0];
+  }
+  return PSB_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -831,6 +1051,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       epi.plql_out = nullptr;
       return run_plql<T>(c, m, Qin ? B2 : nullptr, E, epi);
     }
+    case PSB_DSMAG:
+      return dsmag_rhs<T>(c, io, p, ts, tau_out);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

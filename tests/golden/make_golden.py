@@ -15,7 +15,11 @@ This script executes its unmodified sources under a load-time shim:
 * ``pyfftw`` is a stand-in whose ``FFTW`` object copies into its input buffer,
   runs ``scipy.fft`` (normalised inverse, like pyFFTW's default
   ``normalise_idft=True``) and returns its internal output buffer;
-* ``RHSfunctionsWEAVE`` is an empty module; ``mpi4py`` a single-rank stand-in.
+* ``RHSfunctionsWEAVE`` is an empty module; ``mpi4py`` a single-rank stand-in;
+* ``utilitiesClass.myFilter`` gets its cutoff truncated to an int: the dynamic
+  Smagorinsky model calls it with ``kc/2.`` (``src/RHSfunctions.py:1697``),
+  a float slice bound that the NumPy of the reference's day truncated and
+  NumPy 2 rejects.
 
 ``advanceQ_RK4`` lives in the driver script, which runs a whole simulation at
 import time, so its four lines (``src/PySpec_3d.py:96-105``) are restated in
@@ -24,8 +28,9 @@ import time, so its four lines (``src/PySpec_3d.py:96-105``) are restated in
 Outputs (all FP64, a few hundred KB in total):
 
 * ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
-  closure (DNS, Smagorinsky, t-model, static and dynamic tau-model; DNS and
-  t-model also with rotation), plus the diagnostics;
+  closure (DNS, Smagorinsky, t-model, static and dynamic tau-model, dynamic
+  Smagorinsky; DNS, Smagorinsky, t-model and dynamic Smagorinsky also with
+  rotation), plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
 * ``tgv64_benchmark.npz`` -- the reference's known-answer energy and
   dissipation history (``run/TGV_Validate100/benchmark_sol_64.npz``).
@@ -209,6 +214,8 @@ def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), C
     grid = C.gridclass(N, N, N, x, y, z, kc, 2 * np.pi, 2 * np.pi, 2 * np.pi)
     myFFT = C.FFTclass(N, N, N, 1)
     util = C.utilitiesClass()
+    _filter = util.myFilter
+    util.myFilter = lambda uhat, kc: _filter(uhat, int(kc))
     cfl = -dt if cfl is None else cfl
     with contextlib.redirect_stdout(io.StringIO()):
         main = C.variables(0, turb_model, rotate, Om[0], Om[1], Om[2], grid, state[0].copy(),
@@ -232,6 +239,9 @@ def gen_serial(N, seed):
         ("tmodel_rot", 2, dict(rotate=1, Om=(0.2, 0.0, 0.3))),
         ("stau", "Static tau-model", dict(dt0=0.05, dt1=0.2)),
         ("dtau", "Dynamic tau-model", {}),
+        ("dsmag", 7, {}),
+        ("dsmag_rot", 7, dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
+        ("dsmag_kc", 7, dict(kc=N // 2 - 1)),         # kc/2 fractional: truncated cutoff
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)

@@ -17,6 +17,8 @@ CASES = {
     "tmodel_rot": (2, dict(rotate=1, Om=(0.2, 0.0, 0.3)), dict(rotate=1, Om=(0.2, 0.0, 0.3), Ct=0.1)),
     "stau": ("Static tau-model", dict(dt0=0.05, dt1=0.2), dict(tau_a=0.05, tau_b=0.2)),
     "dtau": ("Dynamic tau-model", {}, {}),
+    "dsmag": (7, {}, {}),
+    "dsmag_rot": (7, dict(rotate=1, Om=(-0.15, 0.35, 0.2)), dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
 }
 NU, DT, T = 0.02, 0.01, 0.37
 

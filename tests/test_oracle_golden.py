@@ -8,7 +8,7 @@ from oracle import spectral_oracle as orc
 from tests.helpers import CASES, DT, NU, T, golden, rel
 
 FN = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "stau": orc.rhs_staumodel,
-      "dtau": orc.rhs_dtaumodel}
+      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag}
 
 
 def _fn(name):
@@ -19,7 +19,7 @@ def _read(name, res, Q):
     base = name.split("_")[0]
     if base == "dns":
         return res[1]
-    if base == "smag":
+    if base in ("smag", "dsmag"):
         return Q
     return res[2]
 
@@ -40,6 +40,37 @@ def test_rhs_and_step_match_reference(N, name):
     Q, read = orc.advance_rk4(st, lambda q: (lambda r: (r[0], _read(name, r, q)))(_fn(name)(g, q, p)), DT)
     assert rel(Q, d[f"{name}_step"]) < 1e-13
     assert rel(read, d[f"{name}_step_uhat"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_dsmag_fractional_cutoff_matches_reference(N):
+    """Dynamic Smagorinsky with kc = N/2 - 1: the test filter kc/2 is
+    fractional and myFilter truncates it (src/RHSfunctions.py:1697,
+    src/Classes.py:1271-1279)."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N, kc=N // 2 - 1)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    st = d["state"]
+    r, w0, cs2 = orc.rhs_dsmag(g, st, p)
+    assert rel(r, d["dsmag_kc_rhs"]) < 1e-13
+    assert rel(w0, d["dsmag_kc_w0"]) < 1e-13
+    Q, _ = orc.advance_rk4(st, lambda q: (orc.rhs_dsmag(g, q, p)[0], q), DT)
+    assert rel(Q, d["dsmag_kc_step"]) < 1e-13
+
+
+def test_myfilter_slice_semantics():
+    """myFilter keeps rows [0:kc] and [-kc+1:]; kc = 1 makes the second slice
+    [0:], the whole axis (Python slicing), and kc = 0 keeps nothing."""
+    g = orc.Grid.periodic(8)
+    m1, m2, m3 = orc.myfilter_axes(g, 3)
+    np.testing.assert_array_equal(m1, [1, 1, 1, 0, 0, 0, 1, 1])
+    np.testing.assert_array_equal(m3, [1, 1, 1, 0, 0])
+    m1, _, m3 = orc.myfilter_axes(g, 1)
+    np.testing.assert_array_equal(m1, np.ones(8))
+    np.testing.assert_array_equal(m3, [1, 0, 0, 0, 0])
+    m1, _, m3 = orc.myfilter_axes(g, 2.5)
+    np.testing.assert_array_equal(m1, [1, 1, 0, 0, 0, 0, 0, 1])
+    assert orc.myfilter_axes(g, 0)[2].sum() == 0
 
 
 @pytest.mark.parametrize("N", [12, 16])
@@ -137,3 +168,42 @@ def test_analytic_properties_of_the_oracle():
     r, _ = orc.rhs_nosgs(g, d, orc.Params(nu=0.01))
     div = g.k1 * r[0] + g.k2 * r[1] + g.k3 * r[2]
     assert np.abs(div).max() < 1e-10 * np.abs(r).max()
+
+
+@pytest.mark.parametrize("N,kc", [(12, 6), (16, 8), (16, 7), (12, 3)])
+def test_dsmag_coefficient_by_parseval(N, kc):
+    """The GPU forms Cs^2 as a spectral sum (k3 > 0 twice, the Hermitian part
+    of the k3 = 0 plane, modes pad() drops excluded) instead of means over the
+    3/2 grid; by Parseval the two agree."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N, kc=kc)
+    u, v, w = d["state"]
+    ref = orc.dsmag_cs2(g, u, v, w)
+    kL = kc / 2.0
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    s = orc.scale_32(g)
+    P = orc._products_32(g, u, v, w)
+    PF = orc._products_32(g, *(orc.myfilter(g, x, kL) for x in (u, v, w)))
+
+    def ss(a, b, c):
+        Sh = (1j * k1 * a, 1j * k2 * b, 1j * k3 * c, 0.5 * (1j * k2 * a + 1j * k1 * b),
+              0.5 * (1j * k3 * a + 1j * k1 * c), 0.5 * (1j * k3 * b + 1j * k2 * c))
+        S = [orc.ifft32(g, orc.pad(x) * s) for x in Sh]
+        mag = np.sqrt(2.0 * (S[0] ** 2 + S[1] ** 2 + S[2] ** 2 + 2 * S[3] ** 2 + 2 * S[4] ** 2 + 2 * S[5] ** 2))
+        return [orc.unpad(orc.fft32(mag * x)) for x in S]
+    A6 = ss(u, v, w)
+    B6 = ss(*(orc.myfilter(g, x, kL) for x in (u, v, w)))
+    L = np.stack([orc.myfilter(g, P[m], kL) - PF[m] for m in range(6)])
+    M = np.stack([-2 * g.Delta ** 2 * (4 * B6[m] - orc.myfilter(g, A6[m], kL)) for m in range(6)])
+    keep = np.ones(L.shape[1:], bool)
+    keep[N // 2] = keep[:, N // 2] = keep[:, :, N // 2] = False
+    wgt = np.where(np.arange(N // 2 + 1) > 0, 2.0, 0.0)[None, None, :] * keep
+    num = np.sum(wgt * np.real(L * np.conj(M)))
+    den = np.sum(wgt * np.abs(M) ** 2)
+    neg = (-np.arange(N)) % N
+    Lm, Mm = L[:, :, :, 0], M[:, :, :, 0]
+    Mp = M[:, neg][:, :, neg, 0]
+    k0 = keep[:, :, 0]
+    num += np.sum(k0 * (0.5 * np.real(Lm * np.conj(Mm)) + 0.5 * np.real(Lm * Mp)))
+    den += np.sum(k0 * (0.5 * np.abs(Mm) ** 2 + 0.5 * np.real(Mm * Mp)))
+    assert num / den == pytest.approx(ref, rel=1e-12)
