@@ -43,6 +43,10 @@ extern "C" {
 #define PSB_DSMAG 8       /* turb_model 7      -> computeRHS_DSMAG  (src/RHSfunctions.py:1663-1862):
                              Smagorinsky with Cs^2 = <L:M>/<M:M> from the test filter
                              myFilter(., kc/2) (src/Classes.py:1271-1279)                          */
+#define PSB_CM1 9         /* turb_model 6      -> computeRHS_CM1    (src/RHSfunctions.py:1411-1542):
+                             6 fields u,v,w,w0_u,w0_v,w0_w; du/dt = unpad_2x(PLu) + w0,
+                             dw0/dt = PLQLu - 250 nu k^2 w0; w0_v read as zero like the
+                             reference's Q2U (src/Classes.py:489); no rotating form           */
 
 /* ---- diagnostic flags --------------------------------------------------- */
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
@@ -98,7 +102,7 @@ const char* psb_create_error(void);
 
 /* One right-hand-side evaluation: main.computeRHS(main,grid,myFFT,utilities)
  * (src/Classes.py:44,95,124,186,227; src_MPI/Classes.py:147).
- * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD).
+ * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD, PSB_MHD_TMODEL, PSB_CM1).
  * w0       : optional closure force main.w0_u/v/w (3 fields; 6 fields u then B for
  *            PSB_MHD_TMODEL) or NULL.
  * read_out : optional copy of the state as the RHS read it (the reference

@@ -485,6 +485,25 @@ def rhs_tmodel(g, state, p):
     return r, w0, ur
 
 
+def rhs_cm1(g, state, p):
+    """First-order complete memory model, ``computeRHS_CM1``
+    (``src/RHSfunctions.py:1411-1542``) on the state ``(u, v, w, w0_u, w0_v,
+    w0_w)``: ``du/dt = unpad_2x(PL u) + w0``, ``dw0/dt = PLQL u - 250 nu k^2 w0``.
+
+    As in the reference, ``w0_v`` is read as zero: its ``Q2U`` takes it from
+    ``Q[3::6, 4::6, 4::6]`` (``src/Classes.py:489``), a slice of the
+    interleaved state that nothing writes.  ``rotate = 1`` raises there (an
+    N-grid Coriolis pressure added to the 2x-grid ``phat``, ``:1463-1465``).
+
+    Returns ``(rhs, w0_read, uhat_read)``."""
+    if p.rotate == 1:
+        raise ValueError("computeRHS_CM1 has no rotating form")
+    r, _, ur, PLQL, _ = _memory_rhs(g, state[:3], p, lambda *a: (0.0, None))
+    w0 = np.stack([state[3], np.zeros_like(state[4]), state[5]])
+    rhs = np.concatenate([r + w0, PLQL - 250 * p.nu * g.ksqr * w0])
+    return rhs, w0, ur
+
+
 def rhs_staumodel(g, state, p):
     """Static tau-model, ``computeRHS_staumodel`` (``src/RHSfunctions.py:366-497``):
     ``tau = max(0, tau_a + tau_b*t)``.  Returns ``(rhs, w0, uhat_read, tau)``

@@ -135,7 +135,8 @@ class variables:
     (src/Classes.py:7-229).
 
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
-    'Dynamic tau-model', 7 (dynamic Smagorinsky).  ``precision`` (64 or 32) selects FP64 or FP32
+    'Dynamic tau-model', 6 (first-order complete memory model, state
+    ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky).  ``precision`` (64 or 32) selects FP64 or FP32
     fields; FP32 runs carry a Kahan compensation array ``comp``."""
 
     def __init__(self, weave, turb_model, rotate, Om1, Om2, Om3, grid, uhat, vhat, what, t, dt, nu, Ct=-10,
@@ -158,6 +159,11 @@ class variables:
         self.Q = torch.stack([_to_dev(a, cd, dev) for a in (uhat, vhat, what)]).contiguous()
         self.U = self.Q.clone()
         self.nvars = 3
+        if turb_model == 6:
+            # complete memory model: the memory variables w0_u, w0_v, w0_w are
+            # state (src/Classes.py:460-475), initially zero
+            self.Q = torch.cat([self.Q, torch.zeros_like(self.Q)]).contiguous()
+            self.nvars = 6
         self.Ct = 0.1 if Ct == -10 else float(Ct)
         self.tau_a, self.tau_b = float(dt0), float(dt1)
         self.tau = 0.0
@@ -168,7 +174,7 @@ class variables:
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
-                 7: R.computeRHS_DSMAG, "learned": R.computeRHS_learned}
+                 6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, "learned": R.computeRHS_learned}
         if turb_model not in table:
             raise ValueError(f"turb_model {turb_model!r} is not on this path")
         self.computeRHS = table[turb_model]
@@ -179,7 +185,7 @@ class variables:
             from .learned import MLPModel
             self.model = MLPModel.load(device=grid.device)
         if turb_model not in (0, "learned"):
-            self.W0 = torch.zeros_like(self.Q)
+            self.W0 = torch.zeros_like(self.U)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
         if turb_model == "Static tau-model":
@@ -211,10 +217,10 @@ class variables:
         return None if self.W0 is None else self.W0[2].unsqueeze(-1)
 
     def U2Q(self):
-        self.Q.copy_(self.U)
+        self.Q[:3].copy_(self.U)
 
     def Q2U(self):
-        self.U.copy_(self.Q)
+        self.U.copy_(self.Q[:3])
 
     def params(self):
         m = self.model
@@ -228,7 +234,8 @@ class variables:
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, 7: _capi.DSMAG, "learned": _capi.LEARNED}[self.turb_model]
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 6: _capi.CM1, 7: _capi.DSMAG,
+                "learned": _capi.LEARNED}[self.turb_model]
 
 
 class utilitiesClass:
@@ -313,6 +320,6 @@ class utilitiesClass:
         return k_m, spec
 
     def computeSGS_DNS(self, main, grid, myFFT):
-        w0 = torch.zeros_like(main.Q)
+        w0 = torch.zeros_like(main.U)
         grid.ctx(main.precision).sgs_dns(main.U, w0)
         return w0[0].unsqueeze(-1), w0[1].unsqueeze(-1), w0[2].unsqueeze(-1)

@@ -47,6 +47,15 @@ def computeRHS_Dtaumodel(main, grid, myFFT=None, utilities=None):
     main.tau = _rhs(main, grid, _capi.TAU_DYNAMIC)
 
 
+def computeRHS_CM1(main, grid, myFFT=None, utilities=None):
+    """First-order complete memory model (turb_model 6),
+    src/RHSfunctions.py:1411-1542: ``main.Q`` holds (u, v, w, w0_u, w0_v,
+    w0_w) and becomes their six right-hand sides; ``main.w0_*`` the memory
+    variables as read (w0_v zero, as the reference's Q2U reads it,
+    src/Classes.py:489).  No rotating form (the reference's raises)."""
+    _rhs(main, grid, _capi.CM1)
+
+
 def computeRHS_DSMAG(main, grid, myFFT=None, utilities=None):
     """Dynamic Smagorinsky (turb_model 7), src/RHSfunctions.py:1663-1862:
     ``Cs^2 = <L:M>/<M:M>`` with the test filter ``myFilter(., kc/2)``, then the

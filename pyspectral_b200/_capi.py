@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
 
 PSB_OK = 0
 PSB_ERR_NONFINITE = 6
-DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG = 0, 1, 2, 3, 4, 5, 6, 7, 8
+DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1 = 0, 1, 2, 3, 4, 5, 6, 7, 8, 9
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
 
@@ -164,7 +164,7 @@ class Context:
         return nfields * self.N1 * self.N2 * (self.N3 // 2 + 1)
 
     def rhs(self, closure, state, rhs, params, w0=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL) else 3
+        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else 3
         self.bind_stream()
         tau = ctypes.c_double(0.0)
         st = self.lib.psb_rhs(self.h, closure, self._ptr(state, self.spec_numel(nf)),
@@ -174,7 +174,7 @@ class Context:
         return tau.value
 
     def step(self, closure, state, params, nsteps=1, comp=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL) else 3
+        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else 3
         self.bind_stream()
         st = self.lib.psb_step_rk4(self.h, closure, self._ptr(state, self.spec_numel(nf)), self._ptr(comp),
                                    self._ptr(read_out), ctypes.byref(params), int(nsteps))

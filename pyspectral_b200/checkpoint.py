@@ -124,7 +124,7 @@ def restart(path, grid, turb_model, dt, nu, precision=64, **kw):
                      kw.pop("Om3", 0), grid, u, v, w, float(d["t"]) + dt, dt, nu, precision=precision, **kw)
     if "Q" in d:
         main.Q.copy_(torch.as_tensor(d["Q"], device=main.Q.device).to(main.Q.dtype))
-        main.U.copy_(main.Q)
+        main.Q2U()
     if "comp" in d and getattr(main, "comp", None) is not None:
         main.comp.copy_(torch.as_tensor(d["comp"], device=main.comp.device).to(main.comp.dtype))
     return main

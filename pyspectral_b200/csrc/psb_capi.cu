@@ -743,7 +743,9 @@ int psb_ctx_set_stream(psb_ctx* c, void* stream) {
 
 const char* psb_last_error(const psb_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-static int closure_fields(int closure) { return closure == PSB_MHD || closure == PSB_MHD_TMODEL ? 6 : 3; }
+static int closure_fields(int closure) {
+  return closure == PSB_MHD || closure == PSB_MHD_TMODEL || closure == PSB_CM1 ? 6 : 3;
+}
 
 int psb_rhs(psb_ctx* c, int closure, const void* state, void* rhs, void* w0, void* read_out, const psb_params* p,
             double* tau_out) {

@@ -892,6 +892,88 @@ __global__ void __launch_bounds__(256) dsmag_epi_kernel(EpiNS<T, true> epi, cons
   }
 }
 
+// ---------------------------------------------------------------------------
+// First-order complete memory model (PySpectral/src/RHSfunctions.py:1411-1542)
+// on the state (u, v, w, w0_u, w0_v, w0_w):
+//   du/dt  = unpad_2x(PL u) + w0
+//   dw0/dt = PLQL u - 250 nu k^2 w0
+// PL and PLQL are the t-model's pipelines (run_pl / run_plql, PLQL stored).
+// w0_v enters as zero, as in the reference: its Q2U reads it from
+// Q[3::6,4::6,4::6] (src/Classes.py:489), a slice nothing writes.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) cm1_combine_kernel(StepIO<T> io, KTabs<T> k, const Cx<T>* __restrict__ PLp,
+                                                          const Cx<T>* __restrict__ PLQL, T nu250, int N1, int N2,
+                                                          int N3) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % io.n3h);
+    const long long t = s / io.n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    const Cx<T> zero = mk<T>(0, 0);
+    const Cx<T> w0u = io.Q[3 * fs + s], w0v = zero, w0w = io.Q[5 * fs + s];
+    if (io.read_out) {
+      const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = nyq ? zero : io.Q[f * fs + s];
+    }
+    if (io.w0_out) {
+      io.w0_out[s] = w0u;
+      io.w0_out[fs + s] = w0v;
+      io.w0_out[2 * fs + s] = w0w;
+    }
+    const T damp = nu250 * ksq;
+    const Cx<T> r0 = PLp[s] + w0u, r1 = PLp[fs + s] + w0v, r2 = PLp[2 * fs + s] + w0w;
+    const Cx<T> r3 = PLQL[s] - damp * w0u, r4 = PLQL[fs + s] - damp * w0v, r5 = PLQL[2 * fs + s] - damp * w0w;
+    io.finish(s, 0, r0);
+    io.finish(s, 1, r1);
+    io.finish(s, 2, r2);
+    io.finish(s, 3, r3);
+    io.finish(s, 4, r4);
+    io.finish(s, 5, r5);
+  }
+}
+
+template <typename T>
+int cm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
+  if (p->rotate)
+    return fail(c, PSB_ERR_UNSUPPORTED, "PSB_CM1: the reference's computeRHS_CM1 has no rotating form");
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* PLp = scratch<T>(c, "mem.PLp", (size_t)3 * fs, &st);
+  Cx<T>* PLQL = scratch<T>(c, "cm1.PLQL", (size_t)3 * fs, &st);
+  if (st != PSB_OK) return st;
+  const Cx<T>* Qin = io.Q;
+  MemCfg m{"memu", nullptr, 0, true, false, 0};
+  if (Qin) PSB_TRY(cuda_ok(c, cudaMemsetAsync(PLp, 0, sizeof(Cx<T>) * 3 * fs, c->stream), "memset"));
+  Cx<T>*B2 = nullptr, *E = nullptr;
+  PSB_TRY(run_pl<T>(c, Qin, p, m, &B2, &E, PLp, nullptr));
+  EpiPLQL<T> epi{};
+  epi.io = io;
+  epi.k = ktabs<T>(c->kx, c->ky, c->kz);
+  epi.PLp = PLp;
+  epi.coef = (T)0;
+  epi.ny1 = N1 / 2;
+  epi.ny2 = N2 / 2;
+  epi.ny3 = N3 / 2;
+  epi.plql_out = PLQL;
+  PSB_TRY(run_plql<T>(c, m, Qin ? B2 : nullptr, E, epi));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "cm1 combine", (double)sizeof(Cx<T>) * fs * (6 + 2 + 6));
+    cm1_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, ktabs<T>(c->kx, c->ky, c->kz), PLp, PLQL,
+                                                         (T)(250 * p->nu), N1, N2, N3);
+  }
+  return launch_ok(c, "cm1 combine");
+}
+
 // myFilter's kept rows (src/Classes.py:1271-1279) with Python slice bounds:
 // [0:kc] and [-kc+1:] on axes 1 and 2, [0:kc] on axis 3
 inline void myfilter_rows(int n, int kc, bool two_sided, double* out) {
@@ -1053,6 +1135,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
     }
     case PSB_DSMAG:
       return dsmag_rhs<T>(c, io, p, ts, tau_out);
+    case PSB_CM1:
+      return cm1_rhs<T>(c, io, p);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

@@ -29,8 +29,8 @@ Outputs (all FP64, a few hundred KB in total):
 
 * ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
   closure (DNS, Smagorinsky, t-model, static and dynamic tau-model, dynamic
-  Smagorinsky; DNS, Smagorinsky, t-model and dynamic Smagorinsky also with
-  rotation), plus the diagnostics;
+  Smagorinsky, first-order complete memory model; DNS, Smagorinsky, t-model
+  and dynamic Smagorinsky also with rotation), plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
 * ``tgv64_benchmark.npz`` -- the reference's known-answer energy and
   dissipation history (``run/TGV_Validate100/benchmark_sol_64.npz``).
@@ -203,8 +203,8 @@ def ref_rk4_step(main, grid, myFFT, utilities):
     utilities.postAdvanceQ_hook(main, grid, myFFT)
 
 
-def _diag(Q):
-    return np.stack([Q[0::3, 0::3, 0::3], Q[1::3, 1::3, 1::3], Q[2::3, 2::3, 2::3]])
+def _diag(Q, nv=3):
+    return np.stack([Q[f::nv, f::nv, f::nv] for f in range(nv)])
 
 
 def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), Ct=-10, dt0=-10,
@@ -242,12 +242,13 @@ def gen_serial(N, seed):
         ("dsmag", 7, {}),
         ("dsmag_rot", 7, dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
         ("dsmag_kc", 7, dict(kc=N // 2 - 1)),         # kc/2 fractional: truncated cutoff
+        ("cm1", 6, {}),
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
         with contextlib.redirect_stdout(io.StringIO()):
             main.computeRHS(main, grid, myFFT, util)
-        out[f"{name}_rhs"] = _diag(main.Q)
+        out[f"{name}_rhs"] = _diag(main.Q, getattr(main, "nvars", 3))
         out[f"{name}_uhat"] = np.stack([main.uhat, main.vhat, main.what])
         if hasattr(main, "w0_u"):
             out[f"{name}_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
@@ -256,8 +257,24 @@ def gen_serial(N, seed):
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
         with contextlib.redirect_stdout(io.StringIO()):
             ref_rk4_step(main, grid, myFFT, util)
-        out[f"{name}_step"] = _diag(main.Q)
+        out[f"{name}_step"] = _diag(main.Q, getattr(main, "nvars", 3))
         out[f"{name}_step_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+    # CM1 from a state with non-zero memory variables (set, then U2Q)
+    w0init = 0.3 * orc.isotropic_state(N, seed + 100, k0=2.0)
+    out["cm1w_init"] = w0init
+    for stage in ("rhs", "step"):
+        grid, myFFT, util, main = serial_case(C, N, st, 6, nu, dt, t)
+        for i, a in enumerate((main.w0_u, main.w0_v, main.w0_w)):
+            a[..., 0] = w0init[i]
+        main.U2Q()
+        with contextlib.redirect_stdout(io.StringIO()):
+            if stage == "rhs":
+                main.computeRHS(main, grid, myFFT, util)
+                out["cm1w_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
+                out["cm1w_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+            else:
+                ref_rk4_step(main, grid, myFFT, util)
+        out[f"cm1w_{stage}"] = _diag(main.Q, 6)
     # diagnostics on the input state; kc = N/4 so that the sharp cutoff Gf
     # (and with it the SGS stress of computeSGS_DNS) is not trivial
     out["diag_kc"] = np.int64(N // 4)

@@ -8,7 +8,7 @@ from oracle import spectral_oracle as orc
 from tests.helpers import CASES, DT, NU, T, golden, rel
 
 FN = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "stau": orc.rhs_staumodel,
-      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag}
+      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag, "cm1": orc.rhs_cm1}
 
 
 def _fn(name):
@@ -31,6 +31,8 @@ def test_rhs_and_step_match_reference(N, name):
     g = orc.Grid.periodic(N)
     p = orc.Params(nu=NU, t=T, dt=DT, **CASES[name][2])
     st = d["state"]
+    if CASES[name][0] == 6:  # complete memory model: memory variables start at zero
+        st = np.concatenate([st, np.zeros_like(st)])
     res = _fn(name)(g, st, p)
     assert rel(res[0], d[f"{name}_rhs"]) < 1e-13
     if f"{name}_w0" in d:
@@ -56,6 +58,25 @@ def test_dsmag_fractional_cutoff_matches_reference(N):
     assert rel(w0, d["dsmag_kc_w0"]) < 1e-13
     Q, _ = orc.advance_rk4(st, lambda q: (orc.rhs_dsmag(g, q, p)[0], q), DT)
     assert rel(Q, d["dsmag_kc_step"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_cm1_with_memory_matches_reference(N):
+    """CM1 from non-zero memory variables: the reference reads w0_v as zero
+    (src/Classes.py:489) while its slot of the state still evolves."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    st = np.concatenate([d["state"], d["cm1w_init"]])
+    r, w0, ur = orc.rhs_cm1(g, st, p)
+    assert rel(r, d["cm1w_rhs"]) < 1e-13
+    assert rel(w0, d["cm1w_w0"]) < 1e-13
+    assert rel(ur, d["cm1w_uhat"]) < 1e-13
+    assert np.abs(d["cm1w_w0"][1]).max() == 0.0 and np.abs(d["cm1w_init"][1]).max() > 0
+    Q, _ = orc.advance_rk4(st, lambda q: (orc.rhs_cm1(g, q, p)[0], q), DT)
+    assert rel(Q, d["cm1w_step"]) < 1e-13
+    with pytest.raises(ValueError):
+        orc.rhs_cm1(g, st, orc.Params(nu=NU, rotate=1, Om=(0.1, 0.2, 0.3)))
 
 
 def test_myfilter_slice_semantics():
