@@ -47,6 +47,10 @@ extern "C" {
                              6 fields u,v,w,w0_u,w0_v,w0_w; du/dt = unpad_2x(PLu) + w0,
                              dw0/dt = PLQLu - 250 nu k^2 w0; w0_v read as zero like the
                              reference's Q2U (src/Classes.py:489); no rotating form           */
+#define PSB_BUDGETS 10    /* turb_model 99     -> computeRHS_BUDGETS (src/RHSfunctions.py:1543-1661):
+                             RHS = unpad_2x(PLu); w0 receives PLQLu with the q part split at
+                             p.kf (0 -> int(max k1), main.kc of src/Classes.py:16); no
+                             rotating form                                                      */
 
 /* ---- diagnostic flags --------------------------------------------------- */
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
@@ -73,7 +77,8 @@ typedef struct {
   double dt;           /* time step */
   double Ct;           /* t-model constant (src/Classes.py:103-108) */
   double tau_a, tau_b; /* static tau-model tau = max(0, tau_a + tau_b t) (src/Classes.py:194-195) */
-  int kf;              /* dynamic tau test-filter wavenumber; 0 -> int(kc*2/3) (src/Classes.py:131) */
+  int kf;              /* dynamic tau test-filter wavenumber; 0 -> int(kc*2/3) (src/Classes.py:131);
+                          PSB_BUDGETS: the budget split main.kc; 0 -> int(max k1) (src/Classes.py:16) */
   int rotate;          /* Coriolis on/off (src/RHSfunctions.py:33-36,47-50) */
   double Om1, Om2, Om3;
   const void* force;   /* MHD: constant forcing spectra, 3 fields, or NULL (src_MPI/Classes.py:91-94) */

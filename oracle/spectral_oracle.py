@@ -504,6 +504,30 @@ def rhs_cm1(g, state, p):
     return rhs, w0, ur
 
 
+def budget_kc(g):
+    """``main.kc = np.amax(grid.k1)`` (``src/Classes.py:16``), truncated as
+    the slices of ``seperateModesBudgets`` take it."""
+    return int(np.amax(np.fft.fftshift(np.linspace(-(g.N1 // 2), g.N1 // 2 - 1, g.N1)) * 2.0 * np.pi / g.L1))
+
+
+def rhs_budgets(g, state, p, kc=None):
+    """DNS with SGS budgets, ``computeRHS_BUDGETS`` (``src/RHSfunctions.py:1543-1661``):
+    RHS ``= unpad_2x(PL u)``; ``PLQL u`` with the q part split at ``main.kc``
+    (``seperateModesBudgets``, ``src/padding.py:81-93``).  ``rotate = 1``
+    raises in the reference (an N-grid Coriolis pressure added to the 2x-grid
+    ``phat``, ``:1605-1607``).
+
+    Returns ``(rhs, PLQL, uhat_read)``; ``rhs`` is also ``main.PLu/v/w``."""
+    if p.rotate == 1:
+        raise ValueError("computeRHS_BUDGETS has no rotating form")
+    kc = budget_kc(g) if kc is None else kc
+    u, v, w = (nyquist_zero(state[i]) for i in range(3))
+    PL, vel, _, _ = _pl_2x(g, pad_2x(u), pad_2x(v), pad_2x(w), p.nu, 0, p.Om)
+    PLq = [separate_modes_testfilter(x, kc)[1] for x in PL]
+    PLQL = _plql(g, vel, PLq)
+    return np.stack([unpad_2x(x) for x in PL]), PLQL, np.stack([u, v, w])
+
+
 def rhs_staumodel(g, state, p):
     """Static tau-model, ``computeRHS_staumodel`` (``src/RHSfunctions.py:366-497``):
     ``tau = max(0, tau_a + tau_b*t)``.  Returns ``(rhs, w0, uhat_read, tau)``

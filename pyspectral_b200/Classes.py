@@ -136,7 +136,9 @@ class variables:
 
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
     'Dynamic tau-model', 6 (first-order complete memory model, state
-    ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky).  ``precision`` (64 or 32) selects FP64 or FP32
+    ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky), 99 (DNS
+    with SGS budgets: ``utilitiesClass``'s hooks write ``budget<it>.npz``
+    every 20 iterations).  ``precision`` (64 or 32) selects FP64 or FP32
     fields; FP32 runs carry a Kahan compensation array ``comp``."""
 
     def __init__(self, weave, turb_model, rotate, Om1, Om2, Om3, grid, uhat, vhat, what, t, dt, nu, Ct=-10,
@@ -174,7 +176,8 @@ class variables:
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
-                 6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, "learned": R.computeRHS_learned}
+                 6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, 99: R.computeRHS_BUDGETS,
+                 "learned": R.computeRHS_learned}
         if turb_model not in table:
             raise ValueError(f"turb_model {turb_model!r} is not on this path")
         self.computeRHS = table[turb_model]
@@ -190,6 +193,9 @@ class variables:
             self.kf = int(grid.kc * 2.0 / 3.0)
         if turb_model == "Static tau-model":
             self.kf = int(grid.kc / 2.0)
+        if turb_model == 99:
+            self.kf = int(self.kc)  # the budget split main.kc = amax(k1) (src/Classes.py:16)
+        self.iteration = 0
 
     # views of the reference's per-component names
     @property
@@ -234,7 +240,7 @@ class variables:
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, 6: _capi.CM1, 7: _capi.DSMAG,
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 6: _capi.CM1, 7: _capi.DSMAG, 99: _capi.BUDGETS,
                 "learned": _capi.LEARNED}[self.turb_model]
 
 
@@ -242,10 +248,33 @@ class utilitiesClass:
     """Diagnostics of src/Classes.py:631-929 (FP64 reductions on the GPU)."""
 
     def preAdvanceQ_hook(self, main, grid, myFFT):
-        pass
+        """SGS budgets (src/Classes.py:632-637): every 20 iterations of a
+        turb_model 99 run keep the state and the SGS force of its filtered field."""
+        if main.turb_model == 99 and main.iteration % 20 == 0:
+            main.u0 = main.U.clone()
+            main.w0_u0, main.w0_v0, main.w0_w0 = self.computeSGS_DNS(main, grid, myFFT)
 
-    def postAdvanceQ_hook(self, main, grid, myFFT):
-        pass
+    def postAdvanceQ_hook(self, main, grid, myFFT, directory="3DSolution"):
+        """SGS budgets (src/Classes.py:638-649): ``budget<it>.npz`` with the
+        rates of change of the SGS force and of the state over the step, the
+        last stage's PLQL (u, v, w) and PL (u).  The step ran fused, so the last
+        stage's PL and PLQL are evaluated again from the state it read
+        (``main.uhat``), which gives the same values."""
+        if not (main.turb_model == 99 and main.iteration % 20 == 0):
+            return
+        import os
+        w0_u, w0_v, w0_w = self.computeSGS_DNS(main, grid, myFFT)
+        rhs = torch.empty_like(main.U)
+        plql = torch.empty_like(main.U)
+        grid.ctx(main.precision).rhs(_capi.BUDGETS, main.U, rhs, main.params(), w0=plql)
+
+        def h(t):
+            return t.detach().cpu().numpy().astype(np.complex128)
+        os.makedirs(directory, exist_ok=True)
+        np.savez_compressed(os.path.join(directory, "budget" + str(main.iteration)),
+                            w0_udot=h((w0_u - main.w0_u0) / main.dt), w0_vdot=h((w0_v - main.w0_v0) / main.dt),
+                            w0_wdot=h((w0_w - main.w0_w0) / main.dt), u_dot=h((main.U[0] - main.u0[0]) / main.dt),
+                            PLQLu=h(plql[0]), PLQLv=h(plql[1]), PLQLw=h(plql[2]), PLu=h(rhs[0]))
 
     def computeEnergy(self, main, grid):
         return grid.ctx(main.precision).energy(main.U, _capi.NORM_SERIAL)

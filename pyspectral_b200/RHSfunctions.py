@@ -56,6 +56,15 @@ def computeRHS_CM1(main, grid, myFFT=None, utilities=None):
     _rhs(main, grid, _capi.CM1)
 
 
+def computeRHS_BUDGETS(main, grid, myFFT=None, utilities=None):
+    """DNS with SGS budgets (turb_model 99), src/RHSfunctions.py:1543-1661:
+    ``main.Q`` becomes ``unpad_2x(PL u)``, kept as ``main.PLu/v/w``;
+    ``main.PLQLu/v/w`` the memory term with the q part split at ``main.kc``."""
+    _rhs(main, grid, _capi.BUDGETS)
+    main.PLu, main.PLv, main.PLw = main.Q.clone().unbind(0)
+    main.PLQLu, main.PLQLv, main.PLQLw = main.W0.unbind(0)
+
+
 def computeRHS_DSMAG(main, grid, myFFT=None, utilities=None):
     """Dynamic Smagorinsky (turb_model 7), src/RHSfunctions.py:1663-1862:
     ``Cs^2 = <L:M>/<M:M>`` with the test filter ``myFilter(., kc/2)``, then the

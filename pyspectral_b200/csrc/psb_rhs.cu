@@ -974,6 +974,70 @@ int cm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
   return launch_ok(c, "cm1 combine");
 }
 
+// ---------------------------------------------------------------------------
+// DNS with SGS budgets (PySpectral/src/RHSfunctions.py:1543-1661, turb_model 99):
+// RHS = unpad_2x(PL u); PLQL u with the q part split at main.kc
+// (seperateModesBudgets, src/padding.py:81-93) is stored for the budget files.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) budgets_finish_kernel(StepIO<T> io, const Cx<T>* __restrict__ PLp, int N1,
+                                                             int N2, int N3) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    if (io.read_out) {
+      const int i3 = (int)(s % io.n3h);
+      const long long t = s / io.n3h;
+      const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+      const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+    }
+    io.finish(s, 0, PLp[s]);
+    io.finish(s, 1, PLp[fs + s]);
+    io.finish(s, 2, PLp[2 * fs + s]);
+  }
+}
+
+template <typename T>
+int budgets_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
+  if (p->rotate)
+    return fail(c, PSB_ERR_UNSUPPORTED, "PSB_BUDGETS: the reference's computeRHS_BUDGETS has no rotating form");
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  // main.kc = amax(grid.k1) (src/Classes.py:16), truncated by the slices of seperateModesBudgets
+  const int kc = p->kf > 0 ? p->kf : (int)(((double)(N1 / 2 - 1) * 2.0) * M_PI / c->L1);
+  if (kc < 2 || kc > N1 || kc > N2 || kc > N3 / 2 + 1)
+    return fail(c, PSB_ERR_ARG, "PSB_BUDGETS: budget split kc (p.kf) out of range");
+  int st = PSB_OK;
+  Cx<T>* PLp = scratch<T>(c, "mem.PLp", (size_t)3 * fs, &st);
+  Cx<T>* PLQL = io.w0_out ? io.w0_out : scratch<T>(c, "budget.PLQL", (size_t)3 * fs, &st);
+  if (st != PSB_OK) return st;
+  const Cx<T>* Qin = io.Q;
+  MemCfg m{"memu", nullptr, kc, true, false, 0};
+  if (Qin) PSB_TRY(cuda_ok(c, cudaMemsetAsync(PLp, 0, sizeof(Cx<T>) * 3 * fs, c->stream), "memset"));
+  Cx<T>*B2 = nullptr, *E = nullptr;
+  PSB_TRY(run_pl<T>(c, Qin, p, m, &B2, &E, PLp, nullptr));
+  EpiPLQL<T> epi{};
+  epi.io = io;
+  epi.k = ktabs<T>(c->kx, c->ky, c->kz);
+  epi.PLp = PLp;
+  epi.coef = (T)0;
+  epi.ny1 = N1 / 2;
+  epi.ny2 = N2 / 2;
+  epi.ny3 = N3 / 2;
+  epi.plql_out = PLQL;
+  PSB_TRY(run_plql<T>(c, m, Qin ? B2 : nullptr, E, epi));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "budgets finish", (double)sizeof(Cx<T>) * fs * (3 + 3 + 3));
+    budgets_finish_kernel<T><<<blocks, 256, 0, c->stream>>>(io, PLp, N1, N2, N3);
+  }
+  return launch_ok(c, "budgets finish");
+}
+
 // myFilter's kept rows (src/Classes.py:1271-1279) with Python slice bounds:
 // [0:kc] and [-kc+1:] on axes 1 and 2, [0:kc] on axis 3
 inline void myfilter_rows(int n, int kc, bool two_sided, double* out) {
@@ -1137,6 +1201,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       return dsmag_rhs<T>(c, io, p, ts, tau_out);
     case PSB_CM1:
       return cm1_rhs<T>(c, io, p);
+    case PSB_BUDGETS:
+      return budgets_rhs<T>(c, io, p);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

@@ -19,7 +19,8 @@ This script executes its unmodified sources under a load-time shim:
 * ``utilitiesClass.myFilter`` gets its cutoff truncated to an int: the dynamic
   Smagorinsky model calls it with ``kc/2.`` (``src/RHSfunctions.py:1697``),
   a float slice bound that the NumPy of the reference's day truncated and
-  NumPy 2 rejects.
+  NumPy 2 rejects; ``seperateModesBudgets`` likewise (the budget RHS passes
+  the float ``main.kc = np.amax(grid.k1)``, ``src/Classes.py:16``).
 
 ``advanceQ_RK4`` lives in the driver script, which runs a whole simulation at
 import time, so its four lines (``src/PySpec_3d.py:96-105``) are restated in
@@ -29,8 +30,9 @@ Outputs (all FP64, a few hundred KB in total):
 
 * ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
   closure (DNS, Smagorinsky, t-model, static and dynamic tau-model, dynamic
-  Smagorinsky, first-order complete memory model; DNS, Smagorinsky, t-model
-  and dynamic Smagorinsky also with rotation), plus the diagnostics;
+  Smagorinsky, first-order complete memory model, DNS with SGS budgets; DNS,
+  Smagorinsky, t-model and dynamic Smagorinsky also with rotation), the
+  budget file the hooks write at iteration 20, plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
 * ``tgv64_benchmark.npz`` -- the reference's known-answer energy and
   dissipation history (``run/TGV_Validate100/benchmark_sol_64.npz``).
@@ -43,6 +45,7 @@ import io
 import math
 import os
 import sys
+import tempfile
 import types
 
 import numpy as np
@@ -167,6 +170,8 @@ def load_serial():
     for k, v in pad.__dict__.items():  # "from padding import *"
         if not k.startswith("__"):
             rhs.__dict__.setdefault(k, v)
+    _split = pad.seperateModesBudgets
+    rhs.__dict__["seperateModesBudgets"] = lambda uhat_pad, arrange, kc: _split(uhat_pad, arrange, int(kc))
     cls = _load(os.path.join(SRC, "Classes.py"), "Classes")
     for k, v in rhs.__dict__.items():  # "from RHSfunctions import *"
         if not k.startswith("__") and k != "np":
@@ -243,6 +248,7 @@ def gen_serial(N, seed):
         ("dsmag_rot", 7, dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
         ("dsmag_kc", 7, dict(kc=N // 2 - 1)),         # kc/2 fractional: truncated cutoff
         ("cm1", 6, {}),
+        ("budgets", 99, {}),
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
@@ -254,11 +260,31 @@ def gen_serial(N, seed):
             out[f"{name}_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
         if hasattr(main, "tau"):
             out[f"{name}_tau"] = np.float64(np.real(main.tau))
+        if tm == 99:
+            out[f"{name}_plql"] = np.stack([main.PLQLu, main.PLQLv, main.PLQLw])
+            out[f"{name}_plu"] = np.stack([main.PLu, main.PLv, main.PLw])
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
         with contextlib.redirect_stdout(io.StringIO()):
             ref_rk4_step(main, grid, myFFT, util)
         out[f"{name}_step"] = _diag(main.Q, getattr(main, "nvars", 3))
         out[f"{name}_step_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+    # the budget hooks (src/Classes.py:632-649) around one step at iteration
+    # 20, kc = N/4 so that the SGS force of the filtered field is not trivial
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.chdir(tmp)
+        os.makedirs("3DSolution")
+        try:
+            grid, myFFT, util, main = serial_case(C, N, st, 99, nu, dt, t, kc=N // 4)
+            main.iteration = 20
+            with contextlib.redirect_stdout(io.StringIO()):
+                ref_rk4_step(main, grid, myFFT, util)
+            with np.load(os.path.join("3DSolution", "budget20.npz")) as b:
+                for k in b.files:
+                    out["budgetfile_" + k] = b[k]
+            out["budgetfile_step"] = _diag(main.Q)
+        finally:
+            os.chdir(cwd)
     # CM1 from a state with non-zero memory variables (set, then U2Q)
     w0init = 0.3 * orc.isotropic_state(N, seed + 100, k0=2.0)
     out["cm1w_init"] = w0init

@@ -20,6 +20,7 @@ CASES = {
     "dsmag": (7, {}, {}),
     "dsmag_rot": (7, dict(rotate=1, Om=(-0.15, 0.35, 0.2)), dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
     "cm1": (6, {}, {}),
+    "budgets": (99, {}, {}),
 }
 NU, DT, T = 0.02, 0.01, 0.37
 

@@ -8,7 +8,7 @@ from oracle import spectral_oracle as orc
 from tests.helpers import CASES, DT, NU, T, golden, rel
 
 FN = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "stau": orc.rhs_staumodel,
-      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag, "cm1": orc.rhs_cm1}
+      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag, "cm1": orc.rhs_cm1, "budgets": orc.rhs_budgets}
 
 
 def _fn(name):
@@ -77,6 +77,38 @@ def test_cm1_with_memory_matches_reference(N):
     assert rel(Q, d["cm1w_step"]) < 1e-13
     with pytest.raises(ValueError):
         orc.rhs_cm1(g, st, orc.Params(nu=NU, rotate=1, Om=(0.1, 0.2, 0.3)))
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_budgets_match_reference(N):
+    """computeRHS_BUDGETS' PL and PLQL, and the budget file its hooks write
+    around a step at iteration 20 (src/Classes.py:632-649)."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    st = d["state"]
+    r, plql, _ = orc.rhs_budgets(g, st, p)
+    assert rel(r, d["budgets_plu"]) < 1e-13
+    assert rel(plql, d["budgets_plql"]) < 1e-13
+    # the file: last stage's PL/PLQL, rates of change over the step
+    gk = orc.Grid.periodic(N, kc=N // 4)
+    last = {}
+
+    def f(q):
+        r, plql, read = orc.rhs_budgets(gk, q, p)
+        last.update(r=r, plql=plql, read=read)
+        return r, read
+    Q, read = orc.advance_rk4(st, f, DT)
+    assert rel(Q, d["budgetfile_step"]) < 1e-13
+    assert rel(last["plql"], np.stack([d[f"budgetfile_PLQL{c}"] for c in "uvw"])) < 1e-13
+    assert rel(last["r"][0], d["budgetfile_PLu"]) < 1e-13
+    assert rel((read[0] - st[0]) / DT, d["budgetfile_u_dot"]) < 1e-12
+    w1, _ = orc.sgs_dns(gk, read)
+    w0, _ = orc.sgs_dns(gk, st)
+    for i, c in enumerate("uvw"):
+        assert rel((w1[i] - w0[i]) / DT, d[f"budgetfile_w0_{c}dot"][..., 0]) < 1e-12
+    with pytest.raises(ValueError):
+        orc.rhs_budgets(g, st, orc.Params(nu=NU, rotate=1, Om=(0.1, 0.2, 0.3)))
 
 
 def test_myfilter_slice_semantics():
