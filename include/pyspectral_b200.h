@@ -56,6 +56,8 @@ extern "C" {
 #define PSB_NORM_SERIAL 0   /* divide by N1*N2*N3      (src/Classes.py:652-659)      */
 #define PSB_NORM_MPI 1      /* divide by (N1*N2*N3)^2  (src_MPI/Classes.py:269-285)  */
 #define PSB_FILTER_GF 2     /* apply the sharp cutoff Gf first (src/Classes.py:584-588) */
+#define PSB_TRANSFER_2D 4   /* psb_transfer / psb_spectrum_nbins: the *_2D transfer variants
+                               (src/Classes.py:1043-1092,1152-1205,1241-1270) */
 
 typedef struct psb_ctx psb_ctx;
 
@@ -163,7 +165,10 @@ int psb_spectrum_nbins(const psb_ctx* ctx, int flags, int* nbins);
  * like psb_spectrum; out[2*nbins] = (Re, Im) per bin, nbins from
  * psb_spectrum_nbins(ctx, 0, &nbins).  flags PSB_FILTER_GF:
  * computeTransfer_resolved (:1093-1150, the fields filtered by Gf).  w0 (3
- * fields) non-NULL: computeTransfer_SGS (:1206-1239), Re sum_i conj(Gf u_i) w0_i. */
+ * fields) non-NULL: computeTransfer_SGS (:1206-1239), Re sum_i conj(Gf u_i) w0_i.
+ * flags PSB_TRANSFER_2D: the *_2D variants of the three (:1043-1092,
+ * :1152-1205, :1241-1270): the k3 = 0 plane only, bins rint(sqrt(k1^2+k2^2)),
+ * u and v only, weight 1; nbins from psb_spectrum_nbins(ctx, PSB_TRANSFER_2D, &nbins). */
 int psb_transfer(psb_ctx* ctx, const void* fields3, const void* w0, int flags, double* out, int nbins);
 /* MPI computeSpectrum / computeMHDSpectrum (src_MPI/Classes.py:370-448):
  * out[nbins] summed over components, int16 shells, k3=N/2 included. */

@@ -839,13 +839,16 @@ def spectrum(g, uvw, filtered=False):
     return kdata, spec / (N1 * N2 * N3)
 
 
-def transfer(g, uvw, filtered=False, w0=None):
+def transfer(g, uvw, filtered=False, w0=None, two_d=False):
     """``computeTransfer`` (``src/Classes.py:988-1040``): energy transfer
     spectrum sum_i conj(u_i) (-i k_j (u_i u_j)^ - i k_i p^), from the state with
     its Nyquist modes zeroed (``unpad(pad(.))``), binned like ``spectrum``
     (k3 = N/2 excluded, k3 > 0 twice) over N1 N2 N3.  ``filtered``:
     ``computeTransfer_resolved`` (``:1093-1150``), the same of Gf u.  ``w0``:
     ``computeTransfer_SGS`` (``:1206-1239``), Re sum_i conj(Gf u_i) w0_i.
+    ``two_d``: the ``*_2D`` variants (``:1043-1092``, ``:1152-1205``,
+    ``:1241-1270``): the k3 = 0 plane only, binned by ``rint(sqrt(k1^2+k2^2))``,
+    the u and v components only, weight 1.
     Returns ``(kdata, T[kmax+1])`` (complex, like the reference)."""
     N1, N2, N3 = g.N1, g.N2, g.N3
     h = N3 // 2
@@ -853,15 +856,23 @@ def transfer(g, uvw, filtered=False, w0=None):
         uvw = [g.Gf * uvw[i] for i in range(3)]
     u, v, w = (nyquist_zero(uvw[i]) for i in range(3))
     if w0 is not None:
-        r = np.real(np.conj(u) * w0[0] + np.conj(v) * w0[1] + np.conj(w) * w0[2]).astype(complex)
+        rc = [np.real(np.conj(a) * b) for a, b in zip((u, v, w), w0)]
     else:
         P = _products_32(g, u, v, w)
         uu, vv, ww, uv, uw, vw = P
         k1, k2, k3 = g.k1, g.k2, g.k3
         phat = _pressure(k1, k2, k3, g.ksqr_i, *P)
-        r = (np.conj(u) * (-1j * k1 * uu - 1j * k2 * uv - 1j * k3 * uw - 1j * k1 * phat)
-             + np.conj(v) * (-1j * k1 * uv - 1j * k2 * vv - 1j * k3 * vw - 1j * k2 * phat)
-             + np.conj(w) * (-1j * k1 * uw - 1j * k2 * vw - 1j * k3 * ww - 1j * k3 * phat))
+        rc = [np.conj(u) * (-1j * k1 * uu - 1j * k2 * uv - 1j * k3 * uw - 1j * k1 * phat),
+              np.conj(v) * (-1j * k1 * uv - 1j * k2 * vv - 1j * k3 * vw - 1j * k2 * phat),
+              np.conj(w) * (-1j * k1 * uw - 1j * k2 * vw - 1j * k3 * ww - 1j * k3 * phat)]
+    if two_d:
+        kh = np.rint(np.sqrt(g.k1 ** 2 + g.k2 ** 2)[:, :, 0])
+        kmax = int(np.round(np.amax(kh)))
+        out = np.zeros(kmax + 1, dtype=complex)
+        for i in range(2):
+            np.add.at(out, kh.astype(np.int64).astype(np.int8).ravel(), rc[i][:, :, 0].ravel())
+        return np.linspace(0, kmax, kmax + 1), out / (N1 * N2 * N3)
+    r = (rc[0] + rc[1] + rc[2]).astype(complex)
     ks = ((g.k1 * g.L1 / (2 * np.pi)) ** 2 + (g.k2 * g.L2 / (2 * np.pi)) ** 2
           + (g.k3 * g.L3 / (2 * np.pi)) ** 2)
     km = np.rint(np.sqrt(ks[:, :, 1:h]))

@@ -338,6 +338,32 @@ class utilitiesClass:
         kmax = tr.shape[0] - 1
         return np.linspace(0, kmax, kmax + 1), tr
 
+    def computeTransfer_2D(self, main, grid, myFFT=None):
+        """``computeTransfer_2D`` (src/Classes.py:1043-1092): the transfer of
+        the k3 = 0 plane binned by rint(|k_h|), u and v components; the same
+        Nyquist side effect on main.uhat/vhat/what as computeTransfer."""
+        N1, N2, N3 = grid.N1, grid.N2, grid.N3
+        main.U[:, N1 // 2, :, :] = 0
+        main.U[:, :, N2 // 2, :] = 0
+        main.U[:, :, :, N3 // 2] = 0
+        tr = grid.ctx(main.precision).transfer(main.U, flags=_capi.TRANSFER_2D)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
+    def computeTransfer_resolved_2D(self, main, grid, myFFT=None):
+        """``computeTransfer_resolved_2D`` (src/Classes.py:1152-1205)."""
+        tr = grid.ctx(main.precision).transfer(main.U, flags=_capi.FILTER_GF | _capi.TRANSFER_2D)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
+    def computeTransfer_SGS_2D(self, main, grid, myFFT=None):
+        """``computeTransfer_SGS_2D`` (src/Classes.py:1241-1270)."""
+        if main.W0 is None:
+            raise ValueError("computeTransfer_SGS_2D needs a closure that keeps w0 (turb_model != 0)")
+        tr = grid.ctx(main.precision).transfer(main.U, w0=main.W0, flags=_capi.TRANSFER_2D)
+        kmax = tr.shape[0] - 1
+        return np.linspace(0, kmax, kmax + 1), tr
+
     def computeSpectrum_resolved(self, main, grid):
         spec = self._spectrum(main, grid, _capi.FILTER_GF)
         N1, N2, N3 = grid.N1, grid.N2, grid.N3

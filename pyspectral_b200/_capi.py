@@ -18,7 +18,7 @@ PSB_ERR_NONFINITE = 6
 DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS = (0, 1, 2, 3, 4, 5, 6, 7, 8,
                                                                                      9, 10)
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
-NORM_SERIAL, NORM_MPI, FILTER_GF = 0, 1, 2
+NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 
 EXPORTS = (
     "psb_ctx_create", "psb_ctx_destroy", "psb_ctx_set_stream", "psb_last_error", "psb_create_error",
@@ -218,11 +218,13 @@ class Context:
 
     def transfer(self, f3, w0=None, flags=0):
         """Complex transfer spectrum (kmax+1 bins) of the 3 fields f3; flags
-        FILTER_GF: of the Gf-filtered fields; w0: the SGS transfer with w0."""
+        FILTER_GF: of the Gf-filtered fields; TRANSFER_2D: the k3 = 0 plane
+        binned by |k_h| (u and v); w0: the SGS transfer with w0."""
         import numpy as np
         self.bind_stream()
         nb = ctypes.c_int()
-        self.check(self.lib.psb_spectrum_nbins(self.h, 0, ctypes.byref(nb)), "psb_spectrum_nbins")
+        self.check(self.lib.psb_spectrum_nbins(self.h, int(flags) & TRANSFER_2D, ctypes.byref(nb)),
+                   "psb_spectrum_nbins")
         out = np.zeros((nb.value, 2), dtype=np.float64)
         self.check(self.lib.psb_transfer(self.h, self._ptr(f3), self._ptr(w0), int(flags),
                                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nb.value),

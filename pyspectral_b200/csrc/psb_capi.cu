@@ -181,9 +181,12 @@ __global__ void __launch_bounds__(256) spectrum_kernel(const Cx<T>* __restrict__
 //    3/2-dealiased products, p = ksqr_i (-k_i k_j P_ij);
 //  mode 1 (computeTransfer_resolved): the same with u -> Gf u (P of Gf u);
 //  mode 2 (computeTransfer_SGS): Re sum_i conj(Gf u_i) W_i (W = w0).
+//  two_d (the *_2D variants, src/Classes.py:1043-1092,1152-1205,1241-1270):
+//  the k3 = 0 plane only, bins rint(sqrt(k1^2 + k2^2)), components u and v,
+//  weight 1.
 template <typename T>
 __global__ void __launch_bounds__(256) transfer_kernel(const Cx<T>* __restrict__ a, const Cx<T>* __restrict__ P,
-                                                       int mode, const double* __restrict__ gx,
+                                                       int mode, int two_d, const double* __restrict__ gx,
                                                        const double* __restrict__ gy, const double* __restrict__ gz,
                                                        const double* __restrict__ kx, const double* __restrict__ ky,
                                                        const double* __restrict__ kz, int N1, int N2, int N3,
@@ -194,22 +197,25 @@ __global__ void __launch_bounds__(256) transfer_kernel(const Cx<T>* __restrict__
        s += (long long)gridDim.x * blockDim.x) {
     const int i3 = (int)(s % n3h);
     if (i3 >= N3 / 2 && i3 != 0) continue;
+    if (two_d && i3 != 0) continue;
     const long long t = s / n3h;
     const int i2 = (int)(t % N2), i1 = (int)(t / N2);
     if (i1 == N1 / 2 || i2 == N2 / 2) continue;
     const long long n1 = i1 < N1 / 2 ? i1 : i1 - N1, n2 = i2 < N2 / 2 ? i2 : i2 - N2, n3 = i3;
-    int bin = (int)(signed char)(long long)rint(sqrt((double)(n1 * n1 + n2 * n2 + n3 * n3)));
+    const double kh = two_d ? sqrt(kx[i1] * kx[i1] + ky[i2] * ky[i2]) : sqrt((double)(n1 * n1 + n2 * n2 + n3 * n3));
+    int bin = (int)(signed char)(long long)rint(kh);
     if (bin < 0) bin += nbins;
     if (bin < 0 || bin >= nbins) continue;
     const double gf = mode ? gx[i1] * gy[i2] * gz[i3] : 1.0;
+    const int ncomp = two_d ? 2 : 3;
+    const double wgt = i3 == 0 ? 1.0 : 2.0;
     if (mode == 2) {
       double re = 0.0;
-#pragma unroll
-      for (int i = 0; i < 3; ++i) {
+      for (int i = 0; i < ncomp; ++i) {
         const Cx<T> u = a[i * fs + s], q = P[i * fs + s];
         re += gf * ((double)u.x * q.x + (double)u.y * q.y);
       }
-      atomicAdd(&spec[2 * bin], (i3 == 0 ? 1.0 : 2.0) * re);
+      atomicAdd(&spec[2 * bin], wgt * re);
       continue;
     }
     const double k[3] = {kx[i1], ky[i2], kz[i3]};
@@ -229,8 +235,7 @@ __global__ void __launch_bounds__(256) transfer_kernel(const Cx<T>* __restrict__
       ph[c] = ksi * (-k[0] * k[0] * pr[0][c] - k[1] * k[1] * pr[1][c] - k[2] * k[2] * pr[2][c] -
                      2.0 * k[0] * k[1] * pr[3][c] - 2.0 * k[0] * k[2] * pr[4][c] - 2.0 * k[1] * k[2] * pr[5][c]);
     double re = 0.0, im = 0.0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < ncomp; ++i) {
       // z = k_j P_ij + k_i p; the advection term is -i z = (z.y, -z.x)
       double zx = k[i] * ph[0], zy = k[i] * ph[1];
 #pragma unroll
@@ -244,9 +249,8 @@ __global__ void __launch_bounds__(256) transfer_kernel(const Cx<T>* __restrict__
       re += ux * ax + uy * ay;  // conj(u) * (-i z)
       im += ux * ay - uy * ax;
     }
-    const double w = i3 == 0 ? 1.0 : 2.0;
-    atomicAdd(&spec[2 * bin], w * re);
-    atomicAdd(&spec[2 * bin + 1], w * im);
+    atomicAdd(&spec[2 * bin], wgt * re);
+    atomicAdd(&spec[2 * bin + 1], wgt * im);
   }
 }
 
@@ -849,7 +853,12 @@ int psb_cross_helicity(psb_ctx* c, const void* u, const void* b, int flags, doub
 
 int psb_spectrum_nbins(const psb_ctx* c, int flags, int* nbins) {
   if (!c || !nbins) return PSB_ERR_ARG;
-  (void)flags;
+  if (flags & PSB_TRANSFER_2D) {
+    // kmax = round(max rint(sqrt(k1^2 + k2^2))) over the k3 = 0 plane (src/Classes.py:1080-1082)
+    const double k1 = ((double)(c->N1 / 2) * 2.0) * M_PI / c->L1, k2 = ((double)(c->N2 / 2) * 2.0) * M_PI / c->L2;
+    *nbins = (int)std::rint(std::sqrt(k1 * k1 + k2 * k2)) + 1;
+    return PSB_OK;
+  }
   // kmax = round(max over k3 in [1, N3/2) of rint(|k|)) (PySpectral/src/Classes.py:764-768)
   const double n1 = c->N1 / 2, n2 = c->N2 / 2, n3 = c->N3 / 2 - 1;
   *nbins = (int)std::rint(std::sqrt(n1 * n1 + n2 * n2 + n3 * n3)) + 1;
@@ -909,11 +918,13 @@ int psb_transfer(psb_ctx* c, const void* f, const void* w0, int flags, double* o
   ++c->launches;
   if (c->prec == 64)
     transfer_kernel<double><<<kRedBlocks, 256, 0, c->stream>>>(
-        reinterpret_cast<const Cx<double>*>(f), reinterpret_cast<const Cx<double>*>(Pp), mode, c->gx, c->gy, c->gz,
+        reinterpret_cast<const Cx<double>*>(f), reinterpret_cast<const Cx<double>*>(Pp), mode,
+        (flags & PSB_TRANSFER_2D) ? 1 : 0, c->gx, c->gy, c->gz,
         c->kx, c->ky, c->kz, c->N1, c->N2, c->N3, nbins, c->red_dev);
   else
     transfer_kernel<float><<<kRedBlocks, 256, 0, c->stream>>>(
-        reinterpret_cast<const Cx<float>*>(f), reinterpret_cast<const Cx<float>*>(Pp), mode, c->gx, c->gy, c->gz,
+        reinterpret_cast<const Cx<float>*>(f), reinterpret_cast<const Cx<float>*>(Pp), mode,
+        (flags & PSB_TRANSFER_2D) ? 1 : 0, c->gx, c->gy, c->gz,
         c->kx, c->ky, c->kz, c->N1, c->N2, c->N3, nbins, c->red_dev);
   PSB_TRY(launch_ok(c, "transfer"));
   PSB_TRY(cuda_ok(c, cudaMemcpyAsync(c->red_host, c->red_dev, sizeof(double) * 2 * nbins, cudaMemcpyDeviceToHost,

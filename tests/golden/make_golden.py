@@ -322,6 +322,13 @@ def gen_serial(N, seed):
     grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t)
     k, tr = util.computeTransfer(main, grid, myFFT)
     out["transfer_k"], out["transfer"] = np.asarray(k), np.asarray(tr)
+    # the k3 = 0-plane variants (:1043-1092, :1152-1205, :1241-1270)
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t)
+    k, tr = util.computeTransfer_2D(main, grid, myFFT)
+    out["transfer2d_k"], out["transfer2d"] = np.asarray(k), np.asarray(tr)
+    grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, kc=N // 4)
+    k, tr = util.computeTransfer_resolved_2D(main, grid, myFFT)
+    out["transfer2d_res"] = np.asarray(tr)
     # resolved transfer (:1093-1150) with kc = N/4, and the SGS transfer
     # (:1206-1239) of the Smagorinsky closure force w0 after one RHS
     grid, myFFT, util, main = serial_case(C, N, st, 0, nu, dt, t, kc=N // 4)
@@ -334,6 +341,8 @@ def gen_serial(N, seed):
     out["transfer_sgs_w0"] = np.stack([main.w0_u[..., 0], main.w0_v[..., 0], main.w0_w[..., 0]])
     k, tr = util.computeTransfer_SGS(main, grid, myFFT)
     out["transfer_sgs"] = np.asarray(tr)
+    k, tr = util.computeTransfer_SGS_2D(main, grid, myFFT)
+    out["transfer2d_sgs"] = np.asarray(tr)
     return out
 
 

@@ -64,3 +64,32 @@ def test_resolved_and_sgs_transfer_match_reference(N, precision, tol):
     k, tr = util.computeTransfer_SGS(main, grid, None)
     np.testing.assert_array_equal(k, d["transfer_k"])
     assert rel(tr, d["transfer_sgs"]) < tol
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-5)])
+def test_2d_transfer_variants_match_reference(N, precision, tol):
+    """computeTransfer_2D / _resolved_2D / _SGS_2D (src/Classes.py:1043-1092,
+    1152-1205, 1241-1270): the k3 = 0 plane binned by |k_h|."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from pyspectral_b200 import Classes as C
+    d = golden(f"serial_N{N}.npz")
+    util = C.utilitiesClass()
+    st = d["state"]
+    grid = C.gridclass.periodic(N)
+    main = C.variables(0, 0, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 1e-3, 0.01, precision=precision)
+    k, tr = util.computeTransfer_2D(main, grid, None)
+    np.testing.assert_array_equal(k, d["transfer2d_k"])
+    assert rel(tr, d["transfer2d"]) < tol
+    grid = C.gridclass.periodic(N, kc=N // 4)
+    main = C.variables(0, 0, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 1e-3, 0.01, precision=precision)
+    _, tr = util.computeTransfer_resolved_2D(main, grid, None)
+    assert rel(tr, d["transfer2d_res"]) < tol
+    su = d["transfer_sgs_u"]
+    main = C.variables(0, 1, 0, 0, 0, 0, grid, su[0], su[1], su[2], 0.0, 1e-3, 0.01, precision=precision)
+    main.W0 = torch.as_tensor(d["transfer_sgs_w0"], device=main.Q.device).to(main.Q.dtype).contiguous()
+    k, tr = util.computeTransfer_SGS_2D(main, grid, None)
+    np.testing.assert_array_equal(k, d["transfer2d_k"])
+    assert rel(tr, d["transfer2d_sgs"]) < tol

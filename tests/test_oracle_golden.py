@@ -166,6 +166,21 @@ def test_transfer_matches_reference(N):
 
 
 @pytest.mark.parametrize("N", [12, 16])
+def test_transfer_2d_matches_reference(N):
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    k, tr = orc.transfer(g, d["state"], two_d=True)
+    np.testing.assert_array_equal(k, d["transfer2d_k"])
+    assert rel(tr, d["transfer2d"]) < 1e-13
+    gq = orc.Grid.periodic(N, kc=N // 4)
+    _, tr = orc.transfer(gq, d["state"], filtered=True, two_d=True)
+    assert rel(tr, d["transfer2d_res"]) < 1e-13
+    _, tr = orc.transfer(gq, d["transfer_sgs_u"], w0=d["transfer_sgs_w0"], two_d=True)
+    assert np.abs(d["transfer2d_sgs"]).max() > 1e-5
+    assert rel(tr, d["transfer2d_sgs"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
 def test_mhd_matches_reference(N):
     d = golden(f"mhd_N{N}.npz")
     g = orc.MHDGrid(N, N, N, N // 2)
