@@ -47,6 +47,12 @@ extern "C" {
                              6 fields u,v,w,w0_u,w0_v,w0_w; du/dt = unpad_2x(PLu) + w0,
                              dw0/dt = PLQLu - 250 nu k^2 w0; w0_v read as zero like the
                              reference's Q2U (src/Classes.py:489); no rotating form           */
+#define PSB_FM1 11        /* turb_model 3      -> computeRHS_FM1    (src/RHSfunctions.py:882-1024):
+                             3 + 3 p.fm_nsub fields u, then (w0_u, w0_v, w0_w) per
+                             subintegration; du/dt = unpad_2x(PLu) + sum_i w0_i,
+                             dw0_i/dt = -2/d w0_i + (-1)^(i+1) 2 PLQLu + S_i, d = dt0/nsub,
+                             S_i the running sum of :1010-1014; w0 (3 p.fm_nsub fields)
+                             receives the memory variables as read; no rotating form        */
 #define PSB_BUDGETS 10    /* turb_model 99     -> computeRHS_BUDGETS (src/RHSfunctions.py:1543-1661):
                              RHS = unpad_2x(PLu); w0 receives PLQLu with the q part split at
                              p.kf (0 -> int(max k1), main.kc of src/Classes.py:16); no
@@ -89,6 +95,8 @@ typedef struct {
   double les_delta;       /* PSB_LEARNED: filter width fed to the MLP; <=0 -> (dx dy dz)^(1/3) */
   int mlp_act;            /* PSB_LEARNED: hidden activation of the model, PSB_ACT_GELU or PSB_ACT_RELU */
   int mlp_hidden;         /* PSB_LEARNED: hidden width of the model, 32 or 64 (0 = 64) */
+  double fm_dt0;          /* PSB_FM1: memory length dt0 (src/Classes.py:236-241; default 0.1) */
+  int fm_nsub;            /* PSB_FM1: dt0_subintegrations, 1..8 (0 = 1) (src/Classes.py:243-248) */
 } psb_params;
 
 /* Hidden activation of the learned closure's MLP (a property of the trained model). */
@@ -109,7 +117,8 @@ const char* psb_create_error(void);
 
 /* One right-hand-side evaluation: main.computeRHS(main,grid,myFFT,utilities)
  * (src/Classes.py:44,95,124,186,227; src_MPI/Classes.py:147).
- * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD, PSB_MHD_TMODEL, PSB_CM1).
+ * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD, PSB_MHD_TMODEL, PSB_CM1;
+ * 3 + 3 p.fm_nsub for PSB_FM1).
  * w0       : optional closure force main.w0_u/v/w (3 fields; 6 fields u then B for
  *            PSB_MHD_TMODEL) or NULL.
  * read_out : optional copy of the state as the RHS read it (the reference

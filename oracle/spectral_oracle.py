@@ -485,6 +485,36 @@ def rhs_tmodel(g, state, p):
     return r, w0, ur
 
 
+def rhs_fm1(g, state, p, dt0=0.1, nsub=1):
+    """First-order finite memory model, ``computeRHS_FM1``
+    (``src/RHSfunctions.py:882-1024``) on the state ``(u, v, w)`` followed by
+    ``(w0_u, w0_v, w0_w)`` of each of the ``nsub`` subintegrations:
+    ``du/dt = unpad_2x(PL u) + sum_i w0^i``,
+    ``dw0^i/dt = -2/d w0^i + (-1)^(i+1) 2 PLQL u + S_i`` with ``d = dt0/nsub``
+    and ``S_i`` the running sum of ``:1010-1014`` (not reset between i).
+
+    The reference source calls ``pad_2x_var``, which none of its files
+    defines; this restatement (and the fixtures) use ``pad_2x`` there.  Only
+    the non-rotating form (its rotating form adds the Coriolis force to PL
+    before the mode split, ``:959-962``).
+
+    Returns ``(rhs, w0_read, uhat_read)``, ``w0_read`` the first
+    subintegration's memory variables (``main.w0_*[..., 0]``)."""
+    if p.rotate == 1:
+        raise NotImplementedError("rotating FM1 is not restated")
+    r, _, ur, PLQL, _ = _memory_rhs(g, state[:3], p, lambda *a: (0.0, None))
+    w = [state[3 + 3 * i:6 + 3 * i] for i in range(nsub)]
+    d = dt0 / nsub
+    out = [r[c] + np.sum(np.stack([w[i][c] for i in range(nsub)], axis=-1), axis=-1) for c in range(3)]
+    run = [np.zeros_like(r[0]) for _ in range(3)]
+    for i in range(1, nsub + 1):
+        for j in range(1, i):
+            for c in range(3):
+                run[c] = run[c] + 4.0 / d * (-1.0) ** (i + j + 1) * w[j - 1][c]
+        out += [-2.0 / d * w[i - 1][c] + (-1.0) ** (i + 1) * 2.0 * PLQL[c] + run[c] for c in range(3)]
+    return np.stack(out), np.stack(w[0]), ur
+
+
 def rhs_cm1(g, state, p):
     """First-order complete memory model, ``computeRHS_CM1``
     (``src/RHSfunctions.py:1411-1542``) on the state ``(u, v, w, w0_u, w0_v,

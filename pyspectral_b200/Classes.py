@@ -135,7 +135,9 @@ class variables:
     (src/Classes.py:7-229).
 
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
-    'Dynamic tau-model', 6 (first-order complete memory model, state
+    'Dynamic tau-model', 3 (first-order finite memory model, state
+    ``Q = (u, v, w)`` then ``(w0_u, w0_v, w0_w)`` per subintegration; dt0 and
+    dt0_subintegrations as in the reference), 6 (first-order complete memory model, state
     ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky), 99 (DNS
     with SGS budgets: ``utilitiesClass``'s hooks write ``budget<it>.npz``
     every 20 iterations).  ``precision`` (64 or 32) selects FP64 or FP32
@@ -166,6 +168,14 @@ class variables:
             # state (src/Classes.py:460-475), initially zero
             self.Q = torch.cat([self.Q, torch.zeros_like(self.Q)]).contiguous()
             self.nvars = 6
+        self.fm_dt0, self.fm_nsub = 0.0, 0
+        if turb_model == 3:
+            # finite memory model: dt0 (default 0.1) split into dt0_subintegrations
+            # memory variables (src/Classes.py:233-268), initially zero
+            self.fm_dt0 = 0.1 if dt0 == -10 else float(dt0)
+            self.fm_nsub = 1 if dt0_subintegrations == -10 else int(dt0_subintegrations)
+            self.Q = torch.cat([self.Q] + [torch.zeros_like(self.Q)] * self.fm_nsub).contiguous()
+            self.nvars = 3 + 3 * self.fm_nsub
         self.Ct = 0.1 if Ct == -10 else float(Ct)
         self.tau_a, self.tau_b = float(dt0), float(dt1)
         self.tau = 0.0
@@ -174,7 +184,7 @@ class variables:
         use_kahan = (precision == 32) if kahan is None else bool(kahan)
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
-        table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel,
+        table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel, 3: R.computeRHS_FM1,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
                  6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, 99: R.computeRHS_BUDGETS,
                  "learned": R.computeRHS_learned}
@@ -188,7 +198,7 @@ class variables:
             from .learned import MLPModel
             self.model = MLPModel.load(device=grid.device)
         if turb_model not in (0, "learned"):
-            self.W0 = torch.zeros_like(self.U)
+            self.W0 = torch.zeros_like(self.Q[3:] if turb_model == 3 else self.U)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
         if turb_model == "Static tau-model":
@@ -210,23 +220,37 @@ class variables:
     def what(self):
         return self.U[2]
 
+    def _w0(self, c):
+        if self.W0 is None:
+            return None
+        if self.turb_model == 3:  # FM1: one memory variable per subintegration, (N1, N2, N3/2+1, nsub)
+            return self.W0[c::3].permute(1, 2, 3, 0)
+        return self.W0[c].unsqueeze(-1)
+
     @property
     def w0_u(self):
-        return None if self.W0 is None else self.W0[0].unsqueeze(-1)
+        return self._w0(0)
 
     @property
     def w0_v(self):
-        return None if self.W0 is None else self.W0[1].unsqueeze(-1)
+        return self._w0(1)
 
     @property
     def w0_w(self):
-        return None if self.W0 is None else self.W0[2].unsqueeze(-1)
+        return self._w0(2)
 
     def U2Q(self):
         self.Q[:3].copy_(self.U)
+        if self.turb_model in (3, 6):  # memory models: w0 is state (src/Classes.py:253-259,476-482)
+            self.Q[3:].copy_(self.W0)
 
     def Q2U(self):
         self.U.copy_(self.Q[:3])
+        if self.turb_model == 3:
+            self.W0.copy_(self.Q[3:])
+        elif self.turb_model == 6:  # w0_v read from a slice nothing writes (src/Classes.py:489)
+            self.W0.copy_(self.Q[3:6])
+            self.W0[1].zero_()
 
     def params(self):
         m = self.model
@@ -236,11 +260,13 @@ class variables:
                                  mlp_params=m.params.data_ptr() if m is not None else None,
                                  mlp_norm=m.norm.data_ptr() if m is not None else None,
                                  les_delta=self.les_delta, mlp_act=m.act if m is not None else 0,
-                                 mlp_hidden=m.hidden if m is not None else 0)
+                                 mlp_hidden=m.hidden if m is not None else 0, fm_dt0=self.fm_dt0,
+                                 fm_nsub=self.fm_nsub)
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, 6: _capi.CM1, 7: _capi.DSMAG, 99: _capi.BUDGETS,
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 6: _capi.CM1, 7: _capi.DSMAG,
+                99: _capi.BUDGETS,
                 "learned": _capi.LEARNED}[self.turb_model]
 
 

@@ -47,6 +47,14 @@ def computeRHS_Dtaumodel(main, grid, myFFT=None, utilities=None):
     main.tau = _rhs(main, grid, _capi.TAU_DYNAMIC)
 
 
+def computeRHS_FM1(main, grid, myFFT=None, utilities=None):
+    """First-order finite memory model (turb_model 3), src/RHSfunctions.py:882-1024:
+    ``main.Q`` holds u and the memory variables of each subintegration and
+    becomes their right-hand sides; ``main.w0_*`` view the memory variables
+    ``(N1, N2, N3/2+1, dt0_subintegrations)``.  No rotating form is built."""
+    _rhs(main, grid, _capi.FM1)
+
+
 def computeRHS_CM1(main, grid, myFFT=None, utilities=None):
     """First-order complete memory model (turb_model 6),
     src/RHSfunctions.py:1411-1542: ``main.Q`` holds (u, v, w, w0_u, w0_v,

@@ -15,8 +15,8 @@ LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
 
 PSB_OK = 0
 PSB_ERR_NONFINITE = 6
-DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS = (0, 1, 2, 3, 4, 5, 6, 7, 8,
-                                                                                     9, 10)
+DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS, FM1 = (
+    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11)
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 
@@ -46,7 +46,8 @@ class Params(ctypes.Structure):
                 ("tau_b", ctypes.c_double), ("kf", ctypes.c_int), ("rotate", ctypes.c_int),
                 ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
                 ("force", ctypes.c_void_p), ("mlp_params", ctypes.c_void_p), ("mlp_norm", ctypes.c_void_p),
-                ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int), ("mlp_hidden", ctypes.c_int)]
+                ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int), ("mlp_hidden", ctypes.c_int),
+                ("fm_dt0", ctypes.c_double), ("fm_nsub", ctypes.c_int)]
 
 
 _lib = None
@@ -102,10 +103,10 @@ def load(path: str = LIB_PATH):
 
 def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
                 Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0,
-                mlp_act=0, mlp_hidden=0) -> Params:
+                mlp_act=0, mlp_hidden=0, fm_dt0=0.0, fm_nsub=0) -> Params:
     return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
                   int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force, mlp_params, mlp_norm,
-                  float(les_delta), int(mlp_act), int(mlp_hidden))
+                  float(les_delta), int(mlp_act), int(mlp_hidden), float(fm_dt0), int(fm_nsub))
 
 
 class Context:
@@ -165,7 +166,7 @@ class Context:
         return nfields * self.N1 * self.N2 * (self.N3 // 2 + 1)
 
     def rhs(self, closure, state, rhs, params, w0=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else 3
+        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else (3 + 3 * max(1, params.fm_nsub) if closure == FM1 else 3)
         self.bind_stream()
         tau = ctypes.c_double(0.0)
         st = self.lib.psb_rhs(self.h, closure, self._ptr(state, self.spec_numel(nf)),
@@ -175,7 +176,7 @@ class Context:
         return tau.value
 
     def step(self, closure, state, params, nsteps=1, comp=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else 3
+        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else (3 + 3 * max(1, params.fm_nsub) if closure == FM1 else 3)
         self.bind_stream()
         st = self.lib.psb_step_rk4(self.h, closure, self._ptr(state, self.spec_numel(nf)), self._ptr(comp),
                                    self._ptr(read_out), ctypes.byref(params), int(nsteps))

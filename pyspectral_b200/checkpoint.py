@@ -67,7 +67,7 @@ def solution_arrays(main):
            "Q": _np(main.Q)}
     if getattr(main, "comp", None) is not None:
         out["comp"] = _np(main.comp)
-    if getattr(main, "W0", None) is not None:
+    if getattr(main, "w0_u", None) is not None:
         out["w0_u"] = _np(main.w0_u).astype(np.complex128)
         out["w0_v"] = _np(main.w0_v).astype(np.complex128)
         out["w0_w"] = _np(main.w0_w).astype(np.complex128)

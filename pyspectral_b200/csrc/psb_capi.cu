@@ -747,7 +747,8 @@ int psb_ctx_set_stream(psb_ctx* c, void* stream) {
 
 const char* psb_last_error(const psb_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-static int closure_fields(int closure) {
+static int closure_fields(int closure, const psb_params* p) {
+  if (closure == PSB_FM1) return 3 + 3 * (p && p->fm_nsub > 0 ? p->fm_nsub : 1);
   return closure == PSB_MHD || closure == PSB_MHD_TMODEL || closure == PSB_CM1 ? 6 : 3;
 }
 
@@ -770,7 +771,7 @@ int psb_prepare(psb_ctx* c, int closure) {
   p.nu = 0;
   p.eta = -1;
   PSB_TRY(set_device(c));
-  const size_t n = (size_t)closure_fields(closure) * c->N1 * c->N2 * c->N3h;
+  const size_t n = (size_t)closure_fields(closure, &p) * c->N1 * c->N2 * c->N3h;
   int st = PSB_OK;
   if (c->prec == 64) {
     scratch<double>(c, "rk.Q0", n, &st);
@@ -789,7 +790,7 @@ int psb_step_rk4(psb_ctx* c, int closure, void* state, void* comp, void* read_ou
   if (!state || !p || nsteps < 0) return fail(c, PSB_ERR_ARG, "psb_step_rk4: bad argument");
   PSB_TRY(set_device(c));
   const double rk[4] = {1. / 4, 1. / 3, 1. / 2, 1.};
-  const size_t n = (size_t)closure_fields(closure) * c->N1 * c->N2 * c->N3h;
+  const size_t n = (size_t)closure_fields(closure, p) * c->N1 * c->N2 * c->N3h;
   int st = PSB_OK;
   for (int s = 0; s < nsteps; ++s) {
     for (int i = 0; i < 4; ++i) {

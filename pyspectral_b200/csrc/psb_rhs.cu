@@ -975,6 +975,92 @@ int cm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
 }
 
 // ---------------------------------------------------------------------------
+// First-order finite memory model (PySpectral/src/RHSfunctions.py:882-1024) on
+// the state (u, v, w, w0_u^1, w0_v^1, w0_w^1, ..., w0_w^n), n = fm_nsub:
+//   du/dt    = unpad_2x(PL u) + sum_i w0^i
+//   dw0^i/dt = -2/d w0^i + (-1)^(i+1) 2 PLQL u + S_i,  d = dt0/n,
+// S_i = sum_{i'<=i} sum_{j<i'} 4/d (-1)^(i'+j+1) w0^j (the reference's running
+// sum is not reset between i).  PL, PLQL: the t-model's pipelines.
+// ---------------------------------------------------------------------------
+constexpr int kFmMaxSub = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256) fm1_combine_kernel(StepIO<T> io, const Cx<T>* __restrict__ PLp,
+                                                          const Cx<T>* __restrict__ PLQL, int nsub, T m2d, T p4d,
+                                                          int N1, int N2, int N3) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    if (io.read_out) {
+      const int i3 = (int)(s % io.n3h);
+      const long long t = s / io.n3h;
+      const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+      const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> w0[kFmMaxSub];
+      Cx<T> sum = mk<T>(0, 0);
+      for (int i = 0; i < nsub; ++i) {
+        w0[i] = io.Q[(3 + 3 * i + c) * fs + s];
+        sum = sum + w0[i];
+        if (io.w0_out) io.w0_out[(3 * i + c) * fs + s] = w0[i];  // the memory variables as read
+      }
+      const Cx<T> plql = PLQL[c * fs + s];
+      io.finish(s, c, PLp[c * fs + s] + sum);
+      Cx<T> run = mk<T>(0, 0);
+      for (int i = 1; i <= nsub; ++i) {
+        for (int j = 1; j < i; ++j) run = run + (((i + j + 1) & 1) ? -p4d : p4d) * w0[j - 1];
+        const T sgn2 = ((i + 1) & 1) ? (T)-2 : (T)2;
+        io.finish(s, 3 + 3 * (i - 1) + c, (m2d * w0[i - 1] + sgn2 * plql) + run);
+      }
+    }
+  }
+}
+
+template <typename T>
+int fm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
+  if (p->rotate)
+    return fail(c, PSB_ERR_UNSUPPORTED, "PSB_FM1: the rotating form (Coriolis inside PL before the split) is not built");
+  const int nsub = p->fm_nsub > 0 ? p->fm_nsub : 1;
+  if (nsub > kFmMaxSub) return fail(c, PSB_ERR_ARG, "PSB_FM1: fm_nsub must be 1..8");
+  const double dt0 = p->fm_dt0 > 0 ? p->fm_dt0 : 0.1;
+  const double d = dt0 / nsub;
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* PLp = scratch<T>(c, "mem.PLp", (size_t)3 * fs, &st);
+  Cx<T>* PLQL = scratch<T>(c, "fm1.PLQL", (size_t)3 * fs, &st);
+  if (st != PSB_OK) return st;
+  const Cx<T>* Qin = io.Q;
+  MemCfg m{"memu", nullptr, 0, true, false, 0};
+  if (Qin) PSB_TRY(cuda_ok(c, cudaMemsetAsync(PLp, 0, sizeof(Cx<T>) * 3 * fs, c->stream), "memset"));
+  Cx<T>*B2 = nullptr, *E = nullptr;
+  PSB_TRY(run_pl<T>(c, Qin, p, m, &B2, &E, PLp, nullptr));
+  EpiPLQL<T> epi{};
+  epi.io = io;
+  epi.k = ktabs<T>(c->kx, c->ky, c->kz);
+  epi.PLp = PLp;
+  epi.coef = (T)0;
+  epi.ny1 = N1 / 2;
+  epi.ny2 = N2 / 2;
+  epi.ny3 = N3 / 2;
+  epi.plql_out = PLQL;
+  PSB_TRY(run_plql<T>(c, m, Qin ? B2 : nullptr, E, epi));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "fm1 combine", (double)sizeof(Cx<T>) * fs * (3 + 3 * nsub) * 2 + sizeof(Cx<T>) * fs * 6);
+    fm1_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, PLp, PLQL, nsub, (T)(-2. / d), (T)(4. / d), N1, N2,
+                                                         N3);
+  }
+  return launch_ok(c, "fm1 combine");
+}
+
+// ---------------------------------------------------------------------------
 // DNS with SGS budgets (PySpectral/src/RHSfunctions.py:1543-1661, turb_model 99):
 // RHS = unpad_2x(PL u); PLQL u with the q part split at main.kc
 // (seperateModesBudgets, src/padding.py:81-93) is stored for the budget files.
@@ -1203,6 +1289,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       return cm1_rhs<T>(c, io, p);
     case PSB_BUDGETS:
       return budgets_rhs<T>(c, io, p);
+    case PSB_FM1:
+      return fm1_rhs<T>(c, io, p);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

@@ -20,7 +20,10 @@ This script executes its unmodified sources under a load-time shim:
   Smagorinsky model calls it with ``kc/2.`` (``src/RHSfunctions.py:1697``),
   a float slice bound that the NumPy of the reference's day truncated and
   NumPy 2 rejects; ``seperateModesBudgets`` likewise (the budget RHS passes
-  the float ``main.kc = np.amax(grid.k1)``, ``src/Classes.py:16``).
+  the float ``main.kc = np.amax(grid.k1)``, ``src/Classes.py:16``);
+* ``pad_2x_var``, called by ``computeRHS_FM1`` but defined in no file of
+  the reference, is bound to ``pad_2x`` (the FM1 fixtures hold under that
+  assumption only).
 
 ``advanceQ_RK4`` lives in the driver script, which runs a whole simulation at
 import time, so its four lines (``src/PySpec_3d.py:96-105``) are restated in
@@ -170,6 +173,8 @@ def load_serial():
     for k, v in pad.__dict__.items():  # "from padding import *"
         if not k.startswith("__"):
             rhs.__dict__.setdefault(k, v)
+    # computeRHS_FM1 calls pad_2x_var, which no file of the reference defines
+    rhs.__dict__.setdefault("pad_2x_var", pad.pad_2x)
     _split = pad.seperateModesBudgets
     rhs.__dict__["seperateModesBudgets"] = lambda uhat_pad, arrange, kc: _split(uhat_pad, arrange, int(kc))
     cls = _load(os.path.join(SRC, "Classes.py"), "Classes")
@@ -213,7 +218,7 @@ def _diag(Q, nv=3):
 
 
 def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), Ct=-10, dt0=-10,
-                dt1=-10, kc=None, cfl=None):
+                dt1=-10, kc=None, cfl=None, dt0s=-10):
     kc = N // 2 if kc is None else kc
     x, y, z = orc.periodic_coords(N)
     grid = C.gridclass(N, N, N, x, y, z, kc, 2 * np.pi, 2 * np.pi, 2 * np.pi)
@@ -224,7 +229,7 @@ def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), C
     cfl = -dt if cfl is None else cfl
     with contextlib.redirect_stdout(io.StringIO()):
         main = C.variables(0, turb_model, rotate, Om[0], Om[1], Om[2], grid, state[0].copy(),
-                           state[1].copy(), state[2].copy(), t, dt, nu, Ct, dt0, -10, dt1, -10, cfl, 3)
+                           state[1].copy(), state[2].copy(), t, dt, nu, Ct, dt0, dt0s, dt1, -10, cfl, 3)
     main.iteration = 1
     return grid, myFFT, util, main
 
@@ -249,6 +254,7 @@ def gen_serial(N, seed):
         ("dsmag_kc", 7, dict(kc=N // 2 - 1)),         # kc/2 fractional: truncated cutoff
         ("cm1", 6, {}),
         ("budgets", 99, {}),
+        ("fm1", 3, dict(dt0=0.05)),
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)
@@ -285,6 +291,21 @@ def gen_serial(N, seed):
             out["budgetfile_step"] = _diag(main.Q)
         finally:
             os.chdir(cwd)
+    # FM1 with three subintegrations from non-zero memory variables
+    w0fm = 0.2 * np.stack([orc.isotropic_state(N, seed + 200 + i, k0=2.0) for i in range(3)])
+    out["fm1w_init"] = w0fm
+    for stage in ("rhs", "step"):
+        grid, myFFT, util, main = serial_case(C, N, st, 3, nu, dt, t, dt0=0.08, dt0s=3)
+        for i in range(3):
+            main.w0_u[..., i], main.w0_v[..., i], main.w0_w[..., i] = w0fm[i]
+        main.U2Q()
+        with contextlib.redirect_stdout(io.StringIO()):
+            if stage == "rhs":
+                main.computeRHS(main, grid, myFFT, util)
+                out["fm1w_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+            else:
+                ref_rk4_step(main, grid, myFFT, util)
+        out[f"fm1w_{stage}"] = _diag(main.Q, 12)
     # CM1 from a state with non-zero memory variables (set, then U2Q)
     w0init = 0.3 * orc.isotropic_state(N, seed + 100, k0=2.0)
     out["cm1w_init"] = w0init

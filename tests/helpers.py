@@ -21,6 +21,7 @@ CASES = {
     "dsmag_rot": (7, dict(rotate=1, Om=(-0.15, 0.35, 0.2)), dict(rotate=1, Om=(-0.15, 0.35, 0.2))),
     "cm1": (6, {}, {}),
     "budgets": (99, {}, {}),
+    "fm1": (3, dict(dt0=0.05), {}),
 }
 NU, DT, T = 0.02, 0.01, 0.37
 

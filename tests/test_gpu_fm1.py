@@ -1,0 +1,78 @@
+"""GPU parity of the first-order finite memory model (turb_model 3,
+PySpectral/src/RHSfunctions.py:882-1024) with three subintegrations from
+non-zero memory variables; the fixtures were made with pad_2x standing in for
+the reference's undefined pad_2x_var.  The fresh-state case runs in
+test_gpu_parity.py."""
+import numpy as np
+import pytest
+
+from tests.helpers import DT, NU, T, golden, rel
+
+pytestmark = pytest.mark.gpu
+TOL64 = 1e-12
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def _main(d, N, precision=64, rotate=0, nsub=3):
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    grid = C.gridclass.periodic(N)
+    st = d["state"]
+    main = C.variables(0, 3, rotate, 0.1, 0.2, 0.3, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.08,
+                       dt0_subintegrations=nsub, precision=precision)
+    # as the reference's case setup would: fill main.w0_* then U2Q (src/Classes.py:253-259)
+    init = torch.as_tensor(d["fm1w_init"][:nsub], device=main.Q.device).to(main.Q.dtype)
+    for i in range(nsub):
+        main.w0_u[..., i], main.w0_v[..., i], main.w0_w[..., i] = init[i]
+    main.U2Q()
+    return grid, main
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_fm1_three_subintegrations_match_reference(N):
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advanceQ_RK4
+    d = golden(f"serial_N{N}.npz")
+    grid, main = _main(d, N)
+    assert main.Q.shape[0] == 12 and main.nvars == 12
+    assert tuple(main.w0_u.shape) == (N, N, N // 2 + 1, 3)
+    Q0 = np_(main.Q)
+    main.computeRHS(main, grid, None, None)
+    assert rel(np_(main.Q), d["fm1w_rhs"]) < TOL64
+    assert rel(np_(main.U), d["fm1w_uhat"]) < TOL64
+    # main.w0_* hold the memory variables the RHS read
+    assert rel(np_(main.w0_v.permute(3, 0, 1, 2)), Q0[4::3]) == 0
+    grid, main = _main(d, N)
+    advanceQ_RK4(main, grid, None, C.utilitiesClass())
+    assert rel(np_(main.Q), d["fm1w_step"]) < TOL64
+
+
+def test_fm1_fp32_tracks_fp64():
+    d = golden("serial_N16.npz")
+    grid, m64 = _main(d, 16)
+    grid32, m32 = _main(d, 16, precision=32)
+    m64.computeRHS(m64, grid, None, None)
+    m32.computeRHS(m32, grid32, None, None)
+    assert rel(np_(m32.Q).astype(np.complex128), np_(m64.Q)) < 2e-5
+
+
+def test_fm1_rejects_rotation_and_too_many_subintegrations():
+    d = golden("serial_N12.npz")
+    grid, main = _main(d, 12, rotate=1)
+    with pytest.raises(RuntimeError, match="rotating form"):
+        main.computeRHS(main, grid, None, None)
+    from pyspectral_b200 import Classes as C
+    st = d["state"]
+    main = C.variables(0, 3, 0, 0, 0, 0, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.08, dt0_subintegrations=9)
+    with pytest.raises(RuntimeError, match="fm_nsub"):
+        main.computeRHS(main, grid, None, None)

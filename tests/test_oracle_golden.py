@@ -8,7 +8,8 @@ from oracle import spectral_oracle as orc
 from tests.helpers import CASES, DT, NU, T, golden, rel
 
 FN = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "stau": orc.rhs_staumodel,
-      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag, "cm1": orc.rhs_cm1, "budgets": orc.rhs_budgets}
+      "dtau": orc.rhs_dtaumodel, "dsmag": orc.rhs_dsmag, "cm1": orc.rhs_cm1, "budgets": orc.rhs_budgets,
+      "fm1": lambda g, st, p: orc.rhs_fm1(g, st, p, dt0=0.05)}
 
 
 def _fn(name):
@@ -31,7 +32,7 @@ def test_rhs_and_step_match_reference(N, name):
     g = orc.Grid.periodic(N)
     p = orc.Params(nu=NU, t=T, dt=DT, **CASES[name][2])
     st = d["state"]
-    if CASES[name][0] == 6:  # complete memory model: memory variables start at zero
+    if CASES[name][0] in (3, 6):  # memory models: the memory variables start at zero
         st = np.concatenate([st, np.zeros_like(st)])
     res = _fn(name)(g, st, p)
     assert rel(res[0], d[f"{name}_rhs"]) < 1e-13
@@ -109,6 +110,22 @@ def test_budgets_match_reference(N):
         assert rel((w1[i] - w0[i]) / DT, d[f"budgetfile_w0_{c}dot"][..., 0]) < 1e-12
     with pytest.raises(ValueError):
         orc.rhs_budgets(g, st, orc.Params(nu=NU, rotate=1, Om=(0.1, 0.2, 0.3)))
+
+
+@pytest.mark.parametrize("N", [12, 16])
+def test_fm1_three_subintegrations_match_reference(N):
+    """FM1 with dt0 = 0.08 in three subintegrations from non-zero memory
+    variables (fixtures made with pad_2x for the reference's undefined
+    pad_2x_var)."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    st = np.concatenate([d["state"], d["fm1w_init"].reshape(9, *d["state"].shape[1:])])
+    r, _, ur = orc.rhs_fm1(g, st, p, dt0=0.08, nsub=3)
+    assert rel(r, d["fm1w_rhs"]) < 1e-13
+    assert rel(ur, d["fm1w_uhat"]) < 1e-13
+    Q, _ = orc.advance_rk4(st, lambda q: (orc.rhs_fm1(g, q, p, dt0=0.08, nsub=3)[0], q), DT)
+    assert rel(Q, d["fm1w_step"]) < 1e-13
 
 
 def test_myfilter_slice_semantics():
