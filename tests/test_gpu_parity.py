@@ -118,7 +118,7 @@ def test_mhd_matches_reference(N):
 
 
 @pytest.mark.parametrize("shape", [(16, 24, 12), (24, 16, 32)])
-@pytest.mark.parametrize("name", ["dns_rot", "smag", "tmodel"])
+@pytest.mark.parametrize("name", ["dns_rot", "smag", "tmodel", "dsmag", "cm1", "budgets", "fm1"])
 def test_noncubic_grid_matches_oracle(shape, name):
     torch = _torch()
     from pyspectral_b200 import Classes as C
@@ -132,8 +132,11 @@ def test_noncubic_grid_matches_oracle(shape, name):
     g = orc.Grid(N1, N2, N3, L / N1, L / N2, L / N3, min(N1, N2, N3) // 2)
     tm, kw, okw = CASES[name]
     p = orc.Params(nu=NU, t=T, dt=DT, **okw)
-    fn = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel}[name.split("_")[0]]
-    ref = fn(g, st, p)[0]
+    fn = {"dns": orc.rhs_nosgs, "smag": orc.rhs_smag, "tmodel": orc.rhs_tmodel, "dsmag": orc.rhs_dsmag,
+          "cm1": orc.rhs_cm1, "budgets": orc.rhs_budgets,
+          "fm1": lambda g, s, p: orc.rhs_fm1(g, s, p, dt0=0.05)}[name.split("_")[0]]
+    ost = np.concatenate([st, np.zeros_like(st)]) if tm in (3, 6) else st
+    ref = fn(g, ost, p)[0]
     a1, a2, a3 = (np.arange(n) * (L / n) for n in shape)
     y, x, z = np.meshgrid(a2, a1, a3)
     grid = C.gridclass(N1, N2, N3, x, y, z, min(N1, N2, N3) // 2)
