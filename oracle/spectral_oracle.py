@@ -494,14 +494,14 @@ def rhs_fm1(g, state, p, dt0=0.1, nsub=1):
     and ``S_i`` the running sum of ``:1010-1014`` (not reset between i).
 
     The reference source calls ``pad_2x_var``, which none of its files
-    defines; this restatement (and the fixtures) use ``pad_2x`` there.  Only
-    the non-rotating form (its rotating form adds the Coriolis force to PL
-    before the mode split, ``:959-962``).
+    defines; this restatement (and the fixtures) use ``pad_2x`` there.  With
+    rotation the reference adds the Coriolis force to PL on the 2x grid before
+    the mode split (``:959-962``); that force lives on the resolved modes only
+    (``pad_2x`` of the Nyquist-zeroed state), so PL_q and PLQL are unchanged
+    and the force joins the velocity RHS, as in ``_memory_rhs``.
 
     Returns ``(rhs, w0_read, uhat_read)``, ``w0_read`` the first
     subintegration's memory variables (``main.w0_*[..., 0]``)."""
-    if p.rotate == 1:
-        raise NotImplementedError("rotating FM1 is not restated")
     r, _, ur, PLQL, _ = _memory_rhs(g, state[:3], p, lambda *a: (0.0, None))
     w = [state[3 + 3 * i:6 + 3 * i] for i in range(nsub)]
     d = dt0 / nsub

@@ -51,7 +51,7 @@ def computeRHS_FM1(main, grid, myFFT=None, utilities=None):
     """First-order finite memory model (turb_model 3), src/RHSfunctions.py:882-1024:
     ``main.Q`` holds u and the memory variables of each subintegration and
     becomes their right-hand sides; ``main.w0_*`` view the memory variables
-    ``(N1, N2, N3/2+1, dt0_subintegrations)``.  No rotating form is built."""
+    ``(N1, N2, N3/2+1, dt0_subintegrations)``."""
     _rhs(main, grid, _capi.FM1)
 
 

@@ -980,25 +980,37 @@ int cm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
 //   du/dt    = unpad_2x(PL u) + sum_i w0^i
 //   dw0^i/dt = -2/d w0^i + (-1)^(i+1) 2 PLQL u + S_i,  d = dt0/n,
 // S_i = sum_{i'<=i} sum_{j<i'} 4/d (-1)^(i'+j+1) w0^j (the reference's running
-// sum is not reset between i).  PL, PLQL: the t-model's pipelines.
+// sum is not reset between i).  PL, PLQL: the t-model's pipelines.  With
+// rotation the reference adds 2 u x Om to PL on the 2x grid before the mode
+// split (:959-962); it is non-zero on the resolved modes only, so PL_q and PLQL
+// are unchanged and it joins the velocity RHS.
 // ---------------------------------------------------------------------------
 constexpr int kFmMaxSub = 8;
 
 template <typename T>
 __global__ void __launch_bounds__(256) fm1_combine_kernel(StepIO<T> io, const Cx<T>* __restrict__ PLp,
                                                           const Cx<T>* __restrict__ PLQL, int nsub, T m2d, T p4d,
-                                                          int N1, int N2, int N3) {
+                                                          int rotate, T Om1, T Om2, T Om3, int N1, int N2, int N3) {
   const long long fs = io.fstride;
   const long long npts = (long long)N1 * N2 * io.n3h;
   for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
        s += (long long)gridDim.x * blockDim.x) {
-    if (io.read_out) {
-      const int i3 = (int)(s % io.n3h);
-      const long long t = s / io.n3h;
-      const int i2 = (int)(t % N2), i1 = (int)(t / N2);
-      const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+    const int i3 = (int)(s % io.n3h);
+    const long long t = s / io.n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+    Cx<T> ur[3];
 #pragma unroll
-      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+    for (int f = 0; f < 3; ++f) ur[f] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+    if (io.read_out) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = ur[f];
+    }
+    Cx<T> cor[3] = {mk<T>(0, 0), mk<T>(0, 0), mk<T>(0, 0)};
+    if (rotate) {
+      cor[0] = (T)2 * (Om3 * ur[1] - Om2 * ur[2]);
+      cor[1] = (T)2 * (Om1 * ur[2] - Om3 * ur[0]);
+      cor[2] = (T)2 * (Om2 * ur[0] - Om1 * ur[1]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -1010,7 +1022,7 @@ __global__ void __launch_bounds__(256) fm1_combine_kernel(StepIO<T> io, const Cx
         if (io.w0_out) io.w0_out[(3 * i + c) * fs + s] = w0[i];  // the memory variables as read
       }
       const Cx<T> plql = PLQL[c * fs + s];
-      io.finish(s, c, PLp[c * fs + s] + sum);
+      io.finish(s, c, (rotate ? PLp[c * fs + s] + cor[c] : PLp[c * fs + s]) + sum);
       Cx<T> run = mk<T>(0, 0);
       for (int i = 1; i <= nsub; ++i) {
         for (int j = 1; j < i; ++j) run = run + (((i + j + 1) & 1) ? -p4d : p4d) * w0[j - 1];
@@ -1023,8 +1035,6 @@ __global__ void __launch_bounds__(256) fm1_combine_kernel(StepIO<T> io, const Cx
 
 template <typename T>
 int fm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
-  if (p->rotate)
-    return fail(c, PSB_ERR_UNSUPPORTED, "PSB_FM1: the rotating form (Coriolis inside PL before the split) is not built");
   const int nsub = p->fm_nsub > 0 ? p->fm_nsub : 1;
   if (nsub > kFmMaxSub) return fail(c, PSB_ERR_ARG, "PSB_FM1: fm_nsub must be 1..8");
   const double dt0 = p->fm_dt0 > 0 ? p->fm_dt0 : 0.1;
@@ -1054,8 +1064,8 @@ int fm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
   const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
   {
     LaunchScope ls(c, "fm1 combine", (double)sizeof(Cx<T>) * fs * (3 + 3 * nsub) * 2 + sizeof(Cx<T>) * fs * 6);
-    fm1_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, PLp, PLQL, nsub, (T)(-2. / d), (T)(4. / d), N1, N2,
-                                                         N3);
+    fm1_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, PLp, PLQL, nsub, (T)(-2. / d), (T)(4. / d), p->rotate,
+                                                         (T)p->Om1, (T)p->Om2, (T)p->Om3, N1, N2, N3);
   }
   return launch_ok(c, "fm1 combine");
 }

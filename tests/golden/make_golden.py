@@ -255,6 +255,7 @@ def gen_serial(N, seed):
         ("cm1", 6, {}),
         ("budgets", 99, {}),
         ("fm1", 3, dict(dt0=0.05)),
+        ("fm1_rot", 3, dict(dt0=0.05, rotate=1, Om=(0.25, -0.1, 0.4))),
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)

@@ -22,6 +22,7 @@ CASES = {
     "cm1": (6, {}, {}),
     "budgets": (99, {}, {}),
     "fm1": (3, dict(dt0=0.05), {}),
+    "fm1_rot": (3, dict(dt0=0.05, rotate=1, Om=(0.25, -0.1, 0.4)), dict(rotate=1, Om=(0.25, -0.1, 0.4))),
 }
 NU, DT, T = 0.02, 0.01, 0.37
 

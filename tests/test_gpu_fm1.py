@@ -66,11 +66,22 @@ def test_fm1_fp32_tracks_fp64():
     assert rel(np_(m32.Q).astype(np.complex128), np_(m64.Q)) < 2e-5
 
 
-def test_fm1_rejects_rotation_and_too_many_subintegrations():
+def test_fm1_rotating_with_memory_matches_oracle():
+    """Rotating FM1 from non-zero memory variables (the fresh rotating case
+    runs against the fixtures in test_gpu_parity.py)."""
+    from oracle import spectral_oracle as orc
     d = golden("serial_N12.npz")
     grid, main = _main(d, 12, rotate=1)
-    with pytest.raises(RuntimeError, match="rotating form"):
-        main.computeRHS(main, grid, None, None)
+    st = np_(main.Q)
+    main.computeRHS(main, grid, None, None)
+    p = orc.Params(nu=NU, t=T, dt=DT, rotate=1, Om=(0.1, 0.2, 0.3))
+    r, _, _ = orc.rhs_fm1(orc.Grid.periodic(12), st, p, dt0=0.08, nsub=3)
+    assert rel(np_(main.Q), r) < TOL64
+
+
+def test_fm1_rejects_too_many_subintegrations():
+    d = golden("serial_N12.npz")
+    grid, _ = _main(d, 12)
     from pyspectral_b200 import Classes as C
     st = d["state"]
     main = C.variables(0, 3, 0, 0, 0, 0, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.08, dt0_subintegrations=9)
