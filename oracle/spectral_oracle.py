@@ -515,6 +515,24 @@ def rhs_fm1(g, state, p, dt0=0.1, nsub=1):
     return np.stack(out), np.stack(w[0]), ur
 
 
+def rhs_fm1_2term(g, state, p, dt0=0.1):
+    """Two-term first-order finite memory model, ``computeRHS_FM1_2term``
+    (``src/RHSfunctions.py:1288-1410``, turb_model 5) on ``(u, w0, w01)``:
+    ``du/dt = unpad_2x(PL u) + w0 + w01``, ``dw0/dt = -2/dt0 w0 + 2 PLQL``,
+    ``dw01/dt = -2/dt0 w01 - 2 PLQL + 4/dt0 w0``.  ``rotate = 1`` raises in
+    the reference (an N-grid Coriolis pressure added to the 2x-grid ``phat``).
+
+    Returns ``(rhs, uhat_read)``."""
+    if p.rotate == 1:
+        raise ValueError("computeRHS_FM1_2term has no rotating form")
+    r, _, ur, PLQL, _ = _memory_rhs(g, state[:3], p, lambda *a: (0.0, None))
+    w0, w01 = state[3:6], state[6:9]
+    out = [r[c] + w0[c] + w01[c] for c in range(3)]
+    out += [-2.0 / dt0 * w0[c] + 2.0 * PLQL[c] for c in range(3)]
+    out += [-2.0 / dt0 * w01[c] - 2.0 * PLQL[c] + 4.0 / dt0 * w0[c] for c in range(3)]
+    return np.stack(out), ur
+
+
 def rhs_cm1(g, state, p):
     """First-order complete memory model, ``computeRHS_CM1``
     (``src/RHSfunctions.py:1411-1542``) on the state ``(u, v, w, w0_u, w0_v,

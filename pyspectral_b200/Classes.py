@@ -137,7 +137,8 @@ class variables:
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
     'Dynamic tau-model', 3 (first-order finite memory model, state
     ``Q = (u, v, w)`` then ``(w0_u, w0_v, w0_w)`` per subintegration; dt0 and
-    dt0_subintegrations as in the reference), 6 (first-order complete memory model, state
+    dt0_subintegrations as in the reference), 5 (its two-term form, state
+    ``(u, w0, w01)``), 6 (first-order complete memory model, state
     ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky), 99 (DNS
     with SGS budgets: ``utilitiesClass``'s hooks write ``budget<it>.npz``
     every 20 iterations).  ``precision`` (64 or 32) selects FP64 or FP32
@@ -176,6 +177,13 @@ class variables:
             self.fm_nsub = 1 if dt0_subintegrations == -10 else int(dt0_subintegrations)
             self.Q = torch.cat([self.Q] + [torch.zeros_like(self.Q)] * self.fm_nsub).contiguous()
             self.nvars = 3 + 3 * self.fm_nsub
+        if turb_model == 5:
+            # two-term finite memory model (src/Classes.py:408-454): state (u, w0, w01);
+            # it is the finite memory model with two subintegrations of 2 dt0
+            self.dt0 = 0.1 if dt0 == -10 else float(dt0)
+            self.fm_dt0, self.fm_nsub = 2.0 * self.dt0, 2
+            self.Q = torch.cat([self.Q] + [torch.zeros_like(self.Q)] * 2).contiguous()
+            self.nvars = 9
         self.Ct = 0.1 if Ct == -10 else float(Ct)
         self.tau_a, self.tau_b = float(dt0), float(dt1)
         self.tau = 0.0
@@ -185,6 +193,7 @@ class variables:
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel, 3: R.computeRHS_FM1,
+                 5: R.computeRHS_FM1_2term,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
                  6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, 99: R.computeRHS_BUDGETS,
                  "learned": R.computeRHS_learned}
@@ -198,7 +207,7 @@ class variables:
             from .learned import MLPModel
             self.model = MLPModel.load(device=grid.device)
         if turb_model not in (0, "learned"):
-            self.W0 = torch.zeros_like(self.Q[3:] if turb_model == 3 else self.U)
+            self.W0 = torch.zeros_like(self.Q[3:] if turb_model in (3, 5) else self.U)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
         if turb_model == "Static tau-model":
@@ -223,6 +232,8 @@ class variables:
     def _w0(self, c):
         if self.W0 is None:
             return None
+        if self.turb_model == 5:  # w0_u, w0_v, w0_w (N1, N2, N3/2+1); w01_* are fields 3..5
+            return self.W0[c]
         if self.turb_model == 3:  # FM1: one memory variable per subintegration, (N1, N2, N3/2+1, nsub)
             return self.W0[c::3].permute(1, 2, 3, 0)
         return self.W0[c].unsqueeze(-1)
@@ -239,14 +250,27 @@ class variables:
     def w0_w(self):
         return self._w0(2)
 
+    # second memory variable of the two-term finite memory model (turb_model 5)
+    @property
+    def w01_u(self):
+        return self.W0[3] if self.turb_model == 5 else None
+
+    @property
+    def w01_v(self):
+        return self.W0[4] if self.turb_model == 5 else None
+
+    @property
+    def w01_w(self):
+        return self.W0[5] if self.turb_model == 5 else None
+
     def U2Q(self):
         self.Q[:3].copy_(self.U)
-        if self.turb_model in (3, 6):  # memory models: w0 is state (src/Classes.py:253-259,476-482)
+        if self.turb_model in (3, 5, 6):  # memory models: w0 is state (src/Classes.py:253-259,432-440,476-482)
             self.Q[3:].copy_(self.W0)
 
     def Q2U(self):
         self.U.copy_(self.Q[:3])
-        if self.turb_model == 3:
+        if self.turb_model in (3, 5):
             self.W0.copy_(self.Q[3:])
         elif self.turb_model == 6:  # w0_v read from a slice nothing writes (src/Classes.py:489)
             self.W0.copy_(self.Q[3:6])
@@ -265,7 +289,7 @@ class variables:
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 6: _capi.CM1, 7: _capi.DSMAG,
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 5: _capi.FM1, 6: _capi.CM1, 7: _capi.DSMAG,
                 99: _capi.BUDGETS,
                 "learned": _capi.LEARNED}[self.turb_model]
 

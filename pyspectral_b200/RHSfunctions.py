@@ -55,6 +55,15 @@ def computeRHS_FM1(main, grid, myFFT=None, utilities=None):
     _rhs(main, grid, _capi.FM1)
 
 
+def computeRHS_FM1_2term(main, grid, myFFT=None, utilities=None):
+    """Two-term finite memory model (turb_model 5), src/RHSfunctions.py:1288-1410,
+    on ``(u, w0, w01)``: the finite memory model with two subintegrations of
+    2 dt0 (the same right-hand sides).  No rotating form (the reference's raises)."""
+    if main.rotate:
+        raise RuntimeError("computeRHS_FM1_2term: the reference has no rotating form")
+    _rhs(main, grid, _capi.FM1)
+
+
 def computeRHS_CM1(main, grid, myFFT=None, utilities=None):
     """First-order complete memory model (turb_model 6),
     src/RHSfunctions.py:1411-1542: ``main.Q`` holds (u, v, w, w0_u, w0_v,

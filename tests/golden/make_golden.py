@@ -33,7 +33,9 @@ Outputs (all FP64, a few hundred KB in total):
 
 * ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
   closure (DNS, Smagorinsky, t-model, static and dynamic tau-model, dynamic
-  Smagorinsky, first-order complete memory model, DNS with SGS budgets; DNS,
+  Smagorinsky, first-order complete memory model, first-order finite memory
+  model (one and three subintegrations, and its two-term form), DNS with SGS
+  budgets; DNS,
   Smagorinsky, t-model and dynamic Smagorinsky also with rotation), the
   budget file the hooks write at iteration 20, plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
@@ -307,6 +309,23 @@ def gen_serial(N, seed):
             else:
                 ref_rk4_step(main, grid, myFFT, util)
         out[f"fm1w_{stage}"] = _diag(main.Q, 12)
+    # the two-term FM1 (turb_model 5), fresh and from non-zero memory variables
+    w0t = 0.2 * np.stack([orc.isotropic_state(N, seed + 300 + i, k0=2.0) for i in range(2)])
+    out["fm2t_init"] = w0t
+    for case in ("fm2t", "fm2tw"):
+        for stage in ("rhs", "step"):
+            grid, myFFT, util, main = serial_case(C, N, st, 5, nu, dt, t, dt0=0.04)
+            if case == "fm2tw":
+                main.w0_u[:], main.w0_v[:], main.w0_w[:] = w0t[0]
+                main.w01_u[:], main.w01_v[:], main.w01_w[:] = w0t[1]
+                main.U2Q()
+            with contextlib.redirect_stdout(io.StringIO()):
+                if stage == "rhs":
+                    main.computeRHS(main, grid, myFFT, util)
+                    out[f"{case}_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+                else:
+                    ref_rk4_step(main, grid, myFFT, util)
+            out[f"{case}_{stage}"] = _diag(main.Q, 9)
     # CM1 from a state with non-zero memory variables (set, then U2Q)
     w0init = 0.3 * orc.isotropic_state(N, seed + 100, k0=2.0)
     out["cm1w_init"] = w0init

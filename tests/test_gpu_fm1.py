@@ -87,3 +87,33 @@ def test_fm1_rejects_too_many_subintegrations():
     main = C.variables(0, 3, 0, 0, 0, 0, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.08, dt0_subintegrations=9)
     with pytest.raises(RuntimeError, match="fm_nsub"):
         main.computeRHS(main, grid, None, None)
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("case", ["fm2t", "fm2tw"])
+def test_fm1_two_term_matches_reference(N, case):
+    """turb_model 5 through PSB_FM1 (two subintegrations of 2 dt0), against the
+    reference's own outputs (it runs as written)."""
+    torch = _torch()
+    from pyspectral_b200 import Classes as C
+    from pyspectral_b200.RHSfunctions import advanceQ_RK4
+    d = golden(f"serial_N{N}.npz")
+    st = d["state"]
+    for stage in ("rhs", "step"):
+        grid = C.gridclass.periodic(N)
+        main = C.variables(0, 5, 0, 0, 0, 0, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.04)
+        assert main.nvars == 9 and tuple(main.w01_u.shape) == (N, N, N // 2 + 1)
+        if case == "fm2tw":
+            init = torch.as_tensor(d["fm2t_init"], device=main.Q.device)
+            main.w0_u[:], main.w0_v[:], main.w0_w[:] = init[0]
+            main.w01_u[:], main.w01_v[:], main.w01_w[:] = init[1]
+            main.U2Q()
+        if stage == "rhs":
+            main.computeRHS(main, grid, None, None)
+            assert rel(np_(main.U), d[f"{case}_uhat"]) < TOL64
+        else:
+            advanceQ_RK4(main, grid, None, C.utilitiesClass())
+        assert rel(np_(main.Q), d[f"{case}_{stage}"]) < TOL64
+    main = C.variables(0, 5, 1, 0.1, 0.2, 0.3, grid, st[0], st[1], st[2], T, DT, NU, dt0=0.04)
+    with pytest.raises(RuntimeError, match="no rotating form"):
+        main.computeRHS(main, grid, None, None)

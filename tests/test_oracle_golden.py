@@ -128,6 +128,25 @@ def test_fm1_three_subintegrations_match_reference(N):
     assert rel(Q, d["fm1w_step"]) < 1e-13
 
 
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("case", ["fm2t", "fm2tw"])
+def test_fm1_two_term_matches_reference(N, case):
+    """turb_model 5 (no undefined names: the reference runs as written)."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    mem = d["fm2t_init"].reshape(6, *d["state"].shape[1:]) if case == "fm2tw" else np.zeros((6,) + d["state"].shape[1:])
+    st = np.concatenate([d["state"], mem])
+    r, ur = orc.rhs_fm1_2term(g, st, p, dt0=0.04)
+    assert rel(r, d[f"{case}_rhs"]) < 1e-13
+    assert rel(ur, d[f"{case}_uhat"]) < 1e-13
+    Q, _ = orc.advance_rk4(st, lambda q: (orc.rhs_fm1_2term(g, q, p, dt0=0.04)[0], q), DT)
+    assert rel(Q, d[f"{case}_step"]) < 1e-13
+    # the same as FM1 with two subintegrations of 2 dt0
+    r1, _, _ = orc.rhs_fm1(g, st, p, dt0=0.08, nsub=2)
+    assert rel(r1, r) < 1e-14
+
+
 def test_myfilter_slice_semantics():
     """myFilter keeps rows [0:kc] and [-kc+1:]; kc = 1 makes the second slice
     [0:], the whole axis (Python slicing), and kc = 0 keeps nothing."""
