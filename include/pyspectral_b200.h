@@ -53,6 +53,9 @@ extern "C" {
                              dw0_i/dt = -2/d w0_i + (-1)^(i+1) 2 PLQLu + S_i, d = dt0/nsub,
                              S_i the running sum of :1010-1014; w0 (3 p.fm_nsub fields)
                              receives the memory variables as read                          */
+#define PSB_ORTHO 12      /* 'Orthogonal Dynamics' -> computeRHS_Orthogonal (src/RHSfunctions.py:53-143):
+                             the DNS RHS of u minus the DNS RHS of Gf u (each with its
+                             pressure and Coriolis terms)                                     */
 #define PSB_BUDGETS 10    /* turb_model 99     -> computeRHS_BUDGETS (src/RHSfunctions.py:1543-1661):
                              RHS = unpad_2x(PLu); w0 receives PLQLu with the q part split at
                              p.kf (0 -> int(max k1), main.kc of src/Classes.py:16); no

@@ -289,6 +289,33 @@ def rhs_nosgs(g, state, p):
     return np.stack(r), np.stack([u, v, w])
 
 
+def rhs_orthogonal(g, state, p):
+    """Orthogonal dynamics, ``computeRHS_Orthogonal`` (``src/RHSfunctions.py:53-143``):
+    the DNS right-hand side of the (Nyquist-zeroed) state minus that of
+    ``Gf u``, each with its own pressure and Coriolis terms.  Returns
+    ``(rhs, uhat_read)``."""
+    u, v, w = (nyquist_zero(state[i]) for i in range(3))
+    k1, k2, k3 = g.k1, g.k2, g.k3
+
+    def part(a, b, c):
+        P = _products_32(g, a, b, c)
+        phat = _pressure(k1, k2, k3, g.ksqr_i, *P)
+        if p.rotate == 1:
+            phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, a, b, c, p.Om)
+        return list(_advection(k1, k2, k3, p.nu, g.ksqr, phat, P, a, b, c))
+    r = part(u, v, w)
+    if p.rotate == 1:
+        cf = _coriolis_force(u, v, w, p.Om)
+        r = [r[i] + cf[i] for i in range(3)]
+    uf, vf, wf = g.Gf * u, g.Gf * v, g.Gf * w
+    rf = part(uf, vf, wf)
+    r = [r[i] - rf[i] for i in range(3)]
+    if p.rotate == 1:
+        cf = _coriolis_force(uf, vf, wf, p.Om)
+        r = [r[i] - cf[i] for i in range(3)]
+    return np.stack(r), np.stack([u, v, w])
+
+
 def _sgs_divergence(g, tau):
     """Projected divergence of a stress, ``src/RHSfunctions.py:215-222``
     (identical form at ``src/Classes.py:917-927``).  Note the reference's

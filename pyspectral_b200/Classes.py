@@ -135,7 +135,7 @@ class variables:
     (src/Classes.py:7-229).
 
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
-    'Dynamic tau-model', 3 (first-order finite memory model, state
+    'Dynamic tau-model', 'Orthogonal Dynamics', 3 (first-order finite memory model, state
     ``Q = (u, v, w)`` then ``(w0_u, w0_v, w0_w)`` per subintegration; dt0 and
     dt0_subintegrations as in the reference), 5 (its two-term form, state
     ``(u, w0, w01)``), 6 (first-order complete memory model, state
@@ -193,6 +193,7 @@ class variables:
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel, 3: R.computeRHS_FM1,
+                 "Orthogonal Dynamics": R.computeRHS_Orthogonal,
                  5: R.computeRHS_FM1_2term,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
                  6: R.computeRHS_CM1, 7: R.computeRHS_DSMAG, 99: R.computeRHS_BUDGETS,
@@ -206,7 +207,7 @@ class variables:
         if turb_model == "learned" and model is None:
             from .learned import MLPModel
             self.model = MLPModel.load(device=grid.device)
-        if turb_model not in (0, "learned"):
+        if turb_model not in (0, "learned", "Orthogonal Dynamics"):
             self.W0 = torch.zeros_like(self.Q[3:] if turb_model in (3, 5) else self.U)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
@@ -290,6 +291,7 @@ class variables:
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
                 "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 5: _capi.FM1, 6: _capi.CM1, 7: _capi.DSMAG,
+                "Orthogonal Dynamics": _capi.ORTHO,
                 99: _capi.BUDGETS,
                 "learned": _capi.LEARNED}[self.turb_model]
 

@@ -55,6 +55,12 @@ def computeRHS_FM1(main, grid, myFFT=None, utilities=None):
     _rhs(main, grid, _capi.FM1)
 
 
+def computeRHS_Orthogonal(main, grid, myFFT=None, utilities=None):
+    """Orthogonal dynamics ('Orthogonal Dynamics'), src/RHSfunctions.py:53-143:
+    the DNS right-hand side of u minus that of ``Gf u``."""
+    _rhs(main, grid, _capi.ORTHO)
+
+
 def computeRHS_FM1_2term(main, grid, myFFT=None, utilities=None):
     """Two-term finite memory model (turb_model 5), src/RHSfunctions.py:1288-1410,
     on ``(u, w0, w01)``: the finite memory model with two subintegrations of

@@ -15,8 +15,8 @@ LIB_PATH = os.path.join(HERE, "libpyspectral_b200.so")
 
 PSB_OK = 0
 PSB_ERR_NONFINITE = 6
-DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS, FM1 = (
-    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11)
+DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS, FM1, ORTHO = (
+    0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12)
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 

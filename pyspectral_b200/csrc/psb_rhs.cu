@@ -1134,6 +1134,96 @@ int budgets_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
   return launch_ok(c, "budgets finish");
 }
 
+// ---------------------------------------------------------------------------
+// Orthogonal dynamics (PySpectral/src/RHSfunctions.py:53-143): the DNS RHS of u
+// minus the DNS RHS of Gf u, each with its own pressure and Coriolis terms.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ Cx<T> ortho_part(T k1, T k2, T k3, T ksq, T ksqi, T nu, const Cx<T>* P, const Cx<T>* u,
+                                            int comp, int rotate, T Om1, T Om2, T Om3, Cx<T>* cor) {
+  const Cx<T> uu = P[0], vv = P[1], ww = P[2], uv = P[3], uw = P[4], vw = P[5];
+  Cx<T> ph = ksqi * ((-k1 * k1) * uu - (k2 * k2) * vv - (k3 * k3) * ww - ((T)2 * k1 * k2) * uv -
+                     ((T)2 * k1 * k3) * uw - ((T)2 * k2 * k3) * vw);
+  const Cx<T> cu = Om3 * u[1] - Om2 * u[2], cv = Om1 * u[2] - Om3 * u[0], cw = Om2 * u[0] - Om1 * u[1];
+  if (rotate) ph = ph - ((T)2 * ksqi) * mul_i(k1 * cu + k2 * cv + k3 * cw);
+  const Cx<T> c3[3] = {cu, cv, cw};
+  *cor = (T)2 * c3[comp];
+  if (comp == 0) return mik(k1, uu) + mik(k2, uv) + mik(k3, uw) + mik(k1, ph) - (nu * ksq) * u[0];
+  if (comp == 1) return mik(k1, uv) + mik(k2, vv) + mik(k3, vw) + mik(k2, ph) - (nu * ksq) * u[1];
+  return mik(k1, uw) + mik(k2, vw) + mik(k3, ww) + mik(k3, ph) - (nu * ksq) * u[2];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) ortho_combine_kernel(StepIO<T> io, KTabs<T> k, const Cx<T>* __restrict__ A,
+                                                            const Cx<T>* __restrict__ B, const double* __restrict__ gx,
+                                                            const double* __restrict__ gy,
+                                                            const double* __restrict__ gz, T nu, int rotate, T Om1,
+                                                            T Om2, T Om3, int N1, int N2, int N3) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % io.n3h);
+    const long long t = s / io.n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+    const T gf = (T)(gx[i1] * gy[i2] * gz[i3]);
+    Cx<T> u[3], uf[3], P[6], Pf[6];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      u[f] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+      uf[f] = gf * u[f];
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      P[m] = A[m * fs + s];
+      Pf[m] = B[m * fs + s];
+    }
+    if (io.read_out) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = u[f];
+    }
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    Cx<T> R[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> cor, corf;
+      const Cx<T> a = ortho_part(k1, k2, k3, ksq, ksqi, nu, P, u, c, rotate, Om1, Om2, Om3, &cor);
+      const Cx<T> af = ortho_part(k1, k2, k3, ksq, ksqi, nu, Pf, uf, c, rotate, Om1, Om2, Om3, &corf);
+      Cx<T> r = rotate ? a + cor : a;
+      r = r - af;
+      R[c] = rotate ? r - corf : r;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) io.finish(s, c, R[c]);
+  }
+}
+
+template <typename T>
+int ortho_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p, const psb_tuned* ts) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "ortho.A", (size_t)6 * fs, &st);
+  Cx<T>* B = scratch<T>(c, "ortho.B", (size_t)6 * fs, &st);
+  if (st != PSB_OK) return st;
+  const Cx<T>* Qin = io.Q;
+  EpiStore<T, 6> sa{A, fs, N2, N3h}, sb{B, fs, N2, N3h};
+  PSB_TRY(run_ns32<T>(c, Qin, PreCopyN<T, 3>{}, PhysProducts<T>{}, sa, ts));
+  PSB_TRY(run_ns32<T>(c, Qin, PreMask3<T>{c->gx, c->gy, c->gz}, PhysProducts<T>{}, sb, ts));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "ortho combine", (double)sizeof(Cx<T>) * fs * (12 + 3) + io.bytes(fs, 3));
+    ortho_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, ktabs<T>(c->kx, c->ky, c->kz), A, B, c->gx, c->gy,
+                                                           c->gz, (T)p->nu, p->rotate, (T)p->Om1, (T)p->Om2,
+                                                           (T)p->Om3, N1, N2, N3);
+  }
+  return launch_ok(c, "ortho combine");
+}
+
 // myFilter's kept rows (src/Classes.py:1271-1279) with Python slice bounds:
 // [0:kc] and [-kc+1:] on axes 1 and 2, [0:kc] on axis 3
 inline void myfilter_rows(int n, int kc, bool two_sided, double* out) {
@@ -1301,6 +1391,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       return budgets_rhs<T>(c, io, p);
     case PSB_FM1:
       return fm1_rhs<T>(c, io, p);
+    case PSB_ORTHO:
+      return ortho_rhs<T>(c, io, p, ts);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

@@ -34,8 +34,8 @@ Outputs (all FP64, a few hundred KB in total):
 * ``serial_N{N}.npz`` -- one RHS evaluation and one RK4 step of every serial
   closure (DNS, Smagorinsky, t-model, static and dynamic tau-model, dynamic
   Smagorinsky, first-order complete memory model, first-order finite memory
-  model (one and three subintegrations, and its two-term form), DNS with SGS
-  budgets; DNS,
+  model (one and three subintegrations, and its two-term form), orthogonal
+  dynamics (+rotation, kc = N/4), DNS with SGS budgets; DNS,
   Smagorinsky, t-model and dynamic Smagorinsky also with rotation), the
   budget file the hooks write at iteration 20, plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
@@ -258,6 +258,8 @@ def gen_serial(N, seed):
         ("budgets", 99, {}),
         ("fm1", 3, dict(dt0=0.05)),
         ("fm1_rot", 3, dict(dt0=0.05, rotate=1, Om=(0.25, -0.1, 0.4))),
+        ("ortho", "Orthogonal Dynamics", dict(kc=N // 4)),   # kc = N/4: Gf u != u
+        ("ortho_rot", "Orthogonal Dynamics", dict(kc=N // 4, rotate=1, Om=(0.3, 0.1, -0.2))),
     ]
     for name, tm, kw in cases:
         grid, myFFT, util, main = serial_case(C, N, st, tm, nu, dt, t, **kw)

@@ -147,6 +147,21 @@ def test_fm1_two_term_matches_reference(N, case):
     assert rel(r1, r) < 1e-14
 
 
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("name,okw", [("ortho", {}), ("ortho_rot", dict(rotate=1, Om=(0.3, 0.1, -0.2)))])
+def test_orthogonal_dynamics_matches_reference(N, name, okw):
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N, kc=N // 4)
+    p = orc.Params(nu=NU, t=T, dt=DT, **okw)
+    st = d["state"]
+    r, ur = orc.rhs_orthogonal(g, st, p)
+    assert rel(r, d[f"{name}_rhs"]) < 1e-13
+    assert rel(ur, d[f"{name}_uhat"]) < 1e-13
+    Q, read = orc.advance_rk4(st, lambda q: orc.rhs_orthogonal(g, q, p), DT)
+    assert rel(Q, d[f"{name}_step"]) < 1e-13
+    assert rel(read, d[f"{name}_step_uhat"]) < 1e-13
+
+
 def test_myfilter_slice_semantics():
     """myFilter keeps rows [0:kc] and [-kc+1:]; kc = 1 makes the second slice
     [0:], the whole axis (Python slicing), and kc = 0 keeps nothing."""
