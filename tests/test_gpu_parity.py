@@ -241,15 +241,17 @@ def test_tgv64_known_answer_history():
 
 
 @pytest.mark.parametrize("precision", [64, 32])
-def test_cuda_graph_replay_equals_eager_steps(precision):
+@pytest.mark.parametrize("name", ["smag", "dsmag", "cm1", "fm1", "budgets"])
+def test_cuda_graph_replay_equals_eager_steps(precision, name):
     """A captured 3-step graph replayed twice gives bit-identical state to
-    6 eager steps."""
+    6 eager steps (closures whose RHS runs reductions, stored passes or
+    memory state included)."""
     torch = _torch()
     from pyspectral_b200 import Classes as C
     from pyspectral_b200.RHSfunctions import StepGraph, advance
     d = golden("serial_N16.npz")
-    grid, a = _main("smag", 16, d["state"], precision)
-    grid2, b = _main("smag", 16, d["state"], precision)
+    grid, a = _main(name, 16, d["state"], precision)
+    grid2, b = _main(name, 16, d["state"], precision)
     g = StepGraph(a, grid, 3)
     g.replay()
     g.replay()
