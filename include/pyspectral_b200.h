@@ -56,6 +56,11 @@ extern "C" {
 #define PSB_ORTHO 12      /* 'Orthogonal Dynamics' -> computeRHS_Orthogonal (src/RHSfunctions.py:53-143):
                              the DNS RHS of u minus the DNS RHS of Gf u (each with its
                              pressure and Coriolis terms)                                     */
+#define PSB_MPI_DNS 13    /* MPI solver turb_model 0 -> computeRHS_NOSGS (src_MPI/RHSfunctions.py:22-93):
+                             2/3-rule dealiasing on the N grid (no padding), + rotation           */
+#define PSB_MPI_ORTHO 14  /* MPI solver 'Orthogonal Dynamics' -> computeRHS_Ortho
+                             (src_MPI/RHSfunctions.py:179-268): the PSB_MPI_DNS RHS of u minus
+                             that of grid.filter(u) (cutoff kc, src_MPI/Classes.py:219-235)   */
 #define PSB_BUDGETS 10    /* turb_model 99     -> computeRHS_BUDGETS (src/RHSfunctions.py:1543-1661):
                              RHS = unpad_2x(PLu); w0 receives PLQLu with the q part split at
                              p.kf (0 -> int(max k1), main.kc of src/Classes.py:16); no

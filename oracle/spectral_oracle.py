@@ -741,6 +741,46 @@ def rhs_mhd(g, state, nu, force=None, eta=None):
     return r, np.stack(s)
 
 
+def rhs_mpi_ns(g, state, nu, rotate=0, Om=(0.0, 0.0, 0.0), ortho=False):
+    """Navier-Stokes of the MPI solver, ``computeRHS_NOSGS``
+    (``src_MPI/RHSfunctions.py:22-93``): 2/3-rule masks on read and on the
+    RHS, products on the N grid, Coriolis after the mask.  ``ortho``:
+    ``computeRHS_Ortho`` (``:179-268``), that RHS minus the same of
+    ``grid.filter(u)`` (``|k_i| < kc`` per axis, ``src_MPI/Classes.py:219-235``).
+    Returns ``(rhs, dealiased_state)``."""
+    D = g.dealias_mask
+    k1 = g.k1[:, None, None]
+    k2 = g.k2[None, :, None]
+    k3 = g.k3[None, None, :]
+    shape = (g.N1, g.N2, g.N3)
+
+    def part(a):
+        u, v, w = (_irfftn(x, s=shape) for x in a)
+        NL = [_rfftn(x * y) for x, y in ((u, u), (v, v), (w, w), (u, v), (u, w), (v, w))]
+        phat = _pressure(k1, k2, k3, g.ksqr_i, *NL)
+        if rotate == 1:
+            phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, a[0], a[1], a[2], Om)
+        r = [D * x for x in _advection(k1, k2, k3, nu, g.ksqr, phat, NL, a[0], a[1], a[2])]
+        c = _coriolis_force(a[0], a[1], a[2], Om) if rotate == 1 else None
+        return r, c
+    s = [D * state[i] for i in range(3)]
+    r, c = part(s)
+    if rotate == 1:
+        r = [r[i] + c[i] for i in range(3)]
+    if ortho:
+        kc = g.kc
+        fx = (np.abs(g.k1) < kc * 2.0 * np.pi / g.L1).astype(float)
+        fy = (np.abs(g.k2) < kc * 2.0 * np.pi / g.L2).astype(float)
+        fz = np.ones(g.N3 // 2 + 1)
+        fz[kc:] = 0.0
+        F = fx[:, None, None] * fy[None, :, None] * fz[None, None, :]
+        rf, cf = part([F * x for x in s])
+        r = [r[i] - rf[i] for i in range(3)]
+        if rotate == 1:
+            r = [r[i] - cf[i] for i in range(3)]
+    return np.stack(r), np.stack(s)
+
+
 def _mhd_nonlinear(k1, k2, k3, ksqr_i, P):
     """Nonlinear MHD operator from the nine product spectra
     P = (u_iu_j - B_iB_j for 11,22,33,12,13,23, then u x B): the momentum

@@ -17,6 +17,7 @@ PSB_OK = 0
 PSB_ERR_NONFINITE = 6
 DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS, FM1, ORTHO = (
     0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12)
+MPI_DNS, MPI_ORTHO = 13, 14
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 

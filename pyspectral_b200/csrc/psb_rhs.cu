@@ -223,11 +223,12 @@ struct EpiSGSDNS {
 // ---------------------------------------------------------------------------
 // MHD: unpadded transforms under the 2/3 rule
 // ---------------------------------------------------------------------------
-template <typename T>
-int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
+template <typename T, class Pre, class Phys, class Epi>
+int run_n23(psb_ctx* c, const Cx<T>* Qin, Pre pre, Phys phys, Epi epi) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int Kz = c->kz_mhd;
-  constexpr int Fi = 6, Fo = 9;
+  constexpr int Fi = Phys::F_IN, Fo = Phys::F_OUT;
+  static_assert(Pre::F_DST == Fi && Epi::F_IN == Fo, "pass field counts");
   int st = PSB_OK;
   Cx<T>* A = scratch<T>(c, "mhd.A", (size_t)Fi * N1 * N2 * Kz, &st);
   Cx<T>* B = scratch<T>(c, "mhd.B", (size_t)Fi * N1 * N2 * Kz, &st);
@@ -252,7 +253,6 @@ int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
   a.out_rows = N1;
   a.in_map = map_id(N1);
   a.out_map = map_id(N1);
-  PreMask6<T> pre{c->mx, c->my, c->mz};
   PSB_TRY((launch_axis<T, true>(c, a, pre, "mhd x-inverse")));
   AxisArgs<T> b = axis_common<T>(c, N2);
   b.in = A;
@@ -283,7 +283,7 @@ int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
   z.fac = (T)(1.0 / ((double)N1 * N2 * N3));
   z.plan = *plan_for(c, N3);
   z.tw = twiddles<T>(c);
-  PSB_TRY(launch_z<T>(c, z, PhysMHD<T>{}, "mhd z-fused"));
+  PSB_TRY(launch_z<T>(c, z, phys, "mhd z-fused"));
   AxisArgs<T> d = axis_common<T>(c, N2);
   d.in = C;
   d.out = D;
@@ -311,6 +311,12 @@ int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
   e.plan = *plan_for(c, N1);
   e.tw = twiddles<T>(c);
   return launch_epi<T>(c, e, epi, "mhd x-forward+epilogue");
+}
+
+// MHD of the MPI solver: the 2/3-masked fields (u, B) -> (u_iu_j - B_iB_j, u x B)
+template <typename T>
+int run_mhd(psb_ctx* c, const Cx<T>* Qin, EpiMHD<T> epi) {
+  return run_n23<T>(c, Qin, PreMask6<T>{c->mx, c->my, c->mz}, PhysMHD<T>{}, epi);
 }
 
 // ---------------------------------------------------------------------------
@@ -1224,6 +1230,149 @@ int ortho_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p, const psb_tuned* ts
   return launch_ok(c, "ortho combine");
 }
 
+// ---------------------------------------------------------------------------
+// Navier-Stokes of the MPI solver (PySpectral/src_MPI/RHSfunctions.py:22-93)
+// and its orthogonal dynamics (:179-268): 2/3-rule masks D on read and on the
+// RHS, products on the N grid (the MHD pipeline's passes, run_n23).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ Cx<T> mpi_ns_part(T k1, T k2, T k3, T ksq, T ksqi, T nu, T D, const Cx<T>* P,
+                                             const Cx<T>* u, int comp, int rotate, T Om1, T Om2, T Om3, Cx<T>* cor) {
+  const Cx<T> ph0 = ksqi * ((-k1 * k1) * P[0] - (k2 * k2) * P[1] - (k3 * k3) * P[2] - ((T)2 * k1 * k2) * P[3] -
+                            ((T)2 * k1 * k3) * P[4] - ((T)2 * k2 * k3) * P[5]);
+  const Cx<T> cu = Om3 * u[1] - Om2 * u[2], cv = Om1 * u[2] - Om3 * u[0], cw = Om2 * u[0] - Om1 * u[1];
+  const Cx<T> ph = rotate ? ph0 - ((T)2 * ksqi) * mul_i(k1 * cu + k2 * cv + k3 * cw) : ph0;
+  const Cx<T> c3[3] = {cu, cv, cw};
+  *cor = (T)2 * c3[comp];
+  if (comp == 0) return D * (mik(k1, P[0]) + mik(k2, P[3]) + mik(k3, P[4]) + mik(k1, ph) - (nu * ksq) * u[0]);
+  if (comp == 1) return D * (mik(k1, P[3]) + mik(k2, P[1]) + mik(k3, P[5]) + mik(k2, ph) - (nu * ksq) * u[1]);
+  return D * (mik(k1, P[4]) + mik(k2, P[5]) + mik(k3, P[2]) + mik(k3, ph) - (nu * ksq) * u[2]);
+}
+
+template <typename T>
+struct EpiMpiNS {
+  static constexpr int F_IN = 6;
+  __host__ double io_bytes(long long npts) const { return io.bytes(npts, 3); }
+  StepIO<T> io;
+  KTabs<T> k;
+  const double *m1, *m2, *m3;
+  T nu;
+  int rotate;
+  T Om1, Om2, Om3;
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = io.sidx(i1, i2, i3);
+    const T D = (T)(m1[i1] * m2[i2] * m3[i3]);
+    Cx<T> u[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) u[f] = D * io.Q[f * io.fstride + s];
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    if (io.read_out) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * io.fstride + s] = u[f];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> cor;
+      const Cx<T> r = mpi_ns_part(k1, k2, k3, ksq, ksqi, nu, D, P, u, c, rotate, Om1, Om2, Om3, &cor);
+      io.finish(s, c, rotate ? r + cor : r);
+    }
+  }
+};
+
+// the 2/3 mask and then grid.filter (src_MPI/Classes.py:219-235) on load
+template <typename T>
+struct PreMask3x2 {
+  static constexpr int F_SRC = 3, F_DST = 3;
+  const double *m1, *m2, *m3, *f1, *f2, *f3;
+  __device__ void operator()(int i, int o, int cc, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const {
+    const T m = (T)(m1[i] * m2[o] * m3[cc]), f = (T)(f1[i] * f2[o] * f3[cc]);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) d[q] = f * (m * s[q]);
+  }
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) mpi_ortho_combine_kernel(StepIO<T> io, KTabs<T> k,
+                                                                const Cx<T>* __restrict__ A,
+                                                                const Cx<T>* __restrict__ B, const double* __restrict__ m1,
+                                                                const double* __restrict__ m2,
+                                                                const double* __restrict__ m3,
+                                                                const double* __restrict__ gx,
+                                                                const double* __restrict__ gy,
+                                                                const double* __restrict__ gz, T nu, int rotate, T Om1,
+                                                                T Om2, T Om3, int N1, int N2) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % io.n3h);
+    const long long t = s / io.n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    const T D = (T)(m1[i1] * m2[i2] * m3[i3]);
+    const T gf = (T)(gx[i1] * gy[i2] * gz[i3]);
+    Cx<T> u[3], uf[3], P[6], Pf[6];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      u[f] = D * io.Q[f * fs + s];
+      uf[f] = gf * u[f];
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      P[m] = A[m * fs + s];
+      Pf[m] = B[m * fs + s];
+    }
+    if (io.read_out) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = u[f];
+    }
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    Cx<T> R[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> cor, corf;
+      const Cx<T> a = mpi_ns_part(k1, k2, k3, ksq, ksqi, nu, D, P, u, c, rotate, Om1, Om2, Om3, &cor);
+      const Cx<T> af = mpi_ns_part(k1, k2, k3, ksq, ksqi, nu, D, Pf, uf, c, rotate, Om1, Om2, Om3, &corf);
+      Cx<T> r = rotate ? a + cor : a;
+      r = r - af;
+      R[c] = rotate ? r - corf : r;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) io.finish(s, c, R[c]);
+  }
+}
+
+template <typename T>
+int mpi_ns_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p, bool ortho) {
+  const int N1 = c->N1, N2 = c->N2, N3h = c->N3h;
+  const Cx<T>* Qin = io.Q;
+  if (!ortho) {
+    EpiMpiNS<T> epi{io, ktabs<T>(c->kx, c->ky, c->kz), c->mx, c->my, c->mz, (T)p->nu, p->rotate,
+                    (T)p->Om1, (T)p->Om2, (T)p->Om3};
+    return run_n23<T>(c, Qin, PreMask3<T>{c->mx, c->my, c->mz}, PhysProducts<T>{}, epi);
+  }
+  const long long fs = (long long)N1 * N2 * N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "mpio.A", (size_t)6 * fs, &st);
+  Cx<T>* B = scratch<T>(c, "mpio.B", (size_t)6 * fs, &st);
+  if (st != PSB_OK) return st;
+  EpiStore<T, 6> sa{A, fs, N2, N3h}, sb{B, fs, N2, N3h};
+  PSB_TRY(run_n23<T>(c, Qin, PreMask3<T>{c->mx, c->my, c->mz}, PhysProducts<T>{}, sa));
+  PSB_TRY(run_n23<T>(c, Qin, PreMask3x2<T>{c->mx, c->my, c->mz, c->gx, c->gy, c->gz}, PhysProducts<T>{}, sb));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "mpi ortho combine", (double)sizeof(Cx<T>) * fs * 12 + io.bytes(fs, 3));
+    mpi_ortho_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, ktabs<T>(c->kx, c->ky, c->kz), A, B, c->mx,
+                                                               c->my, c->mz, c->gx, c->gy, c->gz, (T)p->nu, p->rotate,
+                                                               (T)p->Om1, (T)p->Om2, (T)p->Om3, N1, N2);
+  }
+  return launch_ok(c, "mpi ortho combine");
+}
+
 // myFilter's kept rows (src/Classes.py:1271-1279) with Python slice bounds:
 // [0:kc] and [-kc+1:] on axes 1 and 2, [0:kc] on axis 3
 inline void myfilter_rows(int n, int kc, bool two_sided, double* out) {
@@ -1393,6 +1542,10 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       return fm1_rhs<T>(c, io, p);
     case PSB_ORTHO:
       return ortho_rhs<T>(c, io, p, ts);
+    case PSB_MPI_DNS:
+      return mpi_ns_rhs<T>(c, io, p, false);
+    case PSB_MPI_ORTHO:
+      return mpi_ns_rhs<T>(c, io, p, true);
     case PSB_TAU_DYNAMIC:
       if constexpr (sizeof(T) == 8)
         return dtau_rhs_d(c, io, p, tau_out);

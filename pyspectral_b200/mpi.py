@@ -94,15 +94,17 @@ class FFTclass:
 
 
 class variables:
-    """MPI ``variables`` for ``turb_model='MHD'`` (src_MPI/Classes.py:82-149).
+    """MPI ``variables`` for ``turb_model='MHD'`` (src_MPI/Classes.py:82-149),
+    0 (Navier-Stokes, :58-80) and 'Orthogonal Dynamics' (:152-174).
     ``u,v,w,B1,B2,B3`` are physical fields (``initDomain='Physical'``) or
-    ``uhat..`` spectra (``'Fourier'``, re-symmetrised by a round trip)."""
+    ``uhat..`` spectra (``'Fourier'``, re-symmetrised by a round trip); the B
+    fields are ignored by the Navier-Stokes models."""
 
     def __init__(self, turb_model, rotate, Om1, Om2, Om3, grid, u, v, w, B1, B2, B3, uhat=None, vhat=None,
                  what=None, t=0.0, dt=0.0, nu=0.0, myFFT=None, mpi_rank=0, initDomain="Physical",
                  time_scheme="RK4", precision=64, kahan=None, Bhat=None, forcing=True, closure=None, Ct=0.1):
-        if turb_model != "MHD":
-            raise ValueError("only turb_model='MHD' of the MPI solver is on this path")
+        if turb_model not in ("MHD", 0, "Orthogonal Dynamics"):
+            raise ValueError("turb_model must be 'MHD', 0 or 'Orthogonal Dynamics'")
         if time_scheme != "RK4":
             raise ValueError("Error, time scheme " + str(time_scheme) + " not implemented for MHD equations")
         if closure not in (None, "tmodel"):
@@ -118,20 +120,23 @@ class variables:
         ctx = grid.ctx(precision)
         N1, N2, N3 = grid.N1, grid.N2, grid.N3
         sh = (N1, N2, N3 // 2 + 1)
-        self.Q = torch.zeros((6,) + sh, dtype=_cdtype(precision), device=dev)
+        nf = 6 if turb_model == "MHD" else 3
+        self.Q = torch.zeros((nf,) + sh, dtype=_cdtype(precision), device=dev)
         if initDomain == "Physical":
-            phys = torch.stack([_on(a, dev, _rdtype(precision)) for a in (u, v, w, B1, B2, B3)]).contiguous()
-            ctx.r2c(phys, self.Q, 6)
+            fields = (u, v, w, B1, B2, B3)[:nf]
+            phys = torch.stack([_on(a, dev, _rdtype(precision)) for a in fields]).contiguous()
+            ctx.r2c(phys, self.Q, nf)
         else:
             src = torch.stack([_on(a, dev, _cdtype(precision)) for a in (uhat, vhat, what)] +
-                              [_on(a, dev, _cdtype(precision)) for a in Bhat])
-            phys = torch.empty((6, N1, N2, N3), dtype=_rdtype(precision), device=dev)
-            ctx.c2r(src.contiguous(), phys, 6)
-            ctx.r2c(phys, self.Q, 6)
+                              ([_on(a, dev, _cdtype(precision)) for a in Bhat] if nf == 6 else []))
+            phys = torch.empty((nf, N1, N2, N3), dtype=_rdtype(precision), device=dev)
+            ctx.c2r(src.contiguous(), phys, nf)
+            ctx.r2c(phys, self.Q, nf)
         self.U = self.Q.clone()
-        self.nvars = 6
-        self.force = torch.zeros((3,) + sh, dtype=_cdtype(precision), device=dev)
-        if forcing:  # kf = 2, f0 = 0.25 (src_MPI/Classes.py:91-94)
+        self.nvars = nf
+        self.Om1, self.Om2, self.Om3 = float(Om1), float(Om2), float(Om3)
+        self.force = torch.zeros((3,) + sh, dtype=_cdtype(precision), device=dev) if nf == 6 else None
+        if forcing and nf == 6:  # kf = 2, f0 = 0.25 (src_MPI/Classes.py:91-94)
             kf, f0 = 2, 0.25
             X = torch.as_tensor(np.asarray(grid.x), device=dev, dtype=torch.float64)
             Y = torch.as_tensor(np.asarray(grid.y), device=dev, dtype=torch.float64)
@@ -142,7 +147,8 @@ class variables:
             ctx.r2c(fp, self.force, 3)
         use_kahan = (precision == 32) if kahan is None else bool(kahan)
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
-        self.computeRHS = computeRHS_MHD
+        self.computeRHS = {"MHD": computeRHS_MHD, 0: computeRHS_NOSGS,
+                           "Orthogonal Dynamics": computeRHS_Ortho}[turb_model]
         self.advanceQ = advanceQ_RK4
 
     @property
@@ -176,11 +182,16 @@ class variables:
         self.U.copy_(self.Q)
 
     def closure_code(self):
+        if self.turb_model == 0:
+            return _capi.MPI_DNS
+        if self.turb_model == "Orthogonal Dynamics":
+            return _capi.MPI_ORTHO
         return _capi.MHD_TMODEL if self.closure == "tmodel" else _capi.MHD
 
     def params(self):
         return _capi.make_params(nu=self.nu, eta=self.lam, t=self.t, dt=self.dt, Ct=self.Ct,
-                                 force=self.force.data_ptr() if self.force is not None else None)
+                                 force=self.force.data_ptr() if self.force is not None else None,
+                                 rotate=self.rotate, Om=(self.Om1, self.Om2, self.Om3))
 
 
 def computeRHS_MHD(main, grid, myFFT=None):
@@ -190,6 +201,17 @@ def computeRHS_MHD(main, grid, myFFT=None):
     rhs = torch.empty_like(main.Q)
     ctx.rhs(main.closure_code(), main.Q, rhs, main.params(), read_out=main.U)
     main.Q = rhs
+
+
+def computeRHS_NOSGS(main, grid, myFFT=None):
+    """src_MPI/RHSfunctions.py:22-93 (RK4 form): 2/3-rule Navier-Stokes."""
+    computeRHS_MHD(main, grid, myFFT)
+
+
+def computeRHS_Ortho(main, grid, myFFT=None):
+    """src_MPI/RHSfunctions.py:179-268 (RK4 form): the Navier-Stokes RHS of u
+    minus that of ``grid.filter(u)``."""
+    computeRHS_MHD(main, grid, myFFT)
 
 
 def advanceQ_RK4(main, grid, myFFT=None):

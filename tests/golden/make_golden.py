@@ -39,6 +39,8 @@ Outputs (all FP64, a few hundred KB in total):
   Smagorinsky, t-model and dynamic Smagorinsky also with rotation), the
   budget file the hooks write at iteration 20, plus the diagnostics;
 * ``mhd_N{N}.npz`` -- one MHD RHS and one RK4 step from the MPI solver;
+* ``mpi_ns_N{N}.npz`` -- the MPI solver's Navier-Stokes and orthogonal
+  dynamics, with and without rotation, one RHS and one RK4 step;
 * ``tgv64_benchmark.npz`` -- the reference's known-answer energy and
   dissipation history (``run/TGV_Validate100/benchmark_sol_64.npz``).
 """
@@ -428,6 +430,39 @@ def gen_mhd(N, seed):
     return out
 
 
+def gen_mpi_ns(N, seed):
+    """The MPI solver's Navier-Stokes RHS and RK4 step (turb_model 0 and
+    'Orthogonal Dynamics', with and without rotation; kc = N/4 so that the
+    filtered field differs)."""
+    C = load_mpi()
+    comm = sys.modules["mpi4py.MPI"].COMM_WORLD
+    x, y, z = orc.periodic_coords(N)
+    u = orc.isotropic_state(N, seed, k0=3.0, normalise="none")
+    phys = [np.fft.irfftn(a, s=(N, N, N), axes=(0, 1, 2)) for a in u]
+    zero = np.zeros((N, N, N))
+    nu, dt = 0.02, 0.005
+    out = {"N": N, "nu": nu, "dt": dt, "kc": N // 4}
+    for name, tm, rot in (("dns", 0, (0, 0., 0., 0.)), ("dns_rot", 0, (1, 0.2, -0.3, 0.4)),
+                          ("ortho", "Orthogonal Dynamics", (0, 0., 0., 0.)),
+                          ("ortho_rot", "Orthogonal Dynamics", (1, 0.2, -0.3, 0.4))):
+        for stage in ("rhs", "step"):
+            with contextlib.redirect_stdout(io.StringIO()):
+                grid = C.gridclass(N, N, N, x, y, z, N // 4, 1, 2 * np.pi, 2 * np.pi, 2 * np.pi, 0, comm, tm)
+                myFFT = C.FFTclass(N, N, N, 1, "pyfftw", N, N, 1, comm, 0)
+                uh = np.zeros((N, N, N // 2 + 1), dtype=complex)
+                vh, wh = uh.copy(), uh.copy()
+                main = C.variables(tm, *rot, grid, phys[0].copy(), phys[1].copy(), phys[2].copy(), zero, zero,
+                                   zero, uh, vh, wh, 0.0, dt, nu, myFFT, 0, "Physical", "RK4")
+                if stage == "rhs":
+                    out["state"] = main.Q.copy()
+                    main.computeRHS(main, grid, myFFT)
+                    out[f"{name}_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+                else:
+                    main.advanceQ(main, grid, myFFT)
+            out[f"{name}_{stage}"] = main.Q.copy()
+    return out
+
+
 def main():
     os.makedirs(HERE, exist_ok=True)
     for N, seed in ((12, 11), (16, 5)):
@@ -438,6 +473,9 @@ def main():
         d = gen_mhd(N, seed)
         np.savez_compressed(os.path.join(HERE, f"mhd_N{N}.npz"), **d)
         print("mhd", N)
+        d = gen_mpi_ns(N, seed + 50)
+        np.savez_compressed(os.path.join(HERE, f"mpi_ns_N{N}.npz"), **d)
+        print("mpi ns", N)
     b = np.load(os.path.join(REF, "PySpectral", "run", "TGV_Validate100", "benchmark_sol_64.npz"))
     np.savez_compressed(os.path.join(HERE, "tgv64_benchmark.npz"), t=np.real(b["t"]),
                         Energy=np.real(b["Energy"]), Dissipation=np.real(b["Dissipation"]))

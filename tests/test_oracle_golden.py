@@ -326,3 +326,22 @@ def test_dsmag_coefficient_by_parseval(N, kc):
     num += np.sum(k0 * (0.5 * np.real(Lm * np.conj(Mm)) + 0.5 * np.real(Lm * Mp)))
     den += np.sum(k0 * (0.5 * np.abs(Mm) ** 2 + 0.5 * np.real(Mm * Mp)))
     assert num / den == pytest.approx(ref, rel=1e-12)
+
+
+MPI_NS = [("dns", 0, False), ("dns_rot", 1, False), ("ortho", 0, True), ("ortho_rot", 1, True)]
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("name,rot,ortho", MPI_NS)
+def test_mpi_navier_stokes_matches_reference(N, name, rot, ortho):
+    """The MPI solver's Navier-Stokes (turb_model 0) and orthogonal dynamics
+    (src_MPI/RHSfunctions.py:22-93, 179-268), one RHS and one RK4 step."""
+    d = golden(f"mpi_ns_N{N}.npz")
+    g = orc.MHDGrid(N, N, N, int(d["kc"]))
+    nu, dt = float(d["nu"]), float(d["dt"])
+    Om = (0.2, -0.3, 0.4)
+    r, s = orc.rhs_mpi_ns(g, d["state"], nu, rot, Om, ortho)
+    assert rel(r, d[f"{name}_rhs"]) < 1e-13
+    assert rel(s, d[f"{name}_uhat"]) < 1e-13
+    Q, _ = orc.advance_rk4(d["state"], lambda q: orc.rhs_mpi_ns(g, q, nu, rot, Om, ortho), dt)
+    assert rel(Q, d[f"{name}_step"]) < 1e-13
