@@ -159,6 +159,16 @@ int psb_rhs_dns_noalloc(psb_ctx* ctx, const void* state, void* rhs, const psb_pa
 int psb_step_rk4(psb_ctx* ctx, int closure, void* state, void* comp, void* read_out, const psb_params* p,
                  int nsteps);
 
+/* nsteps of the MPI solver's semi-implicit scheme for Navier-Stokes, advanceQ_SI
+ * (src_MPI/time_schemes.py:9-11) with the 'Semi-Implicit' branch of computeRHS_NOSGS
+ * (src_MPI/RHSfunctions.py:70-93), in place on `state` (3 fields):
+ *   H <- the 2/3-masked nonlinear term (+ Coriolis),
+ *   Q <- (Q + dt/2 (3 H - H_old) + dt/2 (-nu k^2 u)) / (1 + nu dt/2 k^2).
+ * H (3 fields) holds H_old on entry and the last step's H on exit; start it at
+ * zero (the reference allocates it with np.empty).  read_out: optional, the
+ * masked state the last step read (main.uhat). */
+int psb_step_si(psb_ctx* ctx, void* state, void* H, void* read_out, const psb_params* p, int nsteps);
+
 /* Allocate the context's scratch for `closure` now (so that a later call can
  * be captured in a CUDA graph without allocating). */
 int psb_prepare(psb_ctx* ctx, int closure);

@@ -781,6 +781,36 @@ def rhs_mpi_ns(g, state, nu, rotate=0, Om=(0.0, 0.0, 0.0), ortho=False):
     return np.stack(r), np.stack(s)
 
 
+def step_mpi_si(g, state, H, nu, dt, rotate=0, Om=(0.0, 0.0, 0.0)):
+    """One semi-implicit step of the MPI solver's Navier-Stokes, ``advanceQ_SI``
+    (``src_MPI/time_schemes.py:9-11``) with the 'Semi-Implicit' branch of
+    ``computeRHS_NOSGS`` (``src_MPI/RHSfunctions.py:70-93``): H the masked
+    nonlinear term (+ Coriolis),
+    ``Q = (Q + dt/2 (3 H - H_old) + dt/2 (-nu k^2 u)) / (1 + nu dt/2 k^2)``.
+    Returns ``(Q, H)``."""
+    D = g.dealias_mask
+    k1 = g.k1[:, None, None]
+    k2 = g.k2[None, :, None]
+    k3 = g.k3[None, None, :]
+    s = [D * state[i] for i in range(3)]
+    u, v, w = (_irfftn(x, s=(g.N1, g.N2, g.N3)) for x in s)
+    NL = [_rfftn(x * y) for x, y in ((u, u), (v, v), (w, w), (u, v), (u, w), (v, w))]
+    phat = _pressure(k1, k2, k3, g.ksqr_i, *NL)
+    if rotate == 1:
+        phat = phat + _coriolis_pressure(k1, k2, k3, g.ksqr_i, s[0], s[1], s[2], Om)
+    n0, n1, n2, n3, n4, n5 = NL
+    Hn = [D * (-1j * k1 * n0 - 1j * k2 * n3 - 1j * k3 * n4 - 1j * k1 * phat),
+          D * (-1j * k1 * n3 - 1j * k2 * n1 - 1j * k3 * n5 - 1j * k2 * phat),
+          D * (-1j * k1 * n4 - 1j * k2 * n5 - 1j * k3 * n2 - 1j * k3 * phat)]
+    if rotate == 1:
+        c = _coriolis_force(s[0], s[1], s[2], Om)
+        Hn = [Hn[i] + c[i] for i in range(3)]
+    Hn = np.stack(Hn)
+    visc = np.stack([-nu * g.ksqr * s[i] for i in range(3)])
+    Q = (state + dt / 2.0 * (3.0 * Hn - H) + dt / 2.0 * visc) / (1.0 + nu * dt / 2.0 * g.ksqr[None])
+    return Q, Hn
+
+
 def _mhd_nonlinear(k1, k2, k3, ksqr_i, P):
     """Nonlinear MHD operator from the nine product spectra
     P = (u_iu_j - B_iB_j for 11,22,33,12,13,23, then u x B): the momentum

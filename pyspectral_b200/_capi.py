@@ -23,7 +23,7 @@ NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 
 EXPORTS = (
     "psb_ctx_create", "psb_ctx_destroy", "psb_ctx_set_stream", "psb_last_error", "psb_create_error",
-    "psb_rhs", "psb_step_rk4", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
+    "psb_rhs", "psb_step_rk4", "psb_step_si", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
     "psb_spectrum", "psb_spectrum_nbins", "psb_transfer", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
     "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
     "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
@@ -72,6 +72,7 @@ def load(path: str = LIB_PATH):
         "psb_create_error": ([], ctypes.c_char_p),
         "psb_rhs": ([vp, i, vp, vp, vp, vp, ctypes.POINTER(Params), dp], i),
         "psb_step_rk4": ([vp, i, vp, vp, vp, ctypes.POINTER(Params), i], i),
+        "psb_step_si": ([vp, vp, vp, vp, ctypes.POINTER(Params), i], i),
         "psb_prepare": ([vp, i], i),
         "psb_energy": ([vp, vp, i, dp], i),
         "psb_enstrophy": ([vp, vp, i, dp], i),
@@ -175,6 +176,13 @@ class Context:
                               ctypes.byref(params), ctypes.byref(tau))
         self.check(st, "psb_rhs")
         return tau.value
+
+    def step_si(self, state, H, params, nsteps=1, read_out=None):
+        """Semi-implicit steps of the MPI solver's Navier-Stokes (3 fields; H in/out)."""
+        self.bind_stream()
+        st = self.lib.psb_step_si(self.h, self._ptr(state, self.spec_numel(3)), self._ptr(H, self.spec_numel(3)),
+                                  self._ptr(read_out), ctypes.byref(params), int(nsteps))
+        self.check(st, "psb_step_si")
 
     def step(self, closure, state, params, nsteps=1, comp=None, read_out=None):
         nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else (3 + 3 * max(1, params.fm_nsub) if closure == FM1 else 3)

@@ -20,6 +20,7 @@ template <typename T>
 int products_run(psb_ctx* c, const void* fields, void* out6);
 template <typename T>
 int products_filtered_run(psb_ctx* c, const void* fields, void* out6);
+int si_step(psb_ctx* c, void* Q, void* H, void* read_out, const psb_params* p);
 }  // namespace psbh
 
 namespace {
@@ -783,6 +784,14 @@ int psb_prepare(psb_ctx* c, int closure) {
   if (st != PSB_OK) return st;
   StepIO<float> io{};
   return rhs_dispatch<float>(c, closure, io, &p, nullptr);
+}
+
+int psb_step_si(psb_ctx* c, void* state, void* H, void* read_out, const psb_params* p, int nsteps) {
+  PSB_TRY(check_ctx(c));
+  if (!state || !H || !p || nsteps < 0) return fail(c, PSB_ERR_ARG, "psb_step_si: bad argument");
+  PSB_TRY(set_device(c));
+  for (int s = 0; s < nsteps; ++s) PSB_TRY(si_step(c, state, H, s == nsteps - 1 ? read_out : nullptr, p));
+  return PSB_OK;
 }
 
 int psb_step_rk4(psb_ctx* c, int closure, void* state, void* comp, void* read_out, const psb_params* p, int nsteps) {

@@ -1345,6 +1345,61 @@ __global__ void __launch_bounds__(256) mpi_ortho_combine_kernel(StepIO<T> io, KT
   }
 }
 
+// One semi-implicit step of the MPI solver's Navier-Stokes
+// (src_MPI/time_schemes.py:9-11 with the 'Semi-Implicit' branch of
+// computeRHS_NOSGS, src_MPI/RHSfunctions.py:70-93): H = the masked nonlinear
+// term (+ Coriolis), then
+//   Q <- (Q + dt/2 (3 H - H_old) + dt/2 (-nu k^2 u)) / (1 + nu dt/2 k^2)
+// with u the masked state; H holds H_old on entry and H on exit.
+template <typename T>
+struct EpiMpiSI {
+  static constexpr int F_IN = 6;
+  __host__ double io_bytes(long long npts) const { return (double)sizeof(Cx<T>) * npts * 3 * 5; }
+  Cx<T>* Q;
+  Cx<T>* H;
+  Cx<T>* read_out;
+  long long fstride;
+  int n2, n3h;
+  KTabs<T> k;
+  const double *m1, *m2, *m3;
+  T nu, dt;
+  int rotate;
+  T Om1, Om2, Om3;
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const long long s = ((long long)i1 * n2 + i2) * n3h + i3;
+    const T D = (T)(m1[i1] * m2[i2] * m3[i3]);
+    Cx<T> q[3], u[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      q[f] = Q[f * fstride + s];
+      u[f] = D * q[f];
+    }
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    const T half = dt / (T)2, den = (T)1 + ((nu * dt) / (T)2) * ksq;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> cor;
+      Cx<T> h = mpi_ns_part(k1, k2, k3, ksq, ksqi, (T)0, D, P, u, c, rotate, Om1, Om2, Om3, &cor);
+      if (rotate) h = h + cor;
+      const Cx<T> hold = H[c * fstride + s];
+      const Cx<T> visc = (-nu * ksq) * u[c];
+      const Cx<T> num = (q[c] + half * ((T)3 * h - hold)) + half * visc;
+      Q[c * fstride + s] = mk<T>(num.x / den, num.y / den);
+      H[c * fstride + s] = h;
+      if (read_out) read_out[c * fstride + s] = u[c];
+    }
+  }
+};
+
+template <typename T>
+int mpi_si_step(psb_ctx* c, Cx<T>* Q, Cx<T>* H, Cx<T>* read_out, const psb_params* p) {
+  EpiMpiSI<T> epi{Q, H, read_out, (long long)c->N1 * c->N2 * c->N3h, c->N2, c->N3h, ktabs<T>(c->kx, c->ky, c->kz),
+                  c->mx, c->my, c->mz, (T)p->nu, (T)p->dt, p->rotate, (T)p->Om1, (T)p->Om2, (T)p->Om3};
+  return run_n23<T>(c, Q, PreMask3<T>{c->mx, c->my, c->mz}, PhysProducts<T>{}, epi);
+}
+
 template <typename T>
 int mpi_ns_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p, bool ortho) {
   const int N1 = c->N1, N2 = c->N2, N3h = c->N3h;
@@ -1574,6 +1629,14 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
     default:
       return fail(c, PSB_ERR_UNSUPPORTED, "unknown closure");
   }
+}
+
+int si_step(psb_ctx* c, void* Q, void* H, void* read_out, const psb_params* p) {
+  if (c->prec == 64)
+    return mpi_si_step<double>(c, reinterpret_cast<Cx<double>*>(Q), reinterpret_cast<Cx<double>*>(H),
+                               reinterpret_cast<Cx<double>*>(read_out), p);
+  return mpi_si_step<float>(c, reinterpret_cast<Cx<float>*>(Q), reinterpret_cast<Cx<float>*>(H),
+                            reinterpret_cast<Cx<float>*>(read_out), p);
 }
 
 template int rhs_dispatch<double>(psb_ctx*, int, StepIO<double>, const psb_params*, double*);

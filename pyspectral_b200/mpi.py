@@ -105,8 +105,9 @@ class variables:
                  time_scheme="RK4", precision=64, kahan=None, Bhat=None, forcing=True, closure=None, Ct=0.1):
         if turb_model not in ("MHD", 0, "Orthogonal Dynamics"):
             raise ValueError("turb_model must be 'MHD', 0 or 'Orthogonal Dynamics'")
-        if time_scheme != "RK4":
-            raise ValueError("Error, time scheme " + str(time_scheme) + " not implemented for MHD equations")
+        if time_scheme not in ("RK4", "Semi-Implicit") or (time_scheme != "RK4" and turb_model != 0):
+            raise ValueError("Error, time scheme " + str(time_scheme) + " not implemented for "
+                             + str(turb_model) + " (the semi-implicit scheme is turb_model 0's)")
         if closure not in (None, "tmodel"):
             raise ValueError("closure must be None (plain MHD) or 'tmodel'")
         self.closure = closure
@@ -150,6 +151,11 @@ class variables:
         self.computeRHS = {"MHD": computeRHS_MHD, 0: computeRHS_NOSGS,
                            "Orthogonal Dynamics": computeRHS_Ortho}[turb_model]
         self.advanceQ = advanceQ_RK4
+        if time_scheme == "Semi-Implicit":
+            # H of the last step (src_MPI/Classes.py:49-52 allocates it with np.empty;
+            # here it starts at zero)
+            self.H = torch.zeros_like(self.Q)
+            self.advanceQ = advanceQ_SI
 
     @property
     def uhat(self):
@@ -217,6 +223,12 @@ def computeRHS_Ortho(main, grid, myFFT=None):
 def advanceQ_RK4(main, grid, myFFT=None):
     """src_MPI/time_schemes.py:2-7."""
     grid.ctx(main.precision).step(main.closure_code(), main.Q, main.params(), 1, comp=main.comp, read_out=main.U)
+
+
+def advanceQ_SI(main, grid, myFFT=None):
+    """src_MPI/time_schemes.py:9-11 with the 'Semi-Implicit' branch of
+    computeRHS_NOSGS (src_MPI/RHSfunctions.py:70-93), one fused pass."""
+    grid.ctx(main.precision).step_si(main.Q, main.H, main.params(), 1, read_out=main.U)
 
 
 def advance(main, grid, nsteps):

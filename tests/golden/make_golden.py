@@ -460,6 +460,21 @@ def gen_mpi_ns(N, seed):
                 else:
                     main.advanceQ(main, grid, myFFT)
             out[f"{name}_{stage}"] = main.Q.copy()
+    # the semi-implicit scheme (src_MPI/time_schemes.py:9-11), two steps; H is
+    # allocated with np.empty there, so it is zeroed before the first step
+    for name, rot in (("si", (0, 0., 0., 0.)), ("si_rot", (1, 0.2, -0.3, 0.4))):
+        with contextlib.redirect_stdout(io.StringIO()):
+            grid = C.gridclass(N, N, N, x, y, z, N // 4, 1, 2 * np.pi, 2 * np.pi, 2 * np.pi, 0, comm, 0)
+            myFFT = C.FFTclass(N, N, N, 1, "pyfftw", N, N, 1, comm, 0)
+            uh = np.zeros((N, N, N // 2 + 1), dtype=complex)
+            vh, wh = uh.copy(), uh.copy()
+            main = C.variables(0, *rot, grid, phys[0].copy(), phys[1].copy(), phys[2].copy(), zero, zero,
+                               zero, uh, vh, wh, 0.0, dt, nu, myFFT, 0, "Physical", "Semi-Implicit")
+            main.H[:] = 0.0
+            for k in (1, 2):
+                main.advanceQ(main, grid, myFFT)
+                out[f"{name}_step{k}"] = main.Q.copy()
+                out[f"{name}_H{k}"] = main.H.copy()
     return out
 
 

@@ -345,3 +345,17 @@ def test_mpi_navier_stokes_matches_reference(N, name, rot, ortho):
     assert rel(s, d[f"{name}_uhat"]) < 1e-13
     Q, _ = orc.advance_rk4(d["state"], lambda q: orc.rhs_mpi_ns(g, q, nu, rot, Om, ortho), dt)
     assert rel(Q, d[f"{name}_step"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("name,rot", [("si", 0), ("si_rot", 1)])
+def test_mpi_semi_implicit_matches_reference(N, name, rot):
+    """Two AB2/Crank-Nicolson steps of the MPI solver (H zeroed first)."""
+    d = golden(f"mpi_ns_N{N}.npz")
+    g = orc.MHDGrid(N, N, N, int(d["kc"]))
+    nu, dt = float(d["nu"]), float(d["dt"])
+    Q, H = d["state"], np.zeros_like(d["state"])
+    for k in (1, 2):
+        Q, H = orc.step_mpi_si(g, Q, H, nu, dt, rot, (0.2, -0.3, 0.4))
+        assert rel(Q, d[f"{name}_step{k}"]) < 1e-13
+        assert rel(H, d[f"{name}_H{k}"]) < 1e-13
