@@ -7,8 +7,9 @@ libpyspectral_b200 through the C ABI (``_capi``).
 
 One layout difference: the reference packs uhat, vhat, what into the diagonal
 of a stride-3 array ``Q[i::3, i::3, i::3]`` (src/Classes.py:30-34).  Here
-``main.Q`` is the dense ``(3, N1, N2, N3//2+1)`` tensor holding the same three
-spectra; :func:`to_stride3` / :func:`from_stride3` convert for interop.
+``main.Q`` is the dense ``(nvars, N1, N2, N3//2+1)`` tensor holding the same
+spectra (3, or 3 plus the memory variables of the memory models);
+:func:`to_stride3` / :func:`from_stride3` convert for interop.
 """
 from __future__ import annotations
 
@@ -33,18 +34,20 @@ def _to_dev(a, dtype, device):
 
 
 def to_stride3(Q):
-    """Dense (3,N1,N2,N3h) -> the reference's stride-3 ``Q`` (NumPy)."""
+    """Dense (nvars,N1,N2,N3h) -> the reference's stride-nvars ``Q`` (NumPy):
+    field f at ``Q[f::nvars, f::nvars, f::nvars]`` (nvars = 3, or 3 plus the
+    memory variables of the memory models)."""
     Q = Q.detach().cpu().numpy() if isinstance(Q, torch.Tensor) else np.asarray(Q)
-    _, N1, N2, N3h = Q.shape
-    out = np.zeros((3 * N1, 3 * N2, 3 * N3h), dtype=Q.dtype)
-    for i in range(3):
-        out[i::3, i::3, i::3] = Q[i]
+    nv, N1, N2, N3h = Q.shape
+    out = np.zeros((nv * N1, nv * N2, nv * N3h), dtype=Q.dtype)
+    for i in range(nv):
+        out[i::nv, i::nv, i::nv] = Q[i]
     return out
 
 
-def from_stride3(Q3):
-    """The reference's stride-3 ``Q`` -> dense (3,N1,N2,N3h)."""
-    return np.stack([Q3[i::3, i::3, i::3] for i in range(3)])
+def from_stride3(Q3, nvars=3):
+    """The reference's stride-nvars ``Q`` -> dense (nvars,N1,N2,N3h)."""
+    return np.stack([Q3[i::nvars, i::nvars, i::nvars] for i in range(nvars)])
 
 
 class gridclass:
