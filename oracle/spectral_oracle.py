@@ -542,6 +542,112 @@ def rhs_fm1(g, state, p, dt0=0.1, nsub=1):
     return np.stack(out), np.stack(w[0]), ur
 
 
+def fm2_layout(nsub):
+    """Field offsets of w0^i and w1^i in the FM2 state with
+    ``dt0_subintegrations = dt1_subintegrations = nsub``
+    (``src/Classes.py:330-355``: the pairs interleave, w0 from 3, w1 from 6)."""
+    return [3 + 6 * i for i in range(nsub)], [6 + 6 * i for i in range(nsub)]
+
+
+def rhs_fm2(g, state, p, dt0=0.1, dt1=0.05, nsub=1):
+    """Second-order finite memory model, ``computeRHS_FM2``
+    (``src/RHSfunctions.py:1025-1287``, turb_model 4), cubic grids, equal
+    numbers of w0 and w1 subintegrations (unequal ones index past w1 in the
+    reference, ``:1252``).  PL and PLQL on the full 2x grid; the products
+    ``PL_i (PL_q)_j`` on the 3N grid (``pad`` of the 2x grid); ``PLQL_q u_j``
+    on the 2x grid; ``PLQLQL`` as written at ``:1214-1224`` (including the
+    sign of the ``PLQLuq_up`` term of the u component).  No rotating form
+    (the reference's raises).  Returns ``(rhs, uhat_read)``."""
+    if p.rotate == 1:
+        raise ValueError("computeRHS_FM2 has no rotating form")
+    N1, N2, N3 = g.N1, g.N2, g.N3
+    u, v, w = (nyquist_zero(state[i]) for i in range(3))
+    s2 = scale_2x(g)
+    up, vp, wp = pad_2x(u), pad_2x(v), pad_2x(w)
+    ur, vr, wr = ifft2x(g, up * s2), ifft2x(g, vp * s2), ifft2x(g, wp * s2)
+    P = [fft2x(a * b) for a, b in ((ur, ur), (vr, vr), (wr, wr), (ur, vr), (ur, wr), (vr, wr))]
+    K1, K2, K3 = g.k1f, g.k2f, g.k3f
+    phat = _pressure(K1, K2, K3, g.ksqrf_i, *P)
+    PL = _advection(K1, K2, K3, p.nu, g.ksqrf, phat, P, up, vp, wp)
+    PLq = [separate_modes(x)[1] for x in PL]
+    qr = [ifft2x(g, x * s2) for x in PLq]
+    a = [[fft2x(vel * q) for q in qr] for vel in (ur, vr, wr)]  # a[j][i] = (u_j PLq_i)^ on 2x
+    upu, upv, upw = a[0]
+    vpu, vpv, vpw = a[1]
+    wpu, wpv, wpw = a[2]
+    pt = 2.0 * g.ksqrf_i * (K1 * K1 * upu + K2 * K2 * vpv + K3 * K3 * wpw + K1 * K2 * (upv + vpu)
+                            + K1 * K3 * (upw + wpu) + K2 * K3 * (vpw + wpv))
+    PLQL2 = [-1j * K1 * upu - 1j * K2 * vpu - 1j * K3 * wpu - 1j * K1 * upu - 1j * K2 * upv - 1j * K3 * upw
+             + 1j * K1 * pt,
+             -1j * K1 * upv - 1j * K2 * vpv - 1j * K3 * wpv - 1j * K1 * vpu - 1j * K2 * vpv - 1j * K3 * vpw
+             + 1j * K2 * pt,
+             -1j * K1 * upw - 1j * K2 * vpw - 1j * K3 * wpw - 1j * K1 * wpu - 1j * K2 * wpv - 1j * K3 * wpw
+             + 1j * K3 * pt]
+    PLQLq = [separate_modes(x)[1] for x in PLQL2]
+    # PL x PL_q on the 3N grid
+    sc3 = np.sqrt(3.0 ** 3 * np.sqrt(N1 * N2 * N3))
+
+    def i3n(x):
+        return _irfftn(pad(x) * sc3, s=(3 * N1, 3 * N2, 3 * N3))
+    PLr = [i3n(x) for x in PL]
+    PLqr = [i3n(x) for x in PLq]
+
+    def c3n(x, y):
+        return unpad_2x(unpad(_rfftn(x * y)))
+    # names of the reference: PLa_PLbq = PL_a * (PL_q)_b
+    PLu_PLuq, PLv_PLuq, PLw_PLuq = (c3n(PLr[j], PLqr[0]) for j in range(3))
+    PLu_PLvq, PLv_PLvq, PLw_PLvq = (c3n(PLr[j], PLqr[1]) for j in range(3))
+    PLu_PLwq, PLv_PLwq, PLw_PLwq = (c3n(PLr[j], PLqr[2]) for j in range(3))
+    Qr = [ifft2x(g, x * s2) for x in PLQLq]
+
+    def c2(x, y):
+        return unpad_2x(fft2x(x * y))
+    PLQLuq_up, PLQLvq_up, PLQLwq_up = (c2(Qr[i], ur) for i in range(3))
+    PLQLuq_vp, PLQLvq_vp, PLQLwq_vp = (c2(Qr[i], vr) for i in range(3))
+    PLQLuq_wp, PLQLvq_wp, PLQLwq_wp = (c2(Qr[i], wr) for i in range(3))
+    k1, k2, k3 = g.k1, g.k2, g.k3
+    pterm = g.ksqr_i * (k1 * k1 * PLu_PLuq + k2 * k2 * PLv_PLvq + k3 * k3 * PLw_PLwq + k1 * k2 * (PLv_PLuq + PLu_PLvq)
+                        + k1 * k3 * (PLu_PLwq + PLw_PLuq) + k2 * k3 * (PLv_PLwq + PLw_PLvq))
+    pterm2 = g.ksqr_i * (k1 * k1 * PLQLuq_up + k2 * k2 * PLQLvq_vp + k3 * k3 * PLQLwq_wp
+                         + k1 * k2 * (PLQLvq_up + PLQLuq_vp) + k1 * k3 * (PLQLwq_up + PLQLuq_wp)
+                         + k2 * k3 * (PLQLwq_vp + PLQLvq_wp))
+    qu, qv, qw = (unpad_2x(x) for x in PLQLq)
+    nu = p.nu
+    QQu = (2. * -1j * k1 * PLu_PLuq - 1j * k2 * PLv_PLuq - 1j * k3 * PLw_PLuq - 1j * k2 * PLu_PLvq - 1j * k3 * PLu_PLwq
+           + 2. * 1j * k1 * pterm + -2. * -1j * k1 * PLQLuq_up - 1j * k2 * PLQLvq_up - 1j * k3 * PLQLwq_up
+           - 1j * k2 * PLQLuq_vp - 1j * k3 * PLQLuq_wp + 2. * 1j * k1 * pterm2 - nu * g.ksqr * qu)
+    QQv = (-1j * k1 * PLu_PLvq - 2. * 1j * k2 * PLv_PLvq - 1j * k3 * PLw_PLvq - 1j * k1 * PLv_PLuq - 1j * k3 * PLv_PLwq
+           + 2. * 1j * k2 * pterm + -1j * k1 * PLQLuq_vp - 2. * 1j * k2 * PLQLvq_vp - 1j * k3 * PLQLwq_vp
+           - 1j * k1 * PLQLvq_up - 1j * k3 * PLQLvq_wp + 2. * 1j * k2 * pterm2 - nu * g.ksqr * qv)
+    QQw = (-1j * k1 * PLu_PLwq - 1j * k2 * PLv_PLwq - 2. * 1j * k3 * PLw_PLwq - 1j * k1 * PLw_PLuq - 1j * k2 * PLw_PLvq
+           + 2. * 1j * k3 * pterm + -1j * k1 * PLQLuq_wp - 1j * k2 * PLQLvq_wp - 2. * 1j * k3 * PLQLwq_wp
+           - 1j * k1 * PLQLwq_up - 1j * k3 * PLQLwq_vp + 2. * 1j * k3 * pterm2 - nu * g.ksqr * qw)
+    PLQL = [unpad_2x(x) for x in PLQL2]
+    PLQLQL = [QQu, QQv, QQw]
+    o0, o1 = fm2_layout(nsub)
+    w0 = [state[o:o + 3] for o in o0]
+    w1 = [state[o:o + 3] for o in o1]
+    out = np.zeros((3 + 6 * nsub,) + u.shape, dtype=complex)
+    for c in range(3):
+        out[c] = unpad_2x(PL[c]) + np.sum(np.stack([w0[i][c] for i in range(nsub)], axis=-1), axis=-1)
+    d0, d1 = dt0 / nsub, dt1 / nsub
+    run = [np.zeros_like(u) for _ in range(3)]
+    for i in range(1, nsub + 1):
+        for j in range(1, i):
+            for c in range(3):
+                run[c] = run[c] + 4. / d0 * (-1.) ** (i + j + 1) * w0[j - 1][c]
+        for c in range(3):
+            out[o0[i - 1] + c] = -2. / d0 * w0[i - 1][c] + (-1.) ** (i + 1) * 2. * PLQL[c] + run[c] + w1[i - 1][c]
+    run = [np.zeros_like(u) for _ in range(3)]
+    for i in range(1, nsub + 1):
+        for j in range(1, i):
+            for c in range(3):
+                run[c] = run[c] + 4. / d1 * (-1.) ** (i + j + 1) * w1[j - 1][c]
+        for c in range(3):
+            out[o1[i - 1] + c] = -2. / d1 * w1[i - 1][c] + (-1.) ** (i + 1) * 2. * PLQLQL[c] + run[c]
+    return out, np.stack([u, v, w])
+
+
 def rhs_fm1_2term(g, state, p, dt0=0.1):
     """Two-term first-order finite memory model, ``computeRHS_FM1_2term``
     (``src/RHSfunctions.py:1288-1410``, turb_model 5) on ``(u, w0, w01)``:

@@ -222,7 +222,7 @@ def _diag(Q, nv=3):
 
 
 def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), Ct=-10, dt0=-10,
-                dt1=-10, kc=None, cfl=None, dt0s=-10):
+                dt1=-10, kc=None, cfl=None, dt0s=-10, dt1s=-10):
     kc = N // 2 if kc is None else kc
     x, y, z = orc.periodic_coords(N)
     grid = C.gridclass(N, N, N, x, y, z, kc, 2 * np.pi, 2 * np.pi, 2 * np.pi)
@@ -233,7 +233,7 @@ def serial_case(C, N, state, turb_model, nu, dt, t, rotate=0, Om=(0., 0., 0.), C
     cfl = -dt if cfl is None else cfl
     with contextlib.redirect_stdout(io.StringIO()):
         main = C.variables(0, turb_model, rotate, Om[0], Om[1], Om[2], grid, state[0].copy(),
-                           state[1].copy(), state[2].copy(), t, dt, nu, Ct, dt0, dt0s, dt1, -10, cfl, 3)
+                           state[1].copy(), state[2].copy(), t, dt, nu, Ct, dt0, dt0s, dt1, dt1s, cfl, 3)
     main.iteration = 1
     return grid, myFFT, util, main
 
@@ -260,6 +260,7 @@ def gen_serial(N, seed):
         ("budgets", 99, {}),
         ("fm1", 3, dict(dt0=0.05)),
         ("fm1_rot", 3, dict(dt0=0.05, rotate=1, Om=(0.25, -0.1, 0.4))),
+        ("fm2", 4, dict(dt0=0.05, dt1=0.03)),
         ("ortho", "Orthogonal Dynamics", dict(kc=N // 4)),   # kc = N/4: Gf u != u
         ("ortho_rot", "Orthogonal Dynamics", dict(kc=N // 4, rotate=1, Om=(0.3, 0.1, -0.2))),
     ]
@@ -313,6 +314,22 @@ def gen_serial(N, seed):
             else:
                 ref_rk4_step(main, grid, myFFT, util)
         out[f"fm1w_{stage}"] = _diag(main.Q, 12)
+    # FM2 with two subintegrations each, from non-zero memory variables
+    w2init = 0.2 * np.stack([orc.isotropic_state(N, seed + 400 + i, k0=2.0) for i in range(4)])
+    out["fm2w_init"] = w2init                     # w0^1, w0^2, w1^1, w1^2
+    for stage in ("rhs", "step"):
+        grid, myFFT, util, main = serial_case(C, N, st, 4, nu, dt, t, dt0=0.05, dt1=0.03, dt0s=2, dt1s=2)
+        for i in range(2):
+            main.w0_u[..., i], main.w0_v[..., i], main.w0_w[..., i] = w2init[i]
+            main.w1_u[..., i], main.w1_v[..., i], main.w1_w[..., i] = w2init[2 + i]
+        main.U2Q()
+        with contextlib.redirect_stdout(io.StringIO()):
+            if stage == "rhs":
+                main.computeRHS(main, grid, myFFT, util)
+                out["fm2w_uhat"] = np.stack([main.uhat, main.vhat, main.what])
+            else:
+                ref_rk4_step(main, grid, myFFT, util)
+        out[f"fm2w_{stage}"] = _diag(main.Q, 15)
     # the two-term FM1 (turb_model 5), fresh and from non-zero memory variables
     w0t = 0.2 * np.stack([orc.isotropic_state(N, seed + 300 + i, k0=2.0) for i in range(2)])
     out["fm2t_init"] = w0t

@@ -359,3 +359,33 @@ def test_mpi_semi_implicit_matches_reference(N, name, rot):
         Q, H = orc.step_mpi_si(g, Q, H, nu, dt, rot, (0.2, -0.3, 0.4))
         assert rel(Q, d[f"{name}_step{k}"]) < 1e-13
         assert rel(H, d[f"{name}_H{k}"]) < 1e-13
+
+
+@pytest.mark.parametrize("N", [12, 16])
+@pytest.mark.parametrize("case", ["fm2", "fm2w"])
+def test_fm2_matches_reference(N, case):
+    """turb_model 4 (second-order finite memory model; the oracle only, the
+    GPU path is not built): fresh with one subintegration each, and from
+    non-zero memory variables with two each (interleaved w0/w1 layout)."""
+    d = golden(f"serial_N{N}.npz")
+    g = orc.Grid.periodic(N)
+    p = orc.Params(nu=NU, t=T, dt=DT)
+    st = d["state"]
+    if case == "fm2":
+        nsub, full = 1, np.concatenate([st, np.zeros((6,) + st.shape[1:], complex)])
+    else:
+        nsub = 2
+        full = np.zeros((15,) + st.shape[1:], complex)
+        full[:3] = st
+        o0, o1 = orc.fm2_layout(2)
+        for i in range(2):
+            full[o0[i]:o0[i] + 3] = d["fm2w_init"][i]
+            full[o1[i]:o1[i] + 3] = d["fm2w_init"][2 + i]
+
+    def f(q):
+        return orc.rhs_fm2(g, q, p, dt0=0.05, dt1=0.03, nsub=nsub)
+    r, ur = f(full)
+    assert rel(r, d[f"{case}_rhs"]) < 1e-13
+    assert rel(ur, d[f"{case}_uhat"]) < 1e-13
+    Q, _ = orc.advance_rk4(full, f, DT)
+    assert rel(Q, d[f"{case}_step"]) < 1e-13
