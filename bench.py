@@ -19,7 +19,16 @@ the filtered 256^3 DNS, as recorded with the shipped model.
   (copies on a second stream, overlapping the neighbouring steps' compute;
   no L2 flush between these steps: each upload replaces the state).
 * roofline: dominant kernel of the step, its compulsory bytes per launch over
-  its CUDA-event duration, against MEASURED_PEAKS.json.
+  its CUDA-event duration, against MEASURED_PEAKS.json; every kernel's GB/s
+  and fraction beside it.
+* fp64_plain: the plain FP64 Smagorinsky step on the same state, device-timed
+  and through the public API with host buffers (its own e2e).
+* like_for_like: that FP64 path against the reference's CPU path (oracle port)
+  on the same closure, seed, N and dt, timed in this run: the speed-up on the
+  same work.
+* large: the FP32 learned and Smagorinsky steps at --big-N (128^3 by default),
+  where the fields no longer fit in L2, with per-kernel GB/s and fractions of
+  the measured HBM bandwidth.
 * cpu_baseline: the NumPy oracle port (FP64, scipy.fft with all host cores),
   a bounded sample of the same workload, rank 0 at N=1 only.
 * --impl reference: the reference's CPU implementation of the path (the
@@ -56,6 +65,8 @@ def parse():
     ap.add_argument("--N", type=int, default=64)
     ap.add_argument("--closure", choices=["learned", "smag", "dns"], default="learned")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--big-N", type=int, default=128,
+                    help="also time the FP32 learned and Smagorinsky steps at this size (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of autotuned ones")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup+steps plain RK4 steps of the headline case and exit (for ncu captures)")
@@ -282,6 +293,102 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def kernel_records(ctx, main, grid, flush, nsteps=3):
+    """Per-kernel CUDA-event records of `nsteps` flushed RK4 steps:
+    {name: [launches, ms, compulsory bytes]} and the summed step time."""
+    from pyspectral_b200.RHSfunctions import advance
+    ctx.timing(True)
+    for _ in range(nsteps):
+        flush.zero_()
+        advance(main, grid, 1)
+    recs = ctx.timing_records()
+    ctx.timing(False)
+    per = {}
+    for name, ms, by in recs:
+        a = per.setdefault(name, [0, 0.0, 0.0])
+        a[0] += 1
+        a[1] += ms
+        a[2] += by
+    return per, sum(v[1] for v in per.values()) / nsteps
+
+
+def roofline_of(per, nsteps, step_ms):
+    """Dominant kernel of the step and every kernel's achieved GB/s (compulsory
+    bytes per launch over its CUDA-event duration) against the measured peak."""
+    pk, pk_kind = peaks()
+    dom = max(per.items(), key=lambda kv: kv[1][1])
+    n_l, tot_ms, tot_b = dom[1]
+    achieved = (tot_b / n_l) / (tot_ms / n_l / 1e3) / 1e9
+    kern = {}
+    for k, v in per.items():
+        gbs = (v[2] / v[1] * 1e3 / 1e9) if v[1] > 0 else None
+        kern[k] = {"launches_per_step": v[0] / nsteps, "ms_per_step": v[1] / nsteps, "GBps": gbs,
+                   "frac": gbs / pk if gbs else None, "bytes_per_launch": v[2] / v[0]}
+    return {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": pk, "unit": "GB/s",
+            "frac": achieved / pk, "peak_kind": pk_kind, "traffic": None, "bytes_per_launch": tot_b / n_l,
+            "avg_launch_ms": tot_ms / n_l, "share_of_step": tot_ms / nsteps / step_ms, "kernels": kern}
+
+
+def e2e_measure(grid, main_a, graph_a, main_b, K, dist=None):
+    """The step through the public API with host buffers: every step uploads
+    its state (and Kahan compensation) from pinned host memory and reads the
+    new state back, on a copy stream overlapping the neighbouring steps'
+    compute (two device state buffers).  Returns (ms for K steps, h2d bytes
+    per step, d2h bytes per step)."""
+    import torch
+    from pyspectral_b200.RHSfunctions import StepGraph
+    graph_b = StepGraph(main_b, grid, 1)
+    mains, graphs = (main_a, main_b), (graph_a, graph_b)
+    host = torch.empty_like(main_a.Q, device="cpu").pin_memory()
+    host.copy_(main_a.Q.cpu())
+    hostc = None
+    if main_a.comp is not None:
+        hostc = torch.empty_like(main_a.comp, device="cpu").pin_memory()
+        hostc.copy_(main_a.comp.cpu())
+    outs = [torch.empty_like(host).pin_memory() for _ in range(2)]
+    comp_s = torch.cuda.current_stream()
+    copy_s = torch.cuda.Stream()
+    ev_in = [torch.cuda.Event() for _ in range(2)]
+    ev_done = [torch.cuda.Event() for _ in range(2)]
+
+    def upload(k):
+        b = k % 2
+        with torch.cuda.stream(copy_s):
+            mains[b].Q.copy_(host, non_blocking=True)
+            if hostc is not None:
+                mains[b].comp.copy_(hostc, non_blocking=True)
+            ev_in[b].record(copy_s)
+
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(comp_s)
+    copy_s.wait_stream(comp_s)
+    upload(0)
+    for k in range(K):
+        b = k % 2
+        comp_s.wait_event(ev_in[b])
+        graphs[b].replay()
+        ev_done[b].record(comp_s)
+        if k + 1 < K:
+            upload(k + 1)  # buffer (k+1)%2 is free: its read-back of step k-1 precedes on copy_s
+        with torch.cuda.stream(copy_s):
+            copy_s.wait_event(ev_done[b])
+            outs[b].copy_(mains[b].Q, non_blocking=True)
+    comp_s.wait_stream(copy_s)
+    e1.record(comp_s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    del graph_b
+    h2d = host.numel() * host.element_size() + (hostc.numel() * hostc.element_size() if hostc is not None else 0)
+    return ms, int(h2d), int(outs[0].numel() * outs[0].element_size())
+
+
 def run_ours(args):
     import torch
     rank, world, local = dist_env()
@@ -294,7 +401,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     from pyspectral_b200 import _capi
     from pyspectral_b200 import Classes as C
-    from pyspectral_b200.RHSfunctions import StepGraph, advance, autotune
+    from pyspectral_b200.RHSfunctions import StepGraph, autotune
 
     N = args.N
     st64 = make_state(N, 1 + rank)
@@ -364,100 +471,71 @@ def run_ours(args):
         plain32 = {"value": world * N ** 3 * K64 / (msp / 1e3), "ms_per_step": msp / K64,
                    "what": f"FP32 + Kahan {plain} on the same state"}
 
-    # e2e through the public API: pinned host state -> device, step, device -> host.
-    # Two state buffers on one context: while the compute stream runs step k,
-    # a copy stream reads back step k-1 and uploads step k+1's input.
-    ctx = grid32.ctx(32)
+    # e2e through the public API: pinned host state -> device, step, device -> host
     tmain = {"learned": "learned", "smag": 1, "dns": 0}[args.closure]
     m32b = C.variables(0, tmain, 0, 0, 0, 0, grid32, st64[0], st64[1], st64[2], 0.0, 2e-3, 1e-3,
                        precision=32, model=model if args.closure == "learned" else None)
-    g32b = StepGraph(m32b, grid32, 1)
-    mains, graphs = (m32, m32b), (g32, g32b)
-    host = torch.empty_like(m32.Q, device="cpu").pin_memory()
-    host.copy_(m32.Q.cpu())
-    hostc = torch.empty_like(m32.comp, device="cpu").pin_memory()
-    hostc.copy_(m32.comp.cpu())
-    outs = [torch.empty_like(host).pin_memory() for _ in range(2)]
     Ke = max(10, args.steps // 4)
-    comp_s = torch.cuda.current_stream()
-    copy_s = torch.cuda.Stream()
-    ev_in = [torch.cuda.Event() for _ in range(2)]
-    ev_done = [torch.cuda.Event() for _ in range(2)]
-
-    def upload(k):
-        b = k % 2
-        with torch.cuda.stream(copy_s):
-            mains[b].Q.copy_(host, non_blocking=True)
-            mains[b].comp.copy_(hostc, non_blocking=True)
-            ev_in[b].record(copy_s)
-
-    torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(comp_s)
-    copy_s.wait_stream(comp_s)
-    upload(0)
-    for k in range(Ke):
-        b = k % 2
-        comp_s.wait_event(ev_in[b])
-        graphs[b].replay()
-        ev_done[b].record(comp_s)
-        if k + 1 < Ke:
-            upload(k + 1)  # buffer (k+1)%2 is free: its read-back of step k-1 precedes on copy_s
-        with torch.cuda.stream(copy_s):
-            copy_s.wait_event(ev_done[b])
-            outs[b].copy_(mains[b].Q, non_blocking=True)
-    comp_s.wait_stream(copy_s)
-    e1.record(comp_s)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * N ** 3 * Ke / (e2e_ms / 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": int(host.numel() * host.element_size() * 2),
-           "d2h_bytes_per_step": int(outs[0].numel() * outs[0].element_size()),
+    e2e_ms, h2d, d2h = e2e_measure(grid32, m32, g32, m32b, Ke, dist)
+    e2e = {"value": world * N ** 3 * Ke / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h,
            "how": "pinned host state uploaded and the new state read back every step, on a copy stream "
                   "overlapping the previous step's compute (two device state buffers)"}
-    del g32b
+    # the same for the plain FP64 path (like for like with the reference arm)
+    m64b = C.variables(0, {"smag": 1, "dns": 0}[plain], 0, 0, 0, 0, grid64, st64[0], st64[1], st64[2], 0.0,
+                       2e-3, 1e-3, precision=64)
+    g64 = StepGraph(m64, grid64, 1)
+    e64_ms, h2d64, d2h64 = e2e_measure(grid64, m64, g64, m64b, Ke, dist)
+    del g64
+    e2e64 = {"value": world * N ** 3 * Ke / (e64_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d64,
+             "d2h_bytes_per_step": d2h64}
 
     # live per-kernel timing of 3 flushed steps for the roofline
-    ctx.timing(True)
-    for _ in range(3):
-        flush.zero_()
-        advance(m32, grid32, 1)
-    recs = ctx.timing_records()
-    ctx.timing(False)
-    per = {}
-    for name, ms, by in recs:
-        a = per.setdefault(name, [0, 0.0, 0.0])
-        a[0] += 1
-        a[1] += ms
-        a[2] += by
-    dom = max(per.items(), key=lambda kv: kv[1][1])
-    n_l, tot_ms, tot_b = dom[1]
-    pk, pk_kind = peaks()
-    achieved = (tot_b / n_l) / (tot_ms / n_l / 1e3) / 1e9
-    step_ms = sum(v[1] for v in per.values()) / 3.0
-    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": pk, "unit": "GB/s",
-                "frac": achieved / pk, "peak_kind": pk_kind, "traffic": None,
-                "bytes_per_launch": tot_b / n_l, "avg_launch_ms": tot_ms / n_l,
-                "share_of_step": tot_ms / 3.0 / step_ms,
-                "kernels": {k: {"launches_per_step": v[0] / 3, "ms_per_step": v[1] / 3,
-                                "GBps": (v[2] / v[1] * 1e3 / 1e9) if v[1] > 0 else None} for k, v in per.items()}}
+    ctx = grid32.ctx(32)
+    per, step_ms = kernel_records(ctx, m32, grid32, flush, 3)
+    roofline = roofline_of(per, 3, step_ms)
     traffic_file = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(traffic_file):
         try:
             tf = json.load(open(traffic_file))
-            roofline["traffic"] = tf.get(dom[0], {}).get(f"N{N}_f32")
+            roofline["traffic"] = tf.get(roofline["kernel"], {}).get(f"N{N}_f32")
         except Exception:
             pass
+
+    # 128^3: where the fields no longer fit in L2 (the HBM roofline of the FP32 kernels)
+    big = None
+    if args.big_N:  # every rank (the timing's barrier and max-reduce are collective)
+        big = {"N": args.big_N}
+        Nb = args.big_N
+        stb = make_state(Nb, 1 + rank)
+        for cl in ("learned", "smag"):
+            gridb = C.gridclass.periodic(Nb, device=local)
+            mb = C.variables(0, {"learned": "learned", "smag": 1}[cl], 0, 0, 0, 0, gridb, stb[0], stb[1],
+                             stb[2], 0.0, 2e-3, 1e-3, precision=32, model=model if cl == "learned" else None)
+            if not args.no_tune:
+                autotune(mb, gridb)
+            Kb = max(4, args.steps // 8)
+            msb, _, gb = timed(gridb, mb, Kb, args.warmup)
+            del gb
+            perb, stepb = kernel_records(gridb.ctx(32), mb, gridb, flush, 3)
+            rb = roofline_of(perb, 3, stepb)
+            big[cl + "_fp32"] = {"value": world * Nb ** 3 * Kb / (msb / 1e3), "ms_per_step": msb / Kb,
+                                  "roofline": rb}
+        del stb
 
     cufft_ms = cufft_baseline_ms(N, max(5, args.steps // 10), plain, flush) if rank == 0 else None
     if rank == 0:
         cb = cpu_baseline(N, args.closure, args.cpu_seconds) if world == 1 else None
+        # like for like with the reference arm: the same closure (plain FP64
+        # Smagorinsky), seed, N and dt on both sides
+        cref = cpu_baseline(N, plain, args.cpu_seconds) if world == 1 else None
+        lfl = None
+        if cref is not None:
+            lfl = {"what": f"FP64 {plain}, {N}^3, seed 1, dt=2e-3, nu=1e-3: this GPU path vs the reference's "
+                           f"CPU path (oracle port, {cref['cores']} host cores) on the same work",
+                   "gpu_fp64_value": value64, "gpu_fp64_e2e": e2e64["value"], "cpu_fp64_value": cref["value"],
+                   "ratio": value64 / cref["value"], "e2e_ratio": e2e64["value"] / cref["value"],
+                   "cpu_sample": cref["sample"]}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
@@ -470,13 +548,14 @@ def run_ours(args):
                        "launch_shapes": "default" if args.no_tune else
                        "autotuned per path (psb_autotune: tiles and radix orders timed on the state)"},
             "fp64_plain": {"value": value64, "ms_per_step": ms64 / K64, "closure": plain,
-                           "ratio_headline_over_fp64_plain": value / value64},
+                           "ratio_headline_over_fp64_plain": value / value64, "e2e": e2e64},
+            "like_for_like": lfl,
             "fp32_plain": plain32,
             "tuned_shapes": None if args.no_tune else grid32.ctx(32).tuned_shapes(m32.closure_code()),
             "accuracy": accuracy_record(args.closure, model),
             "cufft_library_baseline": {"value": N ** 3 / (cufft_ms / 1e3), "ms_per_step": cufft_ms,
                                        "what": f"FP32 {plain} step from torch.fft (cuFFT) + torch elementwise ops"},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clocks,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cb, "clocks": clocks, "large": big,
             "gpu_launches": int(launches), "finite": bool(ok),
         }
         print(json.dumps(line))

@@ -139,14 +139,17 @@ int psb_rhs(psb_ctx* ctx, int closure, const void* state, void* rhs, void* w0, v
 
 /* DNS right-hand side (same result as psb_rhs with PSB_DNS) that allocates no
  * device memory.  No counterpart in the reference.  For callers that cannot
- * call cudaMalloc when they evaluate the RHS: code inside a CUDA stream
- * capture, hosts whose pool allocator owns the device memory, time-critical
- * loops that cannot take cudaMalloc's implicit synchronisation.  Scratch is a
- * fixed 8,847,360-byte __device__ array in the library (enough for a 32^3
- * grid, FP64 or FP32); larger grids return PSB_ERR_SHAPE.  The first call on
- * a device looks up the array's address (make it before any stream capture).
- * All calls share the array, so calls that overlap on the GPU race; serialise
- * them.  The context itself must already exist (psb_ctx_create allocates). */
+ * call cudaMalloc when they evaluate the RHS: hosts whose pool allocator owns
+ * the device memory (a library cudaMalloc would fail), time-critical loops
+ * that cannot take cudaMalloc's implicit synchronisation.  Scratch is a fixed
+ * 8,847,360-byte __device__ array in the library; a grid needs
+ * 16.875 * N1*N2*N3 complex elements of it (each buffer rounded up to 256 B),
+ * so N1*N2*N3 may be at most 32^3 in FP64 and 2*32^3 in FP32 (e.g. 32^3 or
+ * 32x32x64); larger grids return PSB_ERR_SHAPE.  The first call on a device
+ * looks up the array's address (make it before any stream capture).  All
+ * calls share the array, so calls that overlap on the GPU race; serialise
+ * them.  The caller's current device is left as it was.  The context itself
+ * must already exist (psb_ctx_create allocates). */
 int psb_rhs_dns_noalloc(psb_ctx* ctx, const void* state, void* rhs, const psb_params* p);
 
 /* nsteps of advanceQ_RK4 (src/PySpec_3d.py:96-105; src_MPI/time_schemes.py:2-7):
@@ -297,6 +300,14 @@ int psb_autotune(psb_ctx* ctx, int closure, void* state, const psb_params* p);
 int psb_tuned_shape(const psb_ctx* ctx, int closure, int pass, int* tile, int* radices, int maxr);
 /* Back to the default shapes for closure. */
 int psb_autotune_clear(psb_ctx* ctx, int closure);
+/* Set the launch shape of pass 0..4 of closure (DNS, SMAG, LEARNED) by hand:
+ * tile (columns per CTA, a power of two <= 32; pencils per CTA for the z pass,
+ * a power of two <= the closure's bound) and the radix order of its transform
+ * (nrad radices from {2,3,4,6,8,12,16} whose product is the pass's padded
+ * length).  Replays a saved psb_autotune result (the pyFFTW plans of
+ * src/Classes.py:590-625 carry no such choice: this is the autotuner's cache).
+ * The other passes keep their tuned or default shapes. */
+int psb_set_tuned_shape(psb_ctx* ctx, int closure, int pass, int tile, const int* radices, int nrad);
 
 #ifdef __cplusplus
 }

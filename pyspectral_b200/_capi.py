@@ -30,7 +30,7 @@ EXPORTS = (
     "psb_mlp_forward_tc",
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
-    "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear",
+    "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear", "psb_set_tuned_shape",
 )
 
 
@@ -94,6 +94,7 @@ def load(path: str = LIB_PATH):
         "psb_autotune": ([vp, i, vp, ctypes.POINTER(Params)], i),
         "psb_tuned_shape": ([vp, i, i, ip, ip, i], i),
         "psb_autotune_clear": ([vp, i], i),
+        "psb_set_tuned_shape": ([vp, i, i, i, ip, i], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -287,6 +288,17 @@ class Context:
 
     def autotune_clear(self, closure):
         self.check(self.lib.psb_autotune_clear(self.h, closure), "psb_autotune_clear")
+
+    def set_tuned_shapes(self, closure, shapes):
+        """Use the given launch shapes ([{"tile": t, "radices": [...]}] per pass,
+        as tuned_shapes() returns them; None entries keep a pass's shape)."""
+        for p, sh in enumerate(shapes):
+            if sh is None:
+                continue
+            rad = list(sh["radices"])
+            arr = (ctypes.c_int * max(1, len(rad)))(*rad)
+            self.check(self.lib.psb_set_tuned_shape(self.h, closure, p, int(sh["tile"]), arr, len(rad)),
+                       "psb_set_tuned_shape")
 
     def launch_count(self):
         n = ctypes.c_ulonglong()

@@ -257,6 +257,15 @@ struct Batch {
         epi[i * R + r] = mkepi(c, io, b->params[r]);
       }
     }
+    // The argument blocks are read by every kernel of the previous steps that
+    // may still be queued on the context stream (a non-blocking stream, not
+    // ordered with the legacy default stream): drain it before rewriting
+    // them, then upload on that stream so the next launches follow the copy.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PSB_TRY(cuda_ok(c, cudaStreamIsCapturing(c->stream, &cap), "batch arguments: capture status"));
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(c, PSB_ERR_ARG, "psb_batch: runs changed while the stream is being captured; set them first");
+    PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "batch arguments: drain the stream"));
     if (b->dargs_bytes < ab) {
       if (b->dargs) cudaFree(b->dargs);
       b->dargs = nullptr;
@@ -264,7 +273,8 @@ struct Batch {
       PSB_TRY(cuda_ok(c, cudaMalloc(&b->dargs, ab), "batch arguments"));
       b->dargs_bytes = ab;
     }
-    PSB_TRY(cuda_ok(c, cudaMemcpy(b->dargs, b->host.data(), ab, cudaMemcpyHostToDevice), "batch arguments upload"));
+    PSB_TRY(cuda_ok(c, cudaMemcpyAsync(b->dargs, b->host.data(), ab, cudaMemcpyHostToDevice, c->stream),
+                    "batch arguments upload"));
     views(reinterpret_cast<char*>(b->dargs));
     return PSB_OK;
   }

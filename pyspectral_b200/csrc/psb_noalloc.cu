@@ -1,14 +1,12 @@
 // DNS right-hand side without any device allocation.
 //
 // Who needs this: callers that must not allocate device memory at the time
-// they evaluate the RHS.  Examples are code running inside a CUDA stream
-// capture (a cudaMalloc/cudaFree there is not recorded into the graph and
-// cudaFree is illegal while capturing), host applications whose own pool
-// allocator has reserved the device memory so that a library cudaMalloc fails
-// with out-of-memory, and time-critical loops that cannot afford the implicit
-// device synchronisation of cudaMalloc/cudaFree.  psb_rhs allocates its
-// scratch on first use; psb_rhs_dns_noalloc instead works in a fixed scratch
-// array that is part of the library image.
+// they evaluate the RHS.  Examples are host applications whose own pool
+// allocator has reserved the device memory up front, so that a cudaMalloc
+// from a library fails with out-of-memory, and time-critical loops that
+// cannot afford the implicit device synchronisation of cudaMalloc/cudaFree.
+// psb_rhs allocates its scratch on first use; psb_rhs_dns_noalloc instead
+// works in a fixed scratch array that is part of the library image.
 //
 // The scratch is a file-scope __device__ array of kNoAllocBytes.  Every GPU
 // that loads this part of the library holds it until the process exits.  Host
@@ -18,7 +16,9 @@
 // capture.  All calls share the one array: calls that overlap on the GPU (two
 // streams, two host threads) race on it and must be serialised by the caller.
 // Every scratch element the pipeline reads is written earlier in the same
-// call, so nothing needs clearing between calls.
+// call, so nothing needs clearing between calls.  The caller's current device
+// is restored before the call returns.  Launches are counted and, with
+// psb_timing_enable on, timed like those of psb_rhs (same pass names).
 #include <mutex>
 
 #include "psb_ctx.cuh"
@@ -47,18 +47,31 @@ size_t noalloc_bytes(const psb_ctx* c) {
 }
 
 template <typename T, bool INV, class Pre>
-int axis(psb_ctx* c, AxisArgs<T> a, Pre pre) {
+int axis(psb_ctx* c, AxisArgs<T> a, Pre pre, const char* what) {
   const size_t esz = sizeof(Cx<T>);
   const int L = a.plan.L;
   a.col_tile = pick_ct(a.ncols, Pre::F_DST, L, esz);
   const size_t smem = (size_t)(L + 2 * L * Pre::F_DST * a.col_tile) * esz;
   dim3 grid((a.ncols + a.col_tile - 1) / a.col_tile, a.nouter);
+  const double bytes = (double)esz * a.nouter * a.ncols *
+                       ((double)Pre::F_SRC * count_mapped(a.in_map, a.in_rows) + (double)Pre::F_DST * a.out_rows);
   auto k = axis_pass_kernel<T, INV, Pre>;
   set_smem(k, smem);
-  ++c->launches;
+  LaunchScope scope(c, what, bytes);
   k<<<grid, 256, smem, c->stream>>>(a, pre);
-  return launch_ok(c, "noalloc axis pass");
+  return launch_ok(c, what);
 }
+
+// Restores the caller's current device when the entry point returns.
+struct DeviceGuard {
+  int prev = -1;
+  DeviceGuard() {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 
 template <typename T>
 int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, unsigned char* base) {
@@ -88,7 +101,7 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
   a.out_rows = M1;
   a.in_map = map_pad32(N1);
   a.out_map = map_id(M1);
-  PSB_TRY((axis<T, true>(c, a, PreCopyN<T, 3>{})));
+  PSB_TRY((axis<T, true>(c, a, PreCopyN<T, 3>{}, "x-inverse")));
   AxisArgs<T> b{};
   b.plan = *plan_for(c, M2);
   b.tw = tw;
@@ -105,7 +118,7 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
   b.out_rows = M2;
   b.in_map = map_pad32(N2);
   b.out_map = map_id(M2);
-  PSB_TRY((axis<T, true>(c, b, PreCopy<T>{})));
+  PSB_TRY((axis<T, true>(c, b, PreCopy<T>{}, "y-inverse")));
   ZArgs<T> z{};
   const long long fsP = (long long)M1 * M2 * Kz;
   for (int f = 0; f < 3; ++f) {
@@ -131,9 +144,10 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
     z.ppc = P;
     auto k = zpass_kernel<T, PhysProducts<T>>;
     set_smem(k, smem_for(P));
-    ++c->launches;
+    const double zbytes = (double)e * z.npencils * Kz * (3.0 + 6.0);
+    LaunchScope scope(c, "z-fused", zbytes);
     k<<<(unsigned)((z.npencils + P - 1) / P), 256, smem_for(P), c->stream>>>(z, PhysProducts<T>{});
-    PSB_TRY(launch_ok(c, "noalloc z pass"));
+    PSB_TRY(launch_ok(c, "z-fused"));
   }
   AxisArgs<T> d{};
   d.plan = *plan_for(c, M2);
@@ -151,7 +165,7 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
   d.out_rows = N2;
   d.in_map = map_id(M2);
   d.out_map = map_pad32(N2);
-  PSB_TRY((axis<T, false>(c, d, PreCopy<T>{})));
+  PSB_TRY((axis<T, false>(c, d, PreCopy<T>{}, "y-forward")));
   StepIO<T> io{};
   io.Q = const_cast<Cx<T>*>(Q);
   io.rhs_out = rhs;
@@ -184,9 +198,10 @@ int dns_noalloc(psb_ctx* c, const Cx<T>* Q, Cx<T>* rhs, const psb_params* p, uns
   const size_t smem = (size_t)(M1 + 2 * M1 * 6 * ea.col_tile) * e;
   auto k = xfwd_epi_kernel<T, EpiNS<T, false>>;
   set_smem(k, smem);
-  ++c->launches;
+  const double ebytes = epi.io_bytes((long long)N1 * N2 * N3h) + (double)e * 6 * M1 * N2 * Kz;
+  LaunchScope scope(c, "x-forward+epilogue", ebytes);
   k<<<ea.main_blocks + extra, 256, smem, c->stream>>>(ea, epi);
-  return launch_ok(c, "noalloc x-forward+epilogue");
+  return launch_ok(c, "x-forward+epilogue");
 }
 
 }  // namespace
@@ -198,8 +213,9 @@ extern "C" int psb_rhs_dns_noalloc(psb_ctx* c, const void* state, void* rhs, con
   if (need > kNoAllocBytes)
     return fail(c, PSB_ERR_SHAPE,
                 "psb_rhs_dns_noalloc: grid needs " + std::to_string(need) + " scratch bytes, the fixed array holds " +
-                    std::to_string(kNoAllocBytes) + " (up to a 32^3 grid); use psb_rhs");
+                    std::to_string(kNoAllocBytes) + " (N1*N2*N3 up to 32^3 in FP64, 2*32^3 in FP32); use psb_rhs");
   if (c->dev < 0 || c->dev >= kMaxDevices) return fail(c, PSB_ERR_ARG, "psb_rhs_dns_noalloc: device index too large");
+  DeviceGuard restore;
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   void* base = nullptr;
   {

@@ -1667,31 +1667,59 @@ bool plan_is_wide(const FFTPlan& p) {
   return false;
 }
 
+// Field counts and limits of the five passes of a tunable closure.
+// Fi / Fb: fields after the x / y pass; Fz: z-pass inputs (its smem bound);
+// Fy / Gy: lines per column and outer groups of the y-inverse pass
+struct TuneDims {
+  int Fi, Fb, Fz, Fo, maxppc, defppc, Fy = 1, Gy;
+  size_t zextra = 0;
+  int Ls[5], Fs[5];
+};
+
+template <typename T>
+TuneDims tune_dims(psb_ctx* c, int closure) {
+  TuneDims t;
+  if (closure == PSB_DNS) {
+    t.Fi = t.Fb = t.Gy = 3, t.Fo = 6, t.maxppc = phys_max_ppc<PhysProducts<T>>::value;
+    t.Fz = PhysProducts<T>::F_IN;
+    t.defppc = phys_default_ppc<PhysProducts<T>>::value;
+  } else if (closure == PSB_SMAG) {
+    t.Fi = t.Fb = t.Gy = 9, t.Fo = 12, t.maxppc = phys_max_ppc<PhysSmag<T>>::value;
+    t.Fz = PhysSmag<T>::F_IN;
+    t.defppc = phys_default_ppc<PhysSmag<T>>::value;
+  } else {
+    t.Fi = PreGradXY<T>::F_DST, t.Fb = pre_b_fields<PreGradXY<T>>::value, t.Fo = 6;
+    t.Fy = PreYGrad<T>::F_DST;
+    t.Gy = pre_ypass<T, PreGradXY<T>>::groups;
+    t.Fz = PhysLearned<T>::F_IN;
+    t.maxppc = phys_max_ppc<PhysLearned<T>>::value;
+    t.defppc = phys_default_ppc<PhysLearned<T>>::value;
+    t.zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
+  }
+  const int M1 = 3 * c->N1 / 2, M2 = 3 * c->N2 / 2, M3 = 3 * c->N3 / 2;
+  const int Ls[5] = {M1, M2, M3, M2, M1};
+  const int Fs[5] = {t.Fi, t.Fy, 0, 1, t.Fo};
+  for (int k = 0; k < 5; ++k) {
+    t.Ls[k] = Ls[k];
+    t.Fs[k] = Fs[k];
+  }
+  return t;
+}
+
+// Shared memory of pass k with tile `tile` (columns, or pencils per CTA for the z pass).
+template <typename T>
+size_t pass_smem(const TuneDims& t, int k, int tile) {
+  if (k == 2) return zpass_smem_bytes<T>(std::max(t.Fz, t.Fo), tile, t.Ls[2], t.zextra);
+  return (size_t)(t.Ls[k] + 2 * (size_t)t.Ls[k] * t.Fs[k] * tile) * sizeof(Cx<T>);
+}
+
 template <typename T>
 int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int M1 = 3 * N1 / 2, M2 = 3 * N2 / 2, M3 = 3 * N3 / 2, Kz = N3 / 2;
-  // Fi / Fb: fields after the x / y pass; Fz: z-pass inputs (its smem bound);
-  // Fy / Gy: lines per column and outer groups of the y-inverse pass
-  int Fi, Fb, Fz, Fo, maxppc, defppc, Fy = 1, Gy;
-  size_t zextra = 0;
-  if (closure == PSB_DNS) {
-    Fi = Fb = Gy = 3, Fo = 6, maxppc = phys_max_ppc<PhysProducts<T>>::value;
-    Fz = PhysProducts<T>::F_IN;
-    defppc = phys_default_ppc<PhysProducts<T>>::value;
-  } else if (closure == PSB_SMAG) {
-    Fi = Fb = Gy = 9, Fo = 12, maxppc = phys_max_ppc<PhysSmag<T>>::value;
-    Fz = PhysSmag<T>::F_IN;
-    defppc = phys_default_ppc<PhysSmag<T>>::value;
-  } else {
-    Fi = PreGradXY<T>::F_DST, Fb = pre_b_fields<PreGradXY<T>>::value, Fo = 6;
-    Fy = PreYGrad<T>::F_DST;
-    Gy = pre_ypass<T, PreGradXY<T>>::groups;
-    Fz = PhysLearned<T>::F_IN;
-    maxppc = phys_max_ppc<PhysLearned<T>>::value;
-    defppc = phys_default_ppc<PhysLearned<T>>::value;
-    zextra = (size_t)phys_is_block<PhysLearned<T>>::extra;
-  }
+  const TuneDims td = tune_dims<T>(c, closure);
+  const int Fi = td.Fi, Fz = td.Fz, Fo = td.Fo, maxppc = td.maxppc, defppc = td.defppc, Fy = td.Fy, Gy = td.Gy;
+  const size_t zextra = td.zextra;
   const size_t esz = sizeof(Cx<T>);
   const size_t n = (size_t)3 * N1 * N2 * N3h;
   int st = PSB_OK;
@@ -1709,8 +1737,8 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   while (P > 1 && zsmem(P) > kSmemBudget) P /= 2;
   while (P > 1 && ((long long)M1 * M2 + P - 1) / P < 2 * 148) P /= 2;
   psb_tuned t;
-  const int Ls[5] = {M1, M2, M3, M2, M1};
-  const int Fs[5] = {Fi, Fy, 0, 1, Fo};
+  const int* Ls = td.Ls;
+  const int* Fs = td.Fs;
   t.pass[0].tile = pick_ct(Kz, Fi, M1, esz, N2);
   t.pass[1].tile = pick_ct(Kz, Fy, M2, esz, Gy * M1);
   t.pass[2].tile = P;
@@ -1785,6 +1813,59 @@ int tune_rhs(psb_ctx* c, int closure, const void* state, const psb_params* p) {
   c->timing = timing_was;
   if (status != PSB_OK) c->tuned.erase(closure);
   return status;
+}
+
+// A caller-given launch shape for pass k of `closure` (a saved autotuner
+// result, or a shape a test wants to exercise): checked against the pass's
+// transform length, the radices the kernels have and the shared-memory budget.
+template <typename T>
+int set_shape(psb_ctx* c, int closure, int k, int tile, const int* radices, int nrad) {
+  const TuneDims td = tune_dims<T>(c, closure);
+  const int L = td.Ls[k];
+  if (nrad < 1 || nrad > kMaxPasses) return fail(c, PSB_ERR_ARG, "psb_set_tuned_shape: 1..12 radices");
+  long long prod = 1;
+  bool wide = false;
+  FFTPlan q = *plan_for(c, L);
+  q.npass = nrad;
+  for (int s = 0; s < nrad; ++s) {
+    const int r = radices[s];
+    if (r != 2 && r != 3 && r != 4 && r != 6 && r != 8 && r != 12 && r != 16)
+      return fail(c, PSB_ERR_ARG, "psb_set_tuned_shape: radices must be 2, 3, 4, 6, 8, 12 or 16");
+    wide = wide || r > 8 || r == 6;
+    prod *= r;
+    q.radix[s] = r;
+  }
+  for (int s = nrad; s < kMaxPasses; ++s) q.radix[s] = 0;
+  if (prod != L)
+    return fail(c, PSB_ERR_SHAPE, "psb_set_tuned_shape: the radices multiply to " + std::to_string(prod) +
+                                      ", the pass transforms " + std::to_string(L) + " points");
+  const int tmax = k == 2 ? td.maxppc : 32;
+  if (tile < 1 || tile > tmax || (tile & (tile - 1)))
+    return fail(c, PSB_ERR_ARG, "psb_set_tuned_shape: tile must be a power of two <= " + std::to_string(tmax));
+  if (pass_smem<T>(td, k, tile) > kSmemBudget)
+    return fail(c, PSB_ERR_SHAPE, "psb_set_tuned_shape: tile needs more shared memory than the budget");
+  auto it = c->tuned.find(closure);
+  if (it == c->tuned.end()) {
+    // start from the default shapes of every pass
+    const int Kz = c->N3 / 2;
+    const size_t esz = sizeof(Cx<T>);
+    psb_tuned t;
+    int P = td.defppc;
+    while (P > 1 && pass_smem<T>(td, 2, P) > kSmemBudget) P /= 2;
+    while (P > 1 && ((long long)td.Ls[0] * td.Ls[1] + P - 1) / P < 2 * 148) P /= 2;
+    t.pass[0].tile = pick_ct(Kz, td.Fi, td.Ls[0], esz, c->N2);
+    t.pass[1].tile = pick_ct(Kz, td.Fy, td.Ls[1], esz, td.Gy * td.Ls[0]);
+    t.pass[2].tile = P;
+    t.pass[3].tile = pick_ct(Kz, 1, td.Ls[3], esz, td.Fo * td.Ls[0]);
+    t.pass[4].tile = pick_ct(Kz, td.Fo, td.Ls[4], esz, c->N2);
+    for (int j = 0; j < 5; ++j) t.pass[j].plan = *plan_for(c, td.Ls[j]);
+    it = c->tuned.emplace(closure, t).first;
+  }
+  psb_pass_shape& sh = it->second.pass[k];
+  sh.tile = tile;
+  sh.plan = q;
+  sh.wide = wide;
+  return PSB_OK;
 }
 
 }  // namespace tuning
@@ -1869,5 +1950,14 @@ extern "C" int psb_autotune(psb_ctx* c, int closure, void* state, const psb_para
   PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
   return c->prec == 64 ? psbh::tuning::tune_rhs<double>(c, closure, state, p)
                         : psbh::tuning::tune_rhs<float>(c, closure, state, p);
+}
+
+extern "C" int psb_set_tuned_shape(psb_ctx* c, int closure, int pass, int tile, const int* radices, int nrad) {
+  if (!c) return PSB_ERR_ARG;
+  if (closure != PSB_DNS && closure != PSB_SMAG && closure != PSB_LEARNED)
+    return fail(c, PSB_ERR_UNSUPPORTED, "psb_set_tuned_shape: closure not tunable (DNS, SMAG, LEARNED are)");
+  if (pass < 0 || pass > 4 || !radices) return fail(c, PSB_ERR_ARG, "psb_set_tuned_shape: bad argument");
+  return c->prec == 64 ? psbh::tuning::set_shape<double>(c, closure, pass, tile, radices, nrad)
+                        : psbh::tuning::set_shape<float>(c, closure, pass, tile, radices, nrad);
 }
 

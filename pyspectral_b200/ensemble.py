@@ -14,6 +14,18 @@ The learned closure is used where the model was trained (the filter width
 of its training data, 2 pi/64); the other sizes fall back to Smagorinsky.
 
     python -m pyspectral_b200.ensemble [--steps 500] [--per-size 32]
+
+Across GPUs the runs are independent units (the reference's only
+decomposition, the slab split of one run with an all-to-all per transform,
+src_MPI/Classes.py:244-258, has no counterpart here: every run fits one GPU).
+``shard_specs`` bin-packs the runs by cost N^3 log N onto the ranks (longest
+first, each to the least-loaded rank), every rank advances its share as its
+own ensemble (one process per GPU, its own batches and CUDA graph), and
+``gather_stats`` collects the per-run statistics (energy, enstrophy, FP64
+reductions on each rank's GPU) on every rank in the original run order with
+one all-gather of a few hundred bytes per run -- the only exchange:
+
+    torchrun --nproc-per-node N -m pyspectral_b200.ensemble --steps 500
 """
 from __future__ import annotations
 
@@ -220,6 +232,96 @@ def time_sequential(specs, steps, dt=2e-3, model=None, learned_N=64, device=0):
     return {"steps": steps, "ms": total_ms, "value": pts * steps / (total_ms / 1e3)}
 
 
+def run_cost(spec):
+    """Relative cost of one run's step: N^3 log N (the transforms dominate)."""
+    n = spec["N"]
+    return float(n) ** 3 * math.log(n)
+
+
+def shard_specs(specs, world):
+    """Indices of the runs each of `world` ranks advances: longest-processing-
+    time-first bin packing on run_cost (every run assigned exactly once; the
+    heaviest rank carries at most 4/3 of the optimum)."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(specs)), key=lambda i: (-run_cost(specs[i]), i))
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        shards[r].append(i)
+        load[r] += run_cost(specs[i])
+    return [sorted(sh) for sh in shards]
+
+
+def gather_stats(local, group=None):
+    """All ranks' per-run records {run index: stats} merged into one list in
+    run order (one all-gather of the small host dicts; works over NCCL and
+    gloo).  Every run index must appear exactly once across the ranks."""
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized():
+        parts = [local]
+    else:
+        parts = [None] * dist.get_world_size(group)
+        dist.all_gather_object(parts, local, group=group)
+    merged = {}
+    for part in parts:
+        for i, rec in part.items():
+            if i in merged:
+                raise RuntimeError(f"run {i} reported by two ranks")
+            merged[i] = rec
+    return [merged[i] for i in sorted(merged)]
+
+
+def run_stats(ens):
+    """Per-run energy and enstrophy of an ensemble's current states (FP64
+    reductions on the device), keyed by the run's index in the ensemble's
+    spec list."""
+    out = {}
+    idx = {id(s): i for i, s in enumerate(ens.specs)}
+    for g in ens.groups:
+        ctx = g["ctx"]
+        for s, st in zip(g["runs"], g["states"]):
+            out[idx[id(s)]] = {"N": s["N"], "seed": s["seed"], "energy": ctx.energy(st),
+                               "enstrophy": ctx.enstrophy(st), "closure": g["closure"]}
+    return out
+
+
+def run_sharded(specs, steps, graph_steps=10, model=None, tune=True, log=print):
+    """This rank's share of the ensemble (torchrun / RANK, WORLD_SIZE,
+    LOCAL_RANK): advance it in one CUDA graph per graph_steps, time it on the
+    device, gather per-run stats and the max-over-ranks time.  Returns the
+    whole-job record on every rank."""
+    import datetime
+    import os
+    import torch.distributed as dist
+    rank, world = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    if world > 1 and not dist.is_initialized():
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    shards = shard_specs(specs, world)
+    mine = [specs[i] for i in shards[rank]]
+    ens = Ensemble(mine, model=model, tune=tune, device=local)
+    res = time_batched(ens, steps, graph_steps)
+    stats_local = {shards[rank][j]: rec for j, rec in run_stats(ens).items()}
+    ms = res["ms"]
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    stats = gather_stats(stats_local)
+    pts = sum(s["N"] ** 3 for s in specs)
+    out = {"runs": len(specs), "ranks": world, "steps": res["steps"], "ms_max_over_ranks": ms,
+           "value": pts * res["steps"] / (ms / 1e3), "shards": [len(sh) for sh in shards],
+           "loads": [sum(run_cost(specs[i]) for i in sh) for sh in shards], "stats": stats}
+    if world > 1:
+        ens.graph = None
+        dist.barrier()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--steps", type=int, default=500)
@@ -228,9 +330,20 @@ def main():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--out", default=None)
     a = ap.parse_args()
+    import os
     from .learned import MLPModel
-    model = MLPModel.load()
+    model = MLPModel.load(device=int(os.environ.get("LOCAL_RANK", 0)))
     specs = ensemble_specs(per_size=a.per_size)
+    if int(os.environ.get("WORLD_SIZE", 1)) > 1:
+        import torch.distributed as dist
+        res = run_sharded(specs, a.steps, model=model, tune=not a.no_tune)
+        if int(os.environ.get("RANK", 0)) == 0:
+            print(json.dumps(res))
+            if a.out:
+                with open(a.out, "w") as fh:
+                    json.dump(res, fh)
+        dist.destroy_process_group()
+        return
     t0 = time.time()
     ens = Ensemble(specs, model=model, tune=not a.no_tune)
     setup_s = time.time() - t0

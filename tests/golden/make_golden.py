@@ -1,9 +1,10 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-Run in a container that has the PySpectral sources (default
-``/root/reference``; override with ``PYSPECTRAL_REF``):
+Run in a container that has the PySpectral sources, naming their checkout
+(the directory that holds ``PySpectral/``) by argument or by the
+``PYSPECTRAL_REF`` variable; there is no default:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py /path/to/PySpectral-checkout
 
 The reference is Python 2 code that imports pyFFTW, mpi4py and scipy.weave.
 This script executes its unmodified sources under a load-time shim:
@@ -62,9 +63,18 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
 from oracle import spectral_oracle as orc  # noqa: E402  (inputs only)
 
-REF = os.environ.get("PYSPECTRAL_REF", "/root/reference")
-SRC = os.path.join(REF, "PySpectral", "src")
-SRC_MPI = os.path.join(REF, "PySpectral", "src_MPI")
+REF = SRC = SRC_MPI = None
+
+
+def set_reference(path):
+    """Point the shim at the reference checkout (the directory holding PySpectral/)."""
+    global REF, SRC, SRC_MPI
+    if not path or not os.path.isdir(os.path.join(path, "PySpectral", "src")):
+        raise SystemExit("make_golden.py: give the reference checkout (the directory holding PySpectral/) "
+                         "as the first argument or in PYSPECTRAL_REF")
+    REF = path
+    SRC = os.path.join(REF, "PySpectral", "src")
+    SRC_MPI = os.path.join(REF, "PySpectral", "src_MPI")
 
 
 # ---------------------------------------------------------------- shim ----
@@ -515,4 +525,5 @@ def main():
 
 
 if __name__ == "__main__":
+    set_reference(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYSPECTRAL_REF"))
     main()

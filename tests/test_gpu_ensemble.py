@@ -131,3 +131,29 @@ def test_autotuned_single_run_matches_default_shapes(closure, precision, tol):
         out.append((np_(rhs), np_(main.Q)))
     assert rel(out[1][0], out[0][0]) < tol
     assert rel(out[1][1], out[0][1]) < tol
+
+
+def test_set_run_between_steps_on_a_side_stream():
+    """Changing a run's parameters between two queued steps on a non-blocking
+    stream: the first step runs entirely with the old arguments, the second
+    with the new ones (the library drains the stream before it rewrites the
+    device argument blocks)."""
+    torch = _torch()
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.ensemble import Batch
+    from pyspectral_b200.initial_conditions import isotropic_state
+    N, nu = 16, 2e-3
+    ctx = _capi.Context(N, N, N, precision=64)
+    st0 = isotropic_state(N, 21, k0=3.0).contiguous()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        b = Batch(ctx, _capi.SMAG, 1)
+        st = st0.clone()
+        b.set_run(0, st, None, _capi.make_params(nu=nu, dt=2e-3))
+        b.step(3)
+        b.set_run(0, st, None, _capi.make_params(nu=nu, dt=5e-3))
+        b.step(2)
+    torch.cuda.synchronize()
+    ref = _single(torch, N, np_(st0), nu, 2e-3, "smag", 64, steps=3)
+    ref = _single(torch, N, ref, nu, 5e-3, "smag", 64, steps=2)
+    assert rel(np_(st), ref) < 1e-12
