@@ -53,6 +53,16 @@ extern "C" {
                              dw0_i/dt = -2/d w0_i + (-1)^(i+1) 2 PLQLu + S_i, d = dt0/nsub,
                              S_i the running sum of :1010-1014; w0 (3 p.fm_nsub fields)
                              receives the memory variables as read                          */
+#define PSB_FM2 15        /* turb_model 4      -> computeRHS_FM2    (src/RHSfunctions.py:1025-1286):
+                             3 + 6 p.fm_nsub fields u, then per subintegration i the
+                             pairs w0^i (fields 3+6i..) and w1^i (fields 6+6i..), the
+                             interleaved layout of src/Classes.py:330-355 with equal
+                             dt0/dt1 subintegrations; du/dt = unpad_2x(PLu) + sum_i w0^i,
+                             dw0^i/dt = -2/d0 w0^i + (-1)^(i+1) 2 PLQLu + S0_i + w1^i,
+                             dw1^i/dt = -2/d1 w1^i + (-1)^(i+1) 2 PLQLQLu + S1_i
+                             (d0 = fm_dt0/nsub, d1 = fm_dt1/nsub); PL x PL_q products on
+                             the 3N grid; w0 (6 p.fm_nsub fields, w0^i then w1^i per i)
+                             receives the memory variables as read; no rotating form      */
 #define PSB_ORTHO 12      /* 'Orthogonal Dynamics' -> computeRHS_Orthogonal (src/RHSfunctions.py:53-143):
                              the DNS RHS of u minus the DNS RHS of Gf u (each with its
                              pressure and Coriolis terms)                                     */
@@ -104,7 +114,9 @@ typedef struct {
   int mlp_act;            /* PSB_LEARNED: hidden activation of the model, PSB_ACT_GELU or PSB_ACT_RELU */
   int mlp_hidden;         /* PSB_LEARNED: hidden width of the model, 32 or 64 (0 = 64) */
   double fm_dt0;          /* PSB_FM1: memory length dt0 (src/Classes.py:236-241; default 0.1) */
-  int fm_nsub;            /* PSB_FM1: dt0_subintegrations, 1..8 (0 = 1) (src/Classes.py:243-248) */
+  int fm_nsub;            /* PSB_FM1: dt0_subintegrations, 1..8 (0 = 1) (src/Classes.py:243-248);
+                             PSB_FM2: dt0_ and dt1_subintegrations (equal), 1..8 */
+  double fm_dt1;          /* PSB_FM2: second memory length dt1 (src/Classes.py:302-308; default 0.05) */
 } psb_params;
 
 /* Hidden activation of the learned closure's MLP (a property of the trained model). */
@@ -126,6 +138,7 @@ const char* psb_create_error(void);
 /* One right-hand-side evaluation: main.computeRHS(main,grid,myFFT,utilities)
  * (src/Classes.py:44,95,124,186,227; src_MPI/Classes.py:147).
  * state (read) and rhs (written) hold 3 fields (6 for PSB_MHD, PSB_MHD_TMODEL, PSB_CM1;
+ * 3 + 6 p.fm_nsub for PSB_FM2;
  * 3 + 3 p.fm_nsub for PSB_FM1).
  * w0       : optional closure force main.w0_u/v/w (3 fields; 6 fields u then B for
  *            PSB_MHD_TMODEL) or NULL.

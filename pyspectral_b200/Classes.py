@@ -140,7 +140,9 @@ class variables:
     turb_model: 0 (DNS), 1 (Smagorinsky), 2 (t-model), 'Static tau-model',
     'Dynamic tau-model', 'Orthogonal Dynamics', 3 (first-order finite memory model, state
     ``Q = (u, v, w)`` then ``(w0_u, w0_v, w0_w)`` per subintegration; dt0 and
-    dt0_subintegrations as in the reference), 5 (its two-term form, state
+    dt0_subintegrations as in the reference), 4 (second-order finite memory
+    model, state ``Q = (u, v, w)`` then per subintegration ``w0`` and ``w1``;
+    dt0, dt1 and equal dt0/dt1_subintegrations), 5 (its two-term form, state
     ``(u, w0, w01)``), 6 (first-order complete memory model, state
     ``Q = (u, v, w, w0_u, w0_v, w0_w)``), 7 (dynamic Smagorinsky), 99 (DNS
     with SGS budgets: ``utilitiesClass``'s hooks write ``budget<it>.npz``
@@ -180,6 +182,21 @@ class variables:
             self.fm_nsub = 1 if dt0_subintegrations == -10 else int(dt0_subintegrations)
             self.Q = torch.cat([self.Q] + [torch.zeros_like(self.Q)] * self.fm_nsub).contiguous()
             self.nvars = 3 + 3 * self.fm_nsub
+        self.fm_dt1 = 0.0
+        if turb_model == 4:
+            # second-order finite memory model (src/Classes.py:294-401): dt0 (default
+            # 0.1), dt1 (default 0.05); per subintegration the pair w0, w1
+            # interleaved after u, initially zero.  The reference's layout needs
+            # equal dt0 and dt1 subintegration counts (unequal ones overlap).
+            self.fm_dt0 = 0.1 if dt0 == -10 else float(dt0)
+            self.fm_dt1 = 0.05 if dt1 == -10 else float(dt1)
+            n0 = 1 if dt0_subintegrations == -10 else int(dt0_subintegrations)
+            n1 = 1 if dt1_subintegrations == -10 else int(dt1_subintegrations)
+            if n0 != n1:
+                raise ValueError("turb_model 4: dt0_subintegrations and dt1_subintegrations must be equal")
+            self.fm_nsub = n0
+            self.Q = torch.cat([self.Q] + [torch.zeros_like(self.Q)] * (2 * self.fm_nsub)).contiguous()
+            self.nvars = 3 + 6 * self.fm_nsub
         if turb_model == 5:
             # two-term finite memory model (src/Classes.py:408-454): state (u, w0, w01);
             # it is the finite memory model with two subintegrations of 2 dt0
@@ -196,6 +213,7 @@ class variables:
         self.comp = torch.zeros_like(self.Q) if use_kahan else None
         self.W0 = None
         table = {0: R.computeRHS_NOSGS, 1: R.computeRHS_SMAG, 2: R.computeRHS_tmodel, 3: R.computeRHS_FM1,
+                 4: R.computeRHS_FM2,
                  "Orthogonal Dynamics": R.computeRHS_Orthogonal,
                  5: R.computeRHS_FM1_2term,
                  "Static tau-model": R.computeRHS_staumodel, "Dynamic tau-model": R.computeRHS_Dtaumodel,
@@ -211,7 +229,7 @@ class variables:
             from .learned import MLPModel
             self.model = MLPModel.load(device=grid.device)
         if turb_model not in (0, "learned", "Orthogonal Dynamics"):
-            self.W0 = torch.zeros_like(self.Q[3:] if turb_model in (3, 5) else self.U)
+            self.W0 = torch.zeros_like(self.Q[3:] if turb_model in (3, 4, 5) else self.U)
         if turb_model == "Dynamic tau-model":
             self.kf = int(grid.kc * 2.0 / 3.0)
         if turb_model == "Static tau-model":
@@ -240,7 +258,26 @@ class variables:
             return self.W0[c]
         if self.turb_model == 3:  # FM1: one memory variable per subintegration, (N1, N2, N3/2+1, nsub)
             return self.W0[c::3].permute(1, 2, 3, 0)
+        if self.turb_model == 4:  # FM2: w0 of subintegration i is field 6i + c of W0
+            return self.W0[c::6].permute(1, 2, 3, 0)
         return self.W0[c].unsqueeze(-1)
+
+    def _w1(self, c):
+        if self.turb_model != 4:
+            return None
+        return self.W0[3 + c::6].permute(1, 2, 3, 0)  # FM2: w1 of subintegration i is field 6i + 3 + c
+
+    @property
+    def w1_u(self):
+        return self._w1(0)
+
+    @property
+    def w1_v(self):
+        return self._w1(1)
+
+    @property
+    def w1_w(self):
+        return self._w1(2)
 
     @property
     def w0_u(self):
@@ -269,12 +306,12 @@ class variables:
 
     def U2Q(self):
         self.Q[:3].copy_(self.U)
-        if self.turb_model in (3, 5, 6):  # memory models: w0 is state (src/Classes.py:253-259,432-440,476-482)
+        if self.turb_model in (3, 4, 5, 6):  # memory models: w0 is state (src/Classes.py:253-259,342-355,432-440,476-482)
             self.Q[3:].copy_(self.W0)
 
     def Q2U(self):
         self.U.copy_(self.Q[:3])
-        if self.turb_model in (3, 5):
+        if self.turb_model in (3, 4, 5):
             self.W0.copy_(self.Q[3:])
         elif self.turb_model == 6:  # w0_v read from a slice nothing writes (src/Classes.py:489)
             self.W0.copy_(self.Q[3:6])
@@ -289,12 +326,12 @@ class variables:
                                  mlp_norm=m.norm.data_ptr() if m is not None else None,
                                  les_delta=self.les_delta, mlp_act=m.act if m is not None else 0,
                                  mlp_hidden=m.hidden if m is not None else 0, fm_dt0=self.fm_dt0,
-                                 fm_nsub=self.fm_nsub)
+                                 fm_nsub=self.fm_nsub, fm_dt1=self.fm_dt1)
 
     def closure_code(self):
         return {0: _capi.DNS, 1: _capi.SMAG, 2: _capi.TMODEL, "Static tau-model": _capi.TAU_STATIC,
-                "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 5: _capi.FM1, 6: _capi.CM1, 7: _capi.DSMAG,
-                "Orthogonal Dynamics": _capi.ORTHO,
+                "Dynamic tau-model": _capi.TAU_DYNAMIC, 3: _capi.FM1, 4: _capi.FM2, 5: _capi.FM1, 6: _capi.CM1,
+                7: _capi.DSMAG, "Orthogonal Dynamics": _capi.ORTHO,
                 99: _capi.BUDGETS,
                 "learned": _capi.LEARNED}[self.turb_model]
 

@@ -55,6 +55,18 @@ def computeRHS_FM1(main, grid, myFFT=None, utilities=None):
     _rhs(main, grid, _capi.FM1)
 
 
+def computeRHS_FM2(main, grid, myFFT=None, utilities=None):
+    """Second-order finite memory model (turb_model 4), src/RHSfunctions.py:1025-1286:
+    ``main.Q`` holds u and, per subintegration, the memory variables w0 and w1
+    (interleaved, src/Classes.py:330-355) and becomes their right-hand sides;
+    ``main.w0_*`` and ``main.w1_*`` view the memory variables as read,
+    ``(N1, N2, N3/2+1, subintegrations)``.  No rotating form (the reference's
+    raises)."""
+    if main.rotate:
+        raise RuntimeError("computeRHS_FM2: the reference has no rotating form")
+    _rhs(main, grid, _capi.FM2)
+
+
 def computeRHS_Orthogonal(main, grid, myFFT=None, utilities=None):
     """Orthogonal dynamics ('Orthogonal Dynamics'), src/RHSfunctions.py:53-143:
     the DNS right-hand side of u minus that of ``Gf u``."""

@@ -18,6 +18,7 @@ PSB_ERR_NONFINITE = 6
 DNS, SMAG, TMODEL, TAU_STATIC, TAU_DYNAMIC, MHD, LEARNED, MHD_TMODEL, DSMAG, CM1, BUDGETS, FM1, ORTHO = (
     0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12)
 MPI_DNS, MPI_ORTHO = 13, 14
+FM2 = 15
 ACT_GELU, ACT_RELU = 0, 1  # hidden activation of the learned closure's MLP
 NORM_SERIAL, NORM_MPI, FILTER_GF, TRANSFER_2D = 0, 1, 2, 4
 
@@ -48,7 +49,7 @@ class Params(ctypes.Structure):
                 ("Om1", ctypes.c_double), ("Om2", ctypes.c_double), ("Om3", ctypes.c_double),
                 ("force", ctypes.c_void_p), ("mlp_params", ctypes.c_void_p), ("mlp_norm", ctypes.c_void_p),
                 ("les_delta", ctypes.c_double), ("mlp_act", ctypes.c_int), ("mlp_hidden", ctypes.c_int),
-                ("fm_dt0", ctypes.c_double), ("fm_nsub", ctypes.c_int)]
+                ("fm_dt0", ctypes.c_double), ("fm_nsub", ctypes.c_int), ("fm_dt1", ctypes.c_double)]
 
 
 _lib = None
@@ -106,10 +107,22 @@ def load(path: str = LIB_PATH):
 
 def make_params(nu=0.0, eta=-1.0, t=0.0, dt=0.0, Ct=0.1, tau_a=0.0, tau_b=0.0, kf=0, rotate=0,
                 Om=(0.0, 0.0, 0.0), force=None, mlp_params=None, mlp_norm=None, les_delta=0.0,
-                mlp_act=0, mlp_hidden=0, fm_dt0=0.0, fm_nsub=0) -> Params:
+                mlp_act=0, mlp_hidden=0, fm_dt0=0.0, fm_nsub=0, fm_dt1=0.0) -> Params:
     return Params(float(nu), float(eta), float(t), float(dt), float(Ct), float(tau_a), float(tau_b), int(kf),
                   int(rotate), float(Om[0]), float(Om[1]), float(Om[2]), force, mlp_params, mlp_norm,
-                  float(les_delta), int(mlp_act), int(mlp_hidden), float(fm_dt0), int(fm_nsub))
+                  float(les_delta), int(mlp_act), int(mlp_hidden), float(fm_dt0), int(fm_nsub), float(fm_dt1))
+
+
+def state_fields(closure, params):
+    """Fields of the state (and RHS) of `closure`: 3 velocity components plus
+    the closure's memory variables or magnetic field."""
+    if closure in (MHD, MHD_TMODEL, CM1):
+        return 6
+    if closure == FM1:
+        return 3 + 3 * max(1, params.fm_nsub)
+    if closure == FM2:
+        return 3 + 6 * max(1, params.fm_nsub)
+    return 3
 
 
 class Context:
@@ -169,7 +182,7 @@ class Context:
         return nfields * self.N1 * self.N2 * (self.N3 // 2 + 1)
 
     def rhs(self, closure, state, rhs, params, w0=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else (3 + 3 * max(1, params.fm_nsub) if closure == FM1 else 3)
+        nf = state_fields(closure, params)
         self.bind_stream()
         tau = ctypes.c_double(0.0)
         st = self.lib.psb_rhs(self.h, closure, self._ptr(state, self.spec_numel(nf)),
@@ -186,7 +199,7 @@ class Context:
         self.check(st, "psb_step_si")
 
     def step(self, closure, state, params, nsteps=1, comp=None, read_out=None):
-        nf = 6 if closure in (MHD, MHD_TMODEL, CM1) else (3 + 3 * max(1, params.fm_nsub) if closure == FM1 else 3)
+        nf = state_fields(closure, params)
         self.bind_stream()
         st = self.lib.psb_step_rk4(self.h, closure, self._ptr(state, self.spec_numel(nf)), self._ptr(comp),
                                    self._ptr(read_out), ctypes.byref(params), int(nsteps))

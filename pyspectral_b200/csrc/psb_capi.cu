@@ -650,10 +650,11 @@ int psb_ctx_create(const psb_grid* g, int precision, int device, psb_ctx** out) 
   c->dz = g->dz;
   c->kc = g->kc;
   c->Delta = std::pow(g->dx * g->dy * g->dz, 1.0 / 3.0);
-  // plans + twiddles for N, 3N/2, 2N of each axis
+  // plans + twiddles for N, 3N/2, 2N and 3N of each axis (3N: the second-order
+  // finite memory model's products on the 3/2-padded 2x grid)
   std::vector<int> Ls;
   for (int n : Ns)
-    for (int L : {n, 3 * n / 2, 2 * n})
+    for (int L : {n, 3 * n / 2, 2 * n, 3 * n})
       if (std::find(Ls.begin(), Ls.end(), L) == Ls.end()) Ls.push_back(L);
   std::vector<Cx<double>> twd;
   std::vector<Cx<float>> twf;
@@ -750,6 +751,7 @@ const char* psb_last_error(const psb_ctx* c) { return c ? c->err.c_str() : "null
 
 static int closure_fields(int closure, const psb_params* p) {
   if (closure == PSB_FM1) return 3 + 3 * (p && p->fm_nsub > 0 ? p->fm_nsub : 1);
+  if (closure == PSB_FM2) return 3 + 6 * (p && p->fm_nsub > 0 ? p->fm_nsub : 1);
   return closure == PSB_MHD || closure == PSB_MHD_TMODEL || closure == PSB_CM1 ? 6 : 3;
 }
 

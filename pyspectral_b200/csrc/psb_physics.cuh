@@ -323,7 +323,7 @@ struct EpiPL {
   // npts = 2x-grid points: q part written everywhere, resolved state read / PL_p written on the N grid
   __host__ double io_bytes(long long npts) const {
     const double e = (double)sizeof(Cx<T>);
-    return e * 3 * npts + e * 3 * fstride_n * (PLp ? 2.0 : 1.0);
+    return e * 3 * npts * (PLfull ? 2.0 : 1.0) + e * 3 * fstride_n * (PLp ? 2.0 : 1.0);
   }
   const Cx<T>* Q;  // N-grid state (3 fields)
   long long fstride_n;
@@ -340,6 +340,7 @@ struct EpiPL {
   Cx<T>* PLp;          // (3, N1, N2, n3h) unpad_2x(PL), may be null
   Cx<T>* Lbox;         // (3, 2kfb-1, 2kfb-1, kfb) Leonard pieces, or null
   int kfb;             // box half-size (test-filter kf)
+  Cx<T>* PLfull;       // (3, 2N1, 2N2, N3+1) PL on the whole 2x grid, or null
   __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
     const int n1 = unpad2x_idx(i1, N1), n2 = unpad2x_idx(i2, N2);
     const int n3 = i3 < N3 / 2 ? i3 : -1;
@@ -381,6 +382,11 @@ struct EpiPL {
     PLq[s2] = inp ? z : pu;
     PLq[fstride_2x + s2] = inp ? z : pv;
     PLq[2 * fstride_2x + s2] = inp ? z : pw;
+    if (PLfull) {
+      PLfull[s2] = pu;
+      PLfull[fstride_2x + s2] = pv;
+      PLfull[2 * fstride_2x + s2] = pw;
+    }
     if (PLp && n1 >= 0 && n2 >= 0 && n3 >= 0) {
       const long long s = ((long long)n1 * N2 + n2) * n3h + n3;
       PLp[s] = pu;
@@ -477,6 +483,54 @@ struct EpiPLQL {
     io.finish(s, 0, ru);
     io.finish(s, 1, rv);
     io.finish(s, 2, rw);
+  }
+};
+
+// PLQL on the whole 2x grid (the second-order finite memory model needs its
+// q part there): the formula of EpiPLQL with the 2x-grid wavenumbers
+// (PySpectral/src/RHSfunctions.py:1131-1147), then
+//   PLQLq  = seperateModes(PLQL)[1] on the 2x grid (inverse-transformed next),
+//   PLQLn  = unpad_2x(PLQL) and PLQLqn = unpad_2x(PLQLq) on the N grid
+// (the k3 = N3/2 plane of the N-grid outputs is not written: unpad_2x leaves it zero).
+template <typename T>
+struct EpiPLQLFull {
+  static constexpr int F_IN = 9;
+  __host__ double io_bytes(long long npts) const {
+    return (double)sizeof(Cx<T>) * (3.0 * npts + 6.0 * fstride_n);
+  }
+  KTabs<T> kf;  // 2x-grid wavenumbers
+  int N1, N2, N3, n3h;
+  int nf2, nf3h;
+  long long fstride_2x, fstride_n;
+  Cx<T>* PLQLq;
+  Cx<T>* PLQLn;
+  Cx<T>* PLQLqn;
+  __device__ void operator()(int i1, int i2, int i3, const Cx<T>* P) const {
+    const T k1 = (T)kf.k1[i1], k2 = (T)kf.k2[i2], k3 = (T)kf.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    const Cx<T> upu = P[0], upv = P[1], upw = P[2], vpu = P[3], vpv = P[4], vpw = P[5], wpu = P[6],
+                wpv = P[7], wpw = P[8];
+    const Cx<T> pt = ((T)2 * ksqi) * ((k1 * k1) * upu + (k2 * k2) * vpv + (k3 * k3) * wpw +
+                                      (k1 * k2) * (upv + vpu) + (k1 * k3) * (upw + wpu) + (k2 * k3) * (vpw + wpv));
+    const Cx<T> L[3] = {
+        mik(k1, upu) + mik(k2, vpu) + mik(k3, wpu) + mik(k1, upu) + mik(k2, upv) + mik(k3, upw) + pik(k1, pt),
+        mik(k1, upv) + mik(k2, vpv) + mik(k3, wpv) + mik(k1, vpu) + mik(k2, vpv) + mik(k3, vpw) + pik(k2, pt),
+        mik(k1, upw) + mik(k2, vpw) + mik(k3, wpw) + mik(k1, wpu) + mik(k2, wpv) + mik(k3, wpw) + pik(k3, pt)};
+    const bool inp = in_p_axis(i1, N1) && in_p_axis(i2, N2) && i3 < N3 / 2;
+    const long long s2 = ((long long)i1 * nf2 + i2) * nf3h + i3;
+    const Cx<T> z = mk<T>(0, 0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) PLQLq[c * fstride_2x + s2] = inp ? z : L[c];
+    const int n1 = unpad2x_idx(i1, N1), n2 = unpad2x_idx(i2, N2);
+    if (n1 >= 0 && n2 >= 0 && i3 < N3 / 2) {
+      const long long s = ((long long)n1 * N2 + n2) * n3h + i3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        PLQLn[c * fstride_n + s] = L[c];
+        PLQLqn[c * fstride_n + s] = inp ? z : L[c];
+      }
+    }
   }
 };
 

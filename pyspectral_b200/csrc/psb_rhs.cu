@@ -334,7 +334,7 @@ struct MemCfg {
 // Stage A: u -> PL on the full 2x grid (q part and unpad_2x part).
 template <typename T>
 int run_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const MemCfg& m, Cx<T>** B2_out,
-           Cx<T>** PLq_out, Cx<T>* PLp, Cx<T>* Lbox) {
+           Cx<T>** PLq_out, Cx<T>* PLp, Cx<T>* Lbox, Cx<T>* PLfull = nullptr) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int F1 = 2 * N1, F2 = 2 * N2, F3 = 2 * N3, F3h = N3 + 1, Kz = N3 / 2;
   int st = PSB_OK;
@@ -441,6 +441,7 @@ int run_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const MemCfg& m, C
   epi.PLp = PLp;
   epi.Lbox = Lbox;
   epi.kfb = m.kfb;
+  epi.PLfull = PLfull;
   XEpiArgs<T> e{};
   e.in = D2;
   e.in_fstride = fsC;
@@ -457,15 +458,21 @@ int run_pl(psb_ctx* c, const Cx<T>* Qin, const psb_params* p, const MemCfg& m, C
 }
 
 // Stage B: PLQL from u (B2) and PL_q (E) -> 9 products -> N-grid epilogue.
-template <typename T>
-int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
+// FULL: the products stay on the whole 2x grid (every k3 of the 2x grid, 2N2
+// rows, 2N1 rows) and the epilogue runs there (EpiPLQLFull); otherwise they
+// are truncated to the N grid (unpad_2x) on the way out.  Any epilogue of 9
+// product spectra fits (EpiPLQL, EpiStore<T, 9>, EpiPLQLFull).
+template <typename T, class Epi = EpiPLQL<T>, bool FULL = false>
+int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, Epi epi) {
   const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
   const int F1 = 2 * N1, F2 = 2 * N2, F3 = 2 * N3, F3h = N3 + 1, Kz = N3 / 2;
+  // output k3 count and y rows of the forward passes
+  const int KO = FULL ? F3h : Kz, RY = FULL ? F2 : N2;
   int st = PSB_OK;
   Cx<T>* A3 = scratch<T>(c, "mem.A3", (size_t)3 * F1 * F2 * F3h, &st);
   Cx<T>* B3 = scratch<T>(c, "mem.B3", (size_t)3 * F1 * F2 * F3h, &st);
-  Cx<T>* C3 = scratch<T>(c, "mem.C3", (size_t)9 * F1 * F2 * Kz, &st);
-  Cx<T>* D3 = scratch<T>(c, "mem.D3", (size_t)9 * F1 * N2 * Kz, &st);
+  Cx<T>* C3 = scratch<T>(c, FULL ? "mem.C3f" : "mem.C3", (size_t)9 * F1 * F2 * KO, &st);
+  Cx<T>* D3 = scratch<T>(c, FULL ? "mem.D3f" : "mem.D3", (size_t)9 * F1 * RY * KO, &st);
   if (st != PSB_OK) return st;
   if (!B2) return PSB_OK;
   const long long fsC = (long long)F1 * F2 * F3h;
@@ -509,12 +516,12 @@ int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
     z.in_pstride[3 + f] = F3h;
     z.in_kz[3 + f] = F3h;
   }
-  const long long fsO = (long long)F1 * F2 * Kz;
+  const long long fsO = (long long)F1 * F2 * KO;
   for (int g = 0; g < 9; ++g) {
     z.out[g] = C3 + g * fsO;
-    z.out_pstride[g] = Kz;
+    z.out_pstride[g] = KO;
   }
-  z.out_kz = Kz;
+  z.out_kz = KO;
   z.npencils = (long long)F1 * F2;
   const double s2 = std::sqrt(8.0 * std::sqrt((double)N1 * N2 * N3));
   z.fac = (T)(s2 / ((double)F1 * F2 * F3));
@@ -524,27 +531,27 @@ int run_plql(psb_ctx* c, const MemCfg& m, Cx<T>* B2, Cx<T>* E, EpiPLQL<T> epi) {
   AxisArgs<T> d = axis_common<T>(c, F2);
   d.in = C3;
   d.out = D3;
-  d.in_ostride = (long long)F2 * Kz;
-  d.in_rstride = Kz;
-  d.out_ostride = (long long)N2 * Kz;
-  d.out_rstride = Kz;
+  d.in_ostride = (long long)F2 * KO;
+  d.in_rstride = KO;
+  d.out_ostride = (long long)RY * KO;
+  d.out_rstride = KO;
   d.nouter = 9 * F1;
-  d.ncols = Kz;
+  d.ncols = KO;
   d.in_rows = F2;
-  d.out_rows = N2;
+  d.out_rows = RY;
   d.in_map = map_id(F2);
-  d.out_map = map_pad2x(N2);
+  d.out_map = FULL ? map_id(F2) : map_pad2x(N2);
   PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "PLQL y-forward")));
   XEpiArgs<T> e{};
   e.in = D3;
-  e.in_fstride = (long long)F1 * N2 * Kz;
-  e.in_rstride = (long long)N2 * Kz;
-  e.in_ostride = Kz;
-  e.n1 = N1;
-  e.n2 = N2;
-  e.n3h = N3h;
-  e.kz = Kz;
-  e.out_map = map_pad2x(N1);
+  e.in_fstride = (long long)F1 * RY * KO;
+  e.in_rstride = (long long)RY * KO;
+  e.in_ostride = KO;
+  e.n1 = FULL ? F1 : N1;
+  e.n2 = RY;
+  e.n3h = FULL ? F3h : N3h;
+  e.kz = KO;
+  e.out_map = FULL ? map_id(F1) : map_pad2x(N1);
   e.plan = *plan_for(c, F1);
   e.tw = twiddles<T>(c);
   return launch_epi<T>(c, e, epi, "PLQL x-forward+epilogue");
@@ -1077,6 +1084,258 @@ int fm1_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
 }
 
 // ---------------------------------------------------------------------------
+// Second-order finite memory model (PySpectral/src/RHSfunctions.py:1025-1286,
+// turb_model 4; setup src/Classes.py:294-401).  State: u, then per
+// subintegration i the pairs w0^i (fields 3 + 6i) and w1^i (fields 6 + 6i)
+// (the interleaved layout of src/Classes.py:330-355 with equal numbers of w0
+// and w1 subintegrations).  One RHS =
+//   A  u -> PL on the whole 2x grid (kept), its q part and unpad_2x(PL);
+//   B  u_j (PL_q)_i -> PLQL on the whole 2x grid: its q part (2x grid),
+//      unpad_2x(PLQL) and unpad_2x(PLQL_q) (N grid);
+//   C  PL_a (PL_q)_b on the 3N grid (pad() of the 2x grid), truncated to the
+//      N grid (unpad_2x(unpad(.)), :1168-1186);
+//   D  (PLQL_q)_i u_j on the 2x grid, truncated to the N grid (:1188-1204);
+//   E  one kernel: pterm, pterm2, PLQLQL (:1206-1224) and the memory
+//      equations (:1236-1282), fused with the RK stage update.
+// ---------------------------------------------------------------------------
+
+// Stage C: nine products PL_a (PL_q)_b of two 3-field sets given on the whole
+// 2x grid (3, 2N1, 2N2, N3+1): pad() to the 3N grid (drops the 2x grid's
+// index N of x and y and its k3 = N plane, src/padding.py:16-25), c2r scaled
+// by sqrt(3^3 sqrt(N1 N2 N3)) (:1155), products, r2c, and unpad() then
+// unpad_2x() straight to the N grid: N-grid row i < N/2 comes from 3N-grid row
+// i, row i >= N/2 from row i + 2N; k3 < N3/2.  out9: (9, N1, N2, N3/2+1),
+// product 3a + b = PL_a (PL_q)_b; its k3 = N3/2 plane is written zero.
+template <typename T>
+int run_fm2_3n(psb_ctx* c, const Cx<T>* PL, const Cx<T>* PLq, Cx<T>* out9) {
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const int F1 = 2 * N1, F2 = 2 * N2, F3h = N3 + 1;
+  const int M1 = 3 * N1, M2 = 3 * N2, M3 = 3 * N3, Kz = N3, Ko = N3 / 2;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "fm2.A3n", (size_t)6 * M1 * F2 * Kz, &st);
+  Cx<T>* B = scratch<T>(c, "fm2.B3n", (size_t)6 * M1 * M2 * Kz, &st);
+  Cx<T>* C = scratch<T>(c, "fm2.C3n", (size_t)9 * M1 * M2 * Ko, &st);
+  Cx<T>* D = scratch<T>(c, "fm2.D3n", (size_t)9 * M1 * N2 * Ko, &st);
+  if (st != PSB_OK) return st;
+  if (!PL) return PSB_OK;  // allocation only
+  const long long fsC = (long long)F1 * F2 * F3h, fsA = (long long)M1 * F2 * Kz;
+  const psb::RowMap to3n1 = psb::RowMap{N1, N1 + 1, N1}, to3n2 = psb::RowMap{N2, N2 + 1, N2};
+  for (int set = 0; set < 2; ++set) {
+    AxisArgs<T> a = axis_common<T>(c, M1);
+    a.in = set == 0 ? PL : PLq;
+    a.out = A + set * 3 * fsA;
+    a.in_fstride = fsC;
+    a.in_ostride = F3h;
+    a.in_rstride = (long long)F2 * F3h;
+    a.out_fstride = fsA;
+    a.out_ostride = Kz;
+    a.out_rstride = (long long)F2 * Kz;
+    a.nouter = F2;
+    a.ncols = Kz;
+    a.in_rows = F1;
+    a.out_rows = M1;
+    a.in_map = to3n1;
+    a.out_map = map_id(M1);
+    PSB_TRY((launch_axis<T, true>(c, a, PreCopyN<T, 3>{}, "3n x-inverse")));
+  }
+  AxisArgs<T> b = axis_common<T>(c, M2);
+  b.in = A;
+  b.out = B;
+  b.in_ostride = (long long)F2 * Kz;
+  b.in_rstride = Kz;
+  b.out_ostride = (long long)M2 * Kz;
+  b.out_rstride = Kz;
+  b.nouter = 6 * M1;
+  b.ncols = Kz;
+  b.in_rows = F2;
+  b.out_rows = M2;
+  b.in_map = to3n2;
+  b.out_map = map_id(M2);
+  PSB_TRY((launch_axis<T, true>(c, b, PreCopy<T>{}, "3n y-inverse")));
+  ZArgs<T> z{};
+  const long long fsB = (long long)M1 * M2 * Kz, fsO = (long long)M1 * M2 * Ko;
+  for (int f = 0; f < 6; ++f) {
+    z.in[f] = B + f * fsB;
+    z.in_pstride[f] = Kz;
+    z.in_kz[f] = Kz;
+  }
+  for (int g = 0; g < 9; ++g) {
+    z.out[g] = C + g * fsO;
+    z.out_pstride[g] = Ko;
+  }
+  z.out_kz = Ko;
+  z.npencils = (long long)M1 * M2;
+  const double s3 = std::sqrt(27.0 * std::sqrt((double)N1 * N2 * N3));
+  z.fac = (T)(s3 / ((double)M1 * M2 * M3));
+  z.plan = *plan_for(c, M3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysPLQL<T>{}, "3n z-products"));
+  AxisArgs<T> d = axis_common<T>(c, M2);
+  d.in = C;
+  d.out = D;
+  d.in_ostride = (long long)M2 * Ko;
+  d.in_rstride = Ko;
+  d.out_ostride = (long long)N2 * Ko;
+  d.out_rstride = Ko;
+  d.nouter = 9 * M1;
+  d.ncols = Ko;
+  d.in_rows = M2;
+  d.out_rows = N2;
+  d.in_map = map_id(M2);
+  d.out_map = psb::RowMap{N2 / 2, N2 / 2, 2 * N2};
+  PSB_TRY((launch_axis<T, false>(c, d, PreCopy<T>{}, "3n y-forward")));
+  XEpiArgs<T> e{};
+  e.in = D;
+  e.in_fstride = (long long)M1 * N2 * Ko;
+  e.in_rstride = (long long)N2 * Ko;
+  e.in_ostride = Ko;
+  e.n1 = N1;
+  e.n2 = N2;
+  e.n3h = N3h;
+  e.kz = Ko;
+  e.out_map = psb::RowMap{N1 / 2, N1 / 2, 2 * N1};
+  e.plan = *plan_for(c, M1);
+  e.tw = twiddles<T>(c);
+  return launch_epi<T>(c, e, EpiStore<T, 9>{out9, (long long)N1 * N2 * N3h, N2, N3h}, "3n x-forward+store");
+}
+
+// Stage E: PLQLQL and every right-hand side of the state, with the RK stage
+// update.  P3[3a + b] = PL_a (PL_q)_b, P2[3j + i] = (PLQL_q)_i u_j (N grid).
+template <typename T>
+__global__ void __launch_bounds__(256) fm2_combine_kernel(StepIO<T> io, KTabs<T> k, const Cx<T>* __restrict__ PLp,
+                                                          const Cx<T>* __restrict__ PLQL,
+                                                          const Cx<T>* __restrict__ PLQLq,
+                                                          const Cx<T>* __restrict__ P3, const Cx<T>* __restrict__ P2,
+                                                          int nsub, T nu, T m2d0, T p4d0, T m2d1, T p4d1, int N1,
+                                                          int N2, int N3) {
+  const long long fs = io.fstride;
+  const long long npts = (long long)N1 * N2 * io.n3h;
+  for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < npts;
+       s += (long long)gridDim.x * blockDim.x) {
+    const int i3 = (int)(s % io.n3h);
+    const long long t = s / io.n3h;
+    const int i2 = (int)(t % N2), i1 = (int)(t / N2);
+    if (io.read_out) {
+      const bool nyq = i1 == N1 / 2 || i2 == N2 / 2 || i3 == N3 / 2;
+#pragma unroll
+      for (int f = 0; f < 3; ++f) io.read_out[f * fs + s] = nyq ? mk<T>(0, 0) : io.Q[f * fs + s];
+    }
+    const T k1 = (T)k.k1[i1], k2 = (T)k.k2[i2], k3 = (T)k.k3[i3];
+    T ksq, ksqi;
+    ksq_pair(k1, k2, k3, ksq, ksqi);
+    Cx<T> A[9], B[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) {
+      A[m] = P3[m * fs + s];
+      B[m] = P2[m * fs + s];
+    }
+    // names of the reference: A = PLa_PLbq at 3a + b, B = PLQLiq_jp at 3j + i
+    const Cx<T> uu = A[0], uv = A[1], uw = A[2], vu = A[3], vv = A[4], vw = A[5], wu = A[6], wv = A[7], ww = A[8];
+    const Cx<T> qu_u = B[0], qv_u = B[1], qw_u = B[2], qu_v = B[3], qv_v = B[4], qw_v = B[5], qu_w = B[6],
+                qv_w = B[7], qw_w = B[8];
+    const Cx<T> pterm = ksqi * ((k1 * k1) * uu + (k2 * k2) * vv + (k3 * k3) * ww + (k1 * k2) * (vu + uv) +
+                                (k1 * k3) * (uw + wu) + (k2 * k3) * (vw + wv));
+    const Cx<T> pterm2 = ksqi * ((k1 * k1) * qu_u + (k2 * k2) * qv_v + (k3 * k3) * qw_w + (k1 * k2) * (qv_u + qu_v) +
+                                 (k1 * k3) * (qw_u + qu_w) + (k2 * k3) * (qw_v + qv_w));
+    const T two = (T)2;
+    const Cx<T> QQ[3] = {
+        mik(two * k1, uu) + mik(k2, vu) + mik(k3, wu) + mik(k2, uv) + mik(k3, uw) + pik(two * k1, pterm) +
+            pik(two * k1, qu_u) + mik(k2, qv_u) + mik(k3, qw_u) + mik(k2, qu_v) + mik(k3, qu_w) +
+            pik(two * k1, pterm2) - (nu * ksq) * PLQLq[s],
+        mik(k1, uv) + mik(two * k2, vv) + mik(k3, wv) + mik(k1, vu) + mik(k3, vw) + pik(two * k2, pterm) +
+            mik(k1, qu_v) + mik(two * k2, qv_v) + mik(k3, qw_v) + mik(k1, qv_u) + mik(k3, qv_w) +
+            pik(two * k2, pterm2) - (nu * ksq) * PLQLq[fs + s],
+        mik(k1, uw) + mik(k2, vw) + mik(two * k3, ww) + mik(k1, wu) + mik(k2, wv) + pik(two * k3, pterm) +
+            mik(k1, qu_w) + mik(k2, qv_w) + mik(two * k3, qw_w) + mik(k1, qw_u) + mik(k3, qw_v) +
+            pik(two * k3, pterm2) - (nu * ksq) * PLQLq[2 * fs + s]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Cx<T> w0[kFmMaxSub], w1[kFmMaxSub];
+      Cx<T> sum = mk<T>(0, 0);
+      for (int i = 0; i < nsub; ++i) {
+        w0[i] = io.Q[(3 + 6 * i + c) * fs + s];
+        w1[i] = io.Q[(6 + 6 * i + c) * fs + s];
+        sum = sum + w0[i];
+        if (io.w0_out) {  // the memory variables as read (main.w0_*, main.w1_*)
+          io.w0_out[(6 * i + c) * fs + s] = w0[i];
+          io.w0_out[(6 * i + 3 + c) * fs + s] = w1[i];
+        }
+      }
+      io.finish(s, c, PLp[c * fs + s] + sum);
+      const Cx<T> plql = PLQL[c * fs + s];
+      Cx<T> run0 = mk<T>(0, 0), run1 = mk<T>(0, 0);
+      for (int i = 1; i <= nsub; ++i) {
+        for (int j = 1; j < i; ++j) {
+          const bool neg = ((i + j + 1) & 1) != 0;
+          run0 = run0 + (neg ? -p4d0 : p4d0) * w0[j - 1];
+          run1 = run1 + (neg ? -p4d1 : p4d1) * w1[j - 1];
+        }
+        const T sgn2 = ((i + 1) & 1) ? (T)-2 : (T)2;
+        io.finish(s, 3 + 6 * (i - 1) + c, ((m2d0 * w0[i - 1] + sgn2 * plql) + run0) + w1[i - 1]);
+        io.finish(s, 6 + 6 * (i - 1) + c, (m2d1 * w1[i - 1] + sgn2 * QQ[c]) + run1);
+      }
+    }
+  }
+}
+
+template <typename T>
+int fm2_rhs(psb_ctx* c, StepIO<T> io, const psb_params* p) {
+  if (p->rotate) return fail(c, PSB_ERR_UNSUPPORTED, "PSB_FM2: the reference has no rotating form");
+  const int nsub = p->fm_nsub > 0 ? p->fm_nsub : 1;
+  if (nsub > kFmMaxSub) return fail(c, PSB_ERR_ARG, "PSB_FM2: fm_nsub must be 1..8");
+  // the 3N-grid passes hold one 3N-point line per field in shared memory
+  if (3 * std::max(c->N1, std::max(c->N2, c->N3)) > (c->prec == 64 ? 768 : 1536))
+    return fail(c, PSB_ERR_SHAPE, "PSB_FM2: grid too large for the 3N-grid products (N <= 256 FP64, 512 FP32)");
+  const double d0 = (p->fm_dt0 > 0 ? p->fm_dt0 : 0.1) / nsub;
+  const double d1 = (p->fm_dt1 > 0 ? p->fm_dt1 : 0.05) / nsub;
+  const int N1 = c->N1, N2 = c->N2, N3 = c->N3, N3h = c->N3h;
+  const long long fs = (long long)N1 * N2 * N3h;
+  const long long fs2 = (long long)2 * N1 * 2 * N2 * (N3 + 1);
+  int st = PSB_OK;
+  Cx<T>* PLp = scratch<T>(c, "mem.PLp", (size_t)3 * fs, &st);
+  Cx<T>* PLfull = scratch<T>(c, "fm2.PL", (size_t)3 * fs2, &st);
+  Cx<T>* PLQLq2 = scratch<T>(c, "fm2.PLQLq2", (size_t)3 * fs2, &st);
+  Cx<T>* N6 = scratch<T>(c, "fm2.PLQLn", (size_t)6 * fs, &st);  // unpad_2x(PLQL), unpad_2x(PLQL_q)
+  Cx<T>* P3 = scratch<T>(c, "fm2.P3", (size_t)9 * fs, &st);
+  Cx<T>* P2 = scratch<T>(c, "fm2.P2", (size_t)9 * fs, &st);
+  if (st != PSB_OK) return st;
+  const Cx<T>* Qin = io.Q;
+  MemCfg m{"memu", nullptr, 0, true, false, 0};
+  if (Qin) {
+    PSB_TRY(cuda_ok(c, cudaMemsetAsync(PLp, 0, sizeof(Cx<T>) * 3 * fs, c->stream), "memset"));
+    PSB_TRY(cuda_ok(c, cudaMemsetAsync(N6, 0, sizeof(Cx<T>) * 6 * fs, c->stream), "memset"));
+  }
+  Cx<T>*B2 = nullptr, *E = nullptr;
+  PSB_TRY(run_pl<T>(c, Qin, p, m, &B2, &E, PLp, nullptr, PLfull));
+  EpiPLQLFull<T> ef{};
+  ef.kf = ktabs<T>(c->kxf, c->kyf, c->kzf);
+  ef.N1 = N1;
+  ef.N2 = N2;
+  ef.N3 = N3;
+  ef.n3h = N3h;
+  ef.nf2 = 2 * N2;
+  ef.nf3h = N3 + 1;
+  ef.fstride_2x = fs2;
+  ef.fstride_n = fs;
+  ef.PLQLq = PLQLq2;
+  ef.PLQLn = N6;
+  ef.PLQLqn = N6 + 3 * fs;
+  PSB_TRY((run_plql<T, EpiPLQLFull<T>, true>(c, m, Qin ? B2 : nullptr, E, ef)));
+  PSB_TRY(run_fm2_3n<T>(c, Qin ? PLfull : nullptr, E, P3));
+  PSB_TRY((run_plql<T, EpiStore<T, 9>>(c, m, Qin ? B2 : nullptr, PLQLq2, EpiStore<T, 9>{P2, fs, N2, N3h})));
+  if (!Qin) return PSB_OK;  // allocation only
+  const int blocks = (int)std::min<long long>((fs + 255) / 256, 4 * 148);
+  {
+    LaunchScope ls(c, "fm2 combine",
+                   (double)sizeof(Cx<T>) * fs * ((3 + 6 * nsub) * 2 + 3 + 6 + 18 + (io.read_out ? 3 : 0)));
+    fm2_combine_kernel<T><<<blocks, 256, 0, c->stream>>>(io, ktabs<T>(c->kx, c->ky, c->kz), PLp, N6, N6 + 3 * fs,
+                                                         P3, P2, nsub, (T)p->nu, (T)(-2. / d0), (T)(4. / d0),
+                                                         (T)(-2. / d1), (T)(4. / d1), N1, N2, N3);
+  }
+  return launch_ok(c, "fm2 combine");
+}
+
+// ---------------------------------------------------------------------------
 // DNS with SGS budgets (PySpectral/src/RHSfunctions.py:1543-1661, turb_model 99):
 // RHS = unpad_2x(PL u); PLQL u with the q part split at main.kc
 // (seperateModesBudgets, src/padding.py:81-93) is stored for the budget files.
@@ -1595,6 +1854,8 @@ int rhs_dispatch(psb_ctx* c, int closure, StepIO<T> io, const psb_params* p, dou
       return budgets_rhs<T>(c, io, p);
     case PSB_FM1:
       return fm1_rhs<T>(c, io, p);
+    case PSB_FM2:
+      return fm2_rhs<T>(c, io, p);
     case PSB_ORTHO:
       return ortho_rhs<T>(c, io, p, ts);
     case PSB_MPI_DNS:
