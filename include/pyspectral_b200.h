@@ -130,6 +130,16 @@ int psb_ctx_create(const psb_grid* grid, int precision, int device, psb_ctx** ou
 int psb_ctx_destroy(psb_ctx* ctx);
 /* Stream (cudaStream_t) on which the context queues its work; NULL = legacy default. */
 int psb_ctx_set_stream(psb_ctx* ctx, void* stream);
+/* Stage the inputs of the passes that read their rows unchanged (forward y
+ * pass, the x pass of the spectral epilogue, plain inverse y passes) with
+ * bulk tensor copies (1, the default) or with per-element loads (0).  Same
+ * results either way; no counterpart in the reference (a launch choice). */
+int psb_ctx_set_tma(psb_ctx* ctx, int enable);
+/* Device status of the context's kernels since the last call, then cleared:
+ * 0, or 1 when a bounded wait inside a kernel gave up (that kernel wrote NaN
+ * in place of the tile it could not stage instead of hanging).  Synchronises
+ * the context stream.  No counterpart in the reference (it has no device). */
+int psb_device_status(psb_ctx* ctx, int* status);
 /* Message of the last failure on this context ("" if none). */
 const char* psb_last_error(const psb_ctx* ctx);
 /* Message of the last psb_ctx_create failure (no context exists then). */

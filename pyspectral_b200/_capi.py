@@ -32,6 +32,7 @@ EXPORTS = (
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
     "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear", "psb_set_tuned_shape",
+    "psb_ctx_set_tma", "psb_device_status",
 )
 
 
@@ -96,6 +97,8 @@ def load(path: str = LIB_PATH):
         "psb_tuned_shape": ([vp, i, i, ip, ip, i], i),
         "psb_autotune_clear": ([vp, i], i),
         "psb_set_tuned_shape": ([vp, i, i, i, ip, i], i),
+        "psb_ctx_set_tma": ([vp, i], i),
+        "psb_device_status": ([vp, ip], i),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -312,6 +315,18 @@ class Context:
             arr = (ctypes.c_int * max(1, len(rad)))(*rad)
             self.check(self.lib.psb_set_tuned_shape(self.h, closure, p, int(sh["tile"]), arr, len(rad)),
                        "psb_set_tuned_shape")
+
+    def set_tma(self, on: bool):
+        """Stage eligible pass inputs with bulk tensor copies (default) or plain loads."""
+        self.check(self.lib.psb_ctx_set_tma(self.h, 1 if on else 0), "psb_ctx_set_tma")
+
+    def device_status(self):
+        """0, or 1 if a bounded wait inside one of this context's kernels gave up
+        since the last call (cleared on read; synchronises the stream)."""
+        self.bind_stream()
+        st = ctypes.c_int()
+        self.check(self.lib.psb_device_status(self.h, ctypes.byref(st)), "psb_device_status")
+        return st.value
 
     def launch_count(self):
         n = ctypes.c_ulonglong()

@@ -720,6 +720,9 @@ int psb_ctx_create(const psb_grid* g, int precision, int device, psb_ctx** out) 
   ok = ok && upload(mx.data(), mx.size() * 8, (void**)&c->mx) && upload(my.data(), my.size() * 8, (void**)&c->my) &&
        upload(mz.data(), mz.size() * 8, (void**)&c->mz) && upload(gx.data(), gx.size() * 8, (void**)&c->gx) &&
        upload(gy.data(), gy.size() * 8, (void**)&c->gy) && upload(gz.data(), gz.size() * 8, (void**)&c->gz);
+  // device status word: raised by a kernel whose bounded wait gave up
+  const int zero_status = 0;
+  ok = ok && upload(&zero_status, sizeof(int), (void**)&c->dstatus);
   if (!ok) {
     std::string m = std::string("table upload failed: ") + cudaGetErrorString(cudaGetLastError());
     psb_ctx_destroy(c);
@@ -738,6 +741,24 @@ int psb_ctx_destroy(psb_ctx* c) {
   if (c->red_dev) cudaFree(c->red_dev);
   if (c->red_host) cudaFreeHost(c->red_host);
   delete c;
+  return PSB_OK;
+}
+
+int psb_ctx_set_tma(psb_ctx* c, int enable) {
+  PSB_TRY(check_ctx(c));
+  c->use_tma = enable ? 1 : 0;
+  return PSB_OK;
+}
+
+int psb_device_status(psb_ctx* c, int* status) {
+  PSB_TRY(check_ctx(c));
+  if (!status) return fail(c, PSB_ERR_ARG, "psb_device_status: null argument");
+  PSB_TRY(set_device(c));
+  int h = 0;
+  PSB_TRY(cuda_ok(c, cudaMemcpyAsync(&h, c->dstatus, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status read"));
+  PSB_TRY(cuda_ok(c, cudaMemsetAsync(c->dstatus, 0, sizeof(int), c->stream), "status clear"));
+  PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "status sync"));
+  *status = h;
   return PSB_OK;
 }
 

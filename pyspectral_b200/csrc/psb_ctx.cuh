@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <map>
 #include <string>
 #include <vector>
@@ -61,6 +62,8 @@ struct psb_ctx {
   // with its compulsory HBM bytes (inputs read once + outputs written once)
   unsigned long long launches = 0;
   int timing = 0;
+  int use_tma = 1;          // stage eligible pass inputs with bulk tensor copies
+  int* dstatus = nullptr;   // device status word (a bounded wait gave up), owned
   struct Rec {
     std::string name;
     double bytes;
@@ -155,6 +158,13 @@ struct LaunchScope {
     }
   }
 };
+
+// Boxes of rows of a TMA-staged pass: the fewest that divide L with at most 256 rows each.
+inline int tma_boxes(int L) {
+  for (int nb = 1; nb <= 8; ++nb)
+    if (L % nb == 0 && L / nb <= 256) return nb;
+  return 0;
+}
 
 inline int count_mapped(const psb::RowMap& m, int rows) {
   int n = 0;
@@ -282,6 +292,13 @@ inline int pick_ct(int ncols, int F, int L, size_t esz, int nouter = 0) {
   return ct;
 }
 
+// radix 6/12/16 passes need the wide kernel instantiations
+inline bool plan_is_wide_h(const psb::FFTPlan& p) {
+  for (int s = 0; s < p.npass; ++s)
+    if (p.radix[s] > 8 || p.radix[s] == 6) return true;
+  return false;
+}
+
 // sh: an autotuned shape (TUNABLE launch sites only) or null for the default
 template <typename T, bool INV, class Pre, bool TUNABLE = false>
 int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const psb_pass_shape* sh = nullptr) {
@@ -302,6 +319,38 @@ int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const
     launch_pdl(k, grid, 256, smem, c->stream, a, pre);
     return launch_ok(c, what);
   };
+  // Rows read unchanged (a plain copy, every row at its own position): the
+  // tile is staged by bulk tensor copies when the view meets TMA's rules.
+  if constexpr (std::is_same<Pre, psb::PreCopy<T>>::value) {
+    const int nbox = tma_boxes(L);
+    CUtensorMap map;
+    const bool plain_rows = a.in_rows == L && a.in_map.lo >= L;
+    if (c->use_tma && plain_rows && nbox > 0 && (a.col_tile * esz) % 16 == 0 && !(sh && sh->wide)) {
+      const long long dims[4] = {a.ncols, 1, a.in_rows, a.nouter};
+      const long long strides[3] = {a.in_rstride, a.in_rstride, a.in_ostride};
+      const int box[4] = {a.col_tile, 1, L / nbox, 1};
+      if (tma::encode4d(&map, a.in, (int)esz, dims, strides, box)) {
+        const size_t tsmem = psb::tma_buf_offset<T>(L) + (size_t)2 * L * a.col_tile * esz;
+        auto got = [&](auto k) {
+          set_smem(k, tsmem);
+          LaunchScope scope(c, what, bytes);
+          launch_pdl(k, grid, 256, tsmem, c->stream, a, map, nbox, c->dstatus);
+          return launch_ok(c, what);
+        };
+        switch (psb::fixed_plan_id(a.plan)) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value) return got(psb::axis_pass_tma_kernel<T, INV, ID>); \
+    break;
+          PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+          default:
+            break;
+        }
+        if (!plan_is_wide_h(a.plan)) return got(psb::axis_pass_tma_kernel<T, INV, 0>);
+      }
+    }
+  }
   if constexpr (TUNABLE) {
     switch (psb::fixed_plan_id(a.plan)) {
 #define PSB_FIXED_CASE(ID, ...) \
@@ -391,6 +440,37 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
     launch_pdl(k, dim3((unsigned)(e.main_blocks + extra)), 256, smem, c->stream, e, epi);
     return launch_ok(c, what);
   };
+  // the input tile (ct columns x F fields x L rows) staged by bulk tensor copies
+  {
+    const int nbox = tma_boxes(L);
+    CUtensorMap map;
+    if (c->use_tma && nbox > 0 && (e.col_tile * esz) % 16 == 0 && !(sh && sh->wide)) {
+      const long long dims[4] = {e.kz, Epi::F_IN, L, e.n2};
+      const long long strides[3] = {e.in_fstride, e.in_rstride, e.in_ostride};
+      const int box[4] = {e.col_tile, Epi::F_IN, L / nbox, 1};
+      if (tma::encode4d(&map, e.in, (int)esz, dims, strides, box)) {
+        const size_t tsmem = psb::tma_buf_offset<T>(L) + (size_t)2 * L * Epi::F_IN * e.col_tile * esz;
+        auto got = [&](auto k) {
+          set_smem(k, tsmem);
+          LaunchScope scope(c, what, bytes);
+          launch_pdl(k, dim3((unsigned)(e.main_blocks + extra)), 256, tsmem, c->stream, e, epi, map, nbox,
+                     c->dstatus);
+          return launch_ok(c, what);
+        };
+        switch (psb::fixed_plan_id(e.plan)) {
+#define PSB_FIXED_CASE(ID, ...) \
+  case ID:                      \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value) return got(psb::xfwd_epi_tma_kernel<T, Epi, ID>); \
+    break;
+          PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+          default:
+            break;
+        }
+        if (!plan_is_wide_h(e.plan)) return got(psb::xfwd_epi_tma_kernel<T, Epi, 0>);
+      }
+    }
+  }
   if constexpr (TUNABLE) {
     switch (psb::fixed_plan_id(e.plan)) {
 #define PSB_FIXED_CASE(ID, ...) \

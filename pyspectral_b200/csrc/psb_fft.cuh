@@ -313,21 +313,34 @@ __device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* _
 
 
 // ---- transforms with a compile-time length and schedule --------------------
-// The same Stockham passes over `nlines` contiguous lines of length L (the
-// z-pass layout) with L, the radix and the sub-transform length Ns known to
-// the compiler: work items split into (line, j) by a constant divisor, and
-// every shared-memory offset of an item is a constant from its base.
-template <typename T, int R, bool INV, int L, int NS>
+// The Stockham passes with L, the radix and the sub-transform length Ns known
+// to the compiler, over `nlines` lines of length L held at buf[line*ls + j]
+// (the z-pass layout: each line contiguous, consecutive lines `ls` elements
+// apart; the z pass uses ls = L + 1, odd, so that the same position of
+// consecutive lines falls in different shared-memory banks).
+//
+// LINES_FAST (used when nlines >= 8): consecutive threads take consecutive
+// lines at the same j.  A warp's loads j + r*L/R, its stores (j-k)R + k + r*Ns
+// and its twiddle reads (one k per j: a broadcast) then spread over the banks
+// by the odd line stride, where in the j-fast order the stores of one line
+// land R elements apart and hit one bank up to 16 times per half-warp.
+// Otherwise consecutive threads take consecutive j of a line.  Items are
+// walked as a (fast, slow) counter pair, without a division.
+template <typename T, int R, bool INV, int L, int NS, bool LINES_FAST>
 __device__ __forceinline__ void stockham_pass_c(const Cx<T>* __restrict__ a, Cx<T>* __restrict__ b,
-                                                const Cx<T>* __restrict__ tw, int nlines) {
+                                                const Cx<T>* __restrict__ tw, int nlines, int ls) {
   constexpr int NB = L / R;
   constexpr int TS = L / (NS * R);
-  const int items = nlines * NB;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
-    const int line = it / NB;
-    const int j = it - line * NB;
+  const int mf = LINES_FAST ? nlines : NB;
+  const int ms = LINES_FAST ? NB : nlines;
+  const int nt = blockDim.x;
+  int f = threadIdx.x % mf, sl = threadIdx.x / mf;
+  const int df = nt % mf, ds = nt / mf;
+  while (sl < ms) {
+    const int line = LINES_FAST ? f : sl;
+    const int j = LINES_FAST ? sl : f;
     const int k = j % NS;
-    const Cx<T>* src = a + line * L + j;
+    const Cx<T>* src = a + line * ls + j;
     Cx<T> v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = src[r * NB];
@@ -340,21 +353,27 @@ __device__ __forceinline__ void stockham_pass_c(const Cx<T>* __restrict__ a, Cx<
       }
     }
     small_dft<T, R, INV>(v);
-    Cx<T>* dst = b + line * L + (j - k) * R + k;
+    Cx<T>* dst = b + line * ls + (j - k) * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) dst[r * NS] = v[r];
+    f += df;
+    sl += ds;
+    if (f >= mf) {
+      f -= mf;
+      ++sl;
+    }
   }
 }
 // Passes R, Rest... starting at sub-transform length NS; returns the buffer
 // holding the result.  Ends with __syncthreads.
-template <typename T, bool INV, int L, int NS, int R, int... Rest>
-__device__ __forceinline__ Cx<T>* fft_c(Cx<T>* a, Cx<T>* b, const Cx<T>* __restrict__ tw, int nlines) {
-  stockham_pass_c<T, R, INV, L, NS>(a, b, tw, nlines);
+template <typename T, bool INV, int L, int NS, bool LF, int R, int... Rest>
+__device__ __forceinline__ Cx<T>* fft_c(Cx<T>* a, Cx<T>* b, const Cx<T>* __restrict__ tw, int nlines, int ls) {
+  stockham_pass_c<T, R, INV, L, NS, LF>(a, b, tw, nlines, ls);
   __syncthreads();
   if constexpr (sizeof...(Rest) == 0)
     return b;
   else
-    return fft_c<T, INV, L, NS * R, Rest...>(b, a, tw, nlines);
+    return fft_c<T, INV, L, NS * R, LF, Rest...>(b, a, tw, nlines, ls);
 }
 
 // The same for lines adjacent in memory (element j of line f at f + j*es, the
@@ -429,8 +448,10 @@ struct FixedPlan;
   struct FixedPlan<ID> {                                                                        \
     static constexpr int L = LEN;                                                               \
     template <typename T, bool INV>                                                             \
-    static __device__ __forceinline__ Cx<T>* run(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, int n) { \
-      return fft_c<T, INV, LEN, 1, __VA_ARGS__>(a, b, tw, n);                                   \
+    static __device__ __forceinline__ Cx<T>* run(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, int n,    \
+                                                 int ls) {                                      \
+      if (n >= 8) return fft_c<T, INV, LEN, 1, true, __VA_ARGS__>(a, b, tw, n, ls);             \
+      return fft_c<T, INV, LEN, 1, false, __VA_ARGS__>(a, b, tw, n, ls);                        \
     }                                                                                           \
     template <typename T, bool INV>                                                             \
     static __device__ __forceinline__ Cx<T>* run_adjacent(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, \

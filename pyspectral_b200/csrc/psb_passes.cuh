@@ -26,6 +26,7 @@
 // mode).
 #pragma once
 #include "psb_fft.cuh"
+#include "psb_tma.cuh"
 
 namespace psb {
 
@@ -82,10 +83,10 @@ __device__ __forceinline__ void split_line(int r, int P, int lp, int& f, int& p)
 }
 
 // Phys functors with `static constexpr bool BLOCK = true` provide
-// setup(extra_smem) and block(R, W, P, M, fac, p0, npencils, extra_smem) and
-// ask for EXTRA_SMEM bytes behind the z-pass buffers.  R and W hold packed
+// setup(extra_smem) and block(R, W, P, M, LS, fac, p0, npencils, extra_smem)
+// and ask for EXTRA_SMEM bytes behind the z-pass buffers.  R and W hold packed
 // real line r (field f, pencil p: r = f*P + p) at component r&1 of complex
-// line r>>1, position z at buf[(r>>1)*M + z].
+// line r>>1, position z at buf[(r>>1)*LS + z] (LS = zline(M)).
 template <class P, class = void>
 struct phys_is_block {
   static constexpr bool value = false;
@@ -153,6 +154,41 @@ __device__ __forceinline__ Cx<T>* axfft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, co
     return FixedPlan<FP>::template run_adjacent<T, INV>(a, b, tw, lines);
 }
 
+// Transform of a staged tile (F fields x ct columns, position-major in bufA)
+// and the store of its output rows.  Must be called by all threads.
+template <typename T, bool INV, int F, bool WIDE, int FP>
+__device__ __forceinline__ void axis_transform_store(const AxisArgs<T>& a, Cx<T>* bufA, Cx<T>* bufB,
+                                                     const Cx<T>* tw, int o, int c0) {
+  const int ct = a.col_tile;
+  const int lines = F * ct;
+  const Cx<T> zero = mk<T>(0, 0);
+  const int nt = blockDim.x;
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
+  const int col = c0 + c;
+  const bool colok = col < a.ncols;
+  Cx<T>* res = axfft<T, INV, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
+  Cx<T>* outb = a.out + (long long)o * a.out_ostride;
+  if (!colok || threadIdx.x >= dr * ct) return;
+  const int nrow = a.out_rows * F;
+  for (int t = r0; t < nrow; t += dr) {
+    const int i = t / F, g = t - i * F;
+    const int j = a.out_map(i);
+    outb[g * a.out_fstride + i * a.out_rstride + col] = j >= 0 ? a.scale * res[(size_t)j * lines + g * ct + c] : zero;
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T nan_of() {
+  return sizeof(T) == 8 ? (T)__longlong_as_double(0x7ff8000000000000ll) : (T)__int_as_float(0x7fc00000);
+}
+
+// Offset of the transform buffer behind the twiddles in a TMA-staged pass:
+// bulk tensor copies land on 128-byte boundaries.
+template <typename T>
+__host__ __device__ inline size_t tma_buf_offset(int L) {
+  return ((size_t)L * sizeof(Cx<T>) + 127) / 128 * 128;
+}
+
 template <typename T, bool INV, class Pre, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,15 +251,57 @@ __device__ __forceinline__ void axis_pass_body(const AxisArgs<T>& a, const Pre& 
     }
   }
   __syncthreads();
-  Cx<T>* res = axfft<T, INV, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
-  Cx<T>* outb = a.out + (long long)o * a.out_ostride;
-  if (!colok || threadIdx.x >= dr * ct) return;
-  const int nrow = a.out_rows * Pre::F_DST;
-  for (int t = r0; t < nrow; t += dr) {
-    const int i = t / Pre::F_DST, g = t - i * Pre::F_DST;
-    const int j = a.out_map(i);
-    outb[g * a.out_fstride + i * a.out_rstride + col] = j >= 0 ? a.scale * res[(size_t)j * lines + g * ct + c] : zero;
+  axis_transform_store<T, INV, Pre::F_DST, WIDE, FP>(a, bufA, bufB, tw, o, c0);
+}
+
+// TMA-staged axis pass for passes that read their rows unchanged (PreCopy,
+// identity row map, in_rows = L): one bulk tensor copy per box of rows lands
+// the tile [row][col] directly in the transform buffer.  map: a 4-D view
+// (columns, 1, rows, outer index) of a.in; nbox boxes of L/nbox rows.
+// A copy that does not complete within the poll limit raises *status and the
+// CTA writes NaN in place of its tile (after waiting again, bounded, for the
+// copy to land).
+template <typename T, bool INV, int FP = 0>
+__global__ void __launch_bounds__(256) axis_pass_tma_kernel(AxisArgs<T> a, const __grid_constant__ CUtensorMap map,
+                                                            int nbox, int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ int timed_out;
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int L = a.plan.L;
+  const int ct = a.col_tile;
+  Cx<T>* bufA = reinterpret_cast<Cx<T>*>(smem_raw + tma_buf_offset<T>(L));
+  Cx<T>* bufB = bufA + (size_t)L * ct;
+  const int o = blockIdx.y;
+  const int c0 = blockIdx.x * ct;
+  const uint32_t mb = tma::smem_u32(&mbar);
+  pdl_trigger();
+  if (threadIdx.x == 0) {
+    tma::mbar_init(mb, 1);
+    timed_out = 0;
   }
+  stage_twiddles(tw, a.tw, a.plan);
+  __syncthreads();
+  pdl_wait();
+  const int rows = L / nbox;
+  if (threadIdx.x == 0) {
+    tma::mbar_arrive_expect(mb, (uint32_t)((size_t)L * ct * sizeof(Cx<T>)));
+    for (int b = 0; b < nbox; ++b)
+      tma::load4d(tma::smem_u32(bufA + (size_t)b * rows * ct), &map, c0 * (int)(sizeof(Cx<T>) / 4), 0, b * rows, o,
+                  mb);
+  }
+  if (!tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
+  __syncthreads();
+  if (timed_out) {
+    if (threadIdx.x == 0) {
+      atomicExch(status, 1);
+      tma::mbar_wait(mb, 0, tma::kWaitPolls);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < L * ct; l += blockDim.x) bufA[l] = mk<T>(nan_of<T>(), nan_of<T>());
+    __syncthreads();
+  }
+  axis_transform_store<T, INV, 1, false, FP>(a, bufA, bufB, tw, o, c0);
 }
 
 // grid = (ceil(ncols/col_tile), nouter)
@@ -292,11 +370,17 @@ struct pre_ypass<T, P, decltype((void)sizeof(typename P::YPass), void())> {
   static constexpr int groups = type::GROUPS, in_fields = type::IN_FIELDS, out_fields = type::OUT_FIELDS;
 };
 
+// Line stride of the z-pass buffers: one element more than the (even)
+// transform length, so consecutive lines start in different shared-memory
+// banks (the compiled transforms walk the lines fast, psb_fft.cuh).
+__host__ __device__ constexpr int zline(int M) { return M + 1; }
+
 // Shared memory of one z-pass CTA: twiddles, two buffers of
-// nl = ceil(fmax*P/2) packed lines of length M, and the Phys extra.
+// nl = ceil(fmax*P/2) packed lines of length M at stride zline(M), and the
+// Phys extra (16-byte aligned: M is even).
 template <typename T>
 __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
-  return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * M) * sizeof(Cx<T>) + extra;
+  return (size_t)(M + 2 * (size_t)((fmax * P + 1) / 2) * zline(M)) * sizeof(Cx<T>) + extra;
 }
 
 // Transform of the z-pass's contiguous lines: the plan's schedule (FP = 0) or
@@ -304,9 +388,9 @@ __host__ inline size_t zpass_smem_bytes(int fmax, int P, int M, size_t extra) {
 template <typename T, bool INV, bool WIDE, int FP>
 __device__ __forceinline__ Cx<T>* zfft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* tw, int nlines) {
   if constexpr (FP == 0)
-    return block_fft<T, INV, WIDE>(a, b, p, tw, nlines, p.L, 1, false);
+    return block_fft<T, INV, WIDE>(a, b, p, tw, nlines, zline(p.L), 1, nlines >= 8);
   else
-    return FixedPlan<FP>::template run<T, INV>(a, b, tw, nlines);
+    return FixedPlan<FP>::template run<T, INV>(a, b, tw, nlines, zline(p.L));
 }
 
 // Per-CTA staging of the z-pass: the twiddle table and the Phys extra (the
@@ -319,7 +403,7 @@ __device__ __forceinline__ void zpass_setup(const ZArgs<T>& a, const Phys& phys)
   if constexpr (phys_is_block<Phys>::value) {
     constexpr int FMAX = Phys::F_IN > Phys::F_OUT ? Phys::F_IN : Phys::F_OUT;
     const int nl = (FMAX * a.ppc + 1) / 2;
-    phys.setup(reinterpret_cast<unsigned char*>(tw + a.plan.L + (size_t)2 * nl * a.plan.L));
+    phys.setup(reinterpret_cast<unsigned char*>(tw + a.plan.L + (size_t)2 * nl * zline(a.plan.L)));
   }
 }
 
@@ -335,9 +419,10 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
   const int P = a.ppc;
   constexpr int FMAX = FI > FO ? FI : FO;
   const int nl = (FMAX * P + 1) / 2;
+  const int LS = zline(M);
   Cx<T>* X = tw + M;
-  Cx<T>* Y = X + (size_t)nl * M;
-  unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * M);
+  Cx<T>* Y = X + (size_t)nl * LS;
+  unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * LS);
   const long long p0 = (long long)bx * P;
   const int lp = __ffs(P) - 1;
   const Cx<T> zero = mk<T>(0, 0);
@@ -394,7 +479,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
               va = mk<T>(-kk * va.y, kk * va.x);
               vb = mk<T>(-kk * vb.y, kk * vb.x);
             }
-            Cx<T>* Z = X + (size_t)(cb + u * nw) * M;
+            Cx<T>* Z = X + (size_t)(cb + u * nw) * LS;
             if (k == 0 || k == half) {
               Z[k] = mk<T>(va.x, vb.x);
             } else {
@@ -407,7 +492,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
         for (int u = 0; u < U; ++u) {
           const int c = cb + u * nw;
           if (c >= nin) continue;
-          Cx<T>* Z = X + (size_t)c * M;
+          Cx<T>* Z = X + (size_t)c * LS;
           for (int k = kz[u] + lane; k <= M - kz[u]; k += 32) Z[k] = zero;
         }
       }
@@ -430,7 +515,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
         }
         if (part == 0) A = v; else B = v;
       }
-      Cx<T>* Z = X + (size_t)c * M;
+      Cx<T>* Z = X + (size_t)c * LS;
       if (k == 0 || k == half) {
         Z[k] = mk<T>(A.x, B.x);
       } else {
@@ -445,9 +530,9 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
   const int nout = (FO * P + 1) / 2;
   if constexpr (phys_is_block<Phys>::value) {
     // block-cooperative physics (a tensor-core MLP over the CTA's points)
-    phys.block(R, W, P, M, a.fac, p0, a.npencils, extra);
+    phys.block(R, W, P, M, LS, a.fac, p0, a.npencils, extra);
     if ((FO * P) & 1) {
-      for (int z = threadIdx.x; z < M; z += blockDim.x) reinterpret_cast<T*>(W + (size_t)(nout - 1) * M + z)[1] = (T)0;
+      for (int z = threadIdx.x; z < M; z += blockDim.x) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
     }
   } else {
     // pointwise physics; the last CTA may hold fewer than P pencils
@@ -457,7 +542,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
 #pragma unroll
       for (int f = 0; f < FI; ++f) {
         const int r = f * P + p;
-        const Cx<T> v = R[(size_t)(r >> 1) * M + z];
+        const Cx<T> v = R[(size_t)(r >> 1) * LS + z];
         vin[f] = a.fac * ((r & 1) ? v.y : v.x);
       }
       if (p0 + p < a.npencils) {
@@ -469,11 +554,11 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
 #pragma unroll
       for (int g = 0; g < FO; ++g) {
         const int r = g * P + p;
-        T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + z);
+        T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * LS + z);
         w[r & 1] = vout[g];
       }
       if ((FO * P) & 1) {  // odd count: the last packed line has no partner
-        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * M + z)[1] = (T)0;
+        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
       }
     }
   }
@@ -489,7 +574,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
         const int g = c / hp, p = 2 * (c - g * hp);
         const long long pa = p0 + p;
         const bool oka = pa < a.npencils, okb = pa + 1 < a.npencils;
-        const Cx<T>* Z = R2 + (size_t)c * M;
+        const Cx<T>* Z = R2 + (size_t)c * LS;
         Cx<T>* dst = a.out[g] + pa * a.out_pstride[g];
         const long long ps = a.out_pstride[g];
         for (int k = lane; k < kzo; k += 32) {
@@ -501,7 +586,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
     } else
     for (Walk2 w(kzo); w.s < nout; w.next()) {
       const int k = w.f, c = w.s;
-      const Cx<T>* Z = R2 + (size_t)c * M;
+      const Cx<T>* Z = R2 + (size_t)c * LS;
       const Cx<T> zk = Z[k], zm = Z[k == 0 ? 0 : M - k];
 #pragma unroll
       for (int part = 0; part < 2; ++part) {
@@ -577,30 +662,63 @@ struct XEpiArgs {
   const Cx<T>* tw;
 };
 
+// The blocks past main_blocks: columns kz..n3h-1 carry no products.
+template <typename T, class Epi>
+__device__ __forceinline__ void xfwd_epi_extra(const XEpiArgs<T>& a, const Epi& epi, int bx, int gx) {
+  constexpr int F = Epi::F_IN;
+  Cx<T> P[F];
+  const Cx<T> zero = mk<T>(0, 0);
+  const int ncz = a.n3h - a.kz;
+  const long long tot = (long long)a.n1 * a.n2 * ncz;
+  const int nextra = gx - a.main_blocks;
+  for (long long idx = (long long)(bx - a.main_blocks) * blockDim.x + threadIdx.x; idx < tot;
+       idx += (long long)nextra * blockDim.x) {
+    const int c = (int)(idx % ncz);
+    const long long t = idx / ncz;
+    const int i2 = (int)(t % a.n2), i1 = (int)(t / a.n2);
+#pragma unroll
+    for (int f = 0; f < F; ++f) P[f] = zero;
+    epi(i1, i2, a.kz + c, P);
+  }
+}
+
+// Transform of a staged tile and the epilogue on its output rows.  Must be
+// called by all threads.
+template <typename T, class Epi, bool WIDE, int FP>
+__device__ __forceinline__ void xfwd_transform_epi(const XEpiArgs<T>& a, const Epi& epi, Cx<T>* bufA, Cx<T>* bufB,
+                                                   const Cx<T>* tw, int o, int c0) {
+  constexpr int F = Epi::F_IN;
+  Cx<T> P[F];
+  const Cx<T> zero = mk<T>(0, 0);
+  const int ct = a.col_tile;
+  const int lines = F * ct;
+  const int nt = blockDim.x;
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
+  const int col = c0 + c;
+  const bool colok = col < a.kz;
+  Cx<T>* res = axfft<T, false, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
+  // threads past the last full row of columns would repeat a (row, column)
+  // (only when ct does not divide the CTA size): the epilogue is not idempotent
+  if (!colok || threadIdx.x >= dr * ct) return;
+  for (int i1 = r0; i1 < a.n1; i1 += dr) {
+    const int j = a.out_map(i1);
+#pragma unroll
+    for (int f = 0; f < F; ++f) P[f] = j >= 0 ? res[(size_t)j * lines + f * ct + c] : zero;
+    epi(i1, o, col, P);
+  }
+}
+
 // One CTA of the x-forward epilogue pass: block bx of gx = main_blocks + extra;
 // main block b -> (col tile b % ntile, outer b / ntile)
 template <typename T, class Epi, bool WIDE = false, int FP = 0>
 __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& epi, int bx, int gx) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int F = Epi::F_IN;
-  Cx<T> P[F];
   const Cx<T> zero = mk<T>(0, 0);
   pdl_trigger();
   if (bx >= a.main_blocks) {
     pdl_wait();
-    // columns kz..n3h-1 carry no products
-    const int ncz = a.n3h - a.kz;
-    const long long tot = (long long)a.n1 * a.n2 * ncz;
-    const int nextra = gx - a.main_blocks;
-    for (long long idx = (long long)(bx - a.main_blocks) * blockDim.x + threadIdx.x; idx < tot;
-         idx += (long long)nextra * blockDim.x) {
-      const int c = (int)(idx % ncz);
-      const long long t = idx / ncz;
-      const int i2 = (int)(t % a.n2), i1 = (int)(t / a.n2);
-#pragma unroll
-      for (int f = 0; f < F; ++f) P[f] = zero;
-      epi(i1, i2, a.kz + c, P);
-    }
+    xfwd_epi_extra<T, Epi>(a, epi, bx, gx);
     return;
   }
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
@@ -638,16 +756,64 @@ __device__ __forceinline__ void xfwd_epi_body(const XEpiArgs<T>& a, const Epi& e
     }
   }
   __syncthreads();
-  Cx<T>* res = axfft<T, false, WIDE, FP>(bufA, bufB, a.plan, tw, lines);
-  // threads past the last full row of columns would repeat a (row, column)
-  // (only when ct does not divide the CTA size): the epilogue is not idempotent
-  if (!colok || threadIdx.x >= dr * ct) return;
-  for (int i1 = r0; i1 < a.n1; i1 += dr) {
-    const int j = a.out_map(i1);
-#pragma unroll
-    for (int f = 0; f < F; ++f) P[f] = j >= 0 ? res[(size_t)j * lines + f * ct + c] : zero;
-    epi(i1, o, col, P);
+  xfwd_transform_epi<T, Epi, WIDE, FP>(a, epi, bufA, bufB, tw, o, c0);
+}
+
+// TMA-staged x-forward epilogue pass: the tile (ct columns x F fields x L
+// rows of one outer index) arrives by bulk tensor copies of L/nbox rows each
+// through map, a 4-D view (columns, fields, rows, outer index) of a.in.  A
+// copy that does not complete within the poll limit raises *status and the
+// CTA hands NaN to the epilogue in place of its tile.
+template <typename T, class Epi, int FP = 0>
+__global__ void __launch_bounds__(256) xfwd_epi_tma_kernel(XEpiArgs<T> a, Epi epi,
+                                                           const __grid_constant__ CUtensorMap map, int nbox,
+                                                           int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ int timed_out;
+  constexpr int F = Epi::F_IN;
+  pdl_trigger();
+  if ((int)blockIdx.x >= a.main_blocks) {
+    pdl_wait();
+    xfwd_epi_extra<T, Epi>(a, epi, blockIdx.x, gridDim.x);
+    return;
   }
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int L = a.plan.L;
+  const int ct = a.col_tile;
+  const int lines = F * ct;
+  Cx<T>* bufA = reinterpret_cast<Cx<T>*>(smem_raw + tma_buf_offset<T>(L));
+  Cx<T>* bufB = bufA + (size_t)L * lines;
+  const int ntile = (a.kz + ct - 1) / ct;
+  const int o = blockIdx.x / ntile;
+  const int c0 = (blockIdx.x % ntile) * ct;
+  const uint32_t mb = tma::smem_u32(&mbar);
+  if (threadIdx.x == 0) {
+    tma::mbar_init(mb, 1);
+    timed_out = 0;
+  }
+  stage_twiddles(tw, a.tw, a.plan);
+  __syncthreads();
+  pdl_wait();
+  const int rows = L / nbox;
+  if (threadIdx.x == 0) {
+    tma::mbar_arrive_expect(mb, (uint32_t)((size_t)L * lines * sizeof(Cx<T>)));
+    for (int b = 0; b < nbox; ++b)
+      tma::load4d(tma::smem_u32(bufA + (size_t)b * rows * lines), &map, c0 * (int)(sizeof(Cx<T>) / 4), 0,
+                  b * rows, o, mb);
+  }
+  if (!tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
+  __syncthreads();
+  if (timed_out) {
+    if (threadIdx.x == 0) {
+      atomicExch(status, 1);
+      tma::mbar_wait(mb, 0, tma::kWaitPolls);
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l < L * lines; l += blockDim.x) bufA[l] = mk<T>(nan_of<T>(), nan_of<T>());
+    __syncthreads();
+  }
+  xfwd_transform_epi<T, Epi, false, FP>(a, epi, bufA, bufB, tw, o, c0);
 }
 
 // grid = main_blocks + extra

@@ -731,17 +731,17 @@ struct PhysLearned {
   __device__ void setup(unsigned char* extra) const {
     mlp_stage_fwd<H>(*reinterpret_cast<MlpFwdSmem<H>*>(extra), params, norm);
   }
-  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, T fac, long long, long long,
+  __device__ void block(const Cx<T>* R, Cx<T>* W, int P, int M, int LS, T fac, long long, long long,
                         unsigned char* extra) const {
-    block_act(R, W, P, M, fac, extra);
+    block_act(R, W, P, M, LS, fac, extra);
   }
   // Each warp takes tiles of 16 consecutive points (pencil-major); a lane
   // holds rows g and g+8 of a tile and locates them once per tile.
-  __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, T fac,
+  __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, int LS, T fac,
                                             unsigned char* extra) const {
     const MlpFwdSmem<H>& s = *reinterpret_cast<const MlpFwdSmem<H>*>(extra);
     if ((M & 15) == 0 && (P & 1) == 0) {
-      block_tiles(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, fac, s);
+      block_tiles(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, LS, fac, s);
       return;
     }
     const int npts = P * M;
@@ -762,7 +762,7 @@ struct PhysLearned {
       }
       auto val = [&](int f, int h) -> T {
         const int r = f * P + rp[h];
-        const Cx<T> v = R[(size_t)(r >> 1) * M + rz[h]];
+        const Cx<T> v = R[(size_t)(r >> 1) * LS + rz[h]];
         return (r & 1) ? v.y : v.x;
       };
       uint32_t xa[4];
@@ -783,21 +783,21 @@ struct PhysLearned {
         const T tau = (T)(y[e] * s.ystd[c] + s.ymean[c]);
         const T o = (fac * val(ii, h)) * (fac * val(jj, h)) + tau * is2;
         const int r = c * P + rp[h];
-        reinterpret_cast<T*>(W + (size_t)(r >> 1) * M + rz[h])[r & 1] = o;
+        reinterpret_cast<T*>(W + (size_t)(r >> 1) * LS + rz[h])[r & 1] = o;
       }
     }
   }
   // The same computation when every tile is 16 consecutive z of one pencil
   // (M % 16 == 0) and packed lines pair pencils of one field (P even): real
-  // line (f, p) is half p&1 of packed line f*P/2 + p/2, so field f of pencil
-  // p at z is T element f*P*M + 2((p/2) M + z) + (p&1).  Each lane keeps the
+  // line (f, p) is half p&1 of packed line f*P/2 + p/2 (lines LS apart), so
+  // field f of pencil p at z is T element f*P*LS + 2((p/2) LS + z) + (p&1).  Each lane keeps the
   // offsets, normalisation and output coefficients of its fragment slots in
   // registers; per tile it computes one base index per row.
-  __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, T fac,
-                                              const MlpFwdSmem<H>& s) const {
+  __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, int LS,
+                                              T fac, const MlpFwdSmem<H>& s) const {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int nw = blockDim.x >> 5;
-    const int fst = P * M;
+    const int fst = P * LS;
     const T is2 = (T)1 / (sphys * sphys);
     const T fs = fac * sphys;
     // feature slot q = 2 hk + e holds feature f = 2t + 8hk + e: a gradient
@@ -833,7 +833,7 @@ struct PhysLearned {
     for (int tile = warp; tile < ntile; tile += nw) {
       const int p = tile / tpp;
       const int z0 = (tile - p * tpp) << 4;
-      const int b0 = 2 * ((p >> 1) * M + z0 + g) + (p & 1);  // row g; row g + 8 is b0 + 16
+      const int b0 = 2 * ((p >> 1) * LS + z0 + g) + (p & 1);  // row g; row g + 8 is b0 + 16
       float v[8];
 #pragma unroll
       for (int hr = 0; hr < 2; ++hr)
