@@ -136,9 +136,11 @@ int psb_ctx_set_stream(psb_ctx* ctx, void* stream);
  * results either way; no counterpart in the reference (a launch choice). */
 int psb_ctx_set_tma(psb_ctx* ctx, int enable);
 /* Device status of the context's kernels since the last call, then cleared:
- * 0, or 1 when a bounded wait inside a kernel gave up (that kernel wrote NaN
- * in place of the tile it could not stage instead of hanging).  Synchronises
- * the context stream.  No counterpart in the reference (it has no device). */
+ * 0; 1 when a bounded wait inside a kernel gave up; 2 when a kernel found a
+ * bulk-copy destination off its alignment and issued nothing.  In both cases
+ * that kernel wrote NaN in place of the tile it could not stage instead of
+ * hanging or faulting.  Synchronises the context stream.  No counterpart in
+ * the reference (it has no device). */
 int psb_device_status(psb_ctx* ctx, int* status);
 /* Message of the last failure on this context ("" if none). */
 const char* psb_last_error(const psb_ctx* ctx);
@@ -311,6 +313,24 @@ int psb_batch_step_rk4(psb_batch* b, int nsteps);
  * order of its transform (maxr entries, 0-terminated). */
 int psb_batch_shape(const psb_batch* b, int pass, int* tile, int* radices, int maxr);
 int psb_batch_destroy(psb_batch* b);
+
+/* ---- persistent ensembles (no reference counterpart) ----------------------
+ * Up to 4 batches on one device and precision (grid sizes and closures may
+ * differ: PSB_DNS, PSB_SMAG, PSB_LEARNED with a ReLU width-32 network)
+ * advanced together by ONE cooperative launch per call: the kernel walks the
+ * RK4 stages and the five passes, spreading each pass's tiles over every run
+ * of every batch, with a grid barrier between passes.  Every barrier wait is
+ * bounded (poll_limit polls; 0 = the default of 2^26): a wait that gives up
+ * raises the ensemble's status word and the kernel returns early (the states
+ * are then partly advanced).  The batches' runs and shapes are read at each
+ * call; step once outside a stream capture before capturing calls. */
+typedef struct psb_ensemble psb_ensemble;
+int psb_ensemble_create(psb_batch* const* batches, int nbatch, psb_ensemble** out);
+int psb_ensemble_step_rk4(psb_ensemble* e, int nsteps, unsigned poll_limit);
+/* 0, or 1 when a grid-barrier wait gave up since the last call (then cleared;
+ * synchronises the first batch's stream). */
+int psb_ensemble_status(psb_ensemble* e, int* status);
+int psb_ensemble_destroy(psb_ensemble* e);
 
 /* ---- autotuned single runs (no reference counterpart) --------------------
  * Time the candidate launch shapes of the five passes of closure's RHS

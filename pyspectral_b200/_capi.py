@@ -32,7 +32,8 @@ EXPORTS = (
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
     "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear", "psb_set_tuned_shape",
-    "psb_ctx_set_tma", "psb_device_status",
+    "psb_ctx_set_tma", "psb_device_status", "psb_ensemble_create", "psb_ensemble_step_rk4", "psb_ensemble_status",
+    "psb_ensemble_destroy",
 )
 
 

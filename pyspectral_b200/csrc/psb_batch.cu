@@ -16,6 +16,7 @@
 #include <cstring>
 
 #include "psb_ctx.cuh"
+#include "psb_grid.cuh"
 
 using namespace psb;
 using namespace psbh;
@@ -586,6 +587,140 @@ int dispatch(psb_batch* b, int nsteps, bool tune) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent ensemble: every batch of an ensemble (grid sizes and closures may
+// differ) advanced by ONE cooperative launch per call.  The kernel walks the
+// RK4 stages and the five passes of each; a pass's work items -- the CTA tiles
+// of that pass over every run of every batch -- are spread over the CTAs, and
+// a bounded grid barrier separates consecutive passes (a pass reads what the
+// previous one wrote).  Each item runs the same tile body as the batched
+// launches (runtime transform schedules, every radix), with the batch's own
+// argument blocks, so the results equal the batched step's up to the
+// schedule's rounding.
+// ---------------------------------------------------------------------------
+constexpr int kEnsMaxGroups = 4;
+enum EnsKind : int { kEnsDns = 0, kEnsSmag = 1, kEnsLearnedR32 = 2 };
+
+struct EnsGroup {
+  int kind;
+  int R;
+  int nx[5], ny[5];  // tiles of a pass per run: nx x ny (pass 4: nx = main + extra blocks)
+  long long items[5];
+  const void *ax, *ay, *ayf, *az, *ae, *pre, *ypre, *cpy, *phys, *epi;
+};
+struct EnsDesc {
+  int ngroups;
+  EnsGroup g[kEnsMaxGroups];
+};
+
+template <typename T, class Pre, class Phys, class Epi>
+__device__ __forceinline__ void ens_item(const EnsGroup& g, int pass, int stage, long long i) {
+  using YP = pre_ypass<T, Pre>;
+  using YPre = typename YP::type;
+  const long long per = (long long)g.nx[pass] * g.ny[pass];
+  const int r = (int)(i / per);
+  const int rem = (int)(i - (long long)r * per);
+  const int by = rem / g.nx[pass], bx = rem - by * g.nx[pass];
+  switch (pass) {
+    case 0:
+      axis_pass_body<T, true, Pre, true>(static_cast<const AxisArgs<T>*>(g.ax)[r], static_cast<const Pre*>(g.pre)[r],
+                                         bx, by);
+      break;
+    case 1:
+      axis_pass_body<T, true, YPre, true>(static_cast<const AxisArgs<T>*>(g.ay)[r],
+                                          static_cast<const YPre*>(g.ypre)[r], bx, by);
+      break;
+    case 2:
+      zpass_body<T, Phys, true>(static_cast<const ZArgs<T>*>(g.az)[r], static_cast<const Phys*>(g.phys)[r], bx);
+      break;
+    case 3:
+      axis_pass_body<T, false, PreCopy<T>, true>(static_cast<const AxisArgs<T>*>(g.ayf)[r],
+                                                 static_cast<const PreCopy<T>*>(g.cpy)[r], bx, by);
+      break;
+    default:
+      xfwd_epi_body<T, Epi, true>(static_cast<const XEpiArgs<T>*>(g.ae)[r],
+                                  static_cast<const Epi*>(g.epi)[(size_t)stage * g.R + r], bx, g.nx[4]);
+      break;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) ens_persistent_kernel(const EnsDesc* __restrict__ D, GridBar* gb,
+                                                                int* status, int nsteps, unsigned limit) {
+  const int ng = D->ngroups;
+  for (int step = 0; step < nsteps; ++step)
+    for (int stage = 0; stage < 4; ++stage)
+      for (int pass = 0; pass < 5; ++pass) {
+        long long total = 0;
+        for (int q = 0; q < ng; ++q) total += D->g[q].items[pass];
+        for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+          long long i = it;
+          int q = 0;
+          while (q < ng - 1 && i >= D->g[q].items[pass]) i -= D->g[q++].items[pass];
+          const EnsGroup& g = D->g[q];
+          switch (g.kind) {
+            case kEnsDns:
+              ens_item<T, PreCopyN<T, 3>, PhysProducts<T>, EpiNS<T, false>>(g, pass, stage, i);
+              break;
+            case kEnsSmag:
+              ens_item<T, PreStrain<T>, PhysSmag<T>, EpiNS<T, true>>(g, pass, stage, i);
+              break;
+            default:
+              ens_item<T, PreGradXY<T>, PhysLearned<T, kActRelu, 32>, EpiNS<T, false>>(g, pass, stage, i);
+              break;
+          }
+          __syncthreads();  // the next item reuses the shared memory
+        }
+        if (!grid_barrier(gb, gridDim.x, limit, status)) return;
+      }
+}
+
+// Host view of one batch for the ensemble: its device argument blocks, items and shared memory.
+template <typename T, class Pre, class Phys, class Epi>
+size_t ens_group(psb_batch* b, int kind, EnsGroup& g) {
+  using BT = Batch<T, Pre, Phys, Epi>;
+  BT x;
+  x.b = b;
+  x.c = b->c;
+  x.d = dims(b->c, BT::Fi, BT::Fb, BT::Fo);
+  x.R = b->nruns;
+  x.views(reinterpret_cast<char*>(b->dargs));
+  const Dims& d = x.d;
+  g.kind = kind;
+  g.R = b->nruns;
+  g.ax = x.ax;
+  g.ay = x.ay;
+  g.ayf = x.ayf;
+  g.az = x.az;
+  g.ae = x.ae;
+  g.pre = x.pre;
+  g.ypre = x.ypre;
+  g.cpy = x.cpy;
+  g.phys = x.phys;
+  g.epi = x.epi;
+  const int* t = b->tile.data();
+  g.nx[0] = (d.Kz + t[0] - 1) / t[0];
+  g.ny[0] = d.N2;
+  g.nx[1] = (d.Kz + t[1] - 1) / t[1];
+  g.ny[1] = BT::YP::groups * d.M1;
+  g.nx[2] = (int)(((long long)d.M1 * d.M2 + t[2] - 1) / t[2]);
+  g.ny[2] = 1;
+  g.nx[3] = (d.Kz + t[3] - 1) / t[3];
+  g.ny[3] = BT::Fo * d.M1;
+  const int mainb = ((d.Kz + t[4] - 1) / t[4]) * d.N2;
+  const long long pts = (long long)d.N1 * d.N2 * (d.N3h - d.Kz);
+  g.nx[4] = mainb + (int)std::min<long long>((pts + 255) / 256, 1024);
+  g.ny[4] = 1;
+  for (int k = 0; k < 5; ++k) g.items[k] = (long long)g.nx[k] * g.ny[k] * g.R;
+  size_t sm = 0;
+  sm = std::max(sm, x.smem_axis(d.M1, BT::Fi, t[0]));
+  sm = std::max(sm, x.smem_axis(d.M2, BT::YPre::F_DST, t[1]));
+  sm = std::max(sm, x.smem_z(t[2]));
+  sm = std::max(sm, x.smem_axis(d.M2, 1, t[3]));
+  sm = std::max(sm, x.smem_axis(d.M1, BT::Fo, t[4]));
+  return sm;
+}
+
 }  // namespace
 
 extern "C" {
@@ -672,6 +807,132 @@ int psb_tuned_shape(const psb_ctx* c, int closure, int pass, int* tile, int* rad
 int psb_autotune_clear(psb_ctx* c, int closure) {
   if (!c) return PSB_ERR_ARG;
   c->tuned.erase(closure);
+  return PSB_OK;
+}
+
+struct psb_ensemble {
+  psb_ctx* c = nullptr;  // the first batch's context: stream and device
+  std::vector<psb_batch*> batches;
+  void* dev = nullptr;  // EnsDesc, then GridBar, then the status word
+  int prec = 64;
+  EnsDesc uploaded{};   // the descriptor on the device (uploads happen only when it changes)
+  bool have = false;
+};
+
+int psb_ensemble_create(psb_batch* const* batches, int nbatch, psb_ensemble** out) {
+  if (!batches || !out || nbatch < 1) return PSB_ERR_ARG;
+  *out = nullptr;
+  psb_ctx* c = batches[0] ? batches[0]->c : nullptr;
+  if (!c) return PSB_ERR_ARG;
+  if (nbatch > kEnsMaxGroups) return fail(c, PSB_ERR_ARG, "psb_ensemble_create: at most 4 batches");
+  for (int i = 0; i < nbatch; ++i) {
+    const psb_batch* b = batches[i];
+    if (!b || b->c->dev != c->dev || b->c->prec != c->prec)
+      return fail(c, PSB_ERR_ARG, "psb_ensemble_create: every batch on one device and precision");
+    const bool learned_ok = b->closure == PSB_LEARNED && b->params[0].mlp_act == PSB_ACT_RELU &&
+                            b->params[0].mlp_hidden == 32;
+    if (b->closure != PSB_DNS && b->closure != PSB_SMAG && !learned_ok)
+      return fail(c, PSB_ERR_UNSUPPORTED,
+                  "psb_ensemble_create: batches of PSB_DNS, PSB_SMAG or PSB_LEARNED (ReLU, width 32)");
+  }
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  psb_ensemble* e = new psb_ensemble();
+  e->c = c;
+  e->prec = c->prec;
+  e->batches.assign(batches, batches + nbatch);
+  cudaError_t err = cudaMalloc(&e->dev, sizeof(EnsDesc) + sizeof(GridBar) + 16);
+  if (err == cudaSuccess) err = cudaMemset(e->dev, 0, sizeof(EnsDesc) + sizeof(GridBar) + 16);  // status 0
+  if (err != cudaSuccess) {
+    delete e;
+    return fail(c, PSB_ERR_CUDA, std::string("psb_ensemble_create: ") + cudaGetErrorString(err));
+  }
+  *out = e;
+  return PSB_OK;
+}
+
+}  // extern "C"
+
+template <typename T>
+static int ens_step(psb_ensemble* e, int nsteps, unsigned limit) {
+  psb_ctx* c = e->c;
+  EnsDesc h{};
+  h.ngroups = (int)e->batches.size();
+  size_t smem = 0;
+  for (int i = 0; i < h.ngroups; ++i) {
+    psb_batch* b = e->batches[i];
+    PSB_TRY(psb_batch_step_rk4(b, 0));  // (re)build the argument blocks of a changed batch
+    if (b->closure == PSB_DNS)
+      smem = std::max(smem, ens_group<T, PreCopyN<T, 3>, PhysProducts<T>, EpiNS<T, false>>(b, kEnsDns, h.g[i]));
+    else if (b->closure == PSB_SMAG)
+      smem = std::max(smem, ens_group<T, PreStrain<T>, PhysSmag<T>, EpiNS<T, true>>(b, kEnsSmag, h.g[i]));
+    else
+      smem = std::max(smem, ens_group<T, PreGradXY<T>, PhysLearned<T, kActRelu, 32>, EpiNS<T, false>>(
+                                b, kEnsLearnedR32, h.g[i]));
+  }
+  auto k = ens_persistent_kernel<T>;
+  if (smem > 48 * 1024)
+    PSB_TRY(cuda_ok(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                    "ensemble shared memory"));
+  int per = 0, nsm = 0;
+  PSB_TRY(cuda_ok(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, 256, smem), "ensemble occupancy"));
+  PSB_TRY(cuda_ok(c, cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->dev), "SM count"));
+  if (per < 1) return fail(c, PSB_ERR_SHAPE, "psb_ensemble_step_rk4: the tiles' shared memory leaves no CTA per SM");
+  unsigned grid = (unsigned)(per * nsm);
+  char* dv = static_cast<char*>(e->dev);
+  EnsDesc* dd = reinterpret_cast<EnsDesc*>(dv);
+  GridBar* gb = reinterpret_cast<GridBar*>(dv + sizeof(EnsDesc));
+  int* status = reinterpret_cast<int*>(dv + sizeof(EnsDesc) + sizeof(GridBar));
+  // the descriptor changes only when a batch's runs or shapes do: upload it
+  // then (not while the stream is captured), after the stream drains
+  if (!e->have || std::memcmp(&h, &e->uploaded, sizeof(EnsDesc)) != 0) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PSB_TRY(cuda_ok(c, cudaStreamIsCapturing(c->stream, &cap), "capture status"));
+    if (cap != cudaStreamCaptureStatusNone)
+      return fail(c, PSB_ERR_ARG, "psb_ensemble_step_rk4: step once outside a stream capture first");
+    PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "ensemble: drain the stream"));
+    PSB_TRY(cuda_ok(c, cudaMemcpy(dd, &h, sizeof(EnsDesc), cudaMemcpyHostToDevice), "ensemble descriptor"));
+    e->uploaded = h;
+    e->have = true;
+  }
+  PSB_TRY(cuda_ok(c, cudaMemsetAsync(gb, 0, sizeof(GridBar), c->stream), "grid barrier reset"));
+  if (nsteps == 0) return PSB_OK;
+  void* args[] = {&dd, &gb, &status, &nsteps, &limit};
+  {
+    LaunchScope ls(c, "ensemble persistent", 0.0);
+    PSB_TRY(cuda_ok(c, cudaLaunchCooperativeKernel((const void*)k, dim3(grid), dim3(256), args, smem, c->stream),
+                    "ensemble persistent launch"));
+  }
+  return PSB_OK;
+}
+
+extern "C" {
+
+int psb_ensemble_step_rk4(psb_ensemble* e, int nsteps, unsigned poll_limit) {
+  if (!e) return PSB_ERR_ARG;
+  if (nsteps < 0) return fail(e->c, PSB_ERR_ARG, "psb_ensemble_step_rk4: nsteps < 0");
+  PSB_TRY(cuda_ok(e->c, cudaSetDevice(e->c->dev), "cudaSetDevice"));
+  const unsigned limit = poll_limit ? poll_limit : (1u << 26);
+  return e->prec == 64 ? ens_step<double>(e, nsteps, limit) : ens_step<float>(e, nsteps, limit);
+}
+
+int psb_ensemble_status(psb_ensemble* e, int* status) {
+  if (!e || !status) return PSB_ERR_ARG;
+  psb_ctx* c = e->c;
+  PSB_TRY(cuda_ok(c, cudaSetDevice(c->dev), "cudaSetDevice"));
+  int* st = reinterpret_cast<int*>(static_cast<char*>(e->dev) + sizeof(EnsDesc) + sizeof(GridBar));
+  int h = 0;
+  PSB_TRY(cuda_ok(c, cudaMemcpyAsync(&h, st, sizeof(int), cudaMemcpyDeviceToHost, c->stream), "status read"));
+  PSB_TRY(cuda_ok(c, cudaMemsetAsync(st, 0, sizeof(int), c->stream), "status clear"));
+  PSB_TRY(cuda_ok(c, cudaStreamSynchronize(c->stream), "status sync"));
+  *status = h;
+  return PSB_OK;
+}
+
+int psb_ensemble_destroy(psb_ensemble* e) {
+  if (!e) return PSB_ERR_ARG;
+  cudaSetDevice(e->c->dev);
+  if (e->dev) cudaFree(e->dev);
+  delete e;
   return PSB_OK;
 }
 

@@ -325,7 +325,10 @@ int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const
     const int nbox = tma_boxes(L);
     CUtensorMap map;
     const bool plain_rows = a.in_rows == L && a.in_map.lo >= L;
-    if (c->use_tma && plain_rows && nbox > 0 && (a.col_tile * esz) % 16 == 0 && !(sh && sh->wide)) {
+    // every box lands on a 128-byte boundary: the buffer's start, and box b at b*(L/nbox) rows
+    const bool boxes_aligned = nbox == 1 || ((size_t)(L / nbox) * a.col_tile * esz) % 128 == 0;
+    if (c->use_tma && plain_rows && nbox > 0 && boxes_aligned && (a.col_tile * esz) % 16 == 0 &&
+        !(sh && sh->wide)) {
       const long long dims[4] = {a.ncols, 1, a.in_rows, a.nouter};
       const long long strides[3] = {a.in_rstride, a.in_rstride, a.in_ostride};
       const int box[4] = {a.col_tile, 1, L / nbox, 1};
@@ -444,7 +447,8 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
   {
     const int nbox = tma_boxes(L);
     CUtensorMap map;
-    if (c->use_tma && nbox > 0 && (e.col_tile * esz) % 16 == 0 && !(sh && sh->wide)) {
+    const bool boxes_aligned = nbox == 1 || ((size_t)(L / nbox) * Epi::F_IN * e.col_tile * esz) % 128 == 0;
+    if (c->use_tma && nbox > 0 && boxes_aligned && (e.col_tile * esz) % 16 == 0 && !(sh && sh->wide)) {
       const long long dims[4] = {e.kz, Epi::F_IN, L, e.n2};
       const long long strides[3] = {e.in_fstride, e.in_rstride, e.in_ostride};
       const int box[4] = {e.col_tile, Epi::F_IN, L / nbox, 1};

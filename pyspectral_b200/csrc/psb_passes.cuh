@@ -182,11 +182,36 @@ __device__ __forceinline__ T nan_of() {
   return sizeof(T) == 8 ? (T)__longlong_as_double(0x7ff8000000000000ll) : (T)__int_as_float(0x7fc00000);
 }
 
-// Offset of the transform buffer behind the twiddles in a TMA-staged pass:
-// bulk tensor copies land on 128-byte boundaries.
+// Shared memory of a TMA-staged pass ahead of its two transform buffers: the
+// twiddles and up to 127 bytes that bring the first buffer to a 128-byte
+// boundary of the shared window (bulk tensor copies land on such boundaries;
+// the dynamic region starts behind the kernel's static shared variables).
 template <typename T>
 __host__ __device__ inline size_t tma_buf_offset(int L) {
-  return ((size_t)L * sizeof(Cx<T>) + 127) / 128 * 128;
+  return (size_t)L * sizeof(Cx<T>) + 128;
+}
+// The transform buffer: the first 128-byte boundary of the shared window at
+// or after the twiddles' end.
+template <typename T>
+__device__ __forceinline__ Cx<T>* tma_buf(unsigned char* smem, int L) {
+  const uint32_t a = tma::smem_u32(smem) + (uint32_t)(L * sizeof(Cx<T>));
+  const uint32_t pad = (128u - (a & 127u)) & 127u;
+  return reinterpret_cast<Cx<T>*>(smem + L * sizeof(Cx<T>) + pad);
+}
+// Issue the copies of a tile of nbox boxes of `rows` rows each (box b: rows
+// b*rows.., landing `box_elems` elements after box b-1; x the first column in
+// 32-bit words, outer the outer index) unless a destination or the tensor map
+// breaks the copy's alignment rules; returns false (nothing issued) then.
+template <typename T>
+__device__ __forceinline__ bool tma_issue(const CUtensorMap* map, Cx<T>* dst, size_t box_elems, int nbox, int rows,
+                                          int x, int outer, uint32_t mb, uint32_t bytes) {
+  if ((reinterpret_cast<uintptr_t>(map) & 63) != 0) return false;
+  for (int b = 0; b < nbox; ++b)
+    if ((tma::smem_u32(dst + (size_t)b * box_elems) & 127u) != 0) return false;
+  tma::mbar_arrive_expect(mb, bytes);
+  for (int b = 0; b < nbox; ++b)
+    tma::load4d(tma::smem_u32(dst + (size_t)b * box_elems), map, x, 0, b * rows, outer, mb);
+  return true;
 }
 
 template <typename T, bool INV, class Pre, bool WIDE = false, int FP = 0>
@@ -270,7 +295,7 @@ __global__ void __launch_bounds__(256) axis_pass_tma_kernel(AxisArgs<T> a, const
   Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
   const int L = a.plan.L;
   const int ct = a.col_tile;
-  Cx<T>* bufA = reinterpret_cast<Cx<T>*>(smem_raw + tma_buf_offset<T>(L));
+  Cx<T>* bufA = tma_buf<T>(smem_raw, L);
   Cx<T>* bufB = bufA + (size_t)L * ct;
   const int o = blockIdx.y;
   const int c0 = blockIdx.x * ct;
@@ -284,18 +309,17 @@ __global__ void __launch_bounds__(256) axis_pass_tma_kernel(AxisArgs<T> a, const
   __syncthreads();
   pdl_wait();
   const int rows = L / nbox;
-  if (threadIdx.x == 0) {
-    tma::mbar_arrive_expect(mb, (uint32_t)((size_t)L * ct * sizeof(Cx<T>)));
-    for (int b = 0; b < nbox; ++b)
-      tma::load4d(tma::smem_u32(bufA + (size_t)b * rows * ct), &map, c0 * (int)(sizeof(Cx<T>) / 4), 0, b * rows, o,
-                  mb);
-  }
-  if (!tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
+  if (threadIdx.x == 0 &&
+      !tma_issue<T>(&map, bufA, (size_t)rows * ct, nbox, rows, c0 * (int)(sizeof(Cx<T>) / 4), o, mb,
+                    (uint32_t)((size_t)L * ct * sizeof(Cx<T>))))
+    timed_out = 2;  // nothing issued: the barrier's phase will not complete
+  __syncthreads();
+  if (timed_out == 0 && !tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
   __syncthreads();
   if (timed_out) {
     if (threadIdx.x == 0) {
-      atomicExch(status, 1);
-      tma::mbar_wait(mb, 0, tma::kWaitPolls);
+      atomicExch(status, timed_out);
+      if (timed_out == 1) tma::mbar_wait(mb, 0, tma::kWaitPolls);
     }
     __syncthreads();
     for (int l = threadIdx.x; l < L * ct; l += blockDim.x) bufA[l] = mk<T>(nan_of<T>(), nan_of<T>());
@@ -782,7 +806,7 @@ __global__ void __launch_bounds__(256) xfwd_epi_tma_kernel(XEpiArgs<T> a, Epi ep
   const int L = a.plan.L;
   const int ct = a.col_tile;
   const int lines = F * ct;
-  Cx<T>* bufA = reinterpret_cast<Cx<T>*>(smem_raw + tma_buf_offset<T>(L));
+  Cx<T>* bufA = tma_buf<T>(smem_raw, L);
   Cx<T>* bufB = bufA + (size_t)L * lines;
   const int ntile = (a.kz + ct - 1) / ct;
   const int o = blockIdx.x / ntile;
@@ -796,18 +820,17 @@ __global__ void __launch_bounds__(256) xfwd_epi_tma_kernel(XEpiArgs<T> a, Epi ep
   __syncthreads();
   pdl_wait();
   const int rows = L / nbox;
-  if (threadIdx.x == 0) {
-    tma::mbar_arrive_expect(mb, (uint32_t)((size_t)L * lines * sizeof(Cx<T>)));
-    for (int b = 0; b < nbox; ++b)
-      tma::load4d(tma::smem_u32(bufA + (size_t)b * rows * lines), &map, c0 * (int)(sizeof(Cx<T>) / 4), 0,
-                  b * rows, o, mb);
-  }
-  if (!tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
+  if (threadIdx.x == 0 &&
+      !tma_issue<T>(&map, bufA, (size_t)rows * lines, nbox, rows, c0 * (int)(sizeof(Cx<T>) / 4), o, mb,
+                    (uint32_t)((size_t)L * lines * sizeof(Cx<T>))))
+    timed_out = 2;  // nothing issued: the barrier's phase will not complete
+  __syncthreads();
+  if (timed_out == 0 && !tma::mbar_wait(mb, 0, tma::kWaitPolls)) timed_out = 1;
   __syncthreads();
   if (timed_out) {
     if (threadIdx.x == 0) {
-      atomicExch(status, 1);
-      tma::mbar_wait(mb, 0, tma::kWaitPolls);
+      atomicExch(status, timed_out);
+      if (timed_out == 1) tma::mbar_wait(mb, 0, tma::kWaitPolls);
     }
     __syncthreads();
     for (int l = threadIdx.x; l < L * lines; l += blockDim.x) bufA[l] = mk<T>(nan_of<T>(), nan_of<T>());

@@ -52,7 +52,11 @@ def _lib():
                            ("psb_batch_set_run", [vp, i, vp, vp, ctypes.POINTER(_capi.Params)]),
                            ("psb_batch_autotune", [vp]), ("psb_batch_step_rk4", [vp, i]),
                            ("psb_batch_shape", [vp, i, ctypes.POINTER(i), ctypes.POINTER(i), i]),
-                           ("psb_batch_destroy", [vp])):
+                           ("psb_batch_destroy", [vp]),
+                           ("psb_ensemble_create", [ctypes.POINTER(vp), i, ctypes.POINTER(vp)]),
+                           ("psb_ensemble_step_rk4", [vp, i, ctypes.c_uint]),
+                           ("psb_ensemble_status", [vp, ctypes.POINTER(i)]),
+                           ("psb_ensemble_destroy", [vp])):
             fn = getattr(lib, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int
@@ -100,6 +104,42 @@ class Batch:
         if h:
             try:
                 self.lib.psb_batch_destroy(h)
+            except Exception:
+                pass
+            self.h = None
+
+
+class Persistent:
+    """Up to four batches (one device, one precision) advanced by one
+    cooperative launch per call (``psb_ensemble``): every pass of every RK4
+    stage spreads its tiles over all runs of all batches, with a bounded grid
+    barrier between passes."""
+
+    def __init__(self, batches):
+        self.lib = _lib()
+        self.batches = list(batches)
+        self.ctx = self.batches[0].ctx
+        arr = (ctypes.c_void_p * len(self.batches))(*[b.h.value for b in self.batches])
+        h = ctypes.c_void_p()
+        self.ctx.check(self.lib.psb_ensemble_create(arr, len(self.batches), ctypes.byref(h)), "psb_ensemble_create")
+        self.h = h
+
+    def step(self, nsteps=1, poll_limit=0):
+        self.ctx.bind_stream()
+        self.ctx.check(self.lib.psb_ensemble_step_rk4(self.h, int(nsteps), int(poll_limit)), "psb_ensemble_step_rk4")
+
+    def status(self):
+        """0, or 1 when a grid-barrier wait gave up since the last call (cleared on read)."""
+        self.ctx.bind_stream()
+        st = ctypes.c_int()
+        self.ctx.check(self.lib.psb_ensemble_status(self.h, ctypes.byref(st)), "psb_ensemble_status")
+        return st.value
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            try:
+                self.lib.psb_ensemble_destroy(h)
             except Exception:
                 pass
             self.h = None
@@ -185,6 +225,31 @@ class Ensemble:
     def shapes(self):
         return {g["N"]: g["batch"].shapes() for g in self.groups}
 
+    def persistent(self):
+        """The persistent form: every batch of the ensemble in one cooperative
+        launch per call (requires one context stream: the launches go on the
+        first batch's context's stream, the current torch stream)."""
+        if getattr(self, "_pers", None) is None:
+            self._pers = Persistent([g["batch"] for g in self.groups])
+        return self._pers
+
+    def capture_persistent(self, nsteps=1):
+        """One CUDA graph holding one persistent launch of nsteps steps."""
+        p = self.persistent()
+        saved = [[t.clone() for t in g["states"] + [c for c in g["comps"] if c is not None]] for g in self.groups]
+        p.step(nsteps)  # outside the capture: argument blocks and the launch descriptor
+        torch.cuda.synchronize()
+        for g, sv in zip(self.groups, saved):
+            for t, s in zip(g["states"] + [c for c in g["comps"] if c is not None], sv):
+                t.copy_(s)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        self.pgraph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.pgraph, stream=side):
+            p.step(nsteps)
+        torch.cuda.synchronize()
+        self.pgraph_steps = nsteps
+
 
 def time_batched(ens, steps, graph_steps=10):
     """Aggregate grid-pt x steps / s of the whole ensemble, CUDA-graph replays."""
@@ -201,6 +266,25 @@ def time_batched(ens, steps, graph_steps=10):
     ms = e0.elapsed_time(e1)
     n = reps * graph_steps
     return {"steps": n, "ms": ms, "value": ens.points() * n / (ms / 1e3)}
+
+
+def time_persistent(ens, steps, graph_steps=10):
+    """Aggregate grid-pt x steps / s with one persistent launch per graph
+    replay of graph_steps steps."""
+    ens.capture_persistent(graph_steps)
+    reps = max(1, steps // graph_steps)
+    ens.pgraph.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        ens.pgraph.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    n = reps * graph_steps
+    st = ens.persistent().status()
+    return {"steps": n, "ms": ms, "value": ens.points() * n / (ms / 1e3), "status": st}
 
 
 def time_sequential(specs, steps, dt=2e-3, model=None, learned_N=64, device=0):
@@ -348,10 +432,12 @@ def main():
     ens = Ensemble(specs, model=model, tune=not a.no_tune)
     setup_s = time.time() - t0
     batched = time_batched(ens, a.steps)
+    persistent = time_persistent(ens, a.steps)
     finite = all(bool(torch.isfinite(torch.view_as_real(s)).all()) for g in ens.groups for s in g["states"])
     seq = time_sequential(specs, a.seq_steps, model=model)
-    res = {"runs": len(specs), "sizes": sorted({s["N"] for s in specs}), "batched": batched, "sequential": seq,
-           "speedup": batched["value"] / seq["value"], "shapes": ens.shapes(), "setup_s": setup_s,
+    res = {"runs": len(specs), "sizes": sorted({s["N"] for s in specs}), "batched": batched,
+           "persistent": persistent, "sequential": seq, "speedup": batched["value"] / seq["value"],
+           "speedup_persistent": persistent["value"] / seq["value"], "shapes": ens.shapes(), "setup_s": setup_s,
            "closures": {g["N"]: g["closure"] for g in ens.groups}, "finite": finite}
     print(json.dumps(res))
     if a.out:

@@ -157,3 +157,97 @@ def test_set_run_between_steps_on_a_side_stream():
     ref = _single(torch, N, np_(st0), nu, 2e-3, "smag", 64, steps=3)
     ref = _single(torch, N, ref, nu, 5e-3, "smag", 64, steps=2)
     assert rel(np_(st), ref) < 1e-12
+
+
+def _persistent_groups(torch, specs, precision, model=None):
+    """Batches (one per grid size) of the given (N, closure, seed, nu) runs."""
+    from pyspectral_b200 import _capi
+    from pyspectral_b200.ensemble import Batch
+    from pyspectral_b200.initial_conditions import isotropic_state
+    cdt = torch.complex128 if precision == 64 else torch.complex64
+    groups = []
+    for N, closure, runs in specs:
+        ctx = _capi.Context(N, N, N, precision=precision)
+        code = {"dns": _capi.DNS, "smag": _capi.SMAG, "learned": _capi.LEARNED}[closure]
+        b = Batch(ctx, code, len(runs))
+        states = []
+        for r, (seed, nu) in enumerate(runs):
+            st = isotropic_state(N, seed, k0=3.0).to(cdt).contiguous()
+            comp = torch.zeros_like(st) if precision == 32 else None
+            m = model if closure == "learned" else None
+            p = _capi.make_params(nu=nu, dt=2e-3, mlp_params=m.params.data_ptr() if m else None,
+                                  mlp_norm=m.norm.data_ptr() if m else None, les_delta=2 * np.pi / N,
+                                  mlp_act=m.act if m else 0, mlp_hidden=m.hidden if m else 0)
+            b.set_run(r, st, comp, p)
+            states.append((st, comp))
+        groups.append((N, closure, b, states))
+    return groups
+
+
+@pytest.mark.parametrize("precision,tol", [(64, 1e-12), (32, 2e-5)])
+def test_persistent_ensemble_matches_batched_steps(precision, tol):
+    """One cooperative launch for every batch (sizes 16, 24 and 32; DNS,
+    Smagorinsky and the learned closure) advances each run exactly like the
+    batched launches (FP64 1e-12; FP32 at the FP32 bar: the two paths may take
+    different transform schedules), and no barrier wait gives up."""
+    torch = _torch()
+    from pyspectral_b200.ensemble import Persistent
+    from pyspectral_b200.learned import MLPModel
+    model = MLPModel.load()
+    spec = [(16, "smag", [(31, 1e-3), (32, 3e-3)]), (24, "dns", [(33, 2e-3)]),
+            (32, "learned" if precision == 32 else "smag", [(34, 1e-3), (35, 2e-3), (36, 4e-3)])]
+    ga = _persistent_groups(torch, spec, precision, model)
+    gb = _persistent_groups(torch, spec, precision, model)
+    for _, _, b, _ in ga:
+        b.step(3)
+    p = Persistent([g[2] for g in gb])
+    p.step(2)
+    p.step(1)
+    torch.cuda.synchronize()
+    assert p.status() == 0
+    for (_, _, _, sa), (_, _, _, sb) in zip(ga, gb):
+        for (a, _), (b_, _) in zip(sa, sb):
+            assert rel(np_(b_), np_(a)) < tol
+
+
+def test_persistent_ensemble_barrier_gives_up_and_returns():
+    """With a poll limit of one, the grid barriers give up instead of waiting:
+    the launch returns (the call completes, the device stays usable), the
+    status word reads 1 once and is then cleared, and a later call with the
+    default limit runs normally."""
+    torch = _torch()
+    from pyspectral_b200.ensemble import Persistent
+    spec = [(16, "smag", [(41, 1e-3), (42, 2e-3)])]
+    g = _persistent_groups(torch, spec, 64)
+    p = Persistent([g[0][2]])
+    p.step(1, poll_limit=1)
+    torch.cuda.synchronize()
+    assert p.status() == 1
+    assert p.status() == 0
+    g2 = _persistent_groups(torch, spec, 64)
+    p2 = Persistent([g2[0][2]])
+    p2.step(1)
+    ref = _persistent_groups(torch, spec, 64)
+    ref[0][2].step(1)
+    torch.cuda.synchronize()
+    assert p2.status() == 0
+    for (a, _), (b_, _) in zip(g2[0][3], ref[0][3]):
+        assert rel(np_(a), np_(b_)) < 1e-12
+
+
+def test_persistent_ensemble_in_a_graph():
+    """The uneven ensemble's persistent launch captured in a CUDA graph and
+    replayed advances it like the batched graph does."""
+    torch = _torch()
+    from pyspectral_b200.ensemble import Ensemble, ensemble_specs, time_batched, time_persistent
+    from pyspectral_b200.learned import MLPModel
+    specs = ensemble_specs(sizes=(16, 24, 32), per_size=2)
+    model = MLPModel.load()
+    e1 = Ensemble(specs, model=model, learned_N=32, tune=False)
+    e2 = Ensemble(specs, model=model, learned_N=32, tune=False)
+    r1 = time_batched(e1, 4, graph_steps=2)
+    r2 = time_persistent(e2, 4, graph_steps=2)
+    assert r2["status"] == 0 and r1["steps"] == r2["steps"] == 4
+    for g1, g2 in zip(e1.groups, e2.groups):
+        for a, b_ in zip(g1["states"], g2["states"]):
+            assert rel(np_(b_), np_(a)) < 2e-5
