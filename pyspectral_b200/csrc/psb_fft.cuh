@@ -316,8 +316,8 @@ __device__ Cx<T>* block_fft(Cx<T>* a, Cx<T>* b, const FFTPlan& p, const Cx<T>* _
 // The Stockham passes with L, the radix and the sub-transform length Ns known
 // to the compiler, over `nlines` lines of length L held at buf[line*ls + j]
 // (the z-pass layout: each line contiguous, consecutive lines `ls` elements
-// apart; the z pass uses ls = L + 1, odd, so that the same position of
-// consecutive lines falls in different shared-memory banks).
+// apart; the z pass pads ls to an odd stride, 7 modulo 16, so that the same
+// position of consecutive lines falls in different shared-memory banks).
 //
 // LINES_FAST (used when nlines >= 8): consecutive threads take consecutive
 // lines at the same j.  A warp's loads j + r*L/R, its stores (j-k)R + k + r*Ns

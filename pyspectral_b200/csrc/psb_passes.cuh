@@ -394,10 +394,15 @@ struct pre_ypass<T, P, decltype((void)sizeof(typename P::YPass), void())> {
   static constexpr int groups = type::GROUPS, in_fields = type::IN_FIELDS, out_fields = type::OUT_FIELDS;
 };
 
-// Line stride of the z-pass buffers: one element more than the (even)
-// transform length, so consecutive lines start in different shared-memory
-// banks (the compiled transforms walk the lines fast, psb_fft.cuh).
-__host__ __device__ constexpr int zline(int M) { return M + 1; }
+// Line stride of the z-pass buffers: the (even) transform length padded to
+// 7 modulo 16 elements.  The transforms walk the lines fast (psb_fft.cuh), so
+// a half-warp touches one position of 16 consecutive lines -- distinct banks
+// for any odd stride -- or, with 24 or 12 lines, the tail lines at j and the
+// first lines at j + 1: with a stride of 7 (mod 16) those two sets share at
+// most one or two banks (a stride of 1 would share seven).  At P = 4 the
+// field stride P*LS = 28 (mod 32) words also keeps the MLP's feature gathers
+// (8 rows x 4 features per warp instruction) on 32 distinct banks.
+__host__ __device__ constexpr int zline(int M) { return M + (((7 - M) % 16) + 16) % 16; }
 
 // Shared memory of one z-pass CTA: twiddles, two buffers of
 // nl = ceil(fmax*P/2) packed lines of length M at stride zline(M), and the

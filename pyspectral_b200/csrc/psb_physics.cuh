@@ -740,7 +740,7 @@ struct PhysLearned {
   __device__ __forceinline__ void block_act(const Cx<T>* R, Cx<T>* W, int P, int M, int LS, T fac,
                                             unsigned char* extra) const {
     const MlpFwdSmem<H>& s = *reinterpret_cast<const MlpFwdSmem<H>*>(extra);
-    if ((M & 15) == 0 && (P & 1) == 0) {
+    if ((M & 7) == 0 && (P & 1) == 0) {
       block_tiles(reinterpret_cast<const T*>(R), reinterpret_cast<T*>(W), P, M, LS, fac, s);
       return;
     }
@@ -787,10 +787,14 @@ struct PhysLearned {
       }
     }
   }
-  // The same computation when every tile is 16 consecutive z of one pencil
-  // (M % 16 == 0) and packed lines pair pencils of one field (P even): real
-  // line (f, p) is half p&1 of packed line f*P/2 + p/2 (lines LS apart), so
-  // field f of pencil p at z is T element f*P*LS + 2((p/2) LS + z) + (p&1).  Each lane keeps the
+  // The same computation when packed lines pair pencils of one field (P even)
+  // and M % 8 == 0: real line (f, p) is half p&1 of packed line f*P/2 + p/2
+  // (lines LS apart), so field f of pencil p at z is T element
+  // f*P*LS + 2((p/2) LS + z) + (p&1).  A tile is 16 consecutive T elements of
+  // a packed line -- 8 consecutive z of a pencil pair, both halves -- so the
+  // 8 rows a lane group reads are consecutive words and, with the field
+  // stride P*LS = 28 (mod 32) words at P = 4 (LS = 7 mod 16), the 32 lanes of a
+  // feature gather (8 rows x 4 features) hit 32 different banks.  Each lane keeps the
   // offsets, normalisation and output coefficients of its fragment slots in
   // registers; per tile it computes one base index per row.
   __device__ __forceinline__ void block_tiles(const T* __restrict__ R, T* __restrict__ W, int P, int M, int LS,
@@ -829,17 +833,17 @@ struct PhysLearned {
       ym[e2] = c < kMlpOut ? s.ymean[c] : 0.f;
     }
     const bool out_ok = t < 3;
-    const int tpp = M >> 4, ntile = P * tpp;
+    const int tpp = M >> 3, ntile = (P >> 1) * tpp;
     for (int tile = warp; tile < ntile; tile += nw) {
-      const int p = tile / tpp;
-      const int z0 = (tile - p * tpp) << 4;
-      const int b0 = 2 * ((p >> 1) * LS + z0 + g) + (p & 1);  // row g; row g + 8 is b0 + 16
+      const int pp = tile / tpp;  // pencil pair
+      const int z0 = (tile - pp * tpp) << 3;
+      const int b0 = 2 * (pp * LS + z0) + g;  // row g; row g + 8 is b0 + 8
       float v[8];
 #pragma unroll
       for (int hr = 0; hr < 2; ++hr)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-          const float x = (float)(R[b0 + 16 * hr + foff[q]] * fs);
+          const float x = (float)(R[b0 + 8 * hr + foff[q]] * fs);
           v[hr * 4 + q] = fg[q] ? (x - fm[q]) * fi[q] : fc[q];
         }
       uint32_t xa[4];
@@ -853,7 +857,7 @@ struct PhysLearned {
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           const int e2 = e & 1;
-          const int b = b0 + 16 * (e >> 1);
+          const int b = b0 + 8 * (e >> 1);
           const T tau = (T)(y[e] * ys[e2] + ym[e2]);
           W[b + ooff[e2]] = (fac * R[b + ioff[e2]]) * (fac * R[b + joff[e2]]) + tau * is2;
         }
