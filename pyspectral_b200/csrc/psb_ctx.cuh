@@ -319,6 +319,29 @@ int launch_axis(psb_ctx* c, psb::AxisArgs<T> a, Pre pre, const char* what, const
     launch_pdl(k, grid, 256, smem, c->stream, a, pre);
     return launch_ok(c, what);
   };
+  // A compiled two-pass schedule on a tunable pass whose Pre forms each field
+  // on load: registers straight from and to global memory around a single
+  // shared-memory exchange (psb::axis_rr_body).
+  if constexpr (TUNABLE && psb::pre_fieldwise<Pre>::value) {
+    const size_t rsmem = (size_t)(L + (size_t)L * Pre::F_DST * a.col_tile) * esz;
+    auto gor = [&](auto k) {
+      set_smem(k, rsmem);
+      LaunchScope scope(c, what, bytes);
+      launch_pdl(k, grid, 256, rsmem, c->stream, a, pre);
+      return launch_ok(c, what);
+    };
+    switch (psb::fixed_plan_id(a.plan)) {
+#define PSB_FIXED_CASE(ID, ...)                                                                       \
+  case ID:                                                                                            \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value && psb::FixedPlan<ID>::Radices::NP == 2) \
+      return gor(psb::axis_pass_rr_kernel<T, INV, Pre, ID>);                                          \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
+    }
+  }
   // Rows read unchanged (a plain copy, every row at its own position): the
   // tile is staged by bulk tensor copies when the view meets TMA's rules.
   if constexpr (std::is_same<Pre, psb::PreCopy<T>>::value) {
@@ -443,6 +466,20 @@ int launch_epi(psb_ctx* c, psb::XEpiArgs<T> e, Epi epi, const char* what, const 
     launch_pdl(k, dim3((unsigned)(e.main_blocks + extra)), 256, smem, c->stream, e, epi);
     return launch_ok(c, what);
   };
+  // a compiled two-pass schedule: the first pass loads straight from global memory
+  if constexpr (TUNABLE) {
+    switch (psb::fixed_plan_id(e.plan)) {
+#define PSB_FIXED_CASE(ID, ...)                                                                       \
+  case ID:                                                                                            \
+    if constexpr (psb::fixed_plan_compiled<T, ID>::value && psb::FixedPlan<ID>::Radices::NP == 2) \
+      return go(psb::xfwd_epi_rr_kernel<T, Epi, ID>);                                                 \
+    break;
+      PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+      default:
+        break;
+    }
+  }
   // the input tile (ct columns x F fields x L rows) staged by bulk tensor copies
   {
     const int nbox = tma_boxes(L);

@@ -443,10 +443,15 @@ constexpr int kFixedPlans = 13;
 
 template <int ID>
 struct FixedPlan;
+template <int R1, int R2 = 0, int R3 = 0>
+struct RadixList {
+  static constexpr int NP = R3 ? 3 : (R2 ? 2 : 1), A = R1, B = R2;
+};
 #define PSB_FIXED_PLAN_DEF(ID, LEN, ...)                                                       \
   template <>                                                                                   \
   struct FixedPlan<ID> {                                                                        \
     static constexpr int L = LEN;                                                               \
+    using Radices = RadixList<__VA_ARGS__>; /* NP passes; A, B the first two radices */         \
     template <typename T, bool INV>                                                             \
     static __device__ __forceinline__ Cx<T>* run(Cx<T>* a, Cx<T>* b, const Cx<T>* tw, int n,    \
                                                  int ls) {                                      \

@@ -139,8 +139,30 @@ struct AxisArgs {
 template <typename T>
 struct PreCopy {
   static constexpr int F_SRC = 1, F_DST = 1;
+  static constexpr bool FIELDWISE = true;
   __device__ void operator()(int, int, int, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const { d[0] = s[0]; }
+  __device__ __forceinline__ Cx<T> field(int, int i, int, int col, const AxisArgs<T>& a, const Cx<T>* in) const {
+    return in[i * a.in_rstride + col];
+  }
 };
+
+// Pre functors that can form any one destination field at a row straight
+// from the inputs (`field(g, i, o, col, a, in)`), so a pass can load its
+// first transform pass's elements from global memory into registers.
+template <class P, class = void>
+struct pre_fieldwise {
+  static constexpr bool value = false;
+};
+template <class P>
+struct pre_fieldwise<P, decltype((void)P::FIELDWISE, void())> {
+  static constexpr bool value = P::FIELDWISE;
+};
+
+// Row of a row map's position p (the inverse of RowMap), or -1.
+__device__ __forceinline__ int row_of(const RowMap& m, int p, int rows) {
+  const int i = p < m.lo ? p : (p >= m.hi + m.shift ? p - m.shift : -1);
+  return i < rows ? i : -1;
+}
 
 // One CTA of an axis pass: column tile bx, outer index by.
 // smem = tw[L] + 2 * L*lines
@@ -326,6 +348,85 @@ __global__ void __launch_bounds__(256) axis_pass_tma_kernel(AxisArgs<T> a, const
     __syncthreads();
   }
   axis_transform_store<T, INV, 1, false, FP>(a, bufA, bufB, tw, o, c0);
+}
+
+// ---------------------------------------------------------------------------
+// Two-pass axis transform with global memory on both sides.  For a compiled
+// schedule of exactly two radices (L = R1 R2) the first Stockham pass loads
+// its R1 elements of a line straight from the input rows (the Pre functor
+// forms the line's field on load: `field`), and the second stores its R2
+// results straight to the output rows; the only shared-memory traffic is the
+// exchange between the passes (one store and one load per element instead of
+// the staged tile's six) and the only barrier is the one between them.
+// Items walk the lines fast (line = field * ct + column), so consecutive
+// threads touch consecutive columns in global memory and consecutive lines
+// in the exchange buffer.  smem = L twiddles + L * F * ct elements.
+template <typename T, bool INV, class Pre, int FP>
+__device__ __forceinline__ void axis_rr_body(const AxisArgs<T>& a, const Pre& pre, int bx, int by) {
+  using FPl = FixedPlan<FP>;
+  constexpr int L = FPl::L, R1 = FPl::Radices::A, R2 = FPl::Radices::B;
+  static_assert(FPl::Radices::NP == 2 && R1 * R2 == L, "two-pass schedules only");
+  constexpr int F = Pre::F_DST, NB1 = L / R1, NB2 = L / R2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int ct = a.col_tile, lines = F * ct;
+  Cx<T>* X = tw + L;
+  const int o = by, c0 = bx * ct;
+  const Cx<T> zero = mk<T>(0, 0);
+  pdl_trigger();
+  stage_twiddles(tw, a.tw, a.plan);
+  pdl_wait();
+  const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
+  for (Walk2 w(lines); w.s < NB1; w.next()) {
+    const int line = w.f, j1 = w.s;
+    const int g = line / ct, col = c0 + (line - g * ct);
+    Cx<T> v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int i = row_of(a.in_map, j1 + r * NB1, a.in_rows);
+      v[r] = (i >= 0 && col < a.ncols) ? pre.field(g, i, o, col, a, inb) : zero;
+    }
+    small_dft<T, R1, INV>(v);
+#pragma unroll
+    for (int r = 0; r < R1; ++r) X[(size_t)(j1 * R1 + r) * lines + line] = v[r];
+  }
+  __syncthreads();
+  Cx<T>* outb = a.out + (long long)o * a.out_ostride;
+  for (Walk2 w(lines); w.s < NB2; w.next()) {
+    const int line = w.f, j2 = w.s;
+    const int g = line / ct, col = c0 + (line - g * ct);
+    const int k = j2 % R1;
+    Cx<T> v[R2];
+#pragma unroll
+    for (int r = 0; r < R2; ++r) v[r] = X[(size_t)(j2 + r * NB2) * lines + line];
+    // twiddles W_L^{r k} (sub-transform length R1: the table's stride L / (R1 R2) is 1)
+#pragma unroll
+    for (int r = 1; r < R2; ++r) {
+      Cx<T> t = tw[r * k];
+      if (INV) t.y = -t.y;
+      v[r] = cmul(v[r], t);
+    }
+    small_dft<T, R2, INV>(v);
+    if (col < a.ncols) {
+#pragma unroll
+      for (int r = 0; r < R2; ++r) {
+        const int i = row_of(a.out_map, (j2 - k) * R2 + k + r * R1, a.out_rows);
+        if (i >= 0) outb[g * a.out_fstride + i * a.out_rstride + col] = a.scale * v[r];
+      }
+    }
+  }
+  // output rows the map leaves without a position are zero
+  const int zlo = a.out_map.lo, zhi = min(a.out_map.hi, a.out_rows);
+  for (int t = threadIdx.x; zlo < zhi && t < (zhi - zlo) * lines; t += blockDim.x) {
+    const int line = t % lines, i = zlo + t / lines;
+    const int g = line / ct, col = c0 + (line - g * ct);
+    if (col < a.ncols) outb[g * a.out_fstride + i * a.out_rstride + col] = zero;
+  }
+}
+
+template <typename T, bool INV, class Pre, int FP>
+__global__ void __launch_bounds__(256) axis_pass_rr_kernel(AxisArgs<T> a, Pre pre) {
+  axis_rr_body<T, INV, Pre, FP>(a, pre, blockIdx.x, blockIdx.y);
 }
 
 // grid = (ceil(ncols/col_tile), nouter)
@@ -842,6 +943,72 @@ __global__ void __launch_bounds__(256) xfwd_epi_tma_kernel(XEpiArgs<T> a, Epi ep
     __syncthreads();
   }
   xfwd_transform_epi<T, Epi, false, FP>(a, epi, bufA, bufB, tw, o, c0);
+}
+
+// The x-forward epilogue pass with a two-pass compiled schedule: the first
+// pass loads its elements straight from the input rows, the second writes the
+// transformed tile to shared memory for the epilogue (which needs every field
+// of a point in one thread).  smem = L twiddles + 2 L F ct elements.
+template <typename T, class Epi, int FP>
+__global__ void __launch_bounds__(256) xfwd_epi_rr_kernel(XEpiArgs<T> a, Epi epi) {
+  using FPl = FixedPlan<FP>;
+  constexpr int L = FPl::L, R1 = FPl::Radices::A, R2 = FPl::Radices::B;
+  static_assert(FPl::Radices::NP == 2 && R1 * R2 == L, "two-pass schedules only");
+  constexpr int F = Epi::F_IN, NB1 = L / R1, NB2 = L / R2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  pdl_trigger();
+  if ((int)blockIdx.x >= a.main_blocks) {
+    pdl_wait();
+    xfwd_epi_extra<T, Epi>(a, epi, blockIdx.x, gridDim.x);
+    return;
+  }
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int ct = a.col_tile, lines = F * ct;
+  Cx<T>* X = tw + L;
+  Cx<T>* Y = X + (size_t)L * lines;
+  const int ntile = (a.kz + ct - 1) / ct;
+  const int o = blockIdx.x / ntile;
+  const int c0 = (blockIdx.x % ntile) * ct;
+  const Cx<T> zero = mk<T>(0, 0);
+  stage_twiddles(tw, a.tw, a.plan);
+  pdl_wait();
+  const Cx<T>* inb = a.in + (long long)o * a.in_ostride;
+  for (Walk2 w(lines); w.s < NB1; w.next()) {
+    const int line = w.f, j1 = w.s;
+    const int f = line / ct, col = c0 + (line - f * ct);
+    Cx<T> v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r)
+      v[r] = col < a.kz ? inb[f * a.in_fstride + (j1 + r * NB1) * a.in_rstride + col] : zero;
+    small_dft<T, R1, false>(v);
+#pragma unroll
+    for (int r = 0; r < R1; ++r) X[(size_t)(j1 * R1 + r) * lines + line] = v[r];
+  }
+  __syncthreads();
+  for (Walk2 w(lines); w.s < NB2; w.next()) {
+    const int line = w.f, j2 = w.s;
+    const int k = j2 % R1;
+    Cx<T> v[R2];
+#pragma unroll
+    for (int r = 0; r < R2; ++r) v[r] = X[(size_t)(j2 + r * NB2) * lines + line];
+#pragma unroll
+    for (int r = 1; r < R2; ++r) v[r] = cmul(v[r], tw[r * k]);
+    small_dft<T, R2, false>(v);
+#pragma unroll
+    for (int r = 0; r < R2; ++r) Y[(size_t)((j2 - k) * R2 + k + r * R1) * lines + line] = v[r];
+  }
+  __syncthreads();
+  const int nt = blockDim.x;
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = nt / ct;
+  const int col = c0 + c;
+  if (col >= a.kz || threadIdx.x >= dr * ct) return;
+  Cx<T> P[F];
+  for (int i1 = r0; i1 < a.n1; i1 += dr) {
+    const int j = a.out_map(i1);
+#pragma unroll
+    for (int f = 0; f < F; ++f) P[f] = j >= 0 ? Y[(size_t)j * lines + f * ct + c] : zero;
+    epi(i1, o, col, P);
+  }
 }
 
 // grid = main_blocks + extra

@@ -87,9 +87,14 @@ struct StepIO {
 template <typename T, int F>
 struct PreCopyN {
   static constexpr int F_SRC = F, F_DST = F;
+  static constexpr bool FIELDWISE = true;
   __device__ void operator()(int, int, int, const AxisArgs<T>&, const Cx<T>* s, Cx<T>* d) const {
 #pragma unroll
     for (int f = 0; f < F; ++f) d[f] = s[f];
+  }
+  // field g of row i, column col, read from the row's inputs (in: the outer index's base)
+  __device__ __forceinline__ Cx<T> field(int g, int i, int, int col, const AxisArgs<T>& a, const Cx<T>* in) const {
+    return in[g * a.in_fstride + i * a.in_rstride + col];
   }
 };
 
@@ -98,6 +103,15 @@ struct PreCopyN {
 template <typename T>
 struct PreStrain {
   static constexpr int F_SRC = 3, F_DST = 9;
+  static constexpr bool FIELDWISE = true;
+  __device__ __forceinline__ Cx<T> field(int g, int i, int o, int col, const AxisArgs<T>& a, const Cx<T>* in) const {
+    auto src = [&](int f) { return in[f * a.in_fstride + i * a.in_rstride + col]; };
+    const T k[3] = {(T)a.k_row[i], (T)a.k_outer[o], (T)a.k_col[col]};
+    if (g < 3) return src(g);
+    if (g < 6) return pik(k[g - 3], src(g - 3));
+    const int p = g == 6 ? 0 : (g == 7 ? 0 : 1), q = g == 6 ? 1 : 2;  // S_pq
+    return (T)0.5 * (pik(k[q], src(p)) + pik(k[p], src(q)));
+  }
   __device__ void operator()(int i, int o, int c, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
     const T k1 = (T)a.k_row[i], k2 = (T)a.k_outer[o], k3 = (T)a.k_col[c];
     d[0] = s[0];
@@ -672,6 +686,11 @@ struct PreGrad {
 template <typename T>
 struct PreYGrad {
   static constexpr int F_SRC = 2, F_DST = 3, GROUPS = 3, IN_FIELDS = 3, OUT_FIELDS = 3;
+  static constexpr bool FIELDWISE = true;
+  __device__ __forceinline__ Cx<T> field(int g, int i, int, int col, const AxisArgs<T>& a, const Cx<T>* in) const {
+    const Cx<T> v = in[(g == 1 ? a.in_fstride : 0) + i * a.in_rstride + col];
+    return g == 2 ? pik((T)a.k_row[i], v) : v;
+  }
   __device__ void operator()(int i, int, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
     d[0] = s[0];
     d[1] = s[1];
@@ -687,6 +706,11 @@ struct PreYGrad {
 template <typename T>
 struct PreGradXY {
   static constexpr int F_SRC = 3, F_DST = 6, F_B = 9, Z_DERIVED = 3;
+  static constexpr bool FIELDWISE = true;
+  __device__ __forceinline__ Cx<T> field(int g, int i, int, int col, const AxisArgs<T>& a, const Cx<T>* in) const {
+    const Cx<T> v = in[(g < 3 ? g : g - 3) * a.in_fstride + i * a.in_rstride + col];
+    return g < 3 ? v : pik((T)a.k_row[i], v);
+  }
   using YPass = PreYGrad<T>;
   __device__ void operator()(int i, int, int, const AxisArgs<T>& a, const Cx<T>* s, Cx<T>* d) const {
     const T k1 = (T)a.k_row[i];
