@@ -130,11 +130,19 @@ def restart(path, grid, turb_model, dt, nu, precision=64, **kw):
     return main
 
 
-def run(main, grid, utilities, et, save_freq, directory="3DSolution", turb_model=None, iteration=0, log=None):
+def run(main, grid, utilities, et, save_freq, directory="3DSolution", turb_model=None, iteration=0, log=None,
+        reference_t0=False):
     """The reference's main loop (src/PySpec_3d.py:107-148): grid and run
     information written first, then ``while t <= et``: set main.t, one RK4
     step, t += dt, the savehook every save_freq iterations, the statistics
-    appended; ``stats.npz`` at the end.  Returns the statistics."""
+    appended; ``stats.npz`` at the end.  Returns the statistics.
+
+    The first entry of the time history is the run's starting time, so that a
+    restarted run's ``Dissipation[0]`` is the energy change over its first
+    step.  The reference always writes 0 there (``t_hist[0] = 0``,
+    src/PySpec_3d.py:117-118); for a run from t = 0 the two agree, and
+    ``reference_t0=True`` writes 0 after a restart too, as the reference's
+    loop would."""
     from .RHSfunctions import advanceQ_RK4
     save_grid(grid, directory)
     save_runinfo(directory, main.turb_model if turb_model is None else turb_model, main.dt, save_freq, main.nu)
@@ -142,7 +150,7 @@ def run(main, grid, utilities, et, save_freq, directory="3DSolution", turb_model
     energy = [utilities.computeEnergy(main, grid)]
     enstrophy = [utilities.computeEnstrophy(main, grid)]
     energy_res = [utilities.computeEnergy_resolved(main, grid)]
-    t_hist = [t]
+    t_hist = [0.0 if reference_t0 else t]
     t0 = time.time()
     while t <= et:
         main.t = t

@@ -67,3 +67,36 @@ def test_stats_dissipation_is_the_reference_difference(tmp_path):
     assert set(s.files) == {"Energy", "Dissipation", "Energy_resolved", "Dissipation_resolved", "t", "Enstrophy"}
     assert np.allclose(s["Dissipation"], 1.0 / (t[1:] - t[:-1]) * (E[1:] - E[:-1]), rtol=0, atol=0)
     assert np.allclose(s["Dissipation_resolved"], 1.0 / (t[1:] - t[:-1]) * (Er[1:] - Er[:-1]), rtol=0, atol=0)
+
+
+def _fake_run(tmp_path, monkeypatch, reference_t0):
+    """checkpoint.run with the step replaced by a host stand-in (energy decays
+    by 10% a step), started at t = 0.25 as after a restart."""
+    from pyspectral_b200 import RHSfunctions
+
+    def step(main, grid, myFFT, utilities):
+        main.e *= 0.9
+
+    monkeypatch.setattr(RHSfunctions, "advanceQ_RK4", step)
+    util = types.SimpleNamespace(
+        computeEnergy=lambda m, g: m.e, computeEnstrophy=lambda m, g: 2 * m.e,
+        computeEnergy_resolved=lambda m, g: 0.5 * m.e,
+        computeAllStats=lambda m, g: (2 * m.e, m.e, 0.0, 0.0, 0.0, 0.0))
+    main = _main(8, 0)
+    main.e, main.dt, main.nu = 1.0, 0.05, 0.01
+    return ck.run(main, gridclass.periodic(8), util, 0.39, 100, str(tmp_path / "3DSolution"),
+                  turb_model=0, reference_t0=reference_t0)
+
+
+def test_run_after_restart_starts_its_time_history_at_its_own_time(tmp_path, monkeypatch):
+    s = _fake_run(tmp_path, monkeypatch, False)
+    assert np.allclose(s["t"], [0.25, 0.30, 0.35, 0.40])
+    assert np.allclose(s["Dissipation"][0], (0.9 - 1.0) / 0.05)
+
+
+def test_run_reference_t0_writes_zero_first_as_the_reference(tmp_path, monkeypatch):
+    s = _fake_run(tmp_path, monkeypatch, True)
+    assert s["t"][0] == 0.0 and np.allclose(s["t"][1:], [0.30, 0.35, 0.40])
+    assert np.allclose(s["Dissipation"][0], (0.9 - 1.0) / 0.30)
+    on_disk = np.load(str(tmp_path / "3DSolution" / "stats.npz"))
+    assert on_disk["t"][0] == 0.0
