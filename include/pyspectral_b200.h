@@ -135,6 +135,12 @@ int psb_ctx_set_stream(psb_ctx* ctx, void* stream);
  * bulk tensor copies (1, the default) or with per-element loads (0).  Same
  * results either way; no counterpart in the reference (a launch choice). */
 int psb_ctx_set_tma(psb_ctx* ctx, int enable);
+/* Run the z pass of the 3/2-padded Navier-Stokes closures (DNS products,
+ * Smagorinsky, learned; FP32) with its spectra loaded into and stored from
+ * registers around the transforms when its schedule is a compiled two-pass
+ * one ending in radix 16 (1, the default), or through shared memory (0).
+ * Same results either way; no counterpart in the reference (a launch choice). */
+int psb_ctx_set_zrr(psb_ctx* ctx, int enable);
 /* Device status of the context's kernels since the last call, then cleared:
  * 0; 1 when a bounded wait inside a kernel gave up; 2 when a kernel found a
  * bulk-copy destination off its alignment and issued nothing.  In both cases

@@ -32,7 +32,7 @@ EXPORTS = (
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
     "psb_batch_create", "psb_batch_set_run", "psb_batch_autotune", "psb_batch_step_rk4", "psb_batch_shape",
     "psb_batch_destroy", "psb_autotune", "psb_tuned_shape", "psb_autotune_clear", "psb_set_tuned_shape",
-    "psb_ctx_set_tma", "psb_device_status", "psb_ensemble_create", "psb_ensemble_step_rk4", "psb_ensemble_status",
+    "psb_ctx_set_tma", "psb_ctx_set_zrr", "psb_device_status", "psb_ensemble_create", "psb_ensemble_step_rk4", "psb_ensemble_status",
     "psb_ensemble_destroy",
 )
 
@@ -99,6 +99,7 @@ def load(path: str = LIB_PATH):
         "psb_autotune_clear": ([vp, i], i),
         "psb_set_tuned_shape": ([vp, i, i, i, ip, i], i),
         "psb_ctx_set_tma": ([vp, i], i),
+        "psb_ctx_set_zrr": ([vp, i], i),
         "psb_device_status": ([vp, ip], i),
     }
     for name, (args, res) in sig.items():
@@ -320,6 +321,11 @@ class Context:
     def set_tma(self, on: bool):
         """Stage eligible pass inputs with bulk tensor copies (default) or plain loads."""
         self.check(self.lib.psb_ctx_set_tma(self.h, 1 if on else 0), "psb_ctx_set_tma")
+
+    def set_zrr(self, on: bool):
+        """Register-direct z pass for two-pass (R1, 16) schedules (default) or the
+        shared-memory z pass."""
+        self.check(self.lib.psb_ctx_set_zrr(self.h, 1 if on else 0), "psb_ctx_set_zrr")
 
     def device_status(self):
         """0, or 1 if a bounded wait inside one of this context's kernels gave up

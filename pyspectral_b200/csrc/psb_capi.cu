@@ -750,6 +750,12 @@ int psb_ctx_set_tma(psb_ctx* c, int enable) {
   return PSB_OK;
 }
 
+int psb_ctx_set_zrr(psb_ctx* c, int enable) {
+  PSB_TRY(check_ctx(c));
+  c->use_zrr = enable ? 1 : 0;
+  return PSB_OK;
+}
+
 int psb_device_status(psb_ctx* c, int* status) {
   PSB_TRY(check_ctx(c));
   if (!status) return fail(c, PSB_ERR_ARG, "psb_device_status: null argument");

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <type_traits>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -63,6 +64,7 @@ struct psb_ctx {
   unsigned long long launches = 0;
   int timing = 0;
   int use_tma = 1;          // stage eligible pass inputs with bulk tensor copies
+  int use_zrr = 1;          // register-direct z-pass for two-pass (R1, 16) schedules
   int* dstatus = nullptr;   // device status word (a bounded wait gave up), owned
   struct Rec {
     std::string name;
@@ -175,12 +177,15 @@ inline int count_mapped(const psb::RowMap& m, int rows) {
 constexpr size_t kSmemBudget = 100 * 1024;
 
 // Raise a kernel's dynamic shared-memory limit once per (kernel, device); a
-// fixed table, so that launching never allocates host memory either.
+// fixed table, so that launching never allocates host memory either.  The
+// table is process-wide and shared by every context, so it is guarded by a
+// mutex: host threads that launch on different contexts may meet here.
 struct SmemCache {
   const void* fn[512];
   int dev[512];
   size_t bytes[512];
   int n = 0;
+  std::mutex mu;
 };
 inline SmemCache& smem_cache() {
   static SmemCache c;
@@ -193,6 +198,7 @@ inline void set_smem(K kernel, size_t smem) {
   cudaGetDevice(&dev);
   SmemCache& c = smem_cache();
   const void* f = reinterpret_cast<const void*>(kernel);
+  std::lock_guard<std::mutex> lk(c.mu);
   for (int i = 0; i < c.n; ++i)
     if (c.fn[i] == f && c.dev[i] == dev) {
       if (c.bytes[i] >= smem) return;
@@ -423,6 +429,24 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
     launch_pdl(k, dim3((unsigned)g), 256, smem, c->stream, z, phys);
     return launch_ok(c, what);
   };
+  // A compiled two-pass schedule (R1, 16) with pencils paired per packed line
+  // (P even): the register-direct z-pass, whose transforms read the packed
+  // spectra from and write them to global memory (psb::zpass_rr_tile).
+  if constexpr (psb::phys_fixed_fft<Phys>::value && sizeof(T) == 4) {
+    if ((P & 1) == 0 && c->use_zrr) {
+      switch (psb::fixed_plan_id(z.plan)) {
+#define PSB_FIXED_CASE(ID, ...)                                                                   \
+  case ID:                                                                                        \
+    if constexpr (psb::zrr_plan<ID>::value && psb::zrr_plan<ID>::R2 == 16)                      \
+      return go(psb::zpass_rr_kernel<T, Phys, ID>);                                               \
+    break;
+        PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+        default:
+          break;
+      }
+    }
+  }
   if constexpr (psb::phys_fixed_fft<Phys>::value) {
     switch (psb::fixed_plan_id(z.plan)) {
 #define PSB_FIXED_CASE(ID, ...) \

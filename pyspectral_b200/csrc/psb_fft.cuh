@@ -471,6 +471,25 @@ template <int... R>
 constexpr int count_radices() {
   return (int)sizeof...(R);
 }
+// The compiled-in schedules as a compile-time table, and the id of the
+// two-pass schedule that runs the radices of `id` in the opposite order (0 if
+// `id` is not a two-pass schedule or its reverse is not compiled in).
+struct FixedDesc {
+  int id, L, n, r[3];
+};
+#define PSB_FIXED_PLAN_CDESC(ID, LEN, ...) FixedDesc{ID, LEN, count_radices<__VA_ARGS__>(), {__VA_ARGS__}},
+constexpr FixedDesc kFixedDescs[] = {PSB_FIXED_PLANS(PSB_FIXED_PLAN_CDESC)};
+#undef PSB_FIXED_PLAN_CDESC
+constexpr int fixed_plan_reversed(int id) {
+  for (const FixedDesc& d : kFixedDescs) {
+    if (d.id != id) continue;
+    if (d.n != 2) return 0;
+    for (const FixedDesc& e : kFixedDescs)
+      if (e.L == d.L && e.n == 2 && e.r[0] == d.r[1] && e.r[1] == d.r[0]) return e.id;
+  }
+  return 0;
+}
+
 // Id of the compiled-in schedule equal to p (0 if none).
 __host__ inline int fixed_plan_id(const FFTPlan& p) {
   struct D {

@@ -537,6 +537,52 @@ __device__ __forceinline__ void zpass_setup(const ZArgs<T>& a, const Phys& phys)
   }
 }
 
+// The physics of a z-pass tile: physical fields R (F_IN real lines of P
+// pencils, packed two per complex line at stride LS) -> the F_OUT results W in
+// the same packing.  Block physics (the tensor-core MLP) runs over the CTA's
+// points; pointwise physics calls Phys per point.  The last CTA may hold
+// fewer than P pencils: its missing pencils produce zeros.
+template <typename T, class Phys>
+__device__ __forceinline__ void zpass_physics(const ZArgs<T>& a, const Phys& phys, const Cx<T>* R, Cx<T>* W, int P,
+                                              int M, int LS, long long p0, unsigned char* extra) {
+  constexpr int FI = Phys::F_IN, FO = Phys::F_OUT;
+  const int nout = (FO * P + 1) / 2;
+  if constexpr (phys_is_block<Phys>::value) {
+    // block-cooperative physics (a tensor-core MLP over the CTA's points)
+    phys.block(R, W, P, M, LS, a.fac, p0, a.npencils, extra);
+    if ((FO * P) & 1) {
+      for (int z = threadIdx.x; z < M; z += blockDim.x) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
+    }
+  } else {
+    // pointwise physics; the last CTA may hold fewer than P pencils
+    for (Walk2 w(M); w.s < P; w.next()) {
+      const int z = w.f, p = w.s;
+      T vin[FI > 0 ? FI : 1], vout[FO > 0 ? FO : 1];
+#pragma unroll
+      for (int f = 0; f < FI; ++f) {
+        const int r = f * P + p;
+        const Cx<T> v = R[(size_t)(r >> 1) * LS + z];
+        vin[f] = a.fac * ((r & 1) ? v.y : v.x);
+      }
+      if (p0 + p < a.npencils) {
+        phys(p0 + p, z, vin, vout);
+      } else {
+#pragma unroll
+        for (int g = 0; g < FO; ++g) vout[g] = (T)0;
+      }
+#pragma unroll
+      for (int g = 0; g < FO; ++g) {
+        const int r = g * P + p;
+        T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * LS + z);
+        w[r & 1] = vout[g];
+      }
+      if ((FO * P) & 1) {  // odd count: the last packed line has no partner
+        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
+      }
+    }
+  }
+}
+
 // One tile of the z-pass: pencils bx*ppc ..; smem = zpass_smem_bytes, staged
 // by zpass_setup.  Ends with the results stored; the caller synchronises
 // before the CTA's next tile reuses the buffers.
@@ -658,40 +704,7 @@ __device__ __forceinline__ void zpass_tile(const ZArgs<T>& a, const Phys& phys, 
   }
   Cx<T>* W = (R == X) ? Y : X;
   const int nout = (FO * P + 1) / 2;
-  if constexpr (phys_is_block<Phys>::value) {
-    // block-cooperative physics (a tensor-core MLP over the CTA's points)
-    phys.block(R, W, P, M, LS, a.fac, p0, a.npencils, extra);
-    if ((FO * P) & 1) {
-      for (int z = threadIdx.x; z < M; z += blockDim.x) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
-    }
-  } else {
-    // pointwise physics; the last CTA may hold fewer than P pencils
-    for (Walk2 w(M); w.s < P; w.next()) {
-      const int z = w.f, p = w.s;
-      T vin[FI > 0 ? FI : 1], vout[FO > 0 ? FO : 1];
-#pragma unroll
-      for (int f = 0; f < FI; ++f) {
-        const int r = f * P + p;
-        const Cx<T> v = R[(size_t)(r >> 1) * LS + z];
-        vin[f] = a.fac * ((r & 1) ? v.y : v.x);
-      }
-      if (p0 + p < a.npencils) {
-        phys(p0 + p, z, vin, vout);
-      } else {
-#pragma unroll
-        for (int g = 0; g < FO; ++g) vout[g] = (T)0;
-      }
-#pragma unroll
-      for (int g = 0; g < FO; ++g) {
-        const int r = g * P + p;
-        T* w = reinterpret_cast<T*>(W + (size_t)(r >> 1) * LS + z);
-        w[r & 1] = vout[g];
-      }
-      if ((FO * P) & 1) {  // odd count: the last packed line has no partner
-        if (p == P - 1) reinterpret_cast<T*>(W + (size_t)(nout - 1) * LS + z)[1] = (T)0;
-      }
-    }
-  }
+  zpass_physics<T, Phys>(a, phys, R, W, P, M, LS, p0, extra);
   if constexpr (FO > 0) {
     __syncthreads();
     Cx<T>* R2 = zfft<T, false, WIDE, FP>(W, R, a.plan, tw, nout);
@@ -755,6 +768,155 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_kernel(ZArg
   const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
   for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
     zpass_tile<T, Phys, WIDE, FP>(a, phys, (int)bx);
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z-pass with global memory on both sides of its transforms.  For a compiled
+// two-pass schedule (R1, R2) with R2 = 16 or 8 the inverse runs (R1, R2) and
+// the forward (R2, R1), so that both transforms' global-facing passes have R2
+// items per packed line, one per lane of an aligned R2-lane group:
+//  * inverse pass 1 loads its R1 elements of a packed line, positions
+//    j + R2 r, straight from the two pencils' stored spectra (Hermitian
+//    packing Z = A + iB, z derivatives i k3 u formed on load): the lanes of a
+//    group read R2 consecutive k3 of each pencil;
+//  * forward pass 2 hands its R1 results, positions j + R2 r, straight to the
+//    unpack A_q = (Z_q + conj Z_{M-q})/2, B_q = (Z_q - conj Z_{M-q})/(2i).
+//    For q = j + R2 r (j > 0), M - q = (R2 - j) + R2 (R1 - 1 - r): register
+//    R1 - 1 - r of lane R2 - j of the same group, fetched with a warp shuffle
+//    (lane 0 pairs with itself: M - R2 r is its register (R1 - r) mod R1).
+// A packed line's shared-memory traffic is the exchange inside each transform
+// and the physics' reads and writes; the packed spectra never pass through
+// shared memory.  P must be even (packed lines pair pencils p, p+1 of one
+// field).  smem and staging as zpass_kernel (zpass_smem_bytes, zpass_setup).
+template <int FP>
+struct zrr_plan {
+  using Pl = FixedPlan<FP>;
+  static constexpr int R1 = Pl::Radices::A, R2 = Pl::Radices::B, REV = fixed_plan_reversed(FP);
+  static constexpr bool value = Pl::Radices::NP == 2 && REV != 0 && (R2 == 16 || R2 == 8);
+};
+
+template <typename T, class Phys, int FP>
+__device__ __forceinline__ void zpass_rr_tile(const ZArgs<T>& a, const Phys& phys, int bx) {
+  static_assert(zrr_plan<FP>::value, "two-pass schedule (R1, 16 or 8) with its reverse compiled in");
+  constexpr int M = FixedPlan<FP>::L, R1 = zrr_plan<FP>::R1, R2 = zrr_plan<FP>::R2;
+  constexpr int FI = Phys::F_IN, FO = Phys::F_OUT;
+  static_assert(FI > 0 && FO > 0, "a z-pass with inputs and outputs");
+  constexpr int FMAX = FI > FO ? FI : FO;
+  constexpr int half = M / 2, LS = zline(M);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int P = a.ppc, hp = P >> 1;
+  const int nl = FMAX * hp;
+  Cx<T>* X = tw + M;
+  Cx<T>* Y = X + (size_t)nl * LS;
+  unsigned char* extra = reinterpret_cast<unsigned char*>(Y + (size_t)nl * LS);
+  const long long p0 = (long long)bx * P;
+  const Cx<T> zero = mk<T>(0, 0);
+  const int nin = FI * hp, nout = FO * hp;
+  const int gpc = blockDim.x / R2;  // line groups per CTA
+  const int j = threadIdx.x % R2, grp = threadIdx.x / R2;
+  // ---- inverse pass 1: packed spectra -> registers -> radix R1 -> X
+  for (int c = grp; c < nin; c += gpc) {
+    const int f = c / hp, p = 2 * (c - f * hp);
+    const long long pa = p0 + p;
+    const bool oka = pa < a.npencils, okb = pa + 1 < a.npencils;
+    const long long ps = a.in_pstride[f];
+    const Cx<T>* src = a.in[f] + (oka ? pa * ps : 0);
+    const int kz = min(a.in_kz[f], half + 1);
+    Cx<T> va[R1], vb[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int n = j + R2 * r;
+      const int m = n <= half ? n : M - n;
+      va[r] = (m < kz && oka) ? src[m] : zero;
+      vb[r] = (m < kz && okb) ? src[ps + m] : zero;
+    }
+    const bool dz = a.dz[f] != 0;
+    Cx<T> v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int n = j + R2 * r;
+      const bool lo = n <= half;
+      const int m = lo ? n : M - n;
+      Cx<T> A = va[r], B = vb[r];
+      if (dz) {
+        const T kk = m < kz ? (T)a.k3[m] : (T)0;
+        A = mk<T>(-kk * A.y, kk * A.x);
+        B = mk<T>(-kk * B.y, kk * B.x);
+      }
+      if (lo)
+        v[r] = (n == 0 || n == half) ? mk<T>(A.x, B.x) : mk<T>(A.x - B.y, A.y + B.x);
+      else
+        v[r] = mk<T>(A.x + B.y, B.x - A.y);
+    }
+    small_dft<T, R1, true>(v);
+    Cx<T>* Z = X + (size_t)c * LS + j * R1;
+#pragma unroll
+    for (int r = 0; r < R1; ++r) Z[r] = v[r];
+  }
+  __syncthreads();
+  // ---- inverse pass 2 (X -> Y), the physics (Y -> X), forward pass 1 (X -> Y)
+  if (nin >= 8)
+    stockham_pass_c<T, R2, true, M, R1, true>(X, Y, tw, nin, LS);
+  else
+    stockham_pass_c<T, R2, true, M, R1, false>(X, Y, tw, nin, LS);
+  __syncthreads();
+  zpass_physics<T, Phys>(a, phys, Y, X, P, M, LS, p0, extra);
+  __syncthreads();
+  if (nout >= 8)
+    stockham_pass_c<T, R2, false, M, 1, true>(X, Y, tw, nout, LS);
+  else
+    stockham_pass_c<T, R2, false, M, 1, false>(X, Y, tw, nout, LS);
+  __syncthreads();
+  // ---- forward pass 2: Y -> radix R1 (sub-transform length R2) -> unpack -> global.
+  // Every lane of a warp runs every round (the shuffles need the whole warp);
+  // lanes past the last line compute on zeros and store nothing.
+  const int lane = threadIdx.x & 31;
+  const int partner = (lane & ~(R2 - 1)) | ((R2 - j) & (R2 - 1));
+  const int kzo = a.out_kz;
+  for (int cb = 0; cb < nout; cb += gpc) {
+    const int c = cb + grp;
+    const bool act = c < nout;
+    Cx<T> v[R1];
+#pragma unroll
+    for (int r = 0; r < R1; ++r) v[r] = act ? Y[(size_t)c * LS + j + R2 * r] : zero;
+    // twiddles W_M^{r j} (sub-transform length R2: the table's stride is 1)
+#pragma unroll
+    for (int r = 1; r < R1; ++r) v[r] = cmul(v[r], tw[r * j]);
+    small_dft<T, R1, false>(v);
+    const int g = act ? c / hp : 0, p = 2 * (c - g * hp);
+    const long long pa = p0 + p;
+    const bool oka = act && pa < a.npencils, okb = act && pa + 1 < a.npencils;
+    const long long ps = a.out_pstride[g];
+    Cx<T>* dst = a.out[g] + (oka ? pa * ps : 0);
+#pragma unroll
+    for (int r = 0; r <= R1 / 2; ++r) {
+      if (R2 * r >= kzo) break;  // uniform over the warp
+      Cx<T> pv;
+      pv.x = __shfl_sync(0xffffffffu, v[R1 - 1 - r].x, partner);
+      pv.y = __shfl_sync(0xffffffffu, v[R1 - 1 - r].y, partner);
+      const Cx<T> zk = v[r];
+      const Cx<T> zm = j == 0 ? v[(R1 - r) % R1] : pv;
+      const int q = j + R2 * r;
+      if (q < kzo) {
+        if (oka) dst[q] = mk<T>((T)0.5 * (zk.x + zm.x), (T)0.5 * (zk.y - zm.y));
+        if (okb) dst[ps + q] = mk<T>((T)0.5 * (zk.y + zm.y), (T)0.5 * (zm.x - zk.x));
+      }
+    }
+  }
+}
+
+// Persistent register-direct z-pass (tiles as zpass_kernel).
+template <typename T, class Phys, int FP>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_rr_kernel(ZArgs<T> a, Phys phys) {
+  pdl_trigger();
+  zpass_setup<T, Phys>(a, phys);
+  pdl_wait();
+  const long long ntiles = (a.npencils + a.ppc - 1) / a.ppc;
+  for (long long bx = blockIdx.x; bx < ntiles; bx += gridDim.x) {
+    zpass_rr_tile<T, Phys, FP>(a, phys, (int)bx);
     __syncthreads();
   }
 }
