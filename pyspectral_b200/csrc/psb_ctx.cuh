@@ -414,6 +414,9 @@ int launch_z(psb_ctx* c, psb::ZArgs<T> z, Phys phys, const char* what, double ex
   if (sh && sh->tile) {
     P = sh->tile;
     z.plan = sh->plan;
+  } else if constexpr (psb::phys_fixed_fft<Phys>::value && sizeof(T) == 4) {
+    // default shape: the register-direct z pass where its schedule exists
+    if ((P & 1) == 0 && c->use_zrr) psb::zrr_default_plan(z.plan);
   }
   z.ppc = P;
   const size_t smem = smem_for(P);

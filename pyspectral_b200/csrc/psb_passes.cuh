@@ -797,6 +797,20 @@ struct zrr_plan {
   static constexpr bool value = Pl::Radices::NP == 2 && REV != 0 && (R2 == 16 || R2 == 8);
 };
 
+// The default schedule of a register-direct z pass of length p.L: the
+// compiled two-pass order (p.L / 16, 16) when there is one (48, 96, 192).
+__host__ inline bool zrr_default_plan(FFTPlan& p) {
+  for (const FixedDesc& d : kFixedDescs)
+    if (d.L == p.L && d.n == 2 && d.r[1] == 16 && fixed_plan_reversed(d.id) != 0) {
+      p.npass = 2;
+      p.radix[0] = d.r[0];
+      p.radix[1] = d.r[1];
+      for (int s = 2; s < kMaxPasses; ++s) p.radix[s] = 0;
+      return true;
+    }
+  return false;
+}
+
 template <typename T, class Phys, int FP>
 __device__ __forceinline__ void zpass_rr_tile(const ZArgs<T>& a, const Phys& phys, int bx) {
   static_assert(zrr_plan<FP>::value, "two-pass schedule (R1, 16 or 8) with its reverse compiled in");
