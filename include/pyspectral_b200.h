@@ -244,6 +244,27 @@ int psb_sgs_dns(psb_ctx* ctx, const void* fields3, void* w0, void* tau6);
 int psb_fft_r2c(psb_ctx* ctx, const void* phys, void* spec, int nfields);
 /* numpy irfftn (1/(N1N2N3)-normalised) of nfields spectra. */
 int psb_fft_c2r(psb_ctx* ctx, const void* spec, void* phys, int nfields);
+/* Slab-decomposed 3-D transforms of the MPI solver, FFTclass.myifft3D /
+ * myfft3D (src_MPI/Classes.py:244-258), for one rank of nprocs.  The rank holds
+ * the spectra of an x slab, (Npx, N2, Kz), and the physical field of a y slab,
+ * (N1, Npy, N3), with Npx = N1/nprocs, Npy = N2/nprocs, Kz = N3/2+1 (N1 and N2
+ * multiples of nprocs; ctx is a context of the whole N1 x N2 x N3 grid).
+ * Between the two halves of each transform the caller runs an all-to-all of
+ * nprocs equal blocks (block p of `send` to rank p, block p of `recv` from rank
+ * p), as the reference's comm.Alltoall does; one field per call.
+ *   psb_slab_ifft_y : uhat (Npx, N2, Kz) -> send (nprocs, Npx, Npy, Kz), the
+ *                     inverse DFT along y, block p = rank p's y rows
+ *   psb_slab_ifft_xz: recv (N1, Npy, Kz) -> u (N1, Npy, N3) real: inverse DFT
+ *                     along x, c2r along z, scaled by 1/(N1 N2 N3) (numpy's ifft
+ *                     and irfft2 normalisation together)
+ *   psb_slab_fft_xz : u (N1, Npy, N3) -> send (N1, Npy, Kz): r2c along z, DFT
+ *                     along x (unnormalised); block p = rank p's x rows
+ *   psb_slab_fft_y  : recv (nprocs, Npx, Npy, Kz) -> uhat (Npx, N2, Kz): the DFT
+ *                     along y (unnormalised) */
+int psb_slab_ifft_y(psb_ctx* ctx, int nprocs, const void* uhat, void* send);
+int psb_slab_ifft_xz(psb_ctx* ctx, int nprocs, const void* recv, void* u);
+int psb_slab_fft_xz(psb_ctx* ctx, int nprocs, const void* u, void* send);
+int psb_slab_fft_y(psb_ctx* ctx, int nprocs, const void* recv, void* uhat);
 /* Count of non-finite values in n complex entries -> *count (0 = all finite). */
 int psb_check_finite(psb_ctx* ctx, const void* data, long long n, long long* count);
 

@@ -1279,3 +1279,48 @@ def isotropic_state(N, seed, k0=4.0, u0=1.0, L=2 * np.pi, phases=None, normalise
     if normalise == "none":
         return st * np.sqrt(n3)
     return st
+
+
+# ---- slab-decomposed transforms of the MPI solver ---------------------------
+# FFTclass.myifft3D / myfft3D, src_MPI/Classes.py:244-258, split at the
+# Alltoall into the two local halves one rank computes.  A rank holds the x
+# slab (Npx, N2, N3/2+1) of the spectra and the y slab (N1, Npy, N3) of the
+# physical field; blocks are exchanged so that block p of a rank's send
+# buffer becomes block (this rank) of rank p's receive buffer.  The whole
+# 1/(N1 N2 N3) of numpy's ifft (axis 1) and irfft2 (axes 0, 2) is applied in
+# the second inverse half, the y half being an unnormalised inverse DFT (the
+# two forms are equal up to round-off).
+
+def slab_ifft_y(uhat, P):
+    """x slab (Npx, N2, K) -> send blocks (P, Npx, N2/P, K): inverse DFT along y
+    (src_MPI/Classes.py:245-246; the reshape/rollaxis of :246)."""
+    Npx, N2, K = uhat.shape
+    t = np.fft.ifft(uhat, axis=1) * N2
+    return np.ascontiguousarray(t.reshape(Npx, P, N2 // P, K).transpose(1, 0, 2, 3))
+
+
+def slab_ifft_xz(recv, N2, N3):
+    """received blocks (P, Npx, Npy, K) = (N1, Npy, K) -> y slab (N1, Npy, N3):
+    irfft2 over x and z (src_MPI/Classes.py:248), times 1/N2."""
+    P, Npx, Npy, K = recv.shape
+    return np.fft.irfft2(recv.reshape(P * Npx, Npy, K), s=(P * Npx, N3), axes=(0, 2)) / N2
+
+
+def slab_fft_xz(u):
+    """y slab (N1, Npy, N3) -> send (N1, Npy, N3/2+1): rfft2 over x and z
+    (src_MPI/Classes.py:252)."""
+    return np.fft.rfft2(u, axes=(0, 2))
+
+
+def slab_fft_y(recv):
+    """received blocks (P, Npx, Npy, K) -> x slab (Npx, P Npy, K): the
+    rollaxis/reshape of src_MPI/Classes.py:254, then the DFT along y (:255)."""
+    P, Npx, Npy, K = recv.shape
+    return np.fft.fft(recv.transpose(1, 0, 2, 3).reshape(Npx, P * Npy, K), axis=1)
+
+
+def slab_alltoall(sends):
+    """The Alltoall of one transform over all ranks' send buffers (lists of
+    (P, ...) arrays): rank r receives block r of every rank's send, in rank order."""
+    P = len(sends)
+    return [np.stack([sends[p][r] for p in range(P)]) for r in range(P)]

@@ -26,7 +26,8 @@ EXPORTS = (
     "psb_ctx_create", "psb_ctx_destroy", "psb_ctx_set_stream", "psb_last_error", "psb_create_error",
     "psb_rhs", "psb_step_rk4", "psb_step_si", "psb_prepare", "psb_energy", "psb_enstrophy", "psb_cross_helicity",
     "psb_spectrum", "psb_spectrum_nbins", "psb_transfer", "psb_spectrum_mpi", "psb_cfl_dt", "psb_sgs_dns",
-    "psb_fft_r2c", "psb_fft_c2r", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
+    "psb_fft_r2c", "psb_fft_c2r", "psb_slab_ifft_y", "psb_slab_ifft_xz", "psb_slab_fft_xz",
+    "psb_slab_fft_y", "psb_check_finite", "psb_launch_count", "psb_timing_enable",
     "psb_timing_count", "psb_timing_get", "psb_rhs_dns_noalloc", "psb_mlp_sizes", "psb_mlp_forward",
     "psb_mlp_forward_tc",
     "psb_mlp_grad", "psb_mlp_adam", "psb_physical_fields", "psb_products", "psb_spectral_resample",
@@ -88,6 +89,10 @@ def load(path: str = LIB_PATH):
         "psb_sgs_dns": ([vp, vp, vp, vp], i),
         "psb_fft_r2c": ([vp, vp, vp, i], i),
         "psb_fft_c2r": ([vp, vp, vp, i], i),
+        "psb_slab_ifft_y": ([vp, i, vp, vp], i),
+        "psb_slab_ifft_xz": ([vp, i, vp, vp], i),
+        "psb_slab_fft_xz": ([vp, i, vp, vp], i),
+        "psb_slab_fft_y": ([vp, i, vp, vp], i),
         "psb_check_finite": ([vp, vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], i),
         "psb_launch_count": ([vp, ctypes.POINTER(ctypes.c_ulonglong)], i),
         "psb_timing_enable": ([vp, i], i),
@@ -288,6 +293,23 @@ class Context:
     def c2r(self, spec, phys, nfields):
         self.bind_stream()
         self.check(self.lib.psb_fft_c2r(self.h, self._ptr(spec), self._ptr(phys), int(nfields)), "psb_fft_c2r")
+
+    # slab-decomposed transforms (one rank of nprocs; the caller exchanges the blocks)
+    def slab_ifft_y(self, nprocs, uhat, send):
+        self.bind_stream()
+        self.check(self.lib.psb_slab_ifft_y(self.h, int(nprocs), self._ptr(uhat), self._ptr(send)), "psb_slab_ifft_y")
+
+    def slab_ifft_xz(self, nprocs, recv, u):
+        self.bind_stream()
+        self.check(self.lib.psb_slab_ifft_xz(self.h, int(nprocs), self._ptr(recv), self._ptr(u)), "psb_slab_ifft_xz")
+
+    def slab_fft_xz(self, nprocs, u, send):
+        self.bind_stream()
+        self.check(self.lib.psb_slab_fft_xz(self.h, int(nprocs), self._ptr(u), self._ptr(send)), "psb_slab_fft_xz")
+
+    def slab_fft_y(self, nprocs, recv, uhat):
+        self.bind_stream()
+        self.check(self.lib.psb_slab_fft_y(self.h, int(nprocs), self._ptr(recv), self._ptr(uhat)), "psb_slab_fft_y")
 
     def autotune(self, closure, state, params):
         """Pick the fastest launch shapes of closure's RHS passes on `state`

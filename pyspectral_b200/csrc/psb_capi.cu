@@ -439,6 +439,153 @@ int r2c_impl(psb_ctx* c, const void* phys, void* spec, int nfields) {
   return PSB_OK;
 }
 
+// ---- slab-decomposed transforms of the MPI solver -------------------------
+// One rank of P holds the spectra of an x slab, (Npx, N2, N3/2+1), and the
+// physical field of a y slab, (N1, Npy, N3): FFTclass.myifft3D / myfft3D,
+// PySpectral/src_MPI/Classes.py:244-258.  Between the halves the caller runs
+// an all-to-all of equal blocks (block p of the send buffer to rank p).
+// Inverse: the DFT along y of the x slab is written in the blocked layout
+// (P, Npx, Npy, Kz) -- block p holds the rows of rank p's y slab -- so that
+// every block is contiguous; the block received from rank p holds p's x slab,
+// so the received buffer is (N1, Npy, Kz) in order, transformed along x and
+// (c2r) along z.  Forward: r2c along z and the DFT along x of the y slab give
+// (N1, Npy, Kz) = (P, Npx, Npy, Kz) in order; after the exchange block p holds
+// rank p's y rows, which the y pass reads blocked.
+template <typename T>
+struct SlabY {
+  const Cx<T>* in;
+  Cx<T>* out;
+  int N2, Npx, Npy, Kz, ct;
+  int blocked_out;  // 1: natural in, blocked out (inverse); 0: blocked in, natural out
+  FFTPlan plan;
+  const Cx<T>* tw;
+};
+
+// element (x, y, k3) of a slab: natural (Npx, N2, Kz) or blocked (P, Npx, Npy, Kz)
+template <typename T>
+__device__ __forceinline__ long long slab_off(const SlabY<T>& a, bool blocked, int x, int y, int k) {
+  if (!blocked) return ((long long)x * a.N2 + y) * a.Kz + k;
+  const int p = y / a.Npy, yy = y - p * a.Npy;
+  return (((long long)p * a.Npx + x) * a.Npy + yy) * a.Kz + k;
+}
+
+// grid (ceil(Kz/ct), Npx); a CTA transforms ct consecutive k3 columns of one
+// x along y (ct a power of two dividing the CTA); smem = (N2 + 2 N2 ct) complex
+template <typename T, bool INV>
+__global__ void __launch_bounds__(256) slab_y_kernel(SlabY<T> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Cx<T>* tw = reinterpret_cast<Cx<T>*>(smem_raw);
+  const int L = a.N2, ct = a.ct;
+  Cx<T>* bufA = tw + L;
+  Cx<T>* bufB = bufA + (size_t)L * ct;
+  const int x = blockIdx.y;
+  stage_twiddles(tw, a.tw, a.plan);
+  const int c = threadIdx.x % ct, r0 = threadIdx.x / ct, dr = blockDim.x / ct;
+  const int k = blockIdx.x * ct + c;
+  const bool ok = k < a.Kz;
+  const bool bin = a.blocked_out == 0;
+  for (int y = r0; y < L; y += dr) bufA[(size_t)y * ct + c] = ok ? a.in[slab_off(a, bin, x, y, k)] : mk<T>(0, 0);
+  __syncthreads();
+  const Cx<T>* res = block_fft<T, INV, false>(bufA, bufB, a.plan, tw, ct, 1, ct, true);
+  if (!ok) return;
+  for (int y = r0; y < L; y += dr) a.out[slab_off(a, !bin, x, y, k)] = res[(size_t)y * ct + c];
+}
+
+int slab_check(psb_ctx* c, int P, const char* what) {
+  if (P < 1 || c->N1 % P != 0 || c->N2 % P != 0)
+    return fail(c, PSB_ERR_SHAPE, std::string(what) + ": N1 and N2 must be multiples of nprocs");
+  return PSB_OK;
+}
+
+template <typename T>
+int slab_y_impl(psb_ctx* c, int P, const void* in, void* out, bool inverse) {
+  const size_t esz = sizeof(Cx<T>);
+  SlabY<T> a{};
+  a.in = reinterpret_cast<const Cx<T>*>(in);
+  a.out = reinterpret_cast<Cx<T>*>(out);
+  a.N2 = c->N2;
+  a.Npx = c->N1 / P;
+  a.Npy = c->N2 / P;
+  a.Kz = c->N3h;
+  a.blocked_out = inverse ? 1 : 0;
+  a.plan = *plan_for(c, c->N2);
+  a.tw = twiddles<T>(c);
+  a.ct = pick_ct(a.Kz, 1, a.N2, esz, a.Npx);
+  const size_t smem = (size_t)(a.N2 + 2 * (size_t)a.N2 * a.ct) * esz;
+  const dim3 grid((unsigned)((a.Kz + a.ct - 1) / a.ct), (unsigned)a.Npx);
+  const char* what = inverse ? "slab y-inverse" : "slab y-forward";
+  auto k = inverse ? slab_y_kernel<T, true> : slab_y_kernel<T, false>;
+  set_smem(k, smem);
+  LaunchScope scope(c, what, 2.0 * esz * a.Npx * a.N2 * a.Kz);
+  k<<<grid, 256, smem, c->stream>>>(a);
+  return launch_ok(c, what);
+}
+
+// x pass of a y slab (N1 rows x Npy outer x Kz columns, natural order)
+template <typename T>
+AxisArgs<T> slab_x_args(psb_ctx* c, int P, const Cx<T>* in, Cx<T>* out) {
+  const int N1 = c->N1, Npy = c->N2 / P, Kz = c->N3h;
+  AxisArgs<T> a{};
+  a.plan = *plan_for(c, N1);
+  a.tw = twiddles<T>(c);
+  a.scale = (T)1;
+  a.in = in;
+  a.out = out;
+  a.in_ostride = Kz;
+  a.in_rstride = (long long)Npy * Kz;
+  a.out_ostride = Kz;
+  a.out_rstride = (long long)Npy * Kz;
+  a.nouter = Npy;
+  a.ncols = Kz;
+  a.in_rows = N1;
+  a.out_rows = N1;
+  a.in_map = map_id(N1);
+  a.out_map = map_id(N1);
+  return a;
+}
+
+// received blocks (N1, Npy, Kz) -> physical y slab (N1, Npy, N3): inverse DFT
+// along x, c2r along z, the whole 1/(N1 N2 N3) of the reference's ifft/irfft2
+template <typename T>
+int slab_xz_inverse(psb_ctx* c, int P, const void* recv, void* phys) {
+  const int N1 = c->N1, Npy = c->N2 / P, N3 = c->N3, Kz = c->N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "slab.A", (size_t)N1 * Npy * Kz, &st);
+  if (st != PSB_OK) return st;
+  PSB_TRY((launch_axis<T, true>(c, slab_x_args<T>(c, P, reinterpret_cast<const Cx<T>*>(recv), A), PreCopy<T>{},
+                                "slab x-inverse")));
+  ZArgs<T> z{};
+  z.in[0] = A;
+  z.in_pstride[0] = Kz;
+  z.in_kz[0] = Kz;
+  z.out_kz = 0;
+  z.npencils = (long long)N1 * Npy;
+  z.fac = (T)(1.0 / ((double)N1 * c->N2 * N3));
+  z.plan = *plan_for(c, N3);
+  z.tw = twiddles<T>(c);
+  return launch_z<T>(c, z, PhysStoreReal<T>{reinterpret_cast<T*>(phys), N3}, "slab z c2r");
+}
+
+// physical y slab (N1, Npy, N3) -> send (N1, Npy, Kz): r2c along z, DFT along x
+template <typename T>
+int slab_xz_forward(psb_ctx* c, int P, const void* phys, void* send) {
+  const int N1 = c->N1, Npy = c->N2 / P, N3 = c->N3, Kz = c->N3h;
+  int st = PSB_OK;
+  Cx<T>* A = scratch<T>(c, "slab.A", (size_t)N1 * Npy * Kz, &st);
+  if (st != PSB_OK) return st;
+  ZArgs<T> z{};
+  z.out[0] = A;
+  z.out_pstride[0] = Kz;
+  z.out_kz = Kz;
+  z.npencils = (long long)N1 * Npy;
+  z.fac = (T)1;
+  z.plan = *plan_for(c, N3);
+  z.tw = twiddles<T>(c);
+  PSB_TRY(launch_z<T>(c, z, PhysLoadReal<T>{reinterpret_cast<const T*>(phys), N3}, "slab z r2c"));
+  return launch_axis<T, false>(c, slab_x_args<T>(c, P, A, reinterpret_cast<Cx<T>*>(send)), PreCopy<T>{},
+                               "slab x-forward");
+}
+
 template <typename T, int F>
 struct PhysStoreN {
   static constexpr int F_IN = F, F_OUT = 0;
@@ -1036,6 +1183,40 @@ int psb_fft_c2r(psb_ctx* c, const void* spec, void* phys, int nfields) {
   if (!phys || !spec || nfields <= 0) return fail(c, PSB_ERR_ARG, "psb_fft_c2r: bad argument");
   PSB_TRY(set_device(c));
   return c->prec == 64 ? c2r_impl<double>(c, spec, phys, nfields) : c2r_impl<float>(c, spec, phys, nfields);
+}
+
+int psb_slab_ifft_y(psb_ctx* c, int nprocs, const void* uhat, void* send) {
+  PSB_TRY(check_ctx(c));
+  if (!uhat || !send) return fail(c, PSB_ERR_ARG, "psb_slab_ifft_y: null argument");
+  PSB_TRY(slab_check(c, nprocs, "psb_slab_ifft_y"));
+  PSB_TRY(set_device(c));
+  return c->prec == 64 ? slab_y_impl<double>(c, nprocs, uhat, send, true)
+                        : slab_y_impl<float>(c, nprocs, uhat, send, true);
+}
+
+int psb_slab_ifft_xz(psb_ctx* c, int nprocs, const void* recv, void* u) {
+  PSB_TRY(check_ctx(c));
+  if (!recv || !u) return fail(c, PSB_ERR_ARG, "psb_slab_ifft_xz: null argument");
+  PSB_TRY(slab_check(c, nprocs, "psb_slab_ifft_xz"));
+  PSB_TRY(set_device(c));
+  return c->prec == 64 ? slab_xz_inverse<double>(c, nprocs, recv, u) : slab_xz_inverse<float>(c, nprocs, recv, u);
+}
+
+int psb_slab_fft_xz(psb_ctx* c, int nprocs, const void* u, void* send) {
+  PSB_TRY(check_ctx(c));
+  if (!u || !send) return fail(c, PSB_ERR_ARG, "psb_slab_fft_xz: null argument");
+  PSB_TRY(slab_check(c, nprocs, "psb_slab_fft_xz"));
+  PSB_TRY(set_device(c));
+  return c->prec == 64 ? slab_xz_forward<double>(c, nprocs, u, send) : slab_xz_forward<float>(c, nprocs, u, send);
+}
+
+int psb_slab_fft_y(psb_ctx* c, int nprocs, const void* recv, void* uhat) {
+  PSB_TRY(check_ctx(c));
+  if (!recv || !uhat) return fail(c, PSB_ERR_ARG, "psb_slab_fft_y: null argument");
+  PSB_TRY(slab_check(c, nprocs, "psb_slab_fft_y"));
+  PSB_TRY(set_device(c));
+  return c->prec == 64 ? slab_y_impl<double>(c, nprocs, recv, uhat, false)
+                        : slab_y_impl<float>(c, nprocs, recv, uhat, false);
 }
 
 int psb_check_finite(psb_ctx* c, const void* data, long long n, long long* count) {

@@ -4,9 +4,13 @@ Mirrors PySpectral/src_MPI: ``gridclass`` (Classes.py:177-236), ``FFTclass``
 (Classes.py:238-265), ``variables`` for ``turb_model='MHD'``
 (Classes.py:5-149), ``computeRHS_MHD`` (RHSfunctions.py:95-175),
 ``advanceQ_RK4`` (time_schemes.py:2-7) and the MHD diagnostics
-(Classes.py:269-448).  The slab decomposition and its Alltoall transposes are
-replaced by single-GPU pencil passes, so ``num_processes`` must be 1.
-Spectra are unnormalised ``rfftn`` results, as in the MPI solver.
+(Classes.py:269-448).  The right-hand sides run as single-GPU pencil passes
+(one run per GPU).  ``FFTclass`` also runs the reference's slab-decomposed
+transforms across ranks (``num_processes`` > 1 with a ``torch.distributed``
+process group as ``comm``): each rank holds an x slab of the spectra and a y
+slab of the physical field, and the Alltoall between the halves is
+``all_to_all_single`` (NCCL over NVLink on GPUs).  Spectra are unnormalised
+``rfftn`` results, as in the MPI solver.
 """
 from __future__ import annotations
 
@@ -68,7 +72,17 @@ class gridclass:
 
 class FFTclass:
     """``myfft3D`` (unnormalised rfftn) / ``myifft3D`` (normalised irfftn) and
-    the in-place 2/3-rule ``dealias``."""
+    the in-place 2/3-rule ``dealias``.
+
+    With ``num_processes`` = P > 1 the transforms are the reference's slab
+    decomposition (src_MPI/Classes.py:238-258): ``myifft3D(uhat, u)`` takes this
+    rank's x slab of the spectra, ``uhat`` (Npx, N2, N3/2+1), and returns its y
+    slab of the physical field, ``u`` (N1, Npy, N3), with Npx = N1/P and
+    Npy = N2/P; ``myfft3D(u, uhat)`` goes back.  ``comm`` is the
+    ``torch.distributed`` process group of the P ranks (None: the default
+    group) and ``mpi_rank`` this rank's index in it.  The local halves run in
+    the library (``psb_slab_*``); the exchange of P equal blocks between them
+    is one ``all_to_all_single`` per transform."""
 
     def __init__(self, N1, N2, N3, nthreads=1, fft_type=None, Npx=None, Npy=None, num_processes=1, comm=None,
                  mpi_rank=0, grid=None, precision=64):
@@ -76,20 +90,58 @@ class FFTclass:
         self.grid = grid
         self.precision = precision
         self._own = None
+        self.P = int(num_processes)
+        self.comm = comm
+        self.mpi_rank = int(mpi_rank)
+        if self.P > 1:
+            if N1 % self.P or N2 % self.P:
+                raise ValueError("N1 and N2 must be multiples of num_processes")
+            self.Npx, self.Npy = N1 // self.P, N2 // self.P
+            if (Npx is not None and Npx != self.Npx) or (Npy is not None and Npy != self.Npy):
+                raise ValueError("Npx, Npy must be N1/num_processes, N2/num_processes")
+            self._bufs = None
 
     def _ctx(self):
         if self.grid is not None:
             return self.grid.ctx(self.precision)
         if self._own is None:
-            self._own = _capi.Context(self.N1, self.N2, self.N3, precision=self.precision)
+            self._own = _capi.Context(self.N1, self.N2, self.N3, precision=self.precision,
+                                      device=torch.cuda.current_device())
         return self._own
 
+    def _exchange_buffers(self, device):
+        """send and recv blocks (P, Npx, Npy, N3/2+1) complex, allocated once."""
+        if self._bufs is None:
+            shape = (self.P, self.Npx, self.Npy, self.N3 // 2 + 1)
+            cd = _cdtype(self.precision)
+            self._bufs = (torch.empty(shape, dtype=cd, device=device), torch.empty(shape, dtype=cd, device=device))
+        return self._bufs
+
+    def _alltoall(self, send, recv):
+        """comm.Alltoall(send, recv): block p of send to rank p, block p of recv from rank p."""
+        import torch.distributed as dist
+        dist.all_to_all_single(torch.view_as_real(recv), torch.view_as_real(send), group=self.comm)
+
     def myfft3D(self, u, uhat):
-        self._ctx().r2c(u.contiguous(), uhat, 1)
+        if self.P == 1:
+            self._ctx().r2c(u.contiguous(), uhat, 1)
+            return uhat
+        send, recv = self._exchange_buffers(u.device)
+        ctx = self._ctx()
+        ctx.slab_fft_xz(self.P, u.contiguous(), send)
+        self._alltoall(send, recv)
+        ctx.slab_fft_y(self.P, recv, uhat)
         return uhat
 
     def myifft3D(self, uhat, u):
-        self._ctx().c2r(uhat.contiguous(), u, 1)
+        if self.P == 1:
+            self._ctx().c2r(uhat.contiguous(), u, 1)
+            return u
+        send, recv = self._exchange_buffers(uhat.device)
+        ctx = self._ctx()
+        ctx.slab_ifft_y(self.P, uhat.contiguous(), send)
+        self._alltoall(send, recv)
+        ctx.slab_ifft_xz(self.P, recv, u)
         return u
 
 

@@ -505,8 +505,76 @@ def gen_mpi_ns(N, seed):
     return out
 
 
+class _ThreadComm:
+    """One rank's view of a P-rank communicator whose ranks are threads of this
+    process: ``Alltoall(send, recv)`` hands block p of every rank's send buffer
+    to rank p (blocks in rank order), as MPI's Alltoall does."""
+
+    def __init__(self, rank, size, shared, barrier):
+        self.rank, self.size, self.shared, self.barrier = rank, size, shared, barrier
+
+    def Get_size(self):
+        return self.size
+
+    def Get_rank(self):
+        return self.rank
+
+    def Alltoall(self, send, recv):
+        self.shared[self.rank] = np.array(send).reshape(self.size, -1)
+        self.barrier.wait()
+        got = np.stack([self.shared[p][self.rank] for p in range(self.size)])
+        self.barrier.wait()
+        recv[...] = got.reshape(recv.shape)
+
+
+def gen_slab_fft(shape, seed, P):
+    """The MPI solver's slab-decomposed myifft3D / myfft3D (src_MPI/Classes.py:238-258)
+    run by P ranks (threads sharing a stand-in communicator) on the slabs of one
+    random field: per rank the physical y slab from its spectral x slab, and the
+    spectral x slab from its physical y slab."""
+    import threading
+    C = load_mpi()
+    N1, N2, N3 = shape
+    rng = np.random.default_rng(seed)
+    u = rng.standard_normal(shape)
+    uhat = np.fft.rfftn(u)
+    Npx, Npy = N1 // P, N2 // P
+    shared, barrier = [None] * P, threading.Barrier(P)
+    out = {"u": u, "uhat": uhat}
+    res, errs = {}, []
+
+    def rank(r):
+        try:
+            comm = _ThreadComm(r, P, shared, barrier)
+            fft = C.FFTclass(N1, N2, N3, 1, "numpy", Npx, Npy, P, comm, r)
+            ur = np.zeros((N1, Npy, N3))
+            fft.myifft3D(uhat[r * Npx:(r + 1) * Npx].copy(), ur)
+            uh = np.zeros((Npx, N2, N3 // 2 + 1), dtype=complex)
+            fft.myfft3D(u[:, r * Npy:(r + 1) * Npy].copy(), uh)
+            res[r] = (ur, uh)
+        except Exception as e:  # surfaced after the join
+            errs.append(e)
+            barrier.abort()
+
+    th = [threading.Thread(target=rank, args=(r,)) for r in range(P)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    if errs:
+        raise errs[0]
+    for r in range(P):
+        out[f"P{P}_r{r}_u"], out[f"P{P}_r{r}_uhat"] = res[r]
+    return out
+
+
 def main():
     os.makedirs(HERE, exist_ok=True)
+    d = {}
+    for P in (2, 4):
+        d.update(gen_slab_fft((16, 24, 12), 31, P))
+    np.savez_compressed(os.path.join(HERE, "slab_fft.npz"), **d)
+    print("slab fft", sorted(d.keys()))
     for N, seed in ((12, 11), (16, 5)):
         d = gen_serial(N, seed)
         np.savez_compressed(os.path.join(HERE, f"serial_N{N}.npz"), **d)
