@@ -368,6 +368,21 @@ struct Batch {
           launch_pdl(k, g, 256, sm, c->stream, (const ZArgs<T>*)az, (const Phys*)phys);
           return launch_ok(c, "batch z-fused");
         };
+        // a compiled two-pass (R1, 16) schedule with pencils paired: register-direct
+        if constexpr (phys_fixed_fft<Phys>::value && sizeof(T) == 4) {
+          if ((P & 1) == 0 && c->use_zrr) {
+            switch (fixed_plan_id(b->plan[2])) {
+#define PSB_FIXED_CASE(ID, ...)                                                   \
+  case ID:                                                                        \
+    if constexpr (zrr_plan<ID>::value && zrr_plan<ID>::R2 == 16) return go(zpass_rr_batch<T, Phys, ID>); \
+    break;
+              PSB_FIXED_PLANS(PSB_FIXED_CASE)
+#undef PSB_FIXED_CASE
+              default:
+                break;
+            }
+          }
+        }
         if constexpr (phys_fixed_fft<Phys>::value)
           return by_plan(
               2, [&](auto id) { return go(zpass_batch<T, Phys, false, decltype(id)::value>); },
@@ -555,9 +570,13 @@ int run_batch(psb_batch* b, int nsteps, bool tune, Pre pre0, Phys (*mkphys)(psb_
     PSB_TRY(cuda_ok(c, cudaMalloc(&b->arena, need), "batch scratch"));
     b->arena_bytes = need;
   }
-  if (b->plan[0].L == 0)
+  if (b->plan[0].L == 0) {
     default_shapes(b, BT::Fi, BT::Fb, Phys::F_IN, BT::Fo, BT::YPre::F_DST, BT::YP::groups, sizeof(Cx<T>),
                    phys_default_ppc<Phys>::value, (size_t)phys_is_block<Phys>::extra);
+    // the register-direct z pass's schedule where it exists (as for single runs)
+    if constexpr (phys_fixed_fft<Phys>::value && sizeof(T) == 4)
+      if ((b->tile[2] & 1) == 0 && c->use_zrr) zrr_default_plan(b->plan[2]);
+  }
   if (b->dirty) {
     PSB_TRY(x.build(pre0, mkphys, mkepi));
     b->dirty = false;

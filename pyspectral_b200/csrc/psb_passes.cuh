@@ -935,6 +935,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_rr_kernel(Z
   }
 }
 
+// Batched register-direct z pass: grid = (ceil(npencils/ppc), runs); run
+// blockIdx.y reads A[y], phys[y].
+template <typename T, class Phys, int FP>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    zpass_rr_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
+  const ZArgs<T>& a = A[blockIdx.y];
+  const Phys& ph = phys[blockIdx.y];
+  pdl_trigger();
+  zpass_setup<T, Phys>(a, ph);
+  pdl_wait();
+  zpass_rr_tile<T, Phys, FP>(a, ph, blockIdx.x);
+}
+
 // Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
 template <typename T, class Phys, bool WIDE, int FP = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
