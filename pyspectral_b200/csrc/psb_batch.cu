@@ -360,12 +360,14 @@ struct Batch {
       case 2: {
         const int P = b->tile[2];
         const long long np = (long long)d.M1 * d.M2;
-        dim3 g((unsigned)((np + P - 1) / P), R);
+        const long long items = (np + P - 1) / P * R;
         const size_t sm = smem_z(P);
+        // persistent over (run, tile): at most the resident CTAs of the device
         auto go = [&](auto k) {
           set_smem(k, sm);
+          const long long g = persistent_grid(k, sm, items);
           LaunchScope s(c, "batch z-fused", (double)R * esz * np * d.Kz * (Fb + Fo));
-          launch_pdl(k, g, 256, sm, c->stream, (const ZArgs<T>*)az, (const Phys*)phys);
+          launch_pdl(k, dim3((unsigned)g), 256, sm, c->stream, (const ZArgs<T>*)az, (const Phys*)phys, R);
           return launch_ok(c, "batch z-fused");
         };
         // a compiled two-pass (R1, 16) schedule with pencils paired: register-direct
@@ -632,8 +634,10 @@ struct EnsDesc {
   EnsGroup g[kEnsMaxGroups];
 };
 
+// staged: the z items' (group, run) whose twiddles and Phys extra the CTA's
+// shared memory holds (-1: none); a z item stages only when it changes.
 template <typename T, class Pre, class Phys, class Epi>
-__device__ __forceinline__ void ens_item(const EnsGroup& g, int pass, int stage, long long i) {
+__device__ __forceinline__ void ens_item(const EnsGroup& g, int q, int pass, int stage, long long i, int& staged) {
   using YP = pre_ypass<T, Pre>;
   using YPre = typename YP::type;
   const long long per = (long long)g.nx[pass] * g.ny[pass];
@@ -649,9 +653,17 @@ __device__ __forceinline__ void ens_item(const EnsGroup& g, int pass, int stage,
       axis_pass_body<T, true, YPre, true>(static_cast<const AxisArgs<T>*>(g.ay)[r],
                                           static_cast<const YPre*>(g.ypre)[r], bx, by);
       break;
-    case 2:
-      zpass_body<T, Phys, true>(static_cast<const ZArgs<T>*>(g.az)[r], static_cast<const Phys*>(g.phys)[r], bx);
+    case 2: {
+      const ZArgs<T>& a = static_cast<const ZArgs<T>*>(g.az)[r];
+      const Phys& ph = static_cast<const Phys*>(g.phys)[r];
+      const int key = q * 65536 + r;
+      if (key != staged) {
+        zpass_setup<T, Phys>(a, ph);
+        staged = key;
+      }
+      zpass_tile<T, Phys, true>(a, ph, bx);
       break;
+    }
     case 3:
       axis_pass_body<T, false, PreCopy<T>, true>(static_cast<const AxisArgs<T>*>(g.ayf)[r],
                                                  static_cast<const PreCopy<T>*>(g.cpy)[r], bx, by);
@@ -672,6 +684,7 @@ __global__ void __launch_bounds__(256, 2) ens_persistent_kernel(const EnsDesc* _
       for (int pass = 0; pass < 5; ++pass) {
         long long total = 0;
         for (int q = 0; q < ng; ++q) total += D->g[q].items[pass];
+        int staged = -1;  // the previous pass's items reused the shared memory
         for (long long it = blockIdx.x; it < total; it += gridDim.x) {
           long long i = it;
           int q = 0;
@@ -679,13 +692,13 @@ __global__ void __launch_bounds__(256, 2) ens_persistent_kernel(const EnsDesc* _
           const EnsGroup& g = D->g[q];
           switch (g.kind) {
             case kEnsDns:
-              ens_item<T, PreCopyN<T, 3>, PhysProducts<T>, EpiNS<T, false>>(g, pass, stage, i);
+              ens_item<T, PreCopyN<T, 3>, PhysProducts<T>, EpiNS<T, false>>(g, q, pass, stage, i, staged);
               break;
             case kEnsSmag:
-              ens_item<T, PreStrain<T>, PhysSmag<T>, EpiNS<T, true>>(g, pass, stage, i);
+              ens_item<T, PreStrain<T>, PhysSmag<T>, EpiNS<T, true>>(g, q, pass, stage, i, staged);
               break;
             default:
-              ens_item<T, PreGradXY<T>, PhysLearned<T, kActRelu, 32>, EpiNS<T, false>>(g, pass, stage, i);
+              ens_item<T, PreGradXY<T>, PhysLearned<T, kActRelu, 32>, EpiNS<T, false>>(g, q, pass, stage, i, staged);
               break;
           }
           __syncthreads();  // the next item reuses the shared memory

@@ -935,24 +935,44 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1) zpass_rr_kernel(Z
   }
 }
 
-// Batched register-direct z pass: grid = (ceil(npencils/ppc), runs); run
-// blockIdx.y reads A[y], phys[y].
-template <typename T, class Phys, int FP>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
-    zpass_rr_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
-  const ZArgs<T>& a = A[blockIdx.y];
-  const Phys& ph = phys[blockIdx.y];
+// Batched z passes, persistent: items (run, tile) = (it / ntiles, it % ntiles)
+// for it = blockIdx.x, + gridDim.x, ... < runs * ntiles (run-major, so that a
+// CTA's consecutive items share a run); a CTA stages the twiddles and the
+// Phys extra (the network's weights) again only when its run changes.  Every
+// run of a batch has the same shape (npencils, ppc, plan).
+template <typename T, class Phys, bool RR, bool WIDE, int FP>
+__device__ __forceinline__ void zpass_batch_body(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys,
+                                                 int runs) {
   pdl_trigger();
-  zpass_setup<T, Phys>(a, ph);
-  pdl_wait();
-  zpass_rr_tile<T, Phys, FP>(a, ph, blockIdx.x);
+  const long long ntiles = (A[0].npencils + A[0].ppc - 1) / A[0].ppc;
+  const long long total = ntiles * runs;
+  int staged = -1;
+  for (long long it = blockIdx.x; it < total; it += gridDim.x) {
+    const int r = (int)(it / ntiles);
+    const int bx = (int)(it - (long long)r * ntiles);
+    if (r != staged) {
+      zpass_setup<T, Phys>(A[r], phys[r]);
+      if (staged < 0) pdl_wait();
+      staged = r;
+    }
+    if constexpr (RR)
+      zpass_rr_tile<T, Phys, FP>(A[r], phys[r], bx);
+    else
+      zpass_tile<T, Phys, WIDE, FP>(A[r], phys[r], bx);
+    __syncthreads();  // the next item (or the next run's staging) reuses the shared memory
+  }
 }
 
-// Batched: grid = (ceil(npencils/ppc), runs); run blockIdx.y reads A[y], phys[y].
+template <typename T, class Phys, int FP>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    zpass_rr_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys, int runs) {
+  zpass_batch_body<T, Phys, true, false, FP>(A, phys, runs);
+}
+
 template <typename T, class Phys, bool WIDE, int FP = 0>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
-    zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys) {
-  zpass_body<T, Phys, WIDE, FP>(A[blockIdx.y], phys[blockIdx.y], blockIdx.x);
+    zpass_batch(const ZArgs<T>* __restrict__ A, const Phys* __restrict__ phys, int runs) {
+  zpass_batch_body<T, Phys, false, WIDE, FP>(A, phys, runs);
 }
 
 // Closures whose z-pass is compiled with the fixed schedules (the 3/2-padded
