@@ -424,7 +424,8 @@ __device__ __forceinline__ Cx<T>* fft_cs(Cx<T>* a, Cx<T>* b, const Cx<T>* __rest
 }
 
 // Schedules compiled in with their length (id, L, radices): the default
-// schedule of each common 3/2-padded length and two-pass orders of it.
+// schedule of each common 3/2-padded length (48, 72, 96, 192: grids of 32,
+// 48, 64 and 128 points) and two-pass orders of it.
 #define PSB_FIXED_PLANS(X) \
   X(1, 96, 8, 4, 3)        \
   X(2, 96, 16, 6)          \
@@ -438,8 +439,11 @@ __device__ __forceinline__ Cx<T>* fft_cs(Cx<T>* a, Cx<T>* b, const Cx<T>* __rest
   X(10, 96, 12, 8)         \
   X(11, 96, 8, 12)         \
   X(12, 48, 8, 6)          \
-  X(13, 48, 6, 8)
-constexpr int kFixedPlans = 13;
+  X(13, 48, 6, 8)          \
+  X(14, 72, 8, 3, 3)       \
+  X(15, 72, 6, 12)         \
+  X(16, 72, 12, 6)
+constexpr int kFixedPlans = 16;
 
 template <int ID>
 struct FixedPlan;

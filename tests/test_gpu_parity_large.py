@@ -32,7 +32,7 @@ NU, DT = 1e-3, 2e-3
 
 # compiled-in schedules (psb_fft.cuh PSB_FIXED_PLANS) by length
 FIXED = {96: [(8, 4, 3), (16, 6), (6, 16), (12, 8), (8, 12)], 192: [(8, 8, 3), (16, 12), (12, 16)],
-         48: [(8, 2, 3), (16, 3), (3, 16), (8, 6), (6, 8)]}
+         48: [(8, 2, 3), (16, 3), (3, 16), (8, 6), (6, 8)], 72: [(8, 3, 3), (6, 12), (12, 6)]}
 
 
 def _torch():
@@ -205,6 +205,21 @@ def test_128_smag_fp32_every_schedule():
     grid, main = _main(N, "smag", 32, st)
     assert rel(_rhs(torch, grid, main), ref) < TOL32
     assert _schedule_sweep(torch, grid, main, ref, TOL32, [192] * 5) >= 15
+
+
+def test_48_smag_fp32_every_schedule():
+    """48^3 Smagorinsky in FP32 (the ensemble's middle size): default shapes
+    and every compiled 72-point schedule in every pass, against the FP64
+    oracle at the FP32 bar."""
+    torch = _torch()
+    N = 48
+    st = orc.isotropic_state(N, 4, k0=3.0)
+    st32 = st.astype(np.complex64).astype(np.complex128)
+    g = orc.Grid.periodic(N)
+    ref = orc.rhs_smag(g, st32, orc.Params(nu=NU))[0]
+    grid, main = _main(N, "smag", 32, st)
+    assert rel(_rhs(torch, grid, main), ref) < TOL32
+    assert _schedule_sweep(torch, grid, main, ref, TOL32, [72] * 5) >= 15
 
 
 def test_128_learned_fp32_rhs_matches_oracle():
