@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--big-N", type=int, default=128,
                     help="also time the FP32 learned and Smagorinsky steps at this size (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of autotuned ones")
+    ap.add_argument("--tune-rounds", type=int, default=3,
+                    help="autotuner runs per path; their shape sets and the default are then timed as whole "
+                         "flushed RK4 steps and the fastest is kept (1: one tuner run, no whole-step check)")
     ap.add_argument("--profile", action="store_true",
                     help="run warmup+steps plain RK4 steps of the headline case and exit (for ncu captures)")
     ap.add_argument("--tune", action="store_true",
@@ -420,7 +423,7 @@ def run_ours(args):
         main = C.variables(0, tm, 0, 0, 0, 0, grid, st64[0], st64[1], st64[2], 0.0, 2e-3, 1e-3,
                            precision=precision, model=model if closure == "learned" else None)
         if closure in ("learned", "smag", "dns") and not args.no_tune:
-            autotune(main, grid)  # launch shapes timed on this state (state untouched)
+            autotune(main, grid, rounds=args.tune_rounds)  # shapes timed on this state (state untouched)
         grid.ctx(precision).prepare(main.closure_code())
         return grid, main
 
@@ -516,7 +519,7 @@ def run_ours(args):
             mb = C.variables(0, {"learned": "learned", "smag": 1}[cl], 0, 0, 0, 0, gridb, stb[0], stb[1],
                              stb[2], 0.0, 2e-3, 1e-3, precision=32, model=model if cl == "learned" else None)
             if not args.no_tune:
-                autotune(mb, gridb)
+                autotune(mb, gridb, rounds=args.tune_rounds)
             Kb = max(4, args.steps // 8)
             msb, _, gb = timed(gridb, mb, Kb, args.warmup)
             del gb
@@ -549,7 +552,10 @@ def run_ours(args):
                        "closure": args.closure, "l2": "flushed before every timed step (256 MiB write)",
                        "launch": "one CUDA graph per RK4 step", "parallelism": f"replicas x{world}",
                        "launch_shapes": "default" if args.no_tune else
-                       "autotuned per path (psb_autotune: tiles and radix orders timed on the state)"},
+                       (f"autotuned per path (psb_autotune: tiles and radix orders timed on the state; "
+                        f"{args.tune_rounds} tuner runs, their shape sets and the default then timed as whole "
+                        f"flushed RK4 steps, the fastest kept)" if args.tune_rounds > 1 else
+                        "autotuned per path (psb_autotune: tiles and radix orders timed on the state)")},
             "fp64_plain": {"value": value64, "ms_per_step": ms64 / K64, "closure": plain,
                            "ratio_headline_over_fp64_plain": value / value64, "e2e": e2e64},
             "like_for_like": lfl,
@@ -584,7 +590,7 @@ def run_profile(args):
     main = C.variables(0, tm, 0, 0, 0, 0, grid, st[0], st[1], st[2], 0.0, 2e-3, 1e-3, precision=32, model=model)
     if args.tune:
         from pyspectral_b200.RHSfunctions import autotune
-        autotune(main, grid)
+        autotune(main, grid, rounds=args.tune_rounds)
         print(json.dumps({"tuned_shapes": grid.ctx(32).tuned_shapes(main.closure_code())}))
     torch.cuda.synchronize()
     torch.cuda.profiler.start()  # ncu --profile-from-start off captures from here

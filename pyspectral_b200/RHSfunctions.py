@@ -130,10 +130,61 @@ def advanceQ_RK4(main, grid, myFFT=None, utilities=None):
         utilities.postAdvanceQ_hook(main, grid, myFFT)
 
 
-def autotune(main, grid):
+def autotune(main, grid, rounds=1, confirm_steps=40, flush_bytes=256 << 20):
     """Tune the launch shapes of main's closure on its current state (no
-    reference counterpart; DNS, Smagorinsky and the learned closure)."""
-    grid.ctx(main.precision).autotune(main.closure_code(), main.Q, main.params())
+    reference counterpart; DNS, Smagorinsky and the learned closure).
+
+    The tuner ranks each pass's candidates by that pass's own launch time,
+    which its neighbours' overlap and the timing noise blur; its pick varies
+    by a few percent of the step between calls.  With ``rounds`` > 1 it runs
+    ``rounds`` times from the default shapes, and the distinct shape sets it
+    returns, plus the default, are then timed as whole RK4 steps
+    (``confirm_steps`` steps each, one at a time on a copy of the state, L2
+    flushed with a ``flush_bytes`` write before every step and left out of
+    the timing; sets interleaved, median per set); the fastest set is kept.
+    The state is untouched.  Returns the kept set's median ms per step (None
+    for rounds = 1)."""
+    ctx = grid.ctx(main.precision)
+    code = main.closure_code()
+    if rounds <= 1:
+        ctx.autotune(code, main.Q, main.params())
+        return None
+    sets = []
+    for _ in range(rounds):
+        ctx.autotune_clear(code)
+        ctx.autotune(code, main.Q, main.params())
+        s = ctx.tuned_shapes(code)
+        if s not in sets:
+            sets.append(s)
+    ctx.autotune_clear(code)
+    sets.append(ctx.tuned_shapes(code))  # the default shapes (tile 0: per-pass default)
+    q = main.Q.clone()
+    u = main.U.clone()
+    comp = main.comp.clone() if main.comp is not None else None
+    p = main.params()
+    flush = torch.empty(max(1, flush_bytes // 4), dtype=torch.float32, device=main.Q.device)
+    times = [[] for _ in sets]
+    for _ in range(confirm_steps):
+        for i, s in enumerate(sets):
+            ctx.autotune_clear(code)
+            if any(x["tile"] for x in s):
+                ctx.set_tuned_shapes(code, [x if x["tile"] else None for x in s])
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            ctx.step(code, q, p, 1, comp=comp, read_out=u)
+            b.record()
+            times[i].append((a, b))
+            q.copy_(main.Q)  # every set steps the same state
+            if comp is not None:
+                comp.copy_(main.comp)
+    torch.cuda.synchronize()
+    med = [float(torch.tensor([a.elapsed_time(b) for a, b in t]).median()) for t in times]
+    best = min(range(len(sets)), key=lambda i: med[i])
+    ctx.autotune_clear(code)
+    if any(x["tile"] for x in sets[best]):
+        ctx.set_tuned_shapes(code, [x if x["tile"] else None for x in sets[best]])
+    return med[best]
 
 
 def advance(main, grid, nsteps):
