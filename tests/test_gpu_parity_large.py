@@ -164,6 +164,32 @@ def test_les64_fp64_default_tuned_and_every_schedule(closure):
     assert _schedule_sweep(torch, grid, main, ref, TOL64, [96] * 5) >= 25
 
 
+def test_autotune_rounds_keeps_state_and_parity():
+    """autotune(rounds=3) -- three tuner runs, their shape sets and the default
+    timed as whole flushed RK4 steps on a copy of the state -- leaves the state
+    and its compensation array untouched and keeps a set under which the
+    learned 64^3 FP32 RHS and one RK4 step still match the oracle."""
+    torch = _torch()
+    from pyspectral_b200.learned import MLPModel
+    from pyspectral_b200.RHSfunctions import advanceQ_RK4, autotune
+    N = 64
+    P, nrm, act = _shipped()
+    model = MLPModel.load()
+    st = orc.isotropic_state(N, 2, k0=4.0)
+    st32 = st.astype(np.complex64).astype(np.complex128)  # what the FP32 run holds
+    g, rhs_fn = _learned_ref(N, st32, P, nrm, act)
+    ref = rhs_fn(st32)
+    grid, main = _main(N, "learned", 32, st, model=model)
+    q0, c0 = main.Q.clone(), main.comp.clone()
+    ms = autotune(main, grid, rounds=3, confirm_steps=8)
+    assert ms is not None and ms > 0
+    assert torch.equal(main.Q, q0) and torch.equal(main.comp, c0)
+    assert rel(_rhs(torch, grid, main), ref) < TOL_LEARNED
+    advanceQ_RK4(main, grid, None, None)
+    Q1, _ = orc.advance_rk4(st32, lambda q: (rhs_fn(q), None), DT)
+    assert rel(np_(main.Q).astype(np.complex128) - st32, Q1 - st32) < 1e-3
+
+
 def test_les64_tmodel_fp64_rhs_and_step():
     """t-model at 64^3 (2x grid: 128-point transforms), FP64, t != 0."""
     torch = _torch()
