@@ -231,11 +231,32 @@ def sgs_samples(ctx_dns, ctx_les, uhat, precision=32):
     Pb = filtered_state(P, N, n, precision)
     fuu = torch.cat([physical(ctx_les, Pb[0:3].contiguous(), 0), physical(ctx_les, Pb[3:6].contiguous(), 0)])
     u = f12[0:3]
-    pairs = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
-    tau = torch.stack([fuu[m] - u[a] * u[b] for m, (a, b) in enumerate(pairs)])
+    tau = torch.stack([fuu[m] - u[a] * u[b] for m, (a, b) in enumerate(PAIRS)])
     delta = 2 * math.pi / n
     X = torch.cat([f12[3:12].reshape(9, -1), torch.full((1, n ** 3), delta, device=uhat.device, dtype=f12.dtype)])
     return X.t().float().contiguous(), tau.reshape(6, -1).t().float().contiguous()
+
+
+PAIRS = ((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))
+
+
+def eddy_targets(X, T, eps=1e-30):
+    """Targets of the eddy-viscosity form: per sample the least-squares eddy
+    viscosity of the filtered stress, nu_t = max(0, -(tau:S) / (2 S:S)), and
+    the stress -2 nu_t S it implies (S_ij = (du_i/dx_j + du_j/dx_i)/2 from the
+    9 gradient features, X[:, 3i+j] = du_i/dx_j; components in the order of T,
+    (00, 11, 22, 01, 02, 12)).  The stress keeps the local energy transfer
+    -tau:S of the data where it is forward (nu_t > 0) and drops backscatter
+    and the part of tau not aligned with S; its trace is zero (the trace of
+    tau is a pressure and leaves the projected RHS unchanged)."""
+    G = X[:, :9].double().reshape(-1, 3, 3)
+    S = 0.5 * (G + G.transpose(1, 2))
+    S6 = torch.stack([S[:, a, b] for a, b in PAIRS], 1)
+    w = torch.tensor([1.0, 1.0, 1.0, 2.0, 2.0, 2.0], dtype=S6.dtype, device=S6.device)
+    tS = (T.double() * S6 * w).sum(1)
+    SS = (S6 * S6 * w).sum(1)
+    nu_t = torch.clamp(-tS / (2.0 * SS + eps), min=0.0)
+    return (-2.0 * nu_t[:, None] * S6).float().contiguous()
 
 
 # ---------------------------------------------------------------------------
@@ -350,6 +371,8 @@ def main():
     ap.add_argument("--nu", type=float, default=5e-4, help="viscosity of the DNS and the LES")
     ap.add_argument("--act", choices=sorted(ACTS), default="relu", help="hidden activation of the network")
     ap.add_argument("--hidden", type=int, choices=(32, 64), default=NH, help="hidden width of the network")
+    ap.add_argument("--target", choices=("stress", "eddy"), default="stress",
+                    help="fit the filtered stress itself, or its eddy-viscosity form (eddy_targets)")
     ap.add_argument("--eval-only", action="store_true",
                     help="re-run the a-posteriori evaluation of the model at --out and update its metadata")
     a = ap.parse_args()
@@ -366,6 +389,8 @@ def main():
     print("generating training data ...")
     X, T = generate(N_dns=a.N_dns, nu=a.nu, npoints=a.npoints)
     print(f"  {X.shape[0]} samples ({time.time() - t0:.1f} s)")
+    if a.target == "eddy":
+        T = eddy_targets(X, T)
     model = MLPModel(seed=0, act=a.act, hidden=a.hidden)
     model.fit_norm(X, T)
     ctx = _capi.Context(64, 64, 64, precision=32)
@@ -374,7 +399,7 @@ def main():
         print(f"  step {s:6d}  loss {l:.5f}")
     meta = {"train_samples": int(X.shape[0]), "train_steps": a.steps, "batch": a.batch,
             "final_loss": hist[-1][1] if hist else None, "N_dns": a.N_dns, "nu": a.nu, "act": a.act,
-            "hidden": a.hidden,
+            "hidden": a.hidden, "target": a.target,
             "spectrum": "E(k)=16 sqrt(2/pi) u0^2 k^4/k0^5 exp(-2 k^2/k0^2), k0=4, u0=1"}
     model.meta = meta
     if not a.no_eval:
