@@ -16,8 +16,9 @@ the filtered 256^3 DNS, as recorded with the shipped model.
   excluded from the timing; max over ranks; whole-job aggregate.
 * e2e: the same metric through the public API with the state copied from
   pinned host memory before every step and the new state read back after it
-  (copies on a second stream, overlapping the neighbouring steps' compute;
-  no L2 flush between these steps: each upload replaces the state).
+  (uploads and read-backs on two more streams, overlapping the neighbouring
+  steps' compute and each other; no L2 flush between these steps: each upload
+  replaces the state).
 * roofline: dominant kernel of the step, its compulsory bytes per launch over
   its CUDA-event duration, against MEASURED_PEAKS.json; every kernel's GB/s
   and fraction beside it.
@@ -338,8 +339,8 @@ def roofline_of(per, nsteps, step_ms):
 def e2e_measure(grid, main_a, graph_a, main_b, K, dist=None):
     """The step through the public API with host buffers: every step uploads
     its state (and Kahan compensation) from pinned host memory and reads the
-    new state back, on a copy stream overlapping the neighbouring steps'
-    compute (two device state buffers).  Returns (ms for K steps, h2d bytes
+    new state back, on two copy streams (uploads, read-backs) overlapping the
+    neighbouring steps' compute and each other (two device state buffers).  Returns (ms for K steps, h2d bytes
     per step, d2h bytes per step)."""
     import torch
     from pyspectral_b200.RHSfunctions import StepGraph
@@ -353,24 +354,29 @@ def e2e_measure(grid, main_a, graph_a, main_b, K, dist=None):
         hostc.copy_(main_a.comp.cpu())
     outs = [torch.empty_like(host).pin_memory() for _ in range(2)]
     comp_s = torch.cuda.current_stream()
-    copy_s = torch.cuda.Stream()
+    h2d_s = torch.cuda.Stream()  # uploads and read-backs on separate streams: both link directions at once
+    d2h_s = torch.cuda.Stream()
     ev_in = [torch.cuda.Event() for _ in range(2)]
     ev_done = [torch.cuda.Event() for _ in range(2)]
+    ev_read = [torch.cuda.Event() for _ in range(2)]
 
     def upload(k):
         b = k % 2
-        with torch.cuda.stream(copy_s):
+        with torch.cuda.stream(h2d_s):
+            if k >= 2:
+                h2d_s.wait_event(ev_read[b])  # buffer b's read-back of step k-2 has finished
             mains[b].Q.copy_(host, non_blocking=True)
             if hostc is not None:
                 mains[b].comp.copy_(hostc, non_blocking=True)
-            ev_in[b].record(copy_s)
+            ev_in[b].record(h2d_s)
 
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(comp_s)
-    copy_s.wait_stream(comp_s)
+    h2d_s.wait_stream(comp_s)
+    d2h_s.wait_stream(comp_s)
     upload(0)
     for k in range(K):
         b = k % 2
@@ -378,11 +384,13 @@ def e2e_measure(grid, main_a, graph_a, main_b, K, dist=None):
         graphs[b].replay()
         ev_done[b].record(comp_s)
         if k + 1 < K:
-            upload(k + 1)  # buffer (k+1)%2 is free: its read-back of step k-1 precedes on copy_s
-        with torch.cuda.stream(copy_s):
-            copy_s.wait_event(ev_done[b])
+            upload(k + 1)
+        with torch.cuda.stream(d2h_s):
+            d2h_s.wait_event(ev_done[b])
             outs[b].copy_(mains[b].Q, non_blocking=True)
-    comp_s.wait_stream(copy_s)
+            ev_read[b].record(d2h_s)
+    comp_s.wait_stream(h2d_s)
+    comp_s.wait_stream(d2h_s)
     e1.record(comp_s)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
@@ -485,8 +493,9 @@ def run_ours(args):
     e2e_ms, h2d, d2h = e2e_measure(grid32, m32, g32, m32b, Ke, dist)
     e2e = {"value": world * N ** 3 * Ke / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h,
-           "how": "pinned host state uploaded and the new state read back every step, on a copy stream "
-                  "overlapping the previous step's compute (two device state buffers)"}
+           "how": "pinned host state uploaded and the new state read back every step, on two copy streams "
+                  "(uploads, read-backs) overlapping the neighbouring steps' compute and each other (two device "
+                  "state buffers)"}
     # the same for the plain FP64 path (like for like with the reference arm)
     m64b = C.variables(0, {"smag": 1, "dns": 0}[plain], 0, 0, 0, 0, grid64, st64[0], st64[1], st64[2], 0.0,
                        2e-3, 1e-3, precision=64)

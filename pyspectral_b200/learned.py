@@ -16,9 +16,15 @@ Smagorinsky model of PySpectral/src/RHSfunctions.py:195-212 approximates.
 * Deployment: closure PSB_LEARNED (``variables(..., turb_model='learned')``)
   evaluates the MLP on tensor cores inside the fused z-pass of every RHS.
 
-Command line (the config-4 pipeline; several minutes on one B200):
+* Targets: the filtered stress itself (--target stress), or its
+  eddy-viscosity form (--target eddy, the default: eddy_targets), which keeps
+  the local forward energy transfer of the data and drops backscatter and the
+  part of the stress not aligned with the resolved strain.
 
-    python -m pyspectral_b200.learned --out pyspectral_b200/models/sgs_mlp.npz
+Command line (the config-4 pipeline; about four minutes on one B200; the
+shipped model models/sgs_mlp.npz was made by):
+
+    python -m pyspectral_b200.learned --out pyspectral_b200/models/sgs_mlp.npz --hidden 32 --act relu --target eddy
 """
 from __future__ import annotations
 
@@ -371,7 +377,7 @@ def main():
     ap.add_argument("--nu", type=float, default=5e-4, help="viscosity of the DNS and the LES")
     ap.add_argument("--act", choices=sorted(ACTS), default="relu", help="hidden activation of the network")
     ap.add_argument("--hidden", type=int, choices=(32, 64), default=NH, help="hidden width of the network")
-    ap.add_argument("--target", choices=("stress", "eddy"), default="stress",
+    ap.add_argument("--target", choices=("stress", "eddy"), default="eddy",
                     help="fit the filtered stress itself, or its eddy-viscosity form (eddy_targets)")
     ap.add_argument("--eval-only", action="store_true",
                     help="re-run the a-posteriori evaluation of the model at --out and update its metadata")

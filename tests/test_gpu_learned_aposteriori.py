@@ -7,16 +7,17 @@ src/RHSfunctions.py:146-237) and no model (FP32) for 400 RK4 steps
 (dt = 4e-3) while the DNS advances to the same time; E(k) of each LES is
 compared with the filtered DNS for 1 <= k <= 16 (k_c/2).
 
-Asserted (what holds): every run stays finite; the learned closure drains
-resolved energy as a subgrid model must (its LES ends with less energy than
-the LES without a model); it follows the large scales (E(k) within 15% for
-k <= 3); and the error of every run is recorded next to the others.  Measured
-on a B200 with this case, mean / max relative E(k) error over k = 1..16:
-learned 0.42 / 0.68, Smagorinsky 0.19 / 0.42, no model 0.28 / 0.56 -- the
-network, trained a priori on stresses of a 256^3 DNS, over-dissipates the
-middle wavenumbers (k = 5..13 at -0.5 to -0.7) and is the worst of the three
-here; its a-priori gain (stress error and dissipation correlation against no
-model on an unseen DNS) is tested in test_gpu_learned.py.
+Asserted (what holds): every run stays finite; the learned closure follows
+the large scales (E(k) within 15% for k <= 3); its mean E(k) error is below
+that of the LES without a model (what the network gains a posteriori) and
+within 10% of Smagorinsky's or below it (the same E(k) error as the plain
+closure).  Measured on a B200 with this case and the shipped network (trained
+to the eddy-viscosity form of the filtered stress of a 256^3 DNS), mean / max
+relative E(k) error over k = 1..16: learned 0.17 / 0.38, Smagorinsky
+0.19 / 0.42, no model 0.28 / 0.55.  (A network trained to the stress itself,
+models/sgs_mlp_stress.npz, measured 0.42 / 0.68 here: it left the middle
+wavenumbers 50-70% short of the filtered DNS, as the run without a model
+does.)  Its a-priori gain is tested in test_gpu_learned.py.
 """
 import numpy as np
 import pytest
@@ -37,8 +38,10 @@ def test_learned_closure_a_posteriori_against_filtered_dns():
         assert np.isfinite(r[k]["mean_rel_err"]) and np.isfinite(r[k]["max_rel_err_k_le_kc_half"])
     Eref = np.array(r["E_ref"])
     E = {k: np.array(r[k]["E"]) for k in names}
-    # a subgrid closure removes resolved energy: less than without a model
-    assert E["learned_fp32"].sum() < E["no_model_fp32"].sum()
+    err = {k: r[k]["mean_rel_err"] for k in names}
+    # what the network gains over the method without it, and the plain closure's error
+    assert err["learned_fp32"] < err["no_model_fp32"], err
+    assert err["learned_fp32"] <= 1.1 * err["smagorinsky_fp64"], err
     # the large scales follow the filtered DNS
     low = np.abs(E["learned_fp32"][1:4] - Eref[1:4]) / Eref[1:4]
     assert low.max() < 0.15, low
