@@ -271,11 +271,15 @@ def accuracy_record(closure, model):
         return None
     ev = model.meta["eval"]
     out = {"what": f"max/mean relative E(k) error for 1<=k<={ev['k_compare']} vs the {ev['N_dns']}^3 DNS "
-                   f"sharp-cutoff filtered to {ev['n_les']}^3, LES from t={ev['t0']} to t={ev['t_end']}",
-           "source": "model metadata (pyspectral_b200/models/sgs_mlp.json)"}
+                   f"sharp-cutoff filtered to {ev['n_les']}^3, LES from t={ev['t0']} to t={ev['t_end']} "
+                   f"(at the end; mean_over_run: the mean error averaged over the run's samples)",
+           "source": "model metadata (pyspectral_b200/models/sgs_mlp.json)",
+           "target": model.meta.get("target", "stress")}
     for k in ("learned_fp32", "smagorinsky_fp64", "smagorinsky_fp32", "no_model_fp32"):
         if k in ev:
-            out[k] = {"max": ev[k]["max_rel_err_k_le_kc_half"], "mean": ev[k]["mean_rel_err"]}
+            hist = [h["mean"] for h in ev[k].get("history", [])]
+            out[k] = {"max": ev[k]["max_rel_err_k_le_kc_half"], "mean": ev[k]["mean_rel_err"],
+                      "mean_over_run": sum(hist) / len(hist) if hist else None}
     return out
 
 
